@@ -1,0 +1,1052 @@
+// am_context.cu -- the C ABI (include/aperi_b200.h): context set-up, layout
+// building, the stream-ordered time loop and the checkpointed adjoint.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/aperi_b200.h"
+#include "am_host.hpp"
+#include "am_kernels.cuh"
+
+namespace {
+
+struct AmError {
+    int code;
+    std::string msg;
+};
+
+[[noreturn]] void fail(int code, const std::string& msg) { throw AmError{code, msg}; }
+
+void ck(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return;
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        fail(AM_ENOMEM, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+    fail(AM_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+T* dalloc(size_t count, const char* what) {
+    void* p = nullptr;
+    if (count == 0) return nullptr;
+    ck(cudaMalloc(&p, count * sizeof(T)), what);
+    return static_cast<T*>(p);
+}
+
+template <typename T>
+void dfree(T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+struct Block {
+    int32_t kind = 0;
+    int32_t material = 0;
+    double lambda = 0, mu = 0, density = 0;
+    int64_t num_elems = 0;
+    int64_t num_entries = 0;  // slots of this block
+    int64_t slot_base = 0;
+    int32_t* conn = nullptr;
+    double* mu_field = nullptr;
+    double* kappa_field = nullptr;
+    int32_t* cell_ptr = nullptr;
+    int32_t* cell_nodes = nullptr;
+    double* grads64 = nullptr;
+    float* grads32 = nullptr;
+    double* volumes = nullptr;
+    int32_t max_entries = 0;
+    std::vector<int32_t> host_nodes;  // per slot, for the node CSR
+
+    am::GaussBlockDev gauss() const {
+        am::GaussBlockDev g{};
+        g.kind = kind;
+        g.material = material;
+        g.lambda = lambda;
+        g.mu = mu;
+        g.num_elems = num_elems;
+        g.conn = conn;
+        g.mu_field = mu_field;
+        g.kappa_field = kappa_field;
+        g.slot_base = slot_base;
+        return g;
+    }
+    am::CellBlockDev cells() const {
+        am::CellBlockDev c{};
+        c.material = material;
+        c.lambda = lambda;
+        c.mu = mu;
+        c.num_cells = num_elems;
+        c.ptr = cell_ptr;
+        c.nodes = cell_nodes;
+        c.grads64 = grads64;
+        c.grads32 = grads32;
+        c.volumes = volumes;
+        c.mu_field = mu_field;
+        c.kappa_field = kappa_field;
+        c.slot_base = slot_base;
+        c.max_entries = max_entries;
+        return c;
+    }
+    void release() {
+        dfree(conn);
+        dfree(mu_field);
+        dfree(kappa_field);
+        dfree(cell_ptr);
+        dfree(cell_nodes);
+        dfree(grads64);
+        dfree(grads32);
+        dfree(volumes);
+    }
+};
+
+}  // namespace
+
+struct am_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int64_t N = 0;
+    double4* X4 = nullptr;
+    double4* U4 = nullptr;
+    double4* V4 = nullptr;
+    double4* A4 = nullptr;
+    double4* W4 = nullptr;  // scratch nodal vector (external u)
+    double4* L4 = nullptr;  // cotangent / external lambda
+    double* mass = nullptr;
+    uint32_t* bcword = nullptr;
+    double* bcvalues = nullptr;
+    int* status = nullptr;
+    double* f_scratch = nullptr;   // N x 3
+    double* io_scratch = nullptr;  // N x 3 host<->device staging
+    int32_t* node_ptr = nullptr;
+    int32_t* node_slots = nullptr;
+    double* slots64 = nullptr;
+    float* slots32 = nullptr;
+    int64_t num_slots = 0;
+    am::StepParams* table = nullptr;
+    int64_t table_cap = 0;
+    am::StepParams* table_host = nullptr;  // pinned staging
+    std::vector<Block> blocks;
+    std::vector<am::host::BoundaryCondition> bcs;
+    double g[3] = {0, 0, 0};
+    bool finalized = false;
+    bool mass_set = false;
+    std::string err;
+    int64_t launches = 0;
+    bool profiling = false;
+    double prof_ms[3] = {0, 0, 0};
+    int64_t prof_launches[3] = {0, 0, 0};
+    std::vector<cudaEvent_t> events;
+
+    am::NodeDev node_dev() const {
+        am::NodeDev nd{};
+        nd.num_nodes = N;
+        nd.node_ptr = node_ptr;
+        nd.node_slots = node_slots;
+        nd.mass = mass;
+        nd.bcword = bcword;
+        nd.bcvalues = bcvalues;
+        nd.g[0] = g[0];
+        nd.g[1] = g[1];
+        nd.g[2] = g[2];
+        nd.has_g = (g[0] != 0.0 || g[1] != 0.0 || g[2] != 0.0) ? 1 : 0;
+        return nd;
+    }
+
+    int64_t total_elems() const {
+        int64_t t = 0;
+        for (const auto& b : blocks) t += b.num_elems;
+        return t;
+    }
+
+    void* slots(int mixed) {
+        if (mixed) {
+            if (!slots32) slots32 = dalloc<float>(static_cast<size_t>(num_slots) * 3, "slot buffer (FP32)");
+            return slots32;
+        }
+        return slots64;
+    }
+
+    void check_launch(const char* what) {
+        ck(cudaGetLastError(), what);
+    }
+
+    // Element/cell force kernels of every block into the slot buffer.
+    void element_forces(int mixed, const double4* U) {
+        void* s = slots(mixed);
+        for (const auto& b : blocks) {
+            if (b.kind == AM_SMOOTHED_CELLS) {
+                if (mixed && !b.grads32) fail(AM_ESTATE, "mixed precision needs FP32 cell gradients");
+                am::launch_cell_force(b.cells(), mixed, U, s, status, stream);
+            } else {
+                am::launch_gauss_force(b.gauss(), mixed, X4, U, s, status, stream);
+            }
+            ++launches;
+        }
+        check_launch("element force kernel");
+    }
+
+    void vjp(const double4* U, const double4* L, double* gmu, double* gkappa, int accumulate) {
+        int64_t off = 0;
+        for (const auto& b : blocks) {
+            double* gm = gmu ? gmu + off : nullptr;
+            double* gk = gkappa ? gkappa + off : nullptr;
+            if (b.kind == AM_SMOOTHED_CELLS)
+                am::launch_cell_vjp(b.cells(), U, L, slots64, gm, gk, accumulate, stream);
+            else
+                am::launch_gauss_vjp(b.gauss(), X4, U, L, slots64, gm, gk, accumulate, stream);
+            ++launches;
+            off += b.num_elems;
+        }
+        check_launch("vjp kernel");
+    }
+
+    void reset_status() { ck(cudaMemsetAsync(status, 0, 2 * sizeof(int), stream), "reset status"); }
+
+    void check_status() {
+        int h[2] = {0, 0};
+        ck(cudaMemcpyAsync(h, status, sizeof(h), cudaMemcpyDeviceToHost, stream), "read status");
+        ck(cudaStreamSynchronize(stream), "synchronize");
+        if (h[0] == AM_ENONPOS_J) fail(AM_ENONPOS_J, "non-positive Jacobian determinant at element/cell " + std::to_string(h[1]));
+        if (h[0] == AM_ENAN) fail(AM_ENAN, "non-finite acceleration at node " + std::to_string(h[1]));
+        if (h[0] != 0) fail(h[0], "device status " + std::to_string(h[0]));
+    }
+
+    cudaEvent_t event(size_t k) {
+        while (events.size() <= k) {
+            cudaEvent_t e;
+            ck(cudaEventCreate(&e), "event create");
+            events.push_back(e);
+        }
+        return events[k];
+    }
+
+    // Host time-function evaluation for steps [0, dts.size()) from t0 into the device table.
+    void upload_table(const std::vector<double>& dts, double t0) {
+        const int64_t n = static_cast<int64_t>(dts.size());
+        if (n + 1 > table_cap) {
+            dfree(table);
+            if (table_host) cudaFreeHost(table_host);
+            table_host = nullptr;
+            table_cap = std::max<int64_t>(n + 1, 64);
+            table = dalloc<am::StepParams>(table_cap, "step table");
+            ck(cudaMallocHost(&table_host, table_cap * sizeof(am::StepParams)), "pinned step table");
+        }
+        ck(cudaStreamSynchronize(stream), "synchronize before table upload");
+        double time = t0;
+        for (int64_t k = 0; k < n; ++k) {
+            am::StepParams& P = table_host[k];
+            std::memset(&P, 0, sizeof(P));
+            P.dt = dts[k];
+            P.half = 0.5 * dts[k];
+            const double t_mid = time + 0.5 * dts[k];
+            const double t_next = time + dts[k];
+            for (size_t b = 0; b < bcs.size(); ++b) {
+                if (bcs[b].Active(t_mid)) {
+                    P.vact |= 1u << b;
+                    P.vscale[b] = bcs[b].VelocityScale(t_mid);
+                }
+                if (bcs[b].Active(t_next)) {
+                    P.aact |= 1u << b;
+                    P.ascale[b] = bcs[b].AccelerationScale(t_next);
+                }
+            }
+            time += dts[k];
+        }
+        ck(cudaMemcpyAsync(table, table_host, n * sizeof(am::StepParams), cudaMemcpyHostToDevice, stream), "table upload");
+    }
+
+    // Steps [n0, n1) of the uploaded table, from a consistent (U4, V4, A4). u_hist[k]
+    // (optional) receives the displacement the element kernels use at step n0+k.
+    void run_range(int mixed, int64_t n0, int64_t n1, double4* const* u_hist) {
+        if (n1 <= n0) return;
+        const am::NodeDev nd = node_dev();
+        void* s = slots(mixed);
+        size_t ev = 0;
+        if (profiling) ck(cudaEventRecord(event(ev++), stream), "event");
+        am::launch_prologue(nd, table + n0, U4, V4, A4, u_hist ? u_hist[0] : nullptr, stream);
+        ++launches;
+        check_launch("prologue kernel");
+        if (profiling) ck(cudaEventRecord(event(ev++), stream), "event");
+        for (int64_t n = n0; n < n1; ++n) {
+            element_forces(mixed, U4);
+            if (profiling) ck(cudaEventRecord(event(ev++), stream), "event");
+            const int advance = (n + 1 < n1) ? 1 : 0;
+            double4* uc = (u_hist && advance) ? u_hist[n + 1 - n0] : nullptr;
+            am::launch_node_step(nd, mixed, s, table, n, advance, U4, V4, A4, uc, status, stream);
+            ++launches;
+            check_launch("node step kernel");
+            if (profiling) ck(cudaEventRecord(event(ev++), stream), "event");
+        }
+        if (profiling) {
+            ck(cudaStreamSynchronize(stream), "synchronize (profiling)");
+            float ms = 0.f;
+            ck(cudaEventElapsedTime(&ms, events[0], events[1]), "elapsed");
+            prof_ms[1] += ms;
+            prof_launches[1] += 1;
+            for (int64_t k = 0; k < n1 - n0; ++k) {
+                ck(cudaEventElapsedTime(&ms, events[2 + 2 * k - 1 + 0], events[2 + 2 * k]), "elapsed");
+                prof_ms[0] += ms;
+                prof_launches[0] += static_cast<int64_t>(blocks.size());
+                ck(cudaEventElapsedTime(&ms, events[2 + 2 * k], events[2 + 2 * k + 1]), "elapsed");
+                prof_ms[1] += ms;
+                prof_launches[1] += 1;
+            }
+        }
+    }
+
+    void init_acceleration(int mixed) {
+        element_forces(mixed, U4);
+        am::launch_init_accel(node_dev(), mixed, slots(mixed), A4, status, stream);
+        ++launches;
+        check_launch("init acceleration kernel");
+    }
+
+    void require_finalized() const {
+        if (!finalized) fail(AM_ESTATE, "am_finalize has not been called");
+    }
+
+    void release() {
+        for (auto& b : blocks) b.release();
+        dfree(X4);
+        dfree(U4);
+        dfree(V4);
+        dfree(A4);
+        dfree(W4);
+        dfree(L4);
+        dfree(mass);
+        dfree(bcword);
+        dfree(bcvalues);
+        dfree(status);
+        dfree(f_scratch);
+        dfree(io_scratch);
+        dfree(node_ptr);
+        dfree(node_slots);
+        dfree(slots64);
+        dfree(slots32);
+        dfree(table);
+        if (table_host) cudaFreeHost(table_host);
+        table_host = nullptr;
+        for (auto e : events) cudaEventDestroy(e);
+        events.clear();
+        if (own_stream && stream) cudaStreamDestroy(stream);
+        stream = nullptr;
+    }
+};
+
+namespace {
+
+template <typename F>
+int guarded(am_ctx* ctx, F&& fn) {
+    try {
+        fn();
+        if (ctx) ctx->err.clear();
+        return AM_OK;
+    } catch (const AmError& e) {
+        if (ctx) ctx->err = e.msg;
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        if (ctx) ctx->err = "host allocation failed";
+        return AM_ENOMEM;
+    } catch (const std::exception& e) {
+        if (ctx) ctx->err = e.what();
+        return AM_EINVAL;
+    }
+}
+
+thread_local std::string g_free_error;
+
+// Copies an N x 3 nodal array (host or device) into a double4 device buffer.
+void load_nodal(am_ctx* c, am_memory where, const double* src, double4* dst) {
+    if (src == nullptr) {
+        am::launch_zero4(dst, c->N, c->stream);
+    } else if (where == AM_HOST) {
+        ck(cudaMemcpyAsync(c->io_scratch, src, c->N * 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream), "H2D");
+        am::launch_pack4(c->io_scratch, dst, c->N, c->stream);
+    } else {
+        am::launch_pack4(src, dst, c->N, c->stream);
+    }
+    c->launches += 1;
+    ck(cudaGetLastError(), "pack kernel");
+}
+
+void store_nodal(am_ctx* c, am_memory where, const double4* src, double* dst) {
+    if (dst == nullptr) return;
+    if (where == AM_HOST) {
+        am::launch_unpack4(src, c->io_scratch, c->N, c->stream);
+        ck(cudaMemcpyAsync(dst, c->io_scratch, c->N * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "D2H");
+        ck(cudaStreamSynchronize(c->stream), "synchronize");
+    } else {
+        am::launch_unpack4(src, dst, c->N, c->stream);
+    }
+    c->launches += 1;
+    ck(cudaGetLastError(), "unpack kernel");
+}
+
+void run_schedule(am_ctx* c, int prec, const std::vector<double>& dts, double t0) {
+    c->require_finalized();
+    if (prec != AM_FP64 && prec != AM_MIXED) fail(AM_EINVAL, "unknown precision");
+    for (double d : dts)
+        if (!(d >= 0.0) || !std::isfinite(d)) fail(AM_EINVAL, "time increments must be finite and non-negative");
+    if (dts.empty()) return;
+    c->upload_table(dts, t0);
+    c->reset_status();
+    c->run_range(prec == AM_MIXED, 0, static_cast<int64_t>(dts.size()), nullptr);
+    c->check_status();
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* am_status_string(int status) {
+    switch (status) {
+        case AM_OK: return "ok";
+        case AM_EINVAL: return "invalid argument";
+        case AM_ENOMEM: return "out of device memory";
+        case AM_ECUDA: return "CUDA error";
+        case AM_ENONPOS_J: return "non-positive Jacobian determinant";
+        case AM_ENAN: return "non-finite value";
+        case AM_ESTATE: return "call out of order";
+        case AM_ERANGE: return "size beyond limit";
+        default: return "unknown status";
+    }
+}
+
+const char* am_last_error(const am_ctx* ctx) {
+    if (ctx == nullptr) return g_free_error.c_str();
+    return ctx->err.c_str();
+}
+
+int am_create(int64_t num_nodes, const double* coords, am_ctx** out) {
+    if (out == nullptr) return AM_EINVAL;
+    *out = nullptr;
+    auto c = std::make_unique<am_ctx>();
+    const int rc = guarded(c.get(), [&] {
+        if (num_nodes <= 0 || coords == nullptr) fail(AM_EINVAL, "num_nodes must be positive and coords non-null");
+        if (num_nodes >= (int64_t(1) << 31)) fail(AM_ERANGE, "node count beyond int32 indexing");
+        for (int64_t k = 0; k < num_nodes * 3; ++k)
+            if (!std::isfinite(coords[k])) fail(AM_EINVAL, "non-finite coordinate");
+        ck(cudaGetDevice(&c->device), "cudaGetDevice");
+        ck(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream create");
+        c->own_stream = true;
+        c->N = num_nodes;
+        const size_t N = static_cast<size_t>(num_nodes);
+        c->X4 = dalloc<double4>(N, "coordinates");
+        c->U4 = dalloc<double4>(N, "displacement");
+        c->V4 = dalloc<double4>(N, "velocity");
+        c->A4 = dalloc<double4>(N, "acceleration");
+        c->W4 = dalloc<double4>(N, "scratch");
+        c->L4 = dalloc<double4>(N, "cotangent");
+        c->mass = dalloc<double>(N, "mass");
+        c->bcword = dalloc<uint32_t>(N, "bc word");
+        c->bcvalues = dalloc<double>(AM_MAX_BCS * 3, "bc values");
+        c->status = dalloc<int>(2, "status");
+        c->f_scratch = dalloc<double>(N * 3, "force scratch");
+        c->io_scratch = dalloc<double>(N * 3, "io scratch");
+        std::vector<double4> x(N);
+        for (size_t i = 0; i < N; ++i) x[i] = make_double4(coords[3 * i], coords[3 * i + 1], coords[3 * i + 2], 0.0);
+        ck(cudaMemcpy(c->X4, x.data(), N * sizeof(double4), cudaMemcpyHostToDevice), "coords upload");
+        ck(cudaMemset(c->U4, 0, N * sizeof(double4)), "memset");
+        ck(cudaMemset(c->V4, 0, N * sizeof(double4)), "memset");
+        ck(cudaMemset(c->A4, 0, N * sizeof(double4)), "memset");
+        ck(cudaMemset(c->W4, 0, N * sizeof(double4)), "memset");
+        ck(cudaMemset(c->L4, 0, N * sizeof(double4)), "memset");
+        ck(cudaMemset(c->mass, 0, N * sizeof(double)), "memset");
+        ck(cudaMemset(c->bcword, 0, N * sizeof(uint32_t)), "memset");
+        ck(cudaMemset(c->bcvalues, 0, AM_MAX_BCS * 3 * sizeof(double)), "memset");
+        ck(cudaMemset(c->status, 0, 2 * sizeof(int)), "memset");
+    });
+    if (rc != AM_OK) {
+        g_free_error = c->err;
+        c->release();
+        return rc;
+    }
+    *out = c.release();
+    return AM_OK;
+}
+
+void am_destroy(am_ctx* ctx) {
+    if (!ctx) return;
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    ctx->release();
+    delete ctx;
+}
+
+int am_set_stream(am_ctx* ctx, void* stream) {
+    if (!ctx) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        ck(cudaStreamSynchronize(ctx->stream), "synchronize");
+        if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+        if (stream == nullptr) {
+            ck(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "stream create");
+            ctx->own_stream = true;
+        } else {
+            ctx->stream = static_cast<cudaStream_t>(stream);
+            ctx->own_stream = false;
+        }
+    });
+}
+
+int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
+    if (!ctx) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        if (ctx->finalized) fail(AM_ESTATE, "am_add_block after am_finalize");
+        if (!d) fail(AM_EINVAL, "null block descriptor");
+        if (d->kind < AM_TET4_GAUSS || d->kind > AM_SMOOTHED_CELLS) fail(AM_EINVAL, "unknown block kind");
+        if (d->material < AM_LINEAR_ELASTIC || d->material > AM_ELASTIC_SVK) fail(AM_EINVAL, "unknown material");
+        if (d->num_elems < 0) fail(AM_EINVAL, "negative element count");
+        if (!(d->density > 0.0)) fail(AM_EINVAL, "density must be positive");
+        if (!std::isfinite(d->lambda) || !std::isfinite(d->mu)) fail(AM_EINVAL, "non-finite Lame parameters");
+        Block b;
+        b.kind = d->kind;
+        b.material = d->material;
+        b.lambda = d->lambda;
+        b.mu = d->mu;
+        b.density = d->density;
+        b.num_elems = d->num_elems;
+        b.slot_base = ctx->num_slots;
+        const int64_t E = d->num_elems;
+        try {
+            if (d->kind == AM_SMOOTHED_CELLS) {
+                if (E > 0 && (!d->cell_ptr || !d->cell_nodes || !d->cell_grads || !d->cell_volumes))
+                    fail(AM_EINVAL, "cell block needs cell_ptr, cell_nodes, cell_grads and cell_volumes");
+                const int64_t K = E > 0 ? d->cell_ptr[E] : 0;
+                if (E > 0 && d->cell_ptr[0] != 0) fail(AM_EINVAL, "cell_ptr[0] must be 0");
+                if (K >= (int64_t(1) << 31)) fail(AM_ERANGE, "entry count beyond int32 indexing");
+                std::vector<int32_t> ptr(E + 1);
+                int32_t maxlen = 0;
+                for (int64_t c = 0; c <= E; ++c) {
+                    if (c > 0 && d->cell_ptr[c] < d->cell_ptr[c - 1]) fail(AM_EINVAL, "cell_ptr must be non-decreasing");
+                    ptr[c] = static_cast<int32_t>(d->cell_ptr[c]);
+                    if (c > 0) maxlen = std::max<int32_t>(maxlen, ptr[c] - ptr[c - 1]);
+                }
+                for (int64_t s = 0; s < K; ++s)
+                    if (d->cell_nodes[s] < 0 || d->cell_nodes[s] >= ctx->N) fail(AM_EINVAL, "cell node index out of range");
+                std::vector<float> g32(K * 3);
+                for (int64_t s = 0; s < K * 3; ++s) {
+                    if (!std::isfinite(d->cell_grads[s])) fail(AM_EINVAL, "non-finite cell gradient");
+                    g32[s] = static_cast<float>(d->cell_grads[s]);
+                }
+                for (int64_t c = 0; c < E; ++c)
+                    if (!(d->cell_volumes[c] > 0.0)) fail(AM_EINVAL, "cell volumes must be positive");
+                b.num_entries = K;
+                b.max_entries = maxlen;
+                b.cell_ptr = dalloc<int32_t>(E + 1, "cell ptr");
+                ck(cudaMemcpy(b.cell_ptr, ptr.data(), (E + 1) * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+                if (K > 0) {
+                    b.cell_nodes = dalloc<int32_t>(K, "cell nodes");
+                    b.grads64 = dalloc<double>(K * 3, "cell grads");
+                    b.grads32 = dalloc<float>(K * 3, "cell grads fp32");
+                    ck(cudaMemcpy(b.cell_nodes, d->cell_nodes, K * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+                    ck(cudaMemcpy(b.grads64, d->cell_grads, K * 3 * sizeof(double), cudaMemcpyHostToDevice), "upload");
+                    ck(cudaMemcpy(b.grads32, g32.data(), K * 3 * sizeof(float), cudaMemcpyHostToDevice), "upload");
+                }
+                if (E > 0) {
+                    b.volumes = dalloc<double>(E, "cell volumes");
+                    ck(cudaMemcpy(b.volumes, d->cell_volumes, E * sizeof(double), cudaMemcpyHostToDevice), "upload");
+                }
+                b.host_nodes.assign(d->cell_nodes, d->cell_nodes + K);
+            } else {
+                const int nn = d->kind == AM_HEX8_GAUSS ? 8 : 4;
+                if (E > 0 && !d->conn) fail(AM_EINVAL, "null connectivity");
+                const int64_t S = E * nn;
+                if (ctx->num_slots + S >= (int64_t(1) << 31)) fail(AM_ERANGE, "slot count beyond int32 indexing");
+                for (int64_t s = 0; s < S; ++s)
+                    if (d->conn[s] < 0 || d->conn[s] >= ctx->N) fail(AM_EINVAL, "connectivity index out of range");
+                b.num_entries = S;
+                if (S > 0) {
+                    b.conn = dalloc<int32_t>(S, "connectivity");
+                    ck(cudaMemcpy(b.conn, d->conn, S * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+                }
+                b.host_nodes.assign(d->conn, d->conn + S);
+            }
+            if (ctx->num_slots + b.num_entries >= (int64_t(1) << 31)) fail(AM_ERANGE, "slot count beyond int32 indexing");
+            if (d->mu_field && E > 0) {
+                for (int64_t e = 0; e < E; ++e)
+                    if (!(d->mu_field[e] > 0.0)) fail(AM_EINVAL, "shear modulus field must be positive");
+                b.mu_field = dalloc<double>(E, "mu field");
+                ck(cudaMemcpy(b.mu_field, d->mu_field, E * sizeof(double), cudaMemcpyHostToDevice), "upload");
+            }
+            if (d->kappa_field && E > 0) {
+                for (int64_t e = 0; e < E; ++e)
+                    if (!(d->kappa_field[e] > 0.0)) fail(AM_EINVAL, "bulk modulus field must be positive");
+                b.kappa_field = dalloc<double>(E, "kappa field");
+                ck(cudaMemcpy(b.kappa_field, d->kappa_field, E * sizeof(double), cudaMemcpyHostToDevice), "upload");
+            }
+        } catch (...) {
+            b.release();
+            throw;
+        }
+        ctx->num_slots += b.num_entries;
+        ctx->blocks.push_back(std::move(b));
+        if (block_id) *block_id = static_cast<int32_t>(ctx->blocks.size() - 1);
+    });
+}
+
+int am_set_boundary_conditions(am_ctx* ctx, int32_t num_bcs, const am_bc_desc* bcs) {
+    if (!ctx) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        if (num_bcs < 0 || num_bcs > AM_MAX_BCS) fail(AM_ERANGE, "at most AM_MAX_BCS boundary conditions");
+        if (num_bcs > 0 && !bcs) fail(AM_EINVAL, "null boundary-condition array");
+        std::vector<am::host::BoundaryCondition> list;
+        std::vector<uint32_t> word(ctx->N, 0u);
+        std::vector<double> values(AM_MAX_BCS * 3, 0.0);
+        for (int32_t k = 0; k < num_bcs; ++k) {
+            const am_bc_desc& d = bcs[k];
+            am::host::BoundaryCondition bc;
+            if (d.kind != AM_BC_DISPLACEMENT && d.kind != AM_BC_VELOCITY)
+                fail(AM_EINVAL, "Boundary condition type must be 'velocity' or 'displacement'.");
+            if (d.time_function != AM_TF_RAMP && d.time_function != AM_TF_SMOOTH_STEP) fail(AM_EINVAL, "unknown time function");
+            if (d.num_points <= 0 || !d.abscissa || !d.ordinate) fail(AM_EINVAL, "time function needs at least one point");
+            if (d.num_nodes < 0 || (d.num_nodes > 0 && !d.nodes)) fail(AM_EINVAL, "bad node list");
+            bc.kind = d.kind;
+            bc.time_function = d.time_function;
+            bc.component_mask = d.component_mask & 7;
+            for (int c = 0; c < 3; ++c) bc.values[c] = d.values[c];
+            bc.abscissa.assign(d.abscissa, d.abscissa + d.num_points);
+            bc.ordinate.assign(d.ordinate, d.ordinate + d.num_points);
+            bc.active_start = d.active_start;
+            bc.active_end = d.active_end;
+            bc.Finish();
+            for (int64_t i = 0; i < d.num_nodes; ++i) {
+                const int32_t n = d.nodes[i];
+                if (n < 0 || n >= ctx->N) fail(AM_EINVAL, "boundary-condition node out of range");
+                for (int c = 0; c < 3; ++c)
+                    if (bc.component_mask & (1 << c)) word[n] |= 1u << (10 * c + k);
+            }
+            for (int c = 0; c < 3; ++c) values[k * 3 + c] = d.values[c];
+            bc.nodes.assign(d.nodes, d.nodes + d.num_nodes);
+            list.push_back(std::move(bc));
+        }
+        ck(cudaMemcpy(ctx->bcword, word.data(), ctx->N * sizeof(uint32_t), cudaMemcpyHostToDevice), "bc upload");
+        ck(cudaMemcpy(ctx->bcvalues, values.data(), values.size() * sizeof(double), cudaMemcpyHostToDevice), "bc upload");
+        ctx->bcs = std::move(list);
+    });
+}
+
+int am_set_block_fields(am_ctx* ctx, int32_t block_id, const double* mu_field, const double* kappa_field) {
+    if (!ctx) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        if (block_id < 0 || block_id >= static_cast<int32_t>(ctx->blocks.size())) fail(AM_EINVAL, "no such block");
+        Block& b = ctx->blocks[block_id];
+        const int64_t E = b.num_elems;
+        auto upload = [&](const double* src, double*& dst, const char* what) {
+            if (!src || E == 0) return;
+            for (int64_t e = 0; e < E; ++e)
+                if (!(src[e] > 0.0)) fail(AM_EINVAL, std::string(what) + " field must be positive");
+            if (!dst) dst = dalloc<double>(E, what);
+            ck(cudaMemcpyAsync(dst, src, E * sizeof(double), cudaMemcpyHostToDevice, ctx->stream), "field upload");
+            ck(cudaStreamSynchronize(ctx->stream), "synchronize");
+        };
+        upload(mu_field, b.mu_field, "shear modulus");
+        upload(kappa_field, b.kappa_field, "bulk modulus");
+    });
+}
+
+int am_set_body_acceleration(am_ctx* ctx, const double g[3]) {
+    if (!ctx || !g) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        for (int i = 0; i < 3; ++i) {
+            if (!std::isfinite(g[i])) fail(AM_EINVAL, "non-finite body acceleration");
+            ctx->g[i] = g[i];
+        }
+    });
+}
+
+int am_set_mass(am_ctx* ctx, const double* mass) {
+    if (!ctx || !mass) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        for (int64_t i = 0; i < ctx->N; ++i)
+            if (!(mass[i] > 0.0)) fail(AM_EINVAL, "nodal masses must be positive");
+        ck(cudaMemcpy(ctx->mass, mass, ctx->N * sizeof(double), cudaMemcpyHostToDevice), "mass upload");
+        ctx->mass_set = true;
+    });
+}
+
+int am_finalize(am_ctx* ctx) {
+    if (!ctx) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        if (ctx->finalized) fail(AM_ESTATE, "am_finalize called twice");
+        if (ctx->blocks.empty()) fail(AM_EINVAL, "no blocks");
+        const int64_t N = ctx->N, S = ctx->num_slots;
+        // Node -> slot CSR, slots ascending within each node (block order, then element order).
+        std::vector<int32_t> ptr(N + 1, 0), slots(S);
+        for (const auto& b : ctx->blocks)
+            for (int32_t n : b.host_nodes) ++ptr[n + 1];
+        for (int64_t i = 0; i < N; ++i) ptr[i + 1] += ptr[i];
+        std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
+        for (const auto& b : ctx->blocks)
+            for (int64_t k = 0; k < static_cast<int64_t>(b.host_nodes.size()); ++k)
+                slots[fill[b.host_nodes[k]]++] = static_cast<int32_t>(b.slot_base + k);
+        ctx->node_ptr = dalloc<int32_t>(N + 1, "node ptr");
+        ck(cudaMemcpy(ctx->node_ptr, ptr.data(), (N + 1) * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+        if (S > 0) {
+            ctx->node_slots = dalloc<int32_t>(S, "node slots");
+            ck(cudaMemcpy(ctx->node_slots, slots.data(), S * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+            ctx->slots64 = dalloc<double>(static_cast<size_t>(S) * 3, "slot buffer");
+        }
+        for (auto& b : ctx->blocks) std::vector<int32_t>().swap(b.host_nodes);
+        bool has_cells = false;
+        for (const auto& b : ctx->blocks) has_cells |= b.kind == AM_SMOOTHED_CELLS;
+        if (!ctx->mass_set) {
+            if (has_cells) fail(AM_EINVAL, "smoothed-cell blocks need an explicit lumped mass (am_set_mass)");
+            // Lumped mass (src/MassUtils.cpp:17-112) on the device, summed in element order.
+            for (const auto& b : ctx->blocks) {
+                am::launch_gauss_volume_slots(b.gauss(), b.density, ctx->X4, ctx->slots64, ctx->stream);
+                ++ctx->launches;
+            }
+            am::launch_gather_force(ctx->node_dev(), 0, ctx->slots64, ctx->f_scratch, 0, ctx->stream);
+            ++ctx->launches;
+            ck(cudaGetLastError(), "mass kernels");
+            std::vector<double> f(N * 3), m(N);
+            ck(cudaMemcpyAsync(f.data(), ctx->f_scratch, N * 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+            ck(cudaStreamSynchronize(ctx->stream), "synchronize");
+            for (int64_t i = 0; i < N; ++i) {
+                m[i] = f[3 * i];
+                if (!(m[i] > 0.0)) fail(AM_EINVAL, "node " + std::to_string(i) + " has no mass (not connected to an element)");
+            }
+            ck(cudaMemcpy(ctx->mass, m.data(), N * sizeof(double), cudaMemcpyHostToDevice), "mass upload");
+            ctx->mass_set = true;
+        }
+        ctx->finalized = true;
+    });
+}
+
+int am_get_mass(am_ctx* ctx, double* mass) {
+    if (!ctx || !mass) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        ck(cudaMemcpyAsync(mass, ctx->mass, ctx->N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        ck(cudaStreamSynchronize(ctx->stream), "synchronize");
+    });
+}
+
+int am_set_state(am_ctx* ctx, am_memory where, const double* u, const double* v, const double* a) {
+    if (!ctx) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        load_nodal(ctx, where, u, ctx->U4);
+        load_nodal(ctx, where, v, ctx->V4);
+        load_nodal(ctx, where, a, ctx->A4);
+        if (where == AM_HOST) ck(cudaStreamSynchronize(ctx->stream), "synchronize");
+    });
+}
+
+int am_get_state(am_ctx* ctx, am_memory where, double* u, double* v, double* a) {
+    if (!ctx) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        store_nodal(ctx, where, ctx->U4, u);
+        store_nodal(ctx, where, ctx->V4, v);
+        store_nodal(ctx, where, ctx->A4, a);
+    });
+}
+
+int am_internal_force(am_ctx* ctx, am_precision prec, am_memory where, const double* u, double* f, int accumulate) {
+    if (!ctx) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        ctx->require_finalized();
+        if (!u || !f) fail(AM_EINVAL, "null u or f");
+        const int mixed = prec == AM_MIXED;
+        load_nodal(ctx, where, u, ctx->W4);
+        ctx->reset_status();
+        ctx->element_forces(mixed, ctx->W4);
+        double* out = ctx->f_scratch;
+        if (where == AM_DEVICE) out = f;
+        else if (accumulate) ck(cudaMemcpyAsync(out, f, ctx->N * 3 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream), "H2D");
+        am::launch_gather_force(ctx->node_dev(), mixed, ctx->slots(mixed), out, accumulate, ctx->stream);
+        ++ctx->launches;
+        ck(cudaGetLastError(), "gather kernel");
+        if (where == AM_HOST)
+            ck(cudaMemcpyAsync(f, out, ctx->N * 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        ctx->check_status();
+    });
+}
+
+int am_init_acceleration(am_ctx* ctx, am_precision prec) {
+    if (!ctx) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        ctx->require_finalized();
+        ctx->reset_status();
+        ctx->init_acceleration(prec == AM_MIXED);
+        ctx->check_status();
+    });
+}
+
+int am_run(am_ctx* ctx, am_precision prec, int64_t nsteps, double dt, double t0) {
+    if (!ctx) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        if (nsteps < 0) fail(AM_EINVAL, "negative step count");
+        run_schedule(ctx, prec, std::vector<double>(static_cast<size_t>(nsteps), dt), t0);
+    });
+}
+
+int am_run_schedule(am_ctx* ctx, am_precision prec, int64_t nsteps, const double* dts, double t0) {
+    if (!ctx) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        if (nsteps < 0 || (nsteps > 0 && !dts)) fail(AM_EINVAL, "bad schedule");
+        run_schedule(ctx, prec, std::vector<double>(dts, dts + nsteps), t0);
+    });
+}
+
+int am_solve(am_ctx* ctx, am_precision prec, double dt, double t_end, int64_t max_steps, int64_t* steps_done) {
+    if (!ctx) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        ctx->require_finalized();
+        if (!(dt > 0.0) || !std::isfinite(t_end)) fail(AM_EINVAL, "dt must be positive and t_end finite");
+        ctx->reset_status();
+        ctx->init_acceleration(prec == AM_MIXED);
+        ctx->check_status();
+        const std::vector<double> dts = am::host::DirectTimeSchedule(dt, t_end, max_steps);
+        run_schedule(ctx, prec, dts, 0.0);
+        if (steps_done) *steps_done = static_cast<int64_t>(dts.size());
+    });
+}
+
+int am_vjp_force(am_ctx* ctx, am_memory where, const double* u, const double* lam, double* gu, double* gmu,
+                 double* gkappa) {
+    if (!ctx) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        ctx->require_finalized();
+        if (!u || !lam || !gu) fail(AM_EINVAL, "null u, lam or gu");
+        load_nodal(ctx, where, u, ctx->W4);
+        load_nodal(ctx, where, lam, ctx->L4);
+        const int64_t E = ctx->total_elems();
+        double* gm = nullptr;
+        double* gk = nullptr;
+        std::unique_ptr<double, void (*)(double*)> hold_m(nullptr, [](double* p) { if (p) cudaFree(p); });
+        std::unique_ptr<double, void (*)(double*)> hold_k(nullptr, [](double* p) { if (p) cudaFree(p); });
+        if (gmu) {
+            gm = (where == AM_DEVICE) ? gmu : dalloc<double>(E, "gmu");
+            if (where != AM_DEVICE) hold_m.reset(gm);
+        }
+        if (gkappa) {
+            gk = (where == AM_DEVICE) ? gkappa : dalloc<double>(E, "gkappa");
+            if (where != AM_DEVICE) hold_k.reset(gk);
+        }
+        ctx->vjp(ctx->W4, ctx->L4, gm, gk, 0);
+        double* out = where == AM_DEVICE ? gu : ctx->f_scratch;
+        am::launch_gather_force(ctx->node_dev(), 0, ctx->slots64, out, 0, ctx->stream);
+        ++ctx->launches;
+        ck(cudaGetLastError(), "gather kernel");
+        if (where == AM_HOST) {
+            ck(cudaMemcpyAsync(gu, out, ctx->N * 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+            if (gmu) ck(cudaMemcpyAsync(gmu, gm, E * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+            if (gkappa) ck(cudaMemcpyAsync(gkappa, gk, E * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        }
+        ck(cudaStreamSynchronize(ctx->stream), "synchronize");
+    });
+}
+
+int am_adjoint(am_ctx* ctx, int64_t nsteps, double dt, int32_t ckpt_every, int32_t num_sensors, const int32_t* sensors,
+               double* loss, double* gmu, double* gkappa) {
+    if (!ctx) return AM_EINVAL;
+    struct Bufs {
+        std::vector<double4*> ptrs;
+        ~Bufs() {
+            for (auto p : ptrs)
+                if (p) cudaFree(p);
+        }
+        double4* get(size_t n) {
+            ptrs.push_back(dalloc<double4>(n, "adjoint buffer"));
+            return ptrs.back();
+        }
+    } bufs;
+    return guarded(ctx, [&] {
+        ctx->require_finalized();
+        if (nsteps <= 0 || !(dt > 0.0)) fail(AM_EINVAL, "nsteps and dt must be positive");
+        if (ckpt_every <= 0) fail(AM_EINVAL, "ckpt_every must be positive");
+        if (num_sensors < 0 || (num_sensors > 0 && !sensors)) fail(AM_EINVAL, "bad sensor list");
+        for (int32_t s = 0; s < num_sensors; ++s)
+            if (sensors[s] < 0 || sensors[s] >= ctx->N) fail(AM_EINVAL, "sensor node out of range");
+        const size_t N = static_cast<size_t>(ctx->N);
+        const int64_t E = ctx->total_elems();
+        const int64_t nseg = (nsteps + ckpt_every - 1) / ckpt_every;
+        std::vector<double4*> ck_u(nseg), ck_v(nseg), ck_a(nseg), seg(ckpt_every);
+        for (int64_t s = 0; s < nseg; ++s) {
+            ck_u[s] = bufs.get(N);
+            ck_v[s] = bufs.get(N);
+            ck_a[s] = bufs.get(N);
+        }
+        for (int32_t k = 0; k < ckpt_every; ++k) seg[k] = bufs.get(N);
+        double4* UB = bufs.get(N);
+        double4* VB = bufs.get(N);
+        double4* AB = bufs.get(N);
+        double4* fin_u = bufs.get(N);
+        double4* fin_v = bufs.get(N);
+        double4* fin_a = bufs.get(N);
+        double* gm = reinterpret_cast<double*>(bufs.get((E + 3) / 4));
+        double* gk = reinterpret_cast<double*>(bufs.get((E + 3) / 4));
+        int32_t* dsens = reinterpret_cast<int32_t*>(bufs.get((num_sensors + 7) / 8 + 1));
+        double* dloss = reinterpret_cast<double*>(bufs.get(1));
+        cudaStream_t st = ctx->stream;
+        const size_t bytes = N * sizeof(double4);
+        ck(cudaMemsetAsync(gm, 0, E * sizeof(double), st), "memset");
+        ck(cudaMemsetAsync(gk, 0, E * sizeof(double), st), "memset");
+        if (num_sensors > 0)
+            ck(cudaMemcpyAsync(dsens, sensors, num_sensors * sizeof(int32_t), cudaMemcpyHostToDevice, st), "H2D");
+        // Forward pass (FP64) with checkpoints of (u, v, a) at the start of each segment.
+        ctx->reset_status();
+        ctx->init_acceleration(0);
+        ctx->upload_table(std::vector<double>(static_cast<size_t>(nsteps), dt), 0.0);
+        for (int64_t s = 0; s < nseg; ++s) {
+            ck(cudaMemcpyAsync(ck_u[s], ctx->U4, bytes, cudaMemcpyDeviceToDevice, st), "checkpoint");
+            ck(cudaMemcpyAsync(ck_v[s], ctx->V4, bytes, cudaMemcpyDeviceToDevice, st), "checkpoint");
+            ck(cudaMemcpyAsync(ck_a[s], ctx->A4, bytes, cudaMemcpyDeviceToDevice, st), "checkpoint");
+            ctx->run_range(0, s * ckpt_every, std::min<int64_t>(nsteps, (s + 1) * ckpt_every), nullptr);
+        }
+        ctx->check_status();
+        ck(cudaMemcpyAsync(fin_u, ctx->U4, bytes, cudaMemcpyDeviceToDevice, st), "save");
+        ck(cudaMemcpyAsync(fin_v, ctx->V4, bytes, cudaMemcpyDeviceToDevice, st), "save");
+        ck(cudaMemcpyAsync(fin_a, ctx->A4, bytes, cudaMemcpyDeviceToDevice, st), "save");
+        // Cotangent of the loss.
+        am::launch_zero4(UB, ctx->N, st);
+        am::launch_zero4(VB, ctx->N, st);
+        am::launch_zero4(AB, ctx->N, st);
+        am::launch_sensor_seed(ctx->U4, num_sensors, dsens, UB, dloss, st);
+        ctx->launches += 4;
+        const am::NodeDev nd = ctx->node_dev();
+        am::launch_adj_prep(nd, ctx->table, nsteps - 1, VB, AB, ctx->L4, st);
+        ++ctx->launches;
+        // Reverse pass, one segment at a time: recompute the segment's displacements
+        // from its checkpoint, then transpose its steps in reverse order.
+        for (int64_t s = nseg - 1; s >= 0; --s) {
+            const int64_t n0 = s * ckpt_every, n1 = std::min<int64_t>(nsteps, (s + 1) * ckpt_every);
+            ck(cudaMemcpyAsync(ctx->U4, ck_u[s], bytes, cudaMemcpyDeviceToDevice, st), "restore");
+            ck(cudaMemcpyAsync(ctx->V4, ck_v[s], bytes, cudaMemcpyDeviceToDevice, st), "restore");
+            ck(cudaMemcpyAsync(ctx->A4, ck_a[s], bytes, cudaMemcpyDeviceToDevice, st), "restore");
+            ctx->run_range(0, n0, n1, seg.data());
+            for (int64_t n = n1 - 1; n >= n0; --n) {
+                ctx->vjp(seg[n - n0], ctx->L4, gm, gk, 1);
+                am::launch_adj_update(nd, ctx->slots64, ctx->table, n, UB, VB, AB, ctx->L4, st);
+                ++ctx->launches;
+            }
+            ck(cudaGetLastError(), "adjoint kernels");
+        }
+        // Initial acceleration a^0 = F(u^0)/m: only the material-field cotangent remains.
+        ctx->vjp(ck_u[0], ctx->L4, gm, gk, 1);
+        ck(cudaMemcpyAsync(ctx->U4, fin_u, bytes, cudaMemcpyDeviceToDevice, st), "restore");
+        ck(cudaMemcpyAsync(ctx->V4, fin_v, bytes, cudaMemcpyDeviceToDevice, st), "restore");
+        ck(cudaMemcpyAsync(ctx->A4, fin_a, bytes, cudaMemcpyDeviceToDevice, st), "restore");
+        if (loss) ck(cudaMemcpyAsync(loss, dloss, sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+        if (gmu) ck(cudaMemcpyAsync(gmu, gm, E * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+        if (gkappa) ck(cudaMemcpyAsync(gkappa, gk, E * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+        ctx->check_status();
+    });
+}
+
+int am_stress(int32_t material, double lambda, double mu, int64_t n, am_memory where, const double* H, double* P) {
+    am_ctx* none = nullptr;
+    const int rc = guarded(none, [&] {
+        if (material < AM_LINEAR_ELASTIC || material > AM_ELASTIC_SVK) fail(AM_EINVAL, "unknown material");
+        if (n < 0 || (n > 0 && (!H || !P))) fail(AM_EINVAL, "bad arrays");
+        if (n == 0) return;
+        const double* dH = H;
+        double* dP = P;
+        std::unique_ptr<double, void (*)(double*)> h1(nullptr, [](double* p) { if (p) cudaFree(p); });
+        std::unique_ptr<double, void (*)(double*)> h2(nullptr, [](double* p) { if (p) cudaFree(p); });
+        if (where == AM_HOST) {
+            double* a = dalloc<double>(n * 9, "H");
+            h1.reset(a);
+            double* b = dalloc<double>(n * 9, "P");
+            h2.reset(b);
+            ck(cudaMemcpy(a, H, n * 9 * sizeof(double), cudaMemcpyHostToDevice), "H2D");
+            dH = a;
+            dP = b;
+        }
+        am::launch_stress_batch(material, lambda, mu, n, dH, dP, 0);
+        ck(cudaGetLastError(), "stress kernel");
+        if (where == AM_HOST) ck(cudaMemcpy(P, dP, n * 9 * sizeof(double), cudaMemcpyDeviceToHost), "D2H");
+        ck(cudaDeviceSynchronize(), "synchronize");
+    });
+    if (rc != AM_OK) {
+        // message kept for am_last_error(NULL)
+    }
+    return rc;
+}
+
+int am_quadrature(int32_t kind, int32_t smoothed, int64_t n, am_memory where, const double* X, double* B, double* w) {
+    am_ctx* none = nullptr;
+    return guarded(none, [&] {
+        if (kind != AM_TET4_GAUSS && kind != AM_HEX8_GAUSS) fail(AM_EINVAL, "quadrature kind must be Tet4 or Hex8");
+        if (n < 0 || (n > 0 && (!X || !B || !w))) fail(AM_EINVAL, "bad arrays");
+        if (n == 0) return;
+        const int nn = kind == AM_HEX8_GAUSS ? 8 : 4;
+        const int np = smoothed ? 1 : (kind == AM_HEX8_GAUSS ? 8 : 1);
+        const size_t nx = n * nn * 3, nb = n * np * nn * 3, nw = n * np;
+        const double* dX = X;
+        double* dB = B;
+        double* dw = w;
+        std::vector<std::unique_ptr<double, void (*)(double*)>> hold;
+        if (where == AM_HOST) {
+            double* a = dalloc<double>(nx, "X");
+            hold.emplace_back(a, [](double* p) { cudaFree(p); });
+            double* b = dalloc<double>(nb, "B");
+            hold.emplace_back(b, [](double* p) { cudaFree(p); });
+            double* c = dalloc<double>(nw, "w");
+            hold.emplace_back(c, [](double* p) { cudaFree(p); });
+            ck(cudaMemcpy(a, X, nx * sizeof(double), cudaMemcpyHostToDevice), "H2D");
+            dX = a;
+            dB = b;
+            dw = c;
+        }
+        am::launch_quadrature_batch(kind, smoothed, n, dX, dB, dw, 0);
+        ck(cudaGetLastError(), "quadrature kernel");
+        if (where == AM_HOST) {
+            ck(cudaMemcpy(B, dB, nb * sizeof(double), cudaMemcpyDeviceToHost), "D2H");
+            ck(cudaMemcpy(w, dw, nw * sizeof(double), cudaMemcpyDeviceToHost), "D2H");
+        }
+        ck(cudaDeviceSynchronize(), "synchronize");
+    });
+}
+
+int am_complete_properties(double props[5], char* msg, int msg_len) {
+    if (!props) return AM_EINVAL;
+    try {
+        am::host::LinearElasticProperties p;
+        p.youngs_modulus = props[0];
+        p.poisson_ratio = props[1];
+        p.shear_modulus = props[2];
+        p.lambda = props[3];
+        p.bulk_modulus = props[4];
+        p.CompleteProperties();
+        props[0] = p.youngs_modulus;
+        props[1] = p.poisson_ratio;
+        props[2] = p.shear_modulus;
+        props[3] = p.lambda;
+        props[4] = p.bulk_modulus;
+        return AM_OK;
+    } catch (const std::exception& e) {
+        if (msg && msg_len > 0) std::snprintf(msg, static_cast<size_t>(msg_len), "%s", e.what());
+        return AM_EINVAL;
+    }
+}
+
+int64_t am_launch_count(const am_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int am_profile_enable(am_ctx* ctx, int enable) {
+    if (!ctx) return AM_EINVAL;
+    ctx->profiling = enable != 0;
+    for (int k = 0; k < 3; ++k) {
+        ctx->prof_ms[k] = 0.0;
+        ctx->prof_launches[k] = 0;
+    }
+    return AM_OK;
+}
+
+int am_profile_read(am_ctx* ctx, double ms[3], int64_t launches[3]) {
+    if (!ctx) return AM_EINVAL;
+    for (int k = 0; k < 3; ++k) {
+        if (ms) ms[k] = ctx->prof_ms[k];
+        if (launches) launches[k] = ctx->prof_launches[k];
+    }
+    return AM_OK;
+}
+
+}  // extern "C"

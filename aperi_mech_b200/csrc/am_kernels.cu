@@ -1,0 +1,1038 @@
+// am_kernels.cu -- sm_100a kernels of the explicit-dynamics hot path.
+//
+// Force assembly is two kernels per step, with no atomics anywhere:
+//   1. an element (or smoothed-cell) kernel writes each element's nodal force
+//      contributions to its own "slots" (element e, local node a -> slot);
+//   2. a node kernel sums its slots through a node -> slot CSR in ascending
+//      slot order (deterministic, the oracle's element order) and, in the time
+//      loop, fuses the central-difference update: a = f/m, boundary overwrite,
+//      v^{n+1}, and the next step's v^{n+1/2} and u^{n+2}.
+// Element math runs in FP64 (T = double) or FP32 (T = float, mixed path). The
+// mixed path forms element-local differences (X_a - X_0, u_a - u_0) in FP64
+// before casting, evaluates the neo-Hookean det F and log J in FP64, and
+// accumulates nodal forces and the state in FP64.
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+#include "am_kernels.cuh"
+#include "am_math.cuh"
+
+namespace am {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ void flag(int* status, int code, int64_t idx) {
+    if (status == nullptr) return;
+    if (atomicCAS(status + kStatusCode, 0, code) == 0) status[kStatusIndex] = static_cast<int>(idx);
+}
+
+template <typename F>
+__device__ __forceinline__ void element_lame(const F& b, int64_t e, double& lambda, double& mu) {
+    if (b.mu_field != nullptr || b.kappa_field != nullptr) {
+        const double m = b.mu_field ? b.mu_field[e] : b.mu;
+        const double k = b.kappa_field ? b.kappa_field[e] : b.lambda + 2.0 * b.mu / 3.0;
+        mu = m;
+        lambda = k - 2.0 * m / 3.0;
+    } else {
+        lambda = b.lambda;
+        mu = b.mu;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Hex8 reference-element sign tables (ShapeFunctionsFunctorHex8.h:17-33): node a
+// sits at (sx, sy, sz) in {-1,1}^3; the 2x2x2 Gauss point g sits at the same
+// signs times 1/sqrt(3) (ElementHexahedron8.h:105-117).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int hex_sign(int a, int j) {
+    const int mask = (j == 0) ? 0x66 : (j == 1) ? 0xCC : 0xF0;
+    return ((mask >> a) & 1) ? 1 : -1;
+}
+__host__ __device__ constexpr int hex_sign_c(int a, int j) {
+    return (((j == 0 ? 0x66 : j == 1 ? 0xCC : 0xF0) >> a) & 1) ? 1 : -1;
+}
+
+// ---------------------------------------------------------------------------
+// Tet4, 1-point Gauss: one thread per element.
+// ---------------------------------------------------------------------------
+template <typename T, int MAT>
+__global__ void __launch_bounds__(256) k_tet4_force(GaussBlockDev b, const double4* __restrict__ X4,
+                                                     const double4* __restrict__ U4, T* __restrict__ slots,
+                                                     int* status) {
+    __shared__ T stage[256 * 12];
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    T f[12];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) f[k] = T(0);
+    if (e < b.num_elems) {
+        const int4 c = reinterpret_cast<const int4*>(b.conn)[e];
+        const double4 x0 = X4[c.x], x1 = X4[c.y], x2 = X4[c.z], x3 = X4[c.w];
+        const double4 u0 = U4[c.x], u1 = U4[c.y], u2 = U4[c.z], u3 = U4[c.w];
+        // J = X^T dN with dN rows (-1,-1,-1), e1, e2, e3: column j of J is X_{j+1} - X_0.
+        const T J[9] = {T(x1.x - x0.x), T(x2.x - x0.x), T(x3.x - x0.x), T(x1.y - x0.y), T(x2.y - x0.y),
+                        T(x3.y - x0.y), T(x1.z - x0.z), T(x2.z - x0.z), T(x3.z - x0.z)};
+        const T D[9] = {T(u1.x - u0.x), T(u2.x - u0.x), T(u3.x - u0.x), T(u1.y - u0.y), T(u2.y - u0.y),
+                        T(u3.y - u0.y), T(u1.z - u0.z), T(u2.z - u0.z), T(u3.z - u0.z)};
+        const T det = det3(J);
+        if (!(det > T(0))) flag(status, AM_ENONPOS_J, e);
+        T Ji[9];
+        cof_inv3(J, Ji, det);
+        const T w = det / T(6);
+        // H = u^T B = D J^-1
+        T H[9];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) H[i * 3 + j] = D[i * 3 + 0] * Ji[0 * 3 + j] + D[i * 3 + 1] * Ji[1 * 3 + j] + D[i * 3 + 2] * Ji[2 * 3 + j];
+        double lam, mu;
+        element_lame(b, e, lam, mu);
+        T P[9];
+        const double Jf = stress<T>(MAT, T(lam), T(mu), H, P);
+        if (MAT == kNeoHookean && !(Jf > 0.0)) flag(status, AM_ENONPOS_J, e);
+        // Q = w J^-1 P^T ; f_{k+1} = -Q_k ; f_0 = Q_0 + Q_1 + Q_2
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const T q = w * (Ji[k * 3 + 0] * P[i * 3 + 0] + Ji[k * 3 + 1] * P[i * 3 + 1] + Ji[k * 3 + 2] * P[i * 3 + 2]);
+                f[(k + 1) * 3 + i] = -q;
+                f[i] += q;
+            }
+    }
+    // Stage through shared memory so the block's slots go out as one coalesced run.
+#pragma unroll
+    for (int k = 0; k < 12; ++k) stage[threadIdx.x * 12 + k] = f[k];
+    __syncthreads();
+    const int64_t first = static_cast<int64_t>(blockIdx.x) * blockDim.x;
+    const int64_t count = min(static_cast<int64_t>(blockDim.x), b.num_elems - first) * 12;
+    T* out = slots + (b.slot_base + first * 4) * 3;
+    for (int k = threadIdx.x; k < count; k += blockDim.x) out[k] = stage[k];
+}
+
+// ---------------------------------------------------------------------------
+// Hex8, 2x2x2 Gauss: eight lanes per element. Lane g loads node g, then acts as
+// Gauss point g (J, H, P, Q = w J^-1 P^T), then as node g again to sum its force
+// over the eight Q's. Shared memory carries the node data and the Q's between
+// the two phases; the node-phase sum runs over Gauss points in order.
+// ---------------------------------------------------------------------------
+template <typename T, int MAT>
+__global__ void __launch_bounds__(256) k_hex8_force(GaussBlockDev b, const double4* __restrict__ X4,
+                                                     const double4* __restrict__ U4, T* __restrict__ slots,
+                                                     int* status) {
+    __shared__ T sh[32][120];
+    const int lane = threadIdx.x & 31;
+    const int g = lane & 7;
+    const int el = threadIdx.x >> 3;
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * 32 + el;
+    const bool valid = e < b.num_elems;
+    const int32_t n = valid ? b.conn[e * 8 + g] : 0;
+    const double4 x = X4[n];
+    const double4 u = U4[n];
+    const int src = lane & ~7;
+    const double x0 = __shfl_sync(kFull, x.x, src), y0 = __shfl_sync(kFull, x.y, src), z0 = __shfl_sync(kFull, x.z, src);
+    const double ux0 = __shfl_sync(kFull, u.x, src), uy0 = __shfl_sync(kFull, u.y, src), uz0 = __shfl_sync(kFull, u.z, src);
+    T* s = sh[el];
+    s[g * 6 + 0] = T(x.x - x0);
+    s[g * 6 + 1] = T(x.y - y0);
+    s[g * 6 + 2] = T(x.z - z0);
+    s[g * 6 + 3] = T(u.x - ux0);
+    s[g * 6 + 4] = T(u.y - uy0);
+    s[g * 6 + 5] = T(u.z - uz0);
+    __syncwarp();
+
+    const T c = T(0.57735026918962576451);  // 1/sqrt(3)
+    T cp[3], cm[3], sg[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        sg[j] = T(hex_sign(g, j));
+        cp[j] = T(1) + sg[j] * c;
+        cm[j] = T(1) - sg[j] * c;
+    }
+    // ---- Gauss point g ----
+    T J[9], G[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        J[k] = T(0);
+        G[k] = T(0);
+    }
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        const T f0 = hex_sign_c(a, 0) > 0 ? cp[0] : cm[0];
+        const T f1 = hex_sign_c(a, 1) > 0 ? cp[1] : cm[1];
+        const T f2 = hex_sign_c(a, 2) > 0 ? cp[2] : cm[2];
+        const T dN[3] = {T(0.125 * hex_sign_c(a, 0)) * f1 * f2, T(0.125 * hex_sign_c(a, 1)) * f0 * f2,
+                         T(0.125 * hex_sign_c(a, 2)) * f0 * f1};
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const T xa = s[a * 6 + i], ua = s[a * 6 + 3 + i];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                J[i * 3 + j] += xa * dN[j];
+                G[i * 3 + j] += ua * dN[j];
+            }
+        }
+    }
+    const T det = det3(J);
+    if (valid && !(det > T(0))) flag(status, AM_ENONPOS_J, e);
+    T Ji[9];
+    cof_inv3(J, Ji, det);
+    T H[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) H[i * 3 + j] = G[i * 3 + 0] * Ji[0 * 3 + j] + G[i * 3 + 1] * Ji[1 * 3 + j] + G[i * 3 + 2] * Ji[2 * 3 + j];
+    double lam = 0.0, mu = 0.0;
+    if (valid) element_lame(b, e, lam, mu);
+    T P[9];
+    const double Jf = stress<T>(MAT, T(lam), T(mu), H, P);
+    if (valid && MAT == kNeoHookean && !(Jf > 0.0)) flag(status, AM_ENONPOS_J, e);
+    T* q = s + 48 + g * 9;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            q[k * 3 + i] = det * (Ji[k * 3 + 0] * P[i * 3 + 0] + Ji[k * 3 + 1] * P[i * 3 + 1] + Ji[k * 3 + 2] * P[i * 3 + 2]);
+    __syncwarp();
+    // ---- node g: f_g = -sum_gp dN_g(xi_gp) Q_gp ----
+    T fx = T(0), fy = T(0), fz = T(0);
+#pragma unroll
+    for (int gp = 0; gp < 8; ++gp) {
+        const T f0 = hex_sign_c(gp, 0) > 0 ? cp[0] : cm[0];
+        const T f1 = hex_sign_c(gp, 1) > 0 ? cp[1] : cm[1];
+        const T f2 = hex_sign_c(gp, 2) > 0 ? cp[2] : cm[2];
+        const T d0 = T(0.125) * sg[0] * f1 * f2, d1 = T(0.125) * sg[1] * f0 * f2, d2 = T(0.125) * sg[2] * f0 * f1;
+        const T* Q = s + 48 + gp * 9;
+        fx -= d0 * Q[0] + d1 * Q[3] + d2 * Q[6];
+        fy -= d0 * Q[1] + d1 * Q[4] + d2 * Q[7];
+        fz -= d0 * Q[2] + d1 * Q[5] + d2 * Q[8];
+    }
+    if (valid) {
+        T* out = slots + (b.slot_base + e * 8 + g) * 3;
+        out[0] = fx;
+        out[1] = fy;
+        out[2] = fz;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Smoothed / RKPM cells (ComputeInternalForceSmoothedCell.h:416-442, no F-bar):
+// H = sum_k u_k (x) b_k ; P(H) ; f_k = -V b_k P^T written to the cell's slots.
+// The mixed path subtracts the first entry's displacement (partition of nullity
+// makes H invariant) before casting to FP32.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ const T* cell_grads(const CellBlockDev& b);
+template <>
+__device__ __forceinline__ const double* cell_grads<double>(const CellBlockDev& b) { return b.grads64; }
+template <>
+__device__ __forceinline__ const float* cell_grads<float>(const CellBlockDev& b) { return b.grads32; }
+
+template <typename T, int MAT>
+__global__ void __launch_bounds__(256) k_cell_force_thread(CellBlockDev b, const double4* __restrict__ U4,
+                                                            T* __restrict__ slots, int* status) {
+    const int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (c >= b.num_cells) return;
+    const int32_t s0 = b.ptr[c], s1 = b.ptr[c + 1];
+    if (s1 <= s0) return;
+    const T* gr = cell_grads<T>(b);
+    const bool diff = sizeof(T) == 4;
+    const double4 ur = U4[b.nodes[s0]];
+    T H[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) H[k] = T(0);
+    for (int32_t s = s0; s < s1; ++s) {
+        const double4 u = U4[b.nodes[s]];
+        const T du[3] = {T(diff ? u.x - ur.x : u.x), T(diff ? u.y - ur.y : u.y), T(diff ? u.z - ur.z : u.z)};
+        const T gg[3] = {gr[3 * s], gr[3 * s + 1], gr[3 * s + 2]};
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) H[i * 3 + j] += du[i] * gg[j];
+    }
+    double lam, mu;
+    element_lame(b, c, lam, mu);
+    T P[9];
+    const double Jf = stress<T>(MAT, T(lam), T(mu), H, P);
+    if (MAT == kNeoHookean && !(Jf > 0.0)) flag(status, AM_ENONPOS_J, c);
+    const T V = T(b.volumes[c]);
+    T* out = slots + b.slot_base * 3;
+    for (int32_t s = s0; s < s1; ++s) {
+        const T gg[3] = {gr[3 * s], gr[3 * s + 1], gr[3 * s + 2]};
+#pragma unroll
+        for (int i = 0; i < 3; ++i) out[3 * s + i] = (gg[0] * P[i * 3 + 0] + gg[1] * P[i * 3 + 1] + gg[2] * P[i * 3 + 2]) * -V;
+    }
+}
+
+template <typename T, int MAT>
+__global__ void __launch_bounds__(256) k_cell_force_warp(CellBlockDev b, const double4* __restrict__ U4,
+                                                          T* __restrict__ slots, int* status) {
+    const int lane = threadIdx.x & 31;
+    const int64_t c = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    if (c >= b.num_cells) return;  // whole warp exits together
+    const int32_t s0 = b.ptr[c], s1 = b.ptr[c + 1];
+    if (s1 <= s0) return;
+    const T* gr = cell_grads<T>(b);
+    const bool diff = sizeof(T) == 4;
+    const double4 ur = U4[b.nodes[s0]];
+    T H[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) H[k] = T(0);
+    for (int32_t s = s0 + lane; s < s1; s += 32) {
+        const double4 u = U4[b.nodes[s]];
+        const T du[3] = {T(diff ? u.x - ur.x : u.x), T(diff ? u.y - ur.y : u.y), T(diff ? u.z - ur.z : u.z)};
+        const T gg[3] = {gr[3 * s], gr[3 * s + 1], gr[3 * s + 2]};
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) H[i * 3 + j] += du[i] * gg[j];
+    }
+    // Butterfly reduction: fixed pairing, identical result on every lane.
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+        for (int k = 0; k < 9; ++k) H[k] += __shfl_xor_sync(kFull, H[k], off);
+    double lam, mu;
+    element_lame(b, c, lam, mu);
+    T P[9];
+    const double Jf = stress<T>(MAT, T(lam), T(mu), H, P);
+    if (lane == 0 && MAT == kNeoHookean && !(Jf > 0.0)) flag(status, AM_ENONPOS_J, c);
+    const T V = T(b.volumes[c]);
+    T* out = slots + b.slot_base * 3;
+    for (int32_t s = s0 + lane; s < s1; s += 32) {
+        const T gg[3] = {gr[3 * s], gr[3 * s + 1], gr[3 * s + 2]};
+#pragma unroll
+        for (int i = 0; i < 3; ++i) out[3 * s + i] = (gg[0] * P[i * 3 + 0] + gg[1] * P[i * 3 + 1] + gg[2] * P[i * 3 + 2]) * -V;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// VJP kernels (FP64): slots receive (dF/du)^T lam per element node; gmu/gkappa
+// receive lam^T dF/dmu_e and lam^T dF/dkappa_e (lambda_e = kappa_e - 2/3 mu_e).
+// Lambda = sum_a lam_a (x) B_a ; lam . f_e = -sum_gp w Lambda : P.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void store_theta(double* gmu, double* gk, int64_t e, double w_ldmu_ldlam,
+                                            double w_ldlam, int accumulate) {
+    if (gmu) gmu[e] = accumulate ? gmu[e] + w_ldmu_ldlam : w_ldmu_ldlam;
+    if (gk) gk[e] = accumulate ? gk[e] + w_ldlam : w_ldlam;
+}
+
+template <int MAT>
+__global__ void __launch_bounds__(256) k_tet4_vjp(GaussBlockDev b, const double4* __restrict__ X4,
+                                                   const double4* __restrict__ U4, const double4* __restrict__ L4,
+                                                   double* __restrict__ slots, double* gmu, double* gk,
+                                                   int accumulate) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= b.num_elems) return;
+    const int4 c = reinterpret_cast<const int4*>(b.conn)[e];
+    const double4 x0 = X4[c.x], x1 = X4[c.y], x2 = X4[c.z], x3 = X4[c.w];
+    const double4 u0 = U4[c.x], u1 = U4[c.y], u2 = U4[c.z], u3 = U4[c.w];
+    const double4 l0 = L4[c.x], l1 = L4[c.y], l2 = L4[c.z], l3 = L4[c.w];
+    const double J[9] = {x1.x - x0.x, x2.x - x0.x, x3.x - x0.x, x1.y - x0.y, x2.y - x0.y,
+                         x3.y - x0.y, x1.z - x0.z, x2.z - x0.z, x3.z - x0.z};
+    const double D[9] = {u1.x - u0.x, u2.x - u0.x, u3.x - u0.x, u1.y - u0.y, u2.y - u0.y,
+                         u3.y - u0.y, u1.z - u0.z, u2.z - u0.z, u3.z - u0.z};
+    const double DL[9] = {l1.x - l0.x, l2.x - l0.x, l3.x - l0.x, l1.y - l0.y, l2.y - l0.y,
+                          l3.y - l0.y, l1.z - l0.z, l2.z - l0.z, l3.z - l0.z};
+    const double det = det3(J);
+    double Ji[9];
+    cof_inv3(J, Ji, det);
+    const double w = det / 6.0;
+    double H[9], L[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            H[i * 3 + j] = D[i * 3 + 0] * Ji[0 * 3 + j] + D[i * 3 + 1] * Ji[1 * 3 + j] + D[i * 3 + 2] * Ji[2 * 3 + j];
+            L[i * 3 + j] = DL[i * 3 + 0] * Ji[0 * 3 + j] + DL[i * 3 + 1] * Ji[1 * 3 + j] + DL[i * 3 + 2] * Ji[2 * 3 + j];
+        }
+    double lam, mu;
+    element_lame(b, e, lam, mu);
+    double dP[9], ldl, ldm;
+    stress_vjp(MAT, lam, mu, H, L, dP, &ldl, &ldm);
+    double f[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const double q = w * (Ji[k * 3 + 0] * dP[i * 3 + 0] + Ji[k * 3 + 1] * dP[i * 3 + 1] + Ji[k * 3 + 2] * dP[i * 3 + 2]);
+            f[(k + 1) * 3 + i] = -q;
+            f[i] += q;
+        }
+    double* out = slots + (b.slot_base + e * 4) * 3;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) out[k] = f[k];
+    store_theta(gmu, gk, e, -w * (ldm - 2.0 / 3.0 * ldl), -w * ldl, accumulate);
+}
+
+template <int MAT>
+__global__ void __launch_bounds__(256) k_hex8_vjp(GaussBlockDev b, const double4* __restrict__ X4,
+                                                   const double4* __restrict__ U4, const double4* __restrict__ L4,
+                                                   double* __restrict__ slots, double* gmu, double* gk,
+                                                   int accumulate) {
+    __shared__ double sh[32][144];
+    const int lane = threadIdx.x & 31;
+    const int g = lane & 7;
+    const int el = threadIdx.x >> 3;
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * 32 + el;
+    const bool valid = e < b.num_elems;
+    const int32_t n = valid ? b.conn[e * 8 + g] : 0;
+    const double4 x = X4[n], u = U4[n], l = L4[n];
+    const int src = lane & ~7;
+    double* s = sh[el];
+    s[g * 9 + 0] = x.x - __shfl_sync(kFull, x.x, src);
+    s[g * 9 + 1] = x.y - __shfl_sync(kFull, x.y, src);
+    s[g * 9 + 2] = x.z - __shfl_sync(kFull, x.z, src);
+    s[g * 9 + 3] = u.x - __shfl_sync(kFull, u.x, src);
+    s[g * 9 + 4] = u.y - __shfl_sync(kFull, u.y, src);
+    s[g * 9 + 5] = u.z - __shfl_sync(kFull, u.z, src);
+    s[g * 9 + 6] = l.x - __shfl_sync(kFull, l.x, src);
+    s[g * 9 + 7] = l.y - __shfl_sync(kFull, l.y, src);
+    s[g * 9 + 8] = l.z - __shfl_sync(kFull, l.z, src);
+    __syncwarp();
+    const double c = 0.57735026918962576451;
+    double cp[3], cm[3], sg[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        sg[j] = hex_sign(g, j);
+        cp[j] = 1.0 + sg[j] * c;
+        cm[j] = 1.0 - sg[j] * c;
+    }
+    double J[9], G[9], GL[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) J[k] = G[k] = GL[k] = 0.0;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        const double f0 = hex_sign_c(a, 0) > 0 ? cp[0] : cm[0];
+        const double f1 = hex_sign_c(a, 1) > 0 ? cp[1] : cm[1];
+        const double f2 = hex_sign_c(a, 2) > 0 ? cp[2] : cm[2];
+        const double dN[3] = {0.125 * hex_sign_c(a, 0) * f1 * f2, 0.125 * hex_sign_c(a, 1) * f0 * f2,
+                              0.125 * hex_sign_c(a, 2) * f0 * f1};
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                J[i * 3 + j] += s[a * 9 + i] * dN[j];
+                G[i * 3 + j] += s[a * 9 + 3 + i] * dN[j];
+                GL[i * 3 + j] += s[a * 9 + 6 + i] * dN[j];
+            }
+    }
+    const double det = det3(J);
+    double Ji[9];
+    cof_inv3(J, Ji, det);
+    double H[9], L[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            H[i * 3 + j] = G[i * 3 + 0] * Ji[0 * 3 + j] + G[i * 3 + 1] * Ji[1 * 3 + j] + G[i * 3 + 2] * Ji[2 * 3 + j];
+            L[i * 3 + j] = GL[i * 3 + 0] * Ji[0 * 3 + j] + GL[i * 3 + 1] * Ji[1 * 3 + j] + GL[i * 3 + 2] * Ji[2 * 3 + j];
+        }
+    double lam = 0.0, mu = 0.0;
+    if (valid) element_lame(b, e, lam, mu);
+    double dP[9], ldl, ldm;
+    stress_vjp(MAT, lam, mu, H, L, dP, &ldl, &ldm);
+    double tm = -det * (ldm - 2.0 / 3.0 * ldl), tk = -det * ldl;
+    double* q = s + 72 + g * 9;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            q[k * 3 + i] = det * (Ji[k * 3 + 0] * dP[i * 3 + 0] + Ji[k * 3 + 1] * dP[i * 3 + 1] + Ji[k * 3 + 2] * dP[i * 3 + 2]);
+#pragma unroll
+    for (int off = 4; off > 0; off >>= 1) {
+        tm += __shfl_xor_sync(kFull, tm, off);
+        tk += __shfl_xor_sync(kFull, tk, off);
+    }
+    __syncwarp();
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+#pragma unroll
+    for (int gp = 0; gp < 8; ++gp) {
+        const double f0 = hex_sign_c(gp, 0) > 0 ? cp[0] : cm[0];
+        const double f1 = hex_sign_c(gp, 1) > 0 ? cp[1] : cm[1];
+        const double f2 = hex_sign_c(gp, 2) > 0 ? cp[2] : cm[2];
+        const double d0 = 0.125 * sg[0] * f1 * f2, d1 = 0.125 * sg[1] * f0 * f2, d2 = 0.125 * sg[2] * f0 * f1;
+        const double* Q = s + 72 + gp * 9;
+        fx -= d0 * Q[0] + d1 * Q[3] + d2 * Q[6];
+        fy -= d0 * Q[1] + d1 * Q[4] + d2 * Q[7];
+        fz -= d0 * Q[2] + d1 * Q[5] + d2 * Q[8];
+    }
+    if (valid) {
+        double* out = slots + (b.slot_base + e * 8 + g) * 3;
+        out[0] = fx;
+        out[1] = fy;
+        out[2] = fz;
+        if (g == 0) store_theta(gmu, gk, e, tm, tk, accumulate);
+    }
+}
+
+template <int MAT>
+__global__ void __launch_bounds__(256) k_cell_vjp(CellBlockDev b, const double4* __restrict__ U4,
+                                                   const double4* __restrict__ L4, double* __restrict__ slots,
+                                                   double* gmu, double* gk, int accumulate) {
+    const int lane = threadIdx.x & 31;
+    const int64_t c = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    if (c >= b.num_cells) return;
+    const int32_t s0 = b.ptr[c], s1 = b.ptr[c + 1];
+    double H[9], L[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) H[k] = L[k] = 0.0;
+    for (int32_t s = s0 + lane; s < s1; s += 32) {
+        const int32_t n = b.nodes[s];
+        const double4 u = U4[n], l = L4[n];
+        const double gg[3] = {b.grads64[3 * s], b.grads64[3 * s + 1], b.grads64[3 * s + 2]};
+        const double uu[3] = {u.x, u.y, u.z}, ll[3] = {l.x, l.y, l.z};
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                H[i * 3 + j] += uu[i] * gg[j];
+                L[i * 3 + j] += ll[i] * gg[j];
+            }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            H[k] += __shfl_xor_sync(kFull, H[k], off);
+            L[k] += __shfl_xor_sync(kFull, L[k], off);
+        }
+    double lam, mu;
+    element_lame(b, c, lam, mu);
+    double dP[9], ldl, ldm;
+    stress_vjp(MAT, lam, mu, H, L, dP, &ldl, &ldm);
+    const double V = b.volumes[c];
+    double* out = slots + b.slot_base * 3;
+    for (int32_t s = s0 + lane; s < s1; s += 32) {
+        const double gg[3] = {b.grads64[3 * s], b.grads64[3 * s + 1], b.grads64[3 * s + 2]};
+#pragma unroll
+        for (int i = 0; i < 3; ++i) out[3 * s + i] = (gg[0] * dP[i * 3 + 0] + gg[1] * dP[i * 3 + 1] + gg[2] * dP[i * 3 + 2]) * -V;
+    }
+    if (lane == 0) store_theta(gmu, gk, c, -V * (ldm - 2.0 / 3.0 * ldl), -V * ldl, accumulate);
+}
+
+// ---------------------------------------------------------------------------
+// Lumped mass slots (src/MassUtils.cpp:17-46): slot (e, a) = rho V_e / n_en with
+// V_e = sum_gp w_gp (ComputeElementVolumeFunctor.h:20-79).
+// ---------------------------------------------------------------------------
+__global__ void k_gauss_volume_slots(GaussBlockDev b, double density, const double4* __restrict__ X4,
+                                     double* __restrict__ slots) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= b.num_elems) return;
+    const int nn = b.kind == AM_HEX8_GAUSS ? 8 : 4;
+    double X[24];
+    for (int a = 0; a < nn; ++a) {
+        const double4 x = X4[b.conn[e * nn + a]];
+        X[a * 3 + 0] = x.x;
+        X[a * 3 + 1] = x.y;
+        X[a * 3 + 2] = x.z;
+    }
+    double V = 0.0;
+    const int ngp = nn == 8 ? 8 : 1;
+    for (int gp = 0; gp < ngp; ++gp) {
+        double dN[24];
+        if (nn == 8) {
+            const double loc = 1.0 / sqrt(3.0);
+            const double xi[3] = {hex_sign(gp, 0) * loc, hex_sign(gp, 1) * loc, hex_sign(gp, 2) * loc};
+            for (int a = 0; a < 8; ++a) {
+                const double p0 = hex_sign(a, 0), p1 = hex_sign(a, 1), p2 = hex_sign(a, 2);
+                dN[a * 3 + 0] = 0.125 * p0 * (1.0 + p1 * xi[1]) * (1.0 + p2 * xi[2]);
+                dN[a * 3 + 1] = 0.125 * p1 * (1.0 + p0 * xi[0]) * (1.0 + p2 * xi[2]);
+                dN[a * 3 + 2] = 0.125 * p2 * (1.0 + p0 * xi[0]) * (1.0 + p1 * xi[1]);
+            }
+        } else {
+            const double t[12] = {-1, -1, -1, 1, 0, 0, 0, 1, 0, 0, 0, 1};
+            for (int k = 0; k < 12; ++k) dN[k] = t[k];
+        }
+        double J[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                double acc = 0.0;
+                for (int a = 0; a < nn; ++a) acc += X[a * 3 + i] * dN[a * 3 + j];
+                J[i * 3 + j] = acc;
+            }
+        V += (nn == 8 ? 1.0 : 1.0 / 6.0) * det3(J);
+    }
+    const double me = V * density / nn;
+    for (int a = 0; a < nn; ++a) {
+        double* out = slots + (b.slot_base + e * nn + a) * 3;
+        out[0] = me;
+        out[1] = 0.0;
+        out[2] = 0.0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Node kernels.
+// ---------------------------------------------------------------------------
+template <typename S>
+__device__ __forceinline__ void gather(const NodeDev& nd, const S* __restrict__ slots, int64_t i, double& fx,
+                                       double& fy, double& fz) {
+    const int32_t p0 = nd.node_ptr[i], p1 = nd.node_ptr[i + 1];
+    fx = fy = fz = 0.0;
+    for (int32_t p = p0; p < p1; ++p) {
+        const int64_t s = nd.node_slots[p];
+        fx += static_cast<double>(slots[3 * s + 0]);
+        fy += static_cast<double>(slots[3 * s + 1]);
+        fz += static_cast<double>(slots[3 * s + 2]);
+    }
+}
+
+// BoundaryCondition::ApplyVelocity / ApplyAcceleration: for each component the
+// last active BC in list order that prescribes it overwrites the value.
+__device__ __forceinline__ void apply_bc(uint32_t word, uint32_t active, const double* __restrict__ scale,
+                                         const double* __restrict__ values, double& x, double& y, double& z) {
+    uint32_t m = word & 0x3FFu & active;
+    if (m) {
+        const int k = 31 - __clz(m);
+        x = values[k * 3 + 0] * scale[k];
+    }
+    m = (word >> 10) & 0x3FFu & active;
+    if (m) {
+        const int k = 31 - __clz(m);
+        y = values[k * 3 + 1] * scale[k];
+    }
+    m = (word >> 20) & 0x3FFu & active;
+    if (m) {
+        const int k = 31 - __clz(m);
+        z = values[k * 3 + 2] * scale[k];
+    }
+}
+
+__device__ __forceinline__ void free_mask(uint32_t word, uint32_t active, double& mx, double& my, double& mz) {
+    mx = (word & 0x3FFu & active) ? 0.0 : 1.0;
+    my = ((word >> 10) & 0x3FFu & active) ? 0.0 : 1.0;
+    mz = ((word >> 20) & 0x3FFu & active) ? 0.0 : 1.0;
+}
+
+template <typename S>
+__global__ void __launch_bounds__(256) k_gather_force(NodeDev nd, const S* __restrict__ slots, double* __restrict__ f,
+                                                       int accumulate) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nd.num_nodes) return;
+    double fx, fy, fz;
+    gather(nd, slots, i, fx, fy, fz);
+    if (accumulate) {
+        f[3 * i + 0] += fx;
+        f[3 * i + 1] += fy;
+        f[3 * i + 2] += fz;
+    } else {
+        f[3 * i + 0] = fx;
+        f[3 * i + 1] = fy;
+        f[3 * i + 2] = fz;
+    }
+}
+
+template <typename S>
+__global__ void __launch_bounds__(256) k_init_accel(NodeDev nd, const S* __restrict__ slots, double4* __restrict__ A4,
+                                                     int* status) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nd.num_nodes) return;
+    double fx, fy, fz;
+    gather(nd, slots, i, fx, fy, fz);
+    const double m = nd.mass[i];
+    if (nd.has_g) {
+        fx += nd.g[0] * m;
+        fy += nd.g[1] * m;
+        fz += nd.g[2] * m;
+    }
+    const double ax = fx / m, ay = fy / m, az = fz / m;
+    if (!isfinite(ax) || !isfinite(ay) || !isfinite(az)) flag(status, AM_ENAN, i);
+    A4[i] = make_double4(ax, ay, az, 0.0);
+}
+
+__global__ void __launch_bounds__(256) k_prologue(NodeDev nd, const StepParams* __restrict__ table,
+                                                   double4* __restrict__ U4, double4* __restrict__ V4,
+                                                   const double4* __restrict__ A4, double4* __restrict__ u_copy) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nd.num_nodes) return;
+    const StepParams& P = table[0];
+    const double4 v = V4[i], a = A4[i];
+    double vx = v.x + P.half * a.x, vy = v.y + P.half * a.y, vz = v.z + P.half * a.z;
+    const uint32_t w = nd.bcword[i];
+    if (w) apply_bc(w, P.vact, P.vscale, nd.bcvalues, vx, vy, vz);
+    double4 u = U4[i];
+    u.x = u.x + P.dt * vx;
+    u.y = u.y + P.dt * vy;
+    u.z = u.z + P.dt * vz;
+    U4[i] = u;
+    V4[i] = make_double4(vx, vy, vz, 0.0);
+    if (u_copy) u_copy[i] = u;
+}
+
+template <typename S>
+__global__ void __launch_bounds__(256) k_node_step(NodeDev nd, const S* __restrict__ slots,
+                                                    const StepParams* __restrict__ table, int64_t step, int advance,
+                                                    double4* __restrict__ U4, double4* __restrict__ V4,
+                                                    double4* __restrict__ A4, double4* __restrict__ u_copy,
+                                                    int* status) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nd.num_nodes) return;
+    double fx, fy, fz;
+    gather(nd, slots, i, fx, fy, fz);
+    const double m = nd.mass[i];
+    if (nd.has_g) {
+        fx += nd.g[0] * m;
+        fy += nd.g[1] * m;
+        fz += nd.g[2] * m;
+    }
+    // a^{n+1} = f / m (ExplicitTimeIntegrator.h:247-283), then the acceleration BC at t^{n+1}.
+    double ax = fx / m, ay = fy / m, az = fz / m;
+    const uint32_t w = nd.bcword[i];
+    const StepParams& P = table[step];
+    if (w) apply_bc(w, P.aact, P.ascale, nd.bcvalues, ax, ay, az);
+    if (!isfinite(ax) || !isfinite(ay) || !isfinite(az)) flag(status, AM_ENAN, i);
+    // v^{n+1} = v^{n+1/2} + dt/2 a^{n+1} (:329-364)
+    const double4 vh = V4[i];
+    const double vx = vh.x + P.half * ax, vy = vh.y + P.half * ay, vz = vh.z + P.half * az;
+    if (advance) {
+        // Next step: v^{n+3/2} = v^{n+1} + dt'/2 a^{n+1} (:286-326), velocity BC at t_mid',
+        // u^{n+2} = u^{n+1} + dt' v^{n+3/2} (:97-134).
+        const StepParams& Q = table[step + 1];
+        double wx = vx + Q.half * ax, wy = vy + Q.half * ay, wz = vz + Q.half * az;
+        if (w) apply_bc(w, Q.vact, Q.vscale, nd.bcvalues, wx, wy, wz);
+        double4 u = U4[i];
+        u.x = u.x + Q.dt * wx;
+        u.y = u.y + Q.dt * wy;
+        u.z = u.z + Q.dt * wz;
+        U4[i] = u;
+        V4[i] = make_double4(wx, wy, wz, 0.0);
+        if (u_copy) u_copy[i] = u;
+    } else {
+        V4[i] = make_double4(vx, vy, vz, 0.0);
+        A4[i] = make_double4(ax, ay, az, 0.0);
+    }
+}
+
+// Reverse of the acceleration step: lam = Ma (abar + h vbar) / m, the cotangent
+// of the internal force at step `step`.
+__global__ void k_adj_prep(NodeDev nd, const StepParams* __restrict__ table, int64_t step,
+                           const double4* __restrict__ VB, const double4* __restrict__ AB, double4* __restrict__ L4) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nd.num_nodes) return;
+    const StepParams& P = table[step];
+    const double m = nd.mass[i];
+    double mx, my, mz;
+    free_mask(nd.bcword[i], P.aact, mx, my, mz);
+    const double4 vb = VB[i], ab = AB[i];
+    L4[i] = make_double4(mx * (ab.x + P.half * vb.x) / m, my * (ab.y + P.half * vb.y) / m,
+                         mz * (ab.z + P.half * vb.z) / m, 0.0);
+}
+
+// Reverse of the rest of step `step` given g = (dF/du)^T lam in the slots; then
+// prepares lam for step-1 (or for the initial acceleration when step == 0).
+__global__ void __launch_bounds__(256) k_adj_update(NodeDev nd, const double* __restrict__ slots,
+                                                     const StepParams* __restrict__ table, int64_t step,
+                                                     double4* __restrict__ UB, double4* __restrict__ VB,
+                                                     double4* __restrict__ AB, double4* __restrict__ L4) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nd.num_nodes) return;
+    double gx, gy, gz;
+    gather(nd, slots, i, gx, gy, gz);
+    const StepParams& P = table[step];
+    double4 ub = UB[i];
+    const double4 vb = VB[i];
+    ub.x += gx;
+    ub.y += gy;
+    ub.z += gz;
+    const uint32_t w = nd.bcword[i];
+    double mx, my, mz;
+    free_mask(w, P.vact, mx, my, mz);
+    const double wx = mx * (vb.x + P.dt * ub.x), wy = my * (vb.y + P.dt * ub.y), wz = mz * (vb.z + P.dt * ub.z);
+    const double ax = P.half * wx, ay = P.half * wy, az = P.half * wz;
+    UB[i] = ub;
+    VB[i] = make_double4(wx, wy, wz, 0.0);
+    AB[i] = make_double4(ax, ay, az, 0.0);
+    const double m = nd.mass[i];
+    if (step > 0) {
+        const StepParams& Q = table[step - 1];
+        free_mask(w, Q.aact, mx, my, mz);
+        L4[i] = make_double4(mx * (ax + Q.half * wx) / m, my * (ay + Q.half * wy) / m, mz * (az + Q.half * wz) / m, 0.0);
+    } else {
+        L4[i] = make_double4(ax / m, ay / m, az / m, 0.0);
+    }
+}
+
+// Loss L = sum_s |u_s|^2 and its cotangent 2 u_s, in sensor order (one thread).
+__global__ void k_sensor_seed(const double4* __restrict__ U4, int32_t num_sensors, const int32_t* __restrict__ sensors,
+                              double4* __restrict__ UB, double* loss) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    double L = 0.0;
+    for (int32_t k = 0; k < num_sensors; ++k) {
+        const int32_t n = sensors[k];
+        const double4 u = U4[n];
+        L += u.x * u.x;
+        L += u.y * u.y;
+        L += u.z * u.z;
+        double4 ub = UB[n];
+        ub.x += 2.0 * u.x;
+        ub.y += 2.0 * u.y;
+        ub.z += 2.0 * u.z;
+        UB[n] = ub;
+    }
+    *loss = L;
+}
+
+__global__ void k_pack4(const double* __restrict__ in, double4* __restrict__ out, int64_t n) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = make_double4(in[3 * i], in[3 * i + 1], in[3 * i + 2], 0.0);
+}
+__global__ void k_unpack4(const double4* __restrict__ in, double* __restrict__ out, int64_t n) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4 v = in[i];
+    out[3 * i] = v.x;
+    out[3 * i + 1] = v.y;
+    out[3 * i + 2] = v.z;
+}
+__global__ void k_zero4(double4* __restrict__ out, int64_t n) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = make_double4(0.0, 0.0, 0.0, 0.0);
+}
+
+__global__ void k_stress_batch(int32_t mat, double lambda, double mu, int64_t n, const double* __restrict__ H,
+                               double* __restrict__ P) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double h[9], p[9];
+    for (int k = 0; k < 9; ++k) h[k] = H[9 * i + k];
+    stress<double>(mat, lambda, mu, h, p);
+    for (int k = 0; k < 9; ++k) P[9 * i + k] = p[k];
+}
+
+// Quadrature point kernel: Gauss B and w (QuadratureGaussian.h:17-39) or the
+// smoothed face-normal quadrature (QuadratureSmoothed.h:32-142).
+__global__ void k_quadrature_batch(int32_t kind, int32_t smoothed, int64_t n, const double* __restrict__ Xall,
+                                   double* __restrict__ Ball, double* __restrict__ wall) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const int nn = kind == AM_HEX8_GAUSS ? 8 : 4;
+    const double* X = Xall + e * nn * 3;
+    if (smoothed) {
+        double B[24];
+        for (int k = 0; k < nn * 3; ++k) B[k] = 0.0;
+        double vol = 0.0;
+        if (nn == 4) {
+            const int faces[4][3] = {{0, 1, 3}, {1, 2, 3}, {0, 3, 2}, {0, 2, 1}};
+            for (int j = 0; j < 4; ++j) {
+                const double* p0 = X + 3 * faces[j][0];
+                const double* p1 = X + 3 * faces[j][1];
+                const double* p2 = X + 3 * faces[j][2];
+                const double e1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+                const double e2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
+                const double nr[3] = {(e1[1] * e2[2] - e1[2] * e2[1]) / 2.0, (e1[2] * e2[0] - e1[0] * e2[2]) / 2.0,
+                                      (e1[0] * e2[1] - e1[1] * e2[0]) / 2.0};
+                vol += p0[0] * nr[0] + p0[1] * nr[1] + p0[2] * nr[2];
+                for (int l = 0; l < 3; ++l)
+                    for (int i = 0; i < 3; ++i) B[faces[j][l] * 3 + i] += nr[i] / 3.0;
+            }
+        } else {
+            const int faces[6][4] = {{0, 1, 5, 4}, {1, 2, 6, 5}, {2, 3, 7, 6}, {0, 4, 7, 3}, {0, 3, 2, 1}, {4, 5, 6, 7}};
+            for (int j = 0; j < 6; ++j) {
+                double mid[3] = {0.0, 0.0, 0.0};
+                for (int k = 0; k < 4; ++k)
+                    for (int i = 0; i < 3; ++i) mid[i] += X[faces[j][k] * 3 + i];
+                for (int i = 0; i < 3; ++i) mid[i] /= 4.0;
+                int km1 = 3;
+                for (int k = 0; k < 4; ++k) {
+                    double e1[3], e2[3];
+                    for (int i = 0; i < 3; ++i) {
+                        e1[i] = X[faces[j][km1] * 3 + i] - mid[i];
+                        e2[i] = X[faces[j][k] * 3 + i] - mid[i];
+                    }
+                    const double nr[3] = {(e1[1] * e2[2] - e1[2] * e2[1]) / 2.0, (e1[2] * e2[0] - e1[0] * e2[2]) / 2.0,
+                                          (e1[0] * e2[1] - e1[1] * e2[0]) / 2.0};
+                    vol += mid[0] * nr[0] + mid[1] * nr[1] + mid[2] * nr[2];
+                    for (int l = 0; l < 4; ++l) {
+                        const double wgt = (l == k || l == km1) ? 5.0 / 12.0 : 1.0 / 12.0;
+                        for (int i = 0; i < 3; ++i) B[faces[j][l] * 3 + i] += nr[i] * wgt;
+                    }
+                    km1 = k;
+                }
+            }
+        }
+        vol /= 3.0;
+        for (int k = 0; k < nn * 3; ++k) Ball[e * nn * 3 + k] = B[k] / vol;
+        wall[e] = vol;
+        return;
+    }
+    const int ngp = nn == 8 ? 8 : 1;
+    for (int gp = 0; gp < ngp; ++gp) {
+        double dN[24];
+        if (nn == 8) {
+            const double loc = 1.0 / sqrt(3.0);
+            const double xi[3] = {hex_sign(gp, 0) * loc, hex_sign(gp, 1) * loc, hex_sign(gp, 2) * loc};
+            for (int a = 0; a < 8; ++a) {
+                const double p0 = hex_sign(a, 0), p1 = hex_sign(a, 1), p2 = hex_sign(a, 2);
+                dN[a * 3 + 0] = 0.125 * p0 * (1.0 + p1 * xi[1]) * (1.0 + p2 * xi[2]);
+                dN[a * 3 + 1] = 0.125 * p1 * (1.0 + p0 * xi[0]) * (1.0 + p2 * xi[2]);
+                dN[a * 3 + 2] = 0.125 * p2 * (1.0 + p0 * xi[0]) * (1.0 + p1 * xi[1]);
+            }
+        } else {
+            const double t[12] = {-1, -1, -1, 1, 0, 0, 0, 1, 0, 0, 0, 1};
+            for (int k = 0; k < 12; ++k) dN[k] = t[k];
+        }
+        double J[9], Ji[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                double acc = 0.0;
+                for (int a = 0; a < nn; ++a) acc += X[a * 3 + i] * dN[a * 3 + j];
+                J[i * 3 + j] = acc;
+            }
+        const double det = det3(J);
+        cof_inv3(J, Ji, det);
+        double* B = Ball + (e * ngp + gp) * nn * 3;
+        for (int a = 0; a < nn; ++a)
+            for (int j = 0; j < 3; ++j)
+                B[a * 3 + j] = dN[a * 3 + 0] * Ji[0 * 3 + j] + dN[a * 3 + 1] * Ji[1 * 3 + j] + dN[a * 3 + 2] * Ji[2 * 3 + j];
+        wall[e * ngp + gp] = (nn == 8 ? 1.0 : 1.0 / 6.0) * det;
+    }
+}
+
+inline unsigned grid_for(int64_t n, int per_block) { return static_cast<unsigned>((n + per_block - 1) / per_block); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Launchers
+// ---------------------------------------------------------------------------
+#define AM_DISPATCH_MAT(MATVAR, CALL)                    \
+    switch (MATVAR) {                                    \
+        case kLinearElastic: { constexpr int M = 0; CALL; break; } \
+        case kNeoHookean: { constexpr int M = 1; CALL; break; }    \
+        default: { constexpr int M = 2; CALL; break; }             \
+    }
+
+void launch_gauss_force(const GaussBlockDev& b, int mixed, const double4* X4, const double4* U4, void* slots,
+                        int* status, cudaStream_t s) {
+    if (b.num_elems == 0) return;
+    if (b.kind == AM_TET4_GAUSS) {
+        const unsigned grid = grid_for(b.num_elems, 256);
+        if (mixed) {
+            AM_DISPATCH_MAT(b.material, (k_tet4_force<float, M><<<grid, 256, 0, s>>>(b, X4, U4, static_cast<float*>(slots), status)));
+        } else {
+            AM_DISPATCH_MAT(b.material, (k_tet4_force<double, M><<<grid, 256, 0, s>>>(b, X4, U4, static_cast<double*>(slots), status)));
+        }
+    } else {
+        const unsigned grid = grid_for(b.num_elems, 32);
+        if (mixed) {
+            AM_DISPATCH_MAT(b.material, (k_hex8_force<float, M><<<grid, 256, 0, s>>>(b, X4, U4, static_cast<float*>(slots), status)));
+        } else {
+            AM_DISPATCH_MAT(b.material, (k_hex8_force<double, M><<<grid, 256, 0, s>>>(b, X4, U4, static_cast<double*>(slots), status)));
+        }
+    }
+}
+
+void launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void* slots, int* status, cudaStream_t s) {
+    if (b.num_cells == 0) return;
+    if (b.max_entries <= 8) {
+        const unsigned grid = grid_for(b.num_cells, 256);
+        if (mixed) {
+            AM_DISPATCH_MAT(b.material, (k_cell_force_thread<float, M><<<grid, 256, 0, s>>>(b, U4, static_cast<float*>(slots), status)));
+        } else {
+            AM_DISPATCH_MAT(b.material, (k_cell_force_thread<double, M><<<grid, 256, 0, s>>>(b, U4, static_cast<double*>(slots), status)));
+        }
+    } else {
+        const unsigned grid = grid_for(b.num_cells * 32, 256);
+        if (mixed) {
+            AM_DISPATCH_MAT(b.material, (k_cell_force_warp<float, M><<<grid, 256, 0, s>>>(b, U4, static_cast<float*>(slots), status)));
+        } else {
+            AM_DISPATCH_MAT(b.material, (k_cell_force_warp<double, M><<<grid, 256, 0, s>>>(b, U4, static_cast<double*>(slots), status)));
+        }
+    }
+}
+
+void launch_gauss_vjp(const GaussBlockDev& b, const double4* X4, const double4* U4, const double4* L4, double* slots,
+                      double* gmu, double* gkappa, int accumulate, cudaStream_t s) {
+    if (b.num_elems == 0) return;
+    if (b.kind == AM_TET4_GAUSS) {
+        const unsigned grid = grid_for(b.num_elems, 256);
+        AM_DISPATCH_MAT(b.material, (k_tet4_vjp<M><<<grid, 256, 0, s>>>(b, X4, U4, L4, slots, gmu, gkappa, accumulate)));
+    } else {
+        const unsigned grid = grid_for(b.num_elems, 32);
+        AM_DISPATCH_MAT(b.material, (k_hex8_vjp<M><<<grid, 256, 0, s>>>(b, X4, U4, L4, slots, gmu, gkappa, accumulate)));
+    }
+}
+
+void launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double* slots, double* gmu,
+                     double* gkappa, int accumulate, cudaStream_t s) {
+    if (b.num_cells == 0) return;
+    const unsigned grid = grid_for(b.num_cells * 32, 256);
+    AM_DISPATCH_MAT(b.material, (k_cell_vjp<M><<<grid, 256, 0, s>>>(b, U4, L4, slots, gmu, gkappa, accumulate)));
+}
+
+void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const double4* X4, double* slots,
+                               cudaStream_t s) {
+    if (b.num_elems == 0) return;
+    k_gauss_volume_slots<<<grid_for(b.num_elems, 128), 128, 0, s>>>(b, density, X4, slots);
+}
+
+void launch_gather_force(const NodeDev& nd, int mixed, const void* slots, double* f, int accumulate, cudaStream_t s) {
+    const unsigned grid = grid_for(nd.num_nodes, 256);
+    if (mixed)
+        k_gather_force<float><<<grid, 256, 0, s>>>(nd, static_cast<const float*>(slots), f, accumulate);
+    else
+        k_gather_force<double><<<grid, 256, 0, s>>>(nd, static_cast<const double*>(slots), f, accumulate);
+}
+
+void launch_init_accel(const NodeDev& nd, int mixed, const void* slots, double4* A4, int* status, cudaStream_t s) {
+    const unsigned grid = grid_for(nd.num_nodes, 256);
+    if (mixed)
+        k_init_accel<float><<<grid, 256, 0, s>>>(nd, static_cast<const float*>(slots), A4, status);
+    else
+        k_init_accel<double><<<grid, 256, 0, s>>>(nd, static_cast<const double*>(slots), A4, status);
+}
+
+void launch_prologue(const NodeDev& nd, const StepParams* table, double4* U4, double4* V4, const double4* A4,
+                     double4* u_copy, cudaStream_t s) {
+    k_prologue<<<grid_for(nd.num_nodes, 256), 256, 0, s>>>(nd, table, U4, V4, A4, u_copy);
+}
+
+void launch_node_step(const NodeDev& nd, int mixed, const void* slots, const StepParams* table, int64_t step,
+                      int advance, double4* U4, double4* V4, double4* A4, double4* u_copy, int* status,
+                      cudaStream_t s) {
+    const unsigned grid = grid_for(nd.num_nodes, 256);
+    if (mixed)
+        k_node_step<float><<<grid, 256, 0, s>>>(nd, static_cast<const float*>(slots), table, step, advance, U4, V4, A4, u_copy, status);
+    else
+        k_node_step<double><<<grid, 256, 0, s>>>(nd, static_cast<const double*>(slots), table, step, advance, U4, V4, A4, u_copy, status);
+}
+
+void launch_adj_prep(const NodeDev& nd, const StepParams* table, int64_t step, const double4* VB, const double4* AB,
+                     double4* L4, cudaStream_t s) {
+    k_adj_prep<<<grid_for(nd.num_nodes, 256), 256, 0, s>>>(nd, table, step, VB, AB, L4);
+}
+
+void launch_adj_update(const NodeDev& nd, const double* slots, const StepParams* table, int64_t step, double4* UB,
+                       double4* VB, double4* AB, double4* L4, cudaStream_t s) {
+    k_adj_update<<<grid_for(nd.num_nodes, 256), 256, 0, s>>>(nd, slots, table, step, UB, VB, AB, L4);
+}
+
+void launch_sensor_seed(const double4* U4, int32_t num_sensors, const int32_t* sensors, double4* UB, double* loss,
+                        cudaStream_t s) {
+    k_sensor_seed<<<1, 1, 0, s>>>(U4, num_sensors, sensors, UB, loss);
+}
+
+void launch_pack4(const double* aos3, double4* out, int64_t n, cudaStream_t s) {
+    if (n > 0) k_pack4<<<grid_for(n, 256), 256, 0, s>>>(aos3, out, n);
+}
+void launch_unpack4(const double4* in, double* aos3, int64_t n, cudaStream_t s) {
+    if (n > 0) k_unpack4<<<grid_for(n, 256), 256, 0, s>>>(in, aos3, n);
+}
+void launch_zero4(double4* out, int64_t n, cudaStream_t s) {
+    if (n > 0) k_zero4<<<grid_for(n, 256), 256, 0, s>>>(out, n);
+}
+
+void launch_stress_batch(int32_t mat, double lambda, double mu, int64_t n, const double* H, double* P,
+                         cudaStream_t s) {
+    if (n > 0) k_stress_batch<<<grid_for(n, 128), 128, 0, s>>>(mat, lambda, mu, n, H, P);
+}
+
+void launch_quadrature_batch(int32_t kind, int32_t smoothed, int64_t n, const double* X, double* B, double* w,
+                             cudaStream_t s) {
+    if (n > 0) k_quadrature_batch<<<grid_for(n, 64), 64, 0, s>>>(kind, smoothed, n, X, B, w);
+}
+
+}  // namespace am

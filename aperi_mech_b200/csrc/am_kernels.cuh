@@ -1,0 +1,106 @@
+// am_kernels.cuh -- device kernels of the explicit-dynamics hot path and their launch helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/aperi_b200.h"
+
+namespace am {
+
+// Per-step parameters of the central-difference loop, built on the host from the
+// time stepper and the boundary-condition time functions (device table).
+struct StepParams {
+    double dt;                 // time increment of the step
+    double half;               // 0.5 * dt
+    uint32_t vact;             // bit k: BC k active at t_mid (velocity overwrite)
+    uint32_t aact;             // bit k: BC k active at t_next (acceleration overwrite)
+    double vscale[AM_MAX_BCS]; // velocity time-function value of BC k at t_mid
+    double ascale[AM_MAX_BCS]; // acceleration time-function value of BC k at t_next
+};
+
+// Device status word: [0] = first am_status error code, [1] = offending entity.
+enum StatusSlot { kStatusCode = 0, kStatusIndex = 1 };
+
+// Gauss-element block on the device.
+struct GaussBlockDev {
+    int32_t kind;      // AM_TET4_GAUSS / AM_HEX8_GAUSS
+    int32_t material;
+    double lambda, mu;
+    int64_t num_elems;
+    const int32_t* conn;
+    const double* mu_field;     // may be null
+    const double* kappa_field;  // may be null
+    int64_t slot_base;          // first slot of this block in the global slot array
+};
+
+struct CellBlockDev {
+    int32_t material;
+    double lambda, mu;
+    int64_t num_cells;
+    const int32_t* ptr;         // num_cells + 1 (entry offsets, block-local)
+    const int32_t* nodes;       // entries
+    const double* grads64;      // entries x 3
+    const float* grads32;       // entries x 3 (mixed path), may be null
+    const double* volumes;
+    const double* mu_field;
+    const double* kappa_field;
+    int64_t slot_base;
+    int32_t max_entries;        // longest cell (selects thread- or warp-per-cell)
+};
+
+// Node gather + nodal update configuration.
+struct NodeDev {
+    int64_t num_nodes;
+    const int32_t* node_ptr;    // num_nodes + 1 offsets into node_slots
+    const int32_t* node_slots;  // ascending slot ids of each node
+    const double* mass;
+    const uint32_t* bcword;     // per node: 3 x 10-bit masks of BCs prescribing x, y, z
+    const double* bcvalues;     // AM_MAX_BCS x 3 prescribed values
+    double g[3];                // body acceleration
+    int32_t has_g;
+};
+
+// ---- launchers (am_kernels.cu) ----
+void launch_gauss_force(const GaussBlockDev& b, int mixed, const double4* X4, const double4* U4, void* slots,
+                        int* status, cudaStream_t s);
+void launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void* slots, int* status, cudaStream_t s);
+void launch_gauss_vjp(const GaussBlockDev& b, const double4* X4, const double4* U4, const double4* L4, double* slots,
+                      double* gmu, double* gkappa, int accumulate, cudaStream_t s);
+void launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double* slots, double* gmu,
+                     double* gkappa, int accumulate, cudaStream_t s);
+void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const double4* X4, double* slots,
+                               cudaStream_t s);
+void launch_cell_volume_slots(const CellBlockDev& b, double* slots, cudaStream_t s);
+
+// f (N x 3, row-major) = gather of the slots (FP64 or FP32 slots), overwrite or accumulate.
+void launch_gather_force(const NodeDev& nd, int mixed, const void* slots, double* f, int accumulate, cudaStream_t s);
+// a = (f + g m) / m with no boundary condition (pre-loop acceleration).
+void launch_init_accel(const NodeDev& nd, int mixed, const void* slots, double4* A4, int* status, cudaStream_t s);
+// First half-step of a run: vh = v + h a ; BC(vh) ; u += dt vh.
+void launch_prologue(const NodeDev& nd, const StepParams* table, double4* U4, double4* V4, const double4* A4,
+                     double4* u_copy, cudaStream_t s);
+// Gather + a = f/m ; BC(a) ; v = vh + h a ; then either advance (next vh, BC, u) or store (v, a).
+void launch_node_step(const NodeDev& nd, int mixed, const void* slots, const StepParams* table, int64_t step,
+                      int advance, double4* U4, double4* V4, double4* A4, double4* u_copy, int* status,
+                      cudaStream_t s);
+// Adjoint node kernels.
+void launch_adj_prep(const NodeDev& nd, const StepParams* table, int64_t step, const double4* VB, const double4* AB,
+                     double4* L4, cudaStream_t s);
+void launch_adj_update(const NodeDev& nd, const double* slots, const StepParams* table, int64_t step, double4* UB,
+                       double4* VB, double4* AB, double4* L4, cudaStream_t s);
+void launch_sensor_seed(const double4* U4, int32_t num_sensors, const int32_t* sensors, double4* UB, double* loss,
+                        cudaStream_t s);
+
+// Layout conversion.
+void launch_pack4(const double* aos3, double4* out, int64_t n, cudaStream_t s);
+void launch_unpack4(const double4* in, double* aos3, int64_t n, cudaStream_t s);
+void launch_zero4(double4* out, int64_t n, cudaStream_t s);
+
+// Batched point kernels.
+void launch_stress_batch(int32_t mat, double lambda, double mu, int64_t n, const double* H, double* P,
+                         cudaStream_t s);
+void launch_quadrature_batch(int32_t kind, int32_t smoothed, int64_t n, const double* X, double* B, double* w,
+                             cudaStream_t s);
+
+}  // namespace am

@@ -1,0 +1,103 @@
+"""Seeded synthetic workloads (no public dataset is involved; these arrays are the
+whole workload). Sizes follow the five benchmark configurations:
+
+  hex8_le_cube      20^3 Hex8, linear elastic E=1e9, nu=0.3, rho=1000, bottom fixed,
+                    v0 ~ U[-0.01, 0.01], dt = 0.5 h_min / c, 100 steps
+  tet4_nh_shear     70^3 hexes -> 6 tets each (2,058,000 tets), neo-Hookean mu=3.85e8,
+                    kappa=8.33e8, rho=1000, interior jitter U[-0.2h, 0.2h]^3, bottom fixed,
+                    v0_x = z + U[-0.01, 0.01] noise, dt = 0.5 min(3V/A_max)/c, 1000 steps
+  hex8_nh_lognormal 64^3 (or 128^3) Hex8 neo-Hookean with lognormal per-element shear
+                    (and bulk) modulus fields, sigma 0.3, bottom fixed
+
+The density of the neo-Hookean workloads, the bottom support and the shear-profile
+direction are not fixed by the configuration text; the values here are the stated
+assumptions (rho = 1000, z = 0 face held, shear velocity along x growing with z).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import mesh
+from .model import BoundaryCondition, Material, Part
+
+
+@dataclass
+class Problem:
+    name: str
+    coords: np.ndarray
+    parts: list
+    bcs: list
+    v0: np.ndarray
+    dt: float
+    nsteps: int
+    seed: int
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def num_elems(self) -> int:
+        return sum(p.num_elems for p in self.parts)
+
+    @property
+    def num_nodes(self) -> int:
+        return int(self.coords.shape[0])
+
+
+def wave_speed(lam: float, mu: float, rho: float) -> float:
+    return math.sqrt((lam + 2.0 * mu) / rho)
+
+
+def _initial_velocity(coords, fixed, rng, amplitude=0.01, shear=0.0):
+    v = rng.uniform(-amplitude, amplitude, size=coords.shape)
+    v[:, 0] += shear * coords[:, 2]
+    v[fixed] = 0.0
+    return v
+
+
+def hex8_le_cube(n: int = 20, seed: int = 0, nsteps: int = 100) -> Problem:
+    rng = np.random.default_rng(seed)
+    coords, conn = mesh.box_hex(n, n, n)
+    mat = Material.create("linear_elastic", 1000.0, youngs_modulus=1e9, poissons_ratio=0.3)
+    fixed = mesh.side_sets(coords)["surface_5"]
+    v0 = _initial_velocity(coords, fixed, rng)
+    dt = 0.5 * (1.0 / n) / wave_speed(mat.lam, mat.mu, mat.density)
+    return Problem(f"hex8_le_cube_{n}", coords, [Part("hex8", mat, conn=conn)], [BoundaryCondition.fixed(fixed)],
+                   v0, dt, nsteps, seed, {"config": "Hex8 2x2x2 Gauss, linear elastic"})
+
+
+def tet4_nh_shear(n: int = 70, seed: int = 0, nsteps: int = 1000, jitter: float = 0.2) -> Problem:
+    rng = np.random.default_rng(seed)
+    coords, conn_hex = mesh.box_hex(n, n, n)
+    h = 1.0 / n
+    coords = mesh.jitter_interior(coords, jitter * h, rng)
+    conn = mesh.hex_to_tets(conn_hex)
+    mesh.check_orientation(coords, conn)
+    mat = Material.create("neo_hookean", 1000.0, shear_modulus=3.85e8, bulk_modulus=8.33e8)
+    fixed = mesh.side_sets(coords)["surface_5"]
+    v0 = _initial_velocity(coords, fixed, rng, shear=1.0)
+    c = wave_speed(mat.lam, mat.mu, mat.density)
+    dt = 0.5 * float(mesh.tet_char_length(coords, conn).min()) / c
+    return Problem(f"tet4_nh_shear_{n}", coords, [Part("tet4", mat, conn=conn)], [BoundaryCondition.fixed(fixed)],
+                   v0, dt, nsteps, seed, {"config": "Tet4 1-pt Gauss, neo-Hookean, 6-tet split, jittered"})
+
+
+def hex8_nh_lognormal(n: int = 64, seed: int = 0, nsteps: int = 200, sigma: float = 0.3,
+                      bulk_field: bool = False, num_sensors: int = 512) -> Problem:
+    rng = np.random.default_rng(seed)
+    coords, conn = mesh.box_hex(n, n, n)
+    E = conn.shape[0]
+    mu_e = 3.85e8 * np.exp(sigma * rng.standard_normal(E))
+    kappa_e = 8.33e8 * np.exp(sigma * rng.standard_normal(E)) if bulk_field else np.full(E, 8.33e8)
+    mat = Material.create("neo_hookean", 1000.0, shear_modulus=3.85e8, bulk_modulus=8.33e8)
+    fixed = mesh.side_sets(coords)["surface_5"]
+    v0 = _initial_velocity(coords, fixed, rng)
+    lam_e = kappa_e - 2.0 / 3.0 * mu_e
+    cmax = float(np.sqrt((lam_e + 2.0 * mu_e) / mat.density).max())
+    dt = 0.5 * (1.0 / n) / cmax
+    free = np.setdiff1d(np.arange(coords.shape[0]), fixed)
+    sensors = np.sort(rng.choice(free, size=min(num_sensors, free.size), replace=False)).astype(np.int32)
+    part = Part("hex8", mat, conn=conn, mu_field=mu_e, kappa_field=kappa_e)
+    return Problem(f"hex8_nh_lognormal_{n}", coords, [part], [BoundaryCondition.fixed(fixed)], v0, dt, nsteps, seed,
+                   {"sensors": sensors, "config": "Hex8 2x2x2 Gauss, neo-Hookean, lognormal fields"})

@@ -1,0 +1,377 @@
+"""Benchmark of the explicit-dynamics hot path on B200.
+
+Workload (one "step" = one central-difference step over the whole mesh): the
+neo-Hookean Tet4 shear workload, 70^3 hexes split into 2,058,000 tets (357,911
+nodes), interior jitter +-0.2h, 1000 steps at dt = 0.5 x the stable step.
+Synthetic seeded inputs (numpy PCG64, seed 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line. `value` is the mixed FP32-element / FP64-state path in
+Melem-steps/s (elements x steps / device seconds), with the plain FP64 path, the
+mixed-vs-FP64 errors, the adjoint/forward cost ratio (Hex8 neo-Hookean 64^3,
+200 steps, checkpoints every 20), the dominant kernel's roofline, an end-to-end
+figure through the public API with host buffers, and the CPU oracle timed on
+this host's cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Melem-steps/s, mixed vs FP64 at ≤1e-5 rel force err; adjoint/forward ratio"
+UNIT = "Melem-steps/s"
+WORKLOAD = "tet4_nh_shear_70"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=70, help="hexes per edge of the Tet4 workload")
+    ap.add_argument("--adjoint-n", type=int, default=64)
+    ap.add_argument("--skip-adjoint", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (one process per GPU; timing only, no data-path collective)
+# ---------------------------------------------------------------------------
+def dist_init(n_gpus):
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = str(index)
+        try:
+            import torch
+
+            uuid = str(torch.cuda.get_device_properties(index).uuid)
+            self.index = uuid if uuid.startswith("GPU-") else f"GPU-{uuid}"
+        except Exception:
+            pass
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world, local):
+    import torch
+
+    from aperi_mech_b200 import problems
+    from aperi_mech_b200.model import ExplicitDynamics
+
+    dev = torch.device("cuda", local)
+    prob = problems.tet4_nh_shear(n=args.n, seed=0, nsteps=args.steps)
+    E, N = prob.num_elems, prob.num_nodes
+    stream = torch.cuda.Stream(device=dev)
+    res = {}
+    kernel_ms = {}
+    launches = {}
+    model = ExplicitDynamics(prob.coords, prob.parts, prob.bcs, stream=stream.cuda_stream)
+    hbm_peak, peak_kind = measured_peaks()
+    clocks = None
+    for prec in ("fp64", "mixed"):
+        model.set_state(None, prob.v0)
+        model.init_acceleration(prec)
+        model.run(args.warmup, prob.dt, prec)
+        torch.cuda.synchronize(dev)
+        barrier(world)
+        model.profile(True)
+        n0 = model.launch_count()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        sampler = ClockSampler(local)
+        with sampler:
+            torch.cuda.synchronize(dev)
+            ev0.record(stream)
+            model.run(args.steps, prob.dt, prec, t0=args.warmup * prob.dt)
+            ev1.record(stream)
+            torch.cuda.synchronize(dev)
+        ms = ev0.elapsed_time(ev1)
+        launches[prec] = model.launch_count() - n0
+        kms, kn = model.profile_read()
+        model.profile(False)
+        kernel_ms[prec] = {"element": kms[0] / max(kn[0], 1), "node": kms[1] / max(kn[1], 1),
+                           "element_total": kms[0], "node_total": kms[1]}
+        ms = max_over_ranks(ms, world)
+        res[prec] = {"ms": ms, "value": world * E * args.steps / (ms * 1e-3) / 1e6}
+        if prec == "mixed":
+            clocks = sampler.summary()
+        res[prec]["state"] = model.get_state()
+    # accuracy of the mixed path against the FP64 path (itself 1e-12 from the oracle)
+    u64, um = res["fp64"]["state"][0], res["mixed"]["state"][0]
+    disp_err = float(np.linalg.norm(um - u64) / np.linalg.norm(u64))
+    f64 = model.internal_force(u64, "fp64")
+    f32 = model.internal_force(u64, "mixed")
+    force_err = float(np.linalg.norm(f32 - f64) / np.linalg.norm(f64))
+
+    # end to end through the public API: pinned host state in, K steps, host state out
+    e2e = None
+    if not args.skip_e2e:
+        u_h = torch.zeros((N, 3), dtype=torch.float64).pin_memory()
+        v_h = torch.from_numpy(prob.v0.copy()).pin_memory()
+        out_u = torch.empty((N, 3), dtype=torch.float64).pin_memory()
+        out_v = torch.empty((N, 3), dtype=torch.float64).pin_memory()
+        torch.cuda.synchronize(dev)
+        barrier(world)
+        t0 = time.perf_counter()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        model.set_state(u_h.numpy(), v_h.numpy())
+        model.init_acceleration("mixed")
+        model.run(args.steps, prob.dt, "mixed")
+        model.lib.am_get_state(model.ctx, 0, out_u.data_ptr(), out_v.data_ptr(), None)
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        wall = time.perf_counter() - t0
+        ms_e2e = max_over_ranks(max(ev0.elapsed_time(ev1), wall * 1e3), world)
+        e2e = {"value": world * E * args.steps / (ms_e2e * 1e-3) / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": 2 * N * 3 * 8 / args.steps, "d2h_bytes_per_step": 2 * N * 3 * 8 / args.steps,
+               "ms": ms_e2e, "path": "ExplicitDynamics.set_state/init_acceleration/run/get_state (C ABI, host buffers)"}
+    model.close()
+
+    # adjoint / forward cost (Hex8 neo-Hookean 64^3 with a lognormal shear field)
+    adj = None
+    if not args.skip_adjoint:
+        pa = problems.hex8_nh_lognormal(n=args.adjoint_n, seed=0, nsteps=200)
+        with ExplicitDynamics(pa.coords, pa.parts, pa.bcs, stream=stream.cuda_stream) as ma:
+            times = {}
+            for rep in range(2):
+                ma.set_state(None, pa.v0)
+                torch.cuda.synchronize(dev)
+                a0 = torch.cuda.Event(enable_timing=True)
+                a1 = torch.cuda.Event(enable_timing=True)
+                a0.record(stream)
+                ma.init_acceleration()
+                ma.run(pa.nsteps, pa.dt)
+                a1.record(stream)
+                torch.cuda.synchronize(dev)
+                times["forward"] = a0.elapsed_time(a1)
+                ma.set_state(None, pa.v0)
+                torch.cuda.synchronize(dev)
+                a0.record(stream)
+                loss, gm, gk = ma.adjoint(pa.nsteps, pa.dt, 20, pa.meta["sensors"])
+                a1.record(stream)
+                torch.cuda.synchronize(dev)
+                times["adjoint"] = a0.elapsed_time(a1)
+        adj = {"workload": f"hex8_nh_lognormal_{args.adjoint_n}", "steps": pa.nsteps, "ckpt_every": 20,
+               "forward_ms": times["forward"], "adjoint_ms": times["adjoint"],
+               "ratio": times["adjoint"] / times["forward"]}
+
+    # roofline of the dominant kernel of the headline (mixed) run
+    km = kernel_ms["mixed"]
+    dominant = "node" if km["node_total"] >= km["element_total"] else "element"
+    # Algorithmic bytes per launch (compulsory traffic, each array touched once):
+    #  element kernel (Tet4, mixed): conn 16 B + coordinates and displacement of the
+    #    element's share of nodes (N/E x 2 x 24 B) + its four FP32 force slots (48 B);
+    #  node kernel: its slots (S/N x (4 B index + 12 B FP32 force)) + mass 8 B +
+    #    BC word 4 B + displacement and half-step velocity read and written (4 x 24 B).
+    S = E * 4
+    alg = {"element": E * (16 + 48) + N * 48, "node": S * (4 + 12) + N * (8 + 4 + 96)}
+    ms_launch = km[dominant]
+    achieved = alg[dominant] / (ms_launch * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "peak_source": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_launch": alg[dominant], "ms_per_launch": ms_launch}
+    return prob, res, disp_err, force_err, e2e, adj, roofline, kernel_ms, launches, clocks
+
+
+def cpu_baseline(target_s=10.0, n=24):
+    """The oracle (C++ FP64 restatement, all host threads) on a bounded sample of the
+    same workload family: the neo-Hookean Tet4 shear mesh at n^3 x 6 tets."""
+    from aperi_mech_b200 import problems
+    from oracle import oracle
+
+    p = problems.tet4_nh_shear(n=n, seed=0, nsteps=1)
+    op = oracle.OracleProblem.from_problem(p)
+    u = np.zeros_like(p.coords)
+    a = op.init_acceleration(u)
+    t0 = time.perf_counter()
+    u1, v1, a1 = op.steps(u, p.v0, a, np.full(2, p.dt))
+    t1 = (time.perf_counter() - t0) / 2
+    steps = max(2, int(target_s / max(t1, 1e-6)))
+    t0 = time.perf_counter()
+    op.steps(u, p.v0, a, np.full(steps, p.dt))
+    dt = time.perf_counter() - t0
+    return {"value": p.num_elems * steps / dt / 1e6, "unit": UNIT, "cores": oracle.get_threads(), "kind": "port",
+            "sample": f"tet4_nh_shear_{n} ({p.num_elems} tets), {steps} central-difference steps, FP64, "
+                      f"{oracle.get_threads()} OpenMP threads"}
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the reference's CPU implementation cannot be built here (Kokkos,
+    Trilinos/STK, Eigen, yaml-cpp, MPI absent), so its CPU restatement (oracle) runs on
+    the host cores; each step is one central-difference step of a bounded sample mesh."""
+    if rank != 0:
+        return
+    from aperi_mech_b200 import problems
+    from oracle import oracle
+
+    n = 24
+    p = problems.tet4_nh_shear(n=n, seed=0, nsteps=1)
+    op = oracle.OracleProblem.from_problem(p)
+    u = np.zeros_like(p.coords)
+    a = op.init_acceleration(u)
+    u, v, a = op.steps(u, p.v0, a, np.full(args.warmup, p.dt))
+    t0 = time.perf_counter()
+    op.steps(u, v, a, np.full(args.steps, p.dt), t0=args.warmup * p.dt)
+    dt = time.perf_counter() - t0
+    value = p.num_elems * args.steps / dt / 1e6
+    sample = (f"tet4_nh_shear_{n} ({p.num_elems} tets) per step, FP64 oracle restatement (reference CPU build "
+              f"unavailable: missing Kokkos/Trilinos/Eigen/MPI)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample_workload": f"tet4_nh_shear_{n}"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": oracle.get_threads(), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_init(args.gpus)
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    prob, res, disp_err, force_err, e2e, adj, roofline, kernel_ms, launches, clocks = run_ours(args, rank, world, local)
+    if rank != 0:
+        return
+    cpu = None if args.skip_cpu else cpu_baseline()
+    ms_step = res["mixed"]["ms"] / args.steps
+    line = {
+        "metric": METRIC, "value": res["mixed"]["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "elements": prob.num_elems, "nodes": prob.num_nodes,
+                   "element": "Tet4 1-pt Gauss", "material": "neo-Hookean mu=3.85e8 kappa=8.33e8",
+                   "dt": prob.dt, "seed": prob.seed,
+                   "l2_flush": "inputs larger than L2 (state + slots + connectivity ~ 230 MB per step)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "fp64": {"value": res["fp64"]["value"], "ms_per_step": res["fp64"]["ms"] / args.steps},
+        "mixed_vs_fp64": {"rel_disp_err_l2": disp_err, "rel_force_err_l2": force_err,
+                          "speedup": res["mixed"]["value"] / res["fp64"]["value"]},
+        "adjoint": adj,
+        "roofline": roofline,
+        "kernels_ms_per_launch": kernel_ms,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": launches["mixed"],
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

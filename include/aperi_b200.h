@@ -1,0 +1,179 @@
+/*
+ * aperi_b200.h -- C ABI of the B200-native explicit-dynamics hot path.
+ *
+ * The library replaces, for one GPU, the per-step path of aperi-mech's
+ * explicit solver: the internal-force contributions of the parts
+ * (InternalForceContribution -> ElementBase::ComputeInternalForceAllElements),
+ * their material stress update (Material::StressFunctor::GetStress) and the
+ * central-difference nodal update (ExplicitTimeIntegrator), in the step order of
+ * ExplicitSolver::Solve. Reference interfaces are cited as file:line of the
+ * aperi-mech source tree.
+ *
+ * Conventions
+ *  - Every call returns an am_status code; no C++ exception crosses the ABI.
+ *    am_last_error() gives the message of the last failing call on a context.
+ *  - Nodal vectors are row-major N x 3 FP64 arrays (the layout of an aperi
+ *    3-component node field, Field.h:129-136). Tensors are row-major 3 x 3.
+ *  - Pointers are host or device pointers as selected by the am_memory
+ *    argument. Host arrays passed to am_add_block / am_set_boundary_conditions /
+ *    am_create are copied; the caller keeps ownership.
+ *  - One context owns its device buffers and one CUDA stream (or the stream
+ *    given to am_set_stream). Calls are stream-ordered; the host blocks only
+ *    in am_get_* with AM_HOST, in am_run/am_solve/am_adjoint when the device
+ *    status word must be read, and on errors. A context is not thread-safe.
+ *  - Forces are assembled by a deterministic node-centric gather (no atomics):
+ *    results are bitwise reproducible run to run.
+ */
+#ifndef APERI_B200_H
+#define APERI_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AM_MAX_BCS 10
+
+typedef enum {
+    AM_OK = 0,
+    AM_EINVAL = 1,      /* invalid argument (std::runtime_error in the reference) */
+    AM_ENOMEM = 2,      /* device allocation failed */
+    AM_ECUDA = 3,       /* CUDA runtime error */
+    AM_ENONPOS_J = 4,   /* an element / cell reached det F <= 0 or det J <= 0 */
+    AM_ENAN = 5,        /* a non-finite nodal acceleration was produced */
+    AM_ESTATE = 6,      /* call out of order (e.g. before am_finalize) */
+    AM_ERANGE = 7       /* size beyond a compiled limit */
+} am_status;
+
+typedef enum { AM_FP64 = 0, AM_MIXED = 1 } am_precision;
+typedef enum { AM_HOST = 0, AM_DEVICE = 1 } am_memory;
+
+/* Element kinds: ElementTetrahedron4 (1-pt Gauss), ElementHexahedron8 (2x2x2
+ * Gauss), and strain-smoothed / RKPM cells (ElementSmoothedTetrahedron4,
+ * ElementReproducingKernel; include/Element.h:32-86). */
+typedef enum { AM_TET4_GAUSS = 0, AM_HEX8_GAUSS = 1, AM_SMOOTHED_CELLS = 2 } am_block_kind;
+
+/* Materials/Base.h MaterialType: LINEAR_ELASTIC, NEO_HOOKEAN, ELASTIC (SVK). */
+typedef enum { AM_LINEAR_ELASTIC = 0, AM_NEO_HOOKEAN = 1, AM_ELASTIC_SVK = 2 } am_material_kind;
+
+typedef enum { AM_BC_DISPLACEMENT = 0, AM_BC_VELOCITY = 1 } am_bc_kind;
+typedef enum { AM_TF_RAMP = 0, AM_TF_SMOOTH_STEP = 1 } am_time_function;
+
+/* One part: replaces InternalForceContribution (include/InternalForceContribution.h:26-159)
+ * with its Material (include/Materials/Factory.h:43). lambda/mu are the completed
+ * Lame parameters (LinearElasticProperties::CompleteProperties, Materials/Base.h:47-129).
+ * mu_field / kappa_field (per element or cell, optional) replace them element-wise
+ * with lambda_e = kappa_e - 2/3 mu_e. */
+typedef struct {
+    int32_t kind;               /* am_block_kind */
+    int32_t material;           /* am_material_kind */
+    double lambda, mu, density;
+    const double* mu_field;     /* host, num_elems, or NULL */
+    const double* kappa_field;  /* host, num_elems, or NULL */
+    int64_t num_elems;          /* elements, or cells for AM_SMOOTHED_CELLS */
+    const int32_t* conn;        /* Gauss: num_elems x (4|8), reference node order */
+    const int64_t* cell_ptr;    /* cells: num_elems+1 offsets into the entry arrays */
+    const int32_t* cell_nodes;  /* cells: node of each entry (SmoothedCellData node CSR) */
+    const double* cell_grads;   /* cells: entry x 3 smoothed gradients (function derivatives) */
+    const double* cell_volumes; /* cells: num_elems subcell volumes */
+} am_block_desc;
+
+/* Displacement / velocity boundary condition (src/BoundaryCondition.cpp:14-222).
+ * values = magnitude x normalized direction, or the component values. Later
+ * entries win where node sets overlap, as in the reference's in-order apply. */
+typedef struct {
+    int64_t num_nodes;
+    const int32_t* nodes;       /* host */
+    int32_t component_mask;     /* bit c: component c prescribed */
+    int32_t kind;               /* am_bc_kind */
+    int32_t time_function;      /* am_time_function */
+    int32_t num_points;
+    double values[3];
+    const double* abscissa;     /* host, num_points */
+    const double* ordinate;     /* host, num_points */
+    double active_start, active_end;
+} am_bc_desc;
+
+typedef struct am_ctx am_ctx;
+
+/* ---- context set-up (replaces Application::CreateSolver / Preprocessor) ---- */
+int am_create(int64_t num_nodes, const double* coords, am_ctx** out);
+void am_destroy(am_ctx* ctx);
+int am_set_stream(am_ctx* ctx, void* cuda_stream);
+int am_add_block(am_ctx* ctx, const am_block_desc* desc, int32_t* block_id);
+int am_set_boundary_conditions(am_ctx* ctx, int32_t num_bcs, const am_bc_desc* bcs);
+/* Replace the per-element shear / bulk modulus fields of a block (host arrays of
+ * num_elems; NULL leaves that field unchanged). Allowed after am_finalize. */
+int am_set_block_fields(am_ctx* ctx, int32_t block_id, const double* mu_field, const double* kappa_field);
+int am_set_body_acceleration(am_ctx* ctx, const double g[3]);
+int am_set_mass(am_ctx* ctx, const double* mass);
+int am_finalize(am_ctx* ctx);
+
+/* ---- state (the *_coefficients node fields, states N and NP1 folded) ---- */
+int am_set_state(am_ctx* ctx, am_memory where, const double* u, const double* v, const double* a);
+int am_get_state(am_ctx* ctx, am_memory where, double* u, double* v, double* a);
+int am_get_mass(am_ctx* ctx, double* mass_host);
+
+/* ---- the hot path ---- */
+/* Internal force f = F(u) over all parts: replaces ComputeInternalForceGaussian::operator()
+ * (include/ComputeInternalForceGaussian.h:57-131) and
+ * ComputeInternalForceSmoothedCellBase::ForEachCellComputeForce
+ * (include/ComputeInternalForceSmoothedCell.h:416-442). accumulate=0 overwrites f,
+ * accumulate=1 adds to it (the reference accumulates into a zeroed field). */
+int am_internal_force(am_ctx* ctx, am_precision prec, am_memory where, const double* u, double* f, int accumulate);
+/* Pre-loop force + acceleration of ExplicitSolver::Solve (src/Solvers/Explicit.cpp:357-368). */
+int am_init_acceleration(am_ctx* ctx, am_precision prec);
+/* nsteps central-difference steps at fixed dt from time t0 (loop body of
+ * src/Solvers/Explicit.cpp:383-483 with ExplicitTimeIntegrator.h:97-364). */
+int am_run(am_ctx* ctx, am_precision prec, int64_t nsteps, double dt, double t0);
+/* The same with a per-step time increment. */
+int am_run_schedule(am_ctx* ctx, am_precision prec, int64_t nsteps, const double* dts, double t0);
+/* ExplicitSolver::Solve with a DirectTimeStepper (include/TimeStepper.h:97-128):
+ * initial acceleration, then steps until time >= t_end. */
+int am_solve(am_ctx* ctx, am_precision prec, double dt, double t_end, int64_t max_steps, int64_t* steps_done);
+
+/* ---- adjoint (no counterpart in the reference) ---- */
+/* gu = (dF/du)^T lam ; gmu/gkappa (per element, all parts concatenated, may be NULL)
+ * = (dF/dmu_e)^T lam, (dF/dkappa_e)^T lam. FP64. */
+int am_vjp_force(am_ctx* ctx, am_memory where, const double* u, const double* lam, double* gu, double* gmu,
+                 double* gkappa);
+/* Loss L = sum_s |u_s(nsteps)|^2 over the sensor nodes after nsteps steps from the
+ * current state, and its gradient with respect to the per-element shear and bulk
+ * moduli, by a reverse pass with checkpoints every ckpt_every steps. FP64. The
+ * state is left at the end of the forward trajectory. Host outputs. */
+int am_adjoint(am_ctx* ctx, int64_t nsteps, double dt, int32_t ckpt_every, int32_t num_sensors,
+               const int32_t* sensors, double* loss, double* gmu, double* gkappa);
+
+/* ---- batched point kernels (for the reference's unit-level known answers) ---- */
+/* Material::StressFunctor::GetStress (Materials/Base.h:205-213) on n displacement gradients. */
+int am_stress(int32_t material, double lambda, double mu, int64_t n, am_memory where, const double* H, double* P);
+/* Quadrature::ComputeBMatrixAndWeight (QuadratureGaussian.h:17-39) for each element
+ * and Gauss point of kind (Tet4: 1 point, Hex8: 8 points), or the smoothed
+ * quadrature (QuadratureSmoothed.h:32-142) when smoothed != 0.
+ * X: n x nodes x 3; B: n x points x nodes x 3; w: n x points. */
+int am_quadrature(int32_t kind, int32_t smoothed, int64_t n, am_memory where, const double* X, double* B,
+                  double* w);
+
+/* LinearElasticProperties::CompleteProperties (Materials/Base.h:47-158): props =
+ * {youngs_modulus, poissons_ratio, shear_modulus, lambda, bulk_modulus} with NaN for
+ * the undefined ones; exactly two must be defined. Fills the rest, checks the physical
+ * bounds; on failure returns AM_EINVAL and writes the reason to msg. Host only. */
+int am_complete_properties(double props[5], char* msg, int msg_len);
+
+/* ---- diagnostics ---- */
+const char* am_last_error(const am_ctx* ctx);
+const char* am_status_string(int status);
+/* Kernel launches issued by this context so far (all kinds). */
+int64_t am_launch_count(const am_ctx* ctx);
+/* Per-kernel device timing: when enabled, every launch of the hot loop is
+ * bracketed by CUDA events on the context stream. Slot 0: element/cell force
+ * kernels, slot 1: node gather + update kernels, slot 2: adjoint kernels.
+ * am_profile_read returns accumulated milliseconds and launch counts. */
+int am_profile_enable(am_ctx* ctx, int enable);
+int am_profile_read(am_ctx* ctx, double ms[3], int64_t launches[3]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

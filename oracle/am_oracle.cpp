@@ -1,0 +1,976 @@
+// am_oracle.cpp -- CPU FP64 restatement of aperi-mech's explicit-dynamics hot path.
+//
+// TEST INFRASTRUCTURE ONLY (parity checker and timed CPU baseline). Nothing in
+// the product links or calls this file. Every routine names the reference
+// function it restates; the reference paths are relative to the aperi-mech
+// source tree.
+#include "am_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// 3x3 helpers, row-major a[i*3+j]
+// ---------------------------------------------------------------------------
+inline double det3(const double* m) {
+    return m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
+           m[2] * (m[3] * m[7] - m[4] * m[6]);
+}
+
+// Adjugate inverse (the closed form Eigen uses for fixed 3x3 inverse()).
+inline double inv3(const double* m, double* r) {
+    const double c00 = m[4] * m[8] - m[5] * m[7];
+    const double c01 = m[5] * m[6] - m[3] * m[8];
+    const double c02 = m[3] * m[7] - m[4] * m[6];
+    const double det = m[0] * c00 + m[1] * c01 + m[2] * c02;
+    const double id = 1.0 / det;
+    r[0] = c00 * id;
+    r[1] = (m[2] * m[7] - m[1] * m[8]) * id;
+    r[2] = (m[1] * m[5] - m[2] * m[4]) * id;
+    r[3] = c01 * id;
+    r[4] = (m[0] * m[8] - m[2] * m[6]) * id;
+    r[5] = (m[2] * m[3] - m[0] * m[5]) * id;
+    r[6] = c02 * id;
+    r[7] = (m[1] * m[6] - m[0] * m[7]) * id;
+    r[8] = (m[0] * m[4] - m[1] * m[3]) * id;
+    return det;
+}
+
+inline void matmul3(const double* a, const double* b, double* c) {  // c = a b
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) c[i * 3 + j] = a[i * 3 + 0] * b[0 + j] + a[i * 3 + 1] * b[3 + j] + a[i * 3 + 2] * b[6 + j];
+}
+inline void matmul3_tN(const double* a, const double* b, double* c) {  // c = a^T b
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) c[i * 3 + j] = a[0 + i] * b[0 + j] + a[3 + i] * b[3 + j] + a[6 + i] * b[6 + j];
+}
+inline void matmul3_Nt(const double* a, const double* b, double* c) {  // c = a b^T
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) c[i * 3 + j] = a[i * 3 + 0] * b[j * 3 + 0] + a[i * 3 + 1] * b[j * 3 + 1] + a[i * 3 + 2] * b[j * 3 + 2];
+}
+
+// MathUtils.h:332-339 DetApIm1: det(I + A) - 1 from the principal invariants.
+inline double det_ap_im1(const double* A) {
+    const double a00 = A[0], a01 = A[1], a02 = A[2], a10 = A[3], a11 = A[4], a12 = A[5], a20 = A[6], a21 = A[7], a22 = A[8];
+    return a00 + a11 + a22 - a01 * a10 * (1 + a22) + a00 * a11 * (1 + a22) - a02 * a20 * (1 + a11) -
+           a12 * a21 * (1 + a00) + a00 * a22 + a11 * a22 + a01 * a12 * a20 + a02 * a10 * a21;
+}
+
+// ---------------------------------------------------------------------------
+// Shape functions and Gauss quadrature
+// ---------------------------------------------------------------------------
+// ShapeFunctionsFunctorHex8.h:51-62 (node order :17-33).
+void hex8_dN(const double xi[3], double* dN) {
+    const double x = xi[0], y = xi[1], z = xi[2];
+    const double t[24] = {
+        -0.125 * (1.0 - y) * (1.0 - z), -0.125 * (1.0 - x) * (1.0 - z), -0.125 * (1.0 - x) * (1.0 - y),
+        0.125 * (1.0 - y) * (1.0 - z),  -0.125 * (1.0 + x) * (1.0 - z), -0.125 * (1.0 + x) * (1.0 - y),
+        0.125 * (1.0 + y) * (1.0 - z),  0.125 * (1.0 + x) * (1.0 - z),  -0.125 * (1.0 + x) * (1.0 + y),
+        -0.125 * (1.0 + y) * (1.0 - z), 0.125 * (1.0 - x) * (1.0 - z),  -0.125 * (1.0 - x) * (1.0 + y),
+        -0.125 * (1.0 - y) * (1.0 + z), -0.125 * (1.0 - x) * (1.0 + z), 0.125 * (1.0 - x) * (1.0 - y),
+        0.125 * (1.0 - y) * (1.0 + z),  -0.125 * (1.0 + x) * (1.0 + z), 0.125 * (1.0 + x) * (1.0 - y),
+        0.125 * (1.0 + y) * (1.0 + z),  0.125 * (1.0 + x) * (1.0 + z),  0.125 * (1.0 + x) * (1.0 + y),
+        -0.125 * (1.0 + y) * (1.0 + z), 0.125 * (1.0 - x) * (1.0 + z),  0.125 * (1.0 - x) * (1.0 + y)};
+    std::memcpy(dN, t, sizeof(t));
+}
+
+// ElementHexahedron8.h:105-117: 2x2x2 points at +-1/sqrt(3), weights 1, in node order.
+void hex8_gauss_point(int gp, double xi[3]) {
+    static const int s[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                                {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+    const double loc = 1.0 / std::sqrt(3.0);
+    for (int j = 0; j < 3; ++j) xi[j] = s[gp][j] * loc;
+}
+
+// ShapeFunctionsFunctorTet4.h:27-34.
+const double kTet4dN[12] = {-1.0, -1.0, -1.0, 1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0};
+
+// QuadratureGaussian.h:17-39 ComputeBMatrixAndWeight: J = X^T dN, B = dN J^-1, w = w_g det J.
+template <int NN>
+double gauss_bw(const double* X, const double* dN, double wg, double* B) {
+    double J[9];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double s = 0.0;
+            for (int a = 0; a < NN; ++a) s += X[a * 3 + i] * dN[a * 3 + j];
+            J[i * 3 + j] = s;
+        }
+    double Ji[9];
+    const double detJ = inv3(J, Ji);
+    for (int a = 0; a < NN; ++a)
+        for (int j = 0; j < 3; ++j)
+            B[a * 3 + j] = dN[a * 3 + 0] * Ji[0 * 3 + j] + dN[a * 3 + 1] * Ji[1 * 3 + j] + dN[a * 3 + 2] * Ji[2 * 3 + j];
+    return wg * detJ;
+}
+
+// ---------------------------------------------------------------------------
+// Materials
+// ---------------------------------------------------------------------------
+// LinearElastic.h:79-87: eps = sym(H); P = lambda tr(eps) I + 2 mu eps.
+// NeoHooke.h:79-91: tau = lambda log1p(J-1) I + mu (B - I); P = tau F^-T.
+// Elastic.h:70-78 (St-Venant-Kirchhoff): E = 1/2(H + H^T + H^T H); S = 2 mu E + lambda trE I; P = (I+H) S.
+void stress(int material, double lambda, double mu, const double* H, double* P) {
+    if (material == OB_LINEAR_ELASTIC) {
+        const double tr = H[0] + H[4] + H[8];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                const double eps = 0.5 * (H[i * 3 + j] + H[j * 3 + i]);
+                P[i * 3 + j] = (i == j ? lambda * tr : 0.0) + 2.0 * mu * eps;
+            }
+    } else if (material == OB_NEO_HOOKEAN) {
+        double HHt[9];
+        matmul3_Nt(H, H, HHt);
+        double BmI[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) BmI[i * 3 + j] = HHt[i * 3 + j] + H[j * 3 + i] + H[i * 3 + j];
+        const double Jm1 = det_ap_im1(H);
+        const double lnJ = std::log1p(Jm1);
+        double tau[9];
+        for (int k = 0; k < 9; ++k) tau[k] = mu * BmI[k];
+        for (int i = 0; i < 3; ++i) tau[i * 4] += lambda * lnJ;
+        double F[9], Fi[9];
+        for (int k = 0; k < 9; ++k) F[k] = H[k];
+        F[0] += 1.0; F[4] += 1.0; F[8] += 1.0;
+        inv3(F, Fi);
+        // P = tau * Fi^T
+        matmul3_Nt(tau, Fi, P);
+    } else {
+        double HtH[9];
+        matmul3_tN(H, H, HtH);
+        double E[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) E[i * 3 + j] = 0.5 * (H[i * 3 + j] + H[j * 3 + i] + HtH[i * 3 + j]);
+        const double trE = E[0] + E[4] + E[8];
+        double S[9];
+        for (int k = 0; k < 9; ++k) S[k] = 2.0 * mu * E[k];
+        for (int i = 0; i < 3; ++i) S[i * 4] += lambda * trE;
+        double F[9];
+        for (int k = 0; k < 9; ++k) F[k] = H[k];
+        F[0] += 1.0; F[4] += 1.0; F[8] += 1.0;
+        matmul3(F, S, P);
+    }
+}
+
+// Directional derivative dP[L] of the stress at H (equal to the VJP because all
+// three models are hyperelastic, so dP/dH is major-symmetric), plus the partial
+// derivatives of P with respect to lambda and mu (at fixed H).
+void stress_tangent(int material, double lambda, double mu, const double* H, const double* L,
+                    double* dP, double* dPdlam, double* dPdmu) {
+    double F[9];
+    for (int k = 0; k < 9; ++k) F[k] = H[k];
+    F[0] += 1.0; F[4] += 1.0; F[8] += 1.0;
+    if (material == OB_LINEAR_ELASTIC) {
+        const double trL = L[0] + L[4] + L[8];
+        const double trH = H[0] + H[4] + H[8];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                const int k = i * 3 + j;
+                dP[k] = (i == j ? lambda * trL : 0.0) + mu * (L[k] + L[j * 3 + i]);
+                dPdlam[k] = (i == j ? trH : 0.0);
+                dPdmu[k] = H[k] + H[j * 3 + i];
+            }
+    } else if (material == OB_NEO_HOOKEAN) {
+        double Fi[9];
+        inv3(F, Fi);
+        const double lnJ = std::log1p(det_ap_im1(H));
+        double FiL[9];
+        matmul3(Fi, L, FiL);
+        const double trFiL = FiL[0] + FiL[4] + FiL[8];
+        double LFt[9], FLt[9];
+        matmul3_Nt(L, F, LFt);
+        matmul3_Nt(F, L, FLt);
+        double dtau[9];
+        for (int k = 0; k < 9; ++k) dtau[k] = mu * (LFt[k] + FLt[k]);
+        for (int i = 0; i < 3; ++i) dtau[i * 4] += lambda * trFiL;
+        double FiT[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) FiT[i * 3 + j] = Fi[j * 3 + i];
+        double P[9];
+        stress(material, lambda, mu, H, P);
+        double t1[9], PLt[9], t2[9];
+        matmul3(dtau, FiT, t1);
+        matmul3_Nt(P, L, PLt);
+        matmul3(PLt, FiT, t2);
+        for (int k = 0; k < 9; ++k) dP[k] = t1[k] - t2[k];
+        for (int k = 0; k < 9; ++k) {
+            dPdlam[k] = lnJ * FiT[k];
+            dPdmu[k] = F[k] - FiT[k];
+        }
+    } else {
+        double E[9], FtF[9];
+        matmul3_tN(F, F, FtF);
+        for (int k = 0; k < 9; ++k) E[k] = 0.5 * FtF[k];
+        E[0] -= 0.5; E[4] -= 0.5; E[8] -= 0.5;
+        const double trE = E[0] + E[4] + E[8];
+        double S[9];
+        for (int k = 0; k < 9; ++k) S[k] = 2.0 * mu * E[k];
+        for (int i = 0; i < 3; ++i) S[i * 4] += lambda * trE;
+        double LtF[9], FtL[9];
+        matmul3_tN(L, F, LtF);
+        matmul3_tN(F, L, FtL);
+        double dE[9];
+        for (int k = 0; k < 9; ++k) dE[k] = 0.5 * (LtF[k] + FtL[k]);
+        const double trdE = dE[0] + dE[4] + dE[8];
+        double dS[9];
+        for (int k = 0; k < 9; ++k) dS[k] = 2.0 * mu * dE[k];
+        for (int i = 0; i < 3; ++i) dS[i * 4] += lambda * trdE;
+        double a[9], b[9], FE[9];
+        matmul3(L, S, a);
+        matmul3(F, dS, b);
+        matmul3(F, E, FE);
+        for (int k = 0; k < 9; ++k) {
+            dP[k] = a[k] + b[k];
+            dPdlam[k] = trE * F[k];
+            dPdmu[k] = 2.0 * FE[k];
+        }
+    }
+}
+
+inline void block_lame(const ob_block& b, int64_t e, double* lambda, double* mu) {
+    if (b.mu_field != nullptr || b.kappa_field != nullptr) {
+        const double mu0 = b.mu;
+        const double kappa0 = b.lambda + 2.0 * b.mu / 3.0;
+        const double m = b.mu_field ? b.mu_field[e] : mu0;
+        const double k = b.kappa_field ? b.kappa_field[e] : kappa0;
+        *mu = m;
+        *lambda = k - 2.0 * m / 3.0;
+    } else {
+        *lambda = b.lambda;
+        *mu = b.mu;
+    }
+}
+
+int nodes_per_elem(int kind) { return kind == OB_HEX8_GAUSS ? 8 : 4; }
+
+// Per element: the force contributions of its nodes (ComputeInternalForceGaussian.h:57-131;
+// force.row(i) -= B.row(i) * P^T * w, accumulated over the Gauss points in order).
+void gauss_element_force(const ob_block& b, int64_t e, const double* coords, const double* u, double* fe) {
+    const int nn = nodes_per_elem(b.kind);
+    double X[24], U[24];
+    for (int a = 0; a < nn; ++a) {
+        const int32_t n = b.conn[e * nn + a];
+        for (int i = 0; i < 3; ++i) {
+            X[a * 3 + i] = coords[n * 3 + i];
+            U[a * 3 + i] = u[n * 3 + i];
+        }
+    }
+    double lambda, mu;
+    block_lame(b, e, &lambda, &mu);
+    for (int k = 0; k < nn * 3; ++k) fe[k] = 0.0;
+    const int ngp = (b.kind == OB_HEX8_GAUSS) ? 8 : 1;
+    for (int gp = 0; gp < ngp; ++gp) {
+        double B[24], w;
+        if (b.kind == OB_HEX8_GAUSS) {
+            double xi[3], dN[24];
+            hex8_gauss_point(gp, xi);
+            hex8_dN(xi, dN);
+            w = gauss_bw<8>(X, dN, 1.0, B);
+        } else {
+            w = gauss_bw<4>(X, kTet4dN, 1.0 / 6.0, B);
+        }
+        // ComputeInternalForceBase.h:158-174 (Total Lagrangian): H = u^T B.
+        double H[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                double s = 0.0;
+                for (int a = 0; a < nn; ++a) s += U[a * 3 + i] * B[a * 3 + j];
+                H[i * 3 + j] = s;
+            }
+        double P[9];
+        stress(b.material, lambda, mu, H, P);
+        for (int a = 0; a < nn; ++a)
+            for (int i = 0; i < 3; ++i) {
+                const double t = B[a * 3 + 0] * P[i * 3 + 0] + B[a * 3 + 1] * P[i * 3 + 1] + B[a * 3 + 2] * P[i * 3 + 2];
+                fe[a * 3 + i] -= t * w;
+            }
+    }
+}
+
+// ComputeInternalForceSmoothedCell.h:86-117 (H gather), :186-224 (stress), :312-351 (force):
+// H = sum_k u_k (x) b_k ; f_k += b_k (-V P^T).
+void cell_force(const ob_block& b, int64_t c, const double* u, double* fk) {
+    const int64_t s0 = b.cell_ptr[c], s1 = b.cell_ptr[c + 1];
+    double H[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int64_t s = s0; s < s1; ++s) {
+        const int32_t n = b.cell_nodes[s];
+        const double* g = b.cell_grads + 3 * s;
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) H[i * 3 + j] += u[n * 3 + i] * g[j];
+    }
+    double lambda, mu;
+    block_lame(b, c, &lambda, &mu);
+    double P[9];
+    stress(b.material, lambda, mu, H, P);
+    const double V = b.cell_volumes[c];
+    double st[9];  // stress_term = P^T * -V
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) st[i * 3 + j] = P[j * 3 + i] * -V;
+    for (int64_t s = s0; s < s1; ++s) {
+        const double* g = b.cell_grads + 3 * s;
+        for (int i = 0; i < 3; ++i) fk[(s - s0) * 3 + i] = g[0] * st[0 * 3 + i] + g[1] * st[1 * 3 + i] + g[2] * st[2 * 3 + i];
+    }
+}
+
+void add_block_forces(const ob_problem* p, const ob_block& b, const double* u, double* f) {
+    if (b.kind == OB_CELLS) {
+        const int64_t K = b.cell_ptr[b.num_elems];
+        std::vector<double> slots(static_cast<size_t>(K) * 3);
+#pragma omp parallel for schedule(static)
+        for (int64_t c = 0; c < b.num_elems; ++c) cell_force(b, c, u, slots.data() + 3 * b.cell_ptr[c]);
+        // Scatter in entry order (Field::AtomicAdd in the reference; deterministic here).
+        for (int64_t s = 0; s < K; ++s) {
+            const int32_t n = b.cell_nodes[s];
+            for (int i = 0; i < 3; ++i) f[n * 3 + i] += slots[s * 3 + i];
+        }
+        return;
+    }
+    const int nn = nodes_per_elem(b.kind);
+    std::vector<double> slots(static_cast<size_t>(b.num_elems) * nn * 3);
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < b.num_elems; ++e) gauss_element_force(b, e, p->coords, u, slots.data() + e * nn * 3);
+    for (int64_t e = 0; e < b.num_elems; ++e)
+        for (int a = 0; a < nn; ++a) {
+            const int32_t n = b.conn[e * nn + a];
+            for (int i = 0; i < 3; ++i) f[n * 3 + i] += slots[(e * nn + a) * 3 + i];
+        }
+}
+
+// ---------------------------------------------------------------------------
+// Boundary-condition time functions (MathUtils.h, BoundaryCondition.cpp:86-195)
+// ---------------------------------------------------------------------------
+double constant_interp(double x, const double* ab, const double* ord, int n) {
+    if (n == 1) return ord[0];
+    if (x < ab[0]) return 0.0;
+    if (x > ab[n - 1]) return ord[n - 1];
+    for (int i = 0; i < n - 1; ++i)
+        if (x >= ab[i] && x <= ab[i + 1]) return ord[i];
+    return 0.0;
+}
+double linear_interp(double x, const double* ab, const double* ord, int n) {
+    if (n == 1) return ord[0];
+    if (x < ab[0]) return ord[0];
+    if (x > ab[n - 1]) return ord[n - 1];
+    for (int i = 0; i < n - 1; ++i)
+        if (x >= ab[i] && x <= ab[i + 1]) {
+            const double slope = (ord[i + 1] - ord[i]) / (ab[i + 1] - ab[i]);
+            return ord[i] + slope * (x - ab[i]);
+        }
+    return 0.0;
+}
+double smooth_step_d1(double x, const double* ab, const double* ord, int n) {
+    if (n == 1 || x < ab[0] || x > ab[n - 1]) return 0.0;
+    for (int i = 0; i < n - 1; ++i)
+        if (x >= ab[i] && x <= ab[i + 1]) {
+            const double t = (x - ab[i]) / (ab[i + 1] - ab[i]);
+            return (ord[i + 1] - ord[i]) * (30.0 * t * t - 60.0 * t * t * t + 30.0 * t * t * t * t) / (ab[i + 1] - ab[i]);
+        }
+    return 0.0;
+}
+double smooth_step_d2(double x, const double* ab, const double* ord, int n) {
+    if (n == 1 || x < ab[0] || x > ab[n - 1]) return 0.0;
+    for (int i = 0; i < n - 1; ++i)
+        if (x >= ab[i] && x <= ab[i + 1]) {
+            const double t = (x - ab[i]) / (ab[i + 1] - ab[i]);
+            return (ord[i + 1] - ord[i]) * (60.0 * t - 180.0 * t * t + 120.0 * t * t * t) / ((ab[i + 1] - ab[i]) * (ab[i + 1] - ab[i]));
+        }
+    return 0.0;
+}
+
+// velocity (which=0) or acceleration (which=1) scale of a BC at time t.
+double bc_scale(const ob_bc& bc, int which, double t) {
+    const int n = bc.num_points;
+    if (bc.time_function == OB_TF_RAMP) {
+        std::vector<double> d(n);
+        for (int i = 0; i < n - 1; ++i) d[i] = (bc.ordinate[i + 1] - bc.ordinate[i]) / (bc.abscissa[i + 1] - bc.abscissa[i]);
+        d[n - 1] = 0.0;
+        if (bc.kind == OB_BC_DISPLACEMENT) return which == 0 ? constant_interp(t, bc.abscissa, d.data(), n) : 0.0;
+        return which == 0 ? linear_interp(t, bc.abscissa, bc.ordinate, n) : constant_interp(t, bc.abscissa, d.data(), n);
+    }
+    if (bc.kind == OB_BC_DISPLACEMENT)
+        return which == 0 ? smooth_step_d1(t, bc.abscissa, bc.ordinate, n) : smooth_step_d2(t, bc.abscissa, bc.ordinate, n);
+    // velocity smooth step: v = SmoothStep, a = SmoothStep'
+    if (which == 0) {
+        // SmoothStepInterpolation (MathUtils.h:187-208)
+        if (n == 1 || t < bc.abscissa[0]) return bc.ordinate[0];
+        if (t > bc.abscissa[n - 1]) return bc.ordinate[n - 1];
+        for (int i = 0; i < n - 1; ++i)
+            if (t >= bc.abscissa[i] && t <= bc.abscissa[i + 1]) {
+                const double s = (t - bc.abscissa[i]) / (bc.abscissa[i + 1] - bc.abscissa[i]);
+                return bc.ordinate[i] + (bc.ordinate[i + 1] - bc.ordinate[i]) * s * s * s * (10.0 - 15.0 * s + 6.0 * s * s);
+            }
+        return 0.0;
+    }
+    return smooth_step_d1(t, bc.abscissa, bc.ordinate, n);
+}
+
+// BoundaryCondition::ApplyVelocity / ApplyAcceleration: overwrite prescribed components.
+void apply_bcs(const ob_problem* p, int which, double t, double* x) {
+    for (int k = 0; k < p->num_bcs; ++k) {
+        const ob_bc& bc = p->bcs[k];
+        if (t < bc.active_start || t > bc.active_end) continue;
+        const double s = bc_scale(bc, which, t);
+        for (int c = 0; c < 3; ++c) {
+            if (!(bc.component_mask & (1 << c))) continue;
+            const double val = bc.values[c] * s;
+            for (int64_t i = 0; i < bc.num_nodes; ++i) x[bc.nodes[i] * 3 + c] = val;
+        }
+    }
+}
+
+// 1 where the dof is free at time t (for the adjoint), 0 where a BC overwrites it.
+void free_mask(const ob_problem* p, double t, std::vector<double>& m) {
+    m.assign(static_cast<size_t>(p->num_nodes) * 3, 1.0);
+    for (int k = 0; k < p->num_bcs; ++k) {
+        const ob_bc& bc = p->bcs[k];
+        if (t < bc.active_start || t > bc.active_end) continue;
+        for (int c = 0; c < 3; ++c) {
+            if (!(bc.component_mask & (1 << c))) continue;
+            for (int64_t i = 0; i < bc.num_nodes; ++i) m[bc.nodes[i] * 3 + c] = 0.0;
+        }
+    }
+}
+
+void compute_acceleration(const ob_problem* p, const double* m, const double* u, double* f, double* a) {
+    const int64_t N = p->num_nodes;
+    ob_internal_force(p, u, f);
+    const double* g = p->body_accel;
+    if (g[0] != 0.0 || g[1] != 0.0 || g[2] != 0.0)
+        for (int64_t n = 0; n < N; ++n)
+            for (int i = 0; i < 3; ++i) f[n * 3 + i] += g[i] * m[n];
+    // ExplicitTimeIntegrator.h:247-283: a = f / m.
+#pragma omp parallel for schedule(static)
+    for (int64_t n = 0; n < N; ++n)
+        for (int i = 0; i < 3; ++i) a[n * 3 + i] = f[n * 3 + i] / m[n];
+}
+
+// One central-difference step in the order of ExplicitSolver::Solve (src/Solvers/Explicit.cpp:383-483).
+void cd_step(const ob_problem* p, const double* m, double dtn, double time, double* u, double* v, double* a, double* f) {
+    const int64_t N = p->num_nodes;
+    const double half = 0.5 * dtn;
+    const double t_mid = time + 0.5 * dtn;
+    const double t_next = time + dtn;
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < N * 3; ++k) v[k] = v[k] + half * a[k];  // :286-326
+    apply_bcs(p, 0, t_mid, v);
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < N * 3; ++k) u[k] = u[k] + dtn * v[k];  // :97-134
+    compute_acceleration(p, m, u, f, a);
+    apply_bcs(p, 1, t_next, a);
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < N * 3; ++k) v[k] += half * a[k];  // :329-364
+}
+
+std::vector<double> mass_of(const ob_problem* p) {
+    std::vector<double> m(static_cast<size_t>(p->num_nodes));
+    if (p->mass)
+        std::copy(p->mass, p->mass + p->num_nodes, m.begin());
+    else
+        ob_lumped_mass(p, m.data());
+    return m;
+}
+
+// VJP of the internal force of one block, accumulating gu (nodes) and writing gmu/gkappa (elements).
+void add_block_vjp(const ob_problem* p, const ob_block& b, const double* u, const double* lam, double* gu,
+                   double* gmu, double* gkappa) {
+    const bool cells = b.kind == OB_CELLS;
+    const int nn = cells ? 0 : nodes_per_elem(b.kind);
+    std::vector<int64_t> start(b.num_elems + 1);
+    for (int64_t e = 0; e <= b.num_elems; ++e) start[e] = cells ? b.cell_ptr[e] : e * nn;
+    std::vector<double> slots(static_cast<size_t>(start[b.num_elems]) * 3, 0.0);
+    std::vector<int32_t> dummy;
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < b.num_elems; ++e) {
+        double lambda, mu;
+        block_lame(b, e, &lambda, &mu);
+        double gl = 0.0, gm = 0.0;
+        const int64_t s0 = start[e], s1 = start[e + 1];
+        const int64_t ne = s1 - s0;
+        std::vector<double> Bv(static_cast<size_t>(ne) * 3);
+        std::vector<int32_t> nodes(ne);
+        for (int64_t s = 0; s < ne; ++s) nodes[s] = cells ? b.cell_nodes[s0 + s] : b.conn[s0 + s];
+        const int ngp = cells ? 1 : (b.kind == OB_HEX8_GAUSS ? 8 : 1);
+        double X[24];
+        if (!cells)
+            for (int a = 0; a < nn; ++a)
+                for (int i = 0; i < 3; ++i) X[a * 3 + i] = p->coords[nodes[a] * 3 + i];
+        for (int gp = 0; gp < ngp; ++gp) {
+            double w;
+            if (cells) {
+                for (int64_t s = 0; s < ne * 3; ++s) Bv[s] = b.cell_grads[s0 * 3 + s];
+                w = b.cell_volumes[e];
+            } else if (b.kind == OB_HEX8_GAUSS) {
+                double xi[3], dN[24];
+                hex8_gauss_point(gp, xi);
+                hex8_dN(xi, dN);
+                w = gauss_bw<8>(X, dN, 1.0, Bv.data());
+            } else {
+                w = gauss_bw<4>(X, kTet4dN, 1.0 / 6.0, Bv.data());
+            }
+            double H[9] = {0}, L[9] = {0};
+            for (int64_t s = 0; s < ne; ++s)
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) {
+                        H[i * 3 + j] += u[nodes[s] * 3 + i] * Bv[s * 3 + j];
+                        L[i * 3 + j] += lam[nodes[s] * 3 + i] * Bv[s * 3 + j];
+                    }
+            double dP[9], dPl[9], dPm[9];
+            stress_tangent(b.material, lambda, mu, H, L, dP, dPl, dPm);
+            double sl = 0.0, sm = 0.0;
+            for (int k = 0; k < 9; ++k) {
+                sl += L[k] * dPl[k];
+                sm += L[k] * dPm[k];
+            }
+            gl -= w * sl;
+            gm -= w * sm;
+            for (int64_t s = 0; s < ne; ++s)
+                for (int i = 0; i < 3; ++i)
+                    slots[(s0 + s) * 3 + i] -= w * (Bv[s * 3 + 0] * dP[i * 3 + 0] + Bv[s * 3 + 1] * dP[i * 3 + 1] + Bv[s * 3 + 2] * dP[i * 3 + 2]);
+        }
+        // lambda = kappa - 2/3 mu  =>  d/dmu|kappa = d/dmu|lambda - 2/3 d/dlambda ; d/dkappa = d/dlambda
+        if (gmu) gmu[e] = gm - 2.0 / 3.0 * gl;
+        if (gkappa) gkappa[e] = gl;
+    }
+    for (int64_t e = 0; e < b.num_elems; ++e)
+        for (int64_t s = start[e]; s < start[e + 1]; ++s) {
+            const int32_t n = cells ? b.cell_nodes[s] : b.conn[s];
+            for (int i = 0; i < 3; ++i) gu[n * 3 + i] += slots[s * 3 + i];
+        }
+}
+
+// 4x4 inverse by Gauss-Jordan elimination with partial pivoting (stands in for
+// Eigen's fullPivLu().inverse() used by InvertMatrix<4>, MathUtils.h:307-319).
+bool inv4(const double* M, double* R) {
+    double A[4][8];
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) {
+            A[i][j] = M[i * 4 + j];
+            A[i][j + 4] = (i == j) ? 1.0 : 0.0;
+        }
+    for (int c = 0; c < 4; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < 4; ++r)
+            if (std::fabs(A[r][c]) > std::fabs(A[piv][c])) piv = r;
+        if (A[piv][c] == 0.0) return false;
+        if (piv != c)
+            for (int j = 0; j < 8; ++j) std::swap(A[c][j], A[piv][j]);
+        const double d = 1.0 / A[c][c];
+        for (int j = 0; j < 8; ++j) A[c][j] *= d;
+        for (int r = 0; r < 4; ++r) {
+            if (r == c) continue;
+            const double fct = A[r][c];
+            if (fct == 0.0) continue;
+            for (int j = 0; j < 8; ++j) A[r][j] -= fct * A[c][j];
+        }
+    }
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) R[i * 4 + j] = A[i][j + 4];
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+void ob_set_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
+int ob_get_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+void ob_tet4_gauss_bw(const double X[12], double B[12], double* w) { *w = gauss_bw<4>(X, kTet4dN, 1.0 / 6.0, B); }
+
+void ob_hex8_gauss_bw(const double X[24], int gp, double B[24], double* w) {
+    double xi[3], dN[24];
+    hex8_gauss_point(gp, xi);
+    hex8_dN(xi, dN);
+    *w = gauss_bw<8>(X, dN, 1.0, B);
+}
+
+// QuadratureSmoothed.h:32-63 (Tet4, area-weighted face normals, Seacas face order).
+void ob_tet4_smoothed_bw(const double X[12], double B[12], double* volume) {
+    static const int faces[4][3] = {{0, 1, 3}, {1, 2, 3}, {0, 3, 2}, {0, 2, 1}};
+    for (int k = 0; k < 12; ++k) B[k] = 0.0;
+    double vol = 0.0;
+    for (int j = 0; j < 4; ++j) {
+        const double* p0 = X + 3 * faces[j][0];
+        const double* p1 = X + 3 * faces[j][1];
+        const double* p2 = X + 3 * faces[j][2];
+        const double e1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+        const double e2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
+        const double nrm[3] = {(e1[1] * e2[2] - e1[2] * e2[1]) / 2.0, (e1[2] * e2[0] - e1[0] * e2[2]) / 2.0,
+                               (e1[0] * e2[1] - e1[1] * e2[0]) / 2.0};
+        vol += p0[0] * nrm[0] + p0[1] * nrm[1] + p0[2] * nrm[2];
+        for (int l = 0; l < 3; ++l)
+            for (int i = 0; i < 3; ++i) B[faces[j][l] * 3 + i] += nrm[i] / 3.0;
+    }
+    vol /= 3.0;
+    for (int k = 0; k < 12; ++k) B[k] /= vol;
+    *volume = vol;
+}
+
+// QuadratureSmoothed.h:97-142 (Hex8, each quad face split into 4 triangles about its mid point).
+void ob_hex8_smoothed_bw(const double X[24], double B[24], double* volume) {
+    static const int faces[6][4] = {{0, 1, 5, 4}, {1, 2, 6, 5}, {2, 3, 7, 6}, {0, 4, 7, 3}, {0, 3, 2, 1}, {4, 5, 6, 7}};
+    for (int k = 0; k < 24; ++k) B[k] = 0.0;
+    double vol = 0.0;
+    for (int j = 0; j < 6; ++j) {
+        double mid[3] = {0, 0, 0};
+        for (int k = 0; k < 4; ++k)
+            for (int i = 0; i < 3; ++i) mid[i] += X[faces[j][k] * 3 + i];
+        for (int i = 0; i < 3; ++i) mid[i] /= 4.0;
+        int km1 = 3;
+        for (int k = 0; k < 4; ++k) {
+            double e1[3], e2[3];
+            for (int i = 0; i < 3; ++i) {
+                e1[i] = X[faces[j][km1] * 3 + i] - mid[i];
+                e2[i] = X[faces[j][k] * 3 + i] - mid[i];
+            }
+            const double nrm[3] = {(e1[1] * e2[2] - e1[2] * e2[1]) / 2.0, (e1[2] * e2[0] - e1[0] * e2[2]) / 2.0,
+                                   (e1[0] * e2[1] - e1[1] * e2[0]) / 2.0};
+            vol += mid[0] * nrm[0] + mid[1] * nrm[1] + mid[2] * nrm[2];
+            for (int l = 0; l < 4; ++l) {
+                const double wgt = (l == k || l == km1) ? 5.0 / 12.0 : 1.0 / 12.0;
+                for (int i = 0; i < 3; ++i) B[faces[j][l] * 3 + i] += nrm[i] * wgt;
+            }
+            km1 = k;
+        }
+    }
+    vol /= 3.0;
+    for (int k = 0; k < 24; ++k) B[k] /= vol;
+    *volume = vol;
+}
+
+// Materials/Base.h:47-158 LinearElasticProperties::CompleteProperties + CheckPhysicalBounds.
+int ob_complete_properties(double props[5], char* msg, int msg_len) {
+    double& E = props[0];
+    double& nu = props[1];
+    double& G = props[2];
+    double& lam = props[3];
+    double& K = props[4];
+    auto def = [](double x) { return !std::isnan(x); };
+    const int count = def(E) + def(nu) + def(G) + def(lam) + def(K);
+    auto fail = [&](const char* m) {
+        if (msg && msg_len > 0) std::snprintf(msg, msg_len, "%s", m);
+        return -1;
+    };
+    if (count != 2) {
+        char buf[96];
+        std::snprintf(buf, sizeof(buf), "Exactly two properties must be defined. Defined: %d", count);
+        return fail(buf);
+    }
+    if (def(K) && def(E)) {
+        nu = (3 * K - E) / (6 * K);
+        G = E / (2 * (1 + nu));
+        lam = (E * nu) / ((1 + nu) * (1 - 2 * nu));
+    } else if (def(K) && def(lam)) {
+        G = (3 * (K - lam)) / 2;
+        nu = lam / (2 * (lam + G));
+        E = 2 * G * (1 + nu);
+    } else if (def(K) && def(G)) {
+        lam = K - (2.0 / 3.0) * G;
+        nu = lam / (2 * (lam + G));
+        E = 2 * G * (1 + nu);
+    } else if (def(K) && def(nu)) {
+        E = 3 * K * (1 - 2 * nu);
+        G = E / (2 * (1 + nu));
+        lam = (E * nu) / ((1 + nu) * (1 - 2 * nu));
+    } else if (def(E) && def(lam)) {
+        const double a = 2 * lam, b = lam + E, c = -lam;
+        const double disc = b * b - 4 * a * c;
+        nu = (-b + std::sqrt(disc)) / (2 * a);
+        G = E / (2 * (1 + nu));
+        K = lam + (2.0 / 3.0) * G;
+    } else if (def(E) && def(G)) {
+        nu = (E / (2 * G)) - 1;
+        lam = (E * nu) / ((1 + nu) * (1 - 2 * nu));
+        K = lam + (2.0 / 3.0) * G;
+    } else if (def(E) && def(nu)) {
+        G = E / (2 * (1 + nu));
+        lam = (E * nu) / ((1 + nu) * (1 - 2 * nu));
+        K = E / (3 * (1 - 2 * nu));
+    } else if (def(lam) && def(G)) {
+        K = lam + (2.0 / 3.0) * G;
+        nu = lam / (2 * (lam + G));
+        E = 2 * G * (1 + nu);
+    } else if (def(lam) && def(nu)) {
+        E = (lam * (1 + nu) * (1 - 2 * nu)) / nu;
+        G = E / (2 * (1 + nu));
+        K = lam + (2.0 / 3.0) * G;
+    } else if (def(G) && def(nu)) {
+        E = 2 * G * (1 + nu);
+        lam = (2 * G * nu) / (1 - 2 * nu);
+        K = (2 * G * (1 + nu)) / (3 * (1 - 2 * nu));
+    } else {
+        return fail("Unsupported property pair combination");
+    }
+    if (nu < -1.0 || nu >= 0.5) return fail("Poisson's ratio violation: must be in [-1, 0.5)");
+    if (E <= 0.0) return fail("Young's modulus must be positive");
+    if (G <= 0.0) return fail("Shear modulus must be positive");
+    if (K <= 0.0) return fail("Bulk modulus must be positive");
+    if (lam <= -(2.0 / 3.0) * G) return fail("Lame's parameter violation: lambda must be > -2G/3");
+    return 0;
+}
+
+void ob_stress(int material, double lambda, double mu, int64_t n, const double* H, double* P) {
+    for (int64_t k = 0; k < n; ++k) stress(material, lambda, mu, H + 9 * k, P + 9 * k);
+}
+
+// Internal force over all parts, overwriting f (the solver zeroes the force field
+// before the contributions accumulate, src/Solvers/Explicit.cpp:157-163).
+void ob_internal_force(const ob_problem* p, const double* u, double* f) {
+    std::fill(f, f + p->num_nodes * 3, 0.0);
+    for (int k = 0; k < p->num_blocks; ++k) add_block_forces(p, p->blocks[k], u, f);
+}
+
+// ComputeElementVolumeFunctor.h:20-79: V_e = sum_gp w_gp.
+void ob_element_volumes(const ob_problem* p, int32_t block, double* vol) {
+    const ob_block& b = p->blocks[block];
+    if (b.kind == OB_CELLS) {
+        for (int64_t c = 0; c < b.num_elems; ++c) vol[c] = b.cell_volumes[c];
+        return;
+    }
+    const int nn = nodes_per_elem(b.kind);
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < b.num_elems; ++e) {
+        double X[24];
+        for (int a = 0; a < nn; ++a)
+            for (int i = 0; i < 3; ++i) X[a * 3 + i] = p->coords[b.conn[e * nn + a] * 3 + i];
+        double V = 0.0, B[24];
+        if (b.kind == OB_HEX8_GAUSS) {
+            for (int gp = 0; gp < 8; ++gp) {
+                double xi[3], dN[24];
+                hex8_gauss_point(gp, xi);
+                hex8_dN(xi, dN);
+                V += gauss_bw<8>(X, dN, 1.0, B);
+            }
+        } else {
+            V = gauss_bw<4>(X, kTet4dN, 1.0 / 6.0, B);
+        }
+        vol[e] = V;
+    }
+}
+
+// src/MassUtils.cpp:17-46: m_a += rho V_e / n_en over the Gauss blocks, in element order.
+void ob_lumped_mass(const ob_problem* p, double* m) {
+    std::fill(m, m + p->num_nodes, 0.0);
+    for (int k = 0; k < p->num_blocks; ++k) {
+        const ob_block& b = p->blocks[k];
+        if (b.kind == OB_CELLS) continue;
+        const int nn = nodes_per_elem(b.kind);
+        std::vector<double> vol(b.num_elems);
+        ob_element_volumes(p, k, vol.data());
+        for (int64_t e = 0; e < b.num_elems; ++e) {
+            const double me = vol[e] * b.density / nn;
+            for (int a = 0; a < nn; ++a) m[b.conn[e * nn + a]] += me;
+        }
+    }
+}
+
+// DirectTimeStepper (include/TimeStepper.h:97-128) driven by ExplicitSolver::Solve's
+// `while (!AtEnd(time))` loop with `time += time_increment`.
+int64_t ob_direct_time_schedule(double dt, double t_end, int64_t max_steps, double* dts) {
+    double time = 0.0;
+    int64_t n = 0;
+    while (!(time >= t_end) && n < max_steps) {
+        double d;
+        if (time + dt <= t_end)
+            d = dt;
+        else if (time > t_end)
+            d = 0.0;
+        else
+            d = t_end - time;
+        if (dts) dts[n] = d;
+        time += d;
+        ++n;
+    }
+    return n;
+}
+
+int ob_init_acceleration(const ob_problem* p, const double* u, double* a) {
+    std::vector<double> m = mass_of(p);
+    std::vector<double> f(static_cast<size_t>(p->num_nodes) * 3);
+    compute_acceleration(p, m.data(), u, f.data(), a);
+    return 0;
+}
+
+int ob_explicit_steps(const ob_problem* p, int64_t nsteps, const double* dts, double t0, double* u, double* v, double* a) {
+    std::vector<double> m = mass_of(p);
+    std::vector<double> f(static_cast<size_t>(p->num_nodes) * 3);
+    double time = t0;
+    for (int64_t n = 0; n < nsteps; ++n) {
+        cd_step(p, m.data(), dts[n], time, u, v, a, f.data());
+        time += dts[n];
+    }
+    return 0;
+}
+
+// ExplicitSolver::Solve (src/Solvers/Explicit.cpp:308-498): initial force and
+// acceleration at t=0 (no BC on a^0), then the central-difference loop.
+int ob_explicit_solve(const ob_problem* p, double dt, double t_end, int64_t max_steps, double* u, double* v, double* a,
+                      int64_t* steps_done) {
+    std::vector<double> m = mass_of(p);
+    std::vector<double> f(static_cast<size_t>(p->num_nodes) * 3);
+    compute_acceleration(p, m.data(), u, f.data(), a);
+    const int64_t n = ob_direct_time_schedule(dt, t_end, max_steps, nullptr);
+    std::vector<double> dts(n);
+    ob_direct_time_schedule(dt, t_end, max_steps, dts.data());
+    double time = 0.0;
+    for (int64_t k = 0; k < n; ++k) {
+        cd_step(p, m.data(), dts[k], time, u, v, a, f.data());
+        time += dts[k];
+    }
+    if (steps_done) *steps_done = n;
+    return 0;
+}
+
+void ob_vjp_force(const ob_problem* p, const double* u, const double* lam, double* gu, double* gmu, double* gkappa) {
+    std::fill(gu, gu + p->num_nodes * 3, 0.0);
+    int64_t off = 0;
+    for (int k = 0; k < p->num_blocks; ++k) {
+        add_block_vjp(p, p->blocks[k], u, lam, gu, gmu ? gmu + off : nullptr, gkappa ? gkappa + off : nullptr);
+        off += p->blocks[k].num_elems;
+    }
+}
+
+// Discrete adjoint of the central-difference trajectory (new capability): the
+// forward pass stores every displacement; the reverse pass transposes each
+// operation of cd_step in reverse order. L = sum_s |u_s^K|^2.
+int ob_adjoint(const ob_problem* p, int64_t nsteps, double dt, const double* u0, const double* v0, int32_t num_sensors,
+               const int32_t* sensors, double* loss, double* gmu, double* gkappa) {
+    const int64_t N = p->num_nodes;
+    const size_t N3 = static_cast<size_t>(N) * 3;
+    std::vector<double> m = mass_of(p);
+    std::vector<double> u(u0, u0 + N3), v(v0, v0 + N3), a(N3), f(N3);
+    std::vector<std::vector<double>> us;
+    us.reserve(nsteps + 1);
+    us.push_back(u);
+    compute_acceleration(p, m.data(), u.data(), f.data(), a.data());
+    double time = 0.0;
+    std::vector<double> times(nsteps);
+    for (int64_t n = 0; n < nsteps; ++n) {
+        times[n] = time;
+        cd_step(p, m.data(), dt, time, u.data(), v.data(), a.data(), f.data());
+        time += dt;
+        us.push_back(u);
+    }
+    double L = 0.0;
+    std::vector<double> ub(N3, 0.0), vb(N3, 0.0), ab(N3, 0.0), fb(N3), gu(N3), mk;
+    for (int32_t s = 0; s < num_sensors; ++s)
+        for (int i = 0; i < 3; ++i) {
+            const double x = u[sensors[s] * 3 + i];
+            L += x * x;
+            ub[sensors[s] * 3 + i] += 2.0 * x;
+        }
+    int64_t ne = 0;
+    for (int k = 0; k < p->num_blocks; ++k) ne += p->blocks[k].num_elems;
+    std::vector<double> gm(ne, 0.0), gk(ne, 0.0), tm(ne), tk(ne);
+    const double h = 0.5 * dt;
+    for (int64_t n = nsteps - 1; n >= 0; --n) {
+        const double t_mid = times[n] + 0.5 * dt, t_next = times[n] + dt;
+        std::vector<double> vhb = vb;
+        free_mask(p, t_next, mk);
+        for (size_t k = 0; k < N3; ++k) fb[k] = mk[k] * (ab[k] + h * vb[k]) / m[k / 3];
+        ob_vjp_force(p, us[n + 1].data(), fb.data(), gu.data(), tm.data(), tk.data());
+        for (int64_t e = 0; e < ne; ++e) {
+            gm[e] += tm[e];
+            gk[e] += tk[e];
+        }
+        free_mask(p, t_mid, mk);
+        for (size_t k = 0; k < N3; ++k) {
+            ub[k] += gu[k];
+            vhb[k] += dt * ub[k];
+            const double wb = mk[k] * vhb[k];
+            vb[k] = wb;
+            ab[k] = h * wb;
+        }
+    }
+    for (size_t k = 0; k < N3; ++k) fb[k] = ab[k] / m[k / 3];
+    ob_vjp_force(p, us[0].data(), fb.data(), gu.data(), tm.data(), tk.data());
+    for (int64_t e = 0; e < ne; ++e) {
+        gm[e] += tm[e];
+        gk[e] += tk[e];
+    }
+    if (loss) *loss = L;
+    if (gmu) std::copy(gm.begin(), gm.end(), gmu);
+    if (gkappa) std::copy(gk.begin(), gk.end(), gkappa);
+    return 0;
+}
+
+// MathUtils.h:321-330 ComputeKernel: cubic B-spline of r/R.
+double ob_rk_kernel(const double d[3], double R) {
+    const double r = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) / R;
+    if (r < 0.5) return 1.0 + 6.0 * r * r * (-1.0 + r);
+    if (r < 1.0) return 2.0 * (1.0 + r * (-3.0 + 3.0 * r - 1.0 * r * r));
+    return 0.0;
+}
+
+// FunctionCreationProcessor.h:85-130 + ShapeFunctionsFunctorReproducingKernel.h:189-257
+// (linear basis, BasesLinear :54-63): kernel with the neighbour's radius, moment
+// matrix M = sum phi H H^T, psi_i = (M^-1 row 0) H_i phi_i; Shepard fallback.
+int ob_rk_function_values(int64_t num_points, const double* points, const double* coords, const double* kernel_radius,
+                          const int64_t* nbr_ptr, const int32_t* nbr, double* values) {
+    int bad = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : bad)
+    for (int64_t i = 0; i < num_points; ++i) {
+        const int64_t s0 = nbr_ptr[i], s1 = nbr_ptr[i + 1];
+        const int64_t nn = s1 - s0;
+        if (nn == 0) continue;
+        if (nn == 1) {
+            values[s0] = 1.0;
+            continue;
+        }
+        std::vector<double> sh(nn * 3), phi(nn);
+        double M[16] = {0};
+        double ksum = 0.0;
+        for (int64_t k = 0; k < nn; ++k) {
+            const int32_t j = nbr[s0 + k];
+            for (int c = 0; c < 3; ++c) sh[k * 3 + c] = points[i * 3 + c] - coords[j * 3 + c];
+            phi[k] = ob_rk_kernel(&sh[k * 3], kernel_radius[j]);
+            if (phi[k] == 0.0) continue;
+            const double Hv[4] = {1.0, sh[k * 3], sh[k * 3 + 1], sh[k * 3 + 2]};
+            for (int r = 0; r < 4; ++r)
+                for (int c = 0; c < 4; ++c) M[r * 4 + c] += phi[k] * Hv[r] * Hv[c];
+            ksum += phi[k];
+        }
+        double Mi[16];
+        const bool ok = inv4(M, Mi);
+        double nrm = 0.0;
+        for (int k = 0; k < 16; ++k) nrm += Mi[k] * Mi[k];
+        if (!ok || std::sqrt(nrm) < 1e-15) {
+            for (int64_t k = 0; k < nn; ++k) values[s0 + k] = phi[k] / ksum;
+            ++bad;
+            continue;
+        }
+        for (int64_t k = 0; k < nn; ++k) {
+            if (phi[k] == 0.0) {
+                values[s0 + k] = 0.0;
+                continue;
+            }
+            const double Hv[4] = {1.0, sh[k * 3], sh[k * 3 + 1], sh[k * 3 + 2]};
+            values[s0 + k] = (Mi[0] * Hv[0] + Mi[1] * Hv[1] + Mi[2] * Hv[2] + Mi[3] * Hv[3]) * phi[k];
+        }
+    }
+    return bad;
+}
+
+}  // extern "C"

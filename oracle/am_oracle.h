@@ -1,0 +1,121 @@
+/*
+ * am_oracle.h -- CPU FP64 restatement of aperi-mech's explicit-dynamics hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY. This library is the parity checker for the CUDA
+ * path in aperi_mech_b200: only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline / reference legs of bench.py load it. The product never links,
+ * calls or falls back to it.
+ *
+ * Each routine cites the reference function it restates (paths are relative
+ * to the aperi-mech source tree). The arithmetic is plain FP64 with no Eigen;
+ * 3x3 inverses use the adjugate formula (Eigen's fixed-size inverse is the
+ * same closed form, so results agree to a few ulps).
+ *
+ * Parity pins: the oracle is checked against the known answers of the
+ * reference's own unit tests (QuadratureTests.cpp, MaterialDriverTest.cpp,
+ * SolverTest.cpp gravity/free-flight, ForceTest.cpp/PatchTestFixture.h shear
+ * and tension patch tests, LinearElasticPropertiesTest.cpp) in tests/.
+ * Hex8 2x2x2 Gauss force and the adjoint have no reference known answer
+ * (parity unpinned there); they are pinned by analytic patch/rigid-motion
+ * checks and by finite differences instead.
+ */
+#ifndef AM_ORACLE_H
+#define AM_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { OB_TET4_GAUSS = 0, OB_HEX8_GAUSS = 1, OB_CELLS = 2 };
+enum { OB_LINEAR_ELASTIC = 0, OB_NEO_HOOKEAN = 1, OB_SVK = 2 };
+enum { OB_BC_DISPLACEMENT = 0, OB_BC_VELOCITY = 1 };
+enum { OB_TF_RAMP = 0, OB_TF_SMOOTH_STEP = 1 };
+
+/* One part (InternalForceContribution): element kind + material (+ optional
+ * per-element shear/bulk fields, which replace lambda/mu element-wise with
+ * lambda_e = kappa_e - 2/3 mu_e, mu_e). */
+typedef struct {
+    int32_t kind;
+    int32_t material;
+    double lambda, mu, density;
+    const double* mu_field;     /* per element / cell, or NULL */
+    const double* kappa_field;  /* per element / cell, or NULL */
+    int64_t num_elems;          /* elements (Gauss) or cells (OB_CELLS) */
+    const int32_t* conn;        /* Gauss: num_elems * nodes_per_elem */
+    const int64_t* cell_ptr;    /* cells: num_elems + 1 */
+    const int32_t* cell_nodes;  /* cells: cell_ptr[num_elems] */
+    const double* cell_grads;   /* cells: 3 per entry, row-major */
+    const double* cell_volumes; /* cells: num_elems */
+} ob_block;
+
+/* One displacement/velocity boundary condition (BoundaryCondition.cpp). */
+typedef struct {
+    int64_t num_nodes;
+    const int32_t* nodes;
+    int32_t component_mask; /* bit c: component c prescribed */
+    int32_t kind;           /* OB_BC_DISPLACEMENT / OB_BC_VELOCITY */
+    int32_t time_function;  /* OB_TF_RAMP / OB_TF_SMOOTH_STEP */
+    int32_t num_points;
+    double values[3];
+    const double* abscissa;
+    const double* ordinate;
+    double active_start, active_end;
+} ob_bc;
+
+typedef struct {
+    int64_t num_nodes;
+    const double* coords; /* num_nodes * 3 */
+    int32_t num_blocks;
+    const ob_block* blocks;
+    int32_t num_bcs;
+    const ob_bc* bcs;
+    const double* mass;    /* lumped nodal mass, or NULL = from Gauss blocks */
+    double body_accel[3];  /* gravity vector (ExternalForceContributionGravity) */
+} ob_problem;
+
+/* ---- quadrature (QuadratureGaussian.h, QuadratureSmoothed.h) ---- */
+void ob_tet4_gauss_bw(const double X[12], double B[12], double* w);
+void ob_hex8_gauss_bw(const double X[24], int gp, double B[24], double* w);
+void ob_tet4_smoothed_bw(const double X[12], double B[12], double* volume);
+void ob_hex8_smoothed_bw(const double X[24], double B[24], double* volume);
+
+/* ---- materials (Materials/Base.h, LinearElastic.h, NeoHooke.h, Elastic.h) ---- */
+/* props = {E, nu, mu, lambda, K}; NaN = undefined. Returns 0, or -1 with msg. */
+int ob_complete_properties(double props[5], char* msg, int msg_len);
+void ob_stress(int material, double lambda, double mu, int64_t n, const double* H, double* P);
+
+/* ---- forces, mass, time integration ---- */
+void ob_internal_force(const ob_problem* p, const double* u, double* f);
+void ob_element_volumes(const ob_problem* p, int32_t block, double* vol);
+void ob_lumped_mass(const ob_problem* p, double* m);
+int64_t ob_direct_time_schedule(double dt, double t_end, int64_t max_steps, double* dts);
+int ob_explicit_solve(const ob_problem* p, double dt, double t_end, int64_t max_steps,
+                      double* u, double* v, double* a, int64_t* steps_done);
+int ob_init_acceleration(const ob_problem* p, const double* u, double* a);
+int ob_explicit_steps(const ob_problem* p, int64_t nsteps, const double* dts, double t0,
+                      double* u, double* v, double* a);
+
+/* ---- adjoint (new capability; no reference counterpart) ---- */
+void ob_vjp_force(const ob_problem* p, const double* u, const double* lam, double* gu,
+                  double* gmu, double* gkappa);
+int ob_adjoint(const ob_problem* p, int64_t nsteps, double dt, const double* u0,
+               const double* v0, int32_t num_sensors, const int32_t* sensors, double* loss,
+               double* gmu, double* gkappa);
+
+/* ---- RKPM setup (ShapeFunctionsFunctorReproducingKernel.h, MathUtils.h,
+ *      FunctionCreationProcessor.h, NeighborSearchProcessor) ---- */
+double ob_rk_kernel(const double d[3], double R);
+int ob_rk_function_values(int64_t num_points, const double* points, const double* coords,
+                          const double* kernel_radius, const int64_t* nbr_ptr,
+                          const int32_t* nbr, double* values);
+
+/* ---- threads ---- */
+void ob_set_threads(int n);
+int ob_get_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

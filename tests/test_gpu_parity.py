@@ -1,0 +1,384 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU FP64 oracle.
+
+Tolerances: the FP64 path must agree with the oracle to 1e-12 relative (max-norm
+relative to the largest entry); the mixed FP32-element / FP64-state path to the
+per-test tolerance written below."""
+from __future__ import annotations
+
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from helpers import expected_pk1, integrate_gravity, prescribed_patch, rel_err, svk_patch_material
+
+pytestmark = pytest.mark.gpu
+
+GOLD = Path(__file__).resolve().parent / "golden"
+FP64_TOL = 1e-12
+MIXED_FORCE_TOL = 5e-5
+
+
+def _load(name):
+    return json.loads((GOLD / name).read_text())
+
+
+def _mesh(kind, n, seed=0, jitter=0.2):
+    from aperi_mech_b200 import mesh
+
+    rng = np.random.default_rng(seed)
+    coords, conn = mesh.box_hex(n, n, n)
+    coords = mesh.jitter_interior(coords, jitter / n, rng)
+    if kind == "tet4":
+        conn = mesh.hex_to_tets(conn)
+    return coords, conn
+
+
+def _material(name):
+    from aperi_mech_b200.model import Material
+
+    if name == "neo_hookean":
+        return Material.create(name, 1000.0, shear_modulus=3.85e8, bulk_modulus=8.33e8)
+    return Material.create(name, 1000.0, youngs_modulus=1e9, poissons_ratio=0.3)
+
+
+def _fields(E, seed, with_fields):
+    if not with_fields:
+        return None, None
+    rng = np.random.default_rng(seed)
+    return 3.85e8 * np.exp(0.3 * rng.standard_normal(E)), 8.33e8 * np.exp(0.3 * rng.standard_normal(E))
+
+
+# ---- point kernels against the reference's unit-test known answers --------------------
+def test_quadrature_gpu_golden(gpu):
+    from aperi_mech_b200 import capi
+
+    tets = _load("quadrature_tet4.json")
+    X = np.array([c["X"] for c in tets])
+    for smoothed in (False, True):
+        B, w = capi.quadrature(capi.AM_TET4_GAUSS, X, smoothed=smoothed)
+        for k, c in enumerate(tets):
+            assert np.abs(B[k, 0] - np.array(c["B"])).max() < 1e-12, c["name"]
+            assert abs(w[k, 0] - c["w"]) < 1e-12
+    hexes = _load("quadrature_hex8_smoothed.json")
+    X = np.array([c["X"] for c in hexes])
+    B, w = capi.quadrature(capi.AM_HEX8_GAUSS, X, smoothed=True)
+    for k, c in enumerate(hexes):
+        assert np.abs(B[k, 0] - np.array(c["B"])).max() < 1e-12, c["name"]
+        assert abs(w[k, 0] - c["w"]) < 1e-12
+    Bg, wg = capi.quadrature(capi.AM_HEX8_GAUSS, X[:5])
+    for k in range(5):
+        avg = np.einsum("g,gaj->aj", wg[k], Bg[k]) / wg[k].sum()
+        assert np.abs(avg - np.array(hexes[k]["B"])).max() < 1e-12
+
+
+def test_material_driver_gpu(gpu, oracle_lib):
+    from aperi_mech_b200 import capi
+    from aperi_mech_b200.model import complete_properties
+
+    g = _load("material_driver_nh.json")
+    p = complete_properties(youngs_modulus=g["youngs_modulus"], poissons_ratio=g["poissons_ratio"])
+    P = capi.stress(capi.AM_NEO_HOOKEAN, p["lambda"], p["shear_modulus"], np.array(g["displacement_gradients"]))
+    for k, H in enumerate(g["displacement_gradients"]):
+        F = np.array(H) + np.eye(3)
+        sigma = P[k] @ F.T / np.linalg.det(F)
+        want = np.zeros((3, 3))
+        want[k, k] = g["expected_cauchy_diagonal"]
+        assert np.abs(sigma - want).max() < g["expected_cauchy_diagonal"] * g["rel_tol"]
+    rng = np.random.default_rng(5)
+    H = 0.05 * rng.standard_normal((64, 3, 3))
+    for name, code in (("linear_elastic", 0), ("neo_hookean", 1), ("elastic", 2)):
+        mat = _material(name)
+        got = capi.stress(code, mat.lam, mat.mu, H)
+        want = oracle_lib.stress(name, mat.lam, mat.mu, H)
+        assert rel_err(got, want) < 1e-14, name
+
+
+# ---- internal force ------------------------------------------------------------------
+@pytest.mark.parametrize("kind,n", [("tet4", 5), ("hex8", 6)])
+@pytest.mark.parametrize("material", ["linear_elastic", "neo_hookean", "elastic"])
+@pytest.mark.parametrize("with_fields", [False, True])
+def test_internal_force_parity(gpu, oracle_lib, kind, n, material, with_fields):
+    from aperi_mech_b200.model import ExplicitDynamics, Part
+
+    coords, conn = _mesh(kind, n, seed=1)
+    mu_f, k_f = _fields(conn.shape[0], 2, with_fields)
+    parts = [Part(kind, _material(material), conn=conn, mu_field=mu_f, kappa_field=k_f)]
+    rng = np.random.default_rng(4)
+    u = 2e-3 * rng.standard_normal(coords.shape) + 1e-3 * coords @ rng.standard_normal((3, 3))
+    want = oracle_lib.OracleProblem(coords, parts).internal_force(u)
+    with ExplicitDynamics(coords, parts) as m:
+        f64 = m.internal_force(u, "fp64")
+        f32 = m.internal_force(u, "mixed")
+        assert rel_err(m.mass(), oracle_lib.OracleProblem(coords, parts).lumped_mass()) < 1e-14
+    assert rel_err(f64, want) < FP64_TOL
+    assert rel_err(f32, want) < MIXED_FORCE_TOL
+
+
+def test_internal_force_two_parts_accumulate(gpu, oracle_lib):
+    """Two parts (InternalForceContributions) sharing nodes, and accumulate=1."""
+    from aperi_mech_b200.model import ExplicitDynamics, Part
+
+    coords, conn = _mesh("hex8", 6, seed=3)
+    half = conn.shape[0] // 2
+    parts = [Part("hex8", _material("neo_hookean"), conn=conn[:half]),
+             Part("hex8", _material("elastic"), conn=conn[half:])]
+    u = 1e-3 * np.random.default_rng(0).standard_normal(coords.shape)
+    want = oracle_lib.OracleProblem(coords, parts).internal_force(u)
+    with ExplicitDynamics(coords, parts) as m:
+        f = m.internal_force(u)
+        base = np.ones_like(f)
+        g = m.internal_force(u, out=base.copy(), accumulate=True)
+    assert rel_err(f, want) < FP64_TOL
+    assert rel_err(g - 1.0, want) < 1e-11
+
+
+def test_smoothed_cells_parity(gpu, oracle_lib):
+    from aperi_mech_b200.model import ExplicitDynamics
+    from aperi_mech_b200.smoothing import element_smoothing_part
+
+    coords, conn = _mesh("tet4", 5, seed=7)
+    part, mass = element_smoothing_part(coords, conn, _material("neo_hookean"))
+    u = 1e-3 * np.random.default_rng(1).standard_normal(coords.shape)
+    op = oracle_lib.OracleProblem(coords, [part], mass=mass)
+    want = op.internal_force(u)
+    with ExplicitDynamics(coords, [part], mass=mass) as m:
+        assert rel_err(m.internal_force(u), want) < FP64_TOL
+        assert rel_err(m.internal_force(u, "mixed"), want) < MIXED_FORCE_TOL
+
+
+# ---- time integration ----------------------------------------------------------------
+def _small_problem(name):
+    from aperi_mech_b200 import problems
+
+    if name == "hex8_le":
+        return problems.hex8_le_cube(n=6, seed=3, nsteps=100)
+    if name == "tet4_nh":
+        return problems.tet4_nh_shear(n=5, seed=3, nsteps=100)
+    return problems.hex8_nh_lognormal(n=5, seed=3, nsteps=60, bulk_field=True)
+
+
+@pytest.mark.parametrize("name", ["hex8_le", "tet4_nh", "hex8_nh_fields"])
+def test_run_fp64_matches_oracle(gpu, oracle_lib, name):
+    from aperi_mech_b200.model import ExplicitDynamics
+
+    p = _small_problem(name)
+    u0 = np.zeros_like(p.coords)
+    op = oracle_lib.OracleProblem.from_problem(p)
+    a0 = op.init_acceleration(u0)
+    want = op.steps(u0, p.v0, a0, np.full(p.nsteps, p.dt))
+    with ExplicitDynamics(p.coords, p.parts, p.bcs) as m:
+        m.set_state(u0, p.v0)
+        m.init_acceleration()
+        m.run(p.nsteps // 3, p.dt)
+        m.run(p.nsteps - p.nsteps // 3, p.dt, t0=(p.nsteps // 3) * p.dt)  # two calls == one run
+        got = m.get_state()
+    for g, w in zip(got, want):
+        assert rel_err(g, w) < FP64_TOL
+
+
+def test_run_is_bitwise_deterministic(gpu):
+    from aperi_mech_b200.model import ExplicitDynamics
+
+    p = _small_problem("tet4_nh")
+    outs = []
+    for _ in range(3):
+        with ExplicitDynamics(p.coords, p.parts, p.bcs) as m:
+            m.set_state(None, p.v0)
+            m.init_acceleration("mixed")
+            m.run(50, p.dt, "mixed")
+            outs.append(m.get_state())
+    for o in outs[1:]:
+        for a, b in zip(o, outs[0]):
+            assert np.array_equal(a, b)
+
+
+def test_mixed_accuracy_after_1000_steps(gpu):
+    """Mixed path vs the GPU FP64 path (itself 1e-12 from the oracle) on the neo-Hookean
+    Tet4 shear workload, 1000 steps: relative displacement error (L2) <= 1e-5."""
+    from aperi_mech_b200 import problems
+    from aperi_mech_b200.model import ExplicitDynamics
+    from helpers import l2_rel
+
+    p = problems.tet4_nh_shear(n=12, seed=0, nsteps=1000)
+    res = {}
+    for prec in ("fp64", "mixed"):
+        with ExplicitDynamics(p.coords, p.parts, p.bcs) as m:
+            m.set_state(None, p.v0)
+            m.init_acceleration(prec)
+            m.run(p.nsteps, p.dt, prec)
+            res[prec] = m.get_state()
+    assert l2_rel(res["mixed"][0], res["fp64"][0]) < 1e-5
+
+
+@pytest.mark.parametrize("kind", ["tet4", "hex8"])
+@pytest.mark.parametrize("direction,surface", [(1, 0), (2, 1), (0, 2)])
+def test_shear_patch_gpu(gpu, oracle_lib, kind, direction, surface):
+    from aperi_mech_b200.model import ExplicitDynamics
+
+    mag = 0.1
+    coords, parts, bcs, sets = prescribed_patch(kind, (1, 1, 1), direction, surface, mag)
+    op = oracle_lib.OracleProblem(coords, parts, bcs)
+    zero = np.zeros_like(coords)
+    wu, wv, wa, wn = op.solve(zero, zero, 0.1, 10.0)
+    with ExplicitDynamics(coords, parts, bcs) as m:
+        m.set_state(zero, zero)
+        n = m.solve(0.1, 10.0)
+        u, v, a = m.get_state()
+        f = m.internal_force(u)
+    assert n == wn
+    assert rel_err(u, wu) < FP64_TOL and rel_err(v, wv) < FP64_TOL
+    assert np.abs(a - wa).max() < 1e-12
+    H = np.zeros((3, 3))
+    H[direction, surface] = 2 * mag
+    P = expected_pk1(H, parts[0].material)
+    for i in range(3):
+        e = np.eye(3)[i]
+        assert np.abs(f[sets[f"surface_{2 * i + 1}"]].sum(axis=0) - P @ e).max() < 1e-8
+
+
+@pytest.mark.parametrize("kind", ["tet4", "hex8"])
+def test_tension_patch_gpu(gpu, oracle_lib, kind):
+    from aperi_mech_b200.model import ExplicitDynamics
+
+    coords, parts, bcs, sets = prescribed_patch(kind, (2, 2, 2), 0, 0, 0.1)
+    zero = np.zeros_like(coords)
+    with ExplicitDynamics(coords, parts, bcs) as m:
+        m.set_state(zero, zero)
+        m.solve(0.1, 10.0)
+        u, v, a = m.get_state()
+    H = np.zeros((3, 3))
+    H[0, 0] = 0.1
+    assert np.abs(u - (coords - 1.0) @ H.T).max() < 1e-9
+    assert np.abs(a).max() < 1e-9
+    wu, wv, wa, _ = oracle_lib.OracleProblem(coords, parts, bcs).solve(zero, zero, 0.1, 10.0)
+    assert rel_err(u, wu) < FP64_TOL and rel_err(v, wv) < FP64_TOL
+
+
+@pytest.mark.parametrize("gravity", [False, True])
+def test_free_flight_and_gravity_gpu(gpu, gravity):
+    from helpers import brick
+    from aperi_mech_b200.model import ExplicitDynamics, Part
+
+    coords, conn = brick("tet4", 1, 1, 1)
+    rho = 7850.0 * (1e4 if gravity else 1.0)
+    mat = svk_patch_material(E=2.1e11, nu=0.3, rho=rho)
+    d = np.array([1.4, -2.5, 2.9])
+    v0 = np.tile(1.23 * d / np.linalg.norm(d), (coords.shape[0], 1))
+    g = np.array([0.0, 0.0, -9.81]) if gravity else np.zeros(3)
+    with ExplicitDynamics(coords, [Part("tet4", mat, conn=conn)], body_accel=g) as m:
+        m.set_state(None, v0)
+        assert m.solve(0.1, 1.0) == 11
+        u, v, a = m.get_state()
+        assert abs(m.mass().sum() - rho) < 1e-12 * rho
+    du, dv = integrate_gravity(0.1, g, 1.0)
+    assert np.abs(u - (v0 + du)).max() < 1e-12
+    assert np.abs(v - (v0 + dv)).max() < 1e-12
+    assert np.abs(a - g).max() < 1e-11
+
+
+def test_velocity_bc_with_active_range(gpu, oracle_lib):
+    """Velocity BC (ramp) active only on [0.2, 0.8], overlapping a fixed support."""
+    from aperi_mech_b200 import mesh
+    from aperi_mech_b200.model import BoundaryCondition, ExplicitDynamics, Part
+
+    coords, conn = _mesh("hex8", 4, seed=9)
+    sets = mesh.side_sets(coords)
+    mat = _material("linear_elastic")
+    dt = 0.5 * 0.25 / np.sqrt((mat.lam + 2 * mat.mu) / mat.density)
+    T = 40 * dt
+    bcs = [BoundaryCondition.fixed(sets["surface_5"]),
+           BoundaryCondition(nodes=sets["surface_6"], values=(0.0, 0.0, 0.5), component_mask=4, kind="velocity",
+                             abscissa=(0.0, T), ordinate=(0.0, 1.0), active_range=(0.2 * T, 0.8 * T)),
+           BoundaryCondition(nodes=sets["surface_2"], values=(0.01, 0.0, 0.0), component_mask=1)]
+    parts = [Part("hex8", mat, conn=conn)]
+    zero = np.zeros_like(coords)
+    wu, wv, wa, wn = oracle_lib.OracleProblem(coords, parts, bcs).solve(zero, zero, dt, T)
+    with ExplicitDynamics(coords, parts, bcs) as m:
+        m.set_state(zero, zero)
+        assert m.solve(dt, T) == wn
+        u, v, a = m.get_state()
+    assert rel_err(u, wu) < FP64_TOL and rel_err(v, wv) < FP64_TOL and rel_err(a, wa) < FP64_TOL
+
+
+def test_inverted_element_reports_status(gpu):
+    from aperi_mech_b200.capi import AM_ENONPOS_J, AmError
+    from aperi_mech_b200.model import ExplicitDynamics, Part
+
+    coords, conn = _mesh("tet4", 2, seed=0, jitter=0.0)
+    with ExplicitDynamics(coords, [Part("tet4", _material("neo_hookean"), conn=conn)]) as m:
+        u = np.zeros_like(coords)
+        u[0] = [2.0, 2.0, 2.0]  # drives the corner tets through themselves: J < 0
+        with pytest.raises(AmError) as e:
+            m.internal_force(u)
+        assert e.value.code == AM_ENONPOS_J
+        m.internal_force(np.zeros_like(coords))  # the context stays usable
+
+
+# ---- adjoint ---------------------------------------------------------------------------
+@pytest.mark.parametrize("kind", ["tet4", "hex8"])
+@pytest.mark.parametrize("material", ["linear_elastic", "neo_hookean", "elastic"])
+def test_vjp_matches_oracle(gpu, oracle_lib, kind, material):
+    from aperi_mech_b200.model import ExplicitDynamics, Part
+
+    coords, conn = _mesh(kind, 4, seed=2)
+    mu_f, k_f = _fields(conn.shape[0], 3, True)
+    parts = [Part(kind, _material(material), conn=conn, mu_field=mu_f, kappa_field=k_f)]
+    rng = np.random.default_rng(8)
+    u = 1e-3 * rng.standard_normal(coords.shape)
+    lam = rng.standard_normal(coords.shape)
+    want = oracle_lib.OracleProblem(coords, parts).vjp_force(u, lam)
+    with ExplicitDynamics(coords, parts) as m:
+        got = m.vjp_force(u, lam)
+    for g, w in zip(got, want):
+        assert rel_err(g, w) < 1e-11
+
+
+def test_adjoint_matches_oracle(gpu, oracle_lib):
+    from aperi_mech_b200 import problems
+    from aperi_mech_b200.model import ExplicitDynamics
+
+    p = problems.hex8_nh_lognormal(n=4, seed=5, nsteps=31, bulk_field=True, num_sensors=20)
+    sens = p.meta["sensors"]
+    wl, wm, wk = oracle_lib.OracleProblem.from_problem(p).adjoint(p.nsteps, p.dt, np.zeros_like(p.coords), p.v0, sens)
+    with ExplicitDynamics(p.coords, p.parts, p.bcs) as m:
+        m.set_state(None, p.v0)
+        loss, gm, gk = m.adjoint(p.nsteps, p.dt, 7, sens)
+    assert abs(loss - wl) < 1e-12 * abs(wl)
+    assert rel_err(gm, wm) < 1e-10 and rel_err(gk, wk) < 1e-10
+
+
+def test_adjoint_finite_differences_hex8_64(gpu):
+    """Hex8 neo-Hookean 64^3 with a lognormal shear-modulus field, 200 steps, checkpoints
+    every 20: adjoint gradient vs central finite differences (step 1e-6 relative) on 32
+    seeded elements, relative error <= 1e-4."""
+    from aperi_mech_b200 import problems
+    from aperi_mech_b200.model import ExplicitDynamics
+
+    p = problems.hex8_nh_lognormal(n=64, seed=0, nsteps=200)
+    sens = p.meta["sensors"]
+    mu0 = p.parts[0].mu_field.copy()
+    elems = np.sort(np.random.default_rng(11).choice(mu0.size, size=32, replace=False))
+    with ExplicitDynamics(p.coords, p.parts, p.bcs) as m:
+        m.set_state(None, p.v0)
+        loss, gm, _ = m.adjoint(p.nsteps, p.dt, 20, sens)
+
+        def L(mu):
+            m.set_block_fields(0, mu_field=mu)
+            m.set_state(None, p.v0)
+            m.init_acceleration()
+            m.run(p.nsteps, p.dt)
+            u = m.get_state()[0][sens]
+            return float(np.sum(u * u))
+
+        assert abs(L(mu0) - loss) < 1e-12 * loss
+        errs = []
+        for e in elems:
+            h = 1e-6 * mu0[e]
+            mp, mm = mu0.copy(), mu0.copy()
+            mp[e] += h
+            mm[e] -= h
+            fd = (L(mp) - L(mm)) / (2 * h)
+            errs.append(abs(gm[e] - fd) / abs(fd))
+    assert max(errs) <= 1e-4, max(errs)
