@@ -142,9 +142,11 @@ struct am_ctx {
     std::string err;
     int64_t launches = 0;
     bool profiling = false;
-    double prof_ms[3] = {0, 0, 0};
-    int64_t prof_launches[3] = {0, 0, 0};
+    double prof_ms[4] = {0, 0, 0, 0};
+    int64_t prof_launches[4] = {0, 0, 0, 0};
     std::vector<cudaEvent_t> events;
+    std::vector<std::pair<int, int64_t>> mark_slot;
+    size_t n_marks = 0;
 
     am::NodeDev node_dev() const {
         am::NodeDev nd{};
@@ -220,13 +222,34 @@ struct am_ctx {
         if (h[0] != 0) fail(h[0], "device status " + std::to_string(h[0]));
     }
 
-    cudaEvent_t event(size_t k) {
-        while (events.size() <= k) {
+    // Profiling marks: each mark closes the interval since the previous mark and
+    // books it to a slot (-1: not booked). Elapsed times are read lazily by
+    // am_profile_read, so marks add no host synchronization to the timed work.
+    void mark(int slot, int64_t nlaunch) {
+        if (!profiling) return;
+        if (n_marks >= events.size()) {
             cudaEvent_t e;
             ck(cudaEventCreate(&e), "event create");
             events.push_back(e);
         }
-        return events[k];
+        ck(cudaEventRecord(events[n_marks], stream), "event record");
+        mark_slot.resize(n_marks + 1);
+        mark_slot[n_marks] = {slot, nlaunch};
+        ++n_marks;
+    }
+
+    void collect_marks() {
+        if (n_marks == 0) return;
+        ck(cudaStreamSynchronize(stream), "synchronize (profiling)");
+        for (size_t k = 1; k < n_marks; ++k) {
+            const int slot = mark_slot[k].first;
+            if (slot < 0) continue;
+            float ms = 0.f;
+            ck(cudaEventElapsedTime(&ms, events[k - 1], events[k]), "elapsed");
+            prof_ms[slot] += ms;
+            prof_launches[slot] += mark_slot[k].second;
+        }
+        n_marks = 0;
     }
 
     // Host time-function evaluation for steps [0, dts.size()) from t0 into the device table.
@@ -270,36 +293,20 @@ struct am_ctx {
         if (n1 <= n0) return;
         const am::NodeDev nd = node_dev();
         void* s = slots(mixed);
-        size_t ev = 0;
-        if (profiling) ck(cudaEventRecord(event(ev++), stream), "event");
+        mark(-1, 0);
         am::launch_prologue(nd, table + n0, U4, V4, A4, u_hist ? u_hist[0] : nullptr, stream);
         ++launches;
         check_launch("prologue kernel");
-        if (profiling) ck(cudaEventRecord(event(ev++), stream), "event");
+        mark(1, 1);
         for (int64_t n = n0; n < n1; ++n) {
             element_forces(mixed, U4);
-            if (profiling) ck(cudaEventRecord(event(ev++), stream), "event");
+            mark(0, static_cast<int64_t>(blocks.size()));
             const int advance = (n + 1 < n1) ? 1 : 0;
             double4* uc = (u_hist && advance) ? u_hist[n + 1 - n0] : nullptr;
             am::launch_node_step(nd, mixed, s, table, n, advance, U4, V4, A4, uc, status, stream);
             ++launches;
             check_launch("node step kernel");
-            if (profiling) ck(cudaEventRecord(event(ev++), stream), "event");
-        }
-        if (profiling) {
-            ck(cudaStreamSynchronize(stream), "synchronize (profiling)");
-            float ms = 0.f;
-            ck(cudaEventElapsedTime(&ms, events[0], events[1]), "elapsed");
-            prof_ms[1] += ms;
-            prof_launches[1] += 1;
-            for (int64_t k = 0; k < n1 - n0; ++k) {
-                ck(cudaEventElapsedTime(&ms, events[2 + 2 * k - 1 + 0], events[2 + 2 * k]), "elapsed");
-                prof_ms[0] += ms;
-                prof_launches[0] += static_cast<int64_t>(blocks.size());
-                ck(cudaEventElapsedTime(&ms, events[2 + 2 * k], events[2 + 2 * k + 1]), "elapsed");
-                prof_ms[1] += ms;
-                prof_launches[1] += 1;
-            }
+            mark(1, 1);
         }
     }
 
@@ -922,10 +929,13 @@ int am_adjoint(am_ctx* ctx, int64_t nsteps, double dt, int32_t ckpt_every, int32
             ck(cudaMemcpyAsync(ctx->V4, ck_v[s], bytes, cudaMemcpyDeviceToDevice, st), "restore");
             ck(cudaMemcpyAsync(ctx->A4, ck_a[s], bytes, cudaMemcpyDeviceToDevice, st), "restore");
             ctx->run_range(0, n0, n1, seg.data());
+            ctx->mark(-1, 0);
             for (int64_t n = n1 - 1; n >= n0; --n) {
                 ctx->vjp(seg[n - n0], ctx->L4, gm, gk, 1);
+                ctx->mark(2, static_cast<int64_t>(ctx->blocks.size()));
                 am::launch_adj_update(nd, ctx->slots64, ctx->table, n, UB, VB, AB, ctx->L4, st);
                 ++ctx->launches;
+                ctx->mark(3, 1);
             }
             ck(cudaGetLastError(), "adjoint kernels");
         }
@@ -1032,17 +1042,21 @@ int64_t am_launch_count(const am_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
 int am_profile_enable(am_ctx* ctx, int enable) {
     if (!ctx) return AM_EINVAL;
+    const int rc = guarded(ctx, [&] { ctx->collect_marks(); });
+    if (rc != AM_OK) return rc;
     ctx->profiling = enable != 0;
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < 4; ++k) {
         ctx->prof_ms[k] = 0.0;
         ctx->prof_launches[k] = 0;
     }
     return AM_OK;
 }
 
-int am_profile_read(am_ctx* ctx, double ms[3], int64_t launches[3]) {
+int am_profile_read(am_ctx* ctx, double ms[4], int64_t launches[4]) {
     if (!ctx) return AM_EINVAL;
-    for (int k = 0; k < 3; ++k) {
+    const int rc = guarded(ctx, [&] { ctx->collect_marks(); });
+    if (rc != AM_OK) return rc;
+    for (int k = 0; k < 4; ++k) {
         if (ms) ms[k] = ctx->prof_ms[k];
         if (launches) launches[k] = ctx->prof_launches[k];
     }

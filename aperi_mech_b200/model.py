@@ -266,8 +266,8 @@ class ExplicitDynamics:
         check(self.lib.am_profile_enable(self.ctx, int(enable)), self.ctx)
 
     def profile_read(self):
-        ms = (C.c_double * 3)()
-        n = (C.c_int64 * 3)()
+        ms = (C.c_double * 4)()
+        n = (C.c_int64 * 4)()
         check(self.lib.am_profile_read(self.ctx, ms, n), self.ctx)
         return list(ms), list(n)
 

@@ -198,7 +198,7 @@ def run_ours(args, rank, world, local):
             torch.cuda.synchronize(dev)
         ms = ev0.elapsed_time(ev1)
         launches[prec] = model.launch_count() - n0
-        kms, kn = model.profile_read()
+        kms, kn = model.profile_read()  # per-kernel events recorded inside the timed region
         model.profile(False)
         kernel_ms[prec] = {"element": kms[0] / max(kn[0], 1), "node": kms[1] / max(kn[1], 1),
                            "element_total": kms[0], "node_total": kms[1]}
@@ -259,14 +259,19 @@ def run_ours(args, rank, world, local):
                 times["forward"] = a0.elapsed_time(a1)
                 ma.set_state(None, pa.v0)
                 torch.cuda.synchronize(dev)
+                ma.profile(rep == 1)
                 a0.record(stream)
                 loss, gm, gk = ma.adjoint(pa.nsteps, pa.dt, 20, pa.meta["sensors"])
                 a1.record(stream)
                 torch.cuda.synchronize(dev)
                 times["adjoint"] = a0.elapsed_time(a1)
+            pms, pn = ma.profile_read()
+            ma.profile(False)
         adj = {"workload": f"hex8_nh_lognormal_{args.adjoint_n}", "steps": pa.nsteps, "ckpt_every": 20,
                "forward_ms": times["forward"], "adjoint_ms": times["adjoint"],
-               "ratio": times["adjoint"] / times["forward"]}
+               "ratio": times["adjoint"] / times["forward"],
+               "kernel_ms": {"element": pms[0], "node": pms[1], "vjp": pms[2], "adjoint_node": pms[3]},
+               "kernel_launches": {"element": pn[0], "node": pn[1], "vjp": pn[2], "adjoint_node": pn[3]}}
 
     # roofline of the dominant kernel of the headline (mixed) run
     km = kernel_ms["mixed"]

@@ -167,11 +167,13 @@ const char* am_status_string(int status);
 /* Kernel launches issued by this context so far (all kinds). */
 int64_t am_launch_count(const am_ctx* ctx);
 /* Per-kernel device timing: when enabled, every launch of the hot loop is
- * bracketed by CUDA events on the context stream. Slot 0: element/cell force
- * kernels, slot 1: node gather + update kernels, slot 2: adjoint kernels.
- * am_profile_read returns accumulated milliseconds and launch counts. */
+ * bracketed by CUDA events on the context stream (recorded asynchronously; the
+ * elapsed times are collected, with one synchronization, by am_profile_read).
+ * Slot 0: element/cell force kernels, 1: node gather + update kernels, 2: VJP
+ * kernels, 3: adjoint node kernels. Milliseconds and launch counts accumulate
+ * until am_profile_enable is called again. */
 int am_profile_enable(am_ctx* ctx, int enable);
-int am_profile_read(am_ctx* ctx, double ms[3], int64_t launches[3]);
+int am_profile_read(am_ctx* ctx, double ms[4], int64_t launches[4]);
 
 #ifdef __cplusplus
 }
