@@ -27,6 +27,7 @@ EXPORTED = [
     "am_internal_force", "am_init_acceleration", "am_run", "am_run_schedule", "am_solve", "am_vjp_force",
     "am_adjoint", "am_stress", "am_quadrature", "am_last_error", "am_status_string", "am_launch_count",
     "am_profile_enable", "am_profile_read", "am_complete_properties", "am_set_block_fields",
+    "am_tet4_internal_force_noalloc",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -104,6 +105,8 @@ def load(build_if_missing: bool = False) -> C.CDLL:
         "am_profile_read": (C.c_int, [vp, _dp, _lp]),
         "am_complete_properties": (C.c_int, [_dp, C.c_char_p, C.c_int]),
         "am_set_block_fields": (C.c_int, [vp, C.c_int32, _dp, _dp]),
+        "am_tet4_internal_force_noalloc": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_int64, C.c_int64, vp, vp,
+                                                    vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -412,6 +412,10 @@ void run_schedule(am_ctx* c, int prec, const std::vector<double>& dts, double t0
 
 }  // namespace
 
+namespace am {
+void set_free_error(const std::string& msg) { g_free_error = msg; }
+}  // namespace am
+
 extern "C" {
 
 const char* am_status_string(int status) {

@@ -155,6 +155,28 @@ int am_stress(int32_t material, double lambda, double mu, int64_t n, am_memory w
 int am_quadrature(int32_t kind, int32_t smoothed, int64_t n, am_memory where, const double* X, double* B,
                   double* w);
 
+/* ---- allocation-free Tet4 internal force (no counterpart in the reference) ----
+ * For callers that cannot allocate device memory, e.g. a host framework that owns
+ * every device allocation through its own pool, or a step that must not pay the
+ * latency and implicit synchronization of cudaMalloc/cudaFree. Computes
+ * f = F(u) (overwritten) for one Tet4 1-point-Gauss part without allocating:
+ * all arguments are device pointers owned by the caller, and the per-element
+ * force slots live in a fixed 16 MiB device array inside this library that every
+ * GPU loading it keeps until process exit. Hence at most AM_NOALLOC_MAX_TETS tets;
+ * larger inputs return AM_ERANGE with the reason in am_last_error(NULL).
+ *   coords, u, f : num_nodes x 3 row-major FP64;  conn : num_elems x 4 (reference node order)
+ *   node_ptr (num_nodes+1) / node_slots (4 num_elems): for each node, the slots
+ *   4e+a (element e, local node a) that touch it, ascending.
+ * The first call on a device looks up the scratch array's device address (so make
+ * that call before any stream capture). All calls share the array: each call
+ * overwrites the slots it reads, so nothing needs clearing, but calls that overlap
+ * on the GPU race on it and must be ordered by the caller. Stream-ordered on
+ * cuda_stream (NULL = legacy default stream); nothing is synchronized. */
+#define AM_NOALLOC_MAX_TETS 174762
+int am_tet4_internal_force_noalloc(int32_t material, double lambda, double mu, int64_t num_nodes, int64_t num_elems,
+                                   const double* coords, const double* u, const int32_t* conn,
+                                   const int32_t* node_ptr, const int32_t* node_slots, double* f, void* cuda_stream);
+
 /* LinearElasticProperties::CompleteProperties (Materials/Base.h:47-158): props =
  * {youngs_modulus, poissons_ratio, shear_modulus, lambda, bulk_modulus} with NaN for
  * the undefined ones; exactly two must be defined. Fills the rest, checks the physical
