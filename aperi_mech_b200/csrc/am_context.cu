@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -63,7 +64,15 @@ struct Block {
     float* grads32 = nullptr;
     double* volumes = nullptr;
     int32_t max_entries = 0;
-    std::vector<int32_t> host_nodes;  // per slot, for the node CSR
+    // Tet4 element patches (see GaussBlockDev)
+    int32_t patched = 0;
+    int64_t num_patches = 0;
+    int32_t* patch_first = nullptr;
+    int32_t* patch_nodes = nullptr;
+    uint32_t* patch_local = nullptr;
+    uint32_t* patch_gather = nullptr;
+    const int32_t* slot_pos = nullptr;  // block-local view into the context's position array
+    std::vector<int32_t> host_nodes;    // node of each logical slot (-1: unused), for the node CSR
 
     am::GaussBlockDev gauss() const {
         am::GaussBlockDev g{};
@@ -75,7 +84,13 @@ struct Block {
         g.conn = conn;
         g.mu_field = mu_field;
         g.kappa_field = kappa_field;
-        g.slot_base = slot_base;
+        g.slot_pos = slot_pos;
+        g.patched = patched;
+        g.num_patches = num_patches;
+        g.patch_first = patch_first;
+        g.patch_nodes = patch_nodes;
+        g.patch_local = patch_local;
+        g.patch_gather = patch_gather;
         return g;
     }
     am::CellBlockDev cells() const {
@@ -91,7 +106,7 @@ struct Block {
         c.volumes = volumes;
         c.mu_field = mu_field;
         c.kappa_field = kappa_field;
-        c.slot_base = slot_base;
+        c.slot_pos = slot_pos;
         c.max_entries = max_entries;
         return c;
     }
@@ -104,8 +119,73 @@ struct Block {
         dfree(grads64);
         dfree(grads32);
         dfree(volumes);
+        dfree(patch_first);
+        dfree(patch_nodes);
+        dfree(patch_local);
+        dfree(patch_gather);
     }
 };
+
+// Greedy element patches: consecutive tets are grouped while the patch has at most
+// 6 tets on at most 8 distinct nodes (the six tets of a split hex form one patch).
+struct TetPatches {
+    std::vector<int32_t> first;   // P + 1
+    std::vector<int32_t> nodes;   // P x 8, unused entries repeat entry 0
+    std::vector<int32_t> used;    // distinct nodes per patch
+    std::vector<uint32_t> local;  // per element: packed local ids
+    std::vector<uint32_t> gather; // P x 8: tets touching each patch node and its slot in each
+};
+
+TetPatches build_tet_patches(const int32_t* conn, int64_t E) {
+    TetPatches tp;
+    tp.local.resize(E);
+    tp.first.push_back(0);
+    int32_t cur[8];
+    int nn = 0, nt = 0;
+    auto close = [&](int64_t next_first) {
+        for (int a = 0; a < 8; ++a) tp.nodes.push_back(a < nn ? cur[a] : cur[0]);
+        tp.used.push_back(nn);
+        tp.first.push_back(static_cast<int32_t>(next_first));
+        nn = 0;
+        nt = 0;
+    };
+    for (int64_t e = 0; e < E; ++e) {
+        const int32_t* c = conn + 4 * e;
+        int fresh = 0;
+        for (int k = 0; k < 4; ++k) {
+            bool seen = false;
+            for (int a = 0; a < nn; ++a) seen |= cur[a] == c[k];
+            for (int j = 0; j < k; ++j) seen |= c[j] == c[k];
+            fresh += !seen;
+        }
+        if (nt > 0 && (nt == 6 || nn + fresh > 8)) close(e);
+        uint32_t packed = 0;
+        for (int k = 0; k < 4; ++k) {
+            int id = -1;
+            for (int a = 0; a < nn; ++a)
+                if (cur[a] == c[k]) id = a;
+            if (id < 0) {
+                id = nn;
+                cur[nn++] = c[k];
+            }
+            packed |= static_cast<uint32_t>(id) << (8 * k);
+        }
+        tp.local[e] = packed;
+        ++nt;
+    }
+    if (nt > 0) close(E);
+    const int64_t P = static_cast<int64_t>(tp.used.size());
+    tp.gather.assign(8 * P, 0u);
+    for (int64_t q = 0; q < P; ++q)
+        for (int32_t e = tp.first[q]; e < tp.first[q + 1]; ++e) {
+            const uint32_t t = static_cast<uint32_t>(e - tp.first[q]);
+            for (int k = 0; k < 4; ++k) {
+                const uint32_t a = (tp.local[e] >> (8 * k)) & 0xFFu;
+                tp.gather[8 * q + a] |= (1u << t) | (static_cast<uint32_t>(k) << (8 + 2 * t));
+            }
+        }
+    return tp;
+}
 
 }  // namespace
 
@@ -127,10 +207,14 @@ struct am_ctx {
     double* f_scratch = nullptr;   // N x 3
     double* io_scratch = nullptr;  // N x 3 host<->device staging
     int32_t* node_ptr = nullptr;
-    int32_t* node_slots = nullptr;
-    double* slots64 = nullptr;
-    float* slots32 = nullptr;
-    int64_t num_slots = 0;
+    int32_t* slot_pos = nullptr;   // logical slot -> node-major position (-1: unused)
+    double4* slots64 = nullptr;    // node-major force slots (FP64 path)
+    float4* slots32 = nullptr;     // node-major force slots (mixed path)
+    int64_t num_slots = 0;         // logical slots
+    int64_t num_used_slots = 0;    // slots referenced by a node
+    std::vector<double4*> adj_bufs;  // cached adjoint checkpoint / segment buffers
+    int64_t adj_key[3] = {0, 0, 0};
+    bool tet4_patches = true;  // APERI_B200_TET4_PATCHES=0 turns element patching off
     am::StepParams* table = nullptr;
     int64_t table_cap = 0;
     am::StepParams* table_host = nullptr;  // pinned staging
@@ -152,7 +236,6 @@ struct am_ctx {
         am::NodeDev nd{};
         nd.num_nodes = N;
         nd.node_ptr = node_ptr;
-        nd.node_slots = node_slots;
         nd.mass = mass;
         nd.bcword = bcword;
         nd.bcvalues = bcvalues;
@@ -171,7 +254,7 @@ struct am_ctx {
 
     void* slots(int mixed) {
         if (mixed) {
-            if (!slots32) slots32 = dalloc<float>(static_cast<size_t>(num_slots) * 3, "slot buffer (FP32)");
+            if (!slots32) slots32 = dalloc<float4>(static_cast<size_t>(num_used_slots), "slot buffer (FP32)");
             return slots32;
         }
         return slots64;
@@ -336,9 +419,11 @@ struct am_ctx {
         dfree(f_scratch);
         dfree(io_scratch);
         dfree(node_ptr);
-        dfree(node_slots);
+        dfree(slot_pos);
         dfree(slots64);
         dfree(slots32);
+        for (auto& pbuf : adj_bufs) dfree(pbuf);
+        adj_bufs.clear();
         dfree(table);
         if (table_host) cudaFreeHost(table_host);
         table_host = nullptr;
@@ -449,6 +534,8 @@ int am_create(int64_t num_nodes, const double* coords, am_ctx** out) {
         ck(cudaGetDevice(&c->device), "cudaGetDevice");
         ck(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream create");
         c->own_stream = true;
+        const char* patches = std::getenv("APERI_B200_TET4_PATCHES");
+        c->tet4_patches = !(patches && patches[0] == '0');
         c->N = num_nodes;
         const size_t N = static_cast<size_t>(num_nodes);
         c->X4 = dalloc<double4>(N, "coordinates");
@@ -579,6 +666,37 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
                     ck(cudaMemcpy(b.conn, d->conn, S * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
                 }
                 b.host_nodes.assign(d->conn, d->conn + S);
+                if (d->kind == AM_TET4_GAUSS && E > 0 && ctx->tet4_patches) {
+                    // Patch the tets when patches hold 2.5 tets or more on average; fewer
+                    // would leave most of the eight lanes per patch idle.
+                    TetPatches tp = build_tet_patches(d->conn, E);
+                    const int64_t P = static_cast<int64_t>(tp.used.size());
+                    if (static_cast<double>(E) >= 2.5 * static_cast<double>(P)) {
+                        // Split-hex patches (six tets in the canonical local order) get the
+                        // register-resident kernel; any other patching the generic one.
+                        static const uint32_t kHex6[6] = {0x03020100u, 0x03040200u, 0x03050400u,
+                                                          0x03060500u, 0x03070600u, 0x03010700u};
+                        bool hex6 = true;
+                        for (int64_t q = 0; q < P && hex6; ++q) {
+                            hex6 = (tp.first[q + 1] - tp.first[q] == 6) && tp.used[q] == 8;
+                            for (int t = 0; t < 6 && hex6; ++t) hex6 = tp.local[tp.first[q] + t] == kHex6[t];
+                        }
+                        b.patched = hex6 ? 2 : 1;
+                        b.num_patches = P;
+                        b.num_entries = 8 * P;
+                        b.patch_first = dalloc<int32_t>(P + 1, "patch offsets");
+                        b.patch_nodes = dalloc<int32_t>(8 * P, "patch nodes");
+                        b.patch_local = dalloc<uint32_t>(E, "patch local ids");
+                        b.patch_gather = dalloc<uint32_t>(8 * P, "patch gather masks");
+                        ck(cudaMemcpy(b.patch_gather, tp.gather.data(), 8 * P * sizeof(uint32_t), cudaMemcpyHostToDevice), "upload");
+                        ck(cudaMemcpy(b.patch_first, tp.first.data(), (P + 1) * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+                        ck(cudaMemcpy(b.patch_nodes, tp.nodes.data(), 8 * P * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+                        ck(cudaMemcpy(b.patch_local, tp.local.data(), E * sizeof(uint32_t), cudaMemcpyHostToDevice), "upload");
+                        b.host_nodes.assign(8 * P, -1);
+                        for (int64_t q = 0; q < P; ++q)
+                            for (int a = 0; a < tp.used[q]; ++a) b.host_nodes[8 * q + a] = tp.nodes[8 * q + a];
+                    }
+                }
             }
             if (ctx->num_slots + b.num_entries >= (int64_t(1) << 31)) fail(AM_ERANGE, "slot count beyond int32 indexing");
             if (d->mu_field && E > 0) {
@@ -689,23 +807,29 @@ int am_finalize(am_ctx* ctx) {
         if (ctx->finalized) fail(AM_ESTATE, "am_finalize called twice");
         if (ctx->blocks.empty()) fail(AM_EINVAL, "no blocks");
         const int64_t N = ctx->N, S = ctx->num_slots;
-        // Node -> slot CSR, slots ascending within each node (block order, then element order).
-        std::vector<int32_t> ptr(N + 1, 0), slots(S);
+        // Node-major slot layout: node i owns positions [ptr[i], ptr[i+1]); within a node
+        // the positions follow ascending logical slot (block order, then element order).
+        std::vector<int32_t> ptr(N + 1, 0), pos(S, -1);
         for (const auto& b : ctx->blocks)
-            for (int32_t n : b.host_nodes) ++ptr[n + 1];
+            for (int32_t n : b.host_nodes)
+                if (n >= 0) ++ptr[n + 1];
         for (int64_t i = 0; i < N; ++i) ptr[i + 1] += ptr[i];
         std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
         for (const auto& b : ctx->blocks)
             for (int64_t k = 0; k < static_cast<int64_t>(b.host_nodes.size()); ++k)
-                slots[fill[b.host_nodes[k]]++] = static_cast<int32_t>(b.slot_base + k);
+                if (b.host_nodes[k] >= 0) pos[b.slot_base + k] = fill[b.host_nodes[k]]++;
+        ctx->num_used_slots = ptr[N];
         ctx->node_ptr = dalloc<int32_t>(N + 1, "node ptr");
         ck(cudaMemcpy(ctx->node_ptr, ptr.data(), (N + 1) * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
         if (S > 0) {
-            ctx->node_slots = dalloc<int32_t>(S, "node slots");
-            ck(cudaMemcpy(ctx->node_slots, slots.data(), S * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
-            ctx->slots64 = dalloc<double>(static_cast<size_t>(S) * 3, "slot buffer");
+            ctx->slot_pos = dalloc<int32_t>(S, "slot positions");
+            ck(cudaMemcpy(ctx->slot_pos, pos.data(), S * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+            ctx->slots64 = dalloc<double4>(static_cast<size_t>(std::max<int64_t>(ctx->num_used_slots, 1)), "slot buffer");
         }
-        for (auto& b : ctx->blocks) std::vector<int32_t>().swap(b.host_nodes);
+        for (auto& b : ctx->blocks) {
+            b.slot_pos = ctx->slot_pos + b.slot_base;
+            std::vector<int32_t>().swap(b.host_nodes);
+        }
         bool has_cells = false;
         for (const auto& b : ctx->blocks) has_cells |= b.kind == AM_SMOOTHED_CELLS;
         if (!ctx->mass_set) {
@@ -858,17 +982,6 @@ int am_vjp_force(am_ctx* ctx, am_memory where, const double* u, const double* la
 int am_adjoint(am_ctx* ctx, int64_t nsteps, double dt, int32_t ckpt_every, int32_t num_sensors, const int32_t* sensors,
                double* loss, double* gmu, double* gkappa) {
     if (!ctx) return AM_EINVAL;
-    struct Bufs {
-        std::vector<double4*> ptrs;
-        ~Bufs() {
-            for (auto p : ptrs)
-                if (p) cudaFree(p);
-        }
-        double4* get(size_t n) {
-            ptrs.push_back(dalloc<double4>(n, "adjoint buffer"));
-            return ptrs.back();
-        }
-    } bufs;
     return guarded(ctx, [&] {
         ctx->require_finalized();
         if (nsteps <= 0 || !(dt > 0.0)) fail(AM_EINVAL, "nsteps and dt must be positive");
@@ -879,30 +992,47 @@ int am_adjoint(am_ctx* ctx, int64_t nsteps, double dt, int32_t ckpt_every, int32
         const size_t N = static_cast<size_t>(ctx->N);
         const int64_t E = ctx->total_elems();
         const int64_t nseg = (nsteps + ckpt_every - 1) / ckpt_every;
+        // Buffers (nodal double4 vectors) are cached on the context and reused while the
+        // checkpoint layout and the sizes stay the same.
+        const int64_t n_vec = 3 * nseg + ckpt_every + 6;
+        const int64_t n_aux = 2 * ((E + 3) / 4) + (num_sensors + 7) / 8 + 2;
+        if (ctx->adj_key[0] != n_vec || ctx->adj_key[1] != n_aux || ctx->adj_key[2] != ctx->N) {
+            ck(cudaStreamSynchronize(ctx->stream), "synchronize");
+            for (auto& pbuf : ctx->adj_bufs) dfree(pbuf);
+            ctx->adj_bufs.clear();
+            ctx->adj_key[0] = ctx->adj_key[1] = ctx->adj_key[2] = 0;
+            for (int64_t k = 0; k < n_vec; ++k) ctx->adj_bufs.push_back(dalloc<double4>(N, "adjoint buffer"));
+            ctx->adj_bufs.push_back(dalloc<double4>(n_aux, "adjoint buffer"));
+            ctx->adj_key[0] = n_vec;
+            ctx->adj_key[1] = n_aux;
+            ctx->adj_key[2] = ctx->N;
+        }
+        std::vector<double4*>& B = ctx->adj_bufs;
         std::vector<double4*> ck_u(nseg), ck_v(nseg), ck_a(nseg), seg(ckpt_every);
         for (int64_t s = 0; s < nseg; ++s) {
-            ck_u[s] = bufs.get(N);
-            ck_v[s] = bufs.get(N);
-            ck_a[s] = bufs.get(N);
+            ck_u[s] = B[3 * s];
+            ck_v[s] = B[3 * s + 1];
+            ck_a[s] = B[3 * s + 2];
         }
-        for (int32_t k = 0; k < ckpt_every; ++k) seg[k] = bufs.get(N);
-        double4* UB = bufs.get(N);
-        double4* VB = bufs.get(N);
-        double4* AB = bufs.get(N);
-        double4* fin_u = bufs.get(N);
-        double4* fin_v = bufs.get(N);
-        double4* fin_a = bufs.get(N);
-        double* gm = reinterpret_cast<double*>(bufs.get((E + 3) / 4));
-        double* gk = reinterpret_cast<double*>(bufs.get((E + 3) / 4));
-        int32_t* dsens = reinterpret_cast<int32_t*>(bufs.get((num_sensors + 7) / 8 + 1));
-        double* dloss = reinterpret_cast<double*>(bufs.get(1));
+        for (int32_t k = 0; k < ckpt_every; ++k) seg[k] = B[3 * nseg + k];
+        double4* UB = B[3 * nseg + ckpt_every + 0];
+        double4* VB = B[3 * nseg + ckpt_every + 1];
+        double4* AB = B[3 * nseg + ckpt_every + 2];
+        double4* fin_u = B[3 * nseg + ckpt_every + 3];
+        double4* fin_v = B[3 * nseg + ckpt_every + 4];
+        double4* fin_a = B[3 * nseg + ckpt_every + 5];
+        double* gm = reinterpret_cast<double*>(B[n_vec]);
+        double* gk = gm + 4 * ((E + 3) / 4);
+        int32_t* dsens = reinterpret_cast<int32_t*>(gk + 4 * ((E + 3) / 4));
+        double* dloss = reinterpret_cast<double*>(B[n_vec] + (n_aux - 1));
         cudaStream_t st = ctx->stream;
         const size_t bytes = N * sizeof(double4);
         ck(cudaMemsetAsync(gm, 0, E * sizeof(double), st), "memset");
         ck(cudaMemsetAsync(gk, 0, E * sizeof(double), st), "memset");
         if (num_sensors > 0)
             ck(cudaMemcpyAsync(dsens, sensors, num_sensors * sizeof(int32_t), cudaMemcpyHostToDevice, st), "H2D");
-        // Forward pass (FP64) with checkpoints of (u, v, a) at the start of each segment.
+        // Forward pass (FP64) with checkpoints of (u, v, a) at the start of each segment;
+        // the last segment records its displacements directly, so it needs no recompute.
         ctx->reset_status();
         ctx->init_acceleration(0);
         ctx->upload_table(std::vector<double>(static_cast<size_t>(nsteps), dt), 0.0);
@@ -910,7 +1040,8 @@ int am_adjoint(am_ctx* ctx, int64_t nsteps, double dt, int32_t ckpt_every, int32
             ck(cudaMemcpyAsync(ck_u[s], ctx->U4, bytes, cudaMemcpyDeviceToDevice, st), "checkpoint");
             ck(cudaMemcpyAsync(ck_v[s], ctx->V4, bytes, cudaMemcpyDeviceToDevice, st), "checkpoint");
             ck(cudaMemcpyAsync(ck_a[s], ctx->A4, bytes, cudaMemcpyDeviceToDevice, st), "checkpoint");
-            ctx->run_range(0, s * ckpt_every, std::min<int64_t>(nsteps, (s + 1) * ckpt_every), nullptr);
+            ctx->run_range(0, s * ckpt_every, std::min<int64_t>(nsteps, (s + 1) * ckpt_every),
+                           s == nseg - 1 ? seg.data() : nullptr);
         }
         ctx->check_status();
         ck(cudaMemcpyAsync(fin_u, ctx->U4, bytes, cudaMemcpyDeviceToDevice, st), "save");
@@ -929,10 +1060,12 @@ int am_adjoint(am_ctx* ctx, int64_t nsteps, double dt, int32_t ckpt_every, int32
         // from its checkpoint, then transpose its steps in reverse order.
         for (int64_t s = nseg - 1; s >= 0; --s) {
             const int64_t n0 = s * ckpt_every, n1 = std::min<int64_t>(nsteps, (s + 1) * ckpt_every);
-            ck(cudaMemcpyAsync(ctx->U4, ck_u[s], bytes, cudaMemcpyDeviceToDevice, st), "restore");
-            ck(cudaMemcpyAsync(ctx->V4, ck_v[s], bytes, cudaMemcpyDeviceToDevice, st), "restore");
-            ck(cudaMemcpyAsync(ctx->A4, ck_a[s], bytes, cudaMemcpyDeviceToDevice, st), "restore");
-            ctx->run_range(0, n0, n1, seg.data());
+            if (s != nseg - 1) {
+                ck(cudaMemcpyAsync(ctx->U4, ck_u[s], bytes, cudaMemcpyDeviceToDevice, st), "restore");
+                ck(cudaMemcpyAsync(ctx->V4, ck_v[s], bytes, cudaMemcpyDeviceToDevice, st), "restore");
+                ck(cudaMemcpyAsync(ctx->A4, ck_a[s], bytes, cudaMemcpyDeviceToDevice, st), "restore");
+                ctx->run_range(0, n0, n1, seg.data());
+            }
             ctx->mark(-1, 0);
             for (int64_t n = n1 - 1; n >= n0; --n) {
                 ctx->vjp(seg[n - n0], ctx->L4, gm, gk, 1);

@@ -28,6 +28,22 @@ __device__ __forceinline__ void flag(int* status, int code, int64_t idx) {
     if (atomicCAS(status + kStatusCode, 0, code) == 0) status[kStatusIndex] = static_cast<int>(idx);
 }
 
+template <typename T>
+struct Vec4Of;
+template <>
+struct Vec4Of<float> {
+    using type = float4;
+};
+template <>
+struct Vec4Of<double> {
+    using type = double4;
+};
+template <typename T>
+using vec4_t = typename Vec4Of<T>::type;
+
+__device__ __forceinline__ float4 make4(float x, float y, float z) { return make_float4(x, y, z, 0.f); }
+__device__ __forceinline__ double4 make4(double x, double y, double z) { return make_double4(x, y, z, 0.0); }
+
 template <typename F>
 __device__ __forceinline__ void element_lame(const F& b, int64_t e, double& lambda, double& mu) {
     if (b.mu_field != nullptr || b.kappa_field != nullptr) {
@@ -57,58 +73,235 @@ __host__ __device__ constexpr int hex_sign_c(int a, int j) {
 // ---------------------------------------------------------------------------
 // Tet4, 1-point Gauss: one thread per element.
 // ---------------------------------------------------------------------------
+// Forces of one tet from its node differences relative to node l0: columns of J
+// and D are X_l - X_l0 and u_l - u_l0 for l = l1, l2, l3. Writes f[12] (4 nodes x 3)
+// and returns det J.
+template <typename T, int MAT>
+__device__ __forceinline__ T tet4_forces(const T* J, const T* D, double lam, double mu, T* f, int64_t e, int* status) {
+    const T det = det3(J);
+    if (!(det > T(0))) flag(status, AM_ENONPOS_J, e);
+    T Ji[9];
+    cof_inv3(J, Ji, det);
+    const T w = det / T(6);
+    // H = u^T B = D J^-1
+    T H[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) H[i * 3 + j] = D[i * 3 + 0] * Ji[0 * 3 + j] + D[i * 3 + 1] * Ji[1 * 3 + j] + D[i * 3 + 2] * Ji[2 * 3 + j];
+    T P[9];
+    const double Jf = stress<T>(MAT, T(lam), T(mu), H, P);
+    if (MAT == kNeoHookean && !(Jf > 0.0)) flag(status, AM_ENONPOS_J, e);
+    // Q = w J^-1 P^T ; f_{k+1} = -Q_k ; f_0 = Q_0 + Q_1 + Q_2
+#pragma unroll
+    for (int i = 0; i < 3; ++i) f[i] = T(0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const T q = w * (Ji[k * 3 + 0] * P[i * 3 + 0] + Ji[k * 3 + 1] * P[i * 3 + 1] + Ji[k * 3 + 2] * P[i * 3 + 2]);
+            f[(k + 1) * 3 + i] = -q;
+            f[i] += q;
+        }
+    return det;
+}
+
 template <typename T, int MAT>
 __global__ void __launch_bounds__(256) k_tet4_force(GaussBlockDev b, const double4* __restrict__ X4,
-                                                     const double4* __restrict__ U4, T* __restrict__ slots,
+                                                     const double4* __restrict__ U4, vec4_t<T>* __restrict__ slots,
                                                      int* status) {
-    __shared__ T stage[256 * 12];
     const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= b.num_elems) return;
+    const int4 c = reinterpret_cast<const int4*>(b.conn)[e];
+    const double4 x0 = X4[c.x], x1 = X4[c.y], x2 = X4[c.z], x3 = X4[c.w];
+    const double4 u0 = U4[c.x], u1 = U4[c.y], u2 = U4[c.z], u3 = U4[c.w];
+    // J = X^T dN with dN rows (-1,-1,-1), e1, e2, e3: column j of J is X_{j+1} - X_0.
+    const T J[9] = {T(x1.x - x0.x), T(x2.x - x0.x), T(x3.x - x0.x), T(x1.y - x0.y), T(x2.y - x0.y),
+                    T(x3.y - x0.y), T(x1.z - x0.z), T(x2.z - x0.z), T(x3.z - x0.z)};
+    const T D[9] = {T(u1.x - u0.x), T(u2.x - u0.x), T(u3.x - u0.x), T(u1.y - u0.y), T(u2.y - u0.y),
+                    T(u3.y - u0.y), T(u1.z - u0.z), T(u2.z - u0.z), T(u3.z - u0.z)};
+    double lam, mu;
+    element_lame(b, e, lam, mu);
     T f[12];
-#pragma unroll
-    for (int k = 0; k < 12; ++k) f[k] = T(0);
-    if (e < b.num_elems) {
-        const int4 c = reinterpret_cast<const int4*>(b.conn)[e];
-        const double4 x0 = X4[c.x], x1 = X4[c.y], x2 = X4[c.z], x3 = X4[c.w];
-        const double4 u0 = U4[c.x], u1 = U4[c.y], u2 = U4[c.z], u3 = U4[c.w];
-        // J = X^T dN with dN rows (-1,-1,-1), e1, e2, e3: column j of J is X_{j+1} - X_0.
-        const T J[9] = {T(x1.x - x0.x), T(x2.x - x0.x), T(x3.x - x0.x), T(x1.y - x0.y), T(x2.y - x0.y),
-                        T(x3.y - x0.y), T(x1.z - x0.z), T(x2.z - x0.z), T(x3.z - x0.z)};
-        const T D[9] = {T(u1.x - u0.x), T(u2.x - u0.x), T(u3.x - u0.x), T(u1.y - u0.y), T(u2.y - u0.y),
-                        T(u3.y - u0.y), T(u1.z - u0.z), T(u2.z - u0.z), T(u3.z - u0.z)};
-        const T det = det3(J);
-        if (!(det > T(0))) flag(status, AM_ENONPOS_J, e);
-        T Ji[9];
-        cof_inv3(J, Ji, det);
-        const T w = det / T(6);
-        // H = u^T B = D J^-1
-        T H[9];
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) H[i * 3 + j] = D[i * 3 + 0] * Ji[0 * 3 + j] + D[i * 3 + 1] * Ji[1 * 3 + j] + D[i * 3 + 2] * Ji[2 * 3 + j];
-        double lam, mu;
-        element_lame(b, e, lam, mu);
-        T P[9];
-        const double Jf = stress<T>(MAT, T(lam), T(mu), H, P);
-        if (MAT == kNeoHookean && !(Jf > 0.0)) flag(status, AM_ENONPOS_J, e);
-        // Q = w J^-1 P^T ; f_{k+1} = -Q_k ; f_0 = Q_0 + Q_1 + Q_2
-#pragma unroll
-        for (int k = 0; k < 3; ++k)
+    tet4_forces<T, MAT>(J, D, lam, mu, f, e, status);
+    const int4 pos = make_int4(b.slot_pos[4 * e], b.slot_pos[4 * e + 1], b.slot_pos[4 * e + 2], b.slot_pos[4 * e + 3]);
+    slots[pos.x] = make4(f[0], f[1], f[2]);
+    slots[pos.y] = make4(f[3], f[4], f[5]);
+    slots[pos.z] = make4(f[6], f[7], f[8]);
+    slots[pos.w] = make4(f[9], f[10], f[11]);
+}
+
+// ---------------------------------------------------------------------------
+// Tet4 element patches (at most 6 tets on at most 8 nodes, e.g. the six tets of a
+// split hex): one warp serves 5 patches. The warp first loads the 40 patch nodes
+// into shared memory (FP64), then lane 6q+t computes tet t of patch q (30 busy
+// lanes), then the 40 (patch, node) pairs sum, in tet order, the contributions of
+// the patch's tets to their node and write one slot each.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int local_id(uint32_t packed, int k) { return (packed >> (8 * k)) & 0xFF; }
+
+constexpr int kPatchesPerWarp = 5;
+constexpr int kPatchTets = 6;
+
+template <typename T, int MAT>
+__global__ void __launch_bounds__(256) k_tet4_patch_force(GaussBlockDev b, const double4* __restrict__ X4,
+                                                           const double4* __restrict__ U4,
+                                                           vec4_t<T>* __restrict__ slots, int* status) {
+    __shared__ double nodes[8][kPatchesPerWarp * 8][6];                  // X, u of the warp's patch nodes
+    __shared__ T contrib[8][kPatchesPerWarp * kPatchTets][12];          // per tet: 4 nodes x 3
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    const int64_t p0 = (static_cast<int64_t>(blockIdx.x) * 8 + w) * kPatchesPerWarp;
+    for (int q = lane; q < kPatchesPerWarp * 8; q += 32) {
+        const int64_t p = p0 + q / 8;
+        const int32_t n = p < b.num_patches ? b.patch_nodes[p * 8 + (q & 7)] : 0;
+        const double4 x = X4[n], u = U4[n];
+        double* d = nodes[w][q];
+        d[0] = x.x;
+        d[1] = x.y;
+        d[2] = x.z;
+        d[3] = u.x;
+        d[4] = u.y;
+        d[5] = u.z;
+    }
+    __syncwarp();
+    const int pq = lane / kPatchTets, t = lane % kPatchTets;
+    const int64_t p = p0 + pq;
+    if (pq < kPatchesPerWarp && p < b.num_patches) {
+        const int32_t e0 = b.patch_first[p];
+        if (t < b.patch_first[p + 1] - e0) {
+            const int64_t e = e0 + t;
+            const uint32_t loc = b.patch_local[e];
+            const double* n0 = nodes[w][pq * 8 + local_id(loc, 0)];
+            const double* n1 = nodes[w][pq * 8 + local_id(loc, 1)];
+            const double* n2 = nodes[w][pq * 8 + local_id(loc, 2)];
+            const double* n3 = nodes[w][pq * 8 + local_id(loc, 3)];
+            T J[9], D[9];
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
-                const T q = w * (Ji[k * 3 + 0] * P[i * 3 + 0] + Ji[k * 3 + 1] * P[i * 3 + 1] + Ji[k * 3 + 2] * P[i * 3 + 2]);
-                f[(k + 1) * 3 + i] = -q;
-                f[i] += q;
+                J[i * 3 + 0] = T(n1[i] - n0[i]);
+                J[i * 3 + 1] = T(n2[i] - n0[i]);
+                J[i * 3 + 2] = T(n3[i] - n0[i]);
+                D[i * 3 + 0] = T(n1[3 + i] - n0[3 + i]);
+                D[i * 3 + 1] = T(n2[3 + i] - n0[3 + i]);
+                D[i * 3 + 2] = T(n3[3 + i] - n0[3 + i]);
             }
-    }
-    // Stage through shared memory so the block's slots go out as one coalesced run.
+            double lam, mu;
+            element_lame(b, e, lam, mu);
+            T f[12];
+            tet4_forces<T, MAT>(J, D, lam, mu, f, e, status);
+            T* c = contrib[w][lane];
 #pragma unroll
-    for (int k = 0; k < 12; ++k) stage[threadIdx.x * 12 + k] = f[k];
-    __syncthreads();
-    const int64_t first = static_cast<int64_t>(blockIdx.x) * blockDim.x;
-    const int64_t count = min(static_cast<int64_t>(blockDim.x), b.num_elems - first) * 12;
-    T* out = slots + (b.slot_base + first * 4) * 3;
-    for (int k = threadIdx.x; k < count; k += blockDim.x) out[k] = stage[k];
+            for (int k = 0; k < 12; ++k) c[k] = f[k];
+        }
+    }
+    __syncwarp();
+    for (int q = lane; q < kPatchesPerWarp * 8; q += 32) {
+        const int64_t pp = p0 + q / 8;
+        if (pp >= b.num_patches) continue;
+        const int32_t pos = b.slot_pos[pp * 8 + (q & 7)];
+        if (pos < 0) continue;
+        const uint32_t gm = b.patch_gather[pp * 8 + (q & 7)];
+        T fx = T(0), fy = T(0), fz = T(0);
+        for (uint32_t m = gm & 0xFFu; m; m &= m - 1) {  // tets touching the node, ascending
+            const int tt = __ffs(m) - 1;
+            const T* c = contrib[w][(q / 8) * kPatchTets + tt] + ((gm >> (8 + 2 * tt)) & 3u) * 3;
+            fx += c[0];
+            fy += c[1];
+            fz += c[2];
+        }
+        slots[pos] = make4(fx, fy, fz);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Tet4 patches that are split hexes (the six tets around the 0-6 diagonal, in the
+// patch-local node order the patch builder produces): the local connectivity is a
+// compile-time table, so each thread keeps its patch's 8 nodes and force sums in
+// registers. TPH threads share one patch (6/TPH tets each) and combine their sums
+// with one butterfly step; no shared memory, no divergence.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int hex6_local(int t, int k) {
+    // patch-local ids of tet t's 4 nodes: (0, a_t, b_t, 3), a = 1,2,4,5,6,7 ; b = 2,4,5,6,7,1
+    return k == 0 ? 0 : k == 3 ? 3 : k == 1 ? (t == 0 ? 1 : t == 1 ? 2 : t + 2) : (t == 0 ? 2 : t == 5 ? 1 : t + 3);
+}
+
+template <typename T, int MAT, int TPH>
+__global__ void __launch_bounds__(256) k_tet4_hex6_force(GaussBlockDev b, const double4* __restrict__ X4,
+                                                          const double4* __restrict__ U4,
+                                                          vec4_t<T>* __restrict__ slots, int* status) {
+    const int64_t gt = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t p = gt / TPH;
+    const int r = static_cast<int>(gt % TPH);
+    const bool valid = p < b.num_patches;
+    const int64_t pp = valid ? p : 0;
+    // Node data relative to patch node 0: X in FP64 then T, u likewise.
+    const int32_t n0 = b.patch_nodes[pp * 8];
+    const double4 x0 = X4[n0], u0 = U4[n0];
+    T dx[8][3], du[8][3];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        if (a == 0) {
+            dx[0][0] = dx[0][1] = dx[0][2] = du[0][0] = du[0][1] = du[0][2] = T(0);
+            continue;
+        }
+        const int32_t n = b.patch_nodes[pp * 8 + a];
+        const double4 x = X4[n], u = U4[n];
+        dx[a][0] = T(x.x - x0.x);
+        dx[a][1] = T(x.y - x0.y);
+        dx[a][2] = T(x.z - x0.z);
+        du[a][0] = T(u.x - u0.x);
+        du[a][1] = T(u.y - u0.y);
+        du[a][2] = T(u.z - u0.z);
+    }
+    T acc[8][3];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) acc[a][0] = acc[a][1] = acc[a][2] = T(0);
+    const int64_t e0 = static_cast<int64_t>(b.patch_first[pp]);
+#pragma unroll
+    for (int tt = 0; tt < 6 / TPH; ++tt) {
+        const int t = r * (6 / TPH) + tt;
+#pragma unroll
+        for (int tc = 0; tc < 6; ++tc) {
+            if (tc != t) continue;  // compile-time local connectivity for the selected tet
+            const int l0 = hex6_local(tc, 0), l1 = hex6_local(tc, 1), l2 = hex6_local(tc, 2), l3 = hex6_local(tc, 3);
+            T J[9], D[9];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                J[i * 3 + 0] = dx[l1][i] - dx[l0][i];
+                J[i * 3 + 1] = dx[l2][i] - dx[l0][i];
+                J[i * 3 + 2] = dx[l3][i] - dx[l0][i];
+                D[i * 3 + 0] = du[l1][i] - du[l0][i];
+                D[i * 3 + 1] = du[l2][i] - du[l0][i];
+                D[i * 3 + 2] = du[l3][i] - du[l0][i];
+            }
+            const int64_t e = e0 + tc;
+            double lam, mu;
+            element_lame(b, e, lam, mu);
+            T f[12];
+            tet4_forces<T, MAT>(J, D, lam, mu, f, valid ? e : 0, valid ? status : nullptr);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                acc[l0][i] += f[i];
+                acc[l1][i] += f[3 + i];
+                acc[l2][i] += f[6 + i];
+                acc[l3][i] += f[9 + i];
+            }
+        }
+    }
+    if (TPH > 1) {
+#pragma unroll
+        for (int a = 0; a < 8; ++a)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) acc[a][i] += __shfl_xor_sync(kFull, acc[a][i], 1);
+    }
+    if (!valid) return;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        if (a % TPH != r) continue;
+        const int32_t pos = b.slot_pos[p * 8 + a];
+        if (pos >= 0) slots[pos] = make4(acc[a][0], acc[a][1], acc[a][2]);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -119,7 +312,7 @@ __global__ void __launch_bounds__(256) k_tet4_force(GaussBlockDev b, const doubl
 // ---------------------------------------------------------------------------
 template <typename T, int MAT>
 __global__ void __launch_bounds__(256) k_hex8_force(GaussBlockDev b, const double4* __restrict__ X4,
-                                                     const double4* __restrict__ U4, T* __restrict__ slots,
+                                                     const double4* __restrict__ U4, vec4_t<T>* __restrict__ slots,
                                                      int* status) {
     __shared__ T sh[32][120];
     const int lane = threadIdx.x & 31;
@@ -208,12 +401,7 @@ __global__ void __launch_bounds__(256) k_hex8_force(GaussBlockDev b, const doubl
         fy -= d0 * Q[1] + d1 * Q[4] + d2 * Q[7];
         fz -= d0 * Q[2] + d1 * Q[5] + d2 * Q[8];
     }
-    if (valid) {
-        T* out = slots + (b.slot_base + e * 8 + g) * 3;
-        out[0] = fx;
-        out[1] = fy;
-        out[2] = fz;
-    }
+    if (valid) slots[b.slot_pos[e * 8 + g]] = make4(fx, fy, fz);
 }
 
 // ---------------------------------------------------------------------------
@@ -231,7 +419,7 @@ __device__ __forceinline__ const float* cell_grads<float>(const CellBlockDev& b)
 
 template <typename T, int MAT>
 __global__ void __launch_bounds__(256) k_cell_force_thread(CellBlockDev b, const double4* __restrict__ U4,
-                                                            T* __restrict__ slots, int* status) {
+                                                            vec4_t<T>* __restrict__ slots, int* status) {
     const int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (c >= b.num_cells) return;
     const int32_t s0 = b.ptr[c], s1 = b.ptr[c + 1];
@@ -257,17 +445,18 @@ __global__ void __launch_bounds__(256) k_cell_force_thread(CellBlockDev b, const
     const double Jf = stress<T>(MAT, T(lam), T(mu), H, P);
     if (MAT == kNeoHookean && !(Jf > 0.0)) flag(status, AM_ENONPOS_J, c);
     const T V = T(b.volumes[c]);
-    T* out = slots + b.slot_base * 3;
     for (int32_t s = s0; s < s1; ++s) {
         const T gg[3] = {gr[3 * s], gr[3 * s + 1], gr[3 * s + 2]};
+        T f[3];
 #pragma unroll
-        for (int i = 0; i < 3; ++i) out[3 * s + i] = (gg[0] * P[i * 3 + 0] + gg[1] * P[i * 3 + 1] + gg[2] * P[i * 3 + 2]) * -V;
+        for (int i = 0; i < 3; ++i) f[i] = (gg[0] * P[i * 3 + 0] + gg[1] * P[i * 3 + 1] + gg[2] * P[i * 3 + 2]) * -V;
+        slots[b.slot_pos[s]] = make4(f[0], f[1], f[2]);
     }
 }
 
 template <typename T, int MAT>
 __global__ void __launch_bounds__(256) k_cell_force_warp(CellBlockDev b, const double4* __restrict__ U4,
-                                                          T* __restrict__ slots, int* status) {
+                                                          vec4_t<T>* __restrict__ slots, int* status) {
     const int lane = threadIdx.x & 31;
     const int64_t c = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     if (c >= b.num_cells) return;  // whole warp exits together
@@ -299,11 +488,12 @@ __global__ void __launch_bounds__(256) k_cell_force_warp(CellBlockDev b, const d
     const double Jf = stress<T>(MAT, T(lam), T(mu), H, P);
     if (lane == 0 && MAT == kNeoHookean && !(Jf > 0.0)) flag(status, AM_ENONPOS_J, c);
     const T V = T(b.volumes[c]);
-    T* out = slots + b.slot_base * 3;
     for (int32_t s = s0 + lane; s < s1; s += 32) {
         const T gg[3] = {gr[3 * s], gr[3 * s + 1], gr[3 * s + 2]};
+        T f[3];
 #pragma unroll
-        for (int i = 0; i < 3; ++i) out[3 * s + i] = (gg[0] * P[i * 3 + 0] + gg[1] * P[i * 3 + 1] + gg[2] * P[i * 3 + 2]) * -V;
+        for (int i = 0; i < 3; ++i) f[i] = (gg[0] * P[i * 3 + 0] + gg[1] * P[i * 3 + 1] + gg[2] * P[i * 3 + 2]) * -V;
+        slots[b.slot_pos[s]] = make4(f[0], f[1], f[2]);
     }
 }
 
@@ -318,10 +508,43 @@ __device__ __forceinline__ void store_theta(double* gmu, double* gk, int64_t e, 
     if (gk) gk[e] = accumulate ? gk[e] + w_ldlam : w_ldlam;
 }
 
+// VJP of one tet: J, D, DL hold X, u and lam differences (columns l1-l0, l2-l0,
+// l3-l0). Writes g[12] and the element's (dF/dmu)^T lam, (dF/dkappa)^T lam.
+template <int MAT>
+__device__ __forceinline__ void tet4_vjp(const double* J, const double* D, const double* DL, double lam, double mu,
+                                         double* g, double& tm, double& tk) {
+    const double det = det3(J);
+    double Ji[9];
+    cof_inv3(J, Ji, det);
+    const double w = det / 6.0;
+    double H[9], L[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            H[i * 3 + j] = D[i * 3 + 0] * Ji[0 * 3 + j] + D[i * 3 + 1] * Ji[1 * 3 + j] + D[i * 3 + 2] * Ji[2 * 3 + j];
+            L[i * 3 + j] = DL[i * 3 + 0] * Ji[0 * 3 + j] + DL[i * 3 + 1] * Ji[1 * 3 + j] + DL[i * 3 + 2] * Ji[2 * 3 + j];
+        }
+    double dP[9], ldl, ldm;
+    stress_vjp(MAT, lam, mu, H, L, dP, &ldl, &ldm);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) g[i] = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const double q = w * (Ji[k * 3 + 0] * dP[i * 3 + 0] + Ji[k * 3 + 1] * dP[i * 3 + 1] + Ji[k * 3 + 2] * dP[i * 3 + 2]);
+            g[(k + 1) * 3 + i] = -q;
+            g[i] += q;
+        }
+    tm = -w * (ldm - 2.0 / 3.0 * ldl);
+    tk = -w * ldl;
+}
+
 template <int MAT>
 __global__ void __launch_bounds__(256) k_tet4_vjp(GaussBlockDev b, const double4* __restrict__ X4,
                                                    const double4* __restrict__ U4, const double4* __restrict__ L4,
-                                                   double* __restrict__ slots, double* gmu, double* gk,
+                                                   double4* __restrict__ slots, double* gmu, double* gk,
                                                    int accumulate) {
     const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (e >= b.num_elems) return;
@@ -335,47 +558,99 @@ __global__ void __launch_bounds__(256) k_tet4_vjp(GaussBlockDev b, const double4
                          u3.y - u0.y, u1.z - u0.z, u2.z - u0.z, u3.z - u0.z};
     const double DL[9] = {l1.x - l0.x, l2.x - l0.x, l3.x - l0.x, l1.y - l0.y, l2.y - l0.y,
                           l3.y - l0.y, l1.z - l0.z, l2.z - l0.z, l3.z - l0.z};
-    const double det = det3(J);
-    double Ji[9];
-    cof_inv3(J, Ji, det);
-    const double w = det / 6.0;
-    double H[9], L[9];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            H[i * 3 + j] = D[i * 3 + 0] * Ji[0 * 3 + j] + D[i * 3 + 1] * Ji[1 * 3 + j] + D[i * 3 + 2] * Ji[2 * 3 + j];
-            L[i * 3 + j] = DL[i * 3 + 0] * Ji[0 * 3 + j] + DL[i * 3 + 1] * Ji[1 * 3 + j] + DL[i * 3 + 2] * Ji[2 * 3 + j];
-        }
     double lam, mu;
     element_lame(b, e, lam, mu);
-    double dP[9], ldl, ldm;
-    stress_vjp(MAT, lam, mu, H, L, dP, &ldl, &ldm);
-    double f[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll
-    for (int k = 0; k < 3; ++k)
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            const double q = w * (Ji[k * 3 + 0] * dP[i * 3 + 0] + Ji[k * 3 + 1] * dP[i * 3 + 1] + Ji[k * 3 + 2] * dP[i * 3 + 2]);
-            f[(k + 1) * 3 + i] = -q;
-            f[i] += q;
-        }
-    double* out = slots + (b.slot_base + e * 4) * 3;
-#pragma unroll
-    for (int k = 0; k < 12; ++k) out[k] = f[k];
-    store_theta(gmu, gk, e, -w * (ldm - 2.0 / 3.0 * ldl), -w * ldl, accumulate);
+    double g[12], tm, tk;
+    tet4_vjp<MAT>(J, D, DL, lam, mu, g, tm, tk);
+    for (int a = 0; a < 4; ++a) slots[b.slot_pos[4 * e + a]] = make4(g[3 * a], g[3 * a + 1], g[3 * a + 2]);
+    store_theta(gmu, gk, e, tm, tk, accumulate);
 }
 
 template <int MAT>
-__global__ void __launch_bounds__(256) k_hex8_vjp(GaussBlockDev b, const double4* __restrict__ X4,
+__global__ void __launch_bounds__(256) k_tet4_patch_vjp(GaussBlockDev b, const double4* __restrict__ X4,
+                                                         const double4* __restrict__ U4,
+                                                         const double4* __restrict__ L4, double4* __restrict__ slots,
+                                                         double* gmu, double* gk, int accumulate) {
+    __shared__ double sh[32][168];  // [0, 72): node dX, du, dlam ; [72, 168): 8 tets x 4 nodes x 3
+    const int lane = threadIdx.x & 31;
+    const int g = lane & 7;
+    const int pl = threadIdx.x >> 3;
+    const int64_t p = static_cast<int64_t>(blockIdx.x) * 32 + pl;
+    const bool valid = p < b.num_patches;
+    const int32_t n = valid ? b.patch_nodes[p * 8 + g] : 0;
+    const double4 x = X4[n], u = U4[n], l = L4[n];
+    const int src = lane & ~7;
+    double* s = sh[pl];
+    s[g * 9 + 0] = x.x - __shfl_sync(kFull, x.x, src);
+    s[g * 9 + 1] = x.y - __shfl_sync(kFull, x.y, src);
+    s[g * 9 + 2] = x.z - __shfl_sync(kFull, x.z, src);
+    s[g * 9 + 3] = u.x - __shfl_sync(kFull, u.x, src);
+    s[g * 9 + 4] = u.y - __shfl_sync(kFull, u.y, src);
+    s[g * 9 + 5] = u.z - __shfl_sync(kFull, u.z, src);
+    s[g * 9 + 6] = l.x - __shfl_sync(kFull, l.x, src);
+    s[g * 9 + 7] = l.y - __shfl_sync(kFull, l.y, src);
+    s[g * 9 + 8] = l.z - __shfl_sync(kFull, l.z, src);
+    int32_t e0 = 0, cnt = 0;
+    if (valid) {
+        e0 = b.patch_first[p];
+        cnt = b.patch_first[p + 1] - e0;
+    }
+    const uint32_t loc = (g < cnt) ? b.patch_local[e0 + g] : 0u;
+    __syncwarp();
+    if (g < cnt) {
+        const int64_t e = e0 + g;
+        const double* n0 = s + local_id(loc, 0) * 9;
+        const double* n1 = s + local_id(loc, 1) * 9;
+        const double* n2 = s + local_id(loc, 2) * 9;
+        const double* n3 = s + local_id(loc, 3) * 9;
+        double J[9], D[9], DL[9];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            J[i * 3 + 0] = n1[i] - n0[i];
+            J[i * 3 + 1] = n2[i] - n0[i];
+            J[i * 3 + 2] = n3[i] - n0[i];
+            D[i * 3 + 0] = n1[3 + i] - n0[3 + i];
+            D[i * 3 + 1] = n2[3 + i] - n0[3 + i];
+            D[i * 3 + 2] = n3[3 + i] - n0[3 + i];
+            DL[i * 3 + 0] = n1[6 + i] - n0[6 + i];
+            DL[i * 3 + 1] = n2[6 + i] - n0[6 + i];
+            DL[i * 3 + 2] = n3[6 + i] - n0[6 + i];
+        }
+        double lam, mu;
+        element_lame(b, e, lam, mu);
+        double gv[12], tm, tk;
+        tet4_vjp<MAT>(J, D, DL, lam, mu, gv, tm, tk);
+        double* c = s + 72 + g * 12;
+#pragma unroll
+        for (int k = 0; k < 12; ++k) c[k] = gv[k];
+        store_theta(gmu, gk, e, tm, tk, accumulate);
+    }
+    __syncwarp();
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    const uint32_t gm = valid ? b.patch_gather[p * 8 + g] : 0u;
+    for (uint32_t m = gm & 0xFFu; m; m &= m - 1) {
+        const int t = __ffs(m) - 1;
+        const double* c = s + 72 + t * 12 + ((gm >> (8 + 2 * t)) & 3u) * 3;
+        fx += c[0];
+        fy += c[1];
+        fz += c[2];
+    }
+    if (valid) {
+        const int32_t pos = b.slot_pos[p * 8 + g];
+        if (pos >= 0) slots[pos] = make4(fx, fy, fz);
+    }
+}
+
+template <int MAT>
+__global__ void __launch_bounds__(128) k_hex8_vjp(GaussBlockDev b, const double4* __restrict__ X4,
                                                    const double4* __restrict__ U4, const double4* __restrict__ L4,
-                                                   double* __restrict__ slots, double* gmu, double* gk,
+                                                   double4* __restrict__ slots, double* gmu, double* gk,
                                                    int accumulate) {
-    __shared__ double sh[32][144];
+    __shared__ double sh[16][144];
     const int lane = threadIdx.x & 31;
     const int g = lane & 7;
     const int el = threadIdx.x >> 3;
-    const int64_t e = static_cast<int64_t>(blockIdx.x) * 32 + el;
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * 16 + el;
     const bool valid = e < b.num_elems;
     const int32_t n = valid ? b.conn[e * 8 + g] : 0;
     const double4 x = X4[n], u = U4[n], l = L4[n];
@@ -459,17 +734,14 @@ __global__ void __launch_bounds__(256) k_hex8_vjp(GaussBlockDev b, const double4
         fz -= d0 * Q[2] + d1 * Q[5] + d2 * Q[8];
     }
     if (valid) {
-        double* out = slots + (b.slot_base + e * 8 + g) * 3;
-        out[0] = fx;
-        out[1] = fy;
-        out[2] = fz;
+        slots[b.slot_pos[e * 8 + g]] = make4(fx, fy, fz);
         if (g == 0) store_theta(gmu, gk, e, tm, tk, accumulate);
     }
 }
 
 template <int MAT>
 __global__ void __launch_bounds__(256) k_cell_vjp(CellBlockDev b, const double4* __restrict__ U4,
-                                                   const double4* __restrict__ L4, double* __restrict__ slots,
+                                                   const double4* __restrict__ L4, double4* __restrict__ slots,
                                                    double* gmu, double* gk, int accumulate) {
     const int lane = threadIdx.x & 31;
     const int64_t c = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
@@ -503,11 +775,12 @@ __global__ void __launch_bounds__(256) k_cell_vjp(CellBlockDev b, const double4*
     double dP[9], ldl, ldm;
     stress_vjp(MAT, lam, mu, H, L, dP, &ldl, &ldm);
     const double V = b.volumes[c];
-    double* out = slots + b.slot_base * 3;
     for (int32_t s = s0 + lane; s < s1; s += 32) {
         const double gg[3] = {b.grads64[3 * s], b.grads64[3 * s + 1], b.grads64[3 * s + 2]};
+        double f[3];
 #pragma unroll
-        for (int i = 0; i < 3; ++i) out[3 * s + i] = (gg[0] * dP[i * 3 + 0] + gg[1] * dP[i * 3 + 1] + gg[2] * dP[i * 3 + 2]) * -V;
+        for (int i = 0; i < 3; ++i) f[i] = (gg[0] * dP[i * 3 + 0] + gg[1] * dP[i * 3 + 1] + gg[2] * dP[i * 3 + 2]) * -V;
+        slots[b.slot_pos[s]] = make4(f[0], f[1], f[2]);
     }
     if (lane == 0) store_theta(gmu, gk, c, -V * (ldm - 2.0 / 3.0 * ldl), -V * ldl, accumulate);
 }
@@ -516,18 +789,7 @@ __global__ void __launch_bounds__(256) k_cell_vjp(CellBlockDev b, const double4*
 // Lumped mass slots (src/MassUtils.cpp:17-46): slot (e, a) = rho V_e / n_en with
 // V_e = sum_gp w_gp (ComputeElementVolumeFunctor.h:20-79).
 // ---------------------------------------------------------------------------
-__global__ void k_gauss_volume_slots(GaussBlockDev b, double density, const double4* __restrict__ X4,
-                                     double* __restrict__ slots) {
-    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (e >= b.num_elems) return;
-    const int nn = b.kind == AM_HEX8_GAUSS ? 8 : 4;
-    double X[24];
-    for (int a = 0; a < nn; ++a) {
-        const double4 x = X4[b.conn[e * nn + a]];
-        X[a * 3 + 0] = x.x;
-        X[a * 3 + 1] = x.y;
-        X[a * 3 + 2] = x.z;
-    }
+__device__ double element_volume(int nn, const double* X) {
     double V = 0.0;
     const int ngp = nn == 8 ? 8 : 1;
     for (int gp = 0; gp < ngp; ++gp) {
@@ -554,28 +816,81 @@ __global__ void k_gauss_volume_slots(GaussBlockDev b, double density, const doub
             }
         V += (nn == 8 ? 1.0 : 1.0 / 6.0) * det3(J);
     }
-    const double me = V * density / nn;
-    for (int a = 0; a < nn; ++a) {
-        double* out = slots + (b.slot_base + e * nn + a) * 3;
-        out[0] = me;
-        out[1] = 0.0;
-        out[2] = 0.0;
+    return V;
+}
+
+// Patched Tet4 blocks: per patch node, the sum over the patch's tets (set-up only).
+__global__ void k_tet4_patch_volume_slots(GaussBlockDev b, double density, const double4* __restrict__ X4,
+                                          double4* __restrict__ slots) {
+    const int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= b.num_patches) return;
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int32_t e = b.patch_first[p]; e < b.patch_first[p + 1]; ++e) {
+        double X[12];
+        for (int a = 0; a < 4; ++a) {
+            const double4 x = X4[b.conn[4 * static_cast<int64_t>(e) + a]];
+            X[a * 3 + 0] = x.x;
+            X[a * 3 + 1] = x.y;
+            X[a * 3 + 2] = x.z;
+        }
+        const double me = element_volume(4, X) * density / 4;
+        const uint32_t loc = b.patch_local[e];
+        for (int k = 0; k < 4; ++k) acc[local_id(loc, k)] += me;
     }
+    for (int a = 0; a < 8; ++a) {
+        const int32_t pos = b.slot_pos[p * 8 + a];
+        if (pos >= 0) slots[pos] = make_double4(acc[a], 0.0, 0.0, 0.0);
+    }
+}
+
+__global__ void k_gauss_volume_slots(GaussBlockDev b, double density, const double4* __restrict__ X4,
+                                     double4* __restrict__ slots) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= b.num_elems) return;
+    const int nn = b.kind == AM_HEX8_GAUSS ? 8 : 4;
+    double X[24];
+    for (int a = 0; a < nn; ++a) {
+        const double4 x = X4[b.conn[e * nn + a]];
+        X[a * 3 + 0] = x.x;
+        X[a * 3 + 1] = x.y;
+        X[a * 3 + 2] = x.z;
+    }
+    const double me = element_volume(nn, X) * density / nn;
+    for (int a = 0; a < nn; ++a) slots[b.slot_pos[e * nn + a]] = make_double4(me, 0.0, 0.0, 0.0);
 }
 
 // ---------------------------------------------------------------------------
 // Node kernels.
 // ---------------------------------------------------------------------------
+// Sum of node i's slots: a contiguous node-major range, summed in ascending
+// logical-slot order (FP64 accumulation for both slot types).
 template <typename S>
-__device__ __forceinline__ void gather(const NodeDev& nd, const S* __restrict__ slots, int64_t i, double& fx,
+__device__ __forceinline__ void gather(const NodeDev& nd, const vec4_t<S>* __restrict__ slots, int64_t i, double& fx,
                                        double& fy, double& fz) {
     const int32_t p0 = nd.node_ptr[i], p1 = nd.node_ptr[i + 1];
     fx = fy = fz = 0.0;
-    for (int32_t p = p0; p < p1; ++p) {
-        const int64_t s = nd.node_slots[p];
-        fx += static_cast<double>(slots[3 * s + 0]);
-        fy += static_cast<double>(slots[3 * s + 1]);
-        fz += static_cast<double>(slots[3 * s + 2]);
+    int32_t p = p0;
+    // Four independent loads in flight, then the sums in slot order.
+    for (; p + 4 <= p1; p += 4) {
+        const vec4_t<S> a = slots[p], b = slots[p + 1], c = slots[p + 2], d = slots[p + 3];
+        fx += static_cast<double>(a.x);
+        fy += static_cast<double>(a.y);
+        fz += static_cast<double>(a.z);
+        fx += static_cast<double>(b.x);
+        fy += static_cast<double>(b.y);
+        fz += static_cast<double>(b.z);
+        fx += static_cast<double>(c.x);
+        fy += static_cast<double>(c.y);
+        fz += static_cast<double>(c.z);
+        fx += static_cast<double>(d.x);
+        fy += static_cast<double>(d.y);
+        fz += static_cast<double>(d.z);
+    }
+    for (; p < p1; ++p) {
+        const vec4_t<S> v = slots[p];
+        fx += static_cast<double>(v.x);
+        fy += static_cast<double>(v.y);
+        fz += static_cast<double>(v.z);
     }
 }
 
@@ -607,12 +922,12 @@ __device__ __forceinline__ void free_mask(uint32_t word, uint32_t active, double
 }
 
 template <typename S>
-__global__ void __launch_bounds__(256) k_gather_force(NodeDev nd, const S* __restrict__ slots, double* __restrict__ f,
-                                                       int accumulate) {
+__global__ void __launch_bounds__(256) k_gather_force(NodeDev nd, const vec4_t<S>* __restrict__ slots,
+                                                       double* __restrict__ f, int accumulate) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= nd.num_nodes) return;
     double fx, fy, fz;
-    gather(nd, slots, i, fx, fy, fz);
+    gather<S>(nd, slots, i, fx, fy, fz);
     if (accumulate) {
         f[3 * i + 0] += fx;
         f[3 * i + 1] += fy;
@@ -625,12 +940,12 @@ __global__ void __launch_bounds__(256) k_gather_force(NodeDev nd, const S* __res
 }
 
 template <typename S>
-__global__ void __launch_bounds__(256) k_init_accel(NodeDev nd, const S* __restrict__ slots, double4* __restrict__ A4,
-                                                     int* status) {
+__global__ void __launch_bounds__(256) k_init_accel(NodeDev nd, const vec4_t<S>* __restrict__ slots,
+                                                     double4* __restrict__ A4, int* status) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= nd.num_nodes) return;
     double fx, fy, fz;
-    gather(nd, slots, i, fx, fy, fz);
+    gather<S>(nd, slots, i, fx, fy, fz);
     const double m = nd.mass[i];
     if (nd.has_g) {
         fx += nd.g[0] * m;
@@ -662,7 +977,7 @@ __global__ void __launch_bounds__(256) k_prologue(NodeDev nd, const StepParams* 
 }
 
 template <typename S>
-__global__ void __launch_bounds__(256) k_node_step(NodeDev nd, const S* __restrict__ slots,
+__global__ void __launch_bounds__(256) k_node_step(NodeDev nd, const vec4_t<S>* __restrict__ slots,
                                                     const StepParams* __restrict__ table, int64_t step, int advance,
                                                     double4* __restrict__ U4, double4* __restrict__ V4,
                                                     double4* __restrict__ A4, double4* __restrict__ u_copy,
@@ -670,7 +985,7 @@ __global__ void __launch_bounds__(256) k_node_step(NodeDev nd, const S* __restri
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= nd.num_nodes) return;
     double fx, fy, fz;
-    gather(nd, slots, i, fx, fy, fz);
+    gather<S>(nd, slots, i, fx, fy, fz);
     const double m = nd.mass[i];
     if (nd.has_g) {
         fx += nd.g[0] * m;
@@ -722,14 +1037,14 @@ __global__ void k_adj_prep(NodeDev nd, const StepParams* __restrict__ table, int
 
 // Reverse of the rest of step `step` given g = (dF/du)^T lam in the slots; then
 // prepares lam for step-1 (or for the initial acceleration when step == 0).
-__global__ void __launch_bounds__(256) k_adj_update(NodeDev nd, const double* __restrict__ slots,
+__global__ void __launch_bounds__(256) k_adj_update(NodeDev nd, const double4* __restrict__ slots,
                                                      const StepParams* __restrict__ table, int64_t step,
                                                      double4* __restrict__ UB, double4* __restrict__ VB,
                                                      double4* __restrict__ AB, double4* __restrict__ L4) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= nd.num_nodes) return;
     double gx, gy, gz;
-    gather(nd, slots, i, gx, gy, gz);
+    gather<double>(nd, slots, i, gx, gy, gz);
     const StepParams& P = table[step];
     double4 ub = UB[i];
     const double4 vb = VB[i];
@@ -908,19 +1223,32 @@ inline unsigned grid_for(int64_t n, int per_block) { return static_cast<unsigned
 void launch_gauss_force(const GaussBlockDev& b, int mixed, const double4* X4, const double4* U4, void* slots,
                         int* status, cudaStream_t s) {
     if (b.num_elems == 0) return;
-    if (b.kind == AM_TET4_GAUSS) {
+    if (b.kind == AM_TET4_GAUSS && b.patched == 2) {
+        if (mixed) {
+            AM_DISPATCH_MAT(b.material, (k_tet4_hex6_force<float, M, 1><<<grid_for(b.num_patches, 256), 256, 0, s>>>(b, X4, U4, static_cast<float4*>(slots), status)));
+        } else {
+            AM_DISPATCH_MAT(b.material, (k_tet4_hex6_force<double, M, 1><<<grid_for(b.num_patches, 256), 256, 0, s>>>(b, X4, U4, static_cast<double4*>(slots), status)));
+        }
+    } else if (b.kind == AM_TET4_GAUSS && b.patched) {
+        const unsigned grid = grid_for(b.num_patches, 8 * kPatchesPerWarp);
+        if (mixed) {
+            AM_DISPATCH_MAT(b.material, (k_tet4_patch_force<float, M><<<grid, 256, 0, s>>>(b, X4, U4, static_cast<float4*>(slots), status)));
+        } else {
+            AM_DISPATCH_MAT(b.material, (k_tet4_patch_force<double, M><<<grid, 256, 0, s>>>(b, X4, U4, static_cast<double4*>(slots), status)));
+        }
+    } else if (b.kind == AM_TET4_GAUSS) {
         const unsigned grid = grid_for(b.num_elems, 256);
         if (mixed) {
-            AM_DISPATCH_MAT(b.material, (k_tet4_force<float, M><<<grid, 256, 0, s>>>(b, X4, U4, static_cast<float*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (k_tet4_force<float, M><<<grid, 256, 0, s>>>(b, X4, U4, static_cast<float4*>(slots), status)));
         } else {
-            AM_DISPATCH_MAT(b.material, (k_tet4_force<double, M><<<grid, 256, 0, s>>>(b, X4, U4, static_cast<double*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (k_tet4_force<double, M><<<grid, 256, 0, s>>>(b, X4, U4, static_cast<double4*>(slots), status)));
         }
     } else {
         const unsigned grid = grid_for(b.num_elems, 32);
         if (mixed) {
-            AM_DISPATCH_MAT(b.material, (k_hex8_force<float, M><<<grid, 256, 0, s>>>(b, X4, U4, static_cast<float*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (k_hex8_force<float, M><<<grid, 256, 0, s>>>(b, X4, U4, static_cast<float4*>(slots), status)));
         } else {
-            AM_DISPATCH_MAT(b.material, (k_hex8_force<double, M><<<grid, 256, 0, s>>>(b, X4, U4, static_cast<double*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (k_hex8_force<double, M><<<grid, 256, 0, s>>>(b, X4, U4, static_cast<double4*>(slots), status)));
         }
     }
 }
@@ -930,59 +1258,65 @@ void launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void
     if (b.max_entries <= 8) {
         const unsigned grid = grid_for(b.num_cells, 256);
         if (mixed) {
-            AM_DISPATCH_MAT(b.material, (k_cell_force_thread<float, M><<<grid, 256, 0, s>>>(b, U4, static_cast<float*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (k_cell_force_thread<float, M><<<grid, 256, 0, s>>>(b, U4, static_cast<float4*>(slots), status)));
         } else {
-            AM_DISPATCH_MAT(b.material, (k_cell_force_thread<double, M><<<grid, 256, 0, s>>>(b, U4, static_cast<double*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (k_cell_force_thread<double, M><<<grid, 256, 0, s>>>(b, U4, static_cast<double4*>(slots), status)));
         }
     } else {
         const unsigned grid = grid_for(b.num_cells * 32, 256);
         if (mixed) {
-            AM_DISPATCH_MAT(b.material, (k_cell_force_warp<float, M><<<grid, 256, 0, s>>>(b, U4, static_cast<float*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (k_cell_force_warp<float, M><<<grid, 256, 0, s>>>(b, U4, static_cast<float4*>(slots), status)));
         } else {
-            AM_DISPATCH_MAT(b.material, (k_cell_force_warp<double, M><<<grid, 256, 0, s>>>(b, U4, static_cast<double*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (k_cell_force_warp<double, M><<<grid, 256, 0, s>>>(b, U4, static_cast<double4*>(slots), status)));
         }
     }
 }
 
-void launch_gauss_vjp(const GaussBlockDev& b, const double4* X4, const double4* U4, const double4* L4, double* slots,
+void launch_gauss_vjp(const GaussBlockDev& b, const double4* X4, const double4* U4, const double4* L4, double4* slots,
                       double* gmu, double* gkappa, int accumulate, cudaStream_t s) {
     if (b.num_elems == 0) return;
-    if (b.kind == AM_TET4_GAUSS) {
+    if (b.kind == AM_TET4_GAUSS && b.patched) {
+        const unsigned grid = grid_for(b.num_patches, 32);
+        AM_DISPATCH_MAT(b.material, (k_tet4_patch_vjp<M><<<grid, 256, 0, s>>>(b, X4, U4, L4, slots, gmu, gkappa, accumulate)));
+    } else if (b.kind == AM_TET4_GAUSS) {
         const unsigned grid = grid_for(b.num_elems, 256);
         AM_DISPATCH_MAT(b.material, (k_tet4_vjp<M><<<grid, 256, 0, s>>>(b, X4, U4, L4, slots, gmu, gkappa, accumulate)));
     } else {
-        const unsigned grid = grid_for(b.num_elems, 32);
-        AM_DISPATCH_MAT(b.material, (k_hex8_vjp<M><<<grid, 256, 0, s>>>(b, X4, U4, L4, slots, gmu, gkappa, accumulate)));
+        const unsigned grid = grid_for(b.num_elems, 16);
+        AM_DISPATCH_MAT(b.material, (k_hex8_vjp<M><<<grid, 128, 0, s>>>(b, X4, U4, L4, slots, gmu, gkappa, accumulate)));
     }
 }
 
-void launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double* slots, double* gmu,
+void launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double4* slots, double* gmu,
                      double* gkappa, int accumulate, cudaStream_t s) {
     if (b.num_cells == 0) return;
     const unsigned grid = grid_for(b.num_cells * 32, 256);
     AM_DISPATCH_MAT(b.material, (k_cell_vjp<M><<<grid, 256, 0, s>>>(b, U4, L4, slots, gmu, gkappa, accumulate)));
 }
 
-void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const double4* X4, double* slots,
+void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const double4* X4, double4* slots,
                                cudaStream_t s) {
     if (b.num_elems == 0) return;
-    k_gauss_volume_slots<<<grid_for(b.num_elems, 128), 128, 0, s>>>(b, density, X4, slots);
+    if (b.kind == AM_TET4_GAUSS && b.patched)
+        k_tet4_patch_volume_slots<<<grid_for(b.num_patches, 128), 128, 0, s>>>(b, density, X4, slots);
+    else
+        k_gauss_volume_slots<<<grid_for(b.num_elems, 128), 128, 0, s>>>(b, density, X4, slots);
 }
 
 void launch_gather_force(const NodeDev& nd, int mixed, const void* slots, double* f, int accumulate, cudaStream_t s) {
     const unsigned grid = grid_for(nd.num_nodes, 256);
     if (mixed)
-        k_gather_force<float><<<grid, 256, 0, s>>>(nd, static_cast<const float*>(slots), f, accumulate);
+        k_gather_force<float><<<grid, 256, 0, s>>>(nd, static_cast<const float4*>(slots), f, accumulate);
     else
-        k_gather_force<double><<<grid, 256, 0, s>>>(nd, static_cast<const double*>(slots), f, accumulate);
+        k_gather_force<double><<<grid, 256, 0, s>>>(nd, static_cast<const double4*>(slots), f, accumulate);
 }
 
 void launch_init_accel(const NodeDev& nd, int mixed, const void* slots, double4* A4, int* status, cudaStream_t s) {
     const unsigned grid = grid_for(nd.num_nodes, 256);
     if (mixed)
-        k_init_accel<float><<<grid, 256, 0, s>>>(nd, static_cast<const float*>(slots), A4, status);
+        k_init_accel<float><<<grid, 256, 0, s>>>(nd, static_cast<const float4*>(slots), A4, status);
     else
-        k_init_accel<double><<<grid, 256, 0, s>>>(nd, static_cast<const double*>(slots), A4, status);
+        k_init_accel<double><<<grid, 256, 0, s>>>(nd, static_cast<const double4*>(slots), A4, status);
 }
 
 void launch_prologue(const NodeDev& nd, const StepParams* table, double4* U4, double4* V4, const double4* A4,
@@ -995,9 +1329,9 @@ void launch_node_step(const NodeDev& nd, int mixed, const void* slots, const Ste
                       cudaStream_t s) {
     const unsigned grid = grid_for(nd.num_nodes, 256);
     if (mixed)
-        k_node_step<float><<<grid, 256, 0, s>>>(nd, static_cast<const float*>(slots), table, step, advance, U4, V4, A4, u_copy, status);
+        k_node_step<float><<<grid, 256, 0, s>>>(nd, static_cast<const float4*>(slots), table, step, advance, U4, V4, A4, u_copy, status);
     else
-        k_node_step<double><<<grid, 256, 0, s>>>(nd, static_cast<const double*>(slots), table, step, advance, U4, V4, A4, u_copy, status);
+        k_node_step<double><<<grid, 256, 0, s>>>(nd, static_cast<const double4*>(slots), table, step, advance, U4, V4, A4, u_copy, status);
 }
 
 void launch_adj_prep(const NodeDev& nd, const StepParams* table, int64_t step, const double4* VB, const double4* AB,
@@ -1005,7 +1339,7 @@ void launch_adj_prep(const NodeDev& nd, const StepParams* table, int64_t step, c
     k_adj_prep<<<grid_for(nd.num_nodes, 256), 256, 0, s>>>(nd, table, step, VB, AB, L4);
 }
 
-void launch_adj_update(const NodeDev& nd, const double* slots, const StepParams* table, int64_t step, double4* UB,
+void launch_adj_update(const NodeDev& nd, const double4* slots, const StepParams* table, int64_t step, double4* UB,
                        double4* VB, double4* AB, double4* L4, cudaStream_t s) {
     k_adj_update<<<grid_for(nd.num_nodes, 256), 256, 0, s>>>(nd, slots, table, step, UB, VB, AB, L4);
 }

@@ -22,6 +22,11 @@ struct StepParams {
 // Device status word: [0] = first am_status error code, [1] = offending entity.
 enum StatusSlot { kStatusCode = 0, kStatusIndex = 1 };
 
+// Force slots are stored node-major: the contributions to node i occupy the
+// contiguous range [node_ptr[i], node_ptr[i+1]) of the slot array, in ascending
+// logical slot order (block, then element / patch / entry). Writers map a logical
+// slot s of a block to its position with slot_pos[s] (block-local pointer).
+
 // Gauss-element block on the device.
 struct GaussBlockDev {
     int32_t kind;      // AM_TET4_GAUSS / AM_HEX8_GAUSS
@@ -31,7 +36,16 @@ struct GaussBlockDev {
     const int32_t* conn;
     const double* mu_field;     // may be null
     const double* kappa_field;  // may be null
-    int64_t slot_base;          // first slot of this block in the global slot array
+    const int32_t* slot_pos;    // logical slot -> node-major position (-1: unused)
+    // Tet4 element patches: at most 6 consecutive tets on at most 8 nodes, whose
+    // contributions are summed per patch node before they are written (8 logical
+    // slots per patch).
+    int32_t patched;             // 0: per element, 1: generic patches, 2: split-hex patches
+    int64_t num_patches;
+    const int32_t* patch_first;  // num_patches + 1 element offsets
+    const int32_t* patch_nodes;  // num_patches x 8 (unused entries repeat entry 0)
+    const uint32_t* patch_local; // per element: 4 local node ids, one byte each
+    const uint32_t* patch_gather;// per patch node: bits 0-7 tets touching it, bits 8+2t: its slot in tet t
 };
 
 struct CellBlockDev {
@@ -45,15 +59,14 @@ struct CellBlockDev {
     const double* volumes;
     const double* mu_field;
     const double* kappa_field;
-    int64_t slot_base;
+    const int32_t* slot_pos;    // entry -> node-major position
     int32_t max_entries;        // longest cell (selects thread- or warp-per-cell)
 };
 
 // Node gather + nodal update configuration.
 struct NodeDev {
     int64_t num_nodes;
-    const int32_t* node_ptr;    // num_nodes + 1 offsets into node_slots
-    const int32_t* node_slots;  // ascending slot ids of each node
+    const int32_t* node_ptr;    // num_nodes + 1: node-major slot ranges
     const double* mass;
     const uint32_t* bcword;     // per node: 3 x 10-bit masks of BCs prescribing x, y, z
     const double* bcvalues;     // AM_MAX_BCS x 3 prescribed values
@@ -65,13 +78,12 @@ struct NodeDev {
 void launch_gauss_force(const GaussBlockDev& b, int mixed, const double4* X4, const double4* U4, void* slots,
                         int* status, cudaStream_t s);
 void launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void* slots, int* status, cudaStream_t s);
-void launch_gauss_vjp(const GaussBlockDev& b, const double4* X4, const double4* U4, const double4* L4, double* slots,
+void launch_gauss_vjp(const GaussBlockDev& b, const double4* X4, const double4* U4, const double4* L4, double4* slots,
                       double* gmu, double* gkappa, int accumulate, cudaStream_t s);
-void launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double* slots, double* gmu,
+void launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double4* slots, double* gmu,
                      double* gkappa, int accumulate, cudaStream_t s);
-void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const double4* X4, double* slots,
+void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const double4* X4, double4* slots,
                                cudaStream_t s);
-void launch_cell_volume_slots(const CellBlockDev& b, double* slots, cudaStream_t s);
 
 // f (N x 3, row-major) = gather of the slots (FP64 or FP32 slots), overwrite or accumulate.
 void launch_gather_force(const NodeDev& nd, int mixed, const void* slots, double* f, int accumulate, cudaStream_t s);
@@ -87,7 +99,7 @@ void launch_node_step(const NodeDev& nd, int mixed, const void* slots, const Ste
 // Adjoint node kernels.
 void launch_adj_prep(const NodeDev& nd, const StepParams* table, int64_t step, const double4* VB, const double4* AB,
                      double4* L4, cudaStream_t s);
-void launch_adj_update(const NodeDev& nd, const double* slots, const StepParams* table, int64_t step, double4* UB,
+void launch_adj_update(const NodeDev& nd, const double4* slots, const StepParams* table, int64_t step, double4* UB,
                        double4* VB, double4* AB, double4* L4, cudaStream_t s);
 void launch_sensor_seed(const double4* U4, int32_t num_sensors, const int32_t* sensors, double4* UB, double* loss,
                         cudaStream_t s);

@@ -13,10 +13,15 @@ namespace am {
 
 enum MaterialKind : int32_t { kLinearElastic = 0, kNeoHookean = 1, kElasticSVK = 2 };
 
+// 1/x: IEEE division in FP64; in the FP32 (mixed) path the fast single-precision
+// division intrinsic (about 2 ulp), ample next to FP32 element arithmetic.
+__device__ __forceinline__ double recip(double x) { return 1.0 / x; }
+__device__ __forceinline__ float recip(float x) { return __fdividef(1.0f, x); }
+
 template <typename T>
 __device__ __forceinline__ T cof_inv3(const T* m, T* r, T det) {
     // r = adj(m) / det ; det supplied by the caller (see det3 / det_ap_im1).
-    const T id = T(1) / det;
+    const T id = recip(det);
     r[0] = (m[4] * m[8] - m[5] * m[7]) * id;
     r[1] = (m[2] * m[7] - m[1] * m[8]) * id;
     r[2] = (m[1] * m[5] - m[2] * m[4]) * id;

@@ -47,7 +47,11 @@ def parse():
     ap.add_argument("--skip-adjoint", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
-    return ap.parse_args()
+    ap.add_argument("--no-patches", action="store_true", help="per-element Tet4 kernel instead of element patches")
+    a = ap.parse_args()
+    if a.no_patches:
+        os.environ["APERI_B200_TET4_PATCHES"] = "0"
+    return a
 
 
 # ---------------------------------------------------------------------------

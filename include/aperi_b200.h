@@ -155,6 +155,30 @@ int am_stress(int32_t material, double lambda, double mu, int64_t n, am_memory w
 int am_quadrature(int32_t kind, int32_t smoothed, int64_t n, am_memory where, const double* X, double* B,
                   double* w);
 
+/* ---- RKPM one-pass nodal smoothing cells (set-up) ----
+ * Replaces the reproducing-kernel preprocessing of ElementReproducingKernel with
+ * nodal_smoothing_cell on a thex mesh: the neighbour search
+ * (NeighborSearchProcessor.h:224-319, capped at max_neighbors; the reference caps at
+ * 40, Constants.h:15), the function values (FunctionCreationProcessor.h:72-134, the
+ * 4x4 moment matrices solved in FP64 on the GPU), the one-pass smoothed gradients
+ * (SmoothedCellDataProcessor.h:541-675) and the lumped mass scattered through the
+ * functions (src/MassUtils.cpp:79-112). The thex refinement is implicit: every tet
+ * contributes, at each vertex, the hex through its edge midpoints, face centroids
+ * and centroid; one cell per tet vertex (the active nodes). kernel_radius is per
+ * vertex. The result feeds am_add_block (AM_SMOOTHED_CELLS) and am_set_mass. Host
+ * arrays; errors via am_last_error(NULL). */
+typedef struct am_cells am_cells;
+int am_rkpm_nodal_cells(int64_t num_nodes, const double* coords, int64_t num_tets, const int32_t* tets,
+                        const double* kernel_radius, int32_t max_neighbors, double density, am_cells** out);
+int am_cells_sizes(const am_cells* cells, int64_t* num_cells, int64_t* num_entries, int64_t* num_points,
+                   int64_t* num_nbr_entries);
+/* cell_ptr (num_cells+1), cell_nodes/cell_grads (entries, x3), cell_volumes and mass (num_cells). */
+int am_cells_get(const am_cells* cells, int64_t* cell_ptr, int32_t* cell_nodes, double* cell_grads,
+                 double* cell_volumes, double* mass);
+/* The refinement points (x3), their neighbour CSR and function values. */
+int am_cells_get_points(const am_cells* cells, double* points, int64_t* nbr_ptr, int32_t* nbr, double* values);
+void am_cells_destroy(am_cells* cells);
+
 /* ---- allocation-free Tet4 internal force (no counterpart in the reference) ----
  * For callers that cannot allocate device memory, e.g. a host framework that owns
  * every device allocation through its own pool, or a step that must not pay the

@@ -7,6 +7,7 @@
 #include "am_oracle.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -974,3 +975,192 @@ int ob_rk_function_values(int64_t num_points, const double* points, const double
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// RKPM one-pass nodal smoothing cells on tet-corner hexes.
+//   points: vertices, unique edge midpoints (sorted (a,b)), unique face centroids
+//   (sorted (a,b,c)), tet centroids -- the thex refinement's nodes;
+//   neighbours: ball search with the neighbour's kernel radius, sorted by the
+//   tweaked squared distance then node index, truncated to max_neighbors
+//   (NeighborSearchProcessor.h:224-263, src/NeighborSearchProcessor.cpp:186-245,
+//   NeighborSelectorFunctor.h:60-101);
+//   functions: FunctionCreationProcessor.h:85-130;
+//   cell gradients: SmoothedCellDataProcessor.h:541-675 (one-pass), with the corner
+//   hexes' smoothed quadrature (QuadratureSmoothed.h:97-142);
+//   mass: src/MassUtils.cpp:17-46 on the hexes, then FunctionEvaluationProcessor::ScatterValues
+//   (FunctionEvaluationProcessor.h:130-176).
+// ---------------------------------------------------------------------------
+namespace {
+
+struct ThexPoints {
+    std::vector<double> xyz;                        // P x 3
+    std::vector<std::array<int32_t, 2>> edges;      // sorted
+    std::vector<std::array<int32_t, 3>> faces;      // sorted
+    int64_t n_vert = 0;
+    int64_t edge_id(int32_t a, int32_t b) const {
+        std::array<int32_t, 2> k = {std::min(a, b), std::max(a, b)};
+        return n_vert + (std::lower_bound(edges.begin(), edges.end(), k) - edges.begin());
+    }
+    int64_t face_id(int32_t a, int32_t b, int32_t c) const {
+        std::array<int32_t, 3> k = {a, b, c};
+        std::sort(k.begin(), k.end());
+        return n_vert + static_cast<int64_t>(edges.size()) + (std::lower_bound(faces.begin(), faces.end(), k) - faces.begin());
+    }
+};
+
+ThexPoints thex_points(int64_t N, const double* X, int64_t T, const int32_t* tets) {
+    ThexPoints tp;
+    tp.n_vert = N;
+    for (int64_t t = 0; t < T; ++t) {
+        const int32_t* v = tets + 4 * t;
+        for (int i = 0; i < 4; ++i)
+            for (int j = i + 1; j < 4; ++j) tp.edges.push_back({std::min(v[i], v[j]), std::max(v[i], v[j])});
+        for (int i = 0; i < 4; ++i) {
+            std::array<int32_t, 3> f;
+            int k = 0;
+            for (int j = 0; j < 4; ++j)
+                if (j != i) f[k++] = v[j];
+            std::sort(f.begin(), f.end());
+            tp.faces.push_back(f);
+        }
+    }
+    std::sort(tp.edges.begin(), tp.edges.end());
+    tp.edges.erase(std::unique(tp.edges.begin(), tp.edges.end()), tp.edges.end());
+    std::sort(tp.faces.begin(), tp.faces.end());
+    tp.faces.erase(std::unique(tp.faces.begin(), tp.faces.end()), tp.faces.end());
+    const int64_t P = N + static_cast<int64_t>(tp.edges.size() + tp.faces.size()) + T;
+    tp.xyz.resize(static_cast<size_t>(P) * 3);
+    for (int64_t i = 0; i < N * 3; ++i) tp.xyz[i] = X[i];
+    int64_t p = N;
+    for (const auto& e : tp.edges) {
+        for (int c = 0; c < 3; ++c) tp.xyz[p * 3 + c] = (X[e[0] * 3 + c] + X[e[1] * 3 + c]) * 0.5;
+        ++p;
+    }
+    for (const auto& f : tp.faces) {
+        for (int c = 0; c < 3; ++c) tp.xyz[p * 3 + c] = ((X[f[0] * 3 + c] + X[f[1] * 3 + c]) + X[f[2] * 3 + c]) / 3.0;
+        ++p;
+    }
+    for (int64_t t = 0; t < T; ++t) {
+        std::array<int32_t, 4> s = {tets[4 * t], tets[4 * t + 1], tets[4 * t + 2], tets[4 * t + 3]};
+        std::sort(s.begin(), s.end());
+        for (int c = 0; c < 3; ++c)
+            tp.xyz[p * 3 + c] = (((X[s[0] * 3 + c] + X[s[1] * 3 + c]) + X[s[2] * 3 + c]) + X[s[3] * 3 + c]) * 0.25;
+        ++p;
+    }
+    return tp;
+}
+
+// The 8 thex points of the hex at corner i of tet t, in Hex8 node order.
+void corner_hex(const ThexPoints& tp, const double* X, const int32_t* v, int64_t t, int i, int64_t out[8]) {
+    int32_t o[3];
+    int k = 0;
+    for (int j = 0; j < 4; ++j)
+        if (j != i) o[k++] = v[j];
+    const int32_t c0 = v[i];
+    double d[3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int c = 0; c < 3; ++c) d[a][c] = X[o[a] * 3 + c] - X[c0 * 3 + c];
+    const double det = d[0][0] * (d[1][1] * d[2][2] - d[1][2] * d[2][1]) - d[0][1] * (d[1][0] * d[2][2] - d[1][2] * d[2][0]) +
+                       d[0][2] * (d[1][0] * d[2][1] - d[1][1] * d[2][0]);
+    if (det < 0) std::swap(o[1], o[2]);
+    const int32_t a = o[0], b = o[1], c = o[2];
+    out[0] = c0;
+    out[1] = tp.edge_id(c0, a);
+    out[2] = tp.face_id(c0, a, b);
+    out[3] = tp.edge_id(c0, b);
+    out[4] = tp.edge_id(c0, c);
+    out[5] = tp.face_id(c0, a, c);
+    out[6] = tp.n_vert + static_cast<int64_t>(tp.edges.size() + tp.faces.size()) + t;
+    out[7] = tp.face_id(c0, b, c);
+}
+
+}  // namespace
+
+extern "C" int ob_rkpm_nodal_cells(int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R,
+                                   int32_t max_neighbors, double density, int64_t* num_points, int64_t* num_nbr_entries,
+                                   int64_t* num_cell_entries, double* points, int64_t* nbr_ptr, int32_t* nbr,
+                                   double* values, int64_t* cell_ptr, int32_t* cell_nodes, double* cell_grads,
+                                   double* cell_volumes, double* mass) {
+    const ThexPoints tp = thex_points(N, X, T, tets);
+    const int64_t P = static_cast<int64_t>(tp.xyz.size() / 3);
+    // Neighbours (brute force over the active nodes).
+    std::vector<std::vector<int32_t>> nb(P);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t p = 0; p < P; ++p) {
+        std::vector<std::pair<double, int32_t>> cand;
+        const double* x = &tp.xyz[p * 3];
+        for (int32_t j = 0; j < N; ++j) {
+            const double dx = x[0] - X[j * 3], dy = x[1] - X[j * 3 + 1], dz = x[2] - X[j * 3 + 2];
+            if (dx * dx + dy * dy + dz * dz > R[j] * R[j]) continue;
+            const double tx = X[j * 3] * (1 + 1.0e-6) - x[0], ty = X[j * 3 + 1] * (1 + 1.0e-7) - x[1],
+                         tz = X[j * 3 + 2] * (1 + 1.0e-8) - x[2];
+            cand.push_back({tx * tx + ty * ty + tz * tz, j});
+        }
+        std::sort(cand.begin(), cand.end());
+        if (static_cast<int32_t>(cand.size()) > max_neighbors) cand.resize(max_neighbors);
+        for (const auto& c : cand) nb[p].push_back(c.second);
+    }
+    std::vector<int64_t> ptr(P + 1, 0);
+    for (int64_t p = 0; p < P; ++p) ptr[p + 1] = ptr[p] + static_cast<int64_t>(nb[p].size());
+    std::vector<int32_t> flat(ptr[P]);
+    for (int64_t p = 0; p < P; ++p) std::copy(nb[p].begin(), nb[p].end(), flat.begin() + ptr[p]);
+    std::vector<double> psi(ptr[P]);
+    ob_rk_function_values(P, tp.xyz.data(), X, R, ptr.data(), flat.data(), psi.data());
+    // Corner hexes of each vertex, in tet order.
+    std::vector<std::vector<std::pair<int64_t, int>>> corners(N);
+    for (int64_t t = 0; t < T; ++t)
+        for (int i = 0; i < 4; ++i) corners[tets[4 * t + i]].push_back({t, i});
+    std::vector<std::vector<int32_t>> cn(N);
+    std::vector<std::vector<double>> cg(N);
+    std::vector<double> cv(N, 0.0), mfe(P, 0.0);
+    for (int32_t v = 0; v < N; ++v) {
+        std::vector<int32_t> where(N, -1);
+        for (const auto& ti : corners[v]) {
+            int64_t hp[8];
+            corner_hex(tp, X, tets + 4 * ti.first, ti.first, ti.second, hp);
+            double hx[24], B[24], V;
+            for (int k = 0; k < 8; ++k)
+                for (int c = 0; c < 3; ++c) hx[k * 3 + c] = tp.xyz[hp[k] * 3 + c];
+            ob_hex8_smoothed_bw(hx, B, &V);
+            cv[v] += V;
+            for (int k = 0; k < 8; ++k) mfe[hp[k]] += V * density / 8;
+            for (int k = 0; k < 8; ++k)
+                for (int64_t s = ptr[hp[k]]; s < ptr[hp[k] + 1]; ++s) {
+                    const int32_t j = flat[s];
+                    if (where[j] < 0) {
+                        where[j] = static_cast<int32_t>(cn[v].size());
+                        cn[v].push_back(j);
+                        cg[v].insert(cg[v].end(), {0.0, 0.0, 0.0});
+                    }
+                    for (int c = 0; c < 3; ++c) cg[v][where[j] * 3 + c] += B[k * 3 + c] * V * psi[s];
+                }
+        }
+        for (double& g : cg[v]) g /= cv[v];
+    }
+    int64_t K = 0;
+    for (int32_t v = 0; v < N; ++v) K += static_cast<int64_t>(cn[v].size());
+    if (num_points) *num_points = P;
+    if (num_nbr_entries) *num_nbr_entries = ptr[P];
+    if (num_cell_entries) *num_cell_entries = K;
+    if (points) std::copy(tp.xyz.begin(), tp.xyz.end(), points);
+    if (nbr_ptr) std::copy(ptr.begin(), ptr.end(), nbr_ptr);
+    if (nbr) std::copy(flat.begin(), flat.end(), nbr);
+    if (values) std::copy(psi.begin(), psi.end(), values);
+    if (cell_ptr) {
+        cell_ptr[0] = 0;
+        for (int32_t v = 0; v < N; ++v) cell_ptr[v + 1] = cell_ptr[v] + static_cast<int64_t>(cn[v].size());
+    }
+    int64_t off = 0;
+    for (int32_t v = 0; v < N; ++v) {
+        if (cell_nodes) std::copy(cn[v].begin(), cn[v].end(), cell_nodes + off);
+        if (cell_grads) std::copy(cg[v].begin(), cg[v].end(), cell_grads + 3 * off);
+        off += static_cast<int64_t>(cn[v].size());
+    }
+    if (cell_volumes) std::copy(cv.begin(), cv.end(), cell_volumes);
+    if (mass) {
+        std::fill(mass, mass + N, 0.0);
+        for (int64_t p = 0; p < P; ++p)
+            for (int64_t s = ptr[p]; s < ptr[p + 1]; ++s) mass[flat[s]] += mfe[p] * psi[s];
+    }
+    return 0;
+}

@@ -111,6 +111,20 @@ int ob_rk_function_values(int64_t num_points, const double* points, const double
                           const double* kernel_radius, const int64_t* nbr_ptr,
                           const int32_t* nbr, double* values);
 
+/* RKPM one-pass nodal smoothing cells on the tet-corner hexes (the thex
+ * refinement: each tet splits into 4 hexes at its corners through edge
+ * midpoints, face centroids and the centroid; only the tet vertices are active).
+ * Two calls: sizes first (outputs NULL), then the arrays.
+ *   points (P x 3) and the neighbour CSR (nbr_ptr P+1, nbr) with function values,
+ *   cells (one per vertex): cell_ptr (N+1), cell_nodes, cell_grads (x3), cell_volumes (N),
+ *   mass (N): rho V_hex / 8 to the hex points, scattered through the functions. */
+int ob_rkpm_nodal_cells(int64_t num_nodes, const double* coords, int64_t num_tets, const int32_t* tets,
+                        const double* kernel_radius, int32_t max_neighbors, double density,
+                        int64_t* num_points, int64_t* num_nbr_entries, int64_t* num_cell_entries,
+                        double* points, int64_t* nbr_ptr, int32_t* nbr, double* values,
+                        int64_t* cell_ptr, int32_t* cell_nodes, double* cell_grads, double* cell_volumes,
+                        double* mass);
+
 /* ---- threads ---- */
 void ob_set_threads(int n);
 int ob_get_threads(void);
