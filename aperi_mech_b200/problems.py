@@ -101,3 +101,47 @@ def hex8_nh_lognormal(n: int = 64, seed: int = 0, nsteps: int = 200, sigma: floa
     part = Part("hex8", mat, conn=conn, mu_field=mu_e, kappa_field=kappa_e)
     return Problem(f"hex8_nh_lognormal_{n}", coords, [part], [BoundaryCondition.fixed(fixed)], v0, dt, nsteps, seed,
                    {"sensors": sensors, "config": "Hex8 2x2x2 Gauss, neo-Hookean, lognormal fields"})
+
+
+def _box_tets(n: int, seed: int, jitter: float, lz: float = 2.0):
+    rng = np.random.default_rng(seed)
+    nz = int(round(n * lz))
+    coords, conn_hex = mesh.box_hex(n, n, nz, 1.0, 1.0, lz)
+    coords = mesh.jitter_interior(coords, jitter / n, rng)
+    tets = mesh.hex_to_tets(conn_hex)
+    mesh.check_orientation(coords, tets)
+    return rng, coords, tets
+
+
+def smoothed_tet4_box(n: int = 46, seed: int = 0, nsteps: int = 500, jitter: float = 0.2) -> Problem:
+    """Strain-smoothed Tet4 (element smoothing cells, one cell per tet) on the jittered
+    1 x 1 x 2 lattice of spacing h = 1/n, neo-Hookean as tet4_nh_shear."""
+    from .smoothing import element_smoothing_part
+
+    rng, coords, tets = _box_tets(n, seed, jitter)
+    mat = Material.create("neo_hookean", 1000.0, shear_modulus=3.85e8, bulk_modulus=8.33e8)
+    part, mass = element_smoothing_part(coords, tets, mat)
+    fixed = mesh.side_sets(coords)["surface_5"]
+    v0 = _initial_velocity(coords, fixed, rng, shear=1.0)
+    dt = 0.5 * float(mesh.tet_char_length(coords, tets).min()) / wave_speed(mat.lam, mat.mu, mat.density)
+    return Problem(f"smoothed_tet4_box_{n}", coords, [part], [BoundaryCondition.fixed(fixed)], v0, dt, nsteps, seed,
+                   {"mass": mass, "config": "strain-smoothed Tet4 element cells, neo-Hookean"})
+
+
+def rkpm_box(n: int = 46, seed: int = 0, nsteps: int = 500, jitter: float = 0.2, radius: float = 1.8,
+             max_neighbors: int = 40) -> Problem:
+    """RKPM one-pass nodal smoothing cells on the same lattice: linear basis, cubic
+    B-spline kernel of support radius `radius` x h, neighbours capped at max_neighbors
+    (40 in the reference), neo-Hookean. The cell set-up runs on the GPU."""
+    from .rkpm import nodal_cells
+
+    rng, coords, tets = _box_tets(n, seed, jitter)
+    mat = Material.create("neo_hookean", 1000.0, shear_modulus=3.85e8, bulk_modulus=8.33e8)
+    R = np.full(coords.shape[0], radius / n)
+    cells = nodal_cells(coords, tets, mat, R, max_neighbors=max_neighbors)
+    fixed = mesh.side_sets(coords)["surface_5"]
+    v0 = _initial_velocity(coords, fixed, rng, shear=1.0)
+    dt = 0.5 * float(mesh.tet_char_length(coords, tets).min()) / wave_speed(mat.lam, mat.mu, mat.density)
+    return Problem(f"rkpm_box_{n}", coords, [cells.part], [BoundaryCondition.fixed(fixed)], v0, dt, nsteps, seed,
+                   {"mass": cells.mass, "tets": tets, "entries_per_cell": cells.entries_per_cell,
+                    "config": f"RKPM one-pass nodal cells, R={radius}h, cap {max_neighbors}, neo-Hookean"})

@@ -1,0 +1,83 @@
+"""RKPM one-pass nodal smoothing cells (ElementReproducingKernel with
+nodal_smoothing_cell, include/ElementReproducingKernel.h) built by the library's
+set-up (am_rkpm_nodal_cells): neighbour search, FP64 reproducing-kernel functions
+on the GPU, one-pass smoothed gradients on the tet-corner hexes, lumped mass."""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import capi
+from .capi import check
+from .model import Material, Part
+
+
+@dataclass
+class RKPMCells:
+    part: Part
+    mass: np.ndarray
+    points: np.ndarray | None = None
+    nbr_ptr: np.ndarray | None = None
+    nbr: np.ndarray | None = None
+    values: np.ndarray | None = None
+
+    @property
+    def entries_per_cell(self) -> float:
+        return float(self.part.cell_ptr[-1]) / (len(self.part.cell_ptr) - 1)
+
+
+def thex_max_edge_length(coords: np.ndarray, tets: np.ndarray) -> np.ndarray:
+    """MaxEdgeLengthFunctor (src/MaxEdgeLengthProcessor.cpp:36-60) on the thex refinement:
+    for each vertex, the longest distance to a point of its corner hexes, doubled for
+    inactive points (edge midpoints, face centroids, centroids)."""
+    x = coords[tets]  # T x 4 x 3
+    cen = x.mean(axis=1)
+    out = np.zeros(coords.shape[0])
+    for i in range(4):
+        v = x[:, i]
+        cand = [2.0 * np.linalg.norm(cen - v, axis=1)]
+        others = [j for j in range(4) if j != i]
+        for j in others:
+            cand.append(2.0 * np.linalg.norm((x[:, j] + v) * 0.5 - v, axis=1))
+        for a in range(3):
+            for b in range(a + 1, 3):
+                f = (v + x[:, others[a]] + x[:, others[b]]) / 3.0
+                cand.append(2.0 * np.linalg.norm(f - v, axis=1))
+        np.maximum.at(out, tets[:, i], np.max(np.stack(cand), axis=0))
+    return out
+
+
+def nodal_cells(coords: np.ndarray, tets: np.ndarray, material: Material, kernel_radius: np.ndarray,
+                max_neighbors: int = 40, keep_points: bool = False, mu_field=None, kappa_field=None,
+                name: str = "block_1") -> RKPMCells:
+    lib = capi.load()
+    X = np.ascontiguousarray(coords, dtype=np.float64)
+    T = np.ascontiguousarray(tets, dtype=np.int32)
+    R = np.ascontiguousarray(kernel_radius, dtype=np.float64)
+    h = C.c_void_p()
+    check(lib.am_rkpm_nodal_cells(X.shape[0], capi._ptr(X), T.shape[0], capi._ptr(T, C.c_int32), capi._ptr(R),
+                                  int(max_neighbors), float(material.density), C.byref(h)))
+    try:
+        nc, ne, npnt, nn = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
+        check(lib.am_cells_sizes(h, C.byref(nc), C.byref(ne), C.byref(npnt), C.byref(nn)))
+        ptr = np.empty(nc.value + 1, dtype=np.int64)
+        nodes = np.empty(ne.value, dtype=np.int32)
+        grads = np.empty((ne.value, 3))
+        vols = np.empty(nc.value)
+        mass = np.empty(nc.value)
+        check(lib.am_cells_get(h, capi._ptr(ptr, C.c_int64), capi._ptr(nodes, C.c_int32), capi._ptr(grads),
+                               capi._ptr(vols), capi._ptr(mass)))
+        res = RKPMCells(Part("cells", material, cell_ptr=ptr, cell_nodes=nodes, cell_grads=grads, cell_volumes=vols,
+                             mu_field=mu_field, kappa_field=kappa_field, name=name), mass)
+        if keep_points:
+            res.points = np.empty((npnt.value, 3))
+            res.nbr_ptr = np.empty(npnt.value + 1, dtype=np.int64)
+            res.nbr = np.empty(nn.value, dtype=np.int32)
+            res.values = np.empty(nn.value)
+            check(lib.am_cells_get_points(h, capi._ptr(res.points), capi._ptr(res.nbr_ptr, C.c_int64),
+                                          capi._ptr(res.nbr, C.c_int32), capi._ptr(res.values)))
+        return res
+    finally:
+        lib.am_cells_destroy(h)

@@ -73,6 +73,8 @@ def lib() -> C.CDLL:
         L.ob_rk_kernel.argtypes = [_dp, C.c_double]
         L.ob_rk_kernel.restype = C.c_double
         L.ob_rk_function_values.argtypes = [C.c_int64, _dp, _dp, _dp, _lp, _ip, _dp]
+        L.ob_rkpm_nodal_cells.argtypes = [C.c_int64, _dp, C.c_int64, _ip, _dp, C.c_int32, C.c_double, _lp, _lp, _lp,
+                                          _dp, _lp, _ip, _dp, _lp, _ip, _dp, _dp, _dp]
         L.ob_set_threads.argtypes = [C.c_int]
         L.ob_get_threads.restype = C.c_int
         _lib = L
@@ -235,6 +237,27 @@ def smoothed_bw(kind: str, X):
     w = C.c_double()
     (lib().ob_hex8_smoothed_bw if kind == "hex8" else lib().ob_tet4_smoothed_bw)(_p(X), _p(B), C.byref(w))
     return B, w.value
+
+
+def rkpm_nodal_cells(coords, tets, kernel_radius, max_neighbors=40, density=1000.0):
+    """Oracle RKPM nodal cells: dict with points, nbr_ptr, nbr, values, cell_ptr, cell_nodes,
+    cell_grads, cell_volumes, mass."""
+    X = np.ascontiguousarray(coords, dtype=np.float64)
+    T = np.ascontiguousarray(tets, dtype=np.int32)
+    R = np.ascontiguousarray(kernel_radius, dtype=np.float64)
+    P, S, K = C.c_int64(), C.c_int64(), C.c_int64()
+    args = (X.shape[0], _p(X), T.shape[0], _p(T, C.c_int32), _p(R), int(max_neighbors), float(density))
+    lib().ob_rkpm_nodal_cells(*args, C.byref(P), C.byref(S), C.byref(K), *([None] * 9))
+    N = X.shape[0]
+    out = {"points": np.empty((P.value, 3)), "nbr_ptr": np.empty(P.value + 1, dtype=np.int64),
+           "nbr": np.empty(S.value, dtype=np.int32), "values": np.empty(S.value),
+           "cell_ptr": np.empty(N + 1, dtype=np.int64), "cell_nodes": np.empty(K.value, dtype=np.int32),
+           "cell_grads": np.empty((K.value, 3)), "cell_volumes": np.empty(N), "mass": np.empty(N)}
+    lib().ob_rkpm_nodal_cells(*args, None, None, None, _p(out["points"]), _p(out["nbr_ptr"], C.c_int64),
+                              _p(out["nbr"], C.c_int32), _p(out["values"]), _p(out["cell_ptr"], C.c_int64),
+                              _p(out["cell_nodes"], C.c_int32), _p(out["cell_grads"]), _p(out["cell_volumes"]),
+                              _p(out["mass"]))
+    return out
 
 
 def set_threads(n: int) -> None:

@@ -1,0 +1,116 @@
+"""RKPM one-pass nodal smoothing cells: the oracle's reproducing conditions (CPU) and
+the library's GPU set-up, force and time stepping against the oracle."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from helpers import rel_err
+
+
+def _box(n=4, seed=0, jitter=0.2):
+    from aperi_mech_b200 import problems
+
+    _, X, T = problems._box_tets(n, seed, jitter)
+    return X, T
+
+
+def _rows(ptr):
+    return np.repeat(np.arange(len(ptr) - 1), np.diff(ptr))
+
+
+@pytest.mark.parametrize("cap", [40, 12])
+def test_oracle_rk_reproducing_conditions(oracle_lib, cap):
+    """ShapeFunctionsFunctorsTest.cpp:138-272 (partition of unity, linear completeness) and
+    SmoothedCellDataTest (partition of nullity of the smoothed gradients), plus exact
+    gradients of linear fields, total cell volume and total mass."""
+    X, T = _box()
+    r = oracle_lib.rkpm_nodal_cells(X, T, np.full(X.shape[0], 1.8 / 4), max_neighbors=cap, density=1000.0)
+    P, ptr, nb, v = r["points"], r["nbr_ptr"], r["nbr"], r["values"]
+    assert np.all(np.diff(ptr) <= cap)
+    rows = _rows(ptr)
+    pu = np.bincount(rows, weights=v, minlength=P.shape[0])
+    assert np.abs(pu - 1.0).max() < 4e-12
+    lc = np.zeros_like(P)
+    np.add.at(lc, rows, v[:, None] * X[nb])
+    assert np.abs(lc - P).max() < 4e-11
+    g, cp, cn = r["cell_grads"], r["cell_ptr"], r["cell_nodes"]
+    crow = _rows(cp)
+    nul = np.zeros_like(X)
+    np.add.at(nul, crow, g)
+    assert np.abs(nul).max() < 1e-9
+    A = np.random.default_rng(1).standard_normal((3, 3))
+    H = np.zeros((X.shape[0], 3, 3))
+    np.add.at(H, crow, (X[cn] @ A.T)[:, :, None] * g[:, None, :])
+    assert np.abs(H - A).max() < 1e-9
+    assert abs(r["cell_volumes"].sum() - 2.0) < 1e-12
+    assert abs(r["mass"].sum() - 2000.0) < 1e-9
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cap", [40, 80])
+def test_rkpm_setup_matches_oracle(gpu, oracle_lib, cap):
+    from aperi_mech_b200.model import Material
+    from aperi_mech_b200.rkpm import nodal_cells
+
+    X, T = _box(n=4, seed=3)
+    R = np.full(X.shape[0], 1.8 / 4)
+    mat = Material.create("neo_hookean", 1000.0, shear_modulus=3.85e8, bulk_modulus=8.33e8)
+    got = nodal_cells(X, T, mat, R, max_neighbors=cap, keep_points=True)
+    want = oracle_lib.rkpm_nodal_cells(X, T, R, max_neighbors=cap, density=1000.0)
+    assert np.array_equal(got.points, want["points"])
+    assert np.array_equal(got.nbr_ptr, want["nbr_ptr"]) and np.array_equal(got.nbr, want["nbr"])
+    assert rel_err(got.values, want["values"]) < 1e-12
+    part = got.part
+    assert np.array_equal(part.cell_ptr, want["cell_ptr"]) and np.array_equal(part.cell_nodes, want["cell_nodes"])
+    assert rel_err(part.cell_grads, want["cell_grads"]) < 1e-12
+    assert rel_err(part.cell_volumes, want["cell_volumes"]) < 1e-13
+    assert rel_err(got.mass, want["mass"]) < 1e-12
+
+
+@pytest.mark.gpu
+def test_rkpm_force_and_steps_match_oracle(gpu, oracle_lib):
+    from aperi_mech_b200 import problems
+    from aperi_mech_b200.model import ExplicitDynamics
+
+    p = problems.rkpm_box(n=4, seed=2, nsteps=40)
+    mass = p.meta["mass"]
+    op = oracle_lib.OracleProblem(p.coords, p.parts, p.bcs, mass=mass)
+    rng = np.random.default_rng(0)
+    u = 1e-3 * rng.standard_normal(p.coords.shape)
+    lam = rng.standard_normal(p.coords.shape)
+    want_f = op.internal_force(u)
+    with ExplicitDynamics(p.coords, p.parts, p.bcs, mass=mass) as m:
+        assert rel_err(m.internal_force(u), want_f) < 1e-12
+        assert rel_err(m.internal_force(u, "mixed"), want_f) < 5e-5
+        for g, w in zip(m.vjp_force(u, lam), op.vjp_force(u, lam)):
+            assert rel_err(g, w) < 1e-11
+        m.set_state(None, p.v0)
+        m.init_acceleration()
+        m.run(p.nsteps, p.dt)
+        got = m.get_state()
+    zero = np.zeros_like(p.coords)
+    want = op.steps(zero, p.v0, op.init_acceleration(zero), np.full(p.nsteps, p.dt))
+    for g, w in zip(got, want):
+        assert rel_err(g, w) < 1e-12
+
+
+@pytest.mark.gpu
+def test_rkpm_linear_field_patch(gpu):
+    """Linear displacement -> every nodal cell's displacement gradient is exact, so the
+    forces of a linear-elastic body in constant stress vanish away from the boundary."""
+    from aperi_mech_b200 import mesh
+    from aperi_mech_b200.model import ExplicitDynamics, Material
+    from aperi_mech_b200.rkpm import nodal_cells
+
+    X, T = _box(n=8, seed=4)
+    mat = Material.create("linear_elastic", 1000.0, youngs_modulus=1e9, poissons_ratio=0.3)
+    cells = nodal_cells(X, T, mat, np.full(X.shape[0], 1.8 / 8))
+    A = 1e-3 * np.random.default_rng(5).standard_normal((3, 3))
+    with ExplicitDynamics(X, [cells.part], mass=cells.mass) as m:
+        f = m.internal_force(X @ A.T)
+    # nodes whose cell and neighbours stay off the boundary (2 layers in)
+    lo, hi = X.min(axis=0), X.max(axis=0)
+    deep = np.all((X > lo + 2.5 / 8) & (X < hi - 2.5 / 8), axis=1)
+    assert deep.sum() > 0
+    assert np.abs(f[deep]).max() < 1e-9 * np.abs(f).max()
