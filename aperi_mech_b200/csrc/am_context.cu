@@ -1177,6 +1177,17 @@ int am_complete_properties(double props[5], char* msg, int msg_len) {
 
 int64_t am_launch_count(const am_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+int am_get_layout(const am_ctx* ctx, int64_t* used_slots, int32_t* patched_tet4_blocks) {
+    if (!ctx) return AM_EINVAL;
+    if (used_slots) *used_slots = ctx->num_used_slots;
+    if (patched_tet4_blocks) {
+        int32_t n = 0;
+        for (const auto& b : ctx->blocks) n += b.patched ? 1 : 0;
+        *patched_tet4_blocks = n;
+    }
+    return AM_OK;
+}
+
 int am_profile_enable(am_ctx* ctx, int enable) {
     if (!ctx) return AM_EINVAL;
     const int rc = guarded(ctx, [&] { ctx->collect_marks(); });

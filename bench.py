@@ -44,6 +44,9 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=70, help="hexes per edge of the Tet4 workload")
     ap.add_argument("--adjoint-n", type=int, default=64)
+    ap.add_argument("--box-n", type=int, default=46, help="lattice cells per unit length of the 1x1x2 box workloads")
+    ap.add_argument("--hex-n", type=int, default=128, help="hexes per edge of the large Hex8 workload")
+    ap.add_argument("--skip-extras", action="store_true")
     ap.add_argument("--skip-adjoint", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
@@ -167,6 +170,124 @@ def measured_peaks():
 
 
 # ---------------------------------------------------------------------------
+def _events(torch):
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def time_run(torch, model, prob, steps, warmup, prec, stream, dev, world, sampler_index=None):
+    """Warm-up, then `steps` timed central-difference steps (device events on the
+    library's stream); per-kernel events are recorded inside the timed region."""
+    model.set_state(None, prob.v0)
+    model.init_acceleration(prec)
+    model.run(warmup, prob.dt, prec)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    model.profile(True)
+    n0 = model.launch_count()
+    ev0, ev1 = _events(torch)
+    sampler = ClockSampler(sampler_index) if sampler_index is not None else None
+    if sampler:
+        sampler.__enter__()
+    try:
+        torch.cuda.synchronize(dev)
+        ev0.record(stream)
+        model.run(steps, prob.dt, prec, t0=warmup * prob.dt)
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+    finally:
+        if sampler:
+            sampler.__exit__(None, None, None)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), world)
+    kms, kn = model.profile_read()
+    model.profile(False)
+    return {"ms": ms, "value": world * prob.num_elems * steps / (ms * 1e-3) / 1e6,
+            "launches": model.launch_count() - n0,
+            "kernels": {"element_ms": kms[0] / max(kn[0], 1), "node_ms": kms[1] / max(kn[1], 1),
+                        "element_total_ms": kms[0], "node_total_ms": kms[1]},
+            "clocks": sampler.summary() if sampler else None}
+
+
+def algorithmic_bytes(prob, layout):
+    """Compulsory HBM bytes per launch of the element and node kernels (mixed path):
+    coordinates and displacement read once per node (48 B), connectivity (4 B per
+    element node), the assembled FP32 force slots written once and read once (12 B),
+    and in the node kernel mass 8 B, BC word 4 B, node range 4 B, displacement and
+    half-step velocity read and written (96 B)."""
+    N = prob.num_nodes
+    S = layout["used_slots"]
+    conn = 0
+    for p in prob.parts:
+        if p.kind == "cells":
+            conn += 4 * int(p.cell_ptr[-1]) + 12 * int(p.cell_ptr[-1])  # entry node + FP32 gradient
+        else:
+            conn += 4 * p.conn.size
+    return {"element": conn + 48 * N + 12 * S, "node": 12 * S + (8 + 4 + 4 + 96) * N}
+
+
+def roofline_for(kernels, alg, peak, peak_kind):
+    dominant = "node" if kernels["node_total_ms"] >= kernels["element_total_ms"] else "element"
+    ms = kernels[f"{dominant}_ms"]
+    achieved = alg[dominant] / (ms * 1e-3) / 1e9
+    return {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+            "algorithmic_bytes_per_launch": alg[dominant], "ms_per_launch": ms}
+
+
+def measure_workload(torch, prob, steps, warmup, stream, dev, world, mass=None, precs=("fp64", "mixed")):
+    from aperi_mech_b200.model import ExplicitDynamics
+
+    out = {"workload": prob.name, "elements": prob.num_elems, "nodes": prob.num_nodes, "steps": steps,
+           "dt": prob.dt, "config": prob.meta.get("config")}
+    peak, kind = measured_peaks()
+    with ExplicitDynamics(prob.coords, prob.parts, prob.bcs, mass=mass, stream=stream.cuda_stream) as m:
+        layout = m.layout()
+        states = {}
+        for prec in precs:
+            r = time_run(torch, m, prob, steps, warmup, prec, stream, dev, world)
+            states[prec] = m.get_state()[0]
+            out[prec] = {"value": r["value"], "ms_per_step": r["ms"] / steps, "kernels": r["kernels"]}
+        if "fp64" in states and "mixed" in states:
+            u64 = states["fp64"]
+            out["mixed_rel_disp_err_l2"] = float(np.linalg.norm(states["mixed"] - u64) / np.linalg.norm(u64))
+            f64 = m.internal_force(u64, "fp64")
+            out["mixed_rel_force_err_l2"] = float(np.linalg.norm(m.internal_force(u64, "mixed") - f64) / np.linalg.norm(f64))
+        if "mixed" in precs:
+            out["roofline_mixed"] = roofline_for(out["mixed"]["kernels"], algorithmic_bytes(prob, layout), peak, kind)
+    return out
+
+
+def run_adjoint(torch, pa, ckpt, stream, dev):
+    from aperi_mech_b200.model import ExplicitDynamics
+
+    with ExplicitDynamics(pa.coords, pa.parts, pa.bcs, stream=stream.cuda_stream) as ma:
+        times = {}
+        for rep in range(2):
+            ma.set_state(None, pa.v0)
+            torch.cuda.synchronize(dev)
+            a0, a1 = _events(torch)
+            a0.record(stream)
+            ma.init_acceleration()
+            ma.run(pa.nsteps, pa.dt)
+            a1.record(stream)
+            torch.cuda.synchronize(dev)
+            times["forward"] = a0.elapsed_time(a1)
+            ma.set_state(None, pa.v0)
+            torch.cuda.synchronize(dev)
+            ma.profile(rep == 1)
+            a0.record(stream)
+            loss, gm, gk = ma.adjoint(pa.nsteps, pa.dt, ckpt, pa.meta["sensors"])
+            a1.record(stream)
+            torch.cuda.synchronize(dev)
+            times["adjoint"] = a0.elapsed_time(a1)
+        pms, pn = ma.profile_read()
+        ma.profile(False)
+    return {"workload": pa.name, "elements": pa.num_elems, "steps": pa.nsteps, "ckpt_every": ckpt,
+            "forward_ms": times["forward"], "adjoint_ms": times["adjoint"], "ratio": times["adjoint"] / times["forward"],
+            "loss": loss, "grad_mu_norm": float(np.linalg.norm(gm)), "grad_kappa_norm": float(np.linalg.norm(gk)),
+            "kernel_ms": {"element": pms[0], "node": pms[1], "vjp": pms[2], "adjoint_node": pms[3]},
+            "kernel_launches": {"element": pn[0], "node": pn[1], "vjp": pn[2], "adjoint_node": pn[3]}}
+
+
 def run_ours(args, rank, world, local):
     import torch
 
@@ -178,38 +299,12 @@ def run_ours(args, rank, world, local):
     E, N = prob.num_elems, prob.num_nodes
     stream = torch.cuda.Stream(device=dev)
     res = {}
-    kernel_ms = {}
-    launches = {}
     model = ExplicitDynamics(prob.coords, prob.parts, prob.bcs, stream=stream.cuda_stream)
+    layout = model.layout()
     hbm_peak, peak_kind = measured_peaks()
-    clocks = None
     for prec in ("fp64", "mixed"):
-        model.set_state(None, prob.v0)
-        model.init_acceleration(prec)
-        model.run(args.warmup, prob.dt, prec)
-        torch.cuda.synchronize(dev)
-        barrier(world)
-        model.profile(True)
-        n0 = model.launch_count()
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        sampler = ClockSampler(local)
-        with sampler:
-            torch.cuda.synchronize(dev)
-            ev0.record(stream)
-            model.run(args.steps, prob.dt, prec, t0=args.warmup * prob.dt)
-            ev1.record(stream)
-            torch.cuda.synchronize(dev)
-        ms = ev0.elapsed_time(ev1)
-        launches[prec] = model.launch_count() - n0
-        kms, kn = model.profile_read()  # per-kernel events recorded inside the timed region
-        model.profile(False)
-        kernel_ms[prec] = {"element": kms[0] / max(kn[0], 1), "node": kms[1] / max(kn[1], 1),
-                           "element_total": kms[0], "node_total": kms[1]}
-        ms = max_over_ranks(ms, world)
-        res[prec] = {"ms": ms, "value": world * E * args.steps / (ms * 1e-3) / 1e6}
-        if prec == "mixed":
-            clocks = sampler.summary()
+        res[prec] = time_run(torch, model, prob, args.steps, args.warmup, prec, stream, dev, world,
+                             sampler_index=local if prec == "mixed" else None)
         res[prec]["state"] = model.get_state()
     # accuracy of the mixed path against the FP64 path (itself 1e-12 from the oracle)
     u64, um = res["fp64"]["state"][0], res["mixed"]["state"][0]
@@ -228,8 +323,7 @@ def run_ours(args, rank, world, local):
         torch.cuda.synchronize(dev)
         barrier(world)
         t0 = time.perf_counter()
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0, ev1 = _events(torch)
         ev0.record(stream)
         model.set_state(u_h.numpy(), v_h.numpy())
         model.init_acceleration("mixed")
@@ -244,55 +338,36 @@ def run_ours(args, rank, world, local):
                "ms": ms_e2e, "path": "ExplicitDynamics.set_state/init_acceleration/run/get_state (C ABI, host buffers)"}
     model.close()
 
-    # adjoint / forward cost (Hex8 neo-Hookean 64^3 with a lognormal shear field)
+    roofline = roofline_for(res["mixed"]["kernels"], algorithmic_bytes(prob, layout), hbm_peak, peak_kind)
+    roofline["layout"] = layout
+
+    # the other configurations, each on its own context
+    extras = {}
+    if not args.skip_extras:
+        p1 = problems.hex8_le_cube(n=20, seed=0, nsteps=100)
+        extras["hex8_le_cube_20"] = measure_workload(torch, p1, 100, args.warmup, stream, dev, world)
+        p3a = problems.smoothed_tet4_box(n=args.box_n, seed=0, nsteps=500)
+        extras["smoothed_tet4_box"] = measure_workload(torch, p3a, 500, args.warmup, stream, dev, world,
+                                                       mass=p3a.meta["mass"])
+        for cap in (40, 80):
+            t0 = time.perf_counter()
+            p3b = problems.rkpm_box(n=args.box_n, seed=0, nsteps=500, max_neighbors=cap)
+            setup_s = time.perf_counter() - t0
+            r = measure_workload(torch, p3b, 500, args.warmup, stream, dev, world, mass=p3b.meta["mass"])
+            r["setup_s"] = setup_s
+            r["entries_per_cell"] = p3b.meta["entries_per_cell"]
+            extras[f"rkpm_box_cap{cap}"] = r
+        p5 = problems.hex8_nh_lognormal(n=args.hex_n, seed=0, nsteps=1000, bulk_field=True)
+        extras["hex8_nh_lognormal_large"] = measure_workload(torch, p5, 1000, args.warmup, stream, dev, world)
+        if not args.skip_adjoint:
+            extras["hex8_nh_lognormal_large"]["adjoint"] = run_adjoint(torch, p5, 50, stream, dev)
+
     adj = None
     if not args.skip_adjoint:
-        pa = problems.hex8_nh_lognormal(n=args.adjoint_n, seed=0, nsteps=200)
-        with ExplicitDynamics(pa.coords, pa.parts, pa.bcs, stream=stream.cuda_stream) as ma:
-            times = {}
-            for rep in range(2):
-                ma.set_state(None, pa.v0)
-                torch.cuda.synchronize(dev)
-                a0 = torch.cuda.Event(enable_timing=True)
-                a1 = torch.cuda.Event(enable_timing=True)
-                a0.record(stream)
-                ma.init_acceleration()
-                ma.run(pa.nsteps, pa.dt)
-                a1.record(stream)
-                torch.cuda.synchronize(dev)
-                times["forward"] = a0.elapsed_time(a1)
-                ma.set_state(None, pa.v0)
-                torch.cuda.synchronize(dev)
-                ma.profile(rep == 1)
-                a0.record(stream)
-                loss, gm, gk = ma.adjoint(pa.nsteps, pa.dt, 20, pa.meta["sensors"])
-                a1.record(stream)
-                torch.cuda.synchronize(dev)
-                times["adjoint"] = a0.elapsed_time(a1)
-            pms, pn = ma.profile_read()
-            ma.profile(False)
-        adj = {"workload": f"hex8_nh_lognormal_{args.adjoint_n}", "steps": pa.nsteps, "ckpt_every": 20,
-               "forward_ms": times["forward"], "adjoint_ms": times["adjoint"],
-               "ratio": times["adjoint"] / times["forward"],
-               "kernel_ms": {"element": pms[0], "node": pms[1], "vjp": pms[2], "adjoint_node": pms[3]},
-               "kernel_launches": {"element": pn[0], "node": pn[1], "vjp": pn[2], "adjoint_node": pn[3]}}
-
-    # roofline of the dominant kernel of the headline (mixed) run
-    km = kernel_ms["mixed"]
-    dominant = "node" if km["node_total"] >= km["element_total"] else "element"
-    # Algorithmic bytes per launch (compulsory traffic, each array touched once):
-    #  element kernel (Tet4, mixed): conn 16 B + coordinates and displacement of the
-    #    element's share of nodes (N/E x 2 x 24 B) + its four FP32 force slots (48 B);
-    #  node kernel: its slots (S/N x (4 B index + 12 B FP32 force)) + mass 8 B +
-    #    BC word 4 B + displacement and half-step velocity read and written (4 x 24 B).
-    S = E * 4
-    alg = {"element": E * (16 + 48) + N * 48, "node": S * (4 + 12) + N * (8 + 4 + 96)}
-    ms_launch = km[dominant]
-    achieved = alg[dominant] / (ms_launch * 1e-3) / 1e9
-    roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak, "peak_source": peak_kind, "traffic": None,
-                "algorithmic_bytes_per_launch": alg[dominant], "ms_per_launch": ms_launch}
-    return prob, res, disp_err, force_err, e2e, adj, roofline, kernel_ms, launches, clocks
+        adj = run_adjoint(torch, problems.hex8_nh_lognormal(n=args.adjoint_n, seed=0, nsteps=200), 20, stream, dev)
+    kernel_ms = {p: res[p]["kernels"] for p in ("fp64", "mixed")}
+    launches = {p: res[p]["launches"] for p in ("fp64", "mixed")}
+    return prob, res, disp_err, force_err, e2e, adj, roofline, kernel_ms, launches, res["mixed"]["clocks"], extras
 
 
 def cpu_baseline(target_s=10.0, n=24):
@@ -354,7 +429,8 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
-    prob, res, disp_err, force_err, e2e, adj, roofline, kernel_ms, launches, clocks = run_ours(args, rank, world, local)
+    prob, res, disp_err, force_err, e2e, adj, roofline, kernel_ms, launches, clocks, extras = run_ours(
+        args, rank, world, local)
     if rank != 0:
         return
     cpu = None if args.skip_cpu else cpu_baseline()
@@ -378,6 +454,7 @@ def main():
         "e2e": e2e,
         "gpu_launches": launches["mixed"],
         "clocks": clocks,
+        "other_workloads": extras,
     }
     print(json.dumps(line), flush=True)
 
