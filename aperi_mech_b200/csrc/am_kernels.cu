@@ -66,9 +66,6 @@ __device__ __forceinline__ int hex_sign(int a, int j) {
     const int mask = (j == 0) ? 0x66 : (j == 1) ? 0xCC : 0xF0;
     return ((mask >> a) & 1) ? 1 : -1;
 }
-__host__ __device__ constexpr int hex_sign_c(int a, int j) {
-    return (((j == 0 ? 0x66 : j == 1 ? 0xCC : 0xF0) >> a) & 1) ? 1 : -1;
-}
 
 // ---------------------------------------------------------------------------
 // Tet4, 1-point Gauss: one thread per element.
@@ -305,103 +302,186 @@ __global__ void __launch_bounds__(256) k_tet4_hex6_force(GaussBlockDev b, const 
 }
 
 // ---------------------------------------------------------------------------
-// Hex8, 2x2x2 Gauss: eight lanes per element. Lane g loads node g, then acts as
-// Gauss point g (J, H, P, Q = w J^-1 P^T), then as node g again to sum its force
-// over the eight Q's. Shared memory carries the node data and the Q's between
-// the two phases; the node-phase sum runs over Gauss points in order.
+// Hex8, 2x2x2 Gauss in the monomial basis of the trilinear element: one thread
+// per element, everything in registers.
+//
+// Index the nodes by their corner bits (bit j set where xi_j = +1; node numbers
+// 0,1,3,2,4,5,7,6 in that order). A nodal field v then reads
+//   v(xi) = 1/8 sum_K C_K prod_{j in K} xi_j,   C_K = sum_a S_K(a) v_a,
+// with S_K(a) = prod_{j in K} (+-1 by corner bit j of a): three butterfly stages
+// give all eight C_K from the eight nodal values (hex_butterfly). The derivative
+// d v / d xi_j at a Gauss point xi = c sigma (c = 1/sqrt 3, sigma in {+-1}^3) is
+//   1/8 (C_j + c sigma_l C_jl + c sigma_m C_jm + c^2 sigma_l sigma_m C_jlm),
+// three additions once the C's carry their powers of c. The nodal forces
+//   f_a = -sum_g sum_j dN_a/dxi_j(g) Q_g[j,:],  Q_g = det J_g J_g^-1 P_g^T
+// regroup the same way: f_a = -1/8 sum_K S_K(a) R_K with R_K summed over the Gauss
+// points from the Q's, and an inverse butterfly turns the R_K into the eight nodal
+// forces. The Jacobians are built from 8x the true derivatives (the 1/8 is
+// dropped): H = G J^-1 is scale-free, Q = adj(J) P^T grows by 64, and the nodal
+// sum applies -1/512 once. Per element this is about half the arithmetic of
+// evaluating the 24 shape-function derivatives at every Gauss point.
 // ---------------------------------------------------------------------------
-template <typename T, int MAT>
-__global__ void __launch_bounds__(256) k_hex8_force(GaussBlockDev b, const double4* __restrict__ X4,
-                                                     const double4* __restrict__ U4, vec4_t<T>* __restrict__ slots,
-                                                     int* status) {
-    __shared__ T sh[32][120];
-    const int lane = threadIdx.x & 31;
-    const int g = lane & 7;
-    const int el = threadIdx.x >> 3;
-    const int64_t e = static_cast<int64_t>(blockIdx.x) * 32 + el;
-    const bool valid = e < b.num_elems;
-    const int32_t n = valid ? b.conn[e * 8 + g] : 0;
-    const double4 x = X4[n];
-    const double4 u = U4[n];
-    const int src = lane & ~7;
-    const double x0 = __shfl_sync(kFull, x.x, src), y0 = __shfl_sync(kFull, x.y, src), z0 = __shfl_sync(kFull, x.z, src);
-    const double ux0 = __shfl_sync(kFull, u.x, src), uy0 = __shfl_sync(kFull, u.y, src), uz0 = __shfl_sync(kFull, u.z, src);
-    T* s = sh[el];
-    s[g * 6 + 0] = T(x.x - x0);
-    s[g * 6 + 1] = T(x.y - y0);
-    s[g * 6 + 2] = T(x.z - z0);
-    s[g * 6 + 3] = T(u.x - ux0);
-    s[g * 6 + 4] = T(u.y - uy0);
-    s[g * 6 + 5] = T(u.z - uz0);
-    __syncwarp();
+// Gauss points unrolled two at a time: full unrolling raises the FP32 kernel to
+// 168 registers and spills the FP64 one; two keeps both in registers.
+constexpr int kHexGpUnroll = 2;
 
-    const T c = T(0.57735026918962576451);  // 1/sqrt(3)
-    T cp[3], cm[3], sg[3];
+__host__ __device__ constexpr int hex_node_of_corner(int q) { return q ^ ((q >> 1) & 1); }
+
+// v[K] <- sum_a S_K(a) v[a] (corner-bit order): C_0 in v[0], C_j in v[1 << j].
+template <typename T>
+__device__ __forceinline__ void hex_butterfly(T* v) {
 #pragma unroll
-    for (int j = 0; j < 3; ++j) {
-        sg[j] = T(hex_sign(g, j));
-        cp[j] = T(1) + sg[j] * c;
-        cm[j] = T(1) - sg[j] * c;
-    }
-    // ---- Gauss point g ----
-    T J[9], G[9];
+    for (int j = 0; j < 3; ++j)
 #pragma unroll
-    for (int k = 0; k < 9; ++k) {
-        J[k] = T(0);
-        G[k] = T(0);
-    }
-#pragma unroll
-    for (int a = 0; a < 8; ++a) {
-        const T f0 = hex_sign_c(a, 0) > 0 ? cp[0] : cm[0];
-        const T f1 = hex_sign_c(a, 1) > 0 ? cp[1] : cm[1];
-        const T f2 = hex_sign_c(a, 2) > 0 ? cp[2] : cm[2];
-        const T dN[3] = {T(0.125 * hex_sign_c(a, 0)) * f1 * f2, T(0.125 * hex_sign_c(a, 1)) * f0 * f2,
-                         T(0.125 * hex_sign_c(a, 2)) * f0 * f1};
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            const T xa = s[a * 6 + i], ua = s[a * 6 + 3 + i];
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                J[i * 3 + j] += xa * dN[j];
-                G[i * 3 + j] += ua * dN[j];
+        for (int p = 0; p < 8; ++p)
+            if (!((p >> j) & 1)) {
+                const int q = p | (1 << j);
+                const T sum = v[p] + v[q], dif = v[q] - v[p];
+                v[p] = sum;
+                v[q] = dif;
             }
-        }
+}
+
+// F[a] <- sum_K S_K(a) R[K] (the transpose of hex_butterfly).
+template <typename T>
+__device__ __forceinline__ void hex_butterfly_t(T* v) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int p = 0; p < 8; ++p)
+            if (!((p >> j) & 1)) {
+                const int q = p | (1 << j);
+                const T lo = v[p] - v[q], hi = v[p] + v[q];
+                v[p] = lo;
+                v[q] = hi;
+            }
+}
+
+// Scale the butterfly output by the powers of c the Gauss-point formula needs.
+template <typename T>
+__device__ __forceinline__ void hex_scale_coeffs(T* v) {
+    const T c = T(0.57735026918962576451), c2 = T(1.0 / 3.0);
+    v[3] *= c;
+    v[5] *= c;
+    v[6] *= c;
+    v[7] *= c2;
+}
+
+// 8 d v / d xi_j at the Gauss point of corner bits g (v scaled by hex_scale_coeffs).
+template <typename T>
+__device__ __forceinline__ T hex_dxi(const T* v, int j, int g) {
+    const int l = (j + 1) % 3, m = (j + 2) % 3;
+    const T sl = ((g >> l) & 1) ? T(1) : T(-1), sm = ((g >> m) & 1) ? T(1) : T(-1);
+    return v[1 << j] + sl * v[(1 << j) | (1 << l)] + sm * (v[(1 << j) | (1 << m)] + sl * v[7]);
+}
+
+// R_K += the Gauss point's share (Q row j = d/dxi_j part), before the c powers.
+template <typename T>
+__device__ __forceinline__ void hex_accumulate_r(T (*R)[8], const T* Q, int g) {
+    const T s0 = (g & 1) ? T(1) : T(-1), s1 = (g & 2) ? T(1) : T(-1), s2 = (g & 4) ? T(1) : T(-1);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const T q0 = Q[0 * 3 + i], q1 = Q[1 * 3 + i], q2 = Q[2 * 3 + i];
+        R[i][1] += q0;
+        R[i][2] += q1;
+        R[i][4] += q2;
+        R[i][3] += s1 * q0 + s0 * q1;
+        R[i][5] += s2 * q0 + s0 * q2;
+        R[i][6] += s2 * q1 + s1 * q2;
+        R[i][7] += s1 * s2 * q0 + s0 * s2 * q1 + s0 * s1 * q2;
     }
-    const T det = det3(J);
-    if (valid && !(det > T(0))) flag(status, AM_ENONPOS_J, e);
-    T Ji[9];
-    cof_inv3(J, Ji, det);
-    T H[9];
+}
+
+// Nodal values (corner-bit order) relative to node 0, FP64 difference then T.
+template <typename T>
+__device__ __forceinline__ void hex_load_rel(const double4* __restrict__ A, const int32_t* nd, T (*V)[8]) {
+    const double4 a0 = A[nd[0]];
+    V[0][0] = V[1][0] = V[2][0] = T(0);
+#pragma unroll
+    for (int q = 1; q < 8; ++q) {
+        const double4 a = A[nd[hex_node_of_corner(q)]];
+        V[0][q] = T(a.x - a0.x);
+        V[1][q] = T(a.y - a0.y);
+        V[2][q] = T(a.z - a0.z);
+    }
+}
+
+__device__ __forceinline__ void hex_conn(const GaussBlockDev& b, int64_t e, int32_t* nd) {
+    const int4 c0 = reinterpret_cast<const int4*>(b.conn)[2 * e], c1 = reinterpret_cast<const int4*>(b.conn)[2 * e + 1];
+    nd[0] = c0.x, nd[1] = c0.y, nd[2] = c0.z, nd[3] = c0.w, nd[4] = c1.x, nd[5] = c1.y, nd[6] = c1.z, nd[7] = c1.w;
+}
+
+// The FP32 kernel is held to 128 registers (four 128-thread blocks per SM); the
+// FP64 one keeps its ~250 registers: forcing three blocks per SM spills and was
+// slower on B200.
+template <typename T, int MAT>
+__global__ void __launch_bounds__(128, sizeof(T) == 8 ? 1 : 4) k_hex8_force(GaussBlockDev b, const double4* __restrict__ X4,
+                                                         const double4* __restrict__ U4,
+                                                         vec4_t<T>* __restrict__ slots, int* status) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= b.num_elems) return;
+    int32_t nd[8];
+    hex_conn(b, e, nd);
+    T X[3][8], U[3][8];
+    hex_load_rel(X4, nd, X);
+    hex_load_rel(U4, nd, U);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        hex_butterfly(X[i]);
+        hex_butterfly(U[i]);
+        hex_scale_coeffs(X[i]);
+        hex_scale_coeffs(U[i]);
+    }
+    double lam, mu;
+    element_lame(b, e, lam, mu);
+    T R[3][8];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) H[i * 3 + j] = G[i * 3 + 0] * Ji[0 * 3 + j] + G[i * 3 + 1] * Ji[1 * 3 + j] + G[i * 3 + 2] * Ji[2 * 3 + j];
-    double lam = 0.0, mu = 0.0;
-    if (valid) element_lame(b, e, lam, mu);
-    T P[9];
-    const double Jf = stress<T>(MAT, T(lam), T(mu), H, P);
-    if (valid && MAT == kNeoHookean && !(Jf > 0.0)) flag(status, AM_ENONPOS_J, e);
-    T* q = s + 48 + g * 9;
-#pragma unroll
-    for (int k = 0; k < 3; ++k)
+        for (int k = 0; k < 8; ++k) R[i][k] = T(0);
+    bool bad = false;
+#pragma unroll kHexGpUnroll
+    for (int g = 0; g < 8; ++g) {
+        T J[9], G[9], A[9];
 #pragma unroll
         for (int i = 0; i < 3; ++i)
-            q[k * 3 + i] = det * (Ji[k * 3 + 0] * P[i * 3 + 0] + Ji[k * 3 + 1] * P[i * 3 + 1] + Ji[k * 3 + 2] * P[i * 3 + 2]);
-    __syncwarp();
-    // ---- node g: f_g = -sum_gp dN_g(xi_gp) Q_gp ----
-    T fx = T(0), fy = T(0), fz = T(0);
 #pragma unroll
-    for (int gp = 0; gp < 8; ++gp) {
-        const T f0 = hex_sign_c(gp, 0) > 0 ? cp[0] : cm[0];
-        const T f1 = hex_sign_c(gp, 1) > 0 ? cp[1] : cm[1];
-        const T f2 = hex_sign_c(gp, 2) > 0 ? cp[2] : cm[2];
-        const T d0 = T(0.125) * sg[0] * f1 * f2, d1 = T(0.125) * sg[1] * f0 * f2, d2 = T(0.125) * sg[2] * f0 * f1;
-        const T* Q = s + 48 + gp * 9;
-        fx -= d0 * Q[0] + d1 * Q[3] + d2 * Q[6];
-        fy -= d0 * Q[1] + d1 * Q[4] + d2 * Q[7];
-        fz -= d0 * Q[2] + d1 * Q[5] + d2 * Q[8];
+            for (int j = 0; j < 3; ++j) {
+                J[i * 3 + j] = hex_dxi(X[i], j, g);
+                G[i * 3 + j] = hex_dxi(U[i], j, g);
+            }
+        adj3(J, A);
+        const T det = J[0] * A[0] + J[1] * A[3] + J[2] * A[6];
+        bad |= !(det > T(0));
+        const T id = recip(det);
+        T H[9], P[9];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+                H[i * 3 + j] = (G[i * 3 + 0] * A[0 * 3 + j] + G[i * 3 + 1] * A[1 * 3 + j] + G[i * 3 + 2] * A[2 * 3 + j]) * id;
+        const double Jf = stress<T>(MAT, T(lam), T(mu), H, P);
+        if (MAT == kNeoHookean) bad |= !(Jf > 0.0);
+        T Q[9];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                Q[k * 3 + i] = A[k * 3 + 0] * P[i * 3 + 0] + A[k * 3 + 1] * P[i * 3 + 1] + A[k * 3 + 2] * P[i * 3 + 2];
+        hex_accumulate_r(R, Q, g);
     }
-    if (valid) slots[b.slot_pos[e * 8 + g]] = make4(fx, fy, fz);
+    if (bad) flag(status, AM_ENONPOS_J, e);
+    const int4 p0 = reinterpret_cast<const int4*>(b.slot_pos)[2 * e], p1 = reinterpret_cast<const int4*>(b.slot_pos)[2 * e + 1];
+    const int32_t pos[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        R[i][0] = T(0);
+        hex_scale_coeffs(R[i]);
+        hex_butterfly_t(R[i]);
+    }
+    const T s = T(-1.0 / 512.0);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) slots[pos[hex_node_of_corner(q)]] = make4(s * R[0][q], s * R[1][q], s * R[2][q]);
 }
 
 // ---------------------------------------------------------------------------
@@ -641,102 +721,85 @@ __global__ void __launch_bounds__(256) k_tet4_patch_vjp(GaussBlockDev b, const d
     }
 }
 
+// VJP of the Hex8 forces in the monomial basis (see k_hex8_force): the
+// Gauss point's dP[grad lam] takes the place of P in the same regrouped nodal
+// sum, and the material-field contractions are summed over the Gauss points in
+// order. One thread per element, FP64.
 template <int MAT>
 __global__ void __launch_bounds__(128) k_hex8_vjp(GaussBlockDev b, const double4* __restrict__ X4,
-                                                   const double4* __restrict__ U4, const double4* __restrict__ L4,
-                                                   double4* __restrict__ slots, double* gmu, double* gk,
-                                                   int accumulate) {
-    __shared__ double sh[16][144];
-    const int lane = threadIdx.x & 31;
-    const int g = lane & 7;
-    const int el = threadIdx.x >> 3;
-    const int64_t e = static_cast<int64_t>(blockIdx.x) * 16 + el;
-    const bool valid = e < b.num_elems;
-    const int32_t n = valid ? b.conn[e * 8 + g] : 0;
-    const double4 x = X4[n], u = U4[n], l = L4[n];
-    const int src = lane & ~7;
-    double* s = sh[el];
-    s[g * 9 + 0] = x.x - __shfl_sync(kFull, x.x, src);
-    s[g * 9 + 1] = x.y - __shfl_sync(kFull, x.y, src);
-    s[g * 9 + 2] = x.z - __shfl_sync(kFull, x.z, src);
-    s[g * 9 + 3] = u.x - __shfl_sync(kFull, u.x, src);
-    s[g * 9 + 4] = u.y - __shfl_sync(kFull, u.y, src);
-    s[g * 9 + 5] = u.z - __shfl_sync(kFull, u.z, src);
-    s[g * 9 + 6] = l.x - __shfl_sync(kFull, l.x, src);
-    s[g * 9 + 7] = l.y - __shfl_sync(kFull, l.y, src);
-    s[g * 9 + 8] = l.z - __shfl_sync(kFull, l.z, src);
-    __syncwarp();
-    const double c = 0.57735026918962576451;
-    double cp[3], cm[3], sg[3];
+                                                       const double4* __restrict__ U4, const double4* __restrict__ L4,
+                                                       double4* __restrict__ slots, double* gmu, double* gk,
+                                                       int accumulate) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= b.num_elems) return;
+    int32_t nd[8];
+    hex_conn(b, e, nd);
+    double X[3][8], U[3][8], W[3][8];
+    hex_load_rel(X4, nd, X);
+    hex_load_rel(U4, nd, U);
+    hex_load_rel(L4, nd, W);
 #pragma unroll
-    for (int j = 0; j < 3; ++j) {
-        sg[j] = hex_sign(g, j);
-        cp[j] = 1.0 + sg[j] * c;
-        cm[j] = 1.0 - sg[j] * c;
+    for (int i = 0; i < 3; ++i) {
+        hex_butterfly(X[i]);
+        hex_butterfly(U[i]);
+        hex_butterfly(W[i]);
+        hex_scale_coeffs(X[i]);
+        hex_scale_coeffs(U[i]);
+        hex_scale_coeffs(W[i]);
     }
-    double J[9], G[9], GL[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) J[k] = G[k] = GL[k] = 0.0;
-#pragma unroll
-    for (int a = 0; a < 8; ++a) {
-        const double f0 = hex_sign_c(a, 0) > 0 ? cp[0] : cm[0];
-        const double f1 = hex_sign_c(a, 1) > 0 ? cp[1] : cm[1];
-        const double f2 = hex_sign_c(a, 2) > 0 ? cp[2] : cm[2];
-        const double dN[3] = {0.125 * hex_sign_c(a, 0) * f1 * f2, 0.125 * hex_sign_c(a, 1) * f0 * f2,
-                              0.125 * hex_sign_c(a, 2) * f0 * f1};
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                J[i * 3 + j] += s[a * 9 + i] * dN[j];
-                G[i * 3 + j] += s[a * 9 + 3 + i] * dN[j];
-                GL[i * 3 + j] += s[a * 9 + 6 + i] * dN[j];
-            }
-    }
-    const double det = det3(J);
-    double Ji[9];
-    cof_inv3(J, Ji, det);
-    double H[9], L[9];
+    double lam, mu;
+    element_lame(b, e, lam, mu);
+    double R[3][8];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            H[i * 3 + j] = G[i * 3 + 0] * Ji[0 * 3 + j] + G[i * 3 + 1] * Ji[1 * 3 + j] + G[i * 3 + 2] * Ji[2 * 3 + j];
-            L[i * 3 + j] = GL[i * 3 + 0] * Ji[0 * 3 + j] + GL[i * 3 + 1] * Ji[1 * 3 + j] + GL[i * 3 + 2] * Ji[2 * 3 + j];
-        }
-    double lam = 0.0, mu = 0.0;
-    if (valid) element_lame(b, e, lam, mu);
-    double dP[9], ldl, ldm;
-    stress_vjp(MAT, lam, mu, H, L, dP, &ldl, &ldm);
-    double tm = -det * (ldm - 2.0 / 3.0 * ldl), tk = -det * ldl;
-    double* q = s + 72 + g * 9;
-#pragma unroll
-    for (int k = 0; k < 3; ++k)
+        for (int k = 0; k < 8; ++k) R[i][k] = 0.0;
+    double tm = 0.0, tk = 0.0;
+#pragma unroll 1
+    for (int g = 0; g < 8; ++g) {
+        double J[9], A[9], H[9], L[9];
 #pragma unroll
         for (int i = 0; i < 3; ++i)
-            q[k * 3 + i] = det * (Ji[k * 3 + 0] * dP[i * 3 + 0] + Ji[k * 3 + 1] * dP[i * 3 + 1] + Ji[k * 3 + 2] * dP[i * 3 + 2]);
 #pragma unroll
-    for (int off = 4; off > 0; off >>= 1) {
-        tm += __shfl_xor_sync(kFull, tm, off);
-        tk += __shfl_xor_sync(kFull, tk, off);
-    }
-    __syncwarp();
-    double fx = 0.0, fy = 0.0, fz = 0.0;
+            for (int j = 0; j < 3; ++j) J[i * 3 + j] = hex_dxi(X[i], j, g);
+        adj3(J, A);
+        const double det = J[0] * A[0] + J[1] * A[3] + J[2] * A[6];
+        const double id = 1.0 / det;
 #pragma unroll
-    for (int gp = 0; gp < 8; ++gp) {
-        const double f0 = hex_sign_c(gp, 0) > 0 ? cp[0] : cm[0];
-        const double f1 = hex_sign_c(gp, 1) > 0 ? cp[1] : cm[1];
-        const double f2 = hex_sign_c(gp, 2) > 0 ? cp[2] : cm[2];
-        const double d0 = 0.125 * sg[0] * f1 * f2, d1 = 0.125 * sg[1] * f0 * f2, d2 = 0.125 * sg[2] * f0 * f1;
-        const double* Q = s + 72 + gp * 9;
-        fx -= d0 * Q[0] + d1 * Q[3] + d2 * Q[6];
-        fy -= d0 * Q[1] + d1 * Q[4] + d2 * Q[7];
-        fz -= d0 * Q[2] + d1 * Q[5] + d2 * Q[8];
+        for (int i = 0; i < 3; ++i) {
+            const double g0 = hex_dxi(U[i], 0, g), g1 = hex_dxi(U[i], 1, g), g2 = hex_dxi(U[i], 2, g);
+            const double l0 = hex_dxi(W[i], 0, g), l1 = hex_dxi(W[i], 1, g), l2 = hex_dxi(W[i], 2, g);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                H[i * 3 + j] = (g0 * A[0 * 3 + j] + g1 * A[1 * 3 + j] + g2 * A[2 * 3 + j]) * id;
+                L[i * 3 + j] = (l0 * A[0 * 3 + j] + l1 * A[1 * 3 + j] + l2 * A[2 * 3 + j]) * id;
+            }
+        }
+        double dP[9], ldl, ldm;
+        stress_vjp(MAT, lam, mu, H, L, dP, &ldl, &ldm);
+        const double w = det * (1.0 / 512.0);
+        tm -= w * (ldm - 2.0 / 3.0 * ldl);
+        tk -= w * ldl;
+        double Q[9];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                Q[k * 3 + i] = A[k * 3 + 0] * dP[i * 3 + 0] + A[k * 3 + 1] * dP[i * 3 + 1] + A[k * 3 + 2] * dP[i * 3 + 2];
+        hex_accumulate_r(R, Q, g);
     }
-    if (valid) {
-        slots[b.slot_pos[e * 8 + g]] = make4(fx, fy, fz);
-        if (g == 0) store_theta(gmu, gk, e, tm, tk, accumulate);
+    const int4 p0 = reinterpret_cast<const int4*>(b.slot_pos)[2 * e], p1 = reinterpret_cast<const int4*>(b.slot_pos)[2 * e + 1];
+    const int32_t pos[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        R[i][0] = 0.0;
+        hex_scale_coeffs(R[i]);
+        hex_butterfly_t(R[i]);
     }
+    const double s = -1.0 / 512.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) slots[pos[hex_node_of_corner(q)]] = make4(s * R[0][q], s * R[1][q], s * R[2][q]);
+    store_theta(gmu, gk, e, tm, tk, accumulate);
 }
 
 template <int MAT>
@@ -1244,11 +1307,11 @@ void launch_gauss_force(const GaussBlockDev& b, int mixed, const double4* X4, co
             AM_DISPATCH_MAT(b.material, (k_tet4_force<double, M><<<grid, 256, 0, s>>>(b, X4, U4, static_cast<double4*>(slots), status)));
         }
     } else {
-        const unsigned grid = grid_for(b.num_elems, 32);
+        const unsigned grid = grid_for(b.num_elems, 128);
         if (mixed) {
-            AM_DISPATCH_MAT(b.material, (k_hex8_force<float, M><<<grid, 256, 0, s>>>(b, X4, U4, static_cast<float4*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (k_hex8_force<float, M><<<grid, 128, 0, s>>>(b, X4, U4, static_cast<float4*>(slots), status)));
         } else {
-            AM_DISPATCH_MAT(b.material, (k_hex8_force<double, M><<<grid, 256, 0, s>>>(b, X4, U4, static_cast<double4*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (k_hex8_force<double, M><<<grid, 128, 0, s>>>(b, X4, U4, static_cast<double4*>(slots), status)));
         }
     }
 }
@@ -1282,7 +1345,7 @@ void launch_gauss_vjp(const GaussBlockDev& b, const double4* X4, const double4* 
         const unsigned grid = grid_for(b.num_elems, 256);
         AM_DISPATCH_MAT(b.material, (k_tet4_vjp<M><<<grid, 256, 0, s>>>(b, X4, U4, L4, slots, gmu, gkappa, accumulate)));
     } else {
-        const unsigned grid = grid_for(b.num_elems, 16);
+        const unsigned grid = grid_for(b.num_elems, 128);
         AM_DISPATCH_MAT(b.material, (k_hex8_vjp<M><<<grid, 128, 0, s>>>(b, X4, U4, L4, slots, gmu, gkappa, accumulate)));
     }
 }

@@ -34,6 +34,20 @@ __device__ __forceinline__ T cof_inv3(const T* m, T* r, T det) {
     return det;
 }
 
+// r = adj(m) (the transposed cofactor matrix): m r = det(m) I.
+template <typename T>
+__device__ __forceinline__ void adj3(const T* m, T* r) {
+    r[0] = m[4] * m[8] - m[5] * m[7];
+    r[1] = m[2] * m[7] - m[1] * m[8];
+    r[2] = m[1] * m[5] - m[2] * m[4];
+    r[3] = m[5] * m[6] - m[3] * m[8];
+    r[4] = m[0] * m[8] - m[2] * m[6];
+    r[5] = m[2] * m[3] - m[0] * m[5];
+    r[6] = m[3] * m[7] - m[4] * m[6];
+    r[7] = m[1] * m[6] - m[0] * m[7];
+    r[8] = m[0] * m[4] - m[1] * m[3];
+}
+
 template <typename T>
 __device__ __forceinline__ T det3(const T* m) {
     return m[0] * (m[4] * m[8] - m[5] * m[7]) + m[1] * (m[5] * m[6] - m[3] * m[8]) + m[2] * (m[3] * m[7] - m[4] * m[6]);
@@ -142,40 +156,38 @@ __device__ __forceinline__ void stress_vjp(int32_t mat, double lambda, double mu
         return;
     }
     if (mat == kNeoHookean) {
+        // P = mu (F - F^-T) + lambda log J F^-T, so with d(F^-T) = -F^-T L^T F^-T:
+        //   dP = mu L + (mu - lambda log J) F^-T L^T F^-T + lambda tr(F^-1 L) F^-T
+        //   L : dP/dlambda = log J tr(F^-1 L),  L : dP/dmu = L : (F - F^-T)
         const double Jm1 = det_ap_im1(H);
         const double lnJ = log1p(Jm1);
         double Fi[9];
         cof_inv3(F, Fi, 1.0 + Jm1);
-        // dtau = lambda tr(F^-1 L) I + mu (L F^T + F L^T) ; dP = dtau F^-T - P L^T F^-T
         double trFiL = 0.0;
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
             for (int k = 0; k < 3; ++k) trFiL += Fi[i * 3 + k] * L[k * 3 + i];
-        double P[9];
-        stress<double>(kNeoHookean, lambda, mu, H, P);
-        double M[9];  // M = dtau - P L^T
+        // T1 = L^T F^-T : T1_kj = sum_m L_mk Fi_jm ; then (F^-T T1)_ij = sum_k Fi_ki T1_kj
+        double T1[9];
 #pragma unroll
-        for (int i = 0; i < 3; ++i)
+        for (int k = 0; k < 3; ++k)
 #pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                double s = 0.0;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) s += mu * (L[i * 3 + k] * F[j * 3 + k] + F[i * 3 + k] * L[j * 3 + k]) - P[i * 3 + k] * L[j * 3 + k];
-                M[i * 3 + j] = s + (i == j ? lambda * trFiL : 0.0);
-            }
-        double sl = 0.0, sm = 0.0;
+            for (int j = 0; j < 3; ++j)
+                T1[k * 3 + j] = L[0 * 3 + k] * Fi[j * 3 + 0] + L[1 * 3 + k] * Fi[j * 3 + 1] + L[2 * 3 + k] * Fi[j * 3 + 2];
+        const double a = mu - lambda * lnJ, bt = lambda * trFiL;
+        double sm = 0.0;
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
             for (int j = 0; j < 3; ++j) {
                 const int k = i * 3 + j;
-                dP[k] = M[i * 3 + 0] * Fi[j * 3 + 0] + M[i * 3 + 1] * Fi[j * 3 + 1] + M[i * 3 + 2] * Fi[j * 3 + 2];
                 const double FiT = Fi[j * 3 + i];
-                sl += L[k] * lnJ * FiT;
+                const double t = Fi[0 * 3 + i] * T1[0 * 3 + j] + Fi[1 * 3 + i] * T1[1 * 3 + j] + Fi[2 * 3 + i] * T1[2 * 3 + j];
+                dP[k] = mu * L[k] + a * t + bt * FiT;
                 sm += L[k] * (F[k] - FiT);
             }
-        *l_dlam = sl;
+        *l_dlam = lnJ * trFiL;
         *l_dmu = sm;
         return;
     }

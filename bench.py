@@ -46,6 +46,10 @@ def parse():
     ap.add_argument("--adjoint-n", type=int, default=64)
     ap.add_argument("--box-n", type=int, default=46, help="lattice cells per unit length of the 1x1x2 box workloads")
     ap.add_argument("--hex-n", type=int, default=128, help="hexes per edge of the large Hex8 workload")
+    ap.add_argument("--workload", default="tet4_nh_shear",
+                    choices=["tet4_nh_shear", "hex8_nh_lognormal", "hex8_le_cube", "smoothed_tet4_box", "rkpm_box"],
+                    help="workload of the headline timing (the default is the headline configuration; the others "
+                         "exist to profile one kernel at a time)")
     ap.add_argument("--skip-extras", action="store_true")
     ap.add_argument("--skip-adjoint", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
@@ -99,27 +103,66 @@ def max_over_ranks(x, world):
 
 # ---------------------------------------------------------------------------
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during a region."""
+    """SM clock and clock-event (throttle) reasons sampled during a region: NVML
+    polled every 10 ms from a thread (read-only queries), with one sample at entry
+    and one at exit so that short regions still get a record; nvidia-smi at 200 ms
+    if NVML cannot be loaded."""
 
+    BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index: int):
-        self.index = str(index)
+        self.uuid = None
         try:
             import torch
 
             uuid = str(torch.cuda.get_device_properties(index).uuid)
-            self.index = uuid if uuid.startswith("GPU-") else f"GPU-{uuid}"
+            self.uuid = uuid if uuid.startswith("GPU-") else f"GPU-{uuid}"
         except Exception:
             pass
-        self.proc = None
+        self.index = index
+        self.samples = []  # (sm_mhz, max_mhz, reasons bitmask)
         self.lines = []
+        self.proc = None
+        self.nvml = None
+        self.stop = threading.Event()
+
+    def _nvml_sample(self):
+        n = self.nvml
+        sm = n.nvmlDeviceGetClockInfo(self.h, n.NVML_CLOCK_SM)
+        mx = n.nvmlDeviceGetMaxClockInfo(self.h, n.NVML_CLOCK_SM)
+        try:
+            r = n.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+        except AttributeError:
+            r = n.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+        self.samples.append((float(sm), float(mx), int(r)))
+
+    def _poll(self):
+        while not self.stop.wait(0.01):
+            try:
+                self._nvml_sample()
+            except Exception:
+                return
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+            import pynvml
+
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.h = (pynvml.nvmlDeviceGetHandleByUUID(self.uuid) if self.uuid
+                      else pynvml.nvmlDeviceGetHandleByIndex(self.index))
+            self._nvml_sample()
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nvml = None
+        try:
+            ident = self.uuid or str(self.index)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={ident}", f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
@@ -133,6 +176,14 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *exc):
+        if self.nvml is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
+            try:
+                self._nvml_sample()
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -142,6 +193,10 @@ class ClockSampler:
 
     def summary(self):
         sm, smax, reasons = [], [], set()
+        for s, m, bits in self.samples:
+            sm.append(s)
+            smax.append(m)
+            reasons.update(name for name, b in self.BITS.items() if bits & b)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
             parts = [p.strip() for p in ln.split(",")]
@@ -158,7 +213,7 @@ class ClockSampler:
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvml" if self.samples else "nvidia-smi"}
 
 
 def measured_peaks():
@@ -288,6 +343,21 @@ def run_adjoint(torch, pa, ckpt, stream, dev):
             "kernel_launches": {"element": pn[0], "node": pn[1], "vjp": pn[2], "adjoint_node": pn[3]}}
 
 
+def make_problem(args):
+    from aperi_mech_b200 import problems
+
+    w = args.workload
+    if w == "tet4_nh_shear":
+        return problems.tet4_nh_shear(n=args.n, seed=0, nsteps=args.steps)
+    if w == "hex8_nh_lognormal":
+        return problems.hex8_nh_lognormal(n=args.hex_n, seed=0, nsteps=args.steps, bulk_field=True)
+    if w == "hex8_le_cube":
+        return problems.hex8_le_cube(n=20, seed=0, nsteps=args.steps)
+    if w == "smoothed_tet4_box":
+        return problems.smoothed_tet4_box(n=args.box_n, seed=0, nsteps=args.steps)
+    return problems.rkpm_box(n=args.box_n, seed=0, nsteps=args.steps)
+
+
 def run_ours(args, rank, world, local):
     import torch
 
@@ -295,11 +365,12 @@ def run_ours(args, rank, world, local):
     from aperi_mech_b200.model import ExplicitDynamics
 
     dev = torch.device("cuda", local)
-    prob = problems.tet4_nh_shear(n=args.n, seed=0, nsteps=args.steps)
+    prob = make_problem(args)
     E, N = prob.num_elems, prob.num_nodes
     stream = torch.cuda.Stream(device=dev)
     res = {}
-    model = ExplicitDynamics(prob.coords, prob.parts, prob.bcs, stream=stream.cuda_stream)
+    model = ExplicitDynamics(prob.coords, prob.parts, prob.bcs, mass=prob.meta.get("mass"),
+                             stream=stream.cuda_stream)
     layout = model.layout()
     hbm_peak, peak_kind = measured_peaks()
     for prec in ("fp64", "mixed"):
@@ -349,14 +420,13 @@ def run_ours(args, rank, world, local):
         p3a = problems.smoothed_tet4_box(n=args.box_n, seed=0, nsteps=500)
         extras["smoothed_tet4_box"] = measure_workload(torch, p3a, 500, args.warmup, stream, dev, world,
                                                        mass=p3a.meta["mass"])
-        for cap in (40, 80):
-            t0 = time.perf_counter()
-            p3b = problems.rkpm_box(n=args.box_n, seed=0, nsteps=500, max_neighbors=cap)
-            setup_s = time.perf_counter() - t0
-            r = measure_workload(torch, p3b, 500, args.warmup, stream, dev, world, mass=p3b.meta["mass"])
-            r["setup_s"] = setup_s
-            r["entries_per_cell"] = p3b.meta["entries_per_cell"]
-            extras[f"rkpm_box_cap{cap}"] = r
+        t0 = time.perf_counter()
+        p3b = problems.rkpm_box(n=args.box_n, seed=0, nsteps=500)
+        setup_s = time.perf_counter() - t0
+        r = measure_workload(torch, p3b, 500, args.warmup, stream, dev, world, mass=p3b.meta["mass"])
+        r["setup_s"] = setup_s
+        r["entries_per_cell"] = p3b.meta["entries_per_cell"]
+        extras["rkpm_box"] = r
         p5 = problems.hex8_nh_lognormal(n=args.hex_n, seed=0, nsteps=1000, bulk_field=True)
         extras["hex8_nh_lognormal_large"] = measure_workload(torch, p5, 1000, args.warmup, stream, dev, world)
         if not args.skip_adjoint:
@@ -439,8 +509,9 @@ def main():
         "metric": METRIC, "value": res["mixed"]["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "elements": prob.num_elems, "nodes": prob.num_nodes,
-                   "element": "Tet4 1-pt Gauss", "material": "neo-Hookean mu=3.85e8 kappa=8.33e8",
+        "config": {"workload": prob.name, "elements": prob.num_elems, "nodes": prob.num_nodes,
+                   "description": prob.meta.get("config"), "material": "neo-Hookean mu=3.85e8 kappa=8.33e8"
+                   if "nh" in prob.name or "box" in prob.name else "linear elastic E=1e9 nu=0.3",
                    "dt": prob.dt, "seed": prob.seed,
                    "l2_flush": "inputs larger than L2 (state + slots + connectivity ~ 230 MB per step)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
