@@ -243,6 +243,7 @@ struct am_ctx {
         nd.g[1] = g[1];
         nd.g[2] = g[2];
         nd.has_g = (g[0] != 0.0 || g[1] != 0.0 || g[2] != 0.0) ? 1 : 0;
+        nd.num_slots = num_used_slots;
         return nd;
     }
 

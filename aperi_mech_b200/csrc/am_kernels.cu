@@ -927,33 +927,31 @@ __global__ void k_gauss_volume_slots(GaussBlockDev b, double density, const doub
 // ---------------------------------------------------------------------------
 // Sum of node i's slots: a contiguous node-major range, summed in ascending
 // logical-slot order (FP64 accumulation for both slot types).
-template <typename S>
+constexpr int kNodeBlock = 256;
+
+// Node-centric gather of a node's force slots (node-major, contiguous), summed in
+// FP64 in slot order. BATCH loads are issued before the first add. A node of a hex
+// mesh, or of the split-hex tet patches, has at most eight slots, so BATCH = 8
+// takes every slot in one round; that wins when the slot array sits in L2 (the
+// loads are latency-bound), while BATCH = 4 keeps more warps resident, which wins
+// when the slots stream from HBM (see gather_batch8).
+template <typename S, int BATCH>
 __device__ __forceinline__ void gather(const NodeDev& nd, const vec4_t<S>* __restrict__ slots, int64_t i, double& fx,
                                        double& fy, double& fz) {
     const int32_t p0 = nd.node_ptr[i], p1 = nd.node_ptr[i + 1];
     fx = fy = fz = 0.0;
-    int32_t p = p0;
-    // Four independent loads in flight, then the sums in slot order.
-    for (; p + 4 <= p1; p += 4) {
-        const vec4_t<S> a = slots[p], b = slots[p + 1], c = slots[p + 2], d = slots[p + 3];
-        fx += static_cast<double>(a.x);
-        fy += static_cast<double>(a.y);
-        fz += static_cast<double>(a.z);
-        fx += static_cast<double>(b.x);
-        fy += static_cast<double>(b.y);
-        fz += static_cast<double>(b.z);
-        fx += static_cast<double>(c.x);
-        fy += static_cast<double>(c.y);
-        fz += static_cast<double>(c.z);
-        fx += static_cast<double>(d.x);
-        fy += static_cast<double>(d.y);
-        fz += static_cast<double>(d.z);
-    }
-    for (; p < p1; ++p) {
-        const vec4_t<S> v = slots[p];
-        fx += static_cast<double>(v.x);
-        fy += static_cast<double>(v.y);
-        fz += static_cast<double>(v.z);
+    for (int32_t p = p0; p < p1; p += BATCH) {
+        vec4_t<S> v[BATCH];
+#pragma unroll
+        for (int k = 0; k < BATCH; ++k)
+            if (p + k < p1) v[k] = slots[p + k];
+#pragma unroll
+        for (int k = 0; k < BATCH; ++k)
+            if (p + k < p1) {
+                fx += static_cast<double>(v[k].x);
+                fy += static_cast<double>(v[k].y);
+                fz += static_cast<double>(v[k].z);
+            }
     }
 }
 
@@ -984,13 +982,13 @@ __device__ __forceinline__ void free_mask(uint32_t word, uint32_t active, double
     mz = ((word >> 20) & 0x3FFu & active) ? 0.0 : 1.0;
 }
 
-template <typename S>
-__global__ void __launch_bounds__(256) k_gather_force(NodeDev nd, const vec4_t<S>* __restrict__ slots,
-                                                       double* __restrict__ f, int accumulate) {
+template <typename S, int BATCH>
+__global__ void __launch_bounds__(kNodeBlock) k_gather_force(NodeDev nd, const vec4_t<S>* __restrict__ slots,
+                                                              double* __restrict__ f, int accumulate) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= nd.num_nodes) return;
     double fx, fy, fz;
-    gather<S>(nd, slots, i, fx, fy, fz);
+    gather<S, BATCH>(nd, slots, i, fx, fy, fz);
     if (accumulate) {
         f[3 * i + 0] += fx;
         f[3 * i + 1] += fy;
@@ -1002,13 +1000,13 @@ __global__ void __launch_bounds__(256) k_gather_force(NodeDev nd, const vec4_t<S
     }
 }
 
-template <typename S>
-__global__ void __launch_bounds__(256) k_init_accel(NodeDev nd, const vec4_t<S>* __restrict__ slots,
-                                                     double4* __restrict__ A4, int* status) {
+template <typename S, int BATCH>
+__global__ void __launch_bounds__(kNodeBlock) k_init_accel(NodeDev nd, const vec4_t<S>* __restrict__ slots,
+                                                            double4* __restrict__ A4, int* status) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= nd.num_nodes) return;
     double fx, fy, fz;
-    gather<S>(nd, slots, i, fx, fy, fz);
+    gather<S, BATCH>(nd, slots, i, fx, fy, fz);
     const double m = nd.mass[i];
     if (nd.has_g) {
         fx += nd.g[0] * m;
@@ -1039,17 +1037,21 @@ __global__ void __launch_bounds__(256) k_prologue(NodeDev nd, const StepParams* 
     if (u_copy) u_copy[i] = u;
 }
 
-template <typename S>
-__global__ void __launch_bounds__(256) k_node_step(NodeDev nd, const vec4_t<S>* __restrict__ slots,
-                                                    const StepParams* __restrict__ table, int64_t step, int advance,
-                                                    double4* __restrict__ U4, double4* __restrict__ V4,
-                                                    double4* __restrict__ A4, double4* __restrict__ u_copy,
-                                                    int* status) {
+template <typename S, int BATCH>
+__global__ void __launch_bounds__(kNodeBlock) k_node_step(NodeDev nd, const vec4_t<S>* __restrict__ slots,
+                                                           const StepParams* __restrict__ table, int64_t step,
+                                                           int advance, double4* __restrict__ U4,
+                                                           double4* __restrict__ V4, double4* __restrict__ A4,
+                                                           double4* __restrict__ u_copy, int* status) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= nd.num_nodes) return;
-    double fx, fy, fz;
-    gather<S>(nd, slots, i, fx, fy, fz);
+    // The node's own data is independent of the gather: issue its loads first.
     const double m = nd.mass[i];
+    const uint32_t w = nd.bcword[i];
+    const double4 vh = V4[i];
+    const double4 u0 = advance ? U4[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+    double fx, fy, fz;
+    gather<S, BATCH>(nd, slots, i, fx, fy, fz);
     if (nd.has_g) {
         fx += nd.g[0] * m;
         fy += nd.g[1] * m;
@@ -1057,12 +1059,10 @@ __global__ void __launch_bounds__(256) k_node_step(NodeDev nd, const vec4_t<S>* 
     }
     // a^{n+1} = f / m (ExplicitTimeIntegrator.h:247-283), then the acceleration BC at t^{n+1}.
     double ax = fx / m, ay = fy / m, az = fz / m;
-    const uint32_t w = nd.bcword[i];
     const StepParams& P = table[step];
     if (w) apply_bc(w, P.aact, P.ascale, nd.bcvalues, ax, ay, az);
     if (!isfinite(ax) || !isfinite(ay) || !isfinite(az)) flag(status, AM_ENAN, i);
     // v^{n+1} = v^{n+1/2} + dt/2 a^{n+1} (:329-364)
-    const double4 vh = V4[i];
     const double vx = vh.x + P.half * ax, vy = vh.y + P.half * ay, vz = vh.z + P.half * az;
     if (advance) {
         // Next step: v^{n+3/2} = v^{n+1} + dt'/2 a^{n+1} (:286-326), velocity BC at t_mid',
@@ -1070,7 +1070,7 @@ __global__ void __launch_bounds__(256) k_node_step(NodeDev nd, const vec4_t<S>* 
         const StepParams& Q = table[step + 1];
         double wx = vx + Q.half * ax, wy = vy + Q.half * ay, wz = vz + Q.half * az;
         if (w) apply_bc(w, Q.vact, Q.vscale, nd.bcvalues, wx, wy, wz);
-        double4 u = U4[i];
+        double4 u = u0;
         u.x = u.x + Q.dt * wx;
         u.y = u.y + Q.dt * wy;
         u.z = u.z + Q.dt * wz;
@@ -1100,14 +1100,14 @@ __global__ void k_adj_prep(NodeDev nd, const StepParams* __restrict__ table, int
 
 // Reverse of the rest of step `step` given g = (dF/du)^T lam in the slots; then
 // prepares lam for step-1 (or for the initial acceleration when step == 0).
-__global__ void __launch_bounds__(256) k_adj_update(NodeDev nd, const double4* __restrict__ slots,
-                                                     const StepParams* __restrict__ table, int64_t step,
-                                                     double4* __restrict__ UB, double4* __restrict__ VB,
-                                                     double4* __restrict__ AB, double4* __restrict__ L4) {
+__global__ void __launch_bounds__(kNodeBlock) k_adj_update(NodeDev nd, const double4* __restrict__ slots,
+                                                            const StepParams* __restrict__ table, int64_t step,
+                                                            double4* __restrict__ UB, double4* __restrict__ VB,
+                                                            double4* __restrict__ AB, double4* __restrict__ L4) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= nd.num_nodes) return;
     double gx, gy, gz;
-    gather<double>(nd, slots, i, gx, gy, gz);
+    gather<double, 4>(nd, slots, i, gx, gy, gz);
     const StepParams& P = table[step];
     double4 ub = UB[i];
     const double4 vb = VB[i];
@@ -1132,24 +1132,31 @@ __global__ void __launch_bounds__(256) k_adj_update(NodeDev nd, const double4* _
     }
 }
 
-// Loss L = sum_s |u_s|^2 and its cotangent 2 u_s, in sensor order (one thread).
-__global__ void k_sensor_seed(const double4* __restrict__ U4, int32_t num_sensors, const int32_t* __restrict__ sensors,
-                              double4* __restrict__ UB, double* loss) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+// Loss L = sum_s |u_s|^2 over the sensor list and its seed dL/du = 2 u_s added to UB
+// (UB is zero on entry). One block: each thread takes a strided share of the list,
+// the loss is summed by a fixed tree, so it is the same on every run. A node listed
+// twice receives 2u twice; sums of equal addends starting from zero do not depend
+// on their order, so the atomic adds are deterministic too.
+__global__ void __launch_bounds__(256) k_sensor_seed(const double4* __restrict__ U4, int32_t num_sensors,
+                                                     const int32_t* __restrict__ sensors, double4* __restrict__ UB,
+                                                     double* loss) {
+    __shared__ double part[256];
     double L = 0.0;
-    for (int32_t k = 0; k < num_sensors; ++k) {
+    for (int32_t k = threadIdx.x; k < num_sensors; k += blockDim.x) {
         const int32_t n = sensors[k];
         const double4 u = U4[n];
-        L += u.x * u.x;
-        L += u.y * u.y;
-        L += u.z * u.z;
-        double4 ub = UB[n];
-        ub.x += 2.0 * u.x;
-        ub.y += 2.0 * u.y;
-        ub.z += 2.0 * u.z;
-        UB[n] = ub;
+        L += u.x * u.x + u.y * u.y + u.z * u.z;
+        atomicAdd(&UB[n].x, 2.0 * u.x);
+        atomicAdd(&UB[n].y, 2.0 * u.y);
+        atomicAdd(&UB[n].z, 2.0 * u.z);
     }
-    *loss = L;
+    part[threadIdx.x] = L;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *loss = part[0];
 }
 
 __global__ void k_pack4(const double* __restrict__ in, double4* __restrict__ out, int64_t n) {
@@ -1366,20 +1373,39 @@ void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const dou
         k_gauss_volume_slots<<<grid_for(b.num_elems, 128), 128, 0, s>>>(b, density, X4, slots);
 }
 
+// BATCH = 8 when the slot array fits comfortably in L2 (126 MB on B200), else 4:
+// on B200 the eight-deep batch was ~10% faster for the 70^3 Tet4 mesh's 44 MB of
+// FP32 slots and ~5-10% slower for the 128^3 Hex8 mesh's 268 MB.
+inline bool gather_batch8(const NodeDev& nd, int mixed) {
+    const int64_t bytes = nd.num_slots * (mixed ? 16 : 32);
+    return bytes <= (int64_t{64} << 20);
+}
+
+#define AM_NODE_DISPATCH(KERNEL, ...)                                                    \
+    do {                                                                                 \
+        const unsigned grid = grid_for(nd.num_nodes, kNodeBlock);                        \
+        const bool b8 = gather_batch8(nd, mixed);                                        \
+        if (mixed) {                                                                     \
+            const float4* sl = static_cast<const float4*>(slots);                        \
+            if (b8)                                                                      \
+                KERNEL<float, 8><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);        \
+            else                                                                         \
+                KERNEL<float, 4><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);        \
+        } else {                                                                         \
+            const double4* sl = static_cast<const double4*>(slots);                      \
+            if (b8)                                                                      \
+                KERNEL<double, 8><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);       \
+            else                                                                         \
+                KERNEL<double, 4><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);       \
+        }                                                                                \
+    } while (0)
+
 void launch_gather_force(const NodeDev& nd, int mixed, const void* slots, double* f, int accumulate, cudaStream_t s) {
-    const unsigned grid = grid_for(nd.num_nodes, 256);
-    if (mixed)
-        k_gather_force<float><<<grid, 256, 0, s>>>(nd, static_cast<const float4*>(slots), f, accumulate);
-    else
-        k_gather_force<double><<<grid, 256, 0, s>>>(nd, static_cast<const double4*>(slots), f, accumulate);
+    AM_NODE_DISPATCH(k_gather_force, f, accumulate);
 }
 
 void launch_init_accel(const NodeDev& nd, int mixed, const void* slots, double4* A4, int* status, cudaStream_t s) {
-    const unsigned grid = grid_for(nd.num_nodes, 256);
-    if (mixed)
-        k_init_accel<float><<<grid, 256, 0, s>>>(nd, static_cast<const float4*>(slots), A4, status);
-    else
-        k_init_accel<double><<<grid, 256, 0, s>>>(nd, static_cast<const double4*>(slots), A4, status);
+    AM_NODE_DISPATCH(k_init_accel, A4, status);
 }
 
 void launch_prologue(const NodeDev& nd, const StepParams* table, double4* U4, double4* V4, const double4* A4,
@@ -1390,11 +1416,7 @@ void launch_prologue(const NodeDev& nd, const StepParams* table, double4* U4, do
 void launch_node_step(const NodeDev& nd, int mixed, const void* slots, const StepParams* table, int64_t step,
                       int advance, double4* U4, double4* V4, double4* A4, double4* u_copy, int* status,
                       cudaStream_t s) {
-    const unsigned grid = grid_for(nd.num_nodes, 256);
-    if (mixed)
-        k_node_step<float><<<grid, 256, 0, s>>>(nd, static_cast<const float4*>(slots), table, step, advance, U4, V4, A4, u_copy, status);
-    else
-        k_node_step<double><<<grid, 256, 0, s>>>(nd, static_cast<const double4*>(slots), table, step, advance, U4, V4, A4, u_copy, status);
+    AM_NODE_DISPATCH(k_node_step, table, step, advance, U4, V4, A4, u_copy, status);
 }
 
 void launch_adj_prep(const NodeDev& nd, const StepParams* table, int64_t step, const double4* VB, const double4* AB,
@@ -1409,7 +1431,7 @@ void launch_adj_update(const NodeDev& nd, const double4* slots, const StepParams
 
 void launch_sensor_seed(const double4* U4, int32_t num_sensors, const int32_t* sensors, double4* UB, double* loss,
                         cudaStream_t s) {
-    k_sensor_seed<<<1, 1, 0, s>>>(U4, num_sensors, sensors, UB, loss);
+    k_sensor_seed<<<1, 256, 0, s>>>(U4, num_sensors, sensors, UB, loss);
 }
 
 void launch_pack4(const double* aos3, double4* out, int64_t n, cudaStream_t s) {

@@ -72,6 +72,7 @@ struct NodeDev {
     const double* bcvalues;     // AM_MAX_BCS x 3 prescribed values
     double g[3];                // body acceleration
     int32_t has_g;
+    int64_t num_slots;          // node_ptr[num_nodes]: force slots in use
 };
 
 // ---- launchers (am_kernels.cu) ----
