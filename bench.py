@@ -262,12 +262,13 @@ def time_run(torch, model, prob, steps, warmup, prec, stream, dev, world, sample
             "clocks": sampler.summary() if sampler else None}
 
 
-def algorithmic_bytes(prob, layout):
+def algorithmic_bytes(prob, layout, slot_bytes=12):
     """Compulsory HBM bytes per launch of the element and node kernels (mixed path):
     coordinates and displacement read once per node (48 B), connectivity (4 B per
-    element node), the assembled FP32 force slots written once and read once (12 B),
-    and in the node kernel mass 8 B, BC word 4 B, node range 4 B, displacement and
-    half-step velocity read and written (96 B)."""
+    element node), per-element moduli (8 B per field), the assembled FP32 force
+    slots written once and read once (12 B), and in the node kernel mass 8 B, BC
+    word 4 B, node range 4 B, displacement and half-step velocity read and written
+    (96 B)."""
     N = prob.num_nodes
     S = layout["used_slots"]
     conn = 0
@@ -276,16 +277,51 @@ def algorithmic_bytes(prob, layout):
             conn += 4 * int(p.cell_ptr[-1]) + 12 * int(p.cell_ptr[-1])  # entry node + FP32 gradient
         else:
             conn += 4 * p.conn.size
-    return {"element": conn + 48 * N + 12 * S, "node": 12 * S + (8 + 4 + 4 + 96) * N}
+        conn += 8 * p.num_elems * ((p.mu_field is not None) + (p.kappa_field is not None))
+    return {"element": conn + 48 * N + slot_bytes * S, "node": slot_bytes * S + (8 + 4 + 4 + 96) * N}
 
 
-def roofline_for(kernels, alg, peak, peak_kind):
+def profiled_traffic(workload: str, role: str, prec: str):
+    """DRAM bytes (read + write) per launch of a kernel from the committed ncu
+    summaries under profiles/ (lines 'traffic workload=W role=R prec=P bytes=B');
+    None when no capture of that kernel on that workload is recorded."""
+    for f in sorted((ROOT / "profiles").glob("*.md")):
+        for line in f.read_text().splitlines():
+            t = dict(kv.split("=", 1) for kv in line.split()[1:] if "=" in kv) if line.strip().startswith("traffic ") else {}
+            if t.get("workload") == workload and t.get("role") == role and t.get("prec") == prec:
+                return int(t["bytes"])
+    return None
+
+
+def algorithmic_flop(prob):
+    """Element-kernel flop per launch: about 450 per neo-Hookean Tet4 (250 linear
+    elastic), 6,900 per neo-Hookean Hex8 with shape-function gradients recomputed
+    from X (5,300 linear elastic), and 36 per cell entry + 250 per cell for
+    smoothed/RKPM cells."""
+    total = 0.0
+    for p in prob.parts:
+        nh = p.material.kind != "linear_elastic"
+        if p.kind == "tet4":
+            total += p.num_elems * (450 if nh else 250)
+        elif p.kind == "hex8":
+            total += p.num_elems * (6900 if nh else 5300)
+        else:
+            total += 36 * int(p.cell_ptr[-1]) + 250 * p.num_elems
+    return total
+
+
+def roofline_for(kernels, alg, peak, peak_kind, workload=None, prec="mixed", flop=None):
     dominant = "node" if kernels["node_total_ms"] >= kernels["element_total_ms"] else "element"
     ms = kernels[f"{dominant}_ms"]
     achieved = alg[dominant] / (ms * 1e-3) / 1e9
-    return {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
-            "algorithmic_bytes_per_launch": alg[dominant], "ms_per_launch": ms}
+    out = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+           "frac": achieved / peak, "peak_source": peak_kind,
+           "traffic": profiled_traffic(workload, dominant, prec) if workload else None,
+           "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/",
+           "algorithmic_bytes_per_launch": alg[dominant], "ms_per_launch": ms}
+    if flop and dominant == "element":
+        out["compute"] = {"algorithmic_flop_per_launch": flop, "achieved_tflops": flop / (ms * 1e-3) / 1e12}
+    return out
 
 
 def measure_workload(torch, prob, steps, warmup, stream, dev, world, mass=None, precs=("fp64", "mixed")):
@@ -307,7 +343,11 @@ def measure_workload(torch, prob, steps, warmup, stream, dev, world, mass=None, 
             f64 = m.internal_force(u64, "fp64")
             out["mixed_rel_force_err_l2"] = float(np.linalg.norm(m.internal_force(u64, "mixed") - f64) / np.linalg.norm(f64))
         if "mixed" in precs:
-            out["roofline_mixed"] = roofline_for(out["mixed"]["kernels"], algorithmic_bytes(prob, layout), peak, kind)
+            out["roofline_mixed"] = roofline_for(out["mixed"]["kernels"], algorithmic_bytes(prob, layout), peak, kind,
+                                                 prob.name, "mixed", algorithmic_flop(prob))
+        if "fp64" in precs:
+            out["roofline_fp64"] = roofline_for(out["fp64"]["kernels"], algorithmic_bytes(prob, layout, 24), peak, kind,
+                                                prob.name, "fp64", algorithmic_flop(prob))
     return out
 
 
@@ -409,8 +449,11 @@ def run_ours(args, rank, world, local):
                "ms": ms_e2e, "path": "ExplicitDynamics.set_state/init_acceleration/run/get_state (C ABI, host buffers)"}
     model.close()
 
-    roofline = roofline_for(res["mixed"]["kernels"], algorithmic_bytes(prob, layout), hbm_peak, peak_kind)
+    roofline = roofline_for(res["mixed"]["kernels"], algorithmic_bytes(prob, layout), hbm_peak, peak_kind,
+                            prob.name, "mixed", algorithmic_flop(prob))
     roofline["layout"] = layout
+    roofline_fp64 = roofline_for(res["fp64"]["kernels"], algorithmic_bytes(prob, layout, 24), hbm_peak, peak_kind,
+                                 prob.name, "fp64", algorithmic_flop(prob))
 
     # the other configurations, each on its own context
     extras = {}
@@ -437,7 +480,8 @@ def run_ours(args, rank, world, local):
         adj = run_adjoint(torch, problems.hex8_nh_lognormal(n=args.adjoint_n, seed=0, nsteps=200), 20, stream, dev)
     kernel_ms = {p: res[p]["kernels"] for p in ("fp64", "mixed")}
     launches = {p: res[p]["launches"] for p in ("fp64", "mixed")}
-    return prob, res, disp_err, force_err, e2e, adj, roofline, kernel_ms, launches, res["mixed"]["clocks"], extras
+    return (prob, res, disp_err, force_err, e2e, adj, roofline, roofline_fp64, kernel_ms, launches,
+            res["mixed"]["clocks"], extras)
 
 
 def cpu_baseline(target_s=10.0, n=24):
@@ -499,8 +543,8 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
-    prob, res, disp_err, force_err, e2e, adj, roofline, kernel_ms, launches, clocks, extras = run_ours(
-        args, rank, world, local)
+    (prob, res, disp_err, force_err, e2e, adj, roofline, roofline_fp64, kernel_ms, launches, clocks,
+     extras) = run_ours(args, rank, world, local)
     if rank != 0:
         return
     cpu = None if args.skip_cpu else cpu_baseline()
@@ -520,6 +564,7 @@ def main():
                           "speedup": res["mixed"]["value"] / res["fp64"]["value"]},
         "adjoint": adj,
         "roofline": roofline,
+        "roofline_fp64": roofline_fp64,
         "kernels_ms_per_launch": kernel_ms,
         "cpu_baseline": cpu,
         "e2e": e2e,
