@@ -1,0 +1,468 @@
+"""aperi-mech YAML input for the explicit-dynamics hot path.
+
+Reads the reference's input schema (include/AperiInputSchema/AperiInputSchema.h, consumed in
+the reference by include/IoInputFile.h and the factories it feeds) for the part of it this
+library computes, and builds an ExplicitDynamics model on the GPU:
+
+    procedures:
+      - explicit_dynamics_procedure:
+          geometry:
+            mesh: generated:NxMxK[|sideset:xXyYzZ][|tets][|bbox:x0,y0,z0,x1,y1,z1]  or  <mesh>.npz
+            parts:
+              - part:
+                  set: block_1
+                  formulation:                      (InternalForceContributionParameters.h:58-246)
+                    integration_scheme:
+                      gauss_quadrature: {integration_order: 1}
+                      | strain_smoothing: {element_smoothing_cell | nodal_smoothing_cell: {subdomains: 1},
+                                           force_one_pass_method: true}
+                    approximation_space:
+                      finite_element: ~ | reproducing_kernel: {kernel_radius_scale_factor: s}
+                  material:                         (Materials/Factory.h:19-160)
+                    linear_elastic | neo_hookean | elastic: {density, two elastic constants}
+          initial_conditions: [- velocity: {sets, components: {X, Y, Z} | vector: {magnitude, direction}}]
+          loads: [- gravity_load: {sets, components | vector}]
+          time_stepper: {direct_time_stepper: {time_increment, time_end}}
+          boundary_conditions:                      (src/BoundaryCondition.cpp:197-220)
+            - displacement | velocity: {sets, components | vector,
+                                        time_function: {ramp_function | smooth_step_function:
+                                                        {abscissa_values, ordinate_values}},
+                                        active_time_range: {time_start, time_end}}
+          output: ...                               (ignored: IO is outside this path)
+          x_b200: {precision: fp64 | mixed, seed, jitter, velocity_noise, max_steps,
+                   fields: {<part set>: {shear_modulus | bulk_modulus: {lognormal_sigma}}}}
+
+Keys this build adds live under `x_b200`. Generated meshes follow STK's "generated:" form:
+unit-size hexes on [0,N]x[0,M]x[0,K] (or the bbox), nodes numbered x fastest, block "block_1",
+side sets named surface_1, surface_2, ... in the order their letters appear (x = min-x face,
+X = max-x face, ...), and "|tets" splits each hex into six tets (this library's conforming
+split; STK's own split is not available here). An .npz mesh holds `coords` (N x 3),
+`block_<name>` (E x 4 or E x 8, zero-based) and `set_<name>` (zero-based node ids).
+Anything else (Exodus meshes, the power-method time stepper, F-bar, two-pass RKPM, other
+materials) raises InputError naming the key.
+"""
+from __future__ import annotations
+
+import json
+import math
+import re
+import sys
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+import yaml
+
+from . import mesh as _mesh
+from .model import BoundaryCondition, ExplicitDynamics, Material, Part
+
+_AXES = {"X": 0, "Y": 1, "Z": 2}
+_FACES = {"x": (0, 0), "X": (0, 1), "y": (1, 0), "Y": (1, 1), "z": (2, 0), "Z": (2, 1)}
+
+
+class InputError(ValueError):
+    """An input the reference would reject, or one outside this library's path."""
+
+
+@dataclass
+class Simulation:
+    """Everything the explicit solve needs, as arrays (the GPU model is built from it)."""
+    name: str
+    coords: np.ndarray
+    parts: list
+    bcs: list
+    v0: np.ndarray
+    dt: float
+    time_end: float
+    precision: str = "fp64"
+    body_accel: np.ndarray | None = None
+    mass: np.ndarray | None = None
+    max_steps: int = 1 << 40
+    sets: dict = field(default_factory=dict)
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def num_nodes(self) -> int:
+        return int(self.coords.shape[0])
+
+    @property
+    def num_elems(self) -> int:
+        return sum(p.num_elems for p in self.parts)
+
+    def model(self, stream=None) -> ExplicitDynamics:
+        return ExplicitDynamics(self.coords, self.parts, self.bcs, body_accel=self.body_accel, mass=self.mass,
+                                stream=stream)
+
+    def problem(self):
+        """The same inputs as a problems.Problem (for the oracle and the benchmark)."""
+        from .problems import Problem
+
+        nsteps = len(direct_time_steps(self.dt, self.time_end))
+        meta = dict(self.meta)
+        if self.mass is not None:
+            meta["mass"] = self.mass
+        if self.body_accel is not None:
+            meta["body_accel"] = self.body_accel
+        return Problem(self.name, self.coords, self.parts, self.bcs, self.v0, self.dt, nsteps,
+                       int(self.meta.get("seed", 0)), meta)
+
+
+def direct_time_steps(dt: float, time_end: float, max_steps: int = 1 << 40) -> list:
+    """Step sizes of DirectTimeStepper::GetTimeIncrement (include/TimeStepper.h:97-128) under
+    the `while (!AtEnd(time)) { ...; time += dt; }` loop of ExplicitSolver::Solve: dt while
+    time + dt <= t_end, then the remainder. Floating-point accumulation can leave a tiny
+    remainder and hence one extra short step, exactly as in the reference (am_solve follows
+    the same rule in C++)."""
+    out, t = [], 0.0
+    while not (t >= time_end) and len(out) < max_steps:
+        h = dt if t + dt <= time_end else (0.0 if t > time_end else time_end - t)
+        out.append(h)
+        t += h
+    return out
+
+
+# ---------------------------------------------------------------------------
+# meshes
+def generated_mesh(spec: str, rng=None, jitter: float = 0.0):
+    """STK-style generated box: returns (coords, {block: conn}, {set: node ids})."""
+    body = spec[len("generated:"):] if spec.startswith("generated:") else spec
+    tokens = body.split("|")
+    m = re.fullmatch(r"\s*(\d+)x(\d+)x(\d+)\s*", tokens[0])
+    if not m:
+        raise InputError(f"generated mesh {spec!r}: expected NxMxK")
+    n = [int(v) for v in m.groups()]
+    lo, hi = np.zeros(3), np.array(n, dtype=float)
+    tets, faces = False, ""
+    for tok in tokens[1:]:
+        key, _, val = tok.partition(":")
+        key = key.strip()
+        if key == "tets":
+            tets = True
+        elif key == "sideset":
+            faces = val.strip()
+        elif key == "bbox":
+            b = [float(v) for v in val.split(",")]
+            if len(b) != 6:
+                raise InputError(f"bbox needs six values: {tok!r}")
+            lo, hi = np.array(b[:3]), np.array(b[3:])
+        else:
+            raise InputError(f"generated mesh option {key!r} is not supported")
+    coords, conn = _mesh.box_hex(n[0], n[1], n[2], *(hi - lo))
+    coords = coords + lo
+    sets = {}
+    for k, ch in enumerate(faces):
+        if ch not in _FACES:
+            raise InputError(f"side set letter {ch!r} (expected one of xXyYzZ)")
+        d, side = _FACES[ch]
+        target = hi[d] if side else lo[d]
+        tol = 1e-9 * max(1.0, float(np.abs(hi - lo).max()))
+        sets[f"surface_{k + 1}"] = np.nonzero(np.abs(coords[:, d] - target) < tol)[0].astype(np.int32)
+    if jitter > 0.0:
+        h = float(((hi - lo) / np.array(n)).min())
+        coords = _mesh.jitter_interior(coords, jitter * h, rng if rng is not None else np.random.default_rng(0))
+    blocks = {"block_1": _mesh.hex_to_tets(conn) if tets else conn}
+    return coords, blocks, sets
+
+
+def npz_mesh(path: Path):
+    d = np.load(path)
+    if "coords" not in d:
+        raise InputError(f"{path}: no 'coords' array")
+    coords = np.ascontiguousarray(d["coords"], dtype=np.float64)
+    blocks = {k[len("block_"):]: np.ascontiguousarray(d[k], dtype=np.int32) for k in d.files if k.startswith("block_")}
+    sets = {k[len("set_"):]: np.ascontiguousarray(d[k], dtype=np.int32) for k in d.files if k.startswith("set_")}
+    if not blocks:
+        raise InputError(f"{path}: no 'block_<name>' arrays")
+    return coords, blocks, sets
+
+
+# ---------------------------------------------------------------------------
+# the procedure
+def _one_key(node, what: str):
+    if not isinstance(node, dict) or len(node) != 1:
+        raise InputError(f"{what}: expected a map with exactly one key, got {node!r}")
+    return next(iter(node.items()))
+
+
+def _components(node: dict, what: str):
+    """GetComponentsAndValues (include/IoInputFile.h:280-304): `vector` (magnitude times the
+    normalised direction, all three components) or `components` (the listed X, Y, Z)."""
+    if "vector" in node:
+        vec = node["vector"]
+        d = np.asarray(vec["direction"], dtype=float)
+        n = float(np.linalg.norm(d))
+        if d.shape != (3,) or n == 0.0:
+            raise InputError(f"{what}: vector direction must be three numbers, not all zero")
+        vals = float(vec["magnitude"]) * d / n
+        return vals, 7
+    if "components" in node:
+        vals, mask = np.zeros(3), 0
+        for k, v in node["components"].items():
+            if k not in _AXES:
+                raise InputError(f"{what}: component {k!r} (expected X, Y or Z)")
+            vals[_AXES[k]] = float(v)
+            mask |= 1 << _AXES[k]
+        return vals, mask
+    raise InputError(f"{what}: needs a 'vector' or 'components' node")
+
+
+def _set_nodes(names, sets: dict, what: str) -> np.ndarray:
+    if isinstance(names, str):
+        names = [names]
+    ids = []
+    for s in names:
+        if s not in sets:
+            raise InputError(f"{what}: unknown set {s!r} (known: {sorted(sets)})")
+        ids.append(sets[s])
+    return np.unique(np.concatenate(ids)).astype(np.int32) if ids else np.zeros(0, np.int32)
+
+
+def _material(node: dict) -> Material:
+    kind, props = _one_key(node, "material")
+    if kind not in ("linear_elastic", "neo_hookean", "elastic"):
+        raise InputError(f"material {kind!r} is not on this path (linear_elastic, neo_hookean, elastic)")
+    props = dict(props or {})
+    if "density" not in props:
+        raise InputError(f"material {kind}: density is required")
+    density = float(props.pop("density"))
+    try:
+        return Material.create(kind, density, **{k: float(v) for k, v in props.items()})
+    except ValueError as e:
+        raise InputError(f"material {kind}: {e}") from None
+
+
+def _hex8_volumes(coords, conn) -> np.ndarray:
+    """sum over the 2x2x2 Gauss points of det J (ElementHexahedron8.h:107-117)."""
+    s = np.array([[-1, -1, -1], [1, -1, -1], [1, 1, -1], [-1, 1, -1],
+                  [-1, -1, 1], [1, -1, 1], [1, 1, 1], [-1, 1, 1]], dtype=float)
+    x = coords[conn]  # E x 8 x 3
+    vol = np.zeros(conn.shape[0])
+    for g in s / math.sqrt(3.0):
+        dN = np.stack([s[:, 0] * (1 + s[:, 1] * g[1]) * (1 + s[:, 2] * g[2]),
+                       s[:, 1] * (1 + s[:, 0] * g[0]) * (1 + s[:, 2] * g[2]),
+                       s[:, 2] * (1 + s[:, 0] * g[0]) * (1 + s[:, 1] * g[1])], axis=1) / 8.0
+        vol += np.linalg.det(np.einsum("eai,aj->eij", x, dN))
+    return vol
+
+
+def _lumped_mass(coords, conn, density) -> np.ndarray:
+    """rho V / n_en per element node (src/MassUtils.cpp:17-46), for Gauss parts that share a
+    model with cell parts (whose mass comes from their own set-up)."""
+    m = np.zeros(coords.shape[0])
+    x = coords[conn]
+    if conn.shape[1] == 4:
+        vol = np.abs(np.einsum("ij,ij->i", x[:, 1] - x[:, 0], np.cross(x[:, 2] - x[:, 0], x[:, 3] - x[:, 0]))) / 6.0
+    else:
+        vol = _hex8_volumes(coords, conn)
+    np.add.at(m, conn.ravel(), np.repeat(density * vol / conn.shape[1], conn.shape[1]))
+    return m
+
+
+def _part(pnode: dict, blocks: dict, coords, ext: dict, rng):
+    """One InternalForceContribution: block connectivity + formulation + material."""
+    name = pnode.get("set")
+    if name not in blocks:
+        raise InputError(f"part set {name!r} is not a block of the mesh (blocks: {sorted(blocks)})")
+    conn = blocks[name]
+    mat = _material(pnode.get("material", {}))
+    form = pnode.get("formulation", {}) or {}
+    scheme, snode = _one_key(form.get("integration_scheme", {"gauss_quadrature": {"integration_order": 1}}),
+                             "integration_scheme")
+    space, spnode = _one_key(form.get("approximation_space", {"finite_element": None}), "approximation_space")
+    fields = (ext.get("fields") or {}).get(name, {})
+    mu_f = kappa_f = None
+    E = conn.shape[0]
+    if fields:
+        for key in fields:
+            if key not in ("shear_modulus", "bulk_modulus"):
+                raise InputError(f"x_b200.fields.{name}: {key!r} (shear_modulus or bulk_modulus)")
+        if "shear_modulus" in fields:
+            mu_f = mat.mu * np.exp(float(fields["shear_modulus"]["lognormal_sigma"]) * rng.standard_normal(E))
+        if "bulk_modulus" in fields:
+            kappa_f = mat.kappa * np.exp(float(fields["bulk_modulus"]["lognormal_sigma"]) * rng.standard_normal(E))
+    if scheme == "gauss_quadrature":
+        if space != "finite_element":
+            raise InputError("gauss_quadrature needs approximation_space: finite_element")
+        order = int((snode or {}).get("integration_order", 1))
+        if order != 1:
+            raise InputError(f"gauss_quadrature integration_order {order}: only 1 is defined")
+        kind = {4: "tet4", 8: "hex8"}.get(conn.shape[1])
+        if kind is None:
+            raise InputError(f"block {name}: {conn.shape[1]}-node elements (Tet4 or Hex8 only)")
+        return Part(kind, mat, conn=conn, mu_field=mu_f, kappa_field=kappa_f, name=name), None
+    if scheme != "strain_smoothing":
+        raise InputError(f"integration_scheme {scheme!r} (gauss_quadrature or strain_smoothing)")
+    snode = snode or {}
+    if snode.get("use_f_bar"):
+        raise InputError("use_f_bar: the F-bar smoothed cells are not built yet")
+    if snode.get("force_two_pass_method"):
+        raise InputError("force_two_pass_method: two-pass RKPM is not built yet")
+    if conn.shape[1] != 4:
+        raise InputError(f"strain_smoothing on block {name}: Tet4 meshes only")
+    cell = "nodal_smoothing_cell" if "nodal_smoothing_cell" in snode else "element_smoothing_cell"
+    sub = int(((snode.get(cell) or {}).get("subdomains", 1)))
+    if sub != 1:
+        raise InputError(f"{cell}.subdomains = {sub}: only 1 is built")
+    if space == "finite_element" and cell == "element_smoothing_cell":
+        from .smoothing import element_smoothing_part
+
+        part, mass = element_smoothing_part(coords, conn, mat, mu_field=mu_f, kappa_field=kappa_f)
+        part.name = name
+        return part, mass
+    if space == "reproducing_kernel" and cell == "nodal_smoothing_cell":
+        if mu_f is not None or kappa_f is not None:
+            raise InputError("x_b200.fields on RKPM nodal cells: per-cell fields are not supported")
+        from .rkpm import nodal_cells, thex_max_edge_length
+
+        scale = float((spnode or {}).get("kernel_radius_scale_factor", 1.0))
+        cells = nodal_cells(coords, conn, mat, scale * thex_max_edge_length(coords, conn),
+                            max_neighbors=int(ext.get("max_neighbors", 40)))
+        cells.part.name = name
+        return cells.part, cells.mass
+    raise InputError(f"{space} with {cell}: not built (finite_element + element cells, "
+                     f"or reproducing_kernel + nodal cells)")
+
+
+def load(source, base_dir: Path | None = None) -> Simulation:
+    """Parse an input (a YAML path, YAML text, or the parsed dict) into a Simulation."""
+    if isinstance(source, dict):
+        doc = source
+    else:
+        text = str(source)
+        p = Path(text)
+        if "\n" not in text and p.suffix in (".yaml", ".yml") and p.exists():
+            base_dir = base_dir or p.parent
+            text = p.read_text()
+        doc = yaml.safe_load(text)
+    base_dir = base_dir or Path.cwd()
+    procs = doc.get("procedures") if isinstance(doc, dict) else None
+    if not procs or not isinstance(procs, list):
+        raise InputError("input needs a 'procedures' sequence")
+    if len(procs) != 1:
+        raise InputError(f"{len(procs)} procedures: one explicit_dynamics_procedure is supported")
+    kind, proc = _one_key(procs[0], "procedure")
+    if kind != "explicit_dynamics_procedure":
+        raise InputError(f"procedure {kind!r} (explicit_dynamics_procedure only)")
+    ext = proc.get("x_b200", {}) or {}
+    seed = int(ext.get("seed", 0))
+    rng = np.random.default_rng(seed)
+
+    geo = proc.get("geometry") or {}
+    mesh_spec = geo.get("mesh")
+    if not isinstance(mesh_spec, str):
+        raise InputError("geometry.mesh is required")
+    if mesh_spec.startswith("generated:"):
+        coords, blocks, sets = generated_mesh(mesh_spec, rng, float(ext.get("jitter", 0.0)))
+    elif mesh_spec.endswith(".npz"):
+        coords, blocks, sets = npz_mesh((base_dir / mesh_spec) if not Path(mesh_spec).is_absolute() else Path(mesh_spec))
+    else:
+        raise InputError(f"mesh {mesh_spec!r}: Exodus files are outside this library (use generated: or .npz)")
+    sets = dict(sets)
+    for b, conn in blocks.items():
+        sets.setdefault(b, np.unique(conn).astype(np.int32))
+
+    parts, masses = [], []
+    for entry in geo.get("parts") or []:
+        _, pnode = _one_key(entry, "parts entry")
+        part, mass = _part(pnode, blocks, coords, ext, rng)
+        parts.append(part)
+        masses.append(mass)
+    if not parts:
+        raise InputError("geometry.parts is empty")
+    mass = None
+    if any(m is not None for m in masses):
+        mass = np.zeros(coords.shape[0])
+        for part, m in zip(parts, masses):
+            mass += m if m is not None else _lumped_mass(coords, part.conn, part.material.density)
+
+    v0 = np.zeros_like(coords)
+    for entry in proc.get("initial_conditions") or []:
+        kind, node = _one_key(entry, "initial_conditions entry")
+        if kind != "velocity":
+            raise InputError(f"initial condition {kind!r} (velocity only)")
+        vals, mask = _components(node, "initial velocity")
+        ids = _set_nodes(node.get("sets", []), sets, "initial velocity")
+        for d in range(3):
+            if mask >> d & 1:
+                v0[ids, d] = vals[d]
+    noise = float(ext.get("velocity_noise", 0.0))
+    if noise > 0.0:
+        v0 += rng.uniform(-noise, noise, size=v0.shape)
+
+    body = None
+    for entry in proc.get("loads") or []:
+        kind, node = _one_key(entry, "loads entry")
+        if kind != "gravity_load":
+            raise InputError(f"load {kind!r} (gravity_load only)")
+        ids = _set_nodes(node.get("sets", []), sets, "gravity_load")
+        if ids.size != coords.shape[0]:
+            raise InputError("gravity_load on part of the mesh: only whole-mesh gravity is built")
+        if "time_function" in node:
+            raise InputError("gravity_load time_function: only constant gravity is built")
+        vals, _ = _components(node, "gravity_load")
+        body = vals if body is None else body + vals
+
+    bcs = []
+    for entry in proc.get("boundary_conditions") or []:
+        kind, node = _one_key(entry, "boundary_conditions entry")
+        if kind not in ("displacement", "velocity"):
+            raise InputError(f"boundary condition {kind!r} (displacement or velocity)")
+        vals, mask = _components(node, f"{kind} boundary condition")
+        ids = _set_nodes(node.get("sets", []), sets, f"{kind} boundary condition")
+        tf_kind, tf = _one_key(node.get("time_function", {"ramp_function": {"abscissa_values": [0.0, 1.0],
+                                                                             "ordinate_values": [1.0, 1.0]}}),
+                               "time_function")
+        if tf_kind not in ("ramp_function", "smooth_step_function"):
+            raise InputError(f"time_function {tf_kind!r}")
+        atr = node.get("active_time_range") or {}
+        bcs.append(BoundaryCondition(nodes=ids, values=tuple(float(v) for v in vals), component_mask=mask,
+                                     kind=kind, time_function=tf_kind,
+                                     abscissa=tuple(float(v) for v in tf["abscissa_values"]),
+                                     ordinate=tuple(float(v) for v in tf["ordinate_values"]),
+                                     active_range=(float(atr.get("time_start", 0.0)),
+                                                   float(atr.get("time_end", 1.7976931348623157e308)))))
+
+    ts_kind, ts = _one_key(proc.get("time_stepper") or {}, "time_stepper")
+    if ts_kind != "direct_time_stepper":
+        raise InputError(f"time_stepper {ts_kind!r}: the power-method stepper is not built (direct_time_stepper)")
+    dt, t_end = float(ts["time_increment"]), float(ts["time_end"])
+    if not (dt > 0.0 and t_end >= 0.0):
+        raise InputError("direct_time_stepper needs time_increment > 0 and time_end >= 0")
+    precision = str(ext.get("precision", "fp64"))
+    if precision not in ("fp64", "mixed"):
+        raise InputError(f"x_b200.precision {precision!r} (fp64 or mixed)")
+    name = Path(str(source)).stem if isinstance(source, (str, Path)) and "\n" not in str(source) else "input"
+    return Simulation(name, coords, parts, bcs, v0, dt, t_end, precision, body, mass,
+                      int(ext.get("max_steps", 1 << 40)), sets, {"seed": seed, "mesh": mesh_spec})
+
+
+def run(source, stream=None) -> dict:
+    """Parse, build the GPU model, and Solve(): the initial acceleration, then the direct
+    time stepper's steps (ExplicitSolver::Solve, src/Solvers/Explicit.cpp:308-483)."""
+    sim = source if isinstance(source, Simulation) else load(source)
+    with sim.model(stream) as m:
+        m.set_state(np.zeros_like(sim.coords), sim.v0)
+        m.init_acceleration(sim.precision)
+        steps = m.solve(sim.dt, sim.time_end, sim.precision, sim.max_steps)
+        u, v, a = m.get_state()
+    return {"simulation": sim, "steps": steps, "displacement": u, "velocity": v, "acceleration": a}
+
+
+def main(argv=None) -> int:
+    import argparse
+
+    ap = argparse.ArgumentParser(description="Run an aperi-mech explicit-dynamics input on the GPU.")
+    ap.add_argument("input")
+    ap.add_argument("--save", help="write the final u, v, a to this .npz")
+    a = ap.parse_args(argv)
+    r = run(a.input)
+    sim = r["simulation"]
+    if a.save:
+        np.savez(a.save, displacement=r["displacement"], velocity=r["velocity"], acceleration=r["acceleration"])
+    print(json.dumps({"input": a.input, "nodes": sim.num_nodes, "elements": sim.num_elems, "steps": r["steps"],
+                      "precision": sim.precision, "max_abs_displacement": float(np.abs(r["displacement"]).max())}))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,205 @@
+"""The YAML front-end (aperi-mech's input schema) against the array-level set-up and the oracle."""
+import numpy as np
+import pytest
+
+from aperi_mech_b200 import input as inp
+from helpers import expected_pk1, prescribed_patch
+
+PATCH_YAML = """
+procedures:
+  - explicit_dynamics_procedure:
+      geometry:
+        mesh: generated:1x1x1|sideset:xXyYzZ|tets
+        parts:
+          - part:
+              set: block_1
+              formulation:
+                integration_scheme:
+                  gauss_quadrature:
+                    integration_order: 1
+                approximation_space:
+                  finite_element: ~
+              material:
+                elastic:
+                  density: 0.08
+                  youngs_modulus: 1.0
+                  poissons_ratio: 0.0
+      time_stepper:
+        direct_time_stepper:
+          time_increment: 0.1
+          time_end: 10.0
+      output:
+        file: results.exo
+        time_start: 0
+        time_end: 10.0
+        time_increment: 1.0
+      boundary_conditions:
+        - displacement:
+            sets: [surface_1]
+            vector: {magnitude: 0.2, direction: [0, -1, 0]}
+            time_function:
+              smooth_step_function: {abscissa_values: [0, 20.0], ordinate_values: [0, 1]}
+        - displacement:
+            sets: [surface_2]
+            vector: {magnitude: 0.2, direction: [0, 1, 0]}
+            time_function:
+              smooth_step_function: {abscissa_values: [0, 20.0], ordinate_values: [0, 1]}
+"""
+
+
+def nh_yaml(n=3, mesh_opts="|sideset:z|tets", extra="", stepper="direct_time_stepper: {time_increment: 2.0e-7, time_end: 4.0e-6}"):
+    return f"""
+procedures:
+  - explicit_dynamics_procedure:
+      geometry:
+        mesh: generated:{n}x{n}x{n}{mesh_opts}|bbox:0,0,0,1,1,1
+        parts:
+          - part:
+              set: block_1
+              formulation:
+                integration_scheme:
+                  gauss_quadrature: {{integration_order: 1}}
+                approximation_space:
+                  finite_element: ~
+              material:
+                neo_hookean: {{density: 1000.0, shear_modulus: 3.85e8, bulk_modulus: 8.33e8}}
+      initial_conditions:
+        - velocity:
+            sets: [block_1]
+            components: {{X: 1.0, Z: -0.5}}
+      time_stepper:
+        {stepper}
+      boundary_conditions:
+        - displacement:
+            sets: [surface_1]
+            components: {{X: 0.0, Y: 0.0, Z: 0.0}}
+            time_function:
+              ramp_function: {{abscissa_values: [0, 1], ordinate_values: [0, 1]}}
+{extra}"""
+
+
+def test_generated_mesh_and_sets():
+    coords, blocks, sets = inp.generated_mesh("generated:2x3x4|sideset:xXyYzZ")
+    assert coords.shape == (3 * 4 * 5, 3) and blocks["block_1"].shape == (24, 8)
+    assert np.allclose(coords.max(axis=0), [2, 3, 4])  # unit-size elements
+    assert sets["surface_1"].size == 4 * 5 and np.all(coords[sets["surface_1"], 0] == 0)
+    assert np.all(coords[sets["surface_6"], 2] == 4)
+    _, blocks, sets = inp.generated_mesh("generated:1x1x1|sideset:Zz|tets")
+    assert blocks["block_1"].shape == (6, 4)
+    assert sets["surface_1"].size == 4 and sets["surface_2"].size == 4
+    coords, _, _ = inp.generated_mesh("generated:2x2x2|bbox:-1,-1,-1,1,1,3")
+    assert np.allclose(coords.min(axis=0), [-1, -1, -1]) and np.allclose(coords.max(axis=0), [1, 1, 3])
+
+
+def test_patch_yaml_matches_array_setup_and_known_answer(oracle_lib):
+    sim = inp.load(PATCH_YAML)
+    coords, parts, bcs, sets = prescribed_patch("tet4", (1, 1, 1), 1, 0, 0.1)
+    assert np.array_equal(sim.coords, coords) and np.array_equal(sim.parts[0].conn, parts[0].conn)
+    assert sim.parts[0].material == parts[0].material
+    for a, b in zip(sim.bcs, bcs):
+        assert np.array_equal(np.sort(a.nodes), np.sort(b.nodes))
+        assert np.allclose(a.values, b.values) and a.component_mask == b.component_mask
+        assert (a.kind, a.time_function, a.abscissa, a.ordinate) == (b.kind, b.time_function, b.abscissa, b.ordinate)
+    # ForceTest.cpp shear patch known answer, run from the parsed input by the oracle.
+    prob = oracle_lib.OracleProblem(sim.coords, sim.parts, sim.bcs)
+    u, v, a, n = prob.solve(np.zeros_like(sim.coords), sim.v0, sim.dt, sim.time_end)
+    assert n == len(inp.direct_time_steps(sim.dt, sim.time_end)) == len(oracle_lib.direct_time_schedule(0.1, 10.0))
+    H = np.zeros((3, 3))
+    H[1, 0] = 0.2
+    f = prob.internal_force(u)
+    P = expected_pk1(H, sim.parts[0].material)
+    assert np.abs(f[sim.sets["surface_1"]].sum(axis=0) - P @ [1.0, 0.0, 0.0]).max() < 1e-8
+    assert np.abs(u[sim.sets["surface_2"]] - [0.0, 0.1, 0.0]).max() < 1e-9
+    assert np.abs(a).max() < 1e-12
+
+
+def test_components_vector_initial_conditions_and_extensions():
+    extra = """      loads:
+        - gravity_load:
+            sets: [block_1]
+            vector: {magnitude: 9.81, direction: [0, 0, -2]}
+      x_b200:
+        precision: mixed
+        seed: 4
+        jitter: 0.2
+        velocity_noise: 0.01
+        fields:
+          block_1:
+            shear_modulus: {lognormal_sigma: 0.3}
+"""
+    sim = inp.load(nh_yaml(extra=extra))
+    assert sim.precision == "mixed" and np.allclose(sim.body_accel, [0, 0, -9.81])
+    assert np.abs(sim.v0[:, 0] - 1.0).max() <= 0.01 and np.abs(sim.v0[:, 1]).max() <= 0.01
+    part = sim.parts[0]
+    assert part.mu_field.shape == (part.num_elems,) and part.kappa_field is None
+    assert abs(np.median(np.log(part.mu_field / 3.85e8))) < 0.2
+    bc = sim.bcs[0]
+    assert bc.component_mask == 7 and bc.kind == "displacement" and bc.time_function == "ramp_function"
+    interior = ~np.any((sim.coords == 0) | (sim.coords == 1), axis=1)
+    plain = inp.load(nh_yaml())
+    assert np.abs(sim.coords[interior] - plain.coords[interior]).max() > 0  # jittered
+    assert np.array_equal(sim.coords[~interior], plain.coords[~interior])  # boundary untouched
+
+
+@pytest.mark.parametrize("text, msg", [
+    (nh_yaml(stepper="power_method_time_stepper: {scale_factor: 0.1, update_interval: 10, time_end: 1.0}"),
+     "power-method"),
+    (nh_yaml().replace("generated:3x3x3|sideset:z|tets|bbox:0,0,0,1,1,1", "../mesh/tet.e"), "Exodus"),
+    (nh_yaml().replace("sets: [surface_1]", "sets: [nodeset_9]"), "unknown set"),
+    (nh_yaml().replace("neo_hookean: {density: 1000.0,", "neo_hookean: {"), "density"),
+    (nh_yaml().replace("neo_hookean:", "plastic:"), "not on this path"),
+    (nh_yaml().replace("shear_modulus: 3.85e8, ", ""), "neo_hookean"),
+    (nh_yaml().replace("gauss_quadrature: {integration_order: 1}",
+                       "strain_smoothing: {element_smoothing_cell: {subdomains: 1}, use_f_bar: true}"), "F-bar"),
+    (nh_yaml().replace("components: {X: 1.0, Z: -0.5}", "components: {W: 1.0}"), "component"),
+])
+def test_rejected_inputs(text, msg):
+    with pytest.raises(inp.InputError, match=msg):
+        inp.load(text)
+
+
+def test_strain_smoothing_part_from_yaml():
+    text = nh_yaml().replace("gauss_quadrature: {integration_order: 1}",
+                             "strain_smoothing: {element_smoothing_cell: {subdomains: 1}, force_one_pass_method: true}")
+    sim = inp.load(text)
+    part = sim.parts[0]
+    assert part.kind == "cells" and part.num_elems == 6 * 27
+    assert sim.mass is not None and abs(sim.mass.sum() - 1000.0) < 1e-9
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_yaml_run_matches_oracle(oracle_lib, precision):
+    extra = f"""      x_b200:
+        precision: {precision}
+        seed: 2
+        jitter: 0.2
+        velocity_noise: 0.01
+        fields:
+          block_1:
+            shear_modulus: {{lognormal_sigma: 0.3}}
+            bulk_modulus: {{lognormal_sigma: 0.3}}
+"""
+    sim = inp.load(nh_yaml(n=6, extra=extra))
+    r = inp.run(sim)
+    prob = oracle_lib.OracleProblem(sim.coords, sim.parts, sim.bcs)
+    u, v, a, n = prob.solve(np.zeros_like(sim.coords), sim.v0, sim.dt, sim.time_end)
+    assert r["steps"] == n
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    for got, ref in ((r["displacement"], u), (r["velocity"], v)):
+        assert np.linalg.norm(got - ref) <= tol * np.linalg.norm(ref)
+
+
+@pytest.mark.gpu
+def test_yaml_rkpm_nodal_cells_run_matches_oracle(oracle_lib):
+    text = nh_yaml(n=4).replace(
+        "gauss_quadrature: {integration_order: 1}",
+        "strain_smoothing: {nodal_smoothing_cell: {subdomains: 1}, force_one_pass_method: true}").replace(
+        "finite_element: ~", "reproducing_kernel: {kernel_radius_scale_factor: 1.1}")
+    sim = inp.load(text)
+    assert sim.parts[0].kind == "cells" and sim.mass is not None
+    r = inp.run(sim)
+    prob = oracle_lib.OracleProblem(sim.coords, sim.parts, sim.bcs, mass=sim.mass)
+    u, v, a, n = prob.solve(np.zeros_like(sim.coords), sim.v0, sim.dt, sim.time_end)
+    assert r["steps"] == n
+    assert np.linalg.norm(r["displacement"] - u) <= 1e-12 * np.linalg.norm(u)
