@@ -218,6 +218,7 @@ struct am_ctx {
     am::StepParams* table = nullptr;
     int64_t table_cap = 0;
     am::StepParams* table_host = nullptr;  // pinned staging
+    cudaEvent_t table_copied = nullptr;    // the last upload out of table_host has executed
     std::vector<Block> blocks;
     std::vector<am::host::BoundaryCondition> bcs;
     double g[3] = {0, 0, 0};
@@ -309,13 +310,20 @@ struct am_ctx {
     // Profiling marks: each mark closes the interval since the previous mark and
     // books it to a slot (-1: not booked). Elapsed times are read lazily by
     // am_profile_read, so marks add no host synchronization to the timed work.
-    void mark(int slot, int64_t nlaunch) {
-        if (!profiling) return;
-        if (n_marks >= events.size()) {
+    // Creates events up to `count` pending marks. Called before work is enqueued (at
+    // am_profile_enable and at the start of each run), so event creation never sits
+    // between the kernels being timed.
+    void reserve_marks(size_t count) {
+        while (events.size() < count) {
             cudaEvent_t e;
             ck(cudaEventCreate(&e), "event create");
             events.push_back(e);
         }
+    }
+
+    void mark(int slot, int64_t nlaunch) {
+        if (!profiling) return;
+        if (n_marks >= events.size()) reserve_marks(std::max<size_t>(2 * events.size(), 64));
         ck(cudaEventRecord(events[n_marks], stream), "event record");
         mark_slot.resize(n_marks + 1);
         mark_slot[n_marks] = {slot, nlaunch};
@@ -343,11 +351,14 @@ struct am_ctx {
             dfree(table);
             if (table_host) cudaFreeHost(table_host);
             table_host = nullptr;
-            table_cap = std::max<int64_t>(n + 1, 64);
+            table_cap = std::max<int64_t>({n + 1, 2 * table_cap, 1024});
             table = dalloc<am::StepParams>(table_cap, "step table");
             ck(cudaMallocHost(&table_host, table_cap * sizeof(am::StepParams)), "pinned step table");
         }
-        ck(cudaStreamSynchronize(stream), "synchronize before table upload");
+        // The staging buffer is reused once the previous upload out of it has executed;
+        // kernels still reading the device table are ordered before the new copy.
+        if (!table_copied) ck(cudaEventCreateWithFlags(&table_copied, cudaEventDisableTiming), "event create");
+        ck(cudaEventSynchronize(table_copied), "wait for the previous table upload");
         double time = t0;
         for (int64_t k = 0; k < n; ++k) {
             am::StepParams& P = table_host[k];
@@ -369,12 +380,14 @@ struct am_ctx {
             time += dts[k];
         }
         ck(cudaMemcpyAsync(table, table_host, n * sizeof(am::StepParams), cudaMemcpyHostToDevice, stream), "table upload");
+        ck(cudaEventRecord(table_copied, stream), "event record");
     }
 
     // Steps [n0, n1) of the uploaded table, from a consistent (U4, V4, A4). u_hist[k]
     // (optional) receives the displacement the element kernels use at step n0+k.
     void run_range(int mixed, int64_t n0, int64_t n1, double4* const* u_hist) {
         if (n1 <= n0) return;
+        if (profiling) reserve_marks(n_marks + static_cast<size_t>(2 * (n1 - n0) + 2));
         const am::NodeDev nd = node_dev();
         void* s = slots(mixed);
         mark(-1, 0);
@@ -430,6 +443,8 @@ struct am_ctx {
         table_host = nullptr;
         for (auto e : events) cudaEventDestroy(e);
         events.clear();
+        if (table_copied) cudaEventDestroy(table_copied);
+        table_copied = nullptr;
         if (own_stream && stream) cudaStreamDestroy(stream);
         stream = nullptr;
     }
@@ -1067,6 +1082,7 @@ int am_adjoint(am_ctx* ctx, int64_t nsteps, double dt, int32_t ckpt_every, int32
                 ck(cudaMemcpyAsync(ctx->A4, ck_a[s], bytes, cudaMemcpyDeviceToDevice, st), "restore");
                 ctx->run_range(0, n0, n1, seg.data());
             }
+            if (ctx->profiling) ctx->reserve_marks(ctx->n_marks + static_cast<size_t>(2 * (n1 - n0) + 1));
             ctx->mark(-1, 0);
             for (int64_t n = n1 - 1; n >= n0; --n) {
                 ctx->vjp(seg[n - n0], ctx->L4, gm, gk, 1);
@@ -1194,6 +1210,10 @@ int am_profile_enable(am_ctx* ctx, int enable) {
     const int rc = guarded(ctx, [&] { ctx->collect_marks(); });
     if (rc != AM_OK) return rc;
     ctx->profiling = enable != 0;
+    if (ctx->profiling) {
+        const int rc2 = guarded(ctx, [&] { ctx->reserve_marks(4096); });
+        if (rc2 != AM_OK) return rc2;
+    }
     for (int k = 0; k < 4; ++k) {
         ctx->prof_ms[k] = 0.0;
         ctx->prof_launches[k] = 0;

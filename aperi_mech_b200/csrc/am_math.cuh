@@ -62,6 +62,26 @@ __device__ __forceinline__ double det_ap_im1(const T* A) {
            a12 * a21 * (1 + a00) + a00 * a22 + a11 * a22 + a01 * a12 * a20 + a02 * a10 * a21;
 }
 
+// log1p for the neo-Hookean log J. Near J = 1 (|x| <= 1/16, the usual range) the
+// classical atanh form log1p(x) = 2 atanh(s) = 2 (s + s^3/3 + s^5/5 + ...), s = x/(2+x),
+// truncated after s^11 (next term below 1e-19 relative), with 1/(2+x) from an FP32
+// reciprocal refined by two Newton-Raphson steps; elsewhere CUDA's log1p.
+__device__ __forceinline__ double log1p_nh(double x) {
+    if (!(fabs(x) <= 0.0625)) return log1p(x);
+    const double d = 2.0 + x;
+    double r = static_cast<double>(__frcp_rn(static_cast<float>(d)));
+    r = fma(r, fma(-d, r, 1.0), r);
+    r = fma(r, fma(-d, r, 1.0), r);
+    const double s = x * r, t = s * s;
+    double p = 1.0 / 11.0;
+    p = fma(p, t, 1.0 / 9.0);
+    p = fma(p, t, 1.0 / 7.0);
+    p = fma(p, t, 1.0 / 5.0);
+    p = fma(p, t, 1.0 / 3.0);
+    p = fma(p, t, 1.0);
+    return 2.0 * s * p;
+}
+
 // First Piola-Kirchhoff stress P(H). Returns J (det F) for the neo-Hookean model
 // (so callers can flag J <= 0) and 1 otherwise.
 //   linear elastic  (LinearElastic.h:79-87): P = lambda tr(eps) I + 2 mu eps, eps = sym(H)
@@ -86,7 +106,7 @@ __device__ __forceinline__ double stress(int32_t mat, T lambda, T mu, const T* H
     if (mat == kNeoHookean) {
         const double Jm1 = det_ap_im1(H);
         const double J = 1.0 + Jm1;
-        const T lam_lnJ = T((double)lambda * log1p(Jm1));
+        const T lam_lnJ = T((double)lambda * log1p_nh(Jm1));
         T Fi[9];
         cof_inv3(F, Fi, T(J));
         T tau[9];
@@ -160,7 +180,7 @@ __device__ __forceinline__ void stress_vjp(int32_t mat, double lambda, double mu
         //   dP = mu L + (mu - lambda log J) F^-T L^T F^-T + lambda tr(F^-1 L) F^-T
         //   L : dP/dlambda = log J tr(F^-1 L),  L : dP/dmu = L : (F - F^-T)
         const double Jm1 = det_ap_im1(H);
-        const double lnJ = log1p(Jm1);
+        const double lnJ = log1p_nh(Jm1);
         double Fi[9];
         cof_inv3(F, Fi, 1.0 + Jm1);
         double trFiL = 0.0;

@@ -95,6 +95,23 @@ def test_material_driver_gpu(gpu, oracle_lib):
         assert rel_err(got, want) < 1e-14, name
 
 
+def test_neo_hookean_log_j_across_series_range(gpu, oracle_lib):
+    """The neo-Hookean log J uses a series for |J - 1| <= 1/16 and CUDA's log1p beyond:
+    the volumetric stress of pure dilatations H = a I, J - 1 from -0.5 to 1 (both sides of
+    the switch, and tiny |J - 1|), matches the oracle's std::log1p to a few ulp."""
+    from aperi_mech_b200 import capi
+
+    jm1 = np.concatenate([np.linspace(-0.5, 1.0, 301), [-0.0625, 0.0625, -0.0624999, 0.0625001],
+                          np.geomspace(1e-14, 1e-2, 25), -np.geomspace(1e-14, 1e-2, 25)])
+    a = np.cbrt(1.0 + jm1) - 1.0
+    H = a[:, None, None] * np.eye(3)[None]
+    mat = _material("neo_hookean")
+    got = capi.stress(capi.AM_NEO_HOOKEAN, mat.lam, mat.mu, H)
+    want = oracle_lib.stress("neo_hookean", mat.lam, mat.mu, H)
+    scale = np.abs(want).reshape(len(a), -1).max(axis=1)
+    assert (np.abs(got - want).reshape(len(a), -1).max(axis=1) <= 1e-14 * scale + 1e-300).all()
+
+
 # ---- internal force ------------------------------------------------------------------
 @pytest.mark.parametrize("kind,n", [("tet4", 5), ("hex8", 6)])
 @pytest.mark.parametrize("material", ["linear_elastic", "neo_hookean", "elastic"])
