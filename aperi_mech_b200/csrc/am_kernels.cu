@@ -486,10 +486,20 @@ __global__ void __launch_bounds__(128, sizeof(T) == 8 ? 1 : 4) k_hex8_force(Gaus
 
 // ---------------------------------------------------------------------------
 // Smoothed / RKPM cells (ComputeInternalForceSmoothedCell.h:416-442, no F-bar):
-// H = sum_k u_k (x) b_k ; P(H) ; f_k = -V b_k P^T written to the cell's slots.
+// H = sum_k u_k (x) b_k ; P(H) ; f_k = -V b_k P^T. The cell kernel stops at the cell
+// stress G = -V P (nine numbers per cell, stored as three padded rows); the node
+// kernel forms f_k = G b_k from its node-major copy of the entries. Each entry's
+// gradient is read once per kernel and no per-entry force is written, which for
+// RKPM cells (tens of entries each) removes a third of the step's HBM traffic.
 // The mixed path subtracts the first entry's displacement (partition of nullity
 // makes H invariant) before casting to FP32.
 // ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void store_cell_stress(vec4_t<T>* __restrict__ G, const T* P, T V) {
+    G[0] = make4(-V * P[0], -V * P[1], -V * P[2]);
+    G[1] = make4(-V * P[3], -V * P[4], -V * P[5]);
+    G[2] = make4(-V * P[6], -V * P[7], -V * P[8]);
+}
 template <typename T>
 __device__ __forceinline__ const T* cell_grads(const CellBlockDev& b);
 template <>
@@ -499,7 +509,7 @@ __device__ __forceinline__ const float* cell_grads<float>(const CellBlockDev& b)
 
 template <typename T, int MAT>
 __global__ void __launch_bounds__(256) k_cell_force_thread(CellBlockDev b, const double4* __restrict__ U4,
-                                                            vec4_t<T>* __restrict__ slots, int* status) {
+                                                            vec4_t<T>* __restrict__ cell_stress, int* status) {
     const int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (c >= b.num_cells) return;
     const int32_t s0 = b.ptr[c], s1 = b.ptr[c + 1];
@@ -524,19 +534,12 @@ __global__ void __launch_bounds__(256) k_cell_force_thread(CellBlockDev b, const
     T P[9];
     const double Jf = stress<T>(MAT, T(lam), T(mu), H, P);
     if (MAT == kNeoHookean && !(Jf > 0.0)) flag(status, AM_ENONPOS_J, c);
-    const T V = T(b.volumes[c]);
-    for (int32_t s = s0; s < s1; ++s) {
-        const T gg[3] = {gr[3 * s], gr[3 * s + 1], gr[3 * s + 2]};
-        T f[3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) f[i] = (gg[0] * P[i * 3 + 0] + gg[1] * P[i * 3 + 1] + gg[2] * P[i * 3 + 2]) * -V;
-        slots[b.slot_pos[s]] = make4(f[0], f[1], f[2]);
-    }
+    store_cell_stress<T>(cell_stress + 3 * (b.cell_base + c), P, T(b.volumes[c]));
 }
 
 template <typename T, int MAT>
 __global__ void __launch_bounds__(256) k_cell_force_warp(CellBlockDev b, const double4* __restrict__ U4,
-                                                          vec4_t<T>* __restrict__ slots, int* status) {
+                                                          vec4_t<T>* __restrict__ cell_stress, int* status) {
     const int lane = threadIdx.x & 31;
     const int64_t c = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     if (c >= b.num_cells) return;  // whole warp exits together
@@ -566,14 +569,9 @@ __global__ void __launch_bounds__(256) k_cell_force_warp(CellBlockDev b, const d
     element_lame(b, c, lam, mu);
     T P[9];
     const double Jf = stress<T>(MAT, T(lam), T(mu), H, P);
-    if (lane == 0 && MAT == kNeoHookean && !(Jf > 0.0)) flag(status, AM_ENONPOS_J, c);
-    const T V = T(b.volumes[c]);
-    for (int32_t s = s0 + lane; s < s1; s += 32) {
-        const T gg[3] = {gr[3 * s], gr[3 * s + 1], gr[3 * s + 2]};
-        T f[3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) f[i] = (gg[0] * P[i * 3 + 0] + gg[1] * P[i * 3 + 1] + gg[2] * P[i * 3 + 2]) * -V;
-        slots[b.slot_pos[s]] = make4(f[0], f[1], f[2]);
+    if (lane == 0) {
+        if (MAT == kNeoHookean && !(Jf > 0.0)) flag(status, AM_ENONPOS_J, c);
+        store_cell_stress<T>(cell_stress + 3 * (b.cell_base + c), P, T(b.volumes[c]));
     }
 }
 
@@ -804,7 +802,7 @@ __global__ void __launch_bounds__(128) k_hex8_vjp(GaussBlockDev b, const double4
 
 template <int MAT>
 __global__ void __launch_bounds__(256) k_cell_vjp(CellBlockDev b, const double4* __restrict__ U4,
-                                                   const double4* __restrict__ L4, double4* __restrict__ slots,
+                                                   const double4* __restrict__ L4, double4* __restrict__ cell_stress,
                                                    double* gmu, double* gk, int accumulate) {
     const int lane = threadIdx.x & 31;
     const int64_t c = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
@@ -838,14 +836,10 @@ __global__ void __launch_bounds__(256) k_cell_vjp(CellBlockDev b, const double4*
     double dP[9], ldl, ldm;
     stress_vjp(MAT, lam, mu, H, L, dP, &ldl, &ldm);
     const double V = b.volumes[c];
-    for (int32_t s = s0 + lane; s < s1; s += 32) {
-        const double gg[3] = {b.grads64[3 * s], b.grads64[3 * s + 1], b.grads64[3 * s + 2]};
-        double f[3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) f[i] = (gg[0] * dP[i * 3 + 0] + gg[1] * dP[i * 3 + 1] + gg[2] * dP[i * 3 + 2]) * -V;
-        slots[b.slot_pos[s]] = make4(f[0], f[1], f[2]);
+    if (lane == 0) {
+        store_cell_stress<double>(cell_stress + 3 * (b.cell_base + c), dP, V);
+        store_theta(gmu, gk, c, -V * (ldm - 2.0 / 3.0 * ldl), -V * ldl, accumulate);
     }
-    if (lane == 0) store_theta(gmu, gk, c, -V * (ldm - 2.0 / 3.0 * ldl), -V * ldl, accumulate);
 }
 
 // ---------------------------------------------------------------------------
@@ -935,6 +929,9 @@ constexpr int kNodeBlock = 256;
 // takes every slot in one round; that wins when the slot array sits in L2 (the
 // loads are latency-bound), while BATCH = 4 keeps more warps resident, which wins
 // when the slots stream from HBM (see gather_batch8).
+__device__ __forceinline__ int64_t cell_id(float w) { return __float_as_int(w); }
+__device__ __forceinline__ int64_t cell_id(double w) { return __double_as_longlong(w); }
+
 template <typename S, int BATCH>
 __device__ __forceinline__ void gather(const NodeDev& nd, const vec4_t<S>* __restrict__ slots, int64_t i, double& fx,
                                        double& fy, double& fz) {
@@ -951,6 +948,27 @@ __device__ __forceinline__ void gather(const NodeDev& nd, const vec4_t<S>* __res
                 fx += static_cast<double>(v[k].x);
                 fy += static_cast<double>(v[k].y);
                 fz += static_cast<double>(v[k].z);
+            }
+    }
+    if (nd.cell_ptr == nullptr) return;
+    // Cell entries of this node, in entry order: f += G_c b (G = -V P of cell c).
+    const vec4_t<S>* __restrict__ ent = static_cast<const vec4_t<S>*>(nd.cell_entries);
+    const vec4_t<S>* __restrict__ G = static_cast<const vec4_t<S>*>(nd.cell_stress);
+    const int32_t q0 = nd.cell_ptr[i], q1 = nd.cell_ptr[i + 1];
+    constexpr int CB = 4;
+    for (int32_t q = q0; q < q1; q += CB) {
+        vec4_t<S> e[CB];
+#pragma unroll
+        for (int k = 0; k < CB; ++k)
+            if (q + k < q1) e[k] = ent[q + k];
+#pragma unroll
+        for (int k = 0; k < CB; ++k)
+            if (q + k < q1) {
+                const int64_t c = cell_id(e[k].w);
+                const vec4_t<S> g0 = G[3 * c], g1 = G[3 * c + 1], g2 = G[3 * c + 2];
+                fx += static_cast<double>(g0.x * e[k].x + g0.y * e[k].y + g0.z * e[k].z);
+                fy += static_cast<double>(g1.x * e[k].x + g1.y * e[k].y + g1.z * e[k].z);
+                fz += static_cast<double>(g2.x * e[k].x + g2.y * e[k].y + g2.z * e[k].z);
             }
     }
 }
@@ -1159,6 +1177,16 @@ __global__ void __launch_bounds__(256) k_sensor_seed(const double4* __restrict__
     if (threadIdx.x == 0) *loss = part[0];
 }
 
+// FP32 copy of the node-major cell entries: gradient rounded to FP32, cell id moved
+// from the FP64 word's bits to the FP32 word's bits.
+__global__ void k_cell_entries_fp32(const double4* __restrict__ in, float4* __restrict__ out, int64_t n) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4 e = in[i];
+    out[i] = make_float4(static_cast<float>(e.x), static_cast<float>(e.y), static_cast<float>(e.z),
+                         __int_as_float(static_cast<int>(__double_as_longlong(e.w))));
+}
+
 __global__ void k_pack4(const double* __restrict__ in, double4* __restrict__ out, int64_t n) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -1323,7 +1351,8 @@ void launch_gauss_force(const GaussBlockDev& b, int mixed, const double4* X4, co
     }
 }
 
-void launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void* slots, int* status, cudaStream_t s) {
+void launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void* slots, int* status,
+                       cudaStream_t s) {
     if (b.num_cells == 0) return;
     if (b.max_entries <= 8) {
         const unsigned grid = grid_for(b.num_cells, 256);
@@ -1357,11 +1386,15 @@ void launch_gauss_vjp(const GaussBlockDev& b, const double4* X4, const double4* 
     }
 }
 
-void launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double4* slots, double* gmu,
+void launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double4* cell_stress, double* gmu,
                      double* gkappa, int accumulate, cudaStream_t s) {
     if (b.num_cells == 0) return;
     const unsigned grid = grid_for(b.num_cells * 32, 256);
-    AM_DISPATCH_MAT(b.material, (k_cell_vjp<M><<<grid, 256, 0, s>>>(b, U4, L4, slots, gmu, gkappa, accumulate)));
+    AM_DISPATCH_MAT(b.material, (k_cell_vjp<M><<<grid, 256, 0, s>>>(b, U4, L4, cell_stress, gmu, gkappa, accumulate)));
+}
+
+void launch_cell_entries_fp32(const double4* in, float4* out, int64_t n, cudaStream_t s) {
+    if (n > 0) k_cell_entries_fp32<<<grid_for(n, 256), 256, 0, s>>>(in, out, n);
 }
 
 void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const double4* X4, double4* slots,

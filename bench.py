@@ -263,22 +263,28 @@ def time_run(torch, model, prob, steps, warmup, prec, stream, dev, world, sample
 
 
 def algorithmic_bytes(prob, layout, slot_bytes=12):
-    """Compulsory HBM bytes per launch of the element and node kernels (mixed path):
-    coordinates and displacement read once per node (48 B), connectivity (4 B per
-    element node), per-element moduli (8 B per field), the assembled FP32 force
-    slots written once and read once (12 B), and in the node kernel mass 8 B, BC
-    word 4 B, node range 4 B, displacement and half-step velocity read and written
+    """Compulsory HBM bytes per launch of the element and node kernels; slot_bytes is
+    three reals (12 B mixed, 24 B FP64). Element kernels: coordinates and displacement
+    read once per node (48 B), connectivity (4 B per element node), per-element moduli
+    (8 B per field), the node-major force slots written once (Gauss blocks), or for
+    cell blocks each entry's node id and gradient (4 B + three reals) read once and the
+    cell stress G (nine reals) written once. Node kernel: the slots read once, each cell
+    entry (gradient + cell id) and each cell stress read once, and per node mass 8 B,
+    BC word 4 B, slot range 4 B, displacement and half-step velocity read and written
     (96 B)."""
     N = prob.num_nodes
     S = layout["used_slots"]
-    conn = 0
+    elem = 48 * N + slot_bytes * S
+    node = slot_bytes * S + (8 + 4 + 4 + 96) * N
     for p in prob.parts:
         if p.kind == "cells":
-            conn += 4 * int(p.cell_ptr[-1]) + 12 * int(p.cell_ptr[-1])  # entry node + FP32 gradient
+            K, C = int(p.cell_ptr[-1]), p.num_elems
+            elem += (4 + slot_bytes) * K + 3 * slot_bytes * C
+            node += (4 + slot_bytes) * K + 3 * slot_bytes * C + 4 * N
         else:
-            conn += 4 * p.conn.size
-        conn += 8 * p.num_elems * ((p.mu_field is not None) + (p.kappa_field is not None))
-    return {"element": conn + 48 * N + slot_bytes * S, "node": slot_bytes * S + (8 + 4 + 4 + 96) * N}
+            elem += 4 * p.conn.size
+        elem += 8 * p.num_elems * ((p.mu_field is not None) + (p.kappa_field is not None))
+    return {"element": elem, "node": node}
 
 
 def profiled_traffic(workload: str, role: str, prec: str):
