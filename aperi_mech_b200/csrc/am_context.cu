@@ -76,6 +76,7 @@ struct Block {
     // Cell blocks: position of the first cell in the context's cell-stress array, and the
     // host copies of the entries that am_finalize turns into the node-major entry list.
     int64_t cell_base = 0;
+    int64_t cell_entries = 0;
     std::vector<int32_t> host_cell_ptr, host_cell_nodes;
     std::vector<double> host_cell_grads;
 
@@ -112,6 +113,7 @@ struct Block {
         c.mu_field = mu_field;
         c.kappa_field = kappa_field;
         c.cell_base = cell_base;
+        c.num_entries = cell_entries;
         c.max_entries = max_entries;
         return c;
     }
@@ -251,6 +253,7 @@ struct am_ctx {
         if (num_cells_total > 0) {
             if (mixed) prepare_mixed();
             nd.cell_ptr = cell_node_ptr;
+            nd.num_cell_entries = num_cell_entries;
             nd.cell_entries = mixed ? static_cast<const void*>(cell_entries32) : cell_entries64;
             nd.cell_stress = mixed ? static_cast<const void*>(cell_stress32) : cell_stress64;
         }
@@ -708,6 +711,7 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
                 }
                 // Cells add no slots: their entries reach the nodes through the cell stresses.
                 b.num_entries = 0;
+                b.cell_entries = K;
                 b.cell_base = ctx->num_cells_total;
                 b.host_cell_ptr = std::move(ptr);
                 b.host_cell_nodes.assign(d->cell_nodes, d->cell_nodes + K);

@@ -537,21 +537,26 @@ __global__ void __launch_bounds__(256) k_cell_force_thread(CellBlockDev b, const
     store_cell_stress<T>(cell_stress + 3 * (b.cell_base + c), P, T(b.volumes[c]));
 }
 
-template <typename T, int MAT>
-__global__ void __launch_bounds__(256) k_cell_force_warp(CellBlockDev b, const double4* __restrict__ U4,
+// LPC lanes per cell (a power of two up to 32): the group strides over the cell's
+// entries, combines its partial H by a butterfly over the group, and every lane of
+// the group then holds the same H. Narrow groups keep the lanes busy on cells of a
+// few tens of entries and repeat the stress update on fewer lanes.
+template <typename T, int MAT, int LPC>
+__global__ void __launch_bounds__(256) k_cell_force_group(CellBlockDev b, const double4* __restrict__ U4,
                                                           vec4_t<T>* __restrict__ cell_stress, int* status) {
-    const int lane = threadIdx.x & 31;
-    const int64_t c = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    if (c >= b.num_cells) return;  // whole warp exits together
-    const int32_t s0 = b.ptr[c], s1 = b.ptr[c + 1];
-    if (s1 <= s0) return;
+    const int64_t gt = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t c = gt / LPC;
+    const int r = static_cast<int>(threadIdx.x % LPC);
+    const unsigned gmask = LPC == 32 ? kFull : (((1u << LPC) - 1u) << ((threadIdx.x & 31) & ~(LPC - 1)));
+    const bool valid = c < b.num_cells;
+    const int32_t s0 = valid ? b.ptr[c] : 0, s1 = valid ? b.ptr[c + 1] : 0;
     const T* gr = cell_grads<T>(b);
     const bool diff = sizeof(T) == 4;
-    const double4 ur = U4[b.nodes[s0]];
+    const double4 ur = s1 > s0 ? U4[b.nodes[s0]] : make_double4(0.0, 0.0, 0.0, 0.0);
     T H[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) H[k] = T(0);
-    for (int32_t s = s0 + lane; s < s1; s += 32) {
+    for (int32_t s = s0 + r; s < s1; s += LPC) {
         const double4 u = U4[b.nodes[s]];
         const T du[3] = {T(diff ? u.x - ur.x : u.x), T(diff ? u.y - ur.y : u.y), T(diff ? u.z - ur.z : u.z)};
         const T gg[3] = {gr[3 * s], gr[3 * s + 1], gr[3 * s + 2]};
@@ -560,16 +565,17 @@ __global__ void __launch_bounds__(256) k_cell_force_warp(CellBlockDev b, const d
 #pragma unroll
             for (int j = 0; j < 3; ++j) H[i * 3 + j] += du[i] * gg[j];
     }
-    // Butterfly reduction: fixed pairing, identical result on every lane.
+    // Butterfly over the group: fixed pairing, identical result on every lane.
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1)
+    for (int off = LPC / 2; off > 0; off >>= 1)
 #pragma unroll
-        for (int k = 0; k < 9; ++k) H[k] += __shfl_xor_sync(kFull, H[k], off);
+        for (int k = 0; k < 9; ++k) H[k] += __shfl_xor_sync(gmask, H[k], off);
+    if (!valid || s1 <= s0) return;
     double lam, mu;
     element_lame(b, c, lam, mu);
     T P[9];
     const double Jf = stress<T>(MAT, T(lam), T(mu), H, P);
-    if (lane == 0) {
+    if (r == 0) {
         if (MAT == kNeoHookean && !(Jf > 0.0)) flag(status, AM_ENONPOS_J, c);
         store_cell_stress<T>(cell_stress + 3 * (b.cell_base + c), P, T(b.volumes[c]));
     }
@@ -932,44 +938,59 @@ constexpr int kNodeBlock = 256;
 __device__ __forceinline__ int64_t cell_id(float w) { return __float_as_int(w); }
 __device__ __forceinline__ int64_t cell_id(double w) { return __double_as_longlong(w); }
 
-template <typename S, int BATCH>
-__device__ __forceinline__ void gather(const NodeDev& nd, const vec4_t<S>* __restrict__ slots, int64_t i, double& fx,
-                                       double& fy, double& fz) {
-    const int32_t p0 = nd.node_ptr[i], p1 = nd.node_ptr[i + 1];
+template <typename S, int BATCH, int LPN>
+__device__ __forceinline__ void gather(const NodeDev& nd, const vec4_t<S>* __restrict__ slots, int64_t i, bool own,
+                                       double& fx, double& fy, double& fz) {
+    // LPN lanes per node: lane r takes every LPN-th slot / cell entry from r, then the
+    // group's partial sums combine by a fixed butterfly (every lane gets the total).
+    const int r = LPN == 1 ? 0 : static_cast<int>(threadIdx.x % LPN);
     fx = fy = fz = 0.0;
-    for (int32_t p = p0; p < p1; p += BATCH) {
-        vec4_t<S> v[BATCH];
+    if (own) {
+        const int32_t p0 = nd.node_ptr[i], p1 = nd.node_ptr[i + 1];
+        for (int32_t p = p0 + r; p < p1; p += BATCH * LPN) {
+            vec4_t<S> v[BATCH];
 #pragma unroll
-        for (int k = 0; k < BATCH; ++k)
-            if (p + k < p1) v[k] = slots[p + k];
+            for (int k = 0; k < BATCH; ++k)
+                if (p + k * LPN < p1) v[k] = slots[p + k * LPN];
 #pragma unroll
-        for (int k = 0; k < BATCH; ++k)
-            if (p + k < p1) {
-                fx += static_cast<double>(v[k].x);
-                fy += static_cast<double>(v[k].y);
-                fz += static_cast<double>(v[k].z);
+            for (int k = 0; k < BATCH; ++k)
+                if (p + k * LPN < p1) {
+                    fx += static_cast<double>(v[k].x);
+                    fy += static_cast<double>(v[k].y);
+                    fz += static_cast<double>(v[k].z);
+                }
+        }
+        if (nd.cell_ptr != nullptr) {
+            // Cell entries of this node, in entry order: f += G_c b (G = -V P of cell c).
+            const vec4_t<S>* __restrict__ ent = static_cast<const vec4_t<S>*>(nd.cell_entries);
+            const vec4_t<S>* __restrict__ G = static_cast<const vec4_t<S>*>(nd.cell_stress);
+            const int32_t q0 = nd.cell_ptr[i], q1 = nd.cell_ptr[i + 1];
+            constexpr int CB = 4;
+            for (int32_t q = q0 + r; q < q1; q += CB * LPN) {
+                vec4_t<S> e[CB];
+#pragma unroll
+                for (int k = 0; k < CB; ++k)
+                    if (q + k * LPN < q1) e[k] = ent[q + k * LPN];
+#pragma unroll
+                for (int k = 0; k < CB; ++k)
+                    if (q + k * LPN < q1) {
+                        const int64_t c = cell_id(e[k].w);
+                        const vec4_t<S> g0 = G[3 * c], g1 = G[3 * c + 1], g2 = G[3 * c + 2];
+                        fx += static_cast<double>(g0.x * e[k].x + g0.y * e[k].y + g0.z * e[k].z);
+                        fy += static_cast<double>(g1.x * e[k].x + g1.y * e[k].y + g1.z * e[k].z);
+                        fz += static_cast<double>(g2.x * e[k].x + g2.y * e[k].y + g2.z * e[k].z);
+                    }
             }
+        }
     }
-    if (nd.cell_ptr == nullptr) return;
-    // Cell entries of this node, in entry order: f += G_c b (G = -V P of cell c).
-    const vec4_t<S>* __restrict__ ent = static_cast<const vec4_t<S>*>(nd.cell_entries);
-    const vec4_t<S>* __restrict__ G = static_cast<const vec4_t<S>*>(nd.cell_stress);
-    const int32_t q0 = nd.cell_ptr[i], q1 = nd.cell_ptr[i + 1];
-    constexpr int CB = 4;
-    for (int32_t q = q0; q < q1; q += CB) {
-        vec4_t<S> e[CB];
+    if (LPN > 1) {
+        const unsigned gmask = LPN == 32 ? kFull : (((1u << LPN) - 1u) << ((threadIdx.x & 31) & ~(LPN - 1)));
 #pragma unroll
-        for (int k = 0; k < CB; ++k)
-            if (q + k < q1) e[k] = ent[q + k];
-#pragma unroll
-        for (int k = 0; k < CB; ++k)
-            if (q + k < q1) {
-                const int64_t c = cell_id(e[k].w);
-                const vec4_t<S> g0 = G[3 * c], g1 = G[3 * c + 1], g2 = G[3 * c + 2];
-                fx += static_cast<double>(g0.x * e[k].x + g0.y * e[k].y + g0.z * e[k].z);
-                fy += static_cast<double>(g1.x * e[k].x + g1.y * e[k].y + g1.z * e[k].z);
-                fz += static_cast<double>(g2.x * e[k].x + g2.y * e[k].y + g2.z * e[k].z);
-            }
+        for (int off = LPN / 2; off > 0; off >>= 1) {
+            fx += __shfl_xor_sync(gmask, fx, off);
+            fy += __shfl_xor_sync(gmask, fy, off);
+            fz += __shfl_xor_sync(gmask, fz, off);
+        }
     }
 }
 
@@ -1000,13 +1021,15 @@ __device__ __forceinline__ void free_mask(uint32_t word, uint32_t active, double
     mz = ((word >> 20) & 0x3FFu & active) ? 0.0 : 1.0;
 }
 
-template <typename S, int BATCH>
+template <typename S, int BATCH, int LPN>
 __global__ void __launch_bounds__(kNodeBlock) k_gather_force(NodeDev nd, const vec4_t<S>* __restrict__ slots,
                                                               double* __restrict__ f, int accumulate) {
-    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= nd.num_nodes) return;
+    const int64_t i = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / LPN;
+    const bool own = i < nd.num_nodes;
+    if (LPN == 1 && !own) return;
     double fx, fy, fz;
-    gather<S, BATCH>(nd, slots, i, fx, fy, fz);
+    gather<S, BATCH, LPN>(nd, slots, i, own, fx, fy, fz);
+    if (!own || threadIdx.x % LPN != 0) return;
     if (accumulate) {
         f[3 * i + 0] += fx;
         f[3 * i + 1] += fy;
@@ -1018,13 +1041,15 @@ __global__ void __launch_bounds__(kNodeBlock) k_gather_force(NodeDev nd, const v
     }
 }
 
-template <typename S, int BATCH>
+template <typename S, int BATCH, int LPN>
 __global__ void __launch_bounds__(kNodeBlock) k_init_accel(NodeDev nd, const vec4_t<S>* __restrict__ slots,
                                                             double4* __restrict__ A4, int* status) {
-    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= nd.num_nodes) return;
+    const int64_t i = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / LPN;
+    const bool own = i < nd.num_nodes;
+    if (LPN == 1 && !own) return;
     double fx, fy, fz;
-    gather<S, BATCH>(nd, slots, i, fx, fy, fz);
+    gather<S, BATCH, LPN>(nd, slots, i, own, fx, fy, fz);
+    if (!own || threadIdx.x % LPN != 0) return;
     const double m = nd.mass[i];
     if (nd.has_g) {
         fx += nd.g[0] * m;
@@ -1055,21 +1080,24 @@ __global__ void __launch_bounds__(256) k_prologue(NodeDev nd, const StepParams* 
     if (u_copy) u_copy[i] = u;
 }
 
-template <typename S, int BATCH>
+template <typename S, int BATCH, int LPN>
 __global__ void __launch_bounds__(kNodeBlock) k_node_step(NodeDev nd, const vec4_t<S>* __restrict__ slots,
                                                            const StepParams* __restrict__ table, int64_t step,
                                                            int advance, double4* __restrict__ U4,
                                                            double4* __restrict__ V4, double4* __restrict__ A4,
                                                            double4* __restrict__ u_copy, int* status) {
-    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= nd.num_nodes) return;
+    const int64_t i = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / LPN;
+    const bool own = i < nd.num_nodes;
+    if (LPN == 1 && !own) return;
     // The node's own data is independent of the gather: issue its loads first.
-    const double m = nd.mass[i];
-    const uint32_t w = nd.bcword[i];
-    const double4 vh = V4[i];
-    const double4 u0 = advance ? U4[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+    const int64_t j = own ? i : 0;
+    const double m = nd.mass[j];
+    const uint32_t w = nd.bcword[j];
+    const double4 vh = V4[j];
+    const double4 u0 = advance ? U4[j] : make_double4(0.0, 0.0, 0.0, 0.0);
     double fx, fy, fz;
-    gather<S, BATCH>(nd, slots, i, fx, fy, fz);
+    gather<S, BATCH, LPN>(nd, slots, i, own, fx, fy, fz);
+    if (!own || threadIdx.x % LPN != 0) return;
     if (nd.has_g) {
         fx += nd.g[0] * m;
         fy += nd.g[1] * m;
@@ -1125,7 +1153,7 @@ __global__ void __launch_bounds__(kNodeBlock) k_adj_update(NodeDev nd, const dou
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= nd.num_nodes) return;
     double gx, gy, gz;
-    gather<double, 4>(nd, slots, i, gx, gy, gz);
+    gather<double, 4, 1>(nd, slots, i, true, gx, gy, gz);
     const StepParams& P = table[step];
     double4 ub = UB[i];
     const double4 vb = VB[i];
@@ -1351,6 +1379,16 @@ void launch_gauss_force(const GaussBlockDev& b, int mixed, const double4* X4, co
     }
 }
 
+// Lanes per cell from the block's mean entries per cell (about two entries per lane).
+inline int lanes_per_cell(const CellBlockDev& b, int64_t entries) {
+    const double mean = static_cast<double>(entries) / static_cast<double>(b.num_cells);
+    return mean <= 12.0 ? 4 : mean <= 24.0 ? 8 : mean <= 48.0 ? 16 : 32;
+}
+
+#define AM_CELL_GROUP(T, LPC)                                                                         \
+    AM_DISPATCH_MAT(b.material, (k_cell_force_group<T, M, LPC><<<grid_for(b.num_cells * LPC, 256), 256, 0, s>>>( \
+                                    b, U4, static_cast<vec4_t<T>*>(slots), status)))
+
 void launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void* slots, int* status,
                        cudaStream_t s) {
     if (b.num_cells == 0) return;
@@ -1361,12 +1399,28 @@ void launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void
         } else {
             AM_DISPATCH_MAT(b.material, (k_cell_force_thread<double, M><<<grid, 256, 0, s>>>(b, U4, static_cast<double4*>(slots), status)));
         }
-    } else {
-        const unsigned grid = grid_for(b.num_cells * 32, 256);
-        if (mixed) {
-            AM_DISPATCH_MAT(b.material, (k_cell_force_warp<float, M><<<grid, 256, 0, s>>>(b, U4, static_cast<float4*>(slots), status)));
+        return;
+    }
+    const int lpc = lanes_per_cell(b, b.num_entries);
+    if (mixed) {
+        if (lpc == 4) {
+            AM_CELL_GROUP(float, 4);
+        } else if (lpc == 8) {
+            AM_CELL_GROUP(float, 8);
+        } else if (lpc == 16) {
+            AM_CELL_GROUP(float, 16);
         } else {
-            AM_DISPATCH_MAT(b.material, (k_cell_force_warp<double, M><<<grid, 256, 0, s>>>(b, U4, static_cast<double4*>(slots), status)));
+            AM_CELL_GROUP(float, 32);
+        }
+    } else {
+        if (lpc == 4) {
+            AM_CELL_GROUP(double, 4);
+        } else if (lpc == 8) {
+            AM_CELL_GROUP(double, 8);
+        } else if (lpc == 16) {
+            AM_CELL_GROUP(double, 16);
+        } else {
+            AM_CELL_GROUP(double, 32);
         }
     }
 }
@@ -1406,31 +1460,39 @@ void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const dou
         k_gauss_volume_slots<<<grid_for(b.num_elems, 128), 128, 0, s>>>(b, density, X4, slots);
 }
 
-// BATCH = 8 when the slot array fits comfortably in L2 (126 MB on B200), else 4:
-// on B200 the eight-deep batch was ~10% faster for the 70^3 Tet4 mesh's 44 MB of
-// FP32 slots and ~5-10% slower for the 128^3 Hex8 mesh's 268 MB.
+// Per node the slots (and cell entries) are summed by LPN lanes: one lane for meshes
+// of Gauss elements (at most eight slots per node), four or eight for cell blocks
+// with tens of entries per node. With one lane, BATCH = 8 when the slot array fits
+// comfortably in L2 (126 MB on B200), else 4: on B200 the eight-deep batch was ~10%
+// faster for the 70^3 Tet4 mesh's 44 MB of FP32 slots and ~5-10% slower for the
+// 128^3 Hex8 mesh's 268 MB.
+inline int node_lanes(const NodeDev& nd) {
+    const double per_node = static_cast<double>(nd.num_slots + nd.num_cell_entries) / static_cast<double>(nd.num_nodes);
+    return per_node <= 12.0 ? 1 : per_node <= 40.0 ? 4 : 8;
+}
 inline bool gather_batch8(const NodeDev& nd, int mixed) {
     const int64_t bytes = nd.num_slots * (mixed ? 16 : 32);
     return bytes <= (int64_t{64} << 20);
 }
 
-#define AM_NODE_DISPATCH(KERNEL, ...)                                                    \
-    do {                                                                                 \
-        const unsigned grid = grid_for(nd.num_nodes, kNodeBlock);                        \
-        const bool b8 = gather_batch8(nd, mixed);                                        \
-        if (mixed) {                                                                     \
-            const float4* sl = static_cast<const float4*>(slots);                        \
-            if (b8)                                                                      \
-                KERNEL<float, 8><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);        \
-            else                                                                         \
-                KERNEL<float, 4><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);        \
-        } else {                                                                         \
-            const double4* sl = static_cast<const double4*>(slots);                      \
-            if (b8)                                                                      \
-                KERNEL<double, 8><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);       \
-            else                                                                         \
-                KERNEL<double, 4><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);       \
-        }                                                                                \
+#define AM_NODE_DISPATCH(KERNEL, ...)                                                                 \
+    do {                                                                                              \
+        const int lpn = node_lanes(nd);                                                               \
+        const unsigned grid = grid_for(nd.num_nodes * lpn, kNodeBlock);                               \
+        const bool b8 = gather_batch8(nd, mixed);                                                     \
+        if (mixed) {                                                                                  \
+            const float4* sl = static_cast<const float4*>(slots);                                     \
+            if (lpn == 8) KERNEL<float, 2, 8><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);        \
+            else if (lpn == 4) KERNEL<float, 2, 4><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);   \
+            else if (b8) KERNEL<float, 8, 1><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);         \
+            else KERNEL<float, 4, 1><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);                 \
+        } else {                                                                                      \
+            const double4* sl = static_cast<const double4*>(slots);                                   \
+            if (lpn == 8) KERNEL<double, 2, 8><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);       \
+            else if (lpn == 4) KERNEL<double, 2, 4><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);  \
+            else if (b8) KERNEL<double, 8, 1><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);        \
+            else KERNEL<double, 4, 1><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);                \
+        }                                                                                             \
     } while (0)
 
 void launch_gather_force(const NodeDev& nd, int mixed, const void* slots, double* f, int accumulate, cudaStream_t s) {

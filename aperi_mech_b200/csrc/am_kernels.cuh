@@ -60,7 +60,8 @@ struct CellBlockDev {
     const double* mu_field;
     const double* kappa_field;
     int64_t cell_base;          // index of the block's first cell in the context's cell-stress array
-    int32_t max_entries;        // longest cell (selects thread- or warp-per-cell)
+    int64_t num_entries;        // ptr[num_cells]
+    int32_t max_entries;        // longest cell (selects thread- or group-per-cell)
 };
 
 // Node gather + nodal update configuration.
@@ -76,6 +77,7 @@ struct NodeDev {
     // Smoothed/RKPM cells contribute through their cell stresses instead of slots:
     // node i adds G_c b_{c,i} for each entry of [cell_ptr[i], cell_ptr[i+1]).
     const int32_t* cell_ptr;    // num_nodes + 1, or null when there are no cell blocks
+    int64_t num_cell_entries;   // cell_ptr[num_nodes]
     const void* cell_entries;   // per entry: (b_x, b_y, b_z, cell id bits) as float4 / double4
     const void* cell_stress;    // per cell: the rows of G = -V P as 3 float4 / double4
 };
