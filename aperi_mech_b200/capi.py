@@ -113,7 +113,7 @@ def load(build_if_missing: bool = False) -> C.CDLL:
         "am_cells_get": (C.c_int, [vp, _lp, _ip, _dp, _dp, _dp]),
         "am_cells_get_points": (C.c_int, [vp, _dp, _lp, _ip, _dp]),
         "am_cells_destroy": (None, [vp]),
-        "am_get_layout": (C.c_int, [vp, _lp, _ip, _lp]),
+        "am_get_layout": (C.c_int, [vp, _lp, _ip]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

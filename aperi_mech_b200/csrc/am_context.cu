@@ -73,12 +73,6 @@ struct Block {
     uint32_t* patch_gather = nullptr;
     const int32_t* slot_pos = nullptr;  // block-local view into the context's position array
     std::vector<int32_t> host_nodes;    // node of each logical slot (-1: unused), for the node CSR
-    // Cell blocks: position of the first cell in the context's cell-stress array, and the
-    // host copies of the entries that am_finalize turns into the node-major entry list.
-    int64_t cell_base = 0;
-    int64_t cell_entries = 0;
-    std::vector<int32_t> host_cell_ptr, host_cell_nodes;
-    std::vector<double> host_cell_grads;
 
     am::GaussBlockDev gauss() const {
         am::GaussBlockDev g{};
@@ -112,8 +106,8 @@ struct Block {
         c.volumes = volumes;
         c.mu_field = mu_field;
         c.kappa_field = kappa_field;
-        c.cell_base = cell_base;
-        c.num_entries = cell_entries;
+        c.slot_pos = slot_pos;
+        c.num_entries = num_entries;
         c.max_entries = max_entries;
         return c;
     }
@@ -219,14 +213,6 @@ struct am_ctx {
     float4* slots32 = nullptr;     // node-major force slots (mixed path)
     int64_t num_slots = 0;         // logical slots
     int64_t num_used_slots = 0;    // slots referenced by a node
-    // Smoothed/RKPM cells: per-cell stresses G = -V P and the node-major entry list.
-    int64_t num_cells_total = 0;
-    int64_t num_cell_entries = 0;
-    int32_t* cell_node_ptr = nullptr;   // N + 1
-    double4* cell_entries64 = nullptr;  // (b, cell id bits) per entry, node-major
-    float4* cell_entries32 = nullptr;   // FP32 copy (mixed path), made on first use
-    double4* cell_stress64 = nullptr;   // 3 rows per cell
-    float4* cell_stress32 = nullptr;
     std::vector<double4*> adj_bufs;  // cached adjoint checkpoint / segment buffers
     int64_t adj_key[3] = {0, 0, 0};
     bool tet4_patches = true;  // APERI_B200_TET4_PATCHES=0 turns element patching off
@@ -248,15 +234,8 @@ struct am_ctx {
     std::vector<std::pair<int, int64_t>> mark_slot;
     size_t n_marks = 0;
 
-    am::NodeDev node_dev(int mixed) {
+    am::NodeDev node_dev() const {
         am::NodeDev nd{};
-        if (num_cells_total > 0) {
-            if (mixed) prepare_mixed();
-            nd.cell_ptr = cell_node_ptr;
-            nd.num_cell_entries = num_cell_entries;
-            nd.cell_entries = mixed ? static_cast<const void*>(cell_entries32) : cell_entries64;
-            nd.cell_stress = mixed ? static_cast<const void*>(cell_stress32) : cell_stress64;
-        }
         nd.num_nodes = N;
         nd.node_ptr = node_ptr;
         nd.mass = mass;
@@ -276,21 +255,9 @@ struct am_ctx {
         return t;
     }
 
-    // Buffers of the mixed path, allocated on its first use.
-    void prepare_mixed() {
-        if (!slots32) slots32 = dalloc<float4>(static_cast<size_t>(std::max<int64_t>(num_used_slots, 1)), "slot buffer (FP32)");
-        if (num_cells_total > 0 && !cell_stress32) {
-            cell_stress32 = dalloc<float4>(static_cast<size_t>(3 * num_cells_total), "cell stress (FP32)");
-            cell_entries32 = dalloc<float4>(static_cast<size_t>(std::max<int64_t>(num_cell_entries, 1)), "cell entries (FP32)");
-            am::launch_cell_entries_fp32(cell_entries64, cell_entries32, num_cell_entries, stream);
-            ++launches;
-            ck(cudaGetLastError(), "cell entry conversion");
-        }
-    }
-
     void* slots(int mixed) {
         if (mixed) {
-            prepare_mixed();
+            if (!slots32) slots32 = dalloc<float4>(static_cast<size_t>(num_used_slots), "slot buffer (FP32)");
             return slots32;
         }
         return slots64;
@@ -306,8 +273,7 @@ struct am_ctx {
         for (const auto& b : blocks) {
             if (b.kind == AM_SMOOTHED_CELLS) {
                 if (mixed && !b.grads32) fail(AM_ESTATE, "mixed precision needs FP32 cell gradients");
-                void* cs = mixed ? static_cast<void*>(cell_stress32) : static_cast<void*>(cell_stress64);
-                am::launch_cell_force(b.cells(), mixed, U, cs, status, stream);
+                am::launch_cell_force(b.cells(), mixed, U, s, status, stream);
             } else {
                 am::launch_gauss_force(b.gauss(), mixed, X4, U, s, status, stream);
             }
@@ -322,7 +288,7 @@ struct am_ctx {
             double* gm = gmu ? gmu + off : nullptr;
             double* gk = gkappa ? gkappa + off : nullptr;
             if (b.kind == AM_SMOOTHED_CELLS)
-                am::launch_cell_vjp(b.cells(), U, L, cell_stress64, gm, gk, accumulate, stream);
+                am::launch_cell_vjp(b.cells(), U, L, slots64, gm, gk, accumulate, stream);
             else
                 am::launch_gauss_vjp(b.gauss(), X4, U, L, slots64, gm, gk, accumulate, stream);
             ++launches;
@@ -423,8 +389,8 @@ struct am_ctx {
     void run_range(int mixed, int64_t n0, int64_t n1, double4* const* u_hist) {
         if (n1 <= n0) return;
         if (profiling) reserve_marks(n_marks + static_cast<size_t>(2 * (n1 - n0) + 2));
+        const am::NodeDev nd = node_dev();
         void* s = slots(mixed);
-        const am::NodeDev nd = node_dev(mixed);
         mark(-1, 0);
         am::launch_prologue(nd, table + n0, U4, V4, A4, u_hist ? u_hist[0] : nullptr, stream);
         ++launches;
@@ -444,8 +410,7 @@ struct am_ctx {
 
     void init_acceleration(int mixed) {
         element_forces(mixed, U4);
-        void* s = slots(mixed);
-        am::launch_init_accel(node_dev(mixed), mixed, s, A4, status, stream);
+        am::launch_init_accel(node_dev(), mixed, slots(mixed), A4, status, stream);
         ++launches;
         check_launch("init acceleration kernel");
     }
@@ -472,11 +437,6 @@ struct am_ctx {
         dfree(slot_pos);
         dfree(slots64);
         dfree(slots32);
-        dfree(cell_node_ptr);
-        dfree(cell_entries64);
-        dfree(cell_entries32);
-        dfree(cell_stress64);
-        dfree(cell_stress32);
         for (auto& pbuf : adj_bufs) dfree(pbuf);
         adj_bufs.clear();
         dfree(table);
@@ -709,13 +669,7 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
                     b.volumes = dalloc<double>(E, "cell volumes");
                     ck(cudaMemcpy(b.volumes, d->cell_volumes, E * sizeof(double), cudaMemcpyHostToDevice), "upload");
                 }
-                // Cells add no slots: their entries reach the nodes through the cell stresses.
-                b.num_entries = 0;
-                b.cell_entries = K;
-                b.cell_base = ctx->num_cells_total;
-                b.host_cell_ptr = std::move(ptr);
-                b.host_cell_nodes.assign(d->cell_nodes, d->cell_nodes + K);
-                b.host_cell_grads.assign(d->cell_grads, d->cell_grads + 3 * K);
+                b.host_nodes.assign(d->cell_nodes, d->cell_nodes + K);
             } else {
                 const int nn = d->kind == AM_HEX8_GAUSS ? 8 : 4;
                 if (E > 0 && !d->conn) fail(AM_EINVAL, "null connectivity");
@@ -779,7 +733,6 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
             throw;
         }
         ctx->num_slots += b.num_entries;
-        if (b.kind == AM_SMOOTHED_CELLS) ctx->num_cells_total += b.num_elems;
         ctx->blocks.push_back(std::move(b));
         if (block_id) *block_id = static_cast<int32_t>(ctx->blocks.size() - 1);
     });
@@ -894,41 +847,6 @@ int am_finalize(am_ctx* ctx) {
             b.slot_pos = ctx->slot_pos + b.slot_base;
             std::vector<int32_t>().swap(b.host_nodes);
         }
-        if (ctx->num_cells_total > 0) {
-            // Node-major cell entries: node i's entries in block order, cell order, entry
-            // order, each carrying its gradient and its cell's index in the stress array.
-            std::vector<int64_t> cptr(N + 1, 0);
-            for (const auto& b : ctx->blocks)
-                for (int32_t n : b.host_cell_nodes) ++cptr[n + 1];
-            for (int64_t i = 0; i < N; ++i) cptr[i + 1] += cptr[i];
-            const int64_t K = cptr[N];
-            if (K >= (int64_t(1) << 31)) fail(AM_ERANGE, "cell entry count beyond int32 indexing");
-            std::vector<double4> ent(static_cast<size_t>(std::max<int64_t>(K, 1)));
-            std::vector<int64_t> cfill(cptr.begin(), cptr.end() - 1);
-            for (const auto& b : ctx->blocks) {
-                const int64_t C = static_cast<int64_t>(b.host_cell_ptr.empty() ? 0 : b.host_cell_ptr.size() - 1);
-                for (int64_t c = 0; c < C; ++c)
-                    for (int32_t k = b.host_cell_ptr[c]; k < b.host_cell_ptr[c + 1]; ++k) {
-                        const int64_t id = b.cell_base + c;
-                        double w;
-                        std::memcpy(&w, &id, sizeof(w));
-                        ent[cfill[b.host_cell_nodes[k]]++] = make_double4(b.host_cell_grads[3 * k], b.host_cell_grads[3 * k + 1],
-                                                                          b.host_cell_grads[3 * k + 2], w);
-                    }
-            }
-            std::vector<int32_t> cptr32(cptr.begin(), cptr.end());
-            ctx->num_cell_entries = K;
-            ctx->cell_node_ptr = dalloc<int32_t>(N + 1, "cell entry ptr");
-            ck(cudaMemcpy(ctx->cell_node_ptr, cptr32.data(), (N + 1) * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
-            ctx->cell_entries64 = dalloc<double4>(ent.size(), "cell entries");
-            ck(cudaMemcpy(ctx->cell_entries64, ent.data(), ent.size() * sizeof(double4), cudaMemcpyHostToDevice), "upload");
-            ctx->cell_stress64 = dalloc<double4>(static_cast<size_t>(3 * ctx->num_cells_total), "cell stress");
-            for (auto& b : ctx->blocks) {
-                std::vector<int32_t>().swap(b.host_cell_ptr);
-                std::vector<int32_t>().swap(b.host_cell_nodes);
-                std::vector<double>().swap(b.host_cell_grads);
-            }
-        }
         bool has_cells = false;
         for (const auto& b : ctx->blocks) has_cells |= b.kind == AM_SMOOTHED_CELLS;
         if (!ctx->mass_set) {
@@ -938,7 +856,7 @@ int am_finalize(am_ctx* ctx) {
                 am::launch_gauss_volume_slots(b.gauss(), b.density, ctx->X4, ctx->slots64, ctx->stream);
                 ++ctx->launches;
             }
-            am::launch_gather_force(ctx->node_dev(0), 0, ctx->slots64, ctx->f_scratch, 0, ctx->stream);
+            am::launch_gather_force(ctx->node_dev(), 0, ctx->slots64, ctx->f_scratch, 0, ctx->stream);
             ++ctx->launches;
             ck(cudaGetLastError(), "mass kernels");
             std::vector<double> f(N * 3), m(N);
@@ -994,8 +912,7 @@ int am_internal_force(am_ctx* ctx, am_precision prec, am_memory where, const dou
         double* out = ctx->f_scratch;
         if (where == AM_DEVICE) out = f;
         else if (accumulate) ck(cudaMemcpyAsync(out, f, ctx->N * 3 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream), "H2D");
-        void* sl = ctx->slots(mixed);
-        am::launch_gather_force(ctx->node_dev(mixed), mixed, sl, out, accumulate, ctx->stream);
+        am::launch_gather_force(ctx->node_dev(), mixed, ctx->slots(mixed), out, accumulate, ctx->stream);
         ++ctx->launches;
         ck(cudaGetLastError(), "gather kernel");
         if (where == AM_HOST)
@@ -1067,7 +984,7 @@ int am_vjp_force(am_ctx* ctx, am_memory where, const double* u, const double* la
         }
         ctx->vjp(ctx->W4, ctx->L4, gm, gk, 0);
         double* out = where == AM_DEVICE ? gu : ctx->f_scratch;
-        am::launch_gather_force(ctx->node_dev(0), 0, ctx->slots64, out, 0, ctx->stream);
+        am::launch_gather_force(ctx->node_dev(), 0, ctx->slots64, out, 0, ctx->stream);
         ++ctx->launches;
         ck(cudaGetLastError(), "gather kernel");
         if (where == AM_HOST) {
@@ -1153,7 +1070,7 @@ int am_adjoint(am_ctx* ctx, int64_t nsteps, double dt, int32_t ckpt_every, int32
         am::launch_zero4(AB, ctx->N, st);
         am::launch_sensor_seed(ctx->U4, num_sensors, dsens, UB, dloss, st);
         ctx->launches += 4;
-        const am::NodeDev nd = ctx->node_dev(0);
+        const am::NodeDev nd = ctx->node_dev();
         am::launch_adj_prep(nd, ctx->table, nsteps - 1, VB, AB, ctx->L4, st);
         ++ctx->launches;
         // Reverse pass, one segment at a time: recompute the segment's displacements
@@ -1278,10 +1195,9 @@ int am_complete_properties(double props[5], char* msg, int msg_len) {
 
 int64_t am_launch_count(const am_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
-int am_get_layout(const am_ctx* ctx, int64_t* used_slots, int32_t* patched_tet4_blocks, int64_t* cell_entries) {
+int am_get_layout(const am_ctx* ctx, int64_t* used_slots, int32_t* patched_tet4_blocks) {
     if (!ctx) return AM_EINVAL;
     if (used_slots) *used_slots = ctx->num_used_slots;
-    if (cell_entries) *cell_entries = ctx->num_cell_entries;
     if (patched_tet4_blocks) {
         int32_t n = 0;
         for (const auto& b : ctx->blocks) n += b.patched ? 1 : 0;

@@ -486,20 +486,10 @@ __global__ void __launch_bounds__(128, sizeof(T) == 8 ? 1 : 4) k_hex8_force(Gaus
 
 // ---------------------------------------------------------------------------
 // Smoothed / RKPM cells (ComputeInternalForceSmoothedCell.h:416-442, no F-bar):
-// H = sum_k u_k (x) b_k ; P(H) ; f_k = -V b_k P^T. The cell kernel stops at the cell
-// stress G = -V P (nine numbers per cell, stored as three padded rows); the node
-// kernel forms f_k = G b_k from its node-major copy of the entries. Each entry's
-// gradient is read once per kernel and no per-entry force is written, which for
-// RKPM cells (tens of entries each) removes a third of the step's HBM traffic.
+// H = sum_k u_k (x) b_k ; P(H) ; f_k = -V b_k P^T written to the cell's slots.
 // The mixed path subtracts the first entry's displacement (partition of nullity
 // makes H invariant) before casting to FP32.
 // ---------------------------------------------------------------------------
-template <typename T>
-__device__ __forceinline__ void store_cell_stress(vec4_t<T>* __restrict__ G, const T* P, T V) {
-    G[0] = make4(-V * P[0], -V * P[1], -V * P[2]);
-    G[1] = make4(-V * P[3], -V * P[4], -V * P[5]);
-    G[2] = make4(-V * P[6], -V * P[7], -V * P[8]);
-}
 template <typename T>
 __device__ __forceinline__ const T* cell_grads(const CellBlockDev& b);
 template <>
@@ -509,7 +499,7 @@ __device__ __forceinline__ const float* cell_grads<float>(const CellBlockDev& b)
 
 template <typename T, int MAT>
 __global__ void __launch_bounds__(256) k_cell_force_thread(CellBlockDev b, const double4* __restrict__ U4,
-                                                            vec4_t<T>* __restrict__ cell_stress, int* status) {
+                                                            vec4_t<T>* __restrict__ slots, int* status) {
     const int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (c >= b.num_cells) return;
     const int32_t s0 = b.ptr[c], s1 = b.ptr[c + 1];
@@ -534,16 +524,24 @@ __global__ void __launch_bounds__(256) k_cell_force_thread(CellBlockDev b, const
     T P[9];
     const double Jf = stress<T>(MAT, T(lam), T(mu), H, P);
     if (MAT == kNeoHookean && !(Jf > 0.0)) flag(status, AM_ENONPOS_J, c);
-    store_cell_stress<T>(cell_stress + 3 * (b.cell_base + c), P, T(b.volumes[c]));
+    const T V = T(b.volumes[c]);
+    for (int32_t s = s0; s < s1; ++s) {
+        const T gg[3] = {gr[3 * s], gr[3 * s + 1], gr[3 * s + 2]};
+        T f[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) f[i] = (gg[0] * P[i * 3 + 0] + gg[1] * P[i * 3 + 1] + gg[2] * P[i * 3 + 2]) * -V;
+        slots[b.slot_pos[s]] = make4(f[0], f[1], f[2]);
+    }
 }
 
 // LPC lanes per cell (a power of two up to 32): the group strides over the cell's
-// entries, combines its partial H by a butterfly over the group, and every lane of
-// the group then holds the same H. Narrow groups keep the lanes busy on cells of a
-// few tens of entries and repeat the stress update on fewer lanes.
+// entries, combines its partial H by a butterfly over the group (every lane then
+// holds the same H and P), and each lane writes the forces of its own entries.
+// Narrow groups keep the lanes busy on cells of a few tens of entries and repeat
+// the stress update on fewer lanes.
 template <typename T, int MAT, int LPC>
 __global__ void __launch_bounds__(256) k_cell_force_group(CellBlockDev b, const double4* __restrict__ U4,
-                                                          vec4_t<T>* __restrict__ cell_stress, int* status) {
+                                                          vec4_t<T>* __restrict__ slots, int* status) {
     const int64_t gt = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const int64_t c = gt / LPC;
     const int r = static_cast<int>(threadIdx.x % LPC);
@@ -575,9 +573,14 @@ __global__ void __launch_bounds__(256) k_cell_force_group(CellBlockDev b, const 
     element_lame(b, c, lam, mu);
     T P[9];
     const double Jf = stress<T>(MAT, T(lam), T(mu), H, P);
-    if (r == 0) {
-        if (MAT == kNeoHookean && !(Jf > 0.0)) flag(status, AM_ENONPOS_J, c);
-        store_cell_stress<T>(cell_stress + 3 * (b.cell_base + c), P, T(b.volumes[c]));
+    if (r == 0 && MAT == kNeoHookean && !(Jf > 0.0)) flag(status, AM_ENONPOS_J, c);
+    const T V = T(b.volumes[c]);
+    for (int32_t s = s0 + r; s < s1; s += LPC) {
+        const T gg[3] = {gr[3 * s], gr[3 * s + 1], gr[3 * s + 2]};
+        T f[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) f[i] = (gg[0] * P[i * 3 + 0] + gg[1] * P[i * 3 + 1] + gg[2] * P[i * 3 + 2]) * -V;
+        slots[b.slot_pos[s]] = make4(f[0], f[1], f[2]);
     }
 }
 
@@ -808,7 +811,7 @@ __global__ void __launch_bounds__(128) k_hex8_vjp(GaussBlockDev b, const double4
 
 template <int MAT>
 __global__ void __launch_bounds__(256) k_cell_vjp(CellBlockDev b, const double4* __restrict__ U4,
-                                                   const double4* __restrict__ L4, double4* __restrict__ cell_stress,
+                                                   const double4* __restrict__ L4, double4* __restrict__ slots,
                                                    double* gmu, double* gk, int accumulate) {
     const int lane = threadIdx.x & 31;
     const int64_t c = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
@@ -842,10 +845,14 @@ __global__ void __launch_bounds__(256) k_cell_vjp(CellBlockDev b, const double4*
     double dP[9], ldl, ldm;
     stress_vjp(MAT, lam, mu, H, L, dP, &ldl, &ldm);
     const double V = b.volumes[c];
-    if (lane == 0) {
-        store_cell_stress<double>(cell_stress + 3 * (b.cell_base + c), dP, V);
-        store_theta(gmu, gk, c, -V * (ldm - 2.0 / 3.0 * ldl), -V * ldl, accumulate);
+    for (int32_t s = s0 + lane; s < s1; s += 32) {
+        const double gg[3] = {b.grads64[3 * s], b.grads64[3 * s + 1], b.grads64[3 * s + 2]};
+        double f[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) f[i] = (gg[0] * dP[i * 3 + 0] + gg[1] * dP[i * 3 + 1] + gg[2] * dP[i * 3 + 2]) * -V;
+        slots[b.slot_pos[s]] = make4(f[0], f[1], f[2]);
     }
+    if (lane == 0) store_theta(gmu, gk, c, -V * (ldm - 2.0 / 3.0 * ldl), -V * ldl, accumulate);
 }
 
 // ---------------------------------------------------------------------------
@@ -935,14 +942,12 @@ constexpr int kNodeBlock = 256;
 // takes every slot in one round; that wins when the slot array sits in L2 (the
 // loads are latency-bound), while BATCH = 4 keeps more warps resident, which wins
 // when the slots stream from HBM (see gather_batch8).
-__device__ __forceinline__ int64_t cell_id(float w) { return __float_as_int(w); }
-__device__ __forceinline__ int64_t cell_id(double w) { return __double_as_longlong(w); }
-
 template <typename S, int BATCH, int LPN>
 __device__ __forceinline__ void gather(const NodeDev& nd, const vec4_t<S>* __restrict__ slots, int64_t i, bool own,
                                        double& fx, double& fy, double& fz) {
-    // LPN lanes per node: lane r takes every LPN-th slot / cell entry from r, then the
-    // group's partial sums combine by a fixed butterfly (every lane gets the total).
+    // LPN lanes per node: lane r takes every LPN-th slot from r (the group reads the
+    // node's contiguous range with coalesced loads), then the partial sums combine by
+    // a fixed butterfly, so every lane holds the same total and the order is fixed.
     const int r = LPN == 1 ? 0 : static_cast<int>(threadIdx.x % LPN);
     fx = fy = fz = 0.0;
     if (own) {
@@ -959,28 +964,6 @@ __device__ __forceinline__ void gather(const NodeDev& nd, const vec4_t<S>* __res
                     fy += static_cast<double>(v[k].y);
                     fz += static_cast<double>(v[k].z);
                 }
-        }
-        if (nd.cell_ptr != nullptr) {
-            // Cell entries of this node, in entry order: f += G_c b (G = -V P of cell c).
-            const vec4_t<S>* __restrict__ ent = static_cast<const vec4_t<S>*>(nd.cell_entries);
-            const vec4_t<S>* __restrict__ G = static_cast<const vec4_t<S>*>(nd.cell_stress);
-            const int32_t q0 = nd.cell_ptr[i], q1 = nd.cell_ptr[i + 1];
-            constexpr int CB = 4;
-            for (int32_t q = q0 + r; q < q1; q += CB * LPN) {
-                vec4_t<S> e[CB];
-#pragma unroll
-                for (int k = 0; k < CB; ++k)
-                    if (q + k * LPN < q1) e[k] = ent[q + k * LPN];
-#pragma unroll
-                for (int k = 0; k < CB; ++k)
-                    if (q + k * LPN < q1) {
-                        const int64_t c = cell_id(e[k].w);
-                        const vec4_t<S> g0 = G[3 * c], g1 = G[3 * c + 1], g2 = G[3 * c + 2];
-                        fx += static_cast<double>(g0.x * e[k].x + g0.y * e[k].y + g0.z * e[k].z);
-                        fy += static_cast<double>(g1.x * e[k].x + g1.y * e[k].y + g1.z * e[k].z);
-                        fz += static_cast<double>(g2.x * e[k].x + g2.y * e[k].y + g2.z * e[k].z);
-                    }
-            }
         }
     }
     if (LPN > 1) {
@@ -1205,16 +1188,6 @@ __global__ void __launch_bounds__(256) k_sensor_seed(const double4* __restrict__
     if (threadIdx.x == 0) *loss = part[0];
 }
 
-// FP32 copy of the node-major cell entries: gradient rounded to FP32, cell id moved
-// from the FP64 word's bits to the FP32 word's bits.
-__global__ void k_cell_entries_fp32(const double4* __restrict__ in, float4* __restrict__ out, int64_t n) {
-    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const double4 e = in[i];
-    out[i] = make_float4(static_cast<float>(e.x), static_cast<float>(e.y), static_cast<float>(e.z),
-                         __int_as_float(static_cast<int>(__double_as_longlong(e.w))));
-}
-
 __global__ void k_pack4(const double* __restrict__ in, double4* __restrict__ out, int64_t n) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -1379,18 +1352,18 @@ void launch_gauss_force(const GaussBlockDev& b, int mixed, const double4* X4, co
     }
 }
 
-// Lanes per cell from the block's mean entries per cell (about two entries per lane).
-inline int lanes_per_cell(const CellBlockDev& b, int64_t entries) {
-    const double mean = static_cast<double>(entries) / static_cast<double>(b.num_cells);
-    return mean <= 12.0 ? 4 : mean <= 24.0 ? 8 : mean <= 48.0 ? 16 : 32;
+// Lanes per cell from the block's mean entries per cell: on B200, eight lanes for the
+// RKPM nodal cells (about 66 entries) ran the kernel 1.55x faster than a full warp.
+inline int lanes_per_cell(const CellBlockDev& b) {
+    const double mean = static_cast<double>(b.num_entries) / static_cast<double>(b.num_cells);
+    return mean <= 16.0 ? 4 : mean <= 96.0 ? 8 : mean <= 192.0 ? 16 : 32;
 }
 
 #define AM_CELL_GROUP(T, LPC)                                                                         \
     AM_DISPATCH_MAT(b.material, (k_cell_force_group<T, M, LPC><<<grid_for(b.num_cells * LPC, 256), 256, 0, s>>>( \
                                     b, U4, static_cast<vec4_t<T>*>(slots), status)))
 
-void launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void* slots, int* status,
-                       cudaStream_t s) {
+void launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void* slots, int* status, cudaStream_t s) {
     if (b.num_cells == 0) return;
     if (b.max_entries <= 8) {
         const unsigned grid = grid_for(b.num_cells, 256);
@@ -1401,7 +1374,7 @@ void launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void
         }
         return;
     }
-    const int lpc = lanes_per_cell(b, b.num_entries);
+    const int lpc = lanes_per_cell(b);
     if (mixed) {
         if (lpc == 4) {
             AM_CELL_GROUP(float, 4);
@@ -1440,15 +1413,11 @@ void launch_gauss_vjp(const GaussBlockDev& b, const double4* X4, const double4* 
     }
 }
 
-void launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double4* cell_stress, double* gmu,
+void launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double4* slots, double* gmu,
                      double* gkappa, int accumulate, cudaStream_t s) {
     if (b.num_cells == 0) return;
     const unsigned grid = grid_for(b.num_cells * 32, 256);
-    AM_DISPATCH_MAT(b.material, (k_cell_vjp<M><<<grid, 256, 0, s>>>(b, U4, L4, cell_stress, gmu, gkappa, accumulate)));
-}
-
-void launch_cell_entries_fp32(const double4* in, float4* out, int64_t n, cudaStream_t s) {
-    if (n > 0) k_cell_entries_fp32<<<grid_for(n, 256), 256, 0, s>>>(in, out, n);
+    AM_DISPATCH_MAT(b.material, (k_cell_vjp<M><<<grid, 256, 0, s>>>(b, U4, L4, slots, gmu, gkappa, accumulate)));
 }
 
 void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const double4* X4, double4* slots,
@@ -1460,14 +1429,14 @@ void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const dou
         k_gauss_volume_slots<<<grid_for(b.num_elems, 128), 128, 0, s>>>(b, density, X4, slots);
 }
 
-// Per node the slots (and cell entries) are summed by LPN lanes: one lane for meshes
-// of Gauss elements (at most eight slots per node), four or eight for cell blocks
-// with tens of entries per node. With one lane, BATCH = 8 when the slot array fits
-// comfortably in L2 (126 MB on B200), else 4: on B200 the eight-deep batch was ~10%
-// faster for the 70^3 Tet4 mesh's 44 MB of FP32 slots and ~5-10% slower for the
-// 128^3 Hex8 mesh's 268 MB.
+// Per node the slots are summed by LPN lanes: one lane for meshes of Gauss elements
+// (at most eight slots per node), four or eight for cell blocks with tens of
+// entries per node. With one lane, BATCH = 8 when the slot array fits comfortably
+// in L2 (126 MB on B200), else 4: on B200 the eight-deep batch was ~10% faster for
+// the 70^3 Tet4 mesh's 44 MB of FP32 slots and ~5-10% slower for the 128^3 Hex8
+// mesh's 268 MB.
 inline int node_lanes(const NodeDev& nd) {
-    const double per_node = static_cast<double>(nd.num_slots + nd.num_cell_entries) / static_cast<double>(nd.num_nodes);
+    const double per_node = static_cast<double>(nd.num_slots) / static_cast<double>(nd.num_nodes);
     return per_node <= 12.0 ? 1 : per_node <= 40.0 ? 4 : 8;
 }
 inline bool gather_batch8(const NodeDev& nd, int mixed) {

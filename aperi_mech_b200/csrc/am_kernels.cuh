@@ -59,7 +59,7 @@ struct CellBlockDev {
     const double* volumes;
     const double* mu_field;
     const double* kappa_field;
-    int64_t cell_base;          // index of the block's first cell in the context's cell-stress array
+    const int32_t* slot_pos;    // entry -> node-major position
     int64_t num_entries;        // ptr[num_cells]
     int32_t max_entries;        // longest cell (selects thread- or group-per-cell)
 };
@@ -74,24 +74,16 @@ struct NodeDev {
     double g[3];                // body acceleration
     int32_t has_g;
     int64_t num_slots;          // node_ptr[num_nodes]: force slots in use
-    // Smoothed/RKPM cells contribute through their cell stresses instead of slots:
-    // node i adds G_c b_{c,i} for each entry of [cell_ptr[i], cell_ptr[i+1]).
-    const int32_t* cell_ptr;    // num_nodes + 1, or null when there are no cell blocks
-    int64_t num_cell_entries;   // cell_ptr[num_nodes]
-    const void* cell_entries;   // per entry: (b_x, b_y, b_z, cell id bits) as float4 / double4
-    const void* cell_stress;    // per cell: the rows of G = -V P as 3 float4 / double4
 };
 
 // ---- launchers (am_kernels.cu) ----
 void launch_gauss_force(const GaussBlockDev& b, int mixed, const double4* X4, const double4* U4, void* slots,
                         int* status, cudaStream_t s);
-void launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void* cell_stress, int* status,
-                       cudaStream_t s);
+void launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void* slots, int* status, cudaStream_t s);
 void launch_gauss_vjp(const GaussBlockDev& b, const double4* X4, const double4* U4, const double4* L4, double4* slots,
                       double* gmu, double* gkappa, int accumulate, cudaStream_t s);
-void launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double4* cell_stress, double* gmu,
+void launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double4* slots, double* gmu,
                      double* gkappa, int accumulate, cudaStream_t s);
-void launch_cell_entries_fp32(const double4* in, float4* out, int64_t n, cudaStream_t s);
 void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const double4* X4, double4* slots,
                                cudaStream_t s);
 

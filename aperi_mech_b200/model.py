@@ -260,9 +260,9 @@ class ExplicitDynamics:
 
     # -- diagnostics -----------------------------------------------------------
     def layout(self) -> dict:
-        n, k, c = C.c_int64(), C.c_int32(), C.c_int64()
-        check(self.lib.am_get_layout(self.ctx, C.byref(n), C.byref(k), C.byref(c)), self.ctx)
-        return {"used_slots": n.value, "patched_tet4_blocks": k.value, "cell_entries": c.value}
+        n, k = C.c_int64(), C.c_int32()
+        check(self.lib.am_get_layout(self.ctx, C.byref(n), C.byref(k)), self.ctx)
+        return {"used_slots": n.value, "patched_tet4_blocks": k.value}
 
     def launch_count(self) -> int:
         return int(self.lib.am_launch_count(self.ctx))

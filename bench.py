@@ -265,22 +265,18 @@ def time_run(torch, model, prob, steps, warmup, prec, stream, dev, world, sample
 def algorithmic_bytes(prob, layout, slot_bytes=12):
     """Compulsory HBM bytes per launch of the element and node kernels; slot_bytes is
     three reals (12 B mixed, 24 B FP64). Element kernels: coordinates and displacement
-    read once per node (48 B), connectivity (4 B per element node), per-element moduli
-    (8 B per field), the node-major force slots written once (Gauss blocks), or for
-    cell blocks each entry's node id and gradient (4 B + three reals) read once and the
-    cell stress G (nine reals) written once. Node kernel: the slots read once, each cell
-    entry (gradient + cell id) and each cell stress read once, and per node mass 8 B,
-    BC word 4 B, slot range 4 B, displacement and half-step velocity read and written
-    (96 B)."""
+    read once per node (48 B), connectivity (4 B per element node) or, for cell blocks,
+    each entry's node id and gradient (4 B + three reals), per-element moduli (8 B
+    per field), and the node-major force slots written once. Node kernel: the slots
+    read once, and per node mass 8 B, BC word 4 B, slot range 4 B, displacement and
+    half-step velocity read and written (96 B)."""
     N = prob.num_nodes
     S = layout["used_slots"]
     elem = 48 * N + slot_bytes * S
     node = slot_bytes * S + (8 + 4 + 4 + 96) * N
     for p in prob.parts:
         if p.kind == "cells":
-            K, C = int(p.cell_ptr[-1]), p.num_elems
-            elem += (4 + slot_bytes) * K + 3 * slot_bytes * C
-            node += (4 + slot_bytes) * K + 3 * slot_bytes * C + 4 * N
+            elem += (4 + slot_bytes) * int(p.cell_ptr[-1])
         else:
             elem += 4 * p.conn.size
         elem += 8 * p.num_elems * ((p.mu_field is not None) + (p.kappa_field is not None))

@@ -210,10 +210,9 @@ int am_complete_properties(double props[5], char* msg, int msg_len);
 /* ---- diagnostics ---- */
 const char* am_last_error(const am_ctx* ctx);
 const char* am_status_string(int status);
-/* Force layout after am_finalize: node-major force slots referenced by nodes (Gauss
- * blocks), the number of Tet4 blocks assembled through element patches, and the
- * node-major entries through which cell blocks' stresses reach the nodes. */
-int am_get_layout(const am_ctx* ctx, int64_t* used_slots, int32_t* patched_tet4_blocks, int64_t* cell_entries);
+/* Force-slot layout after am_finalize: node-major slots referenced by nodes, and the
+ * number of Tet4 blocks assembled through element patches. */
+int am_get_layout(const am_ctx* ctx, int64_t* used_slots, int32_t* patched_tet4_blocks);
 /* Kernel launches issued by this context so far (all kinds). */
 int64_t am_launch_count(const am_ctx* ctx);
 /* Per-kernel device timing: when enabled, every launch of the hot loop is
