@@ -1,6 +1,8 @@
 // am_context.cu -- the C ABI (include/aperi_b200.h): context set-up, layout
 // building, the stream-ordered time loop and the checkpointed adjoint.
 #include <cuda_runtime.h>
+#include <dlfcn.h>
+#include <nccl.h>
 
 #include <algorithm>
 #include <cmath>
@@ -46,6 +48,42 @@ template <typename T>
 void dfree(T*& p) {
     if (p) cudaFree(p);
     p = nullptr;
+}
+
+// NCCL, opened at run time (libnccl.so.2: the copy a host framework already loaded, or
+// the system one), so the library carries no link-time dependency on it and a
+// process that never decomposes a mesh never loads it.
+struct NcclApi {
+    void* handle = nullptr;
+    ncclResult_t (*get_unique_id)(ncclUniqueId*) = nullptr;
+    ncclResult_t (*comm_init_rank)(ncclComm_t*, int, ncclUniqueId, int) = nullptr;
+    ncclResult_t (*all_reduce)(const void*, void*, size_t, ncclDataType_t, ncclRedOp_t, ncclComm_t, cudaStream_t) = nullptr;
+    ncclResult_t (*comm_destroy)(ncclComm_t) = nullptr;
+    const char* (*error_string)(ncclResult_t) = nullptr;
+};
+
+const NcclApi& nccl() {
+    static NcclApi api = [] {
+        NcclApi a;
+        a.handle = dlopen("libnccl.so.2", RTLD_NOW | RTLD_LOCAL);
+        if (!a.handle) return a;
+        a.get_unique_id = reinterpret_cast<decltype(a.get_unique_id)>(dlsym(a.handle, "ncclGetUniqueId"));
+        a.comm_init_rank = reinterpret_cast<decltype(a.comm_init_rank)>(dlsym(a.handle, "ncclCommInitRank"));
+        a.all_reduce = reinterpret_cast<decltype(a.all_reduce)>(dlsym(a.handle, "ncclAllReduce"));
+        a.comm_destroy = reinterpret_cast<decltype(a.comm_destroy)>(dlsym(a.handle, "ncclCommDestroy"));
+        a.error_string = reinterpret_cast<decltype(a.error_string)>(dlsym(a.handle, "ncclGetErrorString"));
+        return a;
+    }();
+    if (!api.handle || !api.get_unique_id || !api.comm_init_rank || !api.all_reduce || !api.comm_destroy)
+        fail(AM_ESTATE, "libnccl.so.2 could not be opened");
+    return api;
+}
+
+void nccl_check(ncclResult_t r, const char* what) {
+    if (r != ncclSuccess) {
+        const char* msg = nccl().error_string ? nccl().error_string(r) : "";
+        fail(AM_ECUDA, std::string(what) + ": " + msg);
+    }
 }
 
 struct Block {
@@ -228,8 +266,17 @@ struct am_ctx {
     std::string err;
     int64_t launches = 0;
     bool profiling = false;
-    double prof_ms[4] = {0, 0, 0, 0};
-    int64_t prof_launches[4] = {0, 0, 0, 0};
+    double prof_ms[5] = {0, 0, 0, 0, 0};
+    int64_t prof_launches[5] = {0, 0, 0, 0, 0};
+    bool mass_from_caller = false;
+    // Domain decomposition (am_set_interface / am_set_nccl).
+    int64_t iface_local = 0;          // this rank's interface nodes
+    int64_t iface_global = 0;         // rows of the exchange buffer (all ranks' interface nodes)
+    int32_t* iface_nodes = nullptr;   // local node ids
+    int32_t* iface_rows = nullptr;    // their rows
+    int32_t* iface_row_of = nullptr;  // per local node: row or -1
+    double* iface_buf = nullptr;      // iface_global x 3
+    ncclComm_t comm = nullptr;
     std::vector<cudaEvent_t> events;
     std::vector<std::pair<int, int64_t>> mark_slot;
     size_t n_marks = 0;
@@ -246,6 +293,10 @@ struct am_ctx {
         nd.g[2] = g[2];
         nd.has_g = (g[0] != 0.0 || g[1] != 0.0 || g[2] != 0.0) ? 1 : 0;
         nd.num_slots = num_used_slots;
+        if (iface_row_of) {
+            nd.iface_row = iface_row_of;
+            nd.iface_f = iface_buf;
+        }
         return nd;
     }
 
@@ -280,6 +331,21 @@ struct am_ctx {
             ++launches;
         }
         check_launch("element force kernel");
+    }
+
+    // Interface exchange between the element kernels and the node kernel: each rank's
+    // partial interface forces into their rows, the rows summed over ranks.
+    void exchange(int mixed) {
+        if (!iface_row_of) return;
+        ck(cudaMemsetAsync(iface_buf, 0, static_cast<size_t>(iface_global) * 3 * sizeof(double), stream), "memset");
+        am::NodeDev nd = node_dev();
+        am::launch_iface_gather(nd, mixed, slots(mixed), iface_local, iface_nodes, iface_rows, iface_buf, stream);
+        ++launches;
+        check_launch("interface gather kernel");
+        if (comm)
+            nccl_check(nccl().all_reduce(iface_buf, iface_buf, static_cast<size_t>(iface_global) * 3, ncclDouble, ncclSum,
+                                         comm, stream),
+                       "interface all-reduce");
     }
 
     void vjp(const double4* U, const double4* L, double* gmu, double* gkappa, int accumulate) {
@@ -388,7 +454,7 @@ struct am_ctx {
     // (optional) receives the displacement the element kernels use at step n0+k.
     void run_range(int mixed, int64_t n0, int64_t n1, double4* const* u_hist) {
         if (n1 <= n0) return;
-        if (profiling) reserve_marks(n_marks + static_cast<size_t>(2 * (n1 - n0) + 2));
+        if (profiling) reserve_marks(n_marks + static_cast<size_t>(3 * (n1 - n0) + 2));
         const am::NodeDev nd = node_dev();
         void* s = slots(mixed);
         mark(-1, 0);
@@ -399,6 +465,10 @@ struct am_ctx {
         for (int64_t n = n0; n < n1; ++n) {
             element_forces(mixed, U4);
             mark(0, static_cast<int64_t>(blocks.size()));
+            if (iface_row_of) {
+                exchange(mixed);
+                mark(4, 1);
+            }
             const int advance = (n + 1 < n1) ? 1 : 0;
             double4* uc = (u_hist && advance) ? u_hist[n + 1 - n0] : nullptr;
             am::launch_node_step(nd, mixed, s, table, n, advance, U4, V4, A4, uc, status, stream);
@@ -410,6 +480,7 @@ struct am_ctx {
 
     void init_acceleration(int mixed) {
         element_forces(mixed, U4);
+        exchange(mixed);
         am::launch_init_accel(node_dev(), mixed, slots(mixed), A4, status, stream);
         ++launches;
         check_launch("init acceleration kernel");
@@ -437,6 +508,12 @@ struct am_ctx {
         dfree(slot_pos);
         dfree(slots64);
         dfree(slots32);
+        dfree(iface_nodes);
+        dfree(iface_rows);
+        dfree(iface_row_of);
+        dfree(iface_buf);
+        if (comm) nccl().comm_destroy(comm);
+        comm = nullptr;
         for (auto& pbuf : adj_bufs) dfree(pbuf);
         adj_bufs.clear();
         dfree(table);
@@ -815,6 +892,7 @@ int am_set_mass(am_ctx* ctx, const double* mass) {
             if (!(mass[i] > 0.0)) fail(AM_EINVAL, "nodal masses must be positive");
         ck(cudaMemcpy(ctx->mass, mass, ctx->N * sizeof(double), cudaMemcpyHostToDevice), "mass upload");
         ctx->mass_set = true;
+        ctx->mass_from_caller = true;
     });
 }
 
@@ -909,6 +987,7 @@ int am_internal_force(am_ctx* ctx, am_precision prec, am_memory where, const dou
         load_nodal(ctx, where, u, ctx->W4);
         ctx->reset_status();
         ctx->element_forces(mixed, ctx->W4);
+        ctx->exchange(mixed);
         double* out = ctx->f_scratch;
         if (where == AM_DEVICE) out = f;
         else if (accumulate) ck(cudaMemcpyAsync(out, f, ctx->N * 3 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream), "H2D");
@@ -966,6 +1045,7 @@ int am_vjp_force(am_ctx* ctx, am_memory where, const double* u, const double* la
     if (!ctx) return AM_EINVAL;
     return guarded(ctx, [&] {
         ctx->require_finalized();
+        if (ctx->iface_row_of) fail(AM_ESTATE, "the VJP is not available on a decomposed mesh");
         if (!u || !lam || !gu) fail(AM_EINVAL, "null u, lam or gu");
         load_nodal(ctx, where, u, ctx->W4);
         load_nodal(ctx, where, lam, ctx->L4);
@@ -1001,6 +1081,7 @@ int am_adjoint(am_ctx* ctx, int64_t nsteps, double dt, int32_t ckpt_every, int32
     if (!ctx) return AM_EINVAL;
     return guarded(ctx, [&] {
         ctx->require_finalized();
+        if (ctx->iface_row_of) fail(AM_ESTATE, "the adjoint is not available on a decomposed mesh");
         if (nsteps <= 0 || !(dt > 0.0)) fail(AM_EINVAL, "nsteps and dt must be positive");
         if (ckpt_every <= 0) fail(AM_EINVAL, "ckpt_every must be positive");
         if (num_sensors < 0 || (num_sensors > 0 && !sensors)) fail(AM_EINVAL, "bad sensor list");
@@ -1206,6 +1287,64 @@ int am_get_layout(const am_ctx* ctx, int64_t* used_slots, int32_t* patched_tet4_
     return AM_OK;
 }
 
+int am_set_interface(am_ctx* ctx, int64_t num_local, const int32_t* local_nodes, const int32_t* rows,
+                     int64_t num_global) {
+    if (!ctx) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        ctx->require_finalized();
+        if (!ctx->mass_from_caller)
+            fail(AM_ESTATE, "a decomposed mesh needs the global lumped mass from am_set_mass before am_finalize");
+        if (ctx->iface_row_of) fail(AM_ESTATE, "interface already set");
+        if (num_local < 0 || num_global < num_local || (num_local > 0 && (!local_nodes || !rows)))
+            fail(AM_EINVAL, "bad interface arrays");
+        if (num_global >= (int64_t(1) << 31)) fail(AM_ERANGE, "interface beyond int32 indexing");
+        std::vector<int32_t> row_of(ctx->N, -1);
+        std::vector<char> row_used(static_cast<size_t>(num_global), 0);
+        for (int64_t k = 0; k < num_local; ++k) {
+            if (local_nodes[k] < 0 || local_nodes[k] >= ctx->N) fail(AM_EINVAL, "interface node out of range");
+            if (rows[k] < 0 || rows[k] >= num_global) fail(AM_EINVAL, "interface row out of range");
+            if (row_of[local_nodes[k]] >= 0 || row_used[rows[k]]) fail(AM_EINVAL, "interface node or row repeated");
+            row_of[local_nodes[k]] = rows[k];
+            row_used[rows[k]] = 1;
+        }
+        ctx->iface_local = num_local;
+        ctx->iface_global = num_global;
+        ctx->iface_row_of = dalloc<int32_t>(ctx->N, "interface rows");
+        ck(cudaMemcpy(ctx->iface_row_of, row_of.data(), ctx->N * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+        ctx->iface_buf = dalloc<double>(static_cast<size_t>(std::max<int64_t>(num_global, 1)) * 3, "interface buffer");
+        if (num_local > 0) {
+            ctx->iface_nodes = dalloc<int32_t>(num_local, "interface nodes");
+            ctx->iface_rows = dalloc<int32_t>(num_local, "interface rows");
+            ck(cudaMemcpy(ctx->iface_nodes, local_nodes, num_local * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+            ck(cudaMemcpy(ctx->iface_rows, rows, num_local * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+        }
+    });
+}
+
+int am_nccl_unique_id(unsigned char id[128]) {
+    am_ctx* none = nullptr;
+    const int rc = guarded(none, [&] {
+        if (!id) fail(AM_EINVAL, "null id");
+        static_assert(sizeof(ncclUniqueId) == 128, "ncclUniqueId is 128 bytes");
+        ncclUniqueId u;
+        nccl_check(nccl().get_unique_id(&u), "ncclGetUniqueId");
+        std::memcpy(id, &u, sizeof(u));
+    });
+    return rc;
+}
+
+int am_set_nccl(am_ctx* ctx, const unsigned char id[128], int32_t rank, int32_t nranks) {
+    if (!ctx) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        if (!id || nranks < 1 || rank < 0 || rank >= nranks) fail(AM_EINVAL, "bad NCCL rank or id");
+        if (!ctx->iface_row_of) fail(AM_ESTATE, "am_set_interface first");
+        if (ctx->comm) fail(AM_ESTATE, "communicator already set");
+        ncclUniqueId u;
+        std::memcpy(&u, id, sizeof(u));
+        nccl_check(nccl().comm_init_rank(&ctx->comm, nranks, u, rank), "ncclCommInitRank");
+    });
+}
+
 int am_profile_enable(am_ctx* ctx, int enable) {
     if (!ctx) return AM_EINVAL;
     const int rc = guarded(ctx, [&] { ctx->collect_marks(); });
@@ -1215,18 +1354,18 @@ int am_profile_enable(am_ctx* ctx, int enable) {
         const int rc2 = guarded(ctx, [&] { ctx->reserve_marks(4096); });
         if (rc2 != AM_OK) return rc2;
     }
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < 5; ++k) {
         ctx->prof_ms[k] = 0.0;
         ctx->prof_launches[k] = 0;
     }
     return AM_OK;
 }
 
-int am_profile_read(am_ctx* ctx, double ms[4], int64_t launches[4]) {
+int am_profile_read(am_ctx* ctx, double ms[5], int64_t launches[5]) {
     if (!ctx) return AM_EINVAL;
     const int rc = guarded(ctx, [&] { ctx->collect_marks(); });
     if (rc != AM_OK) return rc;
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < 5; ++k) {
         if (ms) ms[k] = ctx->prof_ms[k];
         if (launches) launches[k] = ctx->prof_launches[k];
     }

@@ -950,7 +950,15 @@ __device__ __forceinline__ void gather(const NodeDev& nd, const vec4_t<S>* __res
     // a fixed butterfly, so every lane holds the same total and the order is fixed.
     const int r = LPN == 1 ? 0 : static_cast<int>(threadIdx.x % LPN);
     fx = fy = fz = 0.0;
-    if (own) {
+    const int32_t row = (own && nd.iface_row != nullptr) ? nd.iface_row[i] : -1;
+    if (row >= 0) {
+        // Interface node: the summed force of all ranks (one lane contributes it).
+        if (r == 0) {
+            fx = nd.iface_f[3 * static_cast<int64_t>(row)];
+            fy = nd.iface_f[3 * static_cast<int64_t>(row) + 1];
+            fz = nd.iface_f[3 * static_cast<int64_t>(row) + 2];
+        }
+    } else if (own) {
         const int32_t p0 = nd.node_ptr[i], p1 = nd.node_ptr[i + 1];
         for (int32_t p = p0 + r; p < p1; p += BATCH * LPN) {
             vec4_t<S> v[BATCH];
@@ -1022,6 +1030,22 @@ __global__ void __launch_bounds__(kNodeBlock) k_gather_force(NodeDev nd, const v
         f[3 * i + 1] = fy;
         f[3 * i + 2] = fz;
     }
+}
+
+// One thread per local interface node: its own slots summed (no interface override).
+template <typename S>
+__global__ void __launch_bounds__(kNodeBlock) k_iface_gather(NodeDev nd, const vec4_t<S>* __restrict__ slots,
+                                                              int64_t num_local, const int32_t* __restrict__ local_nodes,
+                                                              const int32_t* __restrict__ rows, double* __restrict__ buf) {
+    const int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= num_local) return;
+    nd.iface_row = nullptr;
+    double fx, fy, fz;
+    gather<S, 4, 1>(nd, slots, local_nodes[k], true, fx, fy, fz);
+    const int64_t r = rows[k];
+    buf[3 * r] = fx;
+    buf[3 * r + 1] = fy;
+    buf[3 * r + 2] = fz;
 }
 
 template <typename S, int BATCH, int LPN>
@@ -1466,6 +1490,16 @@ inline bool gather_batch8(const NodeDev& nd, int mixed) {
 
 void launch_gather_force(const NodeDev& nd, int mixed, const void* slots, double* f, int accumulate, cudaStream_t s) {
     AM_NODE_DISPATCH(k_gather_force, f, accumulate);
+}
+
+void launch_iface_gather(const NodeDev& nd, int mixed, const void* slots, int64_t num_local,
+                         const int32_t* local_nodes, const int32_t* rows, double* buf, cudaStream_t s) {
+    if (num_local == 0) return;
+    const unsigned grid = grid_for(num_local, kNodeBlock);
+    if (mixed)
+        k_iface_gather<float><<<grid, kNodeBlock, 0, s>>>(nd, static_cast<const float4*>(slots), num_local, local_nodes, rows, buf);
+    else
+        k_iface_gather<double><<<grid, kNodeBlock, 0, s>>>(nd, static_cast<const double4*>(slots), num_local, local_nodes, rows, buf);
 }
 
 void launch_init_accel(const NodeDev& nd, int mixed, const void* slots, double4* A4, int* status, cudaStream_t s) {

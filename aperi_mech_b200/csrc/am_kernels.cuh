@@ -74,6 +74,10 @@ struct NodeDev {
     double g[3];                // body acceleration
     int32_t has_g;
     int64_t num_slots;          // node_ptr[num_nodes]: force slots in use
+    // Domain decomposition: interface nodes take their force from the exchanged
+    // buffer (row iface_row[i], FP64 x 3) instead of their own slots.
+    const int32_t* iface_row;   // per node: row in iface_f, or -1; null when not decomposed
+    const double* iface_f;
 };
 
 // ---- launchers (am_kernels.cu) ----
@@ -89,6 +93,10 @@ void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const dou
 
 // f (N x 3, row-major) = gather of the slots (FP64 or FP32 slots), overwrite or accumulate.
 void launch_gather_force(const NodeDev& nd, int mixed, const void* slots, double* f, int accumulate, cudaStream_t s);
+// Partial force of each local interface node (own slots only) into its row of the
+// exchange buffer (rows of nodes this rank does not hold are left as they are).
+void launch_iface_gather(const NodeDev& nd, int mixed, const void* slots, int64_t num_local,
+                         const int32_t* local_nodes, const int32_t* rows, double* buf, cudaStream_t s);
 // a = (f + g m) / m with no boundary condition (pre-loop acceleration).
 void launch_init_accel(const NodeDev& nd, int mixed, const void* slots, double4* A4, int* status, cudaStream_t s);
 // First half-step of a run: vh = v + h a ; BC(vh) ; u += dt vh.

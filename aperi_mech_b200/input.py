@@ -231,33 +231,6 @@ def _material(node: dict) -> Material:
         raise InputError(f"material {kind}: {e}") from None
 
 
-def _hex8_volumes(coords, conn) -> np.ndarray:
-    """sum over the 2x2x2 Gauss points of det J (ElementHexahedron8.h:107-117)."""
-    s = np.array([[-1, -1, -1], [1, -1, -1], [1, 1, -1], [-1, 1, -1],
-                  [-1, -1, 1], [1, -1, 1], [1, 1, 1], [-1, 1, 1]], dtype=float)
-    x = coords[conn]  # E x 8 x 3
-    vol = np.zeros(conn.shape[0])
-    for g in s / math.sqrt(3.0):
-        dN = np.stack([s[:, 0] * (1 + s[:, 1] * g[1]) * (1 + s[:, 2] * g[2]),
-                       s[:, 1] * (1 + s[:, 0] * g[0]) * (1 + s[:, 2] * g[2]),
-                       s[:, 2] * (1 + s[:, 0] * g[0]) * (1 + s[:, 1] * g[1])], axis=1) / 8.0
-        vol += np.linalg.det(np.einsum("eai,aj->eij", x, dN))
-    return vol
-
-
-def _lumped_mass(coords, conn, density) -> np.ndarray:
-    """rho V / n_en per element node (src/MassUtils.cpp:17-46), for Gauss parts that share a
-    model with cell parts (whose mass comes from their own set-up)."""
-    m = np.zeros(coords.shape[0])
-    x = coords[conn]
-    if conn.shape[1] == 4:
-        vol = np.abs(np.einsum("ij,ij->i", x[:, 1] - x[:, 0], np.cross(x[:, 2] - x[:, 0], x[:, 3] - x[:, 0]))) / 6.0
-    else:
-        vol = _hex8_volumes(coords, conn)
-    np.add.at(m, conn.ravel(), np.repeat(density * vol / conn.shape[1], conn.shape[1]))
-    return m
-
-
 def _part(pnode: dict, blocks: dict, coords, ext: dict, rng):
     """One InternalForceContribution: block connectivity + formulation + material."""
     name = pnode.get("set")
@@ -373,7 +346,7 @@ def load(source, base_dir: Path | None = None) -> Simulation:
     if any(m is not None for m in masses):
         mass = np.zeros(coords.shape[0])
         for part, m in zip(parts, masses):
-            mass += m if m is not None else _lumped_mass(coords, part.conn, part.material.density)
+            mass += m if m is not None else _mesh.lumped_mass(coords, part.conn, part.material.density)
 
     v0 = np.zeros_like(coords)
     for entry in proc.get("initial_conditions") or []:

@@ -10,6 +10,8 @@ gives the gather kernels spatial locality on these boxes.
 """
 from __future__ import annotations
 
+import math
+
 import numpy as np
 
 # Six tets around the 0->6 diagonal of a Hex8; every face diagonal passes
@@ -88,3 +90,31 @@ def check_orientation(coords: np.ndarray, conn: np.ndarray) -> None:
         v = tet_volumes(coords, conn)
         if np.any(v <= 0):
             raise ValueError(f"{int((v <= 0).sum())} tets with non-positive volume")
+
+
+def hex8_volumes(coords: np.ndarray, conn: np.ndarray) -> np.ndarray:
+    """sum over the 2x2x2 Gauss points of det J (ElementHexahedron8.h:107-117)."""
+    s = np.array([[-1, -1, -1], [1, -1, -1], [1, 1, -1], [-1, 1, -1],
+                  [-1, -1, 1], [1, -1, 1], [1, 1, 1], [-1, 1, 1]], dtype=float)
+    x = coords[conn]  # E x 8 x 3
+    vol = np.zeros(conn.shape[0])
+    for g in s / math.sqrt(3.0):
+        dN = np.stack([s[:, 0] * (1 + s[:, 1] * g[1]) * (1 + s[:, 2] * g[2]),
+                       s[:, 1] * (1 + s[:, 0] * g[0]) * (1 + s[:, 2] * g[2]),
+                       s[:, 2] * (1 + s[:, 0] * g[0]) * (1 + s[:, 1] * g[1])], axis=1) / 8.0
+        vol += np.linalg.det(np.einsum("eai,aj->eij", x, dN))
+    return vol
+
+
+def lumped_mass(coords: np.ndarray, conn: np.ndarray, density: float) -> np.ndarray:
+    """Lumped nodal mass rho V_e / n_en summed over the elements (src/MassUtils.cpp:17-46),
+    on the host: for Gauss parts that share a model with cell parts (whose mass comes
+    from their own set-up) and for the global mass of a decomposed mesh."""
+    m = np.zeros(coords.shape[0])
+    x = coords[conn]
+    if conn.shape[1] == 4:
+        vol = np.abs(np.einsum("ij,ij->i", x[:, 1] - x[:, 0], np.cross(x[:, 2] - x[:, 0], x[:, 3] - x[:, 0]))) / 6.0
+    else:
+        vol = hex8_volumes(coords, conn)
+    np.add.at(m, conn.ravel(), np.repeat(density * vol / conn.shape[1], conn.shape[1]))
+    return m

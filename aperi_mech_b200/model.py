@@ -27,6 +27,13 @@ PRECISIONS = {"fp64": capi.AM_FP64, "mixed": capi.AM_MIXED}
 _PROPS = ("youngs_modulus", "poissons_ratio", "shear_modulus", "lambda", "bulk_modulus")
 
 
+def nccl_unique_id() -> bytes:
+    """ncclGetUniqueId through the library (rank 0 makes it and sends it to the others)."""
+    buf = C.create_string_buffer(128)
+    check(capi.load().am_nccl_unique_id(buf))
+    return buf.raw
+
+
 def complete_properties(**props) -> dict:
     """LinearElasticProperties::CompleteProperties (Materials/Base.h:47-158), run by the
     library's C++ host code: exactly two of youngs_modulus, poissons_ratio, shear_modulus,
@@ -258,6 +265,18 @@ class ExplicitDynamics:
                                   C.byref(loss), capi._ptr(gm), capi._ptr(gk)), self.ctx)
         return loss.value, gm, gk
 
+    # -- domain decomposition -------------------------------------------------
+    def set_interface(self, local_nodes: np.ndarray, rows: np.ndarray, num_global: int) -> None:
+        """This rank's interface nodes and their rows of the exchange buffer
+        (partition.Subdomain.iface_local / iface_ids / num_iface)."""
+        ln = np.ascontiguousarray(local_nodes, dtype=np.int32)
+        rw = np.ascontiguousarray(rows, dtype=np.int32)
+        check(self.lib.am_set_interface(self.ctx, ln.size, capi._ptr(ln, C.c_int32), capi._ptr(rw, C.c_int32),
+                                        int(num_global)), self.ctx)
+
+    def set_nccl(self, unique_id: bytes, rank: int, nranks: int) -> None:
+        check(self.lib.am_set_nccl(self.ctx, unique_id, int(rank), int(nranks)), self.ctx)
+
     # -- diagnostics -----------------------------------------------------------
     def layout(self) -> dict:
         n, k = C.c_int64(), C.c_int32()
@@ -271,8 +290,8 @@ class ExplicitDynamics:
         check(self.lib.am_profile_enable(self.ctx, int(enable)), self.ctx)
 
     def profile_read(self):
-        ms = (C.c_double * 4)()
-        n = (C.c_int64 * 4)()
+        ms = (C.c_double * 5)()
+        n = (C.c_int64 * 5)()
         check(self.lib.am_profile_read(self.ctx, ms, n), self.ctx)
         return list(ms), list(n)
 

@@ -219,10 +219,28 @@ int64_t am_launch_count(const am_ctx* ctx);
  * bracketed by CUDA events on the context stream (recorded asynchronously; the
  * elapsed times are collected, with one synchronization, by am_profile_read).
  * Slot 0: element/cell force kernels, 1: node gather + update kernels, 2: VJP
- * kernels, 3: adjoint node kernels. Milliseconds and launch counts accumulate
- * until am_profile_enable is called again. */
+ * kernels, 3: adjoint node kernels, 4: interface exchange (decomposed meshes).
+ * Milliseconds and launch counts accumulate until am_profile_enable is called again. */
 int am_profile_enable(am_ctx* ctx, int enable);
-int am_profile_read(am_ctx* ctx, double ms[4], int64_t launches[4]);
+int am_profile_read(am_ctx* ctx, double ms[5], int64_t launches[5]);
+
+/* ---- domain decomposition (replaces the reference's ParallelSum of the force field
+ * after the element loop, src/Solvers/Explicit.cpp:190-193) ----
+ * A context holds one rank's slab of elements and every node they touch; nodes held by
+ * several ranks are interface nodes. local_nodes[k] (this context's node ids) owns row
+ * rows[k] of an exchange buffer of num_global rows (FP64 x 3, the interface nodes of the
+ * whole mesh). Each step the element kernels run, every interface node's partial force
+ * goes to its row, the rows are summed over the ranks (NCCL all-reduce on the context
+ * stream when a communicator is set; a single rank without one sums nothing), and the
+ * node kernel takes the summed force for interface nodes. Needs the global lumped mass
+ * (am_set_mass before am_finalize); call after am_finalize. The VJP and the adjoint are
+ * not available on a decomposed mesh (AM_ESTATE). */
+int am_set_interface(am_ctx* ctx, int64_t num_local, const int32_t* local_nodes, const int32_t* rows,
+                     int64_t num_global);
+/* ncclGetUniqueId (libnccl.so.2 is opened at run time): rank 0 makes the id, the host
+ * sends it to the other ranks, every rank passes it to am_set_nccl. */
+int am_nccl_unique_id(unsigned char id[128]);
+int am_set_nccl(am_ctx* ctx, const unsigned char id[128], int32_t rank, int32_t nranks);
 
 #ifdef __cplusplus
 }

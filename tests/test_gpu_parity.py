@@ -429,3 +429,39 @@ def test_tet4_patch_layouts(gpu, oracle_lib, monkeypatch, layout):
         assert rel_err(m.mass(), op.lumped_mass()) < 1e-14
         for g, w in zip(m.vjp_force(u, lam), op.vjp_force(u, lam)):
             assert rel_err(g, w) < 1e-11
+
+
+# ---- domain decomposition on one GPU --------------------------------------------------
+@pytest.mark.parametrize("use_nccl", [False, True])
+def test_interface_exchange_single_rank_is_exact(gpu, use_nccl):
+    """With one rank, the decomposed step (interface gather into the exchange buffer,
+    the all-reduce, the node kernel reading interface rows back) must reproduce the
+    plain step bit for bit; rows are a random injection into a larger buffer."""
+    import os
+
+    from aperi_mech_b200 import mesh, problems
+    from aperi_mech_b200.model import ExplicitDynamics, nccl_unique_id
+
+    p = problems.tet4_nh_shear(n=8, seed=3, nsteps=25)
+    mass = mesh.lumped_mass(p.coords, p.parts[0].conn, p.parts[0].material.density)
+    rng = np.random.default_rng(0)
+    iface = np.sort(rng.choice(p.num_nodes, size=p.num_nodes // 3, replace=False)).astype(np.int32)
+    rows = rng.permutation(2 * iface.size)[: iface.size].astype(np.int32)
+    out = {}
+    for decomposed in (False, True):
+        with ExplicitDynamics(p.coords, p.parts, p.bcs, mass=mass) as m:
+            if decomposed:
+                m.set_interface(iface, rows, 2 * iface.size)
+                if use_nccl:
+                    os.environ.setdefault("NCCL_SOCKET_IFNAME", "lo")
+                    m.set_nccl(nccl_unique_id(), 0, 1)
+            for prec in ("fp64", "mixed"):
+                m.set_state(None, p.v0)
+                m.init_acceleration(prec)
+                m.run(p.nsteps, p.dt, prec)
+                out[(decomposed, prec)] = m.get_state()
+            out[(decomposed, "f")] = m.internal_force(out[(decomposed, "fp64")][0])
+    for key in ("fp64", "mixed"):
+        for a, b in zip(out[(False, key)], out[(True, key)]):
+            assert np.array_equal(a, b), key
+    assert np.array_equal(out[(False, "f")], out[(True, "f")])

@@ -1,0 +1,130 @@
+"""Domain decomposition: the partition bookkeeping, and a world-size-2 run on CPU (gloo)
+whose per-rank forces come from the oracle and whose interface forces are summed with
+torch.distributed, against the single-domain oracle."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+from aperi_mech_b200 import partition, problems
+
+
+def _problem(kind):
+    if kind == "tet4":
+        return problems.tet4_nh_shear(n=5, seed=1, nsteps=12)
+    if kind == "hex8":
+        return problems.hex8_nh_lognormal(n=5, seed=1, nsteps=12, bulk_field=True)
+    return problems.smoothed_tet4_box(n=4, seed=1, nsteps=12)
+
+
+@pytest.mark.parametrize("kind", ["tet4", "hex8", "cells"])
+@pytest.mark.parametrize("world", [2, 3])
+def test_decompose_bookkeeping(kind, world):
+    p = _problem(kind)
+    subs = partition.decompose(p.coords, p.parts, p.bcs, p.v0, world, mass=p.meta.get("mass"))
+    N = p.num_nodes
+    # every element (cell) in exactly one rank
+    for k, part in enumerate(p.parts):
+        got = np.sort(np.concatenate([s.elements[k] for s in subs]))
+        assert np.array_equal(got, np.arange(part.num_elems))
+    # owners partition the nodes; interface = nodes held by two or more ranks
+    held = np.zeros(N, dtype=int)
+    owned = np.zeros(N, dtype=int)
+    for s in subs:
+        held[s.global_nodes] += 1
+        owned[s.global_nodes[s.owned]] += 1
+        assert np.array_equal(s.coords, p.coords[s.global_nodes])
+        assert np.array_equal(np.sort(s.global_nodes[s.iface_local]), s.global_nodes[s.iface_local])
+    assert (held >= 1).all() and (owned == 1).all()
+    iface = np.nonzero(held > 1)[0]
+    assert subs[0].num_iface == iface.size > 0
+    for s in subs:
+        assert np.array_equal(iface[s.iface_ids], s.global_nodes[s.iface_local])
+        assert np.array_equal(s.iface_local, np.nonzero(held[s.global_nodes] > 1)[0])
+    # global mass sliced; boundary conditions restricted to held nodes
+    mass = p.meta.get("mass")
+    for s in subs:
+        if mass is not None:
+            assert np.array_equal(s.mass, mass[s.global_nodes])
+        for bc, gbc in zip(s.bcs, p.bcs):
+            assert set(s.global_nodes[bc.nodes]) == set(gbc.nodes) & set(s.global_nodes)
+
+
+def _free_port():
+    with socket.socket() as sock:
+        sock.bind(("127.0.0.1", 0))
+        return sock.getsockname()[1]
+
+
+def _rank_main(rank, world, port, kind, out_dir):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from oracle import oracle
+
+        p = _problem(kind)
+        s = partition.decompose(p.coords, p.parts, p.bcs, p.v0, world, mass=p.meta.get("mass"))[rank]
+        op = oracle.OracleProblem(s.coords, s.parts, s.bcs, mass=s.mass)
+        fixed = np.zeros(s.num_nodes, dtype=bool)
+        for bc in s.bcs:
+            fixed[bc.nodes] = True
+        m = s.mass[:, None]
+
+        def force(u):
+            f = op.internal_force(u)
+            buf = torch.zeros((s.num_iface, 3), dtype=torch.float64)
+            buf[torch.from_numpy(s.iface_ids.astype(np.int64))] = torch.from_numpy(f[s.iface_local])
+            dist.all_reduce(buf)
+            f[s.iface_local] = buf[torch.from_numpy(s.iface_ids.astype(np.int64))].numpy()
+            return f
+
+        # ExplicitSolver::Solve order with homogeneous displacement BCs.
+        u = np.zeros_like(s.coords)
+        v = s.v0.copy()
+        a = force(u) / m
+        h = 0.5 * p.dt
+        for _ in range(p.nsteps):
+            v = v + h * a
+            v[fixed] = 0.0
+            u = u + p.dt * v
+            a = force(u) / m
+            a[fixed] = 0.0
+            v = v + h * a
+        np.savez(os.path.join(out_dir, f"rank{rank}.npz"), u=u, v=v, nodes=s.global_nodes, owned=s.owned)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("kind", ["tet4", "hex8", "cells"])
+def test_two_rank_gloo_run_matches_single_domain(oracle_lib, tmp_path, kind):
+    world = 2
+    mp.start_processes(_rank_main, args=(world, _free_port(), kind, str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    p = _problem(kind)
+    op = oracle_lib.OracleProblem(p.coords, p.parts, p.bcs, mass=p.meta.get("mass"))
+    u0 = np.zeros_like(p.coords)
+    u_ref, v_ref, _ = op.steps(u0, p.v0, op.init_acceleration(u0), np.full(p.nsteps, p.dt))
+    u = np.zeros_like(p.coords)
+    v = np.zeros_like(p.coords)
+    seen = np.zeros(p.num_nodes, dtype=int)
+    for r in range(world):
+        d = np.load(tmp_path / f"rank{r}.npz")
+        nodes, owned = d["nodes"], d["owned"]
+        # interface copies agree bitwise across ranks
+        if r > 0:
+            common = np.intersect1d(nodes, prev_nodes)
+            a_idx = np.searchsorted(nodes, common)
+            b_idx = np.searchsorted(prev_nodes, common)
+            assert np.array_equal(d["u"][a_idx], prev_u[b_idx])
+        prev_nodes, prev_u = nodes, d["u"]
+        u[nodes[owned]] = d["u"][owned]
+        v[nodes[owned]] = d["v"][owned]
+        seen[nodes[owned]] += 1
+    assert (seen == 1).all()
+    assert np.linalg.norm(u - u_ref) <= 1e-12 * np.linalg.norm(u_ref)
+    assert np.linalg.norm(v - v_ref) <= 1e-12 * np.linalg.norm(v_ref)
