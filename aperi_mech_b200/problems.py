@@ -145,3 +145,54 @@ def rkpm_box(n: int = 46, seed: int = 0, nsteps: int = 500, jitter: float = 0.2,
     return Problem(f"rkpm_box_{n}", coords, [cells.part], [BoundaryCondition.fixed(fixed)], v0, dt, nsteps, seed,
                    {"mass": cells.mass, "tets": tets, "entries_per_cell": cells.entries_per_cell,
                     "config": f"RKPM one-pass nodal cells, R={radius}h, cap {max_neighbors}, neo-Hookean"})
+
+
+def tet4_nh_shear_slab(n: int = 70, rank: int = 0, world: int = 1, seed: int = 0, nsteps: int = 1000,
+                       jitter: float = 0.2) -> Problem:
+    """One rank's slab of the weak-scaled tet4_nh_shear mesh: world slabs of n^3 hexes
+    (6 tets each) stacked along z on a box 1 x 1 x world (h = 1/n), built locally
+    without the global mesh. Interior jitter and the initial-velocity noise are drawn
+    per z-plane of nodes from seed and the plane index, so the two slabs sharing an
+    interface plane generate identical nodes. meta holds the interface (local ids and
+    rows of the exchange buffer, one plane of (n+1)^2 rows per slab boundary) and the
+    slab's own lumped mass (interface rows still to be summed over the neighbours)."""
+    h = 1.0 / n
+    m1 = n + 1
+    coords, conn_hex = mesh.box_hex(n, n, n, 1.0, 1.0, 1.0)
+    z0 = n * rank
+    coords[:, 2] += rank  # global z
+    kz = np.rint(coords[:, 2] * n).astype(np.int64)
+    noise = np.empty_like(coords)
+    for p in range(m1):
+        sel = slice(p * m1 * m1, (p + 1) * m1 * m1)
+        rng = np.random.default_rng([seed, z0 + p])
+        jit = rng.uniform(-jitter * h, jitter * h, size=(m1 * m1, 3))
+        noise[sel] = rng.uniform(-0.01, 0.01, size=(m1 * m1, 3))
+        xy = coords[sel, :2]
+        interior = ((xy > 1e-12) & (xy < 1.0 - 1e-12)).all(axis=1) & (z0 + p > 0) & (z0 + p < n * world)
+        block = coords[sel]
+        block[interior] += jit[interior]
+        coords[sel] = block
+    conn = mesh.hex_to_tets(conn_hex)
+    mesh.check_orientation(coords, conn)
+    mat = Material.create("neo_hookean", 1000.0, shear_modulus=3.85e8, bulk_modulus=8.33e8)
+    fixed = np.nonzero(kz == 0)[0].astype(np.int32)
+    v0 = noise.copy()
+    v0[:, 0] += coords[:, 2]
+    v0[fixed] = 0.0
+    c = wave_speed(mat.lam, mat.mu, mat.density)
+    dt = 0.5 * float(mesh.tet_char_length(coords, conn).min()) / c
+    local, rows = [], []
+    if rank > 0:
+        local.append(np.arange(m1 * m1))
+        rows.append((rank - 1) * m1 * m1 + np.arange(m1 * m1))
+    if rank < world - 1:
+        local.append(n * m1 * m1 + np.arange(m1 * m1))
+        rows.append(rank * m1 * m1 + np.arange(m1 * m1))
+    iface_local = np.concatenate(local).astype(np.int32) if local else np.zeros(0, np.int32)
+    iface_rows = np.concatenate(rows).astype(np.int32) if rows else np.zeros(0, np.int32)
+    meta = {"config": f"Tet4 1-pt Gauss, neo-Hookean, slab {rank} of {world}", "iface_local": iface_local,
+            "iface_rows": iface_rows, "num_iface": (world - 1) * m1 * m1,
+            "slab_mass": mesh.lumped_mass(coords, conn, mat.density)}
+    return Problem(f"tet4_nh_shear_{n}_slab{rank}of{world}", coords, [Part("tet4", mat, conn=conn)],
+                   [BoundaryCondition.fixed(fixed)], v0, dt, nsteps, seed, meta)

@@ -5,7 +5,13 @@ neo-Hookean Tet4 shear workload, 70^3 hexes split into 2,058,000 tets (357,911
 nodes), interior jitter +-0.2h, 1000 steps at dt = 0.5 x the stable step.
 Synthetic seeded inputs (numpy PCG64, seed 0).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--decompose]
+
+With N > 1 (under torchrun) every rank runs its own copy of the workload (replicas,
+weak scaling, no collective on the data path) unless --decompose is given: then the
+mesh is one 70^3-hex z-slab per rank stacked into a 1 x 1 x N box, and every step the
+interface nodes' partial forces are summed across ranks with NCCL before the nodal
+update (weak scaling with the exchange the reference does with MPI).
 
 Prints one JSON line. `value` is the mixed FP32-element / FP64-state path in
 Melem-steps/s (elements x steps / device seconds), with the plain FP64 path, the
@@ -51,6 +57,9 @@ def parse():
                     help="workload of the headline timing (the default is the headline configuration; the others "
                          "exist to profile one kernel at a time)")
     ap.add_argument("--skip-extras", action="store_true")
+    ap.add_argument("--decompose", action="store_true",
+                    help="N > 1: one z-slab of the Tet4 shear mesh per rank (weak scaling) with the interface "
+                         "forces summed over NCCL every step, instead of N independent replicas")
     ap.add_argument("--skip-adjoint", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
@@ -385,9 +394,44 @@ def run_adjoint(torch, pa, ckpt, stream, dev):
             "kernel_launches": {"element": pn[0], "node": pn[1], "vjp": pn[2], "adjoint_node": pn[3]}}
 
 
-def make_problem(args):
+def decomposed_setup(args, prob, rank, world, dev):
+    """Global mass and stable step of the slab decomposition (interface rows of the slab
+    masses summed, dt the minimum over ranks), then the exchange and its communicator."""
+    import torch
+
+    mass = prob.meta["slab_mass"].copy()
+    rows = torch.from_numpy(prob.meta["iface_rows"].astype(np.int64)).to(dev)
+    loc = prob.meta["iface_local"]
+    if world > 1:
+        import torch.distributed as dist
+
+        buf = torch.zeros(prob.meta["num_iface"], dtype=torch.float64, device=dev)
+        buf[rows] = torch.from_numpy(mass[loc]).to(dev)
+        dist.all_reduce(buf)
+        mass[loc] = buf[rows].cpu().numpy()
+        dt = torch.tensor([prob.dt], dtype=torch.float64, device=dev)
+        dist.all_reduce(dt, op=dist.ReduceOp.MIN)
+        prob.dt = float(dt.item())
+    return mass
+
+
+def attach_interface(model, prob, rank, world):
+    from aperi_mech_b200.model import nccl_unique_id
+
+    model.set_interface(prob.meta["iface_local"], prob.meta["iface_rows"], prob.meta["num_iface"])
+    if world > 1:
+        import torch.distributed as dist
+
+        box = [nccl_unique_id() if rank == 0 else None]
+        dist.broadcast_object_list(box, src=0)
+        model.set_nccl(box[0], rank, world)
+
+
+def make_problem(args, rank=0, world=1):
     from aperi_mech_b200 import problems
 
+    if args.decompose:
+        return problems.tet4_nh_shear_slab(n=args.n, rank=rank, world=world, seed=0, nsteps=args.steps)
     w = args.workload
     if w == "tet4_nh_shear":
         return problems.tet4_nh_shear(n=args.n, seed=0, nsteps=args.steps)
@@ -407,12 +451,14 @@ def run_ours(args, rank, world, local):
     from aperi_mech_b200.model import ExplicitDynamics
 
     dev = torch.device("cuda", local)
-    prob = make_problem(args)
+    prob = make_problem(args, rank, world)
     E, N = prob.num_elems, prob.num_nodes
     stream = torch.cuda.Stream(device=dev)
     res = {}
-    model = ExplicitDynamics(prob.coords, prob.parts, prob.bcs, mass=prob.meta.get("mass"),
-                             stream=stream.cuda_stream)
+    mass = decomposed_setup(args, prob, rank, world, dev) if args.decompose else prob.meta.get("mass")
+    model = ExplicitDynamics(prob.coords, prob.parts, prob.bcs, mass=mass, stream=stream.cuda_stream)
+    if args.decompose:
+        attach_interface(model, prob, rank, world)
     layout = model.layout()
     hbm_peak, peak_kind = measured_peaks()
     for prec in ("fp64", "mixed"):
@@ -459,6 +505,8 @@ def run_ours(args, rank, world, local):
 
     # the other configurations, each on its own context
     extras = {}
+    if args.decompose:
+        args.skip_extras = args.skip_adjoint = True  # the adjoint is single-domain
     if not args.skip_extras:
         p1 = problems.hex8_le_cube(n=20, seed=0, nsteps=100)
         extras["hex8_le_cube_20"] = measure_workload(torch, p1, 100, args.warmup, stream, dev, world)
@@ -560,7 +608,9 @@ def main():
                    if "nh" in prob.name or "box" in prob.name else "linear elastic E=1e9 nu=0.3",
                    "dt": prob.dt, "seed": prob.seed,
                    "l2_flush": "inputs larger than L2 (state + slots + connectivity ~ 230 MB per step)",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                   "parallelism": (f"z-slab domain decomposition x{world}, interface forces summed over NCCL "
+                                   f"({prob.meta['num_iface']} interface nodes)" if args.decompose else
+                                   f"replicas x{world}" if world > 1 else "single GPU")},
         "fp64": {"value": res["fp64"]["value"], "ms_per_step": res["fp64"]["ms"] / args.steps},
         "mixed_vs_fp64": {"rel_disp_err_l2": disp_err, "rel_force_err_l2": force_err,
                           "speedup": res["mixed"]["value"] / res["fp64"]["value"]},

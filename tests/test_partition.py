@@ -128,3 +128,80 @@ def test_two_rank_gloo_run_matches_single_domain(oracle_lib, tmp_path, kind):
     assert (seen == 1).all()
     assert np.linalg.norm(u - u_ref) <= 1e-12 * np.linalg.norm(u_ref)
     assert np.linalg.norm(v - v_ref) <= 1e-12 * np.linalg.norm(v_ref)
+
+
+def _slab_global_ids(prob, n, rank):
+    m1 = n + 1
+    k = np.arange(prob.num_nodes)
+    return (k % (m1 * m1)) + m1 * m1 * (k // (m1 * m1) + n * rank)
+
+
+def _slab_rank_main(rank, world, port, n, nsteps, out_dir):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from oracle import oracle
+
+        p = problems.tet4_nh_shear_slab(n=n, rank=rank, world=world, seed=2, nsteps=nsteps)
+        rows = torch.from_numpy(p.meta["iface_rows"].astype(np.int64))
+        loc = p.meta["iface_local"]
+
+        def exchange(x):  # sum the interface rows of a nodal array over the ranks
+            buf = torch.zeros((p.meta["num_iface"],) + x.shape[1:], dtype=torch.float64)
+            buf[rows] = torch.from_numpy(x[loc])
+            dist.all_reduce(buf)
+            x[loc] = buf[rows].numpy()
+            return x
+
+        mass = exchange(p.meta["slab_mass"].copy())
+        dt = torch.tensor([p.dt], dtype=torch.float64)
+        dist.all_reduce(dt, op=dist.ReduceOp.MIN)
+        dt = float(dt)
+        op = oracle.OracleProblem(p.coords, p.parts, p.bcs, mass=mass)
+        fixed = p.bcs[0].nodes
+        u = np.zeros_like(p.coords)
+        v = p.v0.copy()
+        a = exchange(op.internal_force(u)) / mass[:, None]
+        for _ in range(nsteps):
+            v = v + 0.5 * dt * a
+            v[fixed] = 0.0
+            u = u + dt * v
+            a = exchange(op.internal_force(u)) / mass[:, None]
+            a[fixed] = 0.0
+            v = v + 0.5 * dt * a
+        np.savez(os.path.join(out_dir, f"slab{rank}.npz"), u=u, dt=dt)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_weak_scaled_slabs_match_the_stacked_mesh(oracle_lib, tmp_path):
+    """The per-rank slabs the multi-GPU benchmark builds (no global mesh on any rank),
+    run on two gloo ranks with interface force and mass exchange, against the oracle on
+    the stacked mesh assembled from the slabs."""
+    from aperi_mech_b200.model import BoundaryCondition, Part
+
+    n, world, nsteps = 4, 2, 10
+    mp.start_processes(_slab_rank_main, args=(world, _free_port(), n, nsteps, str(tmp_path)), nprocs=world,
+                       join=True, start_method="spawn")
+    slabs = [problems.tet4_nh_shear_slab(n=n, rank=r, world=world, seed=2, nsteps=nsteps) for r in range(world)]
+    m1 = n + 1
+    G = m1 * m1 * (n * world + 1)
+    coords, v0 = np.zeros((G, 3)), np.zeros((G, 3))
+    conns, fixed = [], []
+    for r, s in enumerate(slabs):
+        gid = _slab_global_ids(s, n, r)
+        coords[gid], v0[gid] = s.coords, s.v0
+        conns.append(gid[s.parts[0].conn])
+        fixed.append(gid[s.bcs[0].nodes])
+    parts = [Part("tet4", slabs[0].parts[0].material, conn=np.concatenate(conns).astype(np.int32))]
+    bcs = [BoundaryCondition.fixed(np.concatenate(fixed).astype(np.int32))]
+    dt = min(s.dt for s in slabs)
+    op = oracle_lib.OracleProblem(coords, parts, bcs)
+    u0 = np.zeros_like(coords)
+    u_ref, _, _ = op.steps(u0, v0, op.init_acceleration(u0), np.full(nsteps, dt))
+    for r, s in enumerate(slabs):
+        d = np.load(tmp_path / f"slab{r}.npz")
+        assert float(d["dt"]) == dt
+        ref = u_ref[_slab_global_ids(s, n, r)]
+        assert np.linalg.norm(d["u"] - ref) <= 1e-12 * np.linalg.norm(ref)
