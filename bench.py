@@ -71,7 +71,8 @@ def parse():
 
 
 # ---------------------------------------------------------------------------
-# distributed plumbing (one process per GPU; timing only, no data-path collective)
+# distributed plumbing (one process per GPU): timing, set-up reductions, and the
+# NCCL id for --decompose (whose per-step exchange runs inside the library)
 # ---------------------------------------------------------------------------
 def dist_init(n_gpus):
     import torch
@@ -240,13 +241,17 @@ def _events(torch):
 
 def time_run(torch, model, prob, steps, warmup, prec, stream, dev, world, sampler_index=None):
     """Warm-up, then `steps` timed central-difference steps (device events on the
-    library's stream); per-kernel events are recorded inside the timed region."""
-    model.set_state(None, prob.v0)
-    model.init_acceleration(prec)
-    model.run(warmup, prob.dt, prec)
-    torch.cuda.synchronize(dev)
-    barrier(world)
-    model.profile(True)
+    library's stream, max over ranks): the number reported. A second, untimed-for-the-
+    headline run of the same steps records CUDA events between the kernels for the
+    per-kernel breakdown (those events add small gaps, so they stay out of the first)."""
+    def start():
+        model.set_state(None, prob.v0)
+        model.init_acceleration(prec)
+        model.run(warmup, prob.dt, prec)
+        torch.cuda.synchronize(dev)
+        barrier(world)
+
+    start()
     n0 = model.launch_count()
     ev0, ev1 = _events(torch)
     sampler = ClockSampler(sampler_index) if sampler_index is not None else None
@@ -262,11 +267,17 @@ def time_run(torch, model, prob, steps, warmup, prec, stream, dev, world, sample
         if sampler:
             sampler.__exit__(None, None, None)
     ms = max_over_ranks(ev0.elapsed_time(ev1), world)
+    launches = model.launch_count() - n0
+    state = model.get_state()
+    start()
+    model.profile(True)
+    model.run(steps, prob.dt, prec, t0=warmup * prob.dt)
     kms, kn = model.profile_read()
     model.profile(False)
-    return {"ms": ms, "value": world * prob.num_elems * steps / (ms * 1e-3) / 1e6,
-            "launches": model.launch_count() - n0,
+    return {"ms": ms, "value": world * prob.num_elems * steps / (ms * 1e-3) / 1e6, "launches": launches,
+            "state": state,
             "kernels": {"element_ms": kms[0] / max(kn[0], 1), "node_ms": kms[1] / max(kn[1], 1),
+                        "exchange_ms": kms[4] / max(kn[4], 1) if kn[4] else None,
                         "element_total_ms": kms[0], "node_total_ms": kms[1]},
             "clocks": sampler.summary() if sampler else None}
 
@@ -346,7 +357,7 @@ def measure_workload(torch, prob, steps, warmup, stream, dev, world, mass=None, 
         states = {}
         for prec in precs:
             r = time_run(torch, m, prob, steps, warmup, prec, stream, dev, world)
-            states[prec] = m.get_state()[0]
+            states[prec] = r["state"][0]
             out[prec] = {"value": r["value"], "ms_per_step": r["ms"] / steps, "kernels": r["kernels"]}
         if "fp64" in states and "mixed" in states:
             u64 = states["fp64"]
@@ -464,7 +475,6 @@ def run_ours(args, rank, world, local):
     for prec in ("fp64", "mixed"):
         res[prec] = time_run(torch, model, prob, args.steps, args.warmup, prec, stream, dev, world,
                              sampler_index=local if prec == "mixed" else None)
-        res[prec]["state"] = model.get_state()
     # accuracy of the mixed path against the FP64 path (itself 1e-12 from the oracle)
     u64, um = res["fp64"]["state"][0], res["mixed"]["state"][0]
     disp_err = float(np.linalg.norm(um - u64) / np.linalg.norm(u64))
