@@ -223,8 +223,14 @@ __host__ __device__ constexpr int hex6_local(int t, int k) {
     return k == 0 ? 0 : k == 3 ? 3 : k == 1 ? (t == 0 ? 1 : t == 1 ? 2 : t + 2) : (t == 0 ? 2 : t == 5 ? 1 : t + 3);
 }
 
+// Small blocks: on B200 the FP32 kernel (held to 128 registers, four 128-thread blocks
+// per SM) ran 3% faster than with 256-thread blocks, and the FP64 kernel (about 190
+// registers, 64-thread blocks) 20% faster, from the finer granularity at equal occupancy.
+template <typename T>
+constexpr int hex6_block() { return sizeof(T) == 4 ? 128 : 64; }
+
 template <typename T, int MAT, int TPH>
-__global__ void __launch_bounds__(256) k_tet4_hex6_force(GaussBlockDev b, const double4* __restrict__ X4,
+__global__ void __launch_bounds__(hex6_block<T>(), (sizeof(T) == 4 ? 4 : 1)) k_tet4_hex6_force(GaussBlockDev b, const double4* __restrict__ X4,
                                                           const double4* __restrict__ U4,
                                                           vec4_t<T>* __restrict__ slots, int* status) {
     const int64_t gt = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -1348,9 +1354,9 @@ void launch_gauss_force(const GaussBlockDev& b, int mixed, const double4* X4, co
     if (b.num_elems == 0) return;
     if (b.kind == AM_TET4_GAUSS && b.patched == 2) {
         if (mixed) {
-            AM_DISPATCH_MAT(b.material, (k_tet4_hex6_force<float, M, 1><<<grid_for(b.num_patches, 256), 256, 0, s>>>(b, X4, U4, static_cast<float4*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (k_tet4_hex6_force<float, M, 1><<<grid_for(b.num_patches, hex6_block<float>()), hex6_block<float>(), 0, s>>>(b, X4, U4, static_cast<float4*>(slots), status)));
         } else {
-            AM_DISPATCH_MAT(b.material, (k_tet4_hex6_force<double, M, 1><<<grid_for(b.num_patches, 256), 256, 0, s>>>(b, X4, U4, static_cast<double4*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (k_tet4_hex6_force<double, M, 1><<<grid_for(b.num_patches, hex6_block<double>()), hex6_block<double>(), 0, s>>>(b, X4, U4, static_cast<double4*>(slots), status)));
         }
     } else if (b.kind == AM_TET4_GAUSS && b.patched) {
         const unsigned grid = grid_for(b.num_patches, 8 * kPatchesPerWarp);
