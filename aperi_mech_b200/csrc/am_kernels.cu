@@ -418,10 +418,10 @@ __device__ __forceinline__ void hex_conn(const GaussBlockDev& b, int64_t e, int3
 }
 
 // The FP32 kernel is held to 128 registers (four 128-thread blocks per SM); the
-// FP64 one keeps its ~250 registers: forcing three blocks per SM spills and was
-// slower on B200.
+// FP64 one keeps its ~250 registers (forcing three blocks per SM spills and was
+// slower on B200) and runs in 64-thread blocks.
 template <typename T, int MAT>
-__global__ void __launch_bounds__(128, sizeof(T) == 8 ? 1 : 4) k_hex8_force(GaussBlockDev b, const double4* __restrict__ X4,
+__global__ void __launch_bounds__(sizeof(T) == 8 ? 64 : 128, sizeof(T) == 8 ? 1 : 4) k_hex8_force(GaussBlockDev b, const double4* __restrict__ X4,
                                                          const double4* __restrict__ U4,
                                                          vec4_t<T>* __restrict__ slots, int* status) {
     const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -739,7 +739,7 @@ __global__ void __launch_bounds__(256) k_tet4_patch_vjp(GaussBlockDev b, const d
 // sum, and the material-field contractions are summed over the Gauss points in
 // order. One thread per element, FP64.
 template <int MAT>
-__global__ void __launch_bounds__(128) k_hex8_vjp(GaussBlockDev b, const double4* __restrict__ X4,
+__global__ void __launch_bounds__(64) k_hex8_vjp(GaussBlockDev b, const double4* __restrict__ X4,
                                                        const double4* __restrict__ U4, const double4* __restrict__ L4,
                                                        double4* __restrict__ slots, double* gmu, double* gk,
                                                        int accumulate) {
@@ -940,7 +940,7 @@ __global__ void k_gauss_volume_slots(GaussBlockDev b, double density, const doub
 // ---------------------------------------------------------------------------
 // Sum of node i's slots: a contiguous node-major range, summed in ascending
 // logical-slot order (FP64 accumulation for both slot types).
-constexpr int kNodeBlock = 256;
+constexpr int kNodeBlock = 128;  // 7-8% faster node kernels than 256-thread blocks on B200
 
 // Node-centric gather of a node's force slots (node-major, contiguous), summed in
 // FP64 in slot order. BATCH loads are issued before the first add. A node of a hex
@@ -1377,7 +1377,7 @@ void launch_gauss_force(const GaussBlockDev& b, int mixed, const double4* X4, co
         if (mixed) {
             AM_DISPATCH_MAT(b.material, (k_hex8_force<float, M><<<grid, 128, 0, s>>>(b, X4, U4, static_cast<float4*>(slots), status)));
         } else {
-            AM_DISPATCH_MAT(b.material, (k_hex8_force<double, M><<<grid, 128, 0, s>>>(b, X4, U4, static_cast<double4*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (k_hex8_force<double, M><<<grid_for(b.num_elems, 64), 64, 0, s>>>(b, X4, U4, static_cast<double4*>(slots), status)));
         }
     }
 }
@@ -1439,7 +1439,7 @@ void launch_gauss_vjp(const GaussBlockDev& b, const double4* X4, const double4* 
         AM_DISPATCH_MAT(b.material, (k_tet4_vjp<M><<<grid, 256, 0, s>>>(b, X4, U4, L4, slots, gmu, gkappa, accumulate)));
     } else {
         const unsigned grid = grid_for(b.num_elems, 128);
-        AM_DISPATCH_MAT(b.material, (k_hex8_vjp<M><<<grid, 128, 0, s>>>(b, X4, U4, L4, slots, gmu, gkappa, accumulate)));
+        AM_DISPATCH_MAT(b.material, (k_hex8_vjp<M><<<grid_for(b.num_elems, 64), 64, 0, s>>>(b, X4, U4, L4, slots, gmu, gkappa, accumulate)));
     }
 }
 
@@ -1530,7 +1530,7 @@ void launch_adj_prep(const NodeDev& nd, const StepParams* table, int64_t step, c
 
 void launch_adj_update(const NodeDev& nd, const double4* slots, const StepParams* table, int64_t step, double4* UB,
                        double4* VB, double4* AB, double4* L4, cudaStream_t s) {
-    k_adj_update<<<grid_for(nd.num_nodes, 256), 256, 0, s>>>(nd, slots, table, step, UB, VB, AB, L4);
+    k_adj_update<<<grid_for(nd.num_nodes, kNodeBlock), kNodeBlock, 0, s>>>(nd, slots, table, step, UB, VB, AB, L4);
 }
 
 void launch_sensor_seed(const double4* U4, int32_t num_sensors, const int32_t* sensors, double4* UB, double* loss,
