@@ -1481,13 +1481,13 @@ inline bool gather_batch8(const NodeDev& nd, int mixed) {
         const bool b8 = gather_batch8(nd, mixed);                                                     \
         if (mixed) {                                                                                  \
             const float4* sl = static_cast<const float4*>(slots);                                     \
-            if (lpn == 8) KERNEL<float, 2, 8><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);        \
+            if (lpn == 8) KERNEL<float, 4, 8><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);        \
             else if (lpn == 4) KERNEL<float, 2, 4><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);   \
             else if (b8) KERNEL<float, 8, 1><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);         \
             else KERNEL<float, 4, 1><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);                 \
         } else {                                                                                      \
             const double4* sl = static_cast<const double4*>(slots);                                   \
-            if (lpn == 8) KERNEL<double, 2, 8><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);       \
+            if (lpn == 8) KERNEL<double, 4, 8><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);       \
             else if (lpn == 4) KERNEL<double, 2, 4><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);  \
             else if (b8) KERNEL<double, 8, 1><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);        \
             else KERNEL<double, 4, 1><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);                \
