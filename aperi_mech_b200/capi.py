@@ -28,7 +28,7 @@ EXPORTED = [
     "am_adjoint", "am_stress", "am_quadrature", "am_last_error", "am_status_string", "am_launch_count",
     "am_profile_enable", "am_profile_read", "am_complete_properties", "am_set_block_fields",
     "am_tet4_internal_force_noalloc", "am_rkpm_nodal_cells", "am_cells_sizes", "am_cells_get",
-    "am_cells_get_points", "am_cells_destroy", "am_get_layout", "am_set_interface", "am_nccl_unique_id",
+    "am_cells_get_points", "am_cells_destroy", "am_get_layout", "am_rkpm_element_cells", "am_set_interface", "am_nccl_unique_id",
     "am_set_nccl",
 ]
 
@@ -110,6 +110,7 @@ def load(build_if_missing: bool = False) -> C.CDLL:
         "am_tet4_internal_force_noalloc": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_int64, C.c_int64, vp, vp,
                                                     vp, vp, vp, vp, vp]),
         "am_rkpm_nodal_cells": (C.c_int, [C.c_int64, _dp, C.c_int64, _ip, _dp, C.c_int32, C.c_double, C.POINTER(vp)]),
+        "am_rkpm_element_cells": (C.c_int, [C.c_int64, _dp, C.c_int64, _ip, _dp, C.c_int32, C.c_double, C.POINTER(vp)]),
         "am_cells_sizes": (C.c_int, [vp, _lp, _lp, _lp, _lp]),
         "am_cells_get": (C.c_int, [vp, _lp, _ip, _dp, _dp, _dp]),
         "am_cells_get_points": (C.c_int, [vp, _dp, _lp, _ip, _dp]),

@@ -1,5 +1,6 @@
-// am_rkpm.cu -- set-up of RKPM one-pass nodal smoothing cells (the smoothed-cell data
-// consumed by the cell force kernels).
+// am_rkpm.cu -- set-up of RKPM one-pass smoothing cells (the smoothed-cell data
+// consumed by the cell force kernels): nodal cells on the thex corner hexes, and
+// element cells (one per tet, functions at the vertices).
 //
 // The nodal smoothing domain of a tet-mesh vertex is the union of the hexes that
 // the thex refinement puts at that vertex in each of its tets (corners, edge
@@ -208,6 +209,104 @@ void hex_smoothed(const double* X, double* B, double* vol) {
     *vol = V;
 }
 
+// Neighbours of every point of c->points (ball search with the neighbour's kernel
+// radius on a uniform grid of cell size rmax, sorted by the tweaked squared distance,
+// truncated to max_neighbors) and the reproducing-kernel function values there (FP64,
+// on the GPU): fills c->nbr_ptr, c->nbr, c->psi.
+void rk_functions(am_cells* c, int64_t N, const double* X, const double* R, double rmax, int32_t max_neighbors) {
+    const std::vector<double>& pts = c->points;
+    const int64_t P = static_cast<int64_t>(pts.size() / 3);
+    // Uniform grid over the active nodes, cell size = largest kernel radius.
+    double lo[3] = {X[0], X[1], X[2]}, hi[3] = {X[0], X[1], X[2]};
+    for (int64_t j = 0; j < N; ++j)
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = std::min(lo[k], X[3 * j + k]);
+            hi[k] = std::max(hi[k], X[3 * j + k]);
+        }
+    int64_t dim[3];
+    for (int k = 0; k < 3; ++k) dim[k] = std::max<int64_t>(1, static_cast<int64_t>((hi[k] - lo[k]) / rmax) + 1);
+    auto cell_of = [&](const double* x, int k) {
+        return std::min<int64_t>(dim[k] - 1, std::max<int64_t>(0, static_cast<int64_t>((x[k] - lo[k]) / rmax)));
+    };
+    const int64_t ncell = dim[0] * dim[1] * dim[2];
+    std::vector<int64_t> gptr(ncell + 1, 0);
+    std::vector<int32_t> gnode(N);
+    for (int64_t j = 0; j < N; ++j)
+        ++gptr[1 + cell_of(X + 3 * j, 0) + dim[0] * (cell_of(X + 3 * j, 1) + dim[1] * cell_of(X + 3 * j, 2))];
+    for (int64_t g = 0; g < ncell; ++g) gptr[g + 1] += gptr[g];
+    {
+        std::vector<int64_t> fill(gptr.begin(), gptr.end() - 1);
+        for (int64_t j = 0; j < N; ++j)
+            gnode[fill[cell_of(X + 3 * j, 0) + dim[0] * (cell_of(X + 3 * j, 1) + dim[1] * cell_of(X + 3 * j, 2))]++] =
+                static_cast<int32_t>(j);
+    }
+    // Neighbours of every point.
+    std::vector<std::vector<int32_t>> nb(P);
+    parallel_for(P, [&](int64_t q) {
+        const double* x = &pts[q * 3];
+        std::vector<std::pair<double, int32_t>> cand;
+        const int64_t cx = cell_of(x, 0), cy = cell_of(x, 1), cz = cell_of(x, 2);
+        for (int64_t gz = std::max<int64_t>(0, cz - 1); gz <= std::min(dim[2] - 1, cz + 1); ++gz)
+            for (int64_t gy = std::max<int64_t>(0, cy - 1); gy <= std::min(dim[1] - 1, cy + 1); ++gy)
+                for (int64_t gx = std::max<int64_t>(0, cx - 1); gx <= std::min(dim[0] - 1, cx + 1); ++gx) {
+                    const int64_t g = gx + dim[0] * (gy + dim[1] * gz);
+                    for (int64_t s = gptr[g]; s < gptr[g + 1]; ++s) {
+                        const int32_t j = gnode[s];
+                        const double dx = x[0] - X[j * 3], dy = x[1] - X[j * 3 + 1], dz = x[2] - X[j * 3 + 2];
+                        if (dx * dx + dy * dy + dz * dz > R[j] * R[j]) continue;
+                        const double ex = X[j * 3] * (1 + 1.0e-6) - x[0], ey = X[j * 3 + 1] * (1 + 1.0e-7) - x[1],
+                                     ez = X[j * 3 + 2] * (1 + 1.0e-8) - x[2];
+                        cand.push_back({ex * ex + ey * ey + ez * ez, j});
+                    }
+                }
+        std::sort(cand.begin(), cand.end());
+        if (static_cast<int64_t>(cand.size()) > max_neighbors) cand.resize(max_neighbors);
+        nb[q].reserve(cand.size());
+        for (const auto& cd : cand) nb[q].push_back(cd.second);
+    });
+    c->nbr_ptr.assign(P + 1, 0);
+    for (int64_t q = 0; q < P; ++q) c->nbr_ptr[q + 1] = c->nbr_ptr[q] + static_cast<int64_t>(nb[q].size());
+    const int64_t S = c->nbr_ptr[P];
+    c->nbr.resize(S);
+    parallel_for(P, [&](int64_t q) { std::copy(nb[q].begin(), nb[q].end(), c->nbr.begin() + c->nbr_ptr[q]); });
+    std::vector<std::vector<int32_t>>().swap(nb);
+    // Function values on the GPU in FP64.
+    c->psi.assign(S, 0.0);
+    {
+        double *dp = nullptr, *dx = nullptr, *dr = nullptr, *dv = nullptr;
+        int64_t* dptr = nullptr;
+        int32_t* dn = nullptr;
+        auto cleanup = [&] {
+            cudaFree(dp);
+            cudaFree(dx);
+            cudaFree(dr);
+            cudaFree(dv);
+            cudaFree(dptr);
+            cudaFree(dn);
+        };
+        try {
+            ck(cudaMalloc(&dp, P * 3 * sizeof(double)), "rk points");
+            ck(cudaMalloc(&dx, N * 3 * sizeof(double)), "rk coords");
+            ck(cudaMalloc(&dr, N * sizeof(double)), "rk radii");
+            ck(cudaMalloc(&dv, std::max<int64_t>(S, 1) * sizeof(double)), "rk values");
+            ck(cudaMalloc(&dptr, (P + 1) * sizeof(int64_t)), "rk ptr");
+            ck(cudaMalloc(&dn, std::max<int64_t>(S, 1) * sizeof(int32_t)), "rk nbr");
+            ck(cudaMemcpy(dp, pts.data(), P * 3 * sizeof(double), cudaMemcpyHostToDevice), "upload");
+            ck(cudaMemcpy(dx, X, N * 3 * sizeof(double), cudaMemcpyHostToDevice), "upload");
+            ck(cudaMemcpy(dr, R, N * sizeof(double), cudaMemcpyHostToDevice), "upload");
+            ck(cudaMemcpy(dptr, c->nbr_ptr.data(), (P + 1) * sizeof(int64_t), cudaMemcpyHostToDevice), "upload");
+            if (S > 0) ck(cudaMemcpy(dn, c->nbr.data(), S * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+            ck(cudaMemset(dv, 0, std::max<int64_t>(S, 1) * sizeof(double)), "memset");
+            k_rk_values<<<static_cast<unsigned>((P + 127) / 128), 128>>>(P, dp, dx, dr, dptr, dn, dv);
+            ck(cudaGetLastError(), "rk kernel");
+            if (S > 0) ck(cudaMemcpy(c->psi.data(), dv, S * sizeof(double), cudaMemcpyDeviceToHost), "download");
+        } catch (...) {
+            cleanup();
+            throw;
+        }
+        cleanup();
+    }}
+
 }  // namespace
 
 extern "C" {
@@ -273,96 +372,7 @@ int am_rkpm_nodal_cells(int64_t N, const double* X, int64_t T, const int32_t* te
                 pts[p * 3 + k] = (((X[s[0] * 3 + k] + X[s[1] * 3 + k]) + X[s[2] * 3 + k]) + X[s[3] * 3 + k]) * 0.25;
             ++p;
         }
-        // Uniform grid over the active nodes, cell size = largest kernel radius.
-        double lo[3] = {X[0], X[1], X[2]}, hi[3] = {X[0], X[1], X[2]};
-        for (int64_t j = 0; j < N; ++j)
-            for (int k = 0; k < 3; ++k) {
-                lo[k] = std::min(lo[k], X[3 * j + k]);
-                hi[k] = std::max(hi[k], X[3 * j + k]);
-            }
-        int64_t dim[3];
-        for (int k = 0; k < 3; ++k) dim[k] = std::max<int64_t>(1, static_cast<int64_t>((hi[k] - lo[k]) / rmax) + 1);
-        auto cell_of = [&](const double* x, int k) {
-            return std::min<int64_t>(dim[k] - 1, std::max<int64_t>(0, static_cast<int64_t>((x[k] - lo[k]) / rmax)));
-        };
-        const int64_t ncell = dim[0] * dim[1] * dim[2];
-        std::vector<int64_t> gptr(ncell + 1, 0);
-        std::vector<int32_t> gnode(N);
-        for (int64_t j = 0; j < N; ++j)
-            ++gptr[1 + cell_of(X + 3 * j, 0) + dim[0] * (cell_of(X + 3 * j, 1) + dim[1] * cell_of(X + 3 * j, 2))];
-        for (int64_t g = 0; g < ncell; ++g) gptr[g + 1] += gptr[g];
-        {
-            std::vector<int64_t> fill(gptr.begin(), gptr.end() - 1);
-            for (int64_t j = 0; j < N; ++j)
-                gnode[fill[cell_of(X + 3 * j, 0) + dim[0] * (cell_of(X + 3 * j, 1) + dim[1] * cell_of(X + 3 * j, 2))]++] =
-                    static_cast<int32_t>(j);
-        }
-        // Neighbours of every point.
-        std::vector<std::vector<int32_t>> nb(P);
-        parallel_for(P, [&](int64_t q) {
-            const double* x = &pts[q * 3];
-            std::vector<std::pair<double, int32_t>> cand;
-            const int64_t cx = cell_of(x, 0), cy = cell_of(x, 1), cz = cell_of(x, 2);
-            for (int64_t gz = std::max<int64_t>(0, cz - 1); gz <= std::min(dim[2] - 1, cz + 1); ++gz)
-                for (int64_t gy = std::max<int64_t>(0, cy - 1); gy <= std::min(dim[1] - 1, cy + 1); ++gy)
-                    for (int64_t gx = std::max<int64_t>(0, cx - 1); gx <= std::min(dim[0] - 1, cx + 1); ++gx) {
-                        const int64_t g = gx + dim[0] * (gy + dim[1] * gz);
-                        for (int64_t s = gptr[g]; s < gptr[g + 1]; ++s) {
-                            const int32_t j = gnode[s];
-                            const double dx = x[0] - X[j * 3], dy = x[1] - X[j * 3 + 1], dz = x[2] - X[j * 3 + 2];
-                            if (dx * dx + dy * dy + dz * dz > R[j] * R[j]) continue;
-                            const double ex = X[j * 3] * (1 + 1.0e-6) - x[0], ey = X[j * 3 + 1] * (1 + 1.0e-7) - x[1],
-                                         ez = X[j * 3 + 2] * (1 + 1.0e-8) - x[2];
-                            cand.push_back({ex * ex + ey * ey + ez * ez, j});
-                        }
-                    }
-            std::sort(cand.begin(), cand.end());
-            if (static_cast<int64_t>(cand.size()) > max_neighbors) cand.resize(max_neighbors);
-            nb[q].reserve(cand.size());
-            for (const auto& cd : cand) nb[q].push_back(cd.second);
-        });
-        c->nbr_ptr.assign(P + 1, 0);
-        for (int64_t q = 0; q < P; ++q) c->nbr_ptr[q + 1] = c->nbr_ptr[q] + static_cast<int64_t>(nb[q].size());
-        const int64_t S = c->nbr_ptr[P];
-        c->nbr.resize(S);
-        parallel_for(P, [&](int64_t q) { std::copy(nb[q].begin(), nb[q].end(), c->nbr.begin() + c->nbr_ptr[q]); });
-        std::vector<std::vector<int32_t>>().swap(nb);
-        // Function values on the GPU in FP64.
-        c->psi.assign(S, 0.0);
-        {
-            double *dp = nullptr, *dx = nullptr, *dr = nullptr, *dv = nullptr;
-            int64_t* dptr = nullptr;
-            int32_t* dn = nullptr;
-            auto cleanup = [&] {
-                cudaFree(dp);
-                cudaFree(dx);
-                cudaFree(dr);
-                cudaFree(dv);
-                cudaFree(dptr);
-                cudaFree(dn);
-            };
-            try {
-                ck(cudaMalloc(&dp, P * 3 * sizeof(double)), "rk points");
-                ck(cudaMalloc(&dx, N * 3 * sizeof(double)), "rk coords");
-                ck(cudaMalloc(&dr, N * sizeof(double)), "rk radii");
-                ck(cudaMalloc(&dv, std::max<int64_t>(S, 1) * sizeof(double)), "rk values");
-                ck(cudaMalloc(&dptr, (P + 1) * sizeof(int64_t)), "rk ptr");
-                ck(cudaMalloc(&dn, std::max<int64_t>(S, 1) * sizeof(int32_t)), "rk nbr");
-                ck(cudaMemcpy(dp, pts.data(), P * 3 * sizeof(double), cudaMemcpyHostToDevice), "upload");
-                ck(cudaMemcpy(dx, X, N * 3 * sizeof(double), cudaMemcpyHostToDevice), "upload");
-                ck(cudaMemcpy(dr, R, N * sizeof(double), cudaMemcpyHostToDevice), "upload");
-                ck(cudaMemcpy(dptr, c->nbr_ptr.data(), (P + 1) * sizeof(int64_t), cudaMemcpyHostToDevice), "upload");
-                if (S > 0) ck(cudaMemcpy(dn, c->nbr.data(), S * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
-                ck(cudaMemset(dv, 0, std::max<int64_t>(S, 1) * sizeof(double)), "memset");
-                k_rk_values<<<static_cast<unsigned>((P + 127) / 128), 128>>>(P, dp, dx, dr, dptr, dn, dv);
-                ck(cudaGetLastError(), "rk kernel");
-                if (S > 0) ck(cudaMemcpy(c->psi.data(), dv, S * sizeof(double), cudaMemcpyDeviceToHost), "download");
-            } catch (...) {
-                cleanup();
-                throw;
-            }
-            cleanup();
-        }
+        rk_functions(c, N, X, R, rmax, max_neighbors);
         // Corner hexes of each vertex (tet order) -> one-pass cell gradients.
         std::vector<int64_t> vptr(N + 1, 0);
         for (int64_t i = 0; i < 4 * T; ++i) ++vptr[tets[i] + 1];
@@ -445,6 +455,105 @@ int am_rkpm_nodal_cells(int64_t N, const double* X, int64_t T, const int32_t* te
             for (int k = 0; k < 8; ++k) mfe[hexpts[h][k]] += hexvol[h] * density / 8;
         c->mass.assign(N, 0.0);
         for (int64_t q = 0; q < P; ++q)
+            for (int64_t e = c->nbr_ptr[q]; e < c->nbr_ptr[q + 1]; ++e) c->mass[c->nbr[e]] += mfe[q] * c->psi[e];
+        *out = hold.release();
+        return AM_OK;
+    } catch (const Fail& f) {
+        am::set_free_error(f.msg);
+        return f.code;
+    } catch (const std::bad_alloc&) {
+        am::set_free_error("host allocation failed");
+        return AM_ENOMEM;
+    } catch (const std::exception& e) {
+        am::set_free_error(e.what());
+        return AM_EINVAL;
+    }
+}
+
+int am_rkpm_element_cells(int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R,
+                          int32_t max_neighbors, double density, am_cells** out) {
+    am::set_free_error("");
+    if (!out) return AM_EINVAL;
+    *out = nullptr;
+    try {
+        if (N <= 0 || T <= 0 || !X || !tets || !R) throw Fail{AM_EINVAL, "empty mesh or null array"};
+        if (max_neighbors <= 0) throw Fail{AM_EINVAL, "max_neighbors must be positive"};
+        if (!(density > 0.0)) throw Fail{AM_EINVAL, "density must be positive"};
+        for (int64_t i = 0; i < 4 * T; ++i)
+            if (tets[i] < 0 || tets[i] >= N) throw Fail{AM_EINVAL, "tet node index out of range"};
+        double rmax = 0.0;
+        for (int64_t j = 0; j < N; ++j) {
+            if (!(R[j] > 0.0)) throw Fail{AM_EINVAL, "kernel radii must be positive"};
+            rmax = std::max(rmax, R[j]);
+        }
+        auto c = new am_cells();
+        std::unique_ptr<am_cells> hold(c);
+        c->num_nodes = N;
+        // The functions are needed at the vertices only.
+        c->points.assign(X, X + 3 * N);
+        rk_functions(c, N, X, R, rmax, max_neighbors);
+        // One cell per tet: entries = union of the four vertices' neighbours (vertex order,
+        // then neighbour order); b_{t,j} = sum_k B_{t,k} V_t psi_k(j) / V_t.
+        std::vector<std::vector<int32_t>> cn(T);
+        std::vector<std::vector<double>> cg(T);
+        c->cell_volumes.assign(T, 0.0);
+        std::atomic<int> bad(0);
+        parallel_for(T, [&](int64_t t) {
+            const int32_t* v = tets + 4 * t;
+            double J[9];  // J[i][a] = x_{a+1,i} - x_{0,i}
+            for (int i = 0; i < 3; ++i)
+                for (int a = 0; a < 3; ++a) J[i * 3 + a] = X[v[a + 1] * 3 + i] - X[v[0] * 3 + i];
+            const double det = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) +
+                               J[2] * (J[3] * J[7] - J[4] * J[6]);
+            if (!(det > 0.0)) {
+                bad = 1;
+                return;
+            }
+            const double id = 1.0 / det;
+            // Rows of J^-1 are the gradients of the barycentric coordinates 1..3.
+            const double Ji[9] = {(J[4] * J[8] - J[5] * J[7]) * id, (J[2] * J[7] - J[1] * J[8]) * id,
+                                  (J[1] * J[5] - J[2] * J[4]) * id, (J[5] * J[6] - J[3] * J[8]) * id,
+                                  (J[0] * J[8] - J[2] * J[6]) * id, (J[2] * J[3] - J[0] * J[5]) * id,
+                                  (J[3] * J[7] - J[4] * J[6]) * id, (J[1] * J[6] - J[0] * J[7]) * id,
+                                  (J[0] * J[4] - J[1] * J[3]) * id};
+            double B[12];
+            for (int i = 0; i < 3; ++i) {
+                B[3 + i] = Ji[0 * 3 + i];
+                B[6 + i] = Ji[1 * 3 + i];
+                B[9 + i] = Ji[2 * 3 + i];
+                B[i] = -(B[3 + i] + B[6 + i] + B[9 + i]);
+            }
+            const double V = det / 6.0;
+            c->cell_volumes[t] = V;
+            for (int k = 0; k < 4; ++k)
+                for (int64_t e = c->nbr_ptr[v[k]]; e < c->nbr_ptr[v[k] + 1]; ++e) {
+                    const int32_t j = c->nbr[e];
+                    size_t idx = std::find(cn[t].begin(), cn[t].end(), j) - cn[t].begin();
+                    if (idx == cn[t].size()) {
+                        cn[t].push_back(j);
+                        cg[t].insert(cg[t].end(), {0.0, 0.0, 0.0});
+                    }
+                    for (int q = 0; q < 3; ++q) cg[t][idx * 3 + q] += B[k * 3 + q] * V * c->psi[e];
+                }
+            for (double& g : cg[t]) g /= V;
+        });
+        if (bad) throw Fail{AM_ENONPOS_J, "a tet has non-positive volume"};
+        c->cell_ptr.assign(T + 1, 0);
+        for (int64_t t = 0; t < T; ++t) c->cell_ptr[t + 1] = c->cell_ptr[t] + static_cast<int64_t>(cn[t].size());
+        const int64_t K = c->cell_ptr[T];
+        if (K >= (int64_t(1) << 31)) throw Fail{AM_ERANGE, "cell entry count beyond int32 indexing"};
+        c->cell_nodes.resize(K);
+        c->cell_grads.resize(K * 3);
+        parallel_for(T, [&](int64_t t) {
+            std::copy(cn[t].begin(), cn[t].end(), c->cell_nodes.begin() + c->cell_ptr[t]);
+            std::copy(cg[t].begin(), cg[t].end(), c->cell_grads.begin() + 3 * c->cell_ptr[t]);
+        });
+        // Lumped mass: rho V_t / 4 to the vertices, scattered through the functions.
+        std::vector<double> mfe(N, 0.0);
+        for (int64_t t = 0; t < T; ++t)
+            for (int k = 0; k < 4; ++k) mfe[tets[4 * t + k]] += density * c->cell_volumes[t] / 4;
+        c->mass.assign(N, 0.0);
+        for (int64_t q = 0; q < N; ++q)
             for (int64_t e = c->nbr_ptr[q]; e < c->nbr_ptr[q + 1]; ++e) c->mass[c->nbr[e]] += mfe[q] * c->psi[e];
         *out = hold.release();
         return AM_OK;

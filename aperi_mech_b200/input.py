@@ -292,8 +292,17 @@ def _part(pnode: dict, blocks: dict, coords, ext: dict, rng):
                             max_neighbors=int(ext.get("max_neighbors", 40)))
         cells.part.name = name
         return cells.part, cells.mass
-    raise InputError(f"{space} with {cell}: not built (finite_element + element cells, "
-                     f"or reproducing_kernel + nodal cells)")
+    if space == "reproducing_kernel" and cell == "element_smoothing_cell":
+        if mu_f is not None or kappa_f is not None:
+            raise InputError("x_b200.fields on RKPM element cells: per-cell fields are not supported")
+        from .rkpm import element_cells, tet_max_edge_length
+
+        scale = float((spnode or {}).get("kernel_radius_scale_factor", 1.0))
+        cells = element_cells(coords, conn, mat, scale * tet_max_edge_length(coords, conn),
+                              max_neighbors=int(ext.get("max_neighbors", 40)))
+        cells.part.name = name
+        return cells.part, cells.mass
+    raise InputError(f"{space} with {cell}: not built")
 
 
 def load(source, base_dir: Path | None = None) -> Simulation:

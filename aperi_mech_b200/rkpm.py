@@ -1,7 +1,9 @@
-"""RKPM one-pass nodal smoothing cells (ElementReproducingKernel with
-nodal_smoothing_cell, include/ElementReproducingKernel.h) built by the library's
-set-up (am_rkpm_nodal_cells): neighbour search, FP64 reproducing-kernel functions
-on the GPU, one-pass smoothed gradients on the tet-corner hexes, lumped mass."""
+"""RKPM one-pass smoothing cells (ElementReproducingKernel, include/ElementReproducingKernel.h)
+built by the library's set-up: neighbour search, FP64 reproducing-kernel functions on
+the GPU, one-pass smoothed gradients, lumped mass scattered through the functions.
+Nodal cells (nodal_smoothing_cell) live on the tet-corner hexes of the thex refinement
+(am_rkpm_nodal_cells); element cells (element_smoothing_cell) are the tets themselves
+(am_rkpm_element_cells)."""
 from __future__ import annotations
 
 import ctypes as C
@@ -49,16 +51,43 @@ def thex_max_edge_length(coords: np.ndarray, tets: np.ndarray) -> np.ndarray:
     return out
 
 
+def tet_max_edge_length(coords: np.ndarray, tets: np.ndarray) -> np.ndarray:
+    """MaxEdgeLengthFunctor (src/MaxEdgeLengthProcessor.cpp:36-60) on a tet mesh whose
+    nodes are all active: per node, the longest distance to a node of a connected tet."""
+    x = coords[tets]
+    out = np.zeros(coords.shape[0])
+    for a in range(4):
+        for b in range(4):
+            if a != b:
+                np.maximum.at(out, tets[:, a], np.linalg.norm(x[:, a] - x[:, b], axis=1))
+    return out
+
+
 def nodal_cells(coords: np.ndarray, tets: np.ndarray, material: Material, kernel_radius: np.ndarray,
                 max_neighbors: int = 40, keep_points: bool = False, mu_field=None, kappa_field=None,
                 name: str = "block_1") -> RKPMCells:
+    """One cell per vertex on the thex corner hexes (nodal_smoothing_cell)."""
+    return _cells("am_rkpm_nodal_cells", coords, tets, material, kernel_radius, max_neighbors, keep_points,
+                  mu_field, kappa_field, name)
+
+
+def element_cells(coords: np.ndarray, tets: np.ndarray, material: Material, kernel_radius: np.ndarray,
+                  max_neighbors: int = 40, keep_points: bool = False, mu_field=None, kappa_field=None,
+                  name: str = "block_1") -> RKPMCells:
+    """One cell per tet (element_smoothing_cell with the reproducing_kernel space)."""
+    return _cells("am_rkpm_element_cells", coords, tets, material, kernel_radius, max_neighbors, keep_points,
+                  mu_field, kappa_field, name)
+
+
+def _cells(entry: str, coords, tets, material, kernel_radius, max_neighbors, keep_points, mu_field, kappa_field,
+           name) -> RKPMCells:
     lib = capi.load()
     X = np.ascontiguousarray(coords, dtype=np.float64)
     T = np.ascontiguousarray(tets, dtype=np.int32)
     R = np.ascontiguousarray(kernel_radius, dtype=np.float64)
     h = C.c_void_p()
-    check(lib.am_rkpm_nodal_cells(X.shape[0], capi._ptr(X), T.shape[0], capi._ptr(T, C.c_int32), capi._ptr(R),
-                                  int(max_neighbors), float(material.density), C.byref(h)))
+    check(getattr(lib, entry)(X.shape[0], capi._ptr(X), T.shape[0], capi._ptr(T, C.c_int32), capi._ptr(R),
+                              int(max_neighbors), float(material.density), C.byref(h)))
     try:
         nc, ne, npnt, nn = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
         check(lib.am_cells_sizes(h, C.byref(nc), C.byref(ne), C.byref(npnt), C.byref(nn)))
@@ -66,7 +95,7 @@ def nodal_cells(coords: np.ndarray, tets: np.ndarray, material: Material, kernel
         nodes = np.empty(ne.value, dtype=np.int32)
         grads = np.empty((ne.value, 3))
         vols = np.empty(nc.value)
-        mass = np.empty(nc.value)
+        mass = np.empty(X.shape[0])
         check(lib.am_cells_get(h, capi._ptr(ptr, C.c_int64), capi._ptr(nodes, C.c_int32), capi._ptr(grads),
                                capi._ptr(vols), capi._ptr(mass)))
         res = RKPMCells(Part("cells", material, cell_ptr=ptr, cell_nodes=nodes, cell_grads=grads, cell_volumes=vols,

@@ -170,9 +170,19 @@ int am_quadrature(int32_t kind, int32_t smoothed, int64_t n, am_memory where, co
 typedef struct am_cells am_cells;
 int am_rkpm_nodal_cells(int64_t num_nodes, const double* coords, int64_t num_tets, const int32_t* tets,
                         const double* kernel_radius, int32_t max_neighbors, double density, am_cells** out);
+/* RKPM one-pass element smoothing cells (element_smoothing_cell, subdomains 1, with the
+ * reproducing_kernel approximation space): one cell per tet, whose entries are the
+ * union of its four vertices' neighbours, gradients b_{t,j} = sum_k B_{t,k} psi_k(j)
+ * (SmoothedCellDataProcessor.h:541-675 one-pass, QuadratureSmoothed.h:32-63), the
+ * functions evaluated at the vertices only, and the mass rho V_t / 4 to the vertices
+ * scattered through the functions. Same outputs and accessors as the nodal cells
+ * (the points are the vertices). */
+int am_rkpm_element_cells(int64_t num_nodes, const double* coords, int64_t num_tets, const int32_t* tets,
+                          const double* kernel_radius, int32_t max_neighbors, double density, am_cells** out);
 int am_cells_sizes(const am_cells* cells, int64_t* num_cells, int64_t* num_entries, int64_t* num_points,
                    int64_t* num_nbr_entries);
-/* cell_ptr (num_cells+1), cell_nodes/cell_grads (entries, x3), cell_volumes and mass (num_cells). */
+/* cell_ptr (num_cells+1), cell_nodes/cell_grads (entries, x3), cell_volumes (num_cells)
+ * and mass (one per mesh node). */
 int am_cells_get(const am_cells* cells, int64_t* cell_ptr, int32_t* cell_nodes, double* cell_grads,
                  double* cell_volumes, double* mass);
 /* The refinement points (x3), their neighbour CSR and function values. */

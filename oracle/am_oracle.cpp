@@ -1164,3 +1164,91 @@ extern "C" int ob_rkpm_nodal_cells(int64_t N, const double* X, int64_t T, const 
     }
     return 0;
 }
+
+// ---------------------------------------------------------------------------
+// RKPM one-pass element smoothing cells (element_smoothing_cell, subdomains 1, with
+// approximation_space reproducing_kernel): every tet is a cell whose entries are the
+// union of its four vertices' neighbours; b_{t,j} = sum_k B_{t,k} V_t psi_k(j) / V_t
+// (SmoothedCellDataProcessor.h:541-675 one-pass, QuadratureSmoothed.h:32-63 for the tet's
+// smoothed gradients); functions at the vertices only (FunctionCreationProcessor.h:85-130);
+// mass rho V_t / 4 to the vertices, scattered through the functions
+// (src/MassUtils.cpp:17-46, FunctionEvaluationProcessor.h:130-176).
+// Two calls: sizes first (outputs NULL), then the arrays.
+// ---------------------------------------------------------------------------
+extern "C" int ob_rkpm_element_cells(int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R,
+                                     int32_t max_neighbors, double density, int64_t* num_nbr_entries,
+                                     int64_t* num_cell_entries, int64_t* nbr_ptr, int32_t* nbr, double* values,
+                                     int64_t* cell_ptr, int32_t* cell_nodes, double* cell_grads, double* cell_volumes,
+                                     double* mass) {
+    std::vector<std::vector<int32_t>> nb(N);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t p = 0; p < N; ++p) {
+        std::vector<std::pair<double, int32_t>> cand;
+        const double* x = &X[p * 3];
+        for (int32_t j = 0; j < N; ++j) {
+            const double dx = x[0] - X[j * 3], dy = x[1] - X[j * 3 + 1], dz = x[2] - X[j * 3 + 2];
+            if (dx * dx + dy * dy + dz * dz > R[j] * R[j]) continue;
+            const double tx = X[j * 3] * (1 + 1.0e-6) - x[0], ty = X[j * 3 + 1] * (1 + 1.0e-7) - x[1],
+                         tz = X[j * 3 + 2] * (1 + 1.0e-8) - x[2];
+            cand.push_back({tx * tx + ty * ty + tz * tz, j});
+        }
+        std::sort(cand.begin(), cand.end());
+        if (static_cast<int32_t>(cand.size()) > max_neighbors) cand.resize(max_neighbors);
+        for (const auto& c : cand) nb[p].push_back(c.second);
+    }
+    std::vector<int64_t> ptr(N + 1, 0);
+    for (int64_t p = 0; p < N; ++p) ptr[p + 1] = ptr[p] + static_cast<int64_t>(nb[p].size());
+    std::vector<int32_t> flat(ptr[N]);
+    for (int64_t p = 0; p < N; ++p) std::copy(nb[p].begin(), nb[p].end(), flat.begin() + ptr[p]);
+    std::vector<double> psi(ptr[N]);
+    ob_rk_function_values(N, X, X, R, ptr.data(), flat.data(), psi.data());
+    std::vector<std::vector<int32_t>> cn(T);
+    std::vector<std::vector<double>> cg(T);
+    std::vector<double> cv(T, 0.0), mfe(N, 0.0);
+    for (int64_t t = 0; t < T; ++t) {
+        const int32_t* v = tets + 4 * t;
+        double xt[12], B[12], V;
+        for (int k = 0; k < 4; ++k)
+            for (int c = 0; c < 3; ++c) xt[k * 3 + c] = X[v[k] * 3 + c];
+        ob_tet4_smoothed_bw(xt, B, &V);
+        cv[t] = V;
+        std::vector<int32_t> seen;
+        for (int k = 0; k < 4; ++k) {
+            mfe[v[k]] += density * V / 4;
+            for (int64_t s = ptr[v[k]]; s < ptr[v[k] + 1]; ++s) {
+                const int32_t j = flat[s];
+                int64_t idx = std::find(cn[t].begin(), cn[t].end(), j) - cn[t].begin();
+                if (idx == static_cast<int64_t>(cn[t].size())) {
+                    cn[t].push_back(j);
+                    cg[t].insert(cg[t].end(), {0.0, 0.0, 0.0});
+                }
+                for (int c = 0; c < 3; ++c) cg[t][idx * 3 + c] += B[k * 3 + c] * V * psi[s];
+            }
+        }
+        for (double& g : cg[t]) g /= V;
+    }
+    int64_t K = 0;
+    for (int64_t t = 0; t < T; ++t) K += static_cast<int64_t>(cn[t].size());
+    if (num_nbr_entries) *num_nbr_entries = ptr[N];
+    if (num_cell_entries) *num_cell_entries = K;
+    if (nbr_ptr) std::copy(ptr.begin(), ptr.end(), nbr_ptr);
+    if (nbr) std::copy(flat.begin(), flat.end(), nbr);
+    if (values) std::copy(psi.begin(), psi.end(), values);
+    if (cell_ptr) {
+        cell_ptr[0] = 0;
+        for (int64_t t = 0; t < T; ++t) cell_ptr[t + 1] = cell_ptr[t] + static_cast<int64_t>(cn[t].size());
+    }
+    int64_t off = 0;
+    for (int64_t t = 0; t < T; ++t) {
+        if (cell_nodes) std::copy(cn[t].begin(), cn[t].end(), cell_nodes + off);
+        if (cell_grads) std::copy(cg[t].begin(), cg[t].end(), cell_grads + 3 * off);
+        off += static_cast<int64_t>(cn[t].size());
+    }
+    if (cell_volumes) std::copy(cv.begin(), cv.end(), cell_volumes);
+    if (mass) {
+        std::fill(mass, mass + N, 0.0);
+        for (int64_t p = 0; p < N; ++p)
+            for (int64_t s = ptr[p]; s < ptr[p + 1]; ++s) mass[flat[s]] += mfe[p] * psi[s];
+    }
+    return 0;
+}

@@ -125,6 +125,17 @@ int ob_rkpm_nodal_cells(int64_t num_nodes, const double* coords, int64_t num_tet
                         int64_t* cell_ptr, int32_t* cell_nodes, double* cell_grads, double* cell_volumes,
                         double* mass);
 
+/* RKPM one-pass element smoothing cells (each tet a cell; functions at the vertices).
+ * Two calls: sizes first (outputs NULL), then the arrays: the vertices' neighbour CSR
+ * (nbr_ptr N+1, nbr) with function values, cells (one per tet): cell_ptr (T+1),
+ * cell_nodes, cell_grads (x3), cell_volumes (T), mass (N): rho V_t / 4 to the vertices,
+ * scattered through the functions. */
+int ob_rkpm_element_cells(int64_t num_nodes, const double* coords, int64_t num_tets, const int32_t* tets,
+                          const double* kernel_radius, int32_t max_neighbors, double density,
+                          int64_t* num_nbr_entries, int64_t* num_cell_entries, int64_t* nbr_ptr, int32_t* nbr,
+                          double* values, int64_t* cell_ptr, int32_t* cell_nodes, double* cell_grads,
+                          double* cell_volumes, double* mass);
+
 /* ---- threads ---- */
 void ob_set_threads(int n);
 int ob_get_threads(void);

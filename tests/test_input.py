@@ -191,10 +191,13 @@ def test_yaml_run_matches_oracle(oracle_lib, precision):
 
 
 @pytest.mark.gpu
-def test_yaml_rkpm_nodal_cells_run_matches_oracle(oracle_lib):
+@pytest.mark.parametrize("cell", ["nodal_smoothing_cell", "element_smoothing_cell"])
+def test_yaml_rkpm_cells_run_matches_oracle(oracle_lib, cell):
+    """reproducing_kernel with nodal cells (thex corner hexes) or element cells (the tets,
+    as in the reference's RKPM Taylor-bar inputs)."""
     text = nh_yaml(n=4).replace(
         "gauss_quadrature: {integration_order: 1}",
-        "strain_smoothing: {nodal_smoothing_cell: {subdomains: 1}, force_one_pass_method: true}").replace(
+        f"strain_smoothing: {{{cell}: {{subdomains: 1}}, force_one_pass_method: true}}").replace(
         "finite_element: ~", "reproducing_kernel: {kernel_radius_scale_factor: 1.1}")
     sim = inp.load(text)
     assert sim.parts[0].kind == "cells" and sim.mass is not None

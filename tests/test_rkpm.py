@@ -114,3 +114,77 @@ def test_rkpm_linear_field_patch(gpu):
     deep = np.all((X > lo + 2.5 / 8) & (X < hi - 2.5 / 8), axis=1)
     assert deep.sum() > 0
     assert np.abs(f[deep]).max() < 1e-9 * np.abs(f).max()
+
+
+# ---- element smoothing cells with the reproducing-kernel space --------------------------
+def _tet_radius(X, T, scale):
+    from aperi_mech_b200.rkpm import tet_max_edge_length
+
+    return scale * tet_max_edge_length(X, T)
+
+
+def test_oracle_rk_element_cells_reproducing_conditions(oracle_lib):
+    """Element cells: partition of unity and linear completeness of the vertex functions,
+    partition of nullity and exact linear-field gradients per tet cell, total volume and
+    total mass, entries capped by the four vertices' neighbour lists."""
+    X, T = _box(n=4, seed=1)
+    r = oracle_lib.rkpm_element_cells(X, T, _tet_radius(X, T, 1.1), max_neighbors=40, density=1000.0)
+    ptr, nb, v = r["nbr_ptr"], r["nbr"], r["values"]
+    rows = _rows(ptr)
+    assert np.abs(np.bincount(rows, weights=v, minlength=X.shape[0]) - 1.0).max() < 4e-12
+    lc = np.zeros_like(X)
+    np.add.at(lc, rows, v[:, None] * X[nb])
+    assert np.abs(lc - X).max() < 4e-11
+    g, cp, cn = r["cell_grads"], r["cell_ptr"], r["cell_nodes"]
+    assert len(cp) == T.shape[0] + 1
+    crow = _rows(cp)
+    nul = np.zeros((T.shape[0], 3))
+    np.add.at(nul, crow, g)
+    assert np.abs(nul).max() < 1e-9
+    A = np.random.default_rng(2).standard_normal((3, 3))
+    H = np.zeros((T.shape[0], 3, 3))
+    np.add.at(H, crow, (X[cn] @ A.T)[:, :, None] * g[:, None, :])
+    assert np.abs(H - A).max() < 1e-9
+    assert np.all(np.diff(cp) <= 4 * 40)
+    assert abs(r["cell_volumes"].sum() - 2.0) < 1e-12
+    assert abs(r["mass"].sum() - 2000.0) < 1e-9
+
+
+@pytest.mark.gpu
+def test_rkpm_element_cells_setup_force_and_steps_match_oracle(gpu, oracle_lib):
+    from aperi_mech_b200 import mesh
+    from aperi_mech_b200.model import BoundaryCondition, ExplicitDynamics, Material
+    from aperi_mech_b200.rkpm import element_cells
+
+    X, T = _box(n=4, seed=5)
+    R = _tet_radius(X, T, 1.1)
+    mat = Material.create("neo_hookean", 1000.0, shear_modulus=3.85e8, bulk_modulus=8.33e8)
+    got = element_cells(X, T, mat, R, keep_points=True)
+    want = oracle_lib.rkpm_element_cells(X, T, R, max_neighbors=40, density=1000.0)
+    assert np.array_equal(got.nbr_ptr, want["nbr_ptr"]) and np.array_equal(got.nbr, want["nbr"])
+    assert rel_err(got.values, want["values"]) < 1e-12
+    part = got.part
+    assert np.array_equal(part.cell_ptr, want["cell_ptr"]) and np.array_equal(part.cell_nodes, want["cell_nodes"])
+    assert rel_err(part.cell_grads, want["cell_grads"]) < 1e-12
+    assert rel_err(part.cell_volumes, want["cell_volumes"]) < 1e-13
+    assert rel_err(got.mass, want["mass"]) < 1e-12
+    fixed = mesh.side_sets(X)["surface_5"]
+    bcs = [BoundaryCondition.fixed(fixed)]
+    rng = np.random.default_rng(3)
+    v0 = rng.uniform(-0.01, 0.01, size=X.shape)
+    v0[:, 0] += X[:, 2]
+    v0[fixed] = 0.0
+    u = 1e-3 * rng.standard_normal(X.shape)
+    op = oracle_lib.OracleProblem(X, [part], bcs, mass=got.mass)
+    dt = 0.5 * float(mesh.tet_char_length(X, T).min()) / np.sqrt((mat.lam + 2 * mat.mu) / mat.density)
+    with ExplicitDynamics(X, [part], bcs, mass=got.mass) as m:
+        assert rel_err(m.internal_force(u), op.internal_force(u)) < 1e-12
+        assert rel_err(m.internal_force(u, "mixed"), op.internal_force(u)) < 5e-5
+        m.set_state(None, v0)
+        m.init_acceleration()
+        m.run(30, dt)
+        got_state = m.get_state()
+    zero = np.zeros_like(X)
+    want_state = op.steps(zero, v0, op.init_acceleration(zero), np.full(30, dt))
+    for g, w in zip(got_state, want_state):
+        assert rel_err(g, w) < 1e-12
