@@ -572,7 +572,7 @@ int am_rkpm_element_cells(int64_t N, const double* X, int64_t T, const int32_t* 
 int am_cells_sizes(const am_cells* c, int64_t* num_cells, int64_t* num_entries, int64_t* num_points,
                    int64_t* num_nbr_entries) {
     if (!c) return AM_EINVAL;
-    if (num_cells) *num_cells = c->num_nodes;
+    if (num_cells) *num_cells = c->cell_ptr.empty() ? 0 : static_cast<int64_t>(c->cell_ptr.size()) - 1;
     if (num_entries) *num_entries = static_cast<int64_t>(c->cell_nodes.size());
     if (num_points) *num_points = static_cast<int64_t>(c->points.size() / 3);
     if (num_nbr_entries) *num_nbr_entries = static_cast<int64_t>(c->nbr.size());
