@@ -28,7 +28,8 @@ EXPORTED = [
     "am_adjoint", "am_stress", "am_quadrature", "am_last_error", "am_status_string", "am_launch_count",
     "am_profile_enable", "am_profile_read", "am_complete_properties", "am_set_block_fields",
     "am_tet4_internal_force_noalloc", "am_rkpm_nodal_cells", "am_cells_sizes", "am_cells_get",
-    "am_cells_get_points", "am_cells_destroy", "am_get_layout", "am_rkpm_element_cells", "am_set_interface", "am_nccl_unique_id",
+    "am_cells_get_points", "am_cells_destroy", "am_get_layout", "am_rkpm_element_cells", "am_set_power_method",
+    "am_stable_time_increment", "am_solve_power_method", "am_set_interface", "am_nccl_unique_id",
     "am_set_nccl",
 ]
 
@@ -117,6 +118,10 @@ def load(build_if_missing: bool = False) -> C.CDLL:
         "am_cells_destroy": (None, [vp]),
         "am_get_layout": (C.c_int, [vp, _lp, _ip]),
         "am_set_interface": (C.c_int, [vp, C.c_int64, _ip, _ip, C.c_int64]),
+        "am_set_power_method": (C.c_int, [vp, _dp, _dp]),
+        "am_stable_time_increment": (C.c_int, [vp, C.c_double, C.c_int32, C.c_double, C.c_double, C.c_double, _dp, _ip,
+                                               _ip]),
+        "am_solve_power_method": (C.c_int, [vp, C.c_int, C.c_double, C.c_int64, C.c_double, C.c_int64, _lp, _dp]),
         "am_nccl_unique_id": (C.c_int, [C.c_char_p]),
         "am_set_nccl": (C.c_int, [vp, C.c_char_p, C.c_int32, C.c_int32]),
     }

@@ -277,6 +277,14 @@ struct am_ctx {
     int32_t* iface_row_of = nullptr;  // per local node: row or -1
     double* iface_buf = nullptr;      // iface_global x 3
     ncclComm_t comm = nullptr;
+    // Power method for the stable time increment (am_set_power_method).
+    std::vector<double> pm_start;     // N x 3 start vector, scaled by eps l on first use
+    double* pm_l = nullptr;           // N: max edge length per node
+    double4* pm_v = nullptr;          // the eigenvector estimate
+    double* pm_fu = nullptr;          // N x 3: F(u)
+    double* pm_fe = nullptr;          // N x 3: F(u + v l eps)
+    double* pm_partial = nullptr;     // per-block sums of squares
+    bool pm_initialized = false;
     std::vector<cudaEvent_t> events;
     std::vector<std::pair<int, int64_t>> mark_slot;
     size_t n_marks = 0;
@@ -346,6 +354,100 @@ struct am_ctx {
             nccl_check(nccl().all_reduce(iface_buf, iface_buf, static_cast<size_t>(iface_global) * 3, ncclDouble, ncclSum,
                                          comm, stream),
                        "interface all-reduce");
+    }
+
+    // PowerMethodProcessor::ComputeStableTimeIncrement (include/PowerMethodProcessor.h:331-480)
+    // at the current displacement, FP64: the increment 2 / sqrt(lambda) of the largest
+    // eigenvalue of M^-1 K estimated by power iteration on finite differences of the
+    // internal force, with the reference's stopping rules (relative change below
+    // tolerance, or the variance of the last five estimates below variation_tolerance
+    // times their mean) and its choice of result (the last estimate when converged, else
+    // the smallest of the last five).
+    double stable_time_increment(double previous, int32_t num_iterations, double eps, double tol, double vartol,
+                                 int32_t* iterations, int32_t* converged_out) {
+        if (!pm_l) fail(AM_ESTATE, "am_set_power_method first");
+        if (iface_row_of) fail(AM_ESTATE, "the power method is not available on a decomposed mesh");
+        if (num_iterations < 1 || !(eps > 0.0) || !(tol > 0.0)) fail(AM_EINVAL, "bad power-method parameters");
+        if (!pm_initialized) {
+            // InitializeEigenvector: the start vector scaled by eps times the node's edge length.
+            std::vector<double> l(N);
+            ck(cudaMemcpy(l.data(), pm_l, N * sizeof(double), cudaMemcpyDeviceToHost), "D2H");
+            std::vector<double4> v(N);
+            for (int64_t i = 0; i < N; ++i) {
+                const double sc = eps * l[i];
+                v[i] = make_double4(pm_start[3 * i] * sc, pm_start[3 * i + 1] * sc, pm_start[3 * i + 2] * sc, 0.0);
+            }
+            ck(cudaMemcpy(pm_v, v.data(), N * sizeof(double4), cudaMemcpyHostToDevice), "upload");
+            pm_initialized = true;
+        }
+        const am::NodeDev nd = node_dev();
+        element_forces(0, U4);
+        am::launch_gather_force(nd, 0, slots64, pm_fu, 0, stream);
+        ++launches;
+        double stable_np1 = previous == 0.0 ? 1.0e-16 : previous;
+        constexpr int kWindow = 5;
+        double recent[kWindow] = {0, 0, 0, 0, 0};
+        bool converged = false, oscillating = false;
+        int32_t used = num_iterations;
+        const int64_t nblocks = (N + 255) / 256;
+        std::vector<double> part(static_cast<size_t>(nblocks));
+        for (int32_t k = 0; k < num_iterations; ++k) {
+            const double stable_n = stable_np1;
+            am::launch_pm_perturb(nd, U4, pm_v, pm_l, eps, W4, stream);
+            element_forces(0, W4);
+            am::launch_gather_force(nd, 0, slots64, pm_fe, 0, stream);
+            am::launch_pm_next(nd, pm_fe, pm_fu, pm_l, eps, pm_v, pm_partial, stream);
+            launches += 3;
+            check_launch("power-method kernels");
+            ck(cudaMemcpyAsync(part.data(), pm_partial, nblocks * sizeof(double), cudaMemcpyDeviceToHost, stream), "D2H");
+            ck(cudaStreamSynchronize(stream), "synchronize");
+            double sum = 0.0;
+            for (double x : part) sum += x;
+            const double lambda = std::sqrt(sum);
+            if (!(lambda > 0.0) || !std::isfinite(lambda)) fail(AM_ENAN, "power method: zero or non-finite estimate");
+            am::launch_pm_scale(N, pm_v, 1.0 / lambda, stream);
+            ++launches;
+            stable_np1 = 2.0 / std::sqrt(lambda);
+            recent[k % kWindow] = stable_np1;
+            if (std::abs(stable_np1 - stable_n) < tol * stable_np1) {
+                converged = true;
+                used = k + 1;
+                break;
+            }
+            if (k >= kWindow) {
+                double mean = 0.0;
+                for (double r : recent) mean += r;
+                mean /= kWindow;
+                double var = 0.0;
+                for (double r : recent) var += (r - mean) * (r - mean);
+                var /= (kWindow - 1);
+                if (k > kWindow + 1) {
+                    // The reference's alternation test over the window (its first pass
+                    // always ends the scan, so it never reports an oscillation).
+                    double alt = 0.0;
+                    for (int i = 0; i < kWindow - 1; ++i) {
+                        const double diff = recent[i + 1] - recent[i];
+                        if (i > 0 && diff * alt < 0) {
+                            oscillating = true;
+                        } else {
+                            oscillating = false;
+                            break;
+                        }
+                        alt = diff;
+                    }
+                }
+                if (var < vartol * mean || (oscillating && var < vartol * mean * 2.0)) {
+                    converged = true;
+                    used = k + 1;
+                    break;
+                }
+            }
+        }
+        double result = stable_np1;
+        if (!converged || oscillating) result = *std::min_element(recent, recent + kWindow);
+        if (iterations) *iterations = used;
+        if (converged_out) *converged_out = converged ? 1 : 0;
+        return result;
     }
 
     void vjp(const double4* U, const double4* L, double* gmu, double* gkappa, int accumulate) {
@@ -508,6 +610,11 @@ struct am_ctx {
         dfree(slot_pos);
         dfree(slots64);
         dfree(slots32);
+        dfree(pm_l);
+        dfree(pm_v);
+        dfree(pm_fu);
+        dfree(pm_fe);
+        dfree(pm_partial);
         dfree(iface_nodes);
         dfree(iface_rows);
         dfree(iface_row_of);
@@ -1037,6 +1144,72 @@ int am_solve(am_ctx* ctx, am_precision prec, double dt, double t_end, int64_t ma
         const std::vector<double> dts = am::host::DirectTimeSchedule(dt, t_end, max_steps);
         run_schedule(ctx, prec, dts, 0.0);
         if (steps_done) *steps_done = static_cast<int64_t>(dts.size());
+    });
+}
+
+int am_set_power_method(am_ctx* ctx, const double* start, const double* max_edge_length) {
+    if (!ctx) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        ctx->require_finalized();
+        if (!start || !max_edge_length) fail(AM_EINVAL, "null start vector or edge lengths");
+        for (int64_t i = 0; i < ctx->N; ++i)
+            if (!(max_edge_length[i] > 0.0)) fail(AM_EINVAL, "edge lengths must be positive");
+        ctx->pm_start.assign(start, start + 3 * ctx->N);
+        if (!ctx->pm_l) {
+            ctx->pm_l = dalloc<double>(ctx->N, "edge lengths");
+            ctx->pm_v = dalloc<double4>(ctx->N, "eigenvector");
+            ctx->pm_fu = dalloc<double>(3 * ctx->N, "force");
+            ctx->pm_fe = dalloc<double>(3 * ctx->N, "force");
+            ctx->pm_partial = dalloc<double>((ctx->N + 255) / 256, "partial sums");
+        }
+        ck(cudaMemcpy(ctx->pm_l, max_edge_length, ctx->N * sizeof(double), cudaMemcpyHostToDevice), "upload");
+        ctx->pm_initialized = false;
+    });
+}
+
+int am_stable_time_increment(am_ctx* ctx, double previous, int32_t num_iterations, double epsilon, double tolerance,
+                             double variation_tolerance, double* dt, int32_t* iterations, int32_t* converged) {
+    if (!ctx) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        ctx->require_finalized();
+        ctx->reset_status();
+        const double r = ctx->stable_time_increment(previous, num_iterations, epsilon, tolerance, variation_tolerance,
+                                                    iterations, converged);
+        ctx->check_status();
+        if (dt) *dt = r;
+    });
+}
+
+int am_solve_power_method(am_ctx* ctx, am_precision prec, double scale_factor, int64_t update_interval, double t_end,
+                          int64_t max_steps, int64_t* steps_done, double* last_increment) {
+    if (!ctx) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        ctx->require_finalized();
+        if (!(scale_factor > 0.0) || update_interval < 1 || !std::isfinite(t_end))
+            fail(AM_EINVAL, "scale_factor and update_interval must be positive, t_end finite");
+        ctx->reset_status();
+        ctx->init_acceleration(prec == AM_MIXED);
+        ctx->check_status();
+        // ExplicitSolver::Solve with PowerMethodTimeStepper (include/TimeStepper.h:138-221):
+        // at increments 0, k, 2k, ... the stable increment is recomputed at the current
+        // state (seeded with the previous one) and scaled; the last step ends at t_end.
+        double time = 0.0, inc_dt = 0.0;
+        int64_t n = 0;
+        while (!(time >= t_end) && n < max_steps) {
+            const double full = ctx->stable_time_increment(inc_dt / scale_factor, 50, 1.0e-5, 1.0e-3, 1.0e-7, nullptr,
+                                                           nullptr);
+            inc_dt = full * scale_factor;
+            std::vector<double> dts;
+            const double t_chunk = time;
+            for (int64_t k = 0; k < update_interval && !(time >= t_end) && n < max_steps; ++k, ++n) {
+                const double d = time + inc_dt <= t_end ? inc_dt : (time > t_end ? 0.0 : t_end - time);
+                dts.push_back(d);
+                time += d;
+            }
+            run_schedule(ctx, prec, dts, t_chunk);
+        }
+        if (steps_done) *steps_done = n;
+        if (last_increment) *last_increment = inc_dt;
     });
 }
 

@@ -1218,6 +1218,58 @@ __global__ void __launch_bounds__(256) k_sensor_seed(const double4* __restrict__
     if (threadIdx.x == 0) *loss = part[0];
 }
 
+// ---- power method (stable time increment) ----
+// A dof is prescribed when any boundary condition of the list names its component.
+__device__ __forceinline__ void prescribed(uint32_t w, bool& px, bool& py, bool& pz) {
+    px = (w & 0x3FFu) != 0;
+    py = ((w >> 10) & 0x3FFu) != 0;
+    pz = ((w >> 20) & 0x3FFu) != 0;
+}
+
+__global__ void __launch_bounds__(256) k_pm_perturb(NodeDev nd, const double4* __restrict__ U4,
+                                                    const double4* __restrict__ V4, const double* __restrict__ l,
+                                                    double eps, double4* __restrict__ W4) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nd.num_nodes) return;
+    bool px, py, pz;
+    prescribed(nd.bcword[i], px, py, pz);
+    const double4 u = U4[i], v = V4[i];
+    const double le = l[i] * eps;
+    W4[i] = make_double4(px ? u.x : u.x + v.x * le, py ? u.y : u.y + v.y * le, pz ? u.z : u.z + v.z * le, 0.0);
+}
+
+__global__ void __launch_bounds__(256) k_pm_next(NodeDev nd, const double* __restrict__ fe,
+                                                 const double* __restrict__ fu, const double* __restrict__ l, double eps,
+                                                 double4* __restrict__ V4, double* __restrict__ partial) {
+    __shared__ double sq[256];
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    double acc = 0.0;
+    if (i < nd.num_nodes) {
+        bool px, py, pz;
+        prescribed(nd.bcword[i], px, py, pz);
+        const double d = l[i] * eps * nd.mass[i];
+        const double vx = px ? 0.0 : (fe[3 * i] - fu[3 * i]) / d;
+        const double vy = py ? 0.0 : (fe[3 * i + 1] - fu[3 * i + 1]) / d;
+        const double vz = pz ? 0.0 : (fe[3 * i + 2] - fu[3 * i + 2]) / d;
+        V4[i] = make_double4(vx, vy, vz, 0.0);
+        acc = vx * vx + vy * vy + vz * vz;
+    }
+    sq[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sq[threadIdx.x] += sq[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = sq[0];
+}
+
+__global__ void k_pm_scale(int64_t n, double4* __restrict__ V4, double scale) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double4 v = V4[i];
+    V4[i] = make_double4(v.x * scale, v.y * scale, v.z * scale, 0.0);
+}
+
 __global__ void k_pack4(const double* __restrict__ in, double4* __restrict__ out, int64_t n) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -1536,6 +1588,20 @@ void launch_adj_update(const NodeDev& nd, const double4* slots, const StepParams
 void launch_sensor_seed(const double4* U4, int32_t num_sensors, const int32_t* sensors, double4* UB, double* loss,
                         cudaStream_t s) {
     k_sensor_seed<<<1, 256, 0, s>>>(U4, num_sensors, sensors, UB, loss);
+}
+
+void launch_pm_perturb(const NodeDev& nd, const double4* U4, const double4* V4, const double* l, double eps,
+                       double4* W4, cudaStream_t s) {
+    k_pm_perturb<<<grid_for(nd.num_nodes, 256), 256, 0, s>>>(nd, U4, V4, l, eps, W4);
+}
+int64_t launch_pm_next(const NodeDev& nd, const double* f_eps, const double* f_u, const double* l, double eps,
+                       double4* V4, double* partial, cudaStream_t s) {
+    const unsigned grid = grid_for(nd.num_nodes, 256);
+    k_pm_next<<<grid, 256, 0, s>>>(nd, f_eps, f_u, l, eps, V4, partial);
+    return grid;
+}
+void launch_pm_scale(int64_t n, double4* V4, double scale, cudaStream_t s) {
+    if (n > 0) k_pm_scale<<<grid_for(n, 256), 256, 0, s>>>(n, V4, scale);
 }
 
 void launch_pack4(const double* aos3, double4* out, int64_t n, cudaStream_t s) {

@@ -111,6 +111,15 @@ void launch_adj_prep(const NodeDev& nd, const StepParams* table, int64_t step, c
                      double4* L4, cudaStream_t s);
 void launch_adj_update(const NodeDev& nd, const double4* slots, const StepParams* table, int64_t step, double4* UB,
                        double4* VB, double4* AB, double4* L4, cudaStream_t s);
+// Power method for the stable time increment (PowerMethodProcessor.h:196-330):
+// W = U + V l eps on the free dofs (U on the prescribed ones); then
+// V = (f_eps - f_u) / (l eps m) on the free dofs (0 on the prescribed), with the
+// squares of V summed per block into partial[blockIdx] (fixed order); then V *= s.
+void launch_pm_perturb(const NodeDev& nd, const double4* U4, const double4* V4, const double* l, double eps,
+                       double4* W4, cudaStream_t s);
+int64_t launch_pm_next(const NodeDev& nd, const double* f_eps, const double* f_u, const double* l, double eps,
+                       double4* V4, double* partial, cudaStream_t s);
+void launch_pm_scale(int64_t n, double4* V4, double scale, cudaStream_t s);
 void launch_sensor_seed(const double4* U4, int32_t num_sensors, const int32_t* sensors, double4* UB, double* loss,
                         cudaStream_t s);
 

@@ -22,7 +22,8 @@ library computes, and builds an ExplicitDynamics model on the GPU:
                     linear_elastic | neo_hookean | elastic: {density, two elastic constants}
           initial_conditions: [- velocity: {sets, components: {X, Y, Z} | vector: {magnitude, direction}}]
           loads: [- gravity_load: {sets, components | vector}]
-          time_stepper: {direct_time_stepper: {time_increment, time_end}}
+          time_stepper: {direct_time_stepper: {time_increment, time_end}
+                         | power_method_time_stepper: {scale_factor, update_interval, time_end}}
           boundary_conditions:                      (src/BoundaryCondition.cpp:197-220)
             - displacement | velocity: {sets, components | vector,
                                         time_function: {ramp_function | smooth_step_function:
@@ -38,8 +39,8 @@ side sets named surface_1, surface_2, ... in the order their letters appear (x =
 X = max-x face, ...), and "|tets" splits each hex into six tets (this library's conforming
 split; STK's own split is not available here). An .npz mesh holds `coords` (N x 3),
 `block_<name>` (E x 4 or E x 8, zero-based) and `set_<name>` (zero-based node ids).
-Anything else (Exodus meshes, the power-method time stepper, F-bar, two-pass RKPM, other
-materials) raises InputError naming the key.
+Anything else (Exodus meshes, F-bar, two-pass RKPM, other materials) raises InputError
+naming the key.
 """
 from __future__ import annotations
 
@@ -80,6 +81,7 @@ class Simulation:
     max_steps: int = 1 << 40
     sets: dict = field(default_factory=dict)
     meta: dict = field(default_factory=dict)
+    power_method: tuple | None = None  # (scale_factor, update_interval) of power_method_time_stepper
 
     @property
     def num_nodes(self) -> int:
@@ -97,6 +99,8 @@ class Simulation:
         """The same inputs as a problems.Problem (for the oracle and the benchmark)."""
         from .problems import Problem
 
+        if self.power_method is not None:
+            raise InputError("the power-method time stepper has no precomputed step list")
         nsteps = len(direct_time_steps(self.dt, self.time_end))
         meta = dict(self.meta)
         if self.mass is not None:
@@ -405,29 +409,52 @@ def load(source, base_dir: Path | None = None) -> Simulation:
                                                    float(atr.get("time_end", 1.7976931348623157e308)))))
 
     ts_kind, ts = _one_key(proc.get("time_stepper") or {}, "time_stepper")
-    if ts_kind != "direct_time_stepper":
-        raise InputError(f"time_stepper {ts_kind!r}: the power-method stepper is not built (direct_time_stepper)")
-    dt, t_end = float(ts["time_increment"]), float(ts["time_end"])
-    if not (dt > 0.0 and t_end >= 0.0):
-        raise InputError("direct_time_stepper needs time_increment > 0 and time_end >= 0")
+    power = None
+    if ts_kind == "direct_time_stepper":
+        dt, t_end = float(ts["time_increment"]), float(ts["time_end"])
+        if not (dt > 0.0 and t_end >= 0.0):
+            raise InputError("direct_time_stepper needs time_increment > 0 and time_end >= 0")
+    elif ts_kind == "power_method_time_stepper":
+        dt, t_end = 0.0, float(ts["time_end"])
+        power = (float(ts["scale_factor"]), int(ts["update_interval"]))
+        if not (power[0] > 0.0 and power[1] >= 1 and t_end >= 0.0):
+            raise InputError("power_method_time_stepper needs scale_factor > 0, update_interval >= 1, time_end >= 0")
+    else:
+        raise InputError(f"time_stepper {ts_kind!r} (direct_time_stepper or power_method_time_stepper)")
     precision = str(ext.get("precision", "fp64"))
     if precision not in ("fp64", "mixed"):
         raise InputError(f"x_b200.precision {precision!r} (fp64 or mixed)")
     name = Path(str(source)).stem if isinstance(source, (str, Path)) and "\n" not in str(source) else "input"
+    element_blocks = [blocks[(e.get("part") or {}).get("set")] for e in (geo.get("parts") or [])]
     return Simulation(name, coords, parts, bcs, v0, dt, t_end, precision, body, mass,
-                      int(ext.get("max_steps", 1 << 40)), sets, {"seed": seed, "mesh": mesh_spec})
+                      int(ext.get("max_steps", 1 << 40)), sets,
+                      {"seed": seed, "mesh": mesh_spec, "element_blocks": element_blocks}, power)
+
+
+def power_method_inputs(sim: Simulation):
+    """Start vector (uniform in [-1, 1] per node component, from the x_b200 seed; the
+    reference draws it per node from the node id) and each node's longest edge."""
+    rng = np.random.default_rng([int(sim.meta.get("seed", 0)), 1])
+    return rng.uniform(-1.0, 1.0, size=sim.coords.shape), _mesh.max_edge_length(sim.coords, sim.meta["element_blocks"])
 
 
 def run(source, stream=None) -> dict:
-    """Parse, build the GPU model, and Solve(): the initial acceleration, then the direct
-    time stepper's steps (ExplicitSolver::Solve, src/Solvers/Explicit.cpp:308-483)."""
+    """Parse, build the GPU model, and Solve(): the initial acceleration, then the time
+    stepper's steps (ExplicitSolver::Solve, src/Solvers/Explicit.cpp:308-483); with the
+    power-method stepper the increment is recomputed on the GPU every update_interval steps."""
     sim = source if isinstance(source, Simulation) else load(source)
+    dt = sim.dt
     with sim.model(stream) as m:
         m.set_state(np.zeros_like(sim.coords), sim.v0)
-        m.init_acceleration(sim.precision)
-        steps = m.solve(sim.dt, sim.time_end, sim.precision, sim.max_steps)
+        if sim.power_method is not None:
+            m.set_power_method(*power_method_inputs(sim))
+            steps, dt = m.solve_power_method(sim.power_method[0], sim.power_method[1], sim.time_end, sim.precision,
+                                             sim.max_steps)
+        else:
+            steps = m.solve(sim.dt, sim.time_end, sim.precision, sim.max_steps)
         u, v, a = m.get_state()
-    return {"simulation": sim, "steps": steps, "displacement": u, "velocity": v, "acceleration": a}
+    return {"simulation": sim, "steps": steps, "time_increment": dt, "displacement": u, "velocity": v,
+            "acceleration": a}
 
 
 def main(argv=None) -> int:

@@ -118,3 +118,19 @@ def lumped_mass(coords: np.ndarray, conn: np.ndarray, density: float) -> np.ndar
         vol = hex8_volumes(coords, conn)
     np.add.at(m, conn.ravel(), np.repeat(density * vol / conn.shape[1], conn.shape[1]))
     return m
+
+
+def max_edge_length(coords: np.ndarray, conns) -> np.ndarray:
+    """MaxEdgeLengthFunctor (src/MaxEdgeLengthProcessor.cpp:36-60) with every node active:
+    per node, the longest distance to any node of an element it belongs to (for a hex
+    this includes the face and body diagonals). conns: one connectivity array or a list."""
+    if isinstance(conns, np.ndarray):
+        conns = [conns]
+    out = np.zeros(coords.shape[0])
+    for conn in conns:
+        conn = np.asarray(conn)
+        x = coords[conn]
+        for a in range(conn.shape[1]):
+            d = np.linalg.norm(x - x[:, a:a + 1], axis=2).max(axis=1)
+            np.maximum.at(out, conn[:, a], d)
+    return out

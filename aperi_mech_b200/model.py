@@ -265,6 +265,28 @@ class ExplicitDynamics:
                                   C.byref(loss), capi._ptr(gm), capi._ptr(gk)), self.ctx)
         return loss.value, gm, gk
 
+    # -- power-method time stepper ------------------------------------------------
+    def set_power_method(self, start: np.ndarray, max_edge_length: np.ndarray) -> None:
+        st = np.ascontiguousarray(start, dtype=np.float64).reshape(self.N, 3)
+        le = np.ascontiguousarray(max_edge_length, dtype=np.float64)
+        check(self.lib.am_set_power_method(self.ctx, capi._ptr(st), capi._ptr(le)), self.ctx)
+
+    def stable_time_increment(self, previous: float = 0.0, num_iterations: int = 50, epsilon: float = 1e-5,
+                              tolerance: float = 1e-3, variation_tolerance: float = 1e-7):
+        dt, its, conv = C.c_double(), C.c_int32(), C.c_int32()
+        check(self.lib.am_stable_time_increment(self.ctx, float(previous), int(num_iterations), float(epsilon),
+                                                float(tolerance), float(variation_tolerance), C.byref(dt),
+                                                C.byref(its), C.byref(conv)), self.ctx)
+        return dt.value, its.value, bool(conv.value)
+
+    def solve_power_method(self, scale_factor: float, update_interval: int, t_end: float, precision: str = "fp64",
+                           max_steps: int = 1 << 40):
+        n, last = C.c_int64(), C.c_double()
+        check(self.lib.am_solve_power_method(self.ctx, PRECISIONS[precision], float(scale_factor),
+                                             int(update_interval), float(t_end), int(max_steps), C.byref(n),
+                                             C.byref(last)), self.ctx)
+        return n.value, last.value
+
     # -- domain decomposition -------------------------------------------------
     def set_interface(self, local_nodes: np.ndarray, rows: np.ndarray, num_global: int) -> None:
         """This rank's interface nodes and their rows of the exchange buffer

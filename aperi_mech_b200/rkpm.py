@@ -54,13 +54,9 @@ def thex_max_edge_length(coords: np.ndarray, tets: np.ndarray) -> np.ndarray:
 def tet_max_edge_length(coords: np.ndarray, tets: np.ndarray) -> np.ndarray:
     """MaxEdgeLengthFunctor (src/MaxEdgeLengthProcessor.cpp:36-60) on a tet mesh whose
     nodes are all active: per node, the longest distance to a node of a connected tet."""
-    x = coords[tets]
-    out = np.zeros(coords.shape[0])
-    for a in range(4):
-        for b in range(4):
-            if a != b:
-                np.maximum.at(out, tets[:, a], np.linalg.norm(x[:, a] - x[:, b], axis=1))
-    return out
+    from .mesh import max_edge_length
+
+    return max_edge_length(coords, tets)
 
 
 def nodal_cells(coords: np.ndarray, tets: np.ndarray, material: Material, kernel_radius: np.ndarray,

@@ -234,6 +234,26 @@ int64_t am_launch_count(const am_ctx* ctx);
 int am_profile_enable(am_ctx* ctx, int enable);
 int am_profile_read(am_ctx* ctx, double ms[5], int64_t launches[5]);
 
+/* ---- stable time increment by the power method (PowerMethodProcessor,
+ * include/PowerMethodProcessor.h:87-480, and PowerMethodTimeStepper, TimeStepper.h:138-221) ----
+ * am_set_power_method: the start vector (num_nodes x 3, e.g. uniform in [-1, 1]; the
+ * reference draws it per node from its id) and each node's longest edge to a node of a
+ * connected element (MaxEdgeLengthProcessor). The first increment scales the start
+ * vector by epsilon times the edge length; later ones continue from the last estimate.
+ * am_stable_time_increment: 2 / sqrt(lambda_max(M^-1 K)) at the current displacement,
+ * by power iteration on finite differences of the internal force with the reference's
+ * stopping rules; previous is the last (unscaled) increment, 0 at the start.
+ * am_solve_power_method: Solve() with the power-method time stepper: initial
+ * acceleration, then every update_interval steps the increment is recomputed
+ * (50 iterations, epsilon 1e-5, tolerance 1e-3, variation tolerance 1e-7, the
+ * reference's defaults) and multiplied by scale_factor; the last step ends at t_end.
+ * FP64 increments; not available on a decomposed mesh. */
+int am_set_power_method(am_ctx* ctx, const double* start, const double* max_edge_length);
+int am_stable_time_increment(am_ctx* ctx, double previous, int32_t num_iterations, double epsilon, double tolerance,
+                             double variation_tolerance, double* dt, int32_t* iterations, int32_t* converged);
+int am_solve_power_method(am_ctx* ctx, am_precision prec, double scale_factor, int64_t update_interval, double t_end,
+                          int64_t max_steps, int64_t* steps_done, double* last_increment);
+
 /* ---- domain decomposition (replaces the reference's ParallelSum of the force field
  * after the element loop, src/Solvers/Explicit.cpp:190-193) ----
  * A context holds one rank's slab of elements and every node they touch; nodes held by

@@ -1252,3 +1252,78 @@ extern "C" int ob_rkpm_element_cells(int64_t N, const double* X, int64_t T, cons
     }
     return 0;
 }
+
+// ---------------------------------------------------------------------------
+// Stable time increment by the power method: PowerMethodProcessor::ComputeStableTimeIncrement
+// (include/PowerMethodProcessor.h:331-480) with PerturbDisplacementCoefficients (:222-270),
+// ComputeNextEigenvector (:272-330) and NormalizeField (EntityProcessor.h:676-697).
+// v is the current eigenvector estimate (already scaled by eps*l on the first call, as
+// InitializeEigenvector :196-220 does) and is updated in place. A dof is prescribed when
+// any boundary condition names its component (the essential_boundary field).
+// ---------------------------------------------------------------------------
+extern "C" double ob_stable_time_increment(const ob_problem* p, const double* u, double* v, const double* l,
+                                           double previous, int32_t num_iterations, double eps, double tol,
+                                           double vartol, int32_t* iterations, int32_t* converged_out) {
+    const int64_t N = p->num_nodes;
+    std::vector<char> fixed(3 * N, 0);
+    for (int32_t b = 0; b < p->num_bcs; ++b)
+        for (int64_t k = 0; k < p->bcs[b].num_nodes; ++k)
+            for (int c = 0; c < 3; ++c)
+                if (p->bcs[b].component_mask >> c & 1) fixed[3 * p->bcs[b].nodes[k] + c] = 1;
+    const std::vector<double> m = mass_of(p);
+    std::vector<double> fu(3 * N), fe(3 * N), ue(3 * N);
+    ob_internal_force(p, u, fu.data());
+    double stable_np1 = previous == 0.0 ? 1.0e-16 : previous;
+    const int W = 5;
+    double recent[5] = {0, 0, 0, 0, 0};
+    bool converged = false, oscillating = false;
+    int32_t used = num_iterations;
+    for (int32_t k = 0; k < num_iterations; ++k) {
+        const double stable_n = stable_np1;
+        for (int64_t i = 0; i < 3 * N; ++i) ue[i] = fixed[i] ? u[i] : u[i] + v[i] * l[i / 3] * eps;
+        ob_internal_force(p, ue.data(), fe.data());
+        double sum = 0.0;
+        for (int64_t i = 0; i < 3 * N; ++i) {
+            v[i] = fixed[i] ? 0.0 : (fe[i] - fu[i]) / (l[i / 3] * eps * m[i / 3]);
+            sum += v[i] * v[i];
+        }
+        const double lambda = std::sqrt(sum);
+        for (int64_t i = 0; i < 3 * N; ++i) v[i] /= lambda;
+        stable_np1 = 2.0 / std::sqrt(lambda);
+        recent[k % W] = stable_np1;
+        if (std::abs(stable_np1 - stable_n) < tol * stable_np1) {
+            converged = true;
+            used = k + 1;
+            break;
+        }
+        if (k >= W) {
+            double mean = 0.0, var = 0.0;
+            for (double r : recent) mean += r;
+            mean /= W;
+            for (double r : recent) var += (r - mean) * (r - mean);
+            var /= (W - 1);
+            if (k > W + 1) {
+                double alt = 0.0;
+                for (int i = 0; i < W - 1; ++i) {
+                    const double diff = recent[i + 1] - recent[i];
+                    if (i > 0 && diff * alt < 0) {
+                        oscillating = true;
+                    } else {
+                        oscillating = false;
+                        break;
+                    }
+                    alt = diff;
+                }
+            }
+            if (var < vartol * mean || (oscillating && var < vartol * mean * 2.0)) {
+                converged = true;
+                used = k + 1;
+                break;
+            }
+        }
+    }
+    if (iterations) *iterations = used;
+    if (converged_out) *converged_out = converged ? 1 : 0;
+    if (!converged || oscillating) return *std::min_element(recent, recent + W);
+    return stable_np1;
+}

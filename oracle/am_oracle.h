@@ -136,6 +136,13 @@ int ob_rkpm_element_cells(int64_t num_nodes, const double* coords, int64_t num_t
                           double* values, int64_t* cell_ptr, int32_t* cell_nodes, double* cell_grads,
                           double* cell_volumes, double* mass);
 
+/* Stable time increment by the power method (PowerMethodProcessor.h:331-480) at the
+ * displacement u; v (num_nodes x 3) is the eigenvector estimate, updated in place; l is
+ * each node's longest edge. Returns the increment. */
+double ob_stable_time_increment(const ob_problem* p, const double* u, double* v, const double* l, double previous,
+                                int32_t num_iterations, double eps, double tol, double vartol, int32_t* iterations,
+                                int32_t* converged);
+
 /* ---- threads ---- */
 void ob_set_threads(int n);
 int ob_get_threads(void);

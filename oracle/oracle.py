@@ -77,6 +77,9 @@ def lib() -> C.CDLL:
                                           _dp, _lp, _ip, _dp, _lp, _ip, _dp, _dp, _dp]
         L.ob_rkpm_element_cells.argtypes = [C.c_int64, _dp, C.c_int64, _ip, _dp, C.c_int32, C.c_double, _lp, _lp,
                                             _lp, _ip, _dp, _lp, _ip, _dp, _dp, _dp]
+        L.ob_stable_time_increment.argtypes = [C.POINTER(OProblem), _dp, _dp, _dp, C.c_double, C.c_int32, C.c_double,
+                                               C.c_double, C.c_double, _ip, _ip]
+        L.ob_stable_time_increment.restype = C.c_double
         L.ob_set_threads.argtypes = [C.c_int]
         L.ob_get_threads.restype = C.c_int
         _lib = L
@@ -174,6 +177,17 @@ class OracleProblem:
         n = C.c_int64()
         lib().ob_explicit_solve(C.byref(self.s), dt, t_end, max_steps, _p(u), _p(v), _p(a), C.byref(n))
         return u, v, a, n.value
+
+    def stable_time_increment(self, u, v, max_edge_length, previous=0.0, num_iterations=50, epsilon=1e-5,
+                              tolerance=1e-3, variation_tolerance=1e-7):
+        """Returns (dt, iterations, converged); v (the eigenvector estimate) is updated in place."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        assert v.flags.c_contiguous and v.dtype == np.float64
+        le = np.ascontiguousarray(max_edge_length, dtype=np.float64)
+        its, conv = C.c_int32(), C.c_int32()
+        dt = lib().ob_stable_time_increment(C.byref(self.s), _p(u), _p(v), _p(le), previous, num_iterations, epsilon,
+                                            tolerance, variation_tolerance, C.byref(its), C.byref(conv))
+        return dt, its.value, bool(conv.value)
 
     def vjp_force(self, u, lam):
         u = np.ascontiguousarray(u, dtype=np.float64)

@@ -142,8 +142,9 @@ def test_components_vector_initial_conditions_and_extensions():
 
 
 @pytest.mark.parametrize("text, msg", [
-    (nh_yaml(stepper="power_method_time_stepper: {scale_factor: 0.1, update_interval: 10, time_end: 1.0}"),
-     "power-method"),
+    (nh_yaml(stepper="implicit_time_stepper: {time_end: 1.0}"), "time_stepper"),
+    (nh_yaml(stepper="power_method_time_stepper: {scale_factor: 0.0, update_interval: 10, time_end: 1.0}"),
+     "scale_factor"),
     (nh_yaml().replace("generated:3x3x3|sideset:z|tets|bbox:0,0,0,1,1,1", "../mesh/tet.e"), "Exodus"),
     (nh_yaml().replace("sets: [surface_1]", "sets: [nodeset_9]"), "unknown set"),
     (nh_yaml().replace("neo_hookean: {density: 1000.0,", "neo_hookean: {"), "density"),
@@ -206,3 +207,23 @@ def test_yaml_rkpm_cells_run_matches_oracle(oracle_lib, cell):
     u, v, a, n = prob.solve(np.zeros_like(sim.coords), sim.v0, sim.dt, sim.time_end)
     assert r["steps"] == n
     assert np.linalg.norm(r["displacement"] - u) <= 1e-12 * np.linalg.norm(u)
+
+
+@pytest.mark.gpu
+def test_yaml_power_method_stepper_matches_direct_api(gpu):
+    """power_method_time_stepper from YAML equals the same run driven through the model API."""
+    from aperi_mech_b200.model import ExplicitDynamics
+
+    sim = inp.load(nh_yaml(n=4, stepper="power_method_time_stepper: {scale_factor: 0.4, update_interval: 5, "
+                                        "time_end: 2.0e-6}"))
+    assert sim.power_method == (0.4, 5)
+    r = inp.run(sim)
+    assert r["steps"] > 0 and r["time_increment"] > 0
+    with ExplicitDynamics(sim.coords, sim.parts, sim.bcs) as m:
+        m.set_power_method(*inp.power_method_inputs(sim))
+        m.set_state(None, sim.v0)
+        steps, dt = m.solve_power_method(0.4, 5, 2.0e-6)
+        u = m.get_state()[0]
+    assert steps == r["steps"] and dt == r["time_increment"]
+    assert np.array_equal(u, r["displacement"])
+
