@@ -11,6 +11,7 @@
 #include <cstring>
 #include <memory>
 #include <stdexcept>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -285,6 +286,16 @@ struct am_ctx {
     double* pm_fe = nullptr;          // N x 3: F(u + v l eps)
     double* pm_partial = nullptr;     // per-block sums of squares
     bool pm_initialized = false;
+    // Two-pass reproducing-kernel coupling (am_set_rk_functions).
+    int64_t* rk_ptr = nullptr;        // N + 1: rows of Psi
+    int32_t* rk_nbr = nullptr;
+    double* rk_val = nullptr;
+    int64_t* rkt_ptr = nullptr;       // N + 1: columns of Psi (transposed CSR)
+    int32_t* rkt_src = nullptr;
+    double* rkt_val = nullptr;
+    double4* rk_u = nullptr;          // physical displacement Psi U
+    double* rk_f_local = nullptr;     // N x 3: element forces at the nodes
+    double* rk_f = nullptr;           // N x 3: generalized force Psi^T f_local
     std::vector<cudaEvent_t> events;
     std::vector<std::pair<int, int64_t>> mark_slot;
     size_t n_marks = 0;
@@ -305,6 +316,7 @@ struct am_ctx {
             nd.iface_row = iface_row_of;
             nd.iface_f = iface_buf;
         }
+        nd.f_given = rk_f;
         return nd;
     }
 
@@ -326,9 +338,17 @@ struct am_ctx {
         ck(cudaGetLastError(), what);
     }
 
-    // Element/cell force kernels of every block into the slot buffer.
+    // Element/cell force kernels of every block into the slot buffer. With the two-pass
+    // coupling (ExplicitSolver::ComputeForce, src/Solvers/Explicit.cpp:146-186) the blocks
+    // see the physical displacement Psi U, their forces are gathered per node and scattered
+    // to the generalized force Psi^T f, which the node kernels then read (f_given).
     void element_forces(int mixed, const double4* U) {
         void* s = slots(mixed);
+        if (rk_ptr) {
+            am::launch_rk_rows4(N, rk_ptr, rk_nbr, rk_val, U, rk_u, stream);
+            ++launches;
+            U = rk_u;
+        }
         for (const auto& b : blocks) {
             if (b.kind == AM_SMOOTHED_CELLS) {
                 if (mixed && !b.grads32) fail(AM_ESTATE, "mixed precision needs FP32 cell gradients");
@@ -337,6 +357,13 @@ struct am_ctx {
                 am::launch_gauss_force(b.gauss(), mixed, X4, U, s, status, stream);
             }
             ++launches;
+        }
+        if (rk_ptr) {
+            am::NodeDev nd = node_dev();
+            nd.f_given = nullptr;
+            am::launch_gather_force(nd, mixed, s, rk_f_local, 0, stream);
+            am::launch_rk_cols3(N, rkt_ptr, rkt_src, rkt_val, rk_f_local, rk_f, stream);
+            launches += 2;
         }
         check_launch("element force kernel");
     }
@@ -615,6 +642,15 @@ struct am_ctx {
         dfree(pm_fu);
         dfree(pm_fe);
         dfree(pm_partial);
+        dfree(rk_ptr);
+        dfree(rk_nbr);
+        dfree(rk_val);
+        dfree(rkt_ptr);
+        dfree(rkt_src);
+        dfree(rkt_val);
+        dfree(rk_u);
+        dfree(rk_f_local);
+        dfree(rk_f);
         dfree(iface_nodes);
         dfree(iface_rows);
         dfree(iface_row_of);
@@ -1219,6 +1255,7 @@ int am_vjp_force(am_ctx* ctx, am_memory where, const double* u, const double* la
     return guarded(ctx, [&] {
         ctx->require_finalized();
         if (ctx->iface_row_of) fail(AM_ESTATE, "the VJP is not available on a decomposed mesh");
+        if (ctx->rk_ptr) fail(AM_ESTATE, "the VJP is not available with the two-pass coupling");
         if (!u || !lam || !gu) fail(AM_EINVAL, "null u, lam or gu");
         load_nodal(ctx, where, u, ctx->W4);
         load_nodal(ctx, where, lam, ctx->L4);
@@ -1255,6 +1292,7 @@ int am_adjoint(am_ctx* ctx, int64_t nsteps, double dt, int32_t ckpt_every, int32
     return guarded(ctx, [&] {
         ctx->require_finalized();
         if (ctx->iface_row_of) fail(AM_ESTATE, "the adjoint is not available on a decomposed mesh");
+        if (ctx->rk_ptr) fail(AM_ESTATE, "the adjoint is not available with the two-pass coupling");
         if (nsteps <= 0 || !(dt > 0.0)) fail(AM_EINVAL, "nsteps and dt must be positive");
         if (ckpt_every <= 0) fail(AM_EINVAL, "ckpt_every must be positive");
         if (num_sensors < 0 || (num_sensors > 0 && !sensors)) fail(AM_EINVAL, "bad sensor list");
@@ -1468,6 +1506,7 @@ int am_set_interface(am_ctx* ctx, int64_t num_local, const int32_t* local_nodes,
         if (!ctx->mass_from_caller)
             fail(AM_ESTATE, "a decomposed mesh needs the global lumped mass from am_set_mass before am_finalize");
         if (ctx->iface_row_of) fail(AM_ESTATE, "interface already set");
+        if (ctx->rk_ptr) fail(AM_ESTATE, "a decomposed mesh with the two-pass coupling is not built");
         if (num_local < 0 || num_global < num_local || (num_local > 0 && (!local_nodes || !rows)))
             fail(AM_EINVAL, "bad interface arrays");
         if (num_global >= (int64_t(1) << 31)) fail(AM_ERANGE, "interface beyond int32 indexing");
@@ -1491,6 +1530,61 @@ int am_set_interface(am_ctx* ctx, int64_t num_local, const int32_t* local_nodes,
             ck(cudaMemcpy(ctx->iface_nodes, local_nodes, num_local * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
             ck(cudaMemcpy(ctx->iface_rows, rows, num_local * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
         }
+    });
+}
+
+int am_set_rk_functions(am_ctx* ctx, const int64_t* nbr_ptr, const int32_t* nbr, const double* values) {
+    if (!ctx) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        ctx->require_finalized();
+        if (ctx->rk_ptr) fail(AM_ESTATE, "reproducing-kernel functions already set");
+        if (ctx->iface_row_of) fail(AM_ESTATE, "a decomposed mesh with the two-pass coupling is not built");
+        if (!ctx->mass_from_caller)
+            fail(AM_ESTATE, "the two-pass coupling needs the generalized lumped mass from am_set_mass before am_finalize");
+        if (!nbr_ptr) fail(AM_EINVAL, "null neighbour offsets");
+        const int64_t N = ctx->N, K = nbr_ptr[N];
+        if (nbr_ptr[0] != 0 || K < 0 || (K > 0 && (!nbr || !values))) fail(AM_EINVAL, "bad neighbour arrays");
+        for (int64_t i = 0; i < N; ++i)
+            if (nbr_ptr[i + 1] < nbr_ptr[i]) fail(AM_EINVAL, "neighbour offsets must not decrease");
+        for (int64_t k = 0; k < K; ++k)
+            if (nbr[k] < 0 || nbr[k] >= N) fail(AM_EINVAL, "neighbour out of range");
+        // Transposed functions: column j lists (i, psi_j(x_i)) for ascending i; a row
+        // without neighbours contributes a unit entry to its own column.
+        std::vector<int64_t> tptr(N + 1, 0);
+        for (int64_t i = 0; i < N; ++i) {
+            if (nbr_ptr[i] == nbr_ptr[i + 1]) ++tptr[i + 1];
+            for (int64_t k = nbr_ptr[i]; k < nbr_ptr[i + 1]; ++k) ++tptr[nbr[k] + 1];
+        }
+        for (int64_t j = 0; j < N; ++j) tptr[j + 1] += tptr[j];
+        const int64_t T = tptr[N];
+        if (T >= (int64_t(1) << 31)) fail(AM_ERANGE, "functions beyond int32 indexing");
+        std::vector<int32_t> tsrc(static_cast<size_t>(T));
+        std::vector<double> tval(static_cast<size_t>(T));
+        std::vector<int64_t> fill(tptr.begin(), tptr.end() - 1);
+        for (int64_t i = 0; i < N; ++i) {
+            if (nbr_ptr[i] == nbr_ptr[i + 1]) {
+                tsrc[fill[i]] = static_cast<int32_t>(i);
+                tval[fill[i]++] = 1.0;
+            }
+            for (int64_t k = nbr_ptr[i]; k < nbr_ptr[i + 1]; ++k) {
+                tsrc[fill[nbr[k]]] = static_cast<int32_t>(i);
+                tval[fill[nbr[k]]++] = values[k];
+            }
+        }
+        auto up = [&](auto*& dst, const auto* src, int64_t n, const char* what) {
+            using T0 = std::remove_reference_t<decltype(*dst)>;
+            dst = dalloc<T0>(static_cast<size_t>(std::max<int64_t>(n, 1)), what);
+            if (n > 0) ck(cudaMemcpy(dst, src, n * sizeof(T0), cudaMemcpyHostToDevice), "upload");
+        };
+        up(ctx->rk_ptr, nbr_ptr, N + 1, "function offsets");
+        up(ctx->rk_nbr, nbr, K, "function neighbours");
+        up(ctx->rk_val, values, K, "function values");
+        up(ctx->rkt_ptr, tptr.data(), N + 1, "transposed offsets");
+        up(ctx->rkt_src, tsrc.data(), T, "transposed sources");
+        up(ctx->rkt_val, tval.data(), T, "transposed values");
+        ctx->rk_u = dalloc<double4>(N, "physical displacement");
+        ctx->rk_f_local = dalloc<double>(3 * N, "local force");
+        ctx->rk_f = dalloc<double>(3 * N, "generalized force");
     });
 }
 

@@ -957,7 +957,14 @@ __device__ __forceinline__ void gather(const NodeDev& nd, const vec4_t<S>* __res
     const int r = LPN == 1 ? 0 : static_cast<int>(threadIdx.x % LPN);
     fx = fy = fz = 0.0;
     const int32_t row = (own && nd.iface_row != nullptr) ? nd.iface_row[i] : -1;
-    if (row >= 0) {
+    if (own && nd.f_given != nullptr) {
+        // Two-pass coupling: the node's generalized force, already summed.
+        if (r == 0) {
+            fx = nd.f_given[3 * i];
+            fy = nd.f_given[3 * i + 1];
+            fz = nd.f_given[3 * i + 2];
+        }
+    } else if (row >= 0) {
         // Interface node: the summed force of all ranks (one lane contributes it).
         if (r == 0) {
             fx = nd.iface_f[3 * static_cast<int64_t>(row)];
@@ -1268,6 +1275,72 @@ __global__ void k_pm_scale(int64_t n, double4* __restrict__ V4, double scale) {
     if (i >= n) return;
     double4 v = V4[i];
     V4[i] = make_double4(v.x * scale, v.y * scale, v.z * scale, 0.0);
+}
+
+// Two-pass coupling. kRkLanes lanes share a row (or column): lane r takes every
+// kRkLanes-th entry, so the group reads the row's contiguous entries together, and the
+// partial sums combine by a fixed butterfly (a fixed order for every run).
+constexpr int kRkLanes = 8;
+
+__device__ __forceinline__ void rk_combine(double& x, double& y, double& z) {
+#pragma unroll
+    for (int off = kRkLanes / 2; off > 0; off >>= 1) {
+        x += __shfl_xor_sync(kFull, x, off);
+        y += __shfl_xor_sync(kFull, y, off);
+        z += __shfl_xor_sync(kFull, z, off);
+    }
+}
+
+// Physical displacement P = Psi U (ComputeValues: neighbours taken from the last; a
+// row without neighbours copies the coefficient).
+__global__ void __launch_bounds__(128) k_rk_rows4(int64_t n, const int64_t* __restrict__ ptr,
+                                                 const int32_t* __restrict__ nbr, const double* __restrict__ val,
+                                                 const double4* __restrict__ U4, double4* __restrict__ P4) {
+    const int64_t i = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / kRkLanes;
+    const int r = static_cast<int>(threadIdx.x % kRkLanes);
+    const bool own = i < n;
+    double x = 0.0, y = 0.0, z = 0.0;
+    int64_t b = 0, e = 0;
+    if (own) {
+        b = ptr[i];
+        e = ptr[i + 1];
+        for (int64_t k = e - 1 - r; k >= b; k -= kRkLanes) {
+            const double4 u = U4[nbr[k]];
+            const double w = val[k];
+            x += w * u.x;
+            y += w * u.y;
+            z += w * u.z;
+        }
+    }
+    rk_combine(x, y, z);
+    if (!own || r != 0) return;
+    P4[i] = b == e ? U4[i] : make_double4(x, y, z, 0.0);
+}
+
+// Generalized force f = Psi^T f_local (ScatterValues as a gather over the transposed
+// functions, no atomics).
+__global__ void __launch_bounds__(128) k_rk_cols3(int64_t n, const int64_t* __restrict__ tptr,
+                                                 const int32_t* __restrict__ tsrc, const double* __restrict__ tval,
+                                                 const double* __restrict__ fl, double* __restrict__ f) {
+    const int64_t j = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / kRkLanes;
+    const int r = static_cast<int>(threadIdx.x % kRkLanes);
+    const bool own = j < n;
+    double x = 0.0, y = 0.0, z = 0.0;
+    if (own) {
+        const int64_t e = tptr[j + 1];
+        for (int64_t k = tptr[j] + r; k < e; k += kRkLanes) {
+            const int64_t i = tsrc[k];
+            const double w = tval[k];
+            x += w * fl[3 * i];
+            y += w * fl[3 * i + 1];
+            z += w * fl[3 * i + 2];
+        }
+    }
+    rk_combine(x, y, z);
+    if (!own || r != 0) return;
+    f[3 * j] = x;
+    f[3 * j + 1] = y;
+    f[3 * j + 2] = z;
 }
 
 __global__ void k_pack4(const double* __restrict__ in, double4* __restrict__ out, int64_t n) {
@@ -1602,6 +1675,15 @@ int64_t launch_pm_next(const NodeDev& nd, const double* f_eps, const double* f_u
 }
 void launch_pm_scale(int64_t n, double4* V4, double scale, cudaStream_t s) {
     if (n > 0) k_pm_scale<<<grid_for(n, 256), 256, 0, s>>>(n, V4, scale);
+}
+
+void launch_rk_rows4(int64_t n, const int64_t* ptr, const int32_t* nbr, const double* val, const double4* U4,
+                     double4* P4, cudaStream_t s) {
+    if (n > 0) k_rk_rows4<<<grid_for(n * kRkLanes, 128), 128, 0, s>>>(n, ptr, nbr, val, U4, P4);
+}
+void launch_rk_cols3(int64_t n, const int64_t* tptr, const int32_t* tsrc, const double* tval, const double* f_local,
+                     double* f, cudaStream_t s) {
+    if (n > 0) k_rk_cols3<<<grid_for(n * kRkLanes, 128), 128, 0, s>>>(n, tptr, tsrc, tval, f_local, f);
 }
 
 void launch_pack4(const double* aos3, double4* out, int64_t n, cudaStream_t s) {

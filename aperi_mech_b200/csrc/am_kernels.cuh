@@ -78,6 +78,9 @@ struct NodeDev {
     // buffer (row iface_row[i], FP64 x 3) instead of their own slots.
     const int32_t* iface_row;   // per node: row in iface_f, or -1; null when not decomposed
     const double* iface_f;
+    // Two-pass reproducing-kernel coupling: every node takes its force from this FP64
+    // x 3 array (the scattered generalized force) instead of its slots; null otherwise.
+    const double* f_given;
 };
 
 // ---- launchers (am_kernels.cu) ----
@@ -120,6 +123,14 @@ void launch_pm_perturb(const NodeDev& nd, const double4* U4, const double4* V4, 
 int64_t launch_pm_next(const NodeDev& nd, const double* f_eps, const double* f_u, const double* l, double eps,
                        double4* V4, double* partial, cudaStream_t s);
 void launch_pm_scale(int64_t n, double4* V4, double scale, cudaStream_t s);
+// Two-pass reproducing-kernel coupling (FunctionEvaluationProcessor): Psi in CSR rows
+// (row i: psi_j(x_i) for the neighbours j of node i). rows4: P = Psi U, a row without
+// neighbours copying U[i]; cols3: f = Psi^T f_local from the transposed CSR (column j:
+// the rows i that hold j, ascending i, with a unit entry for each empty row).
+void launch_rk_rows4(int64_t n, const int64_t* ptr, const int32_t* nbr, const double* val, const double4* U4,
+                     double4* P4, cudaStream_t s);
+void launch_rk_cols3(int64_t n, const int64_t* tptr, const int32_t* tsrc, const double* tval, const double* f_local,
+                     double* f, cudaStream_t s);
 void launch_sensor_seed(const double4* U4, int32_t num_sensors, const int32_t* sensors, double4* UB, double* loss,
                         cudaStream_t s);
 

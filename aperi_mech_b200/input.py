@@ -15,7 +15,7 @@ library computes, and builds an ExplicitDynamics model on the GPU:
                     integration_scheme:
                       gauss_quadrature: {integration_order: 1}
                       | strain_smoothing: {element_smoothing_cell | nodal_smoothing_cell: {subdomains: 1},
-                                           force_one_pass_method: true}
+                                           force_one_pass_method | force_two_pass_method: true}
                     approximation_space:
                       finite_element: ~ | reproducing_kernel: {kernel_radius_scale_factor: s}
                   material:                         (Materials/Factory.h:19-160)
@@ -39,8 +39,10 @@ side sets named surface_1, surface_2, ... in the order their letters appear (x =
 X = max-x face, ...), and "|tets" splits each hex into six tets (this library's conforming
 split; STK's own split is not available here). An .npz mesh holds `coords` (N x 3),
 `block_<name>` (E x 4 or E x 8, zero-based) and `set_<name>` (zero-based node ids).
-Anything else (Exodus meshes, F-bar, two-pass RKPM, other materials) raises InputError
-naming the key.
+Element cells with the reproducing_kernel space use the two-pass method unless
+force_one_pass_method is set, nodal cells the one-pass method (the reference's defaults).
+Anything else (Exodus meshes, F-bar, two-pass nodal cells, other materials) raises
+InputError naming the key.
 """
 from __future__ import annotations
 
@@ -82,6 +84,7 @@ class Simulation:
     sets: dict = field(default_factory=dict)
     meta: dict = field(default_factory=dict)
     power_method: tuple | None = None  # (scale_factor, update_interval) of power_method_time_stepper
+    rk: tuple | None = None  # (nbr_ptr, nbr, values): two-pass reproducing-kernel coupling
 
     @property
     def num_nodes(self) -> int:
@@ -93,7 +96,7 @@ class Simulation:
 
     def model(self, stream=None) -> ExplicitDynamics:
         return ExplicitDynamics(self.coords, self.parts, self.bcs, body_accel=self.body_accel, mass=self.mass,
-                                stream=stream)
+                                stream=stream, rk=self.rk)
 
     def problem(self):
         """The same inputs as a problems.Problem (for the oracle and the benchmark)."""
@@ -107,6 +110,8 @@ class Simulation:
             meta["mass"] = self.mass
         if self.body_accel is not None:
             meta["body_accel"] = self.body_accel
+        if self.rk is not None:
+            meta["rk"] = self.rk
         return Problem(self.name, self.coords, self.parts, self.bcs, self.v0, self.dt, nsteps,
                        int(self.meta.get("seed", 0)), meta)
 
@@ -236,7 +241,8 @@ def _material(node: dict) -> Material:
 
 
 def _part(pnode: dict, blocks: dict, coords, ext: dict, rng):
-    """One InternalForceContribution: block connectivity + formulation + material."""
+    """One InternalForceContribution: block connectivity + formulation + material.
+    Returns (part, lumped mass or None, two-pass functions or None)."""
     name = pnode.get("set")
     if name not in blocks:
         raise InputError(f"part set {name!r} is not a block of the mesh (blocks: {sorted(blocks)})")
@@ -266,14 +272,18 @@ def _part(pnode: dict, blocks: dict, coords, ext: dict, rng):
         kind = {4: "tet4", 8: "hex8"}.get(conn.shape[1])
         if kind is None:
             raise InputError(f"block {name}: {conn.shape[1]}-node elements (Tet4 or Hex8 only)")
-        return Part(kind, mat, conn=conn, mu_field=mu_f, kappa_field=kappa_f, name=name), None
+        return Part(kind, mat, conn=conn, mu_field=mu_f, kappa_field=kappa_f, name=name), None, None
     if scheme != "strain_smoothing":
         raise InputError(f"integration_scheme {scheme!r} (gauss_quadrature or strain_smoothing)")
     snode = snode or {}
     if snode.get("use_f_bar"):
         raise InputError("use_f_bar: the F-bar smoothed cells are not built yet")
-    if snode.get("force_two_pass_method"):
-        raise InputError("force_two_pass_method: two-pass RKPM is not built yet")
+    # IntegrationSchemeStrainSmoothingParameters (InternalForceContributionParameters.h:164-194):
+    # one-pass by default, two-pass for element cells, either forced by a key.
+    force_one, force_two = bool(snode.get("force_one_pass_method")), bool(snode.get("force_two_pass_method"))
+    if force_one and force_two:
+        raise InputError("Cannot force both one pass and two pass methods")
+    one_pass = force_one or (not force_two and "element_smoothing_cell" not in snode)
     if conn.shape[1] != 4:
         raise InputError(f"strain_smoothing on block {name}: Tet4 meshes only")
     cell = "nodal_smoothing_cell" if "nodal_smoothing_cell" in snode else "element_smoothing_cell"
@@ -285,8 +295,10 @@ def _part(pnode: dict, blocks: dict, coords, ext: dict, rng):
 
         part, mass = element_smoothing_part(coords, conn, mat, mu_field=mu_f, kappa_field=kappa_f)
         part.name = name
-        return part, mass
+        return part, mass, None
     if space == "reproducing_kernel" and cell == "nodal_smoothing_cell":
+        if not one_pass:
+            raise InputError("force_two_pass_method on nodal_smoothing_cell: two-pass nodal cells are not built")
         if mu_f is not None or kappa_f is not None:
             raise InputError("x_b200.fields on RKPM nodal cells: per-cell fields are not supported")
         from .rkpm import nodal_cells, thex_max_edge_length
@@ -295,7 +307,15 @@ def _part(pnode: dict, blocks: dict, coords, ext: dict, rng):
         cells = nodal_cells(coords, conn, mat, scale * thex_max_edge_length(coords, conn),
                             max_neighbors=int(ext.get("max_neighbors", 40)))
         cells.part.name = name
-        return cells.part, cells.mass
+        return cells.part, cells.mass, None
+    if space == "reproducing_kernel" and cell == "element_smoothing_cell" and not one_pass:
+        from .rkpm import tet_max_edge_length, two_pass_element_cells
+
+        scale = float((spnode or {}).get("kernel_radius_scale_factor", 1.0))
+        cells = two_pass_element_cells(coords, conn, mat, scale * tet_max_edge_length(coords, conn),
+                                       max_neighbors=int(ext.get("max_neighbors", 40)), mu_field=mu_f,
+                                       kappa_field=kappa_f, name=name)
+        return cells.part, cells.mass, cells.functions()
     if space == "reproducing_kernel" and cell == "element_smoothing_cell":
         if mu_f is not None or kappa_f is not None:
             raise InputError("x_b200.fields on RKPM element cells: per-cell fields are not supported")
@@ -305,7 +325,7 @@ def _part(pnode: dict, blocks: dict, coords, ext: dict, rng):
         cells = element_cells(coords, conn, mat, scale * tet_max_edge_length(coords, conn),
                               max_neighbors=int(ext.get("max_neighbors", 40)))
         cells.part.name = name
-        return cells.part, cells.mass
+        return cells.part, cells.mass, None
     raise InputError(f"{space} with {cell}: not built")
 
 
@@ -347,14 +367,20 @@ def load(source, base_dir: Path | None = None) -> Simulation:
     for b, conn in blocks.items():
         sets.setdefault(b, np.unique(conn).astype(np.int32))
 
-    parts, masses = [], []
+    parts, masses, rk = [], [], None
     for entry in geo.get("parts") or []:
         _, pnode = _one_key(entry, "parts entry")
-        part, mass = _part(pnode, blocks, coords, ext, rng)
+        part, mass, functions = _part(pnode, blocks, coords, ext, rng)
         parts.append(part)
         masses.append(mass)
+        if functions is not None:
+            if rk is not None:
+                raise InputError("two-pass reproducing-kernel coupling on more than one part is not built")
+            rk = functions
     if not parts:
         raise InputError("geometry.parts is empty")
+    if rk is not None and len(parts) > 1:
+        raise InputError("two-pass reproducing-kernel parts beside other parts are not built")
     mass = None
     if any(m is not None for m in masses):
         mass = np.zeros(coords.shape[0])
@@ -428,7 +454,7 @@ def load(source, base_dir: Path | None = None) -> Simulation:
     element_blocks = [blocks[(e.get("part") or {}).get("set")] for e in (geo.get("parts") or [])]
     return Simulation(name, coords, parts, bcs, v0, dt, t_end, precision, body, mass,
                       int(ext.get("max_steps", 1 << 40)), sets,
-                      {"seed": seed, "mesh": mesh_spec, "element_blocks": element_blocks}, power)
+                      {"seed": seed, "mesh": mesh_spec, "element_blocks": element_blocks}, power, rk)
 
 
 def power_method_inputs(sim: Simulation):
@@ -453,8 +479,14 @@ def run(source, stream=None) -> dict:
         else:
             steps = m.solve(sim.dt, sim.time_end, sim.precision, sim.max_steps)
         u, v, a = m.get_state()
-    return {"simulation": sim, "steps": steps, "time_increment": dt, "displacement": u, "velocity": v,
-            "acceleration": a}
+    out = {"simulation": sim, "steps": steps, "time_increment": dt, "displacement": u, "velocity": v,
+           "acceleration": a}
+    if sim.rk is not None:
+        # The state holds generalized coefficients; the physical displacement is Psi u.
+        from .rkpm import apply_functions
+
+        out["physical_displacement"] = apply_functions(sim.rk, u)
+    return out
 
 
 def main(argv=None) -> int:

@@ -108,7 +108,9 @@ class ExplicitDynamics:
     """Device-resident explicit-dynamics model (one am_ctx)."""
 
     def __init__(self, coords: np.ndarray, parts: list[Part], bcs: list[BoundaryCondition] = (),
-                 body_accel=None, mass: np.ndarray | None = None, stream=None):
+                 body_accel=None, mass: np.ndarray | None = None, stream=None, rk=None):
+        """rk = (nbr_ptr, nbr, values) sets the two-pass reproducing-kernel coupling
+        (set_rk_functions); mass is then the generalized lumped mass."""
         self.lib = capi.load()
         self.coords = np.ascontiguousarray(coords, dtype=np.float64)
         self.N = int(self.coords.shape[0])
@@ -131,6 +133,8 @@ class ExplicitDynamics:
                 m = np.ascontiguousarray(mass, dtype=np.float64)
                 check(self.lib.am_set_mass(self.ctx, m.ctypes.data_as(C.POINTER(C.c_double))), self.ctx)
             check(self.lib.am_finalize(self.ctx), self.ctx)
+            if rk is not None:
+                self.set_rk_functions(*rk)
         except Exception:
             self.close()
             raise
@@ -295,6 +299,19 @@ class ExplicitDynamics:
         rw = np.ascontiguousarray(rows, dtype=np.int32)
         check(self.lib.am_set_interface(self.ctx, ln.size, capi._ptr(ln, C.c_int32), capi._ptr(rw, C.c_int32),
                                         int(num_global)), self.ctx)
+
+    def set_rk_functions(self, nbr_ptr: np.ndarray, nbr: np.ndarray, values: np.ndarray) -> None:
+        """Two-pass reproducing-kernel coupling: the state holds generalized coefficients,
+        the blocks run on the physical displacement Psi u and their forces reach the
+        coefficients as Psi^T f. Row i of Psi: values[nbr_ptr[i]:nbr_ptr[i+1]] at the
+        neighbours nbr[...] of node i (rkpm.RKPMCells.functions())."""
+        ptr = np.ascontiguousarray(nbr_ptr, dtype=np.int64)
+        nb = np.ascontiguousarray(nbr, dtype=np.int32)
+        val = np.ascontiguousarray(values, dtype=np.float64)
+        if ptr.size != self.N + 1 or nb.size != val.size or nb.size != ptr[-1]:
+            raise ValueError("nbr_ptr needs num_nodes + 1 offsets and nbr/values nbr_ptr[-1] entries")
+        check(self.lib.am_set_rk_functions(self.ctx, capi._ptr(ptr, C.c_int64), capi._ptr(nb, C.c_int32),
+                                           capi._ptr(val)), self.ctx)
 
     def set_nccl(self, unique_id: bytes, rank: int, nranks: int) -> None:
         check(self.lib.am_set_nccl(self.ctx, unique_id, int(rank), int(nranks)), self.ctx)

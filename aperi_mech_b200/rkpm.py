@@ -1,9 +1,11 @@
-"""RKPM one-pass smoothing cells (ElementReproducingKernel, include/ElementReproducingKernel.h)
+"""RKPM smoothing cells (ElementReproducingKernel, include/ElementReproducingKernel.h)
 built by the library's set-up: neighbour search, FP64 reproducing-kernel functions on
 the GPU, one-pass smoothed gradients, lumped mass scattered through the functions.
 Nodal cells (nodal_smoothing_cell) live on the tet-corner hexes of the thex refinement
 (am_rkpm_nodal_cells); element cells (element_smoothing_cell) are the tets themselves
-(am_rkpm_element_cells)."""
+(am_rkpm_element_cells). The two-pass method on element cells keeps the tets' own
+smoothed FEM gradients and couples them to the coefficients through the functions at
+the vertices (two_pass_element_cells, ExplicitDynamics.set_rk_functions)."""
 from __future__ import annotations
 
 import ctypes as C
@@ -28,6 +30,15 @@ class RKPMCells:
     @property
     def entries_per_cell(self) -> float:
         return float(self.part.cell_ptr[-1]) / (len(self.part.cell_ptr) - 1)
+
+    def functions(self):
+        """(nbr_ptr, nbr, values) of the functions at the mesh nodes, for the two-pass
+        coupling (element cells: the points are the vertices)."""
+        if self.nbr_ptr is None:
+            raise ValueError("built without keep_points")
+        if self.points is not None and self.points.shape[0] != self.mass.shape[0]:
+            raise ValueError("the functions live on refinement points, not on the mesh nodes")
+        return self.nbr_ptr, self.nbr, self.values
 
 
 def thex_max_edge_length(coords: np.ndarray, tets: np.ndarray) -> np.ndarray:
@@ -73,6 +84,33 @@ def element_cells(coords: np.ndarray, tets: np.ndarray, material: Material, kern
     """One cell per tet (element_smoothing_cell with the reproducing_kernel space)."""
     return _cells("am_rkpm_element_cells", coords, tets, material, kernel_radius, max_neighbors, keep_points,
                   mu_field, kappa_field, name)
+
+
+def two_pass_element_cells(coords: np.ndarray, tets: np.ndarray, material: Material, kernel_radius: np.ndarray,
+                           max_neighbors: int = 40, mu_field=None, kappa_field=None, name: str = "block_1") -> RKPMCells:
+    """element_smoothing_cell with the reproducing_kernel space and the two-pass method
+    (the reference's default for element cells): the cells are the tets with their own
+    smoothed gradients (SmoothedCellDataProcessor.h:541-675, two-pass branch), the mass is
+    rho V_t / 4 scattered through the functions, and functions() gives the coupling."""
+    from .smoothing import element_smoothing_part
+
+    rk = element_cells(coords, tets, material, kernel_radius, max_neighbors, keep_points=True, name=name)
+    part, _ = element_smoothing_part(np.asarray(coords, dtype=np.float64), np.asarray(tets), material,
+                                     mu_field=mu_field, kappa_field=kappa_field, name=name)
+    return RKPMCells(part, rk.mass, rk.points, rk.nbr_ptr, rk.nbr, rk.values)
+
+
+def apply_functions(functions, d: np.ndarray) -> np.ndarray:
+    """Physical field Psi d at the nodes from generalized coefficients d (N x 3): row i
+    sums psi_j(x_i) d_j over its neighbours; a row without neighbours copies d_i."""
+    ptr, nbr, val = (np.asarray(a) for a in functions)
+    d = np.asarray(d, dtype=np.float64)
+    counts = np.diff(ptr)
+    out = np.zeros_like(d)
+    np.add.at(out, np.repeat(np.arange(counts.size), counts), val[:, None] * d[nbr])
+    empty = counts == 0
+    out[empty] = d[empty]
+    return out
 
 
 def _cells(entry: str, coords, tets, material, kernel_radius, max_neighbors, keep_points, mu_field, kappa_field,

@@ -254,6 +254,21 @@ int am_stable_time_increment(am_ctx* ctx, double previous, int32_t num_iteration
 int am_solve_power_method(am_ctx* ctx, am_precision prec, double scale_factor, int64_t update_interval, double t_end,
                           int64_t max_steps, int64_t* steps_done, double* last_increment);
 
+/* ---- two-pass reproducing-kernel coupling (the solver's generalized-field path with the
+ * two-pass method, src/Solvers/Explicit.cpp:146-186; FunctionEvaluationProcessor::ComputeValues
+ * and ScatterValues, include/FunctionEvaluationProcessor.h:70-174) ----
+ * The state (u, v, a) holds the generalized coefficients. Row i of Psi (nbr_ptr num_nodes+1,
+ * nbr, values; host arrays) lists psi_j(x_i) for the neighbours j of node i, as
+ * am_cells_get_points returns them for element cells. Every force evaluation then runs
+ * the blocks (FEM smoothed cells, Gauss elements) on the physical displacement Psi u
+ * (a row without neighbours copies its coefficient), gathers their forces per node and
+ * scatters them to the coefficients as Psi^T f (a row without neighbours passes its
+ * force through), summed in a fixed order instead of the reference's atomics. Needs the
+ * generalized lumped mass (the element mass scattered through the functions, as
+ * am_cells_get returns it) from am_set_mass before am_finalize; call once after
+ * am_finalize. Not available with the VJP, the adjoint or a decomposed mesh (AM_ESTATE). */
+int am_set_rk_functions(am_ctx* ctx, const int64_t* nbr_ptr, const int32_t* nbr, const double* values);
+
 /* ---- domain decomposition (replaces the reference's ParallelSum of the force field
  * after the element loop, src/Solvers/Explicit.cpp:190-193) ----
  * A context holds one rank's slab of elements and every node they touch; nodes held by

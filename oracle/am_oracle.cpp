@@ -739,8 +739,42 @@ void ob_stress(int material, double lambda, double mu, int64_t n, const double* 
 // Internal force over all parts, overwriting f (the solver zeroes the force field
 // before the contributions accumulate, src/Solvers/Explicit.cpp:157-163).
 void ob_internal_force(const ob_problem* p, const double* u, double* f) {
-    std::fill(f, f + p->num_nodes * 3, 0.0);
-    for (int k = 0; k < p->num_blocks; ++k) add_block_forces(p, p->blocks[k], u, f);
+    const int64_t N = p->num_nodes;
+    std::fill(f, f + N * 3, 0.0);
+    if (!p->rk_ptr) {
+        for (int k = 0; k < p->num_blocks; ++k) add_block_forces(p, p->blocks[k], u, f);
+        return;
+    }
+    // Two-pass method (ExplicitSolver::ComputeForce, src/Solvers/Explicit.cpp:146-186).
+    // Physical displacement from the coefficients (FunctionEvaluationProcessor::ComputeValues,
+    // include/FunctionEvaluationProcessor.h:86-121): a row without neighbours copies its
+    // coefficient, others sum psi * coefficient over the neighbours in reverse order.
+    std::vector<double> up(N * 3), fl(N * 3, 0.0);
+    for (int64_t i = 0; i < N; ++i) {
+        const int64_t b = p->rk_ptr[i], e = p->rk_ptr[i + 1];
+        for (int c = 0; c < 3; ++c) {
+            if (b == e) {
+                up[i * 3 + c] = u[i * 3 + c];
+                continue;
+            }
+            double s = 0.0;
+            for (int64_t k = e; k-- > b;) s += u[p->rk_nbr[k] * 3 + c] * p->rk_values[k];
+            up[i * 3 + c] = s;
+        }
+    }
+    for (int k = 0; k < p->num_blocks; ++k) add_block_forces(p, p->blocks[k], up.data(), fl.data());
+    // Local forces scattered to the coefficients (ScatterValues, :130-174): psi_j(x_i) f_i
+    // added to node j; a row without neighbours passes its force through. The reference
+    // adds with atomics in no fixed order; here the sum for each node runs over i ascending.
+    for (int64_t i = 0; i < N; ++i) {
+        const int64_t b = p->rk_ptr[i], e = p->rk_ptr[i + 1];
+        if (b == e) {
+            for (int c = 0; c < 3; ++c) f[i * 3 + c] += fl[i * 3 + c];
+            continue;
+        }
+        for (int64_t k = b; k < e; ++k)
+            for (int c = 0; c < 3; ++c) f[p->rk_nbr[k] * 3 + c] += p->rk_values[k] * fl[i * 3 + c];
+    }
 }
 
 // ComputeElementVolumeFunctor.h:20-79: V_e = sum_gp w_gp.

@@ -73,6 +73,12 @@ typedef struct {
     const ob_bc* bcs;
     const double* mass;    /* lumped nodal mass, or NULL = from Gauss blocks */
     double body_accel[3];  /* gravity vector (ExternalForceContributionGravity) */
+    /* Two-pass reproducing-kernel coupling, or NULL: row i of Psi (rk_ptr num_nodes+1,
+     * rk_nbr / rk_values) holds the functions psi_j(x_i). The blocks then see the
+     * physical displacement Psi u and their forces reach the nodes as Psi^T f. */
+    const int64_t* rk_ptr;
+    const int32_t* rk_nbr;
+    const double* rk_values;
 } ob_problem;
 
 /* ---- quadrature (QuadratureGaussian.h, QuadratureSmoothed.h) ---- */

@@ -37,7 +37,8 @@ class OBC(C.Structure):
 
 class OProblem(C.Structure):
     _fields_ = [("num_nodes", C.c_int64), ("coords", _dp), ("num_blocks", C.c_int32), ("blocks", C.POINTER(OBlock)),
-                ("num_bcs", C.c_int32), ("bcs", C.POINTER(OBC)), ("mass", _dp), ("body_accel", C.c_double * 3)]
+                ("num_bcs", C.c_int32), ("bcs", C.POINTER(OBC)), ("mass", _dp), ("body_accel", C.c_double * 3),
+                ("rk_ptr", _lp), ("rk_nbr", _ip), ("rk_values", _dp)]
 
 
 def build() -> Path:
@@ -93,7 +94,9 @@ def _p(a, t=C.c_double):
 class OracleProblem:
     """Holds the ctypes view of a problem (coords, parts, BCs) and its buffers."""
 
-    def __init__(self, coords, parts, bcs=(), mass=None, body_accel=(0.0, 0.0, 0.0)):
+    def __init__(self, coords, parts, bcs=(), mass=None, body_accel=(0.0, 0.0, 0.0), rk=None):
+        """rk = (nbr_ptr, nbr, values): the two-pass reproducing-kernel functions at the
+        nodes (row i: psi_j(x_i) for the neighbours j of node i), or None."""
         self.keep = []
         self.coords = self._arr(coords, np.float64)
         self.N = self.coords.shape[0]
@@ -132,6 +135,10 @@ class OracleProblem:
         self.num_elems = sum(p.num_elems for p in parts)
         self.s = OProblem(self.N, _p(self.coords), len(parts), blocks, len(bcs), obcs, _p(self.mass),
                           (C.c_double * 3)(*body_accel))
+        if rk is not None:
+            ptr, nbr, val = (self._arr(a, t) for a, t in zip(rk, (np.int64, np.int32, np.float64)))
+            assert ptr.size == self.N + 1 and nbr.size == val.size == ptr[-1]
+            self.s.rk_ptr, self.s.rk_nbr, self.s.rk_values = _p(ptr, C.c_int64), _p(nbr, C.c_int32), _p(val)
 
     def _arr(self, a, dt):
         if a is None:

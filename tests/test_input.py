@@ -153,6 +153,12 @@ def test_components_vector_initial_conditions_and_extensions():
     (nh_yaml().replace("gauss_quadrature: {integration_order: 1}",
                        "strain_smoothing: {element_smoothing_cell: {subdomains: 1}, use_f_bar: true}"), "F-bar"),
     (nh_yaml().replace("components: {X: 1.0, Z: -0.5}", "components: {W: 1.0}"), "component"),
+    (nh_yaml().replace("gauss_quadrature: {integration_order: 1}",
+                       "strain_smoothing: {element_smoothing_cell: {subdomains: 1}, force_one_pass_method: true, "
+                       "force_two_pass_method: true}"), "Cannot force both"),
+    (nh_yaml().replace("gauss_quadrature: {integration_order: 1}",
+                       "strain_smoothing: {nodal_smoothing_cell: {subdomains: 1}, force_two_pass_method: true}").replace(
+        "finite_element: ~", "reproducing_kernel: {kernel_radius_scale_factor: 1.1}"), "two-pass nodal"),
 ])
 def test_rejected_inputs(text, msg):
     with pytest.raises(inp.InputError, match=msg):
@@ -207,6 +213,32 @@ def test_yaml_rkpm_cells_run_matches_oracle(oracle_lib, cell):
     u, v, a, n = prob.solve(np.zeros_like(sim.coords), sim.v0, sim.dt, sim.time_end)
     assert r["steps"] == n
     assert np.linalg.norm(r["displacement"] - u) <= 1e-12 * np.linalg.norm(u)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_yaml_rkpm_two_pass_default_matches_oracle(oracle_lib, precision):
+    """element_smoothing_cell with reproducing_kernel and no force key runs the two-pass
+    method (InternalForceContributionParameters.h:164-194): FEM smoothed tet cells coupled
+    to the coefficients through the vertex functions, against the oracle given them."""
+    text = nh_yaml(n=4, extra=f"""      x_b200:
+        precision: {precision}
+""").replace(
+        "gauss_quadrature: {integration_order: 1}",
+        "strain_smoothing: {element_smoothing_cell: {subdomains: 1}}").replace(
+        "finite_element: ~", "reproducing_kernel: {kernel_radius_scale_factor: 1.1}")
+    sim = inp.load(text)
+    assert sim.rk is not None and sim.parts[0].kind == "cells" and sim.parts[0].num_elems == 6 * 64
+    r = inp.run(sim)
+    prob = oracle_lib.OracleProblem(sim.coords, sim.parts, sim.bcs, mass=sim.mass, rk=sim.rk)
+    u, v, a, n = prob.solve(np.zeros_like(sim.coords), sim.v0, sim.dt, sim.time_end)
+    assert r["steps"] == n
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    assert np.linalg.norm(r["displacement"] - u) <= tol * np.linalg.norm(u)
+    from aperi_mech_b200.rkpm import apply_functions
+
+    up = apply_functions(sim.rk, u)
+    assert np.linalg.norm(r["physical_displacement"] - up) <= tol * np.linalg.norm(up)
 
 
 @pytest.mark.gpu

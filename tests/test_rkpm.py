@@ -188,3 +188,126 @@ def test_rkpm_element_cells_setup_force_and_steps_match_oracle(gpu, oracle_lib):
     want_state = op.steps(zero, v0, op.init_acceleration(zero), np.full(30, dt))
     for g, w in zip(got_state, want_state):
         assert rel_err(g, w) < 1e-12
+
+
+# ---- two-pass method on element cells (the reference's default for element cells) ------
+def _two_pass_inputs(oracle_lib, X, T, mat, scale=1.1):
+    """Oracle functions and generalized mass at the vertices, FEM smoothed tet cells."""
+    from aperi_mech_b200.smoothing import element_smoothing_part
+
+    r = oracle_lib.rkpm_element_cells(X, T, _tet_radius(X, T, scale), max_neighbors=40, density=mat.density)
+    part, _ = element_smoothing_part(X, T, mat)
+    return part, r["mass"], (r["nbr_ptr"], r["nbr"], r["values"])
+
+
+def _dense(rk, N):
+    ptr, nb, v = rk
+    Psi = np.zeros((N, N))
+    np.add.at(Psi, (_rows(ptr), nb), v)
+    return Psi
+
+
+def test_oracle_two_pass_is_psi_transpose_fem_psi(oracle_lib):
+    """ExplicitSolver::ComputeForce with the two-pass method: f = Psi^T F_fem(Psi d); the
+    work identity d . f = (Psi d) . F_fem and a zero force sum (partition of unity)."""
+    from aperi_mech_b200.model import Material
+
+    X, T = _box(n=4, seed=6)
+    mat = Material.create("neo_hookean", 1000.0, shear_modulus=3.85e8, bulk_modulus=8.33e8)
+    part, mass, rk = _two_pass_inputs(oracle_lib, X, T, mat)
+    Psi = _dense(rk, X.shape[0])
+    d = 1e-3 * np.random.default_rng(2).standard_normal(X.shape)
+    fem = oracle_lib.OracleProblem(X, [part]).internal_force(Psi @ d)
+    got = oracle_lib.OracleProblem(X, [part], mass=mass, rk=rk).internal_force(d)
+    assert rel_err(got, Psi.T @ fem) < 1e-13
+    assert abs(np.sum(got * d) - np.sum(fem * (Psi @ d))) < 1e-12 * np.abs(fem).max() * np.abs(d).max() * d.size
+    assert np.abs(got.sum(axis=0)).max() < 1e-9 * np.abs(got).max()
+    assert abs(mass.sum() - 2000.0) < 1e-9
+
+
+SHEAR = [(1, 0), (2, 0), (0, 1), (2, 1), (0, 2), (1, 2)]
+
+
+@pytest.mark.parametrize("direction,surface", SHEAR)
+def test_oracle_two_pass_shear_patch(oracle_lib, direction, surface):
+    """ForceTest.cpp ExplicitShearForceReproducingKernel (element smoothing cells, the
+    two-pass default, kernel radius scale 1.1, PatchTestFixture.h:118-123): mass, the
+    physical displacement gradient of every cell, zero acceleration, the local force of
+    each surface pair +/- P n A, the physical displacement and velocity of the faces."""
+    from helpers import expected_pk1, prescribed_patch
+
+    mag = 0.1
+    X, parts, bcs, sets = prescribed_patch("tet4", (1, 1, 1), direction, surface, mag)
+    mat = parts[0].material
+    part, mass, rk = _two_pass_inputs(oracle_lib, X, parts[0].conn, mat)
+    op = oracle_lib.OracleProblem(X, [part], bcs, mass=mass, rk=rk)
+    d, v, a, _ = op.solve(np.zeros_like(X), np.zeros_like(X), 0.1, 10.0)
+    Psi = _dense(rk, X.shape[0])
+    u, vp = Psi @ d, Psi @ v
+    H = np.zeros((3, 3))
+    H[direction, surface] = 2.0 * mag
+    assert abs(mass.sum() - 0.08) < 1e-12
+    B = part.cell_grads.reshape(-1, 4, 3)
+    conn = part.cell_nodes.reshape(-1, 4)
+    for c in range(conn.shape[0]):
+        assert np.abs(u[conn[c]].T @ B[c] - H).max() < 1e-9
+    assert np.abs(a).max() < 1e-12
+    f_local = oracle_lib.OracleProblem(X, [part]).internal_force(u)
+    P = expected_pk1(H, mat)
+    for i in range(3):
+        n_i = np.zeros(3)
+        n_i[i] = 1.0
+        assert np.abs(f_local[sets[f"surface_{2 * i + 1}"]].sum(axis=0) - P @ n_i).max() < 1e-8
+        assert np.abs(f_local[sets[f"surface_{2 * i + 2}"]].sum(axis=0) + P @ n_i).max() < 1e-8
+    s_lo, s_hi = sets[f"surface_{2 * surface + 1}"], sets[f"surface_{2 * surface + 2}"]
+    dd = np.zeros(3)
+    dd[direction] = mag
+    assert np.abs(u[s_hi] - dd).max() < 1e-9 and np.abs(u[s_lo] + dd).max() < 1e-9
+    assert np.abs(vp[s_hi] - 1.875 * dd / 10.0).max() < 1e-4
+
+
+@pytest.mark.gpu
+def test_rkpm_two_pass_force_and_steps_match_oracle(gpu, oracle_lib):
+    """The library's two-pass coupling (set-up, force in FP64 and mixed precision, 30
+    steps with a fixed face) against the oracle fed the same functions."""
+    from aperi_mech_b200 import mesh
+    from aperi_mech_b200.model import BoundaryCondition, ExplicitDynamics, Material
+    from aperi_mech_b200.rkpm import apply_functions, two_pass_element_cells
+
+    X, T = _box(n=4, seed=7)
+    R = _tet_radius(X, T, 1.1)
+    mat = Material.create("neo_hookean", 1000.0, shear_modulus=3.85e8, bulk_modulus=8.33e8)
+    cells = two_pass_element_cells(X, T, mat, R)
+    part, mass, rk = _two_pass_inputs(oracle_lib, X, T, mat)
+    assert np.array_equal(cells.part.cell_nodes, part.cell_nodes)
+    assert rel_err(cells.mass, mass) < 1e-12
+    assert np.array_equal(cells.nbr_ptr, rk[0]) and np.array_equal(cells.nbr, rk[1])
+    assert rel_err(cells.values, rk[2]) < 1e-12
+    fixed = mesh.side_sets(X)["surface_5"]
+    bcs = [BoundaryCondition.fixed(fixed)]
+    rng = np.random.default_rng(4)
+    v0 = rng.uniform(-0.01, 0.01, size=X.shape)
+    v0[:, 0] += X[:, 2]
+    v0[fixed] = 0.0
+    u = 1e-3 * rng.standard_normal(X.shape)
+    op = oracle_lib.OracleProblem(X, [cells.part], bcs, mass=cells.mass, rk=cells.functions())
+    dt = 0.5 * float(mesh.tet_char_length(X, T).min()) / np.sqrt((mat.lam + 2 * mat.mu) / mat.density)
+    zero = np.zeros_like(X)
+    want_state = op.steps(zero, v0, op.init_acceleration(zero), np.full(30, dt))
+    with ExplicitDynamics(X, [cells.part], bcs, mass=cells.mass, rk=cells.functions()) as m:
+        assert rel_err(m.internal_force(u), op.internal_force(u)) < 1e-12
+        assert rel_err(m.internal_force(u, "mixed"), op.internal_force(u)) < 5e-5
+        m.set_state(None, v0)
+        m.init_acceleration()
+        m.run(30, dt)
+        got_state = m.get_state()
+        m.set_state(zero, v0)
+        m.init_acceleration("mixed")
+        m.run(30, dt, "mixed")
+        mixed_u = m.get_state()[0]
+    for g, w in zip(got_state, want_state):
+        assert rel_err(g, w) < 1e-12
+    assert rel_err(mixed_u, want_state[0]) < 1e-5
+    # the physical displacement reproduces a linear field of the coefficients
+    A = 1e-3 * rng.standard_normal((3, 3))
+    assert np.abs(apply_functions(cells.functions(), X @ A.T) - X @ A.T).max() < 1e-12
