@@ -30,7 +30,7 @@ EXPORTED = [
     "am_tet4_internal_force_noalloc", "am_rkpm_nodal_cells", "am_cells_sizes", "am_cells_get",
     "am_cells_get_points", "am_cells_destroy", "am_get_layout", "am_rkpm_element_cells", "am_set_power_method",
     "am_stable_time_increment", "am_solve_power_method", "am_set_interface", "am_nccl_unique_id",
-    "am_set_nccl", "am_set_rk_functions",
+    "am_set_nccl", "am_set_rk_functions", "am_set_cell_groups", "am_rkpm_nodal_subcells", "am_cells_groups",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -125,6 +125,10 @@ def load(build_if_missing: bool = False) -> C.CDLL:
         "am_nccl_unique_id": (C.c_int, [C.c_char_p]),
         "am_set_nccl": (C.c_int, [vp, C.c_char_p, C.c_int32, C.c_int32]),
         "am_set_rk_functions": (C.c_int, [vp, _lp, _ip, _dp]),
+        "am_set_cell_groups": (C.c_int, [vp, C.c_int32, C.c_int64, _lp]),
+        "am_rkpm_nodal_subcells": (C.c_int, [C.c_int64, _dp, C.c_int64, _ip, _dp, C.c_int32, C.c_double,
+                                             C.POINTER(vp)]),
+        "am_cells_groups": (C.c_int, [vp, _lp, _lp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -103,6 +103,11 @@ struct Block {
     float* grads32 = nullptr;
     double* volumes = nullptr;
     int32_t max_entries = 0;
+    // F-bar cells (am_set_cell_groups): the cells are subcells grouped by group_ptr.
+    int64_t num_groups = 0;
+    int64_t* group_ptr = nullptr;
+    double* fbar64 = nullptr;  // kFbarStride per subcell, allocated on first use
+    float* fbar32 = nullptr;
     // Tet4 element patches (see GaussBlockDev)
     int32_t patched = 0;
     int64_t num_patches = 0;
@@ -148,6 +153,23 @@ struct Block {
         c.slot_pos = slot_pos;
         c.num_entries = num_entries;
         c.max_entries = max_entries;
+        c.num_groups = num_groups;
+        c.group_ptr = group_ptr;
+        return c;
+    }
+    // The device view for a force evaluation at the given precision (F-bar scratch attached).
+    am::CellBlockDev cells_for(int mixed) {
+        am::CellBlockDev c = cells();
+        if (group_ptr) {
+            const size_t n = static_cast<size_t>(std::max<int64_t>(num_elems, 1)) * am::kFbarStride;
+            if (mixed) {
+                if (!fbar32) fbar32 = dalloc<float>(n, "F-bar scratch (FP32)");
+                c.fbar = fbar32;
+            } else {
+                if (!fbar64) fbar64 = dalloc<double>(n, "F-bar scratch");
+                c.fbar = fbar64;
+            }
+        }
         return c;
     }
     void release() {
@@ -163,6 +185,9 @@ struct Block {
         dfree(patch_nodes);
         dfree(patch_local);
         dfree(patch_gather);
+        dfree(group_ptr);
+        dfree(fbar64);
+        dfree(fbar32);
     }
 };
 
@@ -349,14 +374,14 @@ struct am_ctx {
             ++launches;
             U = rk_u;
         }
-        for (const auto& b : blocks) {
+        for (auto& b : blocks) {
             if (b.kind == AM_SMOOTHED_CELLS) {
                 if (mixed && !b.grads32) fail(AM_ESTATE, "mixed precision needs FP32 cell gradients");
-                am::launch_cell_force(b.cells(), mixed, U, s, status, stream);
+                launches += am::launch_cell_force(b.cells_for(mixed), mixed, U, s, status, stream);
             } else {
                 am::launch_gauss_force(b.gauss(), mixed, X4, U, s, status, stream);
+                ++launches;
             }
-            ++launches;
         }
         if (rk_ptr) {
             am::NodeDev nd = node_dev();
@@ -1018,6 +1043,28 @@ int am_set_block_fields(am_ctx* ctx, int32_t block_id, const double* mu_field, c
     });
 }
 
+int am_set_cell_groups(am_ctx* ctx, int32_t block_id, int64_t num_cells, const int64_t* group_ptr) {
+    if (!ctx) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        if (ctx->finalized) fail(AM_ESTATE, "am_set_cell_groups after am_finalize");
+        if (block_id < 0 || block_id >= static_cast<int32_t>(ctx->blocks.size())) fail(AM_EINVAL, "bad block id");
+        Block& b = ctx->blocks[block_id];
+        if (b.kind != AM_SMOOTHED_CELLS) fail(AM_EINVAL, "cell groups need a smoothed-cell block");
+        if (b.group_ptr) fail(AM_ESTATE, "cell groups already set");
+        if (num_cells < 0 || !group_ptr) fail(AM_EINVAL, "null cell groups");
+        if (group_ptr[0] != 0 || group_ptr[num_cells] != b.num_elems)
+            fail(AM_EINVAL, "group_ptr must run from 0 to the block's subcell count");
+        for (int64_t g = 0; g < num_cells; ++g)
+            if (group_ptr[g + 1] < group_ptr[g]) fail(AM_EINVAL, "group_ptr must be non-decreasing");
+        // As the reference, F-bar applies only when the cells hold more than one subcell
+        // in total (ForEachCellComputeForce_Impl: num_subcells != num_cells).
+        if (num_cells == b.num_elems) return;
+        b.num_groups = num_cells;
+        b.group_ptr = dalloc<int64_t>(num_cells + 1, "cell groups");
+        ck(cudaMemcpy(b.group_ptr, group_ptr, (num_cells + 1) * sizeof(int64_t), cudaMemcpyHostToDevice), "upload");
+    });
+}
+
 int am_set_body_acceleration(am_ctx* ctx, const double g[3]) {
     if (!ctx || !g) return AM_EINVAL;
     return guarded(ctx, [&] {
@@ -1256,6 +1303,8 @@ int am_vjp_force(am_ctx* ctx, am_memory where, const double* u, const double* la
         ctx->require_finalized();
         if (ctx->iface_row_of) fail(AM_ESTATE, "the VJP is not available on a decomposed mesh");
         if (ctx->rk_ptr) fail(AM_ESTATE, "the VJP is not available with the two-pass coupling");
+        for (const auto& b : ctx->blocks)
+            if (b.group_ptr) fail(AM_ESTATE, "the VJP is not available on F-bar cells");
         if (!u || !lam || !gu) fail(AM_EINVAL, "null u, lam or gu");
         load_nodal(ctx, where, u, ctx->W4);
         load_nodal(ctx, where, lam, ctx->L4);
@@ -1293,6 +1342,8 @@ int am_adjoint(am_ctx* ctx, int64_t nsteps, double dt, int32_t ckpt_every, int32
         ctx->require_finalized();
         if (ctx->iface_row_of) fail(AM_ESTATE, "the adjoint is not available on a decomposed mesh");
         if (ctx->rk_ptr) fail(AM_ESTATE, "the adjoint is not available with the two-pass coupling");
+        for (const auto& b : ctx->blocks)
+            if (b.group_ptr) fail(AM_ESTATE, "the adjoint is not available on F-bar cells");
         if (nsteps <= 0 || !(dt > 0.0)) fail(AM_EINVAL, "nsteps and dt must be positive");
         if (ckpt_every <= 0) fail(AM_EINVAL, "ckpt_every must be positive");
         if (num_sensors < 0 || (num_sensors > 0 && !sensors)) fail(AM_EINVAL, "bad sensor list");

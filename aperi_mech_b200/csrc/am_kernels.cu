@@ -591,6 +591,159 @@ __global__ void __launch_bounds__(256) k_cell_force_group(CellBlockDev b, const 
 }
 
 // ---------------------------------------------------------------------------
+// F-bar smoothed cells (ForEachCellComputeForceFbar, ComputeInternalForceSmoothedCell.h:
+// 354-413) in three passes over the scratch fb (kFbarStride values per subcell):
+//   k_fbar_h     per subcell: H_s = sum_k u_k (x) b_k, J_s = DetApIm1(H_s) + 1 -> fb[0..9]
+//   k_fbar_cell  per cell (kFbarLanes lanes striding over its subcells):
+//                Jbar = sum J_s V_s / sum V_s; Hbar_s = js H_s + (js - 1) I with
+//                js = cbrt(Jbar / J_s) (H_s itself when Jbar / J_s is within 3 eps of 1);
+//                Pbar_s = P(Hbar_s); the dual pressure p = sum js / (3 Jbar) V_s Pbar_s : F_s
+//                / sum V_s; P_s = js Pbar_s + (p - js / (3 J_s) Pbar_s : F_s) cof(F_s) -> fb[10..18]
+//   k_fbar_force per subcell: f_k = -V_s b_k P_s^T into the subcell's slots.
+// Lane sums combine by fixed butterflies, so the result does not depend on scheduling.
+// The scalar chain (Jbar, js, p) is FP64 in both precisions.
+// ---------------------------------------------------------------------------
+constexpr int kFbarLanes = 8;
+
+template <typename T, int LPC>
+__global__ void __launch_bounds__(256) k_fbar_h(CellBlockDev b, const double4* __restrict__ U4, int* status) {
+    const int64_t c = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / LPC;
+    const int r = static_cast<int>(threadIdx.x % LPC);
+    const unsigned gmask = LPC == 32 ? kFull : (((1u << LPC) - 1u) << ((threadIdx.x & 31) & ~(LPC - 1)));
+    const bool valid = c < b.num_cells;
+    const int32_t s0 = valid ? b.ptr[c] : 0, s1 = valid ? b.ptr[c + 1] : 0;
+    const T* gr = cell_grads<T>(b);
+    const bool diff = sizeof(T) == 4;
+    const double4 ur = s1 > s0 ? U4[b.nodes[s0]] : make_double4(0.0, 0.0, 0.0, 0.0);
+    T H[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) H[k] = T(0);
+    for (int32_t s = s0 + r; s < s1; s += LPC) {
+        const double4 u = U4[b.nodes[s]];
+        const T du[3] = {T(diff ? u.x - ur.x : u.x), T(diff ? u.y - ur.y : u.y), T(diff ? u.z - ur.z : u.z)};
+        const T gg[3] = {gr[3 * s], gr[3 * s + 1], gr[3 * s + 2]};
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) H[i * 3 + j] += du[i] * gg[j];
+    }
+#pragma unroll
+    for (int off = LPC / 2; off > 0; off >>= 1)
+#pragma unroll
+        for (int k = 0; k < 9; ++k) H[k] += __shfl_xor_sync(gmask, H[k], off);
+    if (!valid || r != 0) return;
+    const double J = det_ap_im1(H) + 1.0;
+    if (!(J > 0.0)) flag(status, AM_ENONPOS_J, c);
+    T* o = static_cast<T*>(b.fbar) + kFbarStride * c;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) o[k] = H[k];
+    o[9] = T(J);
+}
+
+__device__ __forceinline__ void fbar_combine(double& x, double& y) {
+#pragma unroll
+    for (int off = kFbarLanes / 2; off > 0; off >>= 1) {
+        x += __shfl_xor_sync(kFull, x, off);
+        y += __shfl_xor_sync(kFull, y, off);
+    }
+}
+
+template <typename T, int MAT>
+__global__ void __launch_bounds__(256) k_fbar_cell(CellBlockDev b, int* status) {
+    const int64_t g = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / kFbarLanes;
+    const int r = static_cast<int>(threadIdx.x % kFbarLanes);
+    const bool valid = g < b.num_groups;
+    const int64_t s0 = valid ? b.group_ptr[g] : 0, s1 = valid ? b.group_ptr[g + 1] : 0;
+    T* fb = static_cast<T*>(b.fbar);
+    double jv = 0.0, vol = 0.0;
+    for (int64_t s = s0 + r; s < s1; s += kFbarLanes) {
+        jv += static_cast<double>(fb[kFbarStride * s + 9]) * b.volumes[s];
+        vol += b.volumes[s];
+    }
+    fbar_combine(jv, vol);
+    const double Jbar = s1 > s0 ? jv / vol : 1.0;
+    double pd = 0.0, unused = 0.0;
+    for (int64_t s = s0 + r; s < s1; s += kFbarLanes) {
+        T* o = fb + kFbarStride * s;
+        T H[9], Hb[9], Pb[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) H[k] = o[k];
+        const double ratio = Jbar / static_cast<double>(o[9]);
+        const double js = cbrt(ratio);
+        if (fabs(ratio - 1.0) < 3.0 * 2.2204460492503131e-16) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) Hb[k] = H[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) Hb[k] = H[k] * T(js);
+            Hb[0] += T(js - 1.0);
+            Hb[4] += T(js - 1.0);
+            Hb[8] += T(js - 1.0);
+        }
+        double lam, mu;
+        element_lame(b, s, lam, mu);
+        const double Jb = stress<T>(MAT, T(lam), T(mu), Hb, Pb);
+        if (MAT == kNeoHookean && !(Jb > 0.0)) flag(status, AM_ENONPOS_J, s);
+        double pf = static_cast<double>(Pb[0] + Pb[4] + Pb[8]);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) pf += static_cast<double>(Pb[k] * H[k]);
+        pd += js / (3.0 * Jbar) * b.volumes[s] * pf;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) o[10 + k] = Pb[k];
+    }
+    fbar_combine(pd, unused);
+    if (s1 <= s0) return;
+    pd /= vol;
+    for (int64_t s = s0 + r; s < s1; s += kFbarLanes) {
+        T* o = fb + kFbarStride * s;
+        T F[9], Pb[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            F[k] = o[k];
+            Pb[k] = o[10 + k];
+        }
+        F[0] += T(1);
+        F[4] += T(1);
+        F[8] += T(1);
+        const double J = static_cast<double>(o[9]);
+        const double js = cbrt(Jbar / J);
+        double pf = 0.0;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) pf += static_cast<double>(Pb[k] * F[k]);
+        // (p - js / (3 J) Pbar : F) J F^-T = (p - js / (3 J) Pbar : F) cof(F)
+        const T scal = T(pd - js / (3.0 * J) * pf);
+        T A[9];
+        adj3(F, A);  // cof(F) = adj(F)^T
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) o[10 + i * 3 + j] = Pb[i * 3 + j] * T(js) + scal * A[j * 3 + i];
+    }
+}
+
+template <typename T, int LPC>
+__global__ void __launch_bounds__(256) k_fbar_force(CellBlockDev b, vec4_t<T>* __restrict__ slots) {
+    const int64_t c = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / LPC;
+    const int r = static_cast<int>(threadIdx.x % LPC);
+    if (c >= b.num_cells) return;
+    const int32_t s0 = b.ptr[c], s1 = b.ptr[c + 1];
+    if (s1 <= s0) return;
+    const T* gr = cell_grads<T>(b);
+    const T* o = static_cast<const T*>(b.fbar) + kFbarStride * c + 10;
+    T P[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) P[k] = o[k];
+    const T V = T(b.volumes[c]);
+    for (int32_t s = s0 + r; s < s1; s += LPC) {
+        const T gg[3] = {gr[3 * s], gr[3 * s + 1], gr[3 * s + 2]};
+        T f[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) f[i] = (gg[0] * P[i * 3 + 0] + gg[1] * P[i * 3 + 1] + gg[2] * P[i * 3 + 2]) * -V;
+        slots[b.slot_pos[s]] = make4(f[0], f[1], f[2]);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // VJP kernels (FP64): slots receive (dF/du)^T lam per element node; gmu/gkappa
 // receive lam^T dF/dmu_e and lam^T dF/dkappa_e (lambda_e = kappa_e - 2/3 mu_e).
 // Lambda = sum_a lam_a (x) B_a ; lam . f_e = -sum_gp w Lambda : P.
@@ -1518,8 +1671,37 @@ inline int lanes_per_cell(const CellBlockDev& b) {
     AM_DISPATCH_MAT(b.material, (k_cell_force_group<T, M, LPC><<<grid_for(b.num_cells * LPC, 256), 256, 0, s>>>( \
                                     b, U4, static_cast<vec4_t<T>*>(slots), status)))
 
-void launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void* slots, int* status, cudaStream_t s) {
-    if (b.num_cells == 0) return;
+template <typename T, int LPC>
+void launch_fbar_lpc(const CellBlockDev& b, const double4* U4, void* slots, int* status, cudaStream_t s) {
+    const unsigned gs = grid_for(b.num_cells * LPC, 256);
+    k_fbar_h<T, LPC><<<gs, 256, 0, s>>>(b, U4, status);
+    AM_DISPATCH_MAT(b.material, (k_fbar_cell<T, M><<<grid_for(b.num_groups * kFbarLanes, 256), 256, 0, s>>>(b, status)));
+    k_fbar_force<T, LPC><<<gs, 256, 0, s>>>(b, static_cast<vec4_t<T>*>(slots));
+}
+
+template <typename T>
+void launch_fbar(const CellBlockDev& b, const double4* U4, void* slots, int* status, cudaStream_t s) {
+    const int lpc = lanes_per_cell(b);
+    if (lpc == 4) {
+        launch_fbar_lpc<T, 4>(b, U4, slots, status, s);
+    } else if (lpc == 8) {
+        launch_fbar_lpc<T, 8>(b, U4, slots, status, s);
+    } else if (lpc == 16) {
+        launch_fbar_lpc<T, 16>(b, U4, slots, status, s);
+    } else {
+        launch_fbar_lpc<T, 32>(b, U4, slots, status, s);
+    }
+}
+
+int launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void* slots, int* status, cudaStream_t s) {
+    if (b.num_cells == 0) return 0;
+    if (b.fbar != nullptr) {
+        if (mixed)
+            launch_fbar<float>(b, U4, slots, status, s);
+        else
+            launch_fbar<double>(b, U4, slots, status, s);
+        return 3;
+    }
     if (b.max_entries <= 8) {
         const unsigned grid = grid_for(b.num_cells, 256);
         if (mixed) {
@@ -1527,7 +1709,7 @@ void launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void
         } else {
             AM_DISPATCH_MAT(b.material, (k_cell_force_thread<double, M><<<grid, 256, 0, s>>>(b, U4, static_cast<double4*>(slots), status)));
         }
-        return;
+        return 1;
     }
     const int lpc = lanes_per_cell(b);
     if (mixed) {
@@ -1551,6 +1733,7 @@ void launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void
             AM_CELL_GROUP(double, 32);
         }
     }
+    return 1;
 }
 
 void launch_gauss_vjp(const GaussBlockDev& b, const double4* X4, const double4* U4, const double4* L4, double4* slots,

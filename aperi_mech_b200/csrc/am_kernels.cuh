@@ -62,7 +62,14 @@ struct CellBlockDev {
     const int32_t* slot_pos;    // entry -> node-major position
     int64_t num_entries;        // ptr[num_cells]
     int32_t max_entries;        // longest cell (selects thread- or group-per-cell)
+    // F-bar (ComputeInternalForceSmoothedCell.h:354-413): the cells above are subcells,
+    // grouped into num_groups cells by group_ptr; fbar is the per-subcell scratch
+    // (kFbarStride values of the slot precision: H, J, then the stress). null: no F-bar.
+    int64_t num_groups;
+    const int64_t* group_ptr;
+    void* fbar;
 };
+constexpr int kFbarStride = 20;
 
 // Node gather + nodal update configuration.
 struct NodeDev {
@@ -86,7 +93,8 @@ struct NodeDev {
 // ---- launchers (am_kernels.cu) ----
 void launch_gauss_force(const GaussBlockDev& b, int mixed, const double4* X4, const double4* U4, void* slots,
                         int* status, cudaStream_t s);
-void launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void* slots, int* status, cudaStream_t s);
+// Returns the number of kernels launched (3 for an F-bar block).
+int launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void* slots, int* status, cudaStream_t s);
 void launch_gauss_vjp(const GaussBlockDev& b, const double4* X4, const double4* U4, const double4* L4, double4* slots,
                       double* gmu, double* gkappa, int accumulate, cudaStream_t s);
 void launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double4* slots, double* gmu,

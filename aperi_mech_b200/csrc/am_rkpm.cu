@@ -46,6 +46,7 @@ struct am_cells {
     std::vector<double> cell_grads;  // x 3
     std::vector<double> cell_volumes;
     std::vector<double> mass;
+    std::vector<int64_t> group_ptr;  // subcells of each cell, when the cells hold subcells
 };
 
 namespace {
@@ -305,14 +306,13 @@ void rk_functions(am_cells* c, int64_t N, const double* X, const double* R, doub
             throw;
         }
         cleanup();
-    }}
+    }
+}
 
-}  // namespace
-
-extern "C" {
-
-int am_rkpm_nodal_cells(int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R,
-                        int32_t max_neighbors, double density, am_cells** out) {
+// Nodal cells on the thex corner hexes; with subcells every corner hex is its own
+// subcell and group_ptr collects the hexes of each vertex.
+int nodal_cells(int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R, int32_t max_neighbors,
+                double density, bool subcells, am_cells** out) {
     am::set_free_error("");
     if (!out) return AM_EINVAL;
     *out = nullptr;
@@ -407,6 +407,53 @@ int am_rkpm_nodal_cells(int64_t N, const double* X, int64_t T, const int32_t* te
             }
         });
         std::atomic<int> bad(0);
+        if (subcells) {
+            // One subcell per corner hex, in vertex order then tet order; entries are the
+            // union of the hex points' neighbours (first appearance), b = sum_k B_k V psi / V.
+            const int64_t S = 4 * T;
+            std::vector<std::vector<int32_t>> sn(S);
+            std::vector<std::vector<double>> sg(S);
+            c->cell_volumes.assign(S, 0.0);
+            parallel_for(S, [&](int64_t q) {
+                thread_local std::vector<int32_t> where;
+                if (static_cast<int64_t>(where.size()) < N) where.assign(N, -1);
+                const int64_t h = vcorner[q];
+                const auto& hp = hexpts[h];
+                double hx[24], B[24], V;
+                for (int k = 0; k < 8; ++k)
+                    for (int d = 0; d < 3; ++d) hx[k * 3 + d] = pts[hp[k] * 3 + d];
+                hex_smoothed(hx, B, &V);
+                if (!(V > 0.0)) bad = 1;
+                hexvol[h] = V;
+                c->cell_volumes[q] = V;
+                for (int k = 0; k < 8; ++k)
+                    for (int64_t e = c->nbr_ptr[hp[k]]; e < c->nbr_ptr[hp[k] + 1]; ++e) {
+                        const int32_t j = c->nbr[e];
+                        int32_t idx = where[j];
+                        if (idx < 0) {
+                            idx = static_cast<int32_t>(sn[q].size());
+                            where[j] = idx;
+                            sn[q].push_back(j);
+                            sg[q].insert(sg[q].end(), {0.0, 0.0, 0.0});
+                        }
+                        for (int d = 0; d < 3; ++d) sg[q][idx * 3 + d] += B[k * 3 + d] * V * c->psi[e];
+                    }
+                for (double& g : sg[q]) g /= V;
+                for (int32_t j : sn[q]) where[j] = -1;
+            });
+            if (bad) throw Fail{AM_ENONPOS_J, "a corner hex of the thex refinement has non-positive volume"};
+            c->cell_ptr.assign(S + 1, 0);
+            for (int64_t q = 0; q < S; ++q) c->cell_ptr[q + 1] = c->cell_ptr[q] + static_cast<int64_t>(sn[q].size());
+            const int64_t K = c->cell_ptr[S];
+            if (K >= (int64_t(1) << 31)) throw Fail{AM_ERANGE, "cell entry count beyond int32 indexing"};
+            c->cell_nodes.resize(K);
+            c->cell_grads.resize(K * 3);
+            parallel_for(S, [&](int64_t q) {
+                std::copy(sn[q].begin(), sn[q].end(), c->cell_nodes.begin() + c->cell_ptr[q]);
+                std::copy(sg[q].begin(), sg[q].end(), c->cell_grads.begin() + 3 * c->cell_ptr[q]);
+            });
+            c->group_ptr = vptr;
+        } else {
         parallel_for(N, [&](int64_t vtx) {
             thread_local std::vector<int32_t> where;  // node -> entry of the current cell, -1 if none
             if (static_cast<int64_t>(where.size()) < N) where.assign(N, -1);
@@ -449,6 +496,7 @@ int am_rkpm_nodal_cells(int64_t N, const double* X, int64_t T, const int32_t* te
             std::copy(cn[j].begin(), cn[j].end(), c->cell_nodes.begin() + c->cell_ptr[j]);
             std::copy(cg[j].begin(), cg[j].end(), c->cell_grads.begin() + 3 * c->cell_ptr[j]);
         });
+        }
         // Lumped mass: rho V_hex / 8 to each hex point, scattered to the neighbours.
         std::vector<double> mfe(P, 0.0);
         for (int64_t h = 0; h < 4 * T; ++h)
@@ -468,6 +516,20 @@ int am_rkpm_nodal_cells(int64_t N, const double* X, int64_t T, const int32_t* te
         am::set_free_error(e.what());
         return AM_EINVAL;
     }
+}
+
+}  // namespace
+
+extern "C" {
+
+int am_rkpm_nodal_cells(int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R,
+                        int32_t max_neighbors, double density, am_cells** out) {
+    return nodal_cells(N, X, T, tets, R, max_neighbors, density, false, out);
+}
+
+int am_rkpm_nodal_subcells(int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R,
+                           int32_t max_neighbors, double density, am_cells** out) {
+    return nodal_cells(N, X, T, tets, R, max_neighbors, density, true, out);
 }
 
 int am_rkpm_element_cells(int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R,
@@ -576,6 +638,13 @@ int am_cells_sizes(const am_cells* c, int64_t* num_cells, int64_t* num_entries, 
     if (num_entries) *num_entries = static_cast<int64_t>(c->cell_nodes.size());
     if (num_points) *num_points = static_cast<int64_t>(c->points.size() / 3);
     if (num_nbr_entries) *num_nbr_entries = static_cast<int64_t>(c->nbr.size());
+    return AM_OK;
+}
+
+int am_cells_groups(const am_cells* c, int64_t* num_groups, int64_t* group_ptr) {
+    if (!c) return AM_EINVAL;
+    if (num_groups) *num_groups = c->group_ptr.empty() ? 0 : static_cast<int64_t>(c->group_ptr.size()) - 1;
+    if (group_ptr) std::copy(c->group_ptr.begin(), c->group_ptr.end(), group_ptr);
     return AM_OK;
 }
 

@@ -14,8 +14,9 @@ library computes, and builds an ExplicitDynamics model on the GPU:
                   formulation:                      (InternalForceContributionParameters.h:58-246)
                     integration_scheme:
                       gauss_quadrature: {integration_order: 1}
-                      | strain_smoothing: {element_smoothing_cell | nodal_smoothing_cell: {subdomains: 1},
-                                           force_one_pass_method | force_two_pass_method: true}
+                      | strain_smoothing: {element_smoothing_cell | nodal_smoothing_cell: {subdomains: 1 | 0},
+                                           force_one_pass_method | force_two_pass_method: true,
+                                           use_f_bar: true}
                     approximation_space:
                       finite_element: ~ | reproducing_kernel: {kernel_radius_scale_factor: s}
                   material:                         (Materials/Factory.h:19-160)
@@ -41,8 +42,10 @@ split; STK's own split is not available here). An .npz mesh holds `coords` (N x 
 `block_<name>` (E x 4 or E x 8, zero-based) and `set_<name>` (zero-based node ids).
 Element cells with the reproducing_kernel space use the two-pass method unless
 force_one_pass_method is set, nodal cells the one-pass method (the reference's defaults).
-Anything else (Exodus meshes, F-bar, two-pass nodal cells, other materials) raises
-InputError naming the key.
+Nodal cells with subdomains 0 split into one subcell per corner hex, and use_f_bar then
+applies F-bar over each vertex's subcells; with one subcell per cell (subdomains 1, or
+element cells) use_f_bar changes nothing, as in the reference. Anything else (Exodus
+meshes, two-pass nodal cells, other materials) raises InputError naming the key.
 """
 from __future__ import annotations
 
@@ -276,8 +279,7 @@ def _part(pnode: dict, blocks: dict, coords, ext: dict, rng):
     if scheme != "strain_smoothing":
         raise InputError(f"integration_scheme {scheme!r} (gauss_quadrature or strain_smoothing)")
     snode = snode or {}
-    if snode.get("use_f_bar"):
-        raise InputError("use_f_bar: the F-bar smoothed cells are not built yet")
+    use_f_bar = bool(snode.get("use_f_bar", False))
     # IntegrationSchemeStrainSmoothingParameters (InternalForceContributionParameters.h:164-194):
     # one-pass by default, two-pass for element cells, either forced by a key.
     force_one, force_two = bool(snode.get("force_one_pass_method")), bool(snode.get("force_two_pass_method"))
@@ -288,8 +290,13 @@ def _part(pnode: dict, blocks: dict, coords, ext: dict, rng):
         raise InputError(f"strain_smoothing on block {name}: Tet4 meshes only")
     cell = "nodal_smoothing_cell" if "nodal_smoothing_cell" in snode else "element_smoothing_cell"
     sub = int(((snode.get(cell) or {}).get("subdomains", 1)))
-    if sub != 1:
-        raise InputError(f"{cell}.subdomains = {sub}: only 1 is built")
+    # MeshLabelerProcessor.h:832-870: element cells always hold one subcell (other values
+    # only warn); nodal cells split into one subcell per element for subdomains < 1 and
+    # refuse more than one.
+    if cell == "nodal_smoothing_cell" and sub > 1:
+        raise InputError(f"nodal_smoothing_cell.subdomains = {sub}: num_subcells > 1 is not implemented")
+    if cell == "element_smoothing_cell":
+        sub = 1
     if space == "finite_element" and cell == "element_smoothing_cell":
         from .smoothing import element_smoothing_part
 
@@ -301,11 +308,15 @@ def _part(pnode: dict, blocks: dict, coords, ext: dict, rng):
             raise InputError("force_two_pass_method on nodal_smoothing_cell: two-pass nodal cells are not built")
         if mu_f is not None or kappa_f is not None:
             raise InputError("x_b200.fields on RKPM nodal cells: per-cell fields are not supported")
-        from .rkpm import nodal_cells, thex_max_edge_length
+        from .rkpm import nodal_cells, nodal_subcells, thex_max_edge_length
 
         scale = float((spnode or {}).get("kernel_radius_scale_factor", 1.0))
-        cells = nodal_cells(coords, conn, mat, scale * thex_max_edge_length(coords, conn),
-                            max_neighbors=int(ext.get("max_neighbors", 40)))
+        radius = scale * thex_max_edge_length(coords, conn)
+        if sub < 1:
+            cells = nodal_subcells(coords, conn, mat, radius, max_neighbors=int(ext.get("max_neighbors", 40)),
+                                   fbar=use_f_bar)
+        else:
+            cells = nodal_cells(coords, conn, mat, radius, max_neighbors=int(ext.get("max_neighbors", 40)))
         cells.part.name = name
         return cells.part, cells.mass, None
     if space == "reproducing_kernel" and cell == "element_smoothing_cell" and not one_pass:

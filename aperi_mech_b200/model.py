@@ -68,7 +68,8 @@ class Material:
 @dataclass
 class Part:
     """One element block. kind: 'tet4' (1-pt Gauss), 'hex8' (2x2x2 Gauss) or 'cells'
-    (strain-smoothed / RKPM cells given as a CSR of (node, gradient) entries)."""
+    (strain-smoothed / RKPM cells given as a CSR of (node, gradient) entries). With
+    cell_groups (offsets into the cells) the cells are subcells of F-bar cells."""
     kind: str
     material: Material
     conn: np.ndarray | None = None
@@ -79,6 +80,7 @@ class Part:
     mu_field: np.ndarray | None = None
     kappa_field: np.ndarray | None = None
     name: str = "block_1"
+    cell_groups: np.ndarray | None = None  # F-bar: the cells above are subcells of these cells
 
     @property
     def num_elems(self) -> int:
@@ -167,6 +169,9 @@ class ExplicitDynamics:
         d.kappa_field = capi._ptr(arr(p.kappa_field, np.float64))
         bid = C.c_int32()
         check(self.lib.am_add_block(self.ctx, C.byref(d), C.byref(bid)), self.ctx)
+        if p.kind == "cells" and p.cell_groups is not None:
+            g = arr(p.cell_groups, np.int64)
+            check(self.lib.am_set_cell_groups(self.ctx, bid.value, g.size - 1, capi._ptr(g, C.c_int64)), self.ctx)
 
     def _set_bcs(self, bcs: list[BoundaryCondition]) -> None:
         arr_t = capi.BCDesc * len(bcs)

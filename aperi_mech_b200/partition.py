@@ -89,6 +89,8 @@ def decompose(coords: np.ndarray, parts: list, bcs: list, v0: np.ndarray, world:
     N = coords.shape[0]
     if world < 1:
         raise ValueError("world must be >= 1")
+    if any(getattr(p, "cell_groups", None) is not None for p in parts):
+        raise ValueError("F-bar cells are not decomposed (a cell's subcells must stay on one rank)")
     if mass is None:
         if any(p.kind == "cells" for p in parts):
             raise ValueError("cell parts need the global lumped mass")

@@ -78,6 +78,16 @@ def nodal_cells(coords: np.ndarray, tets: np.ndarray, material: Material, kernel
                   mu_field, kappa_field, name)
 
 
+def nodal_subcells(coords: np.ndarray, tets: np.ndarray, material: Material, kernel_radius: np.ndarray,
+                   max_neighbors: int = 40, keep_points: bool = False, fbar: bool = True, mu_field=None,
+                   kappa_field=None, name: str = "block_1") -> RKPMCells:
+    """Nodal cells split into one subcell per corner hex (nodal_smoothing_cell with
+    subdomains 0); with fbar the part carries the vertex cells they form (use_f_bar),
+    otherwise every subcell integrates on its own."""
+    return _cells("am_rkpm_nodal_subcells", coords, tets, material, kernel_radius, max_neighbors, keep_points,
+                  mu_field, kappa_field, name, groups=fbar)
+
+
 def element_cells(coords: np.ndarray, tets: np.ndarray, material: Material, kernel_radius: np.ndarray,
                   max_neighbors: int = 40, keep_points: bool = False, mu_field=None, kappa_field=None,
                   name: str = "block_1") -> RKPMCells:
@@ -114,7 +124,7 @@ def apply_functions(functions, d: np.ndarray) -> np.ndarray:
 
 
 def _cells(entry: str, coords, tets, material, kernel_radius, max_neighbors, keep_points, mu_field, kappa_field,
-           name) -> RKPMCells:
+           name, groups: bool = False) -> RKPMCells:
     lib = capi.load()
     X = np.ascontiguousarray(coords, dtype=np.float64)
     T = np.ascontiguousarray(tets, dtype=np.int32)
@@ -132,8 +142,14 @@ def _cells(entry: str, coords, tets, material, kernel_radius, max_neighbors, kee
         mass = np.empty(X.shape[0])
         check(lib.am_cells_get(h, capi._ptr(ptr, C.c_int64), capi._ptr(nodes, C.c_int32), capi._ptr(grads),
                                capi._ptr(vols), capi._ptr(mass)))
+        cell_groups = None
+        if groups:
+            ng = C.c_int64()
+            check(lib.am_cells_groups(h, C.byref(ng), None))
+            cell_groups = np.empty(ng.value + 1, dtype=np.int64)
+            check(lib.am_cells_groups(h, C.byref(ng), capi._ptr(cell_groups, C.c_int64)))
         res = RKPMCells(Part("cells", material, cell_ptr=ptr, cell_nodes=nodes, cell_grads=grads, cell_volumes=vols,
-                             mu_field=mu_field, kappa_field=kappa_field, name=name), mass)
+                             mu_field=mu_field, kappa_field=kappa_field, name=name, cell_groups=cell_groups), mass)
         if keep_points:
             res.points = np.empty((npnt.value, 3))
             res.nbr_ptr = np.empty(npnt.value + 1, dtype=np.int64)

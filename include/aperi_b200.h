@@ -106,6 +106,16 @@ int am_set_boundary_conditions(am_ctx* ctx, int32_t num_bcs, const am_bc_desc* b
 /* Replace the per-element shear / bulk modulus fields of a block (host arrays of
  * num_elems; NULL leaves that field unchanged). Allowed after am_finalize. */
 int am_set_block_fields(am_ctx* ctx, int32_t block_id, const double* mu_field, const double* kappa_field);
+/* F-bar smoothed cells (use_f_bar; ComputeInternalForceSmoothedCell.h:120-183 J-bar and
+ * F-bar, :227-309 the stress un-barring, :354-413 the pass order). The block's cells
+ * become subcells, grouped into num_cells cells: cell g holds subcells
+ * [group_ptr[g], group_ptr[g+1]) (host array). Per force evaluation: H and J of every
+ * subcell, Jbar = sum J_s V_s / V_cell per cell, the subcells' stresses at
+ * Fbar = (Jbar / J_s)^(1/3) F, the cell's dual pressure, the un-barred stresses, and the
+ * subcell forces -V_s b P^T. As in the reference, when num_cells equals the subcell
+ * count the call changes nothing. Before am_finalize; not available with the VJP or
+ * the adjoint (AM_ESTATE). */
+int am_set_cell_groups(am_ctx* ctx, int32_t block_id, int64_t num_cells, const int64_t* group_ptr);
 int am_set_body_acceleration(am_ctx* ctx, const double g[3]);
 int am_set_mass(am_ctx* ctx, const double* mass);
 int am_finalize(am_ctx* ctx);
@@ -177,6 +187,16 @@ int am_rkpm_nodal_cells(int64_t num_nodes, const double* coords, int64_t num_tet
  * functions evaluated at the vertices only, and the mass rho V_t / 4 to the vertices
  * scattered through the functions. Same outputs and accessors as the nodal cells
  * (the points are the vertices). */
+/* Nodal cells split into subcells (nodal_smoothing_cell with subdomains 0,
+ * MeshLabelerProcessor.h:832-853): every corner hex is a subcell with its own one-pass
+ * gradients sum_k B_hex,k psi_k(j) and volume; the cell arrays hold the subcells
+ * (vertex order, then tet order), am_cells_groups gives the vertex cells they form
+ * (for am_set_cell_groups). Same functions and mass as am_rkpm_nodal_cells. */
+int am_rkpm_nodal_subcells(int64_t num_nodes, const double* coords, int64_t num_tets, const int32_t* tets,
+                           const double* kernel_radius, int32_t max_neighbors, double density, am_cells** out);
+/* Cells formed by the subcells: num_groups (0 when every cell is one subcell) and, when
+ * group_ptr is not NULL, its num_groups + 1 offsets. */
+int am_cells_groups(const am_cells* cells, int64_t* num_groups, int64_t* group_ptr);
 int am_rkpm_element_cells(int64_t num_nodes, const double* coords, int64_t num_tets, const int32_t* tets,
                           const double* kernel_radius, int32_t max_neighbors, double density, am_cells** out);
 int am_cells_sizes(const am_cells* cells, int64_t* num_cells, int64_t* num_entries, int64_t* num_points,

@@ -322,12 +322,96 @@ void cell_force(const ob_block& b, int64_t c, const double* u, double* fk) {
     }
 }
 
+// F-bar smoothed cells (ForEachCellComputeForceFbar, ComputeInternalForceSmoothedCell.h:354-413),
+// one cell g of subcells s in [group_ptr[g], group_ptr[g+1]):
+//   H_s = sum_k u_k (x) b_k, J_s = DetApIm1(H_s) + 1                     (:86-117)
+//   Jbar = sum_s J_s V_s / V_g, V_g = sum_s V_s                          (:120-148)
+//   Hbar_s = js H_s + (js - 1) I, js = cbrt(Jbar / J_s), H itself when
+//            |Jbar / J_s - 1| < 3 eps                                    (:150-183)
+//   Pbar_s = P(Hbar_s)                                                   (:186-224)
+//   p = sum_s js / (3 Jbar) V_s (Pbar_s : H_s + tr Pbar_s) / V_g          (:227-264)
+//   P_s = js Pbar_s + (p - js / (3 J_s) Pbar_s : F_s) J_s F_s^-T          (:266-309)
+//   f_k += b_k (-V_s P_s^T)                                              (:312-351)
+void fbar_cell_forces(const ob_block& b, int64_t g, const double* u, double* slots) {
+    const int64_t s0 = b.group_ptr[g], s1 = b.group_ptr[g + 1];
+    if (s1 <= s0) return;
+    const int64_t n = s1 - s0;
+    std::vector<double> H(9 * n), J(n), js(n), Pb(9 * n);
+    double Vg = 0.0, jv = 0.0;
+    for (int64_t s = s0; s < s1; ++s) {
+        double* h = &H[9 * (s - s0)];
+        std::fill(h, h + 9, 0.0);
+        for (int64_t e = b.cell_ptr[s]; e < b.cell_ptr[s + 1]; ++e) {
+            const int32_t nd = b.cell_nodes[e];
+            const double* gr = b.cell_grads + 3 * e;
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) h[i * 3 + j] += u[nd * 3 + i] * gr[j];
+        }
+        J[s - s0] = det_ap_im1(h) + 1.0;
+        jv += J[s - s0] * b.cell_volumes[s];
+        Vg += b.cell_volumes[s];
+    }
+    const double Jbar = jv / Vg;
+    double p = 0.0;
+    for (int64_t s = s0; s < s1; ++s) {
+        const int64_t q = s - s0;
+        const double* h = &H[9 * q];
+        const double ratio = Jbar / J[q];
+        js[q] = std::cbrt(ratio);
+        double hb[9];
+        if (std::abs(ratio - 1.0) < 3.0 * 2.2204460492503131e-16) {
+            std::copy(h, h + 9, hb);
+        } else {
+            for (int k = 0; k < 9; ++k) hb[k] = h[k] * js[q];
+            for (int i = 0; i < 3; ++i) hb[i * 4] += js[q] - 1.0;
+        }
+        double lambda, mu;
+        block_lame(b, s, &lambda, &mu);
+        stress(b.material, lambda, mu, hb, &Pb[9 * q]);
+        const double* P = &Pb[9 * q];
+        double pf = P[0] + P[4] + P[8];
+        for (int k = 0; k < 9; ++k) pf += P[k] * h[k];
+        p += js[q] / (3.0 * Jbar) * b.cell_volumes[s] * pf;
+    }
+    p /= Vg;
+    for (int64_t s = s0; s < s1; ++s) {
+        const int64_t q = s - s0;
+        const double* h = &H[9 * q];
+        const double* Pbar = &Pb[9 * q];
+        double F[9];
+        std::copy(h, h + 9, F);
+        F[0] += 1.0;
+        F[4] += 1.0;
+        F[8] += 1.0;
+        double pf = 0.0;
+        for (int k = 0; k < 9; ++k) pf += Pbar[k] * F[k];
+        const double scal = (p - js[q] / (3.0 * J[q]) * pf) * J[q];
+        // F^-T: (F^-T)_ij = cof(F)_ij / det F
+        const double cof[9] = {F[4] * F[8] - F[5] * F[7], F[5] * F[6] - F[3] * F[8], F[3] * F[7] - F[4] * F[6],
+                               F[2] * F[7] - F[1] * F[8], F[0] * F[8] - F[2] * F[6], F[1] * F[6] - F[0] * F[7],
+                               F[1] * F[5] - F[2] * F[4], F[2] * F[3] - F[0] * F[5], F[0] * F[4] - F[1] * F[3]};
+        double P[9];
+        for (int k = 0; k < 9; ++k) P[k] = Pbar[k] * js[q] + scal * cof[k] / J[q];
+        const double V = b.cell_volumes[s];
+        for (int64_t e = b.cell_ptr[s]; e < b.cell_ptr[s + 1]; ++e) {
+            const double* gr = b.cell_grads + 3 * e;
+            for (int i = 0; i < 3; ++i)
+                slots[e * 3 + i] = (gr[0] * P[i * 3 + 0] + gr[1] * P[i * 3 + 1] + gr[2] * P[i * 3 + 2]) * -V;
+        }
+    }
+}
+
 void add_block_forces(const ob_problem* p, const ob_block& b, const double* u, double* f) {
     if (b.kind == OB_CELLS) {
         const int64_t K = b.cell_ptr[b.num_elems];
         std::vector<double> slots(static_cast<size_t>(K) * 3);
+        if (b.group_ptr) {
+#pragma omp parallel for schedule(dynamic, 16)
+            for (int64_t g = 0; g < b.num_groups; ++g) fbar_cell_forces(b, g, u, slots.data());
+        } else {
 #pragma omp parallel for schedule(static)
-        for (int64_t c = 0; c < b.num_elems; ++c) cell_force(b, c, u, slots.data() + 3 * b.cell_ptr[c]);
+            for (int64_t c = 0; c < b.num_elems; ++c) cell_force(b, c, u, slots.data() + 3 * b.cell_ptr[c]);
+        }
         // Scatter in entry order (Field::AtomicAdd in the reference; deterministic here).
         for (int64_t s = 0; s < K; ++s) {
             const int32_t n = b.cell_nodes[s];
@@ -1110,12 +1194,12 @@ void corner_hex(const ThexPoints& tp, const double* X, const int32_t* v, int64_t
 
 }  // namespace
 
-extern "C" int ob_rkpm_nodal_cells(int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R,
-                                   int32_t max_neighbors, double density, int64_t* num_points, int64_t* num_nbr_entries,
-                                   int64_t* num_cell_entries, double* points, int64_t* nbr_ptr, int32_t* nbr,
-                                   double* values, int64_t* cell_ptr, int32_t* cell_nodes, double* cell_grads,
-                                   double* cell_volumes, double* mass) {
-    const ThexPoints tp = thex_points(N, X, T, tets);
+namespace {
+
+// Neighbours of every thex point (brute force over the active nodes, sorted by the tweaked
+// squared distance, truncated to max_neighbors) and the function values there.
+void thex_functions(int64_t N, const double* X, const double* R, int32_t max_neighbors, const ThexPoints& tp,
+                    std::vector<int64_t>& ptr, std::vector<int32_t>& flat, std::vector<double>& psi) {
     const int64_t P = static_cast<int64_t>(tp.xyz.size() / 3);
     // Neighbours (brute force over the active nodes).
     std::vector<std::vector<int32_t>> nb(P);
@@ -1134,12 +1218,27 @@ extern "C" int ob_rkpm_nodal_cells(int64_t N, const double* X, int64_t T, const 
         if (static_cast<int32_t>(cand.size()) > max_neighbors) cand.resize(max_neighbors);
         for (const auto& c : cand) nb[p].push_back(c.second);
     }
-    std::vector<int64_t> ptr(P + 1, 0);
+    ptr.assign(P + 1, 0);
     for (int64_t p = 0; p < P; ++p) ptr[p + 1] = ptr[p] + static_cast<int64_t>(nb[p].size());
-    std::vector<int32_t> flat(ptr[P]);
+    flat.resize(ptr[P]);
     for (int64_t p = 0; p < P; ++p) std::copy(nb[p].begin(), nb[p].end(), flat.begin() + ptr[p]);
-    std::vector<double> psi(ptr[P]);
+    psi.resize(ptr[P]);
     ob_rk_function_values(P, tp.xyz.data(), X, R, ptr.data(), flat.data(), psi.data());
+}
+
+}  // namespace
+
+extern "C" int ob_rkpm_nodal_cells(int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R,
+                                   int32_t max_neighbors, double density, int64_t* num_points, int64_t* num_nbr_entries,
+                                   int64_t* num_cell_entries, double* points, int64_t* nbr_ptr, int32_t* nbr,
+                                   double* values, int64_t* cell_ptr, int32_t* cell_nodes, double* cell_grads,
+                                   double* cell_volumes, double* mass) {
+    const ThexPoints tp = thex_points(N, X, T, tets);
+    const int64_t P = static_cast<int64_t>(tp.xyz.size() / 3);
+    std::vector<int64_t> ptr;
+    std::vector<int32_t> flat;
+    std::vector<double> psi;
+    thex_functions(N, X, R, max_neighbors, tp, ptr, flat, psi);
     // Corner hexes of each vertex, in tet order.
     std::vector<std::vector<std::pair<int64_t, int>>> corners(N);
     for (int64_t t = 0; t < T; ++t)
@@ -1196,6 +1295,66 @@ extern "C" int ob_rkpm_nodal_cells(int64_t N, const double* X, int64_t T, const 
         for (int64_t p = 0; p < P; ++p)
             for (int64_t s = ptr[p]; s < ptr[p + 1]; ++s) mass[flat[s]] += mfe[p] * psi[s];
     }
+    return 0;
+}
+
+// Nodal cells split into subcells (subdomains 0): each corner hex keeps its own entries
+// (the union of its eight points' neighbours, first appearance order) and gradients
+// b_j = sum_k B_hex,k psi_k(j) (SmoothedCellDataProcessor.h:541-675 one-pass, with the
+// subcell volume equal to the hex volume); the hexes of a vertex, in tet order, form its
+// cell.
+extern "C" int ob_rkpm_nodal_subcells(int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R,
+                                      int32_t max_neighbors, double density, int64_t* num_cell_entries,
+                                      int64_t* cell_ptr, int32_t* cell_nodes, double* cell_grads, double* cell_volumes,
+                                      int64_t* group_ptr) {
+    (void)density;
+    const ThexPoints tp = thex_points(N, X, T, tets);
+    std::vector<int64_t> ptr;
+    std::vector<int32_t> flat;
+    std::vector<double> psi;
+    thex_functions(N, X, R, max_neighbors, tp, ptr, flat, psi);
+    std::vector<std::vector<std::pair<int64_t, int>>> corners(N);
+    for (int64_t t = 0; t < T; ++t)
+        for (int i = 0; i < 4; ++i) corners[tets[4 * t + i]].push_back({t, i});
+    std::vector<int32_t> where(N, -1);
+    std::vector<int32_t> sn;
+    std::vector<double> sg, sv;
+    std::vector<int64_t> sptr(1, 0), gptr(1, 0);
+    for (int32_t v = 0; v < N; ++v) {
+        for (const auto& ti : corners[v]) {
+            int64_t hp[8];
+            corner_hex(tp, X, tets + 4 * ti.first, ti.first, ti.second, hp);
+            double hx[24], B[24], V;
+            for (int k = 0; k < 8; ++k)
+                for (int c = 0; c < 3; ++c) hx[k * 3 + c] = tp.xyz[hp[k] * 3 + c];
+            ob_hex8_smoothed_bw(hx, B, &V);
+            const int64_t base = sptr.back();
+            std::vector<int32_t> used;
+            for (int k = 0; k < 8; ++k)
+                for (int64_t s = ptr[hp[k]]; s < ptr[hp[k] + 1]; ++s) {
+                    const int32_t j = flat[s];
+                    if (where[j] < 0) {
+                        where[j] = static_cast<int32_t>(sn.size() - base);
+                        sn.push_back(j);
+                        sg.insert(sg.end(), {0.0, 0.0, 0.0});
+                        used.push_back(j);
+                    }
+                    for (int c = 0; c < 3; ++c) sg[(base + where[j]) * 3 + c] += B[k * 3 + c] * V * psi[s];
+                }
+            for (int64_t e = base; e < static_cast<int64_t>(sn.size()); ++e)
+                for (int c = 0; c < 3; ++c) sg[e * 3 + c] /= V;
+            for (int32_t j : used) where[j] = -1;
+            sv.push_back(V);
+            sptr.push_back(static_cast<int64_t>(sn.size()));
+        }
+        gptr.push_back(static_cast<int64_t>(sv.size()));
+    }
+    if (num_cell_entries) *num_cell_entries = static_cast<int64_t>(sn.size());
+    if (cell_ptr) std::copy(sptr.begin(), sptr.end(), cell_ptr);
+    if (cell_nodes) std::copy(sn.begin(), sn.end(), cell_nodes);
+    if (cell_grads) std::copy(sg.begin(), sg.end(), cell_grads);
+    if (cell_volumes) std::copy(sv.begin(), sv.end(), cell_volumes);
+    if (group_ptr) std::copy(gptr.begin(), gptr.end(), group_ptr);
     return 0;
 }
 

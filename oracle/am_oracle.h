@@ -48,6 +48,10 @@ typedef struct {
     const int32_t* cell_nodes;  /* cells: cell_ptr[num_elems] */
     const double* cell_grads;   /* cells: 3 per entry, row-major */
     const double* cell_volumes; /* cells: num_elems */
+    /* F-bar (ComputeInternalForceSmoothedCell.h:354-413): the cells above are subcells,
+     * grouped into num_groups cells by group_ptr (num_groups + 1 offsets); NULL = none. */
+    int64_t num_groups;
+    const int64_t* group_ptr;
 } ob_block;
 
 /* One displacement/velocity boundary condition (BoundaryCondition.cpp). */
@@ -136,6 +140,16 @@ int ob_rkpm_nodal_cells(int64_t num_nodes, const double* coords, int64_t num_tet
  * (nbr_ptr N+1, nbr) with function values, cells (one per tet): cell_ptr (T+1),
  * cell_nodes, cell_grads (x3), cell_volumes (T), mass (N): rho V_t / 4 to the vertices,
  * scattered through the functions. */
+/* The same set-up with every corner hex its own subcell (nodal_smoothing_cell with
+ * subdomains 0, LabelSubcellIds in MeshLabelerProcessor.h:832-853): the cell arrays hold
+ * one entry per corner hex (vertex order, then tet order) with its own one-pass
+ * gradients b = sum_k B_hex,k psi_k and volume, and group_ptr (num_nodes + 1) groups the
+ * hexes of each vertex into its cell. num_cell_entries counts the subcell entries. */
+int ob_rkpm_nodal_subcells(int64_t num_nodes, const double* coords, int64_t num_tets, const int32_t* tets,
+                           const double* kernel_radius, int32_t max_neighbors, double density,
+                           int64_t* num_cell_entries, int64_t* cell_ptr, int32_t* cell_nodes, double* cell_grads,
+                           double* cell_volumes, int64_t* group_ptr);
+
 int ob_rkpm_element_cells(int64_t num_nodes, const double* coords, int64_t num_tets, const int32_t* tets,
                           const double* kernel_radius, int32_t max_neighbors, double density,
                           int64_t* num_nbr_entries, int64_t* num_cell_entries, int64_t* nbr_ptr, int32_t* nbr,

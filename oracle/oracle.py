@@ -26,7 +26,8 @@ MATERIAL = {"linear_elastic": 0, "neo_hookean": 1, "elastic": 2}
 class OBlock(C.Structure):
     _fields_ = [("kind", C.c_int32), ("material", C.c_int32), ("lam", C.c_double), ("mu", C.c_double),
                 ("density", C.c_double), ("mu_field", _dp), ("kappa_field", _dp), ("num_elems", C.c_int64),
-                ("conn", _ip), ("cell_ptr", _lp), ("cell_nodes", _ip), ("cell_grads", _dp), ("cell_volumes", _dp)]
+                ("conn", _ip), ("cell_ptr", _lp), ("cell_nodes", _ip), ("cell_grads", _dp), ("cell_volumes", _dp),
+                ("num_groups", C.c_int64), ("group_ptr", _lp)]
 
 
 class OBC(C.Structure):
@@ -78,6 +79,8 @@ def lib() -> C.CDLL:
                                           _dp, _lp, _ip, _dp, _lp, _ip, _dp, _dp, _dp]
         L.ob_rkpm_element_cells.argtypes = [C.c_int64, _dp, C.c_int64, _ip, _dp, C.c_int32, C.c_double, _lp, _lp,
                                             _lp, _ip, _dp, _lp, _ip, _dp, _dp, _dp]
+        L.ob_rkpm_nodal_subcells.argtypes = [C.c_int64, _dp, C.c_int64, _ip, _dp, C.c_int32, C.c_double, _lp, _lp,
+                                             _ip, _dp, _dp, _lp]
         L.ob_stable_time_increment.argtypes = [C.POINTER(OProblem), _dp, _dp, _dp, C.c_double, C.c_int32, C.c_double,
                                                C.c_double, C.c_double, _ip, _ip]
         L.ob_stable_time_increment.restype = C.c_double
@@ -113,6 +116,10 @@ class OracleProblem:
                 b.cell_nodes = _p(self._arr(p.cell_nodes, np.int32), C.c_int32)
                 b.cell_grads = _p(self._arr(p.cell_grads, np.float64))
                 b.cell_volumes = _p(self._arr(p.cell_volumes, np.float64))
+                if getattr(p, "cell_groups", None) is not None:
+                    g = self._arr(p.cell_groups, np.int64)
+                    b.num_groups = g.size - 1
+                    b.group_ptr = _p(g, C.c_int64)
             else:
                 b.conn = _p(self._arr(p.conn, np.int32), C.c_int32)
         obcs = (OBC * max(1, len(bcs)))()
@@ -300,6 +307,24 @@ def rkpm_element_cells(coords, tets, kernel_radius, max_neighbors=40, density=10
     lib().ob_rkpm_element_cells(*args, None, None, _p(out["nbr_ptr"], C.c_int64), _p(out["nbr"], C.c_int32),
                                 _p(out["values"]), _p(out["cell_ptr"], C.c_int64), _p(out["cell_nodes"], C.c_int32),
                                 _p(out["cell_grads"]), _p(out["cell_volumes"]), _p(out["mass"]))
+    return out
+
+
+def rkpm_nodal_subcells(coords, tets, kernel_radius, max_neighbors=40, density=1000.0):
+    """Oracle RKPM nodal cells split into corner-hex subcells: dict with cell_ptr,
+    cell_nodes, cell_grads, cell_volumes (per subcell) and group_ptr (per vertex)."""
+    X = np.ascontiguousarray(coords, dtype=np.float64)
+    T = np.ascontiguousarray(tets, dtype=np.int32)
+    R = np.ascontiguousarray(kernel_radius, dtype=np.float64)
+    K = C.c_int64()
+    args = (X.shape[0], _p(X), T.shape[0], _p(T, C.c_int32), _p(R), int(max_neighbors), float(density))
+    lib().ob_rkpm_nodal_subcells(*args, C.byref(K), *([None] * 5))
+    S = 4 * T.shape[0]
+    out = {"cell_ptr": np.empty(S + 1, dtype=np.int64), "cell_nodes": np.empty(K.value, dtype=np.int32),
+           "cell_grads": np.empty((K.value, 3)), "cell_volumes": np.empty(S),
+           "group_ptr": np.empty(X.shape[0] + 1, dtype=np.int64)}
+    lib().ob_rkpm_nodal_subcells(*args, None, _p(out["cell_ptr"], C.c_int64), _p(out["cell_nodes"], C.c_int32),
+                                 _p(out["cell_grads"]), _p(out["cell_volumes"]), _p(out["group_ptr"], C.c_int64))
     return out
 
 

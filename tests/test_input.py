@@ -151,7 +151,8 @@ def test_components_vector_initial_conditions_and_extensions():
     (nh_yaml().replace("neo_hookean:", "plastic:"), "not on this path"),
     (nh_yaml().replace("shear_modulus: 3.85e8, ", ""), "neo_hookean"),
     (nh_yaml().replace("gauss_quadrature: {integration_order: 1}",
-                       "strain_smoothing: {element_smoothing_cell: {subdomains: 1}, use_f_bar: true}"), "F-bar"),
+                       "strain_smoothing: {nodal_smoothing_cell: {subdomains: 2}, use_f_bar: true}").replace(
+        "finite_element: ~", "reproducing_kernel: {kernel_radius_scale_factor: 1.1}"), "num_subcells > 1"),
     (nh_yaml().replace("components: {X: 1.0, Z: -0.5}", "components: {W: 1.0}"), "component"),
     (nh_yaml().replace("gauss_quadrature: {integration_order: 1}",
                        "strain_smoothing: {element_smoothing_cell: {subdomains: 1}, force_one_pass_method: true, "
@@ -163,6 +164,16 @@ def test_components_vector_initial_conditions_and_extensions():
 def test_rejected_inputs(text, msg):
     with pytest.raises(inp.InputError, match=msg):
         inp.load(text)
+
+
+def test_f_bar_on_single_subcell_cells_is_a_no_op():
+    """ForEachCellComputeForce_Impl uses F-bar only when the cells hold several subcells;
+    element cells hold one (MeshLabelerProcessor.h:855-870), so use_f_bar changes nothing."""
+    base = "strain_smoothing: {element_smoothing_cell: {subdomains: 1}%s}"
+    plain = inp.load(nh_yaml().replace("gauss_quadrature: {integration_order: 1}", base % ""))
+    fbar = inp.load(nh_yaml().replace("gauss_quadrature: {integration_order: 1}", base % ", use_f_bar: true"))
+    assert fbar.parts[0].cell_groups is None
+    assert np.array_equal(fbar.parts[0].cell_grads, plain.parts[0].cell_grads)
 
 
 def test_strain_smoothing_part_from_yaml():
@@ -239,6 +250,25 @@ def test_yaml_rkpm_two_pass_default_matches_oracle(oracle_lib, precision):
 
     up = apply_functions(sim.rk, u)
     assert np.linalg.norm(r["physical_displacement"] - up) <= tol * np.linalg.norm(up)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("use_f_bar", [True, False])
+def test_yaml_rkpm_nodal_subcells_match_oracle(oracle_lib, use_f_bar):
+    """nodal_smoothing_cell with subdomains 0 (one subcell per corner hex), with and
+    without use_f_bar, as the reference's rkpm_fbar Taylor-bar input sets it up."""
+    text = nh_yaml(n=3).replace(
+        "gauss_quadrature: {integration_order: 1}",
+        f"strain_smoothing: {{nodal_smoothing_cell: {{subdomains: 0}}, use_f_bar: {str(use_f_bar).lower()}}}").replace(
+        "finite_element: ~", "reproducing_kernel: {kernel_radius_scale_factor: 1.1}")
+    sim = inp.load(text)
+    part = sim.parts[0]
+    assert part.num_elems == 4 * 6 * 27 and (part.cell_groups is not None) == use_f_bar
+    r = inp.run(sim)
+    prob = oracle_lib.OracleProblem(sim.coords, sim.parts, sim.bcs, mass=sim.mass)
+    u, v, a, n = prob.solve(np.zeros_like(sim.coords), sim.v0, sim.dt, sim.time_end)
+    assert r["steps"] == n
+    assert np.linalg.norm(r["displacement"] - u) <= 1e-12 * np.linalg.norm(u)
 
 
 @pytest.mark.gpu
