@@ -147,6 +147,45 @@ def rkpm_box(n: int = 46, seed: int = 0, nsteps: int = 500, jitter: float = 0.2,
                     "config": f"RKPM one-pass nodal cells, R={radius}h, cap {max_neighbors}, neo-Hookean"})
 
 
+def rkpm_fbar_box(n: int = 32, seed: int = 0, nsteps: int = 500, jitter: float = 0.2, radius: float = 1.8,
+                  max_neighbors: int = 40) -> Problem:
+    """RKPM nodal cells split into one subcell per corner hex with F-bar over each
+    vertex's subcells (nodal_smoothing_cell subdomains 0 + use_f_bar, the reference's
+    rkpm_fbar Taylor-bar formulation) on the jittered 1 x 1 x 2 lattice, neo-Hookean."""
+    from .rkpm import nodal_subcells
+
+    rng, coords, tets = _box_tets(n, seed, jitter)
+    mat = Material.create("neo_hookean", 1000.0, shear_modulus=3.85e8, bulk_modulus=8.33e8)
+    cells = nodal_subcells(coords, tets, mat, np.full(coords.shape[0], radius / n), max_neighbors=max_neighbors)
+    fixed = mesh.side_sets(coords)["surface_5"]
+    v0 = _initial_velocity(coords, fixed, rng, shear=1.0)
+    dt = 0.5 * float(mesh.tet_char_length(coords, tets).min()) / wave_speed(mat.lam, mat.mu, mat.density)
+    return Problem(f"rkpm_fbar_box_{n}", coords, [cells.part], [BoundaryCondition.fixed(fixed)], v0, dt, nsteps, seed,
+                   {"mass": cells.mass, "entries_per_cell": cells.entries_per_cell,
+                    "config": f"RKPM nodal subcells (corner hexes) with F-bar, R={radius}h, cap {max_neighbors}, "
+                              "neo-Hookean"})
+
+
+def rkpm_two_pass_box(n: int = 46, seed: int = 0, nsteps: int = 500, jitter: float = 0.2, scale: float = 1.1,
+                      max_neighbors: int = 40) -> Problem:
+    """RKPM element cells with the two-pass method (the reference's default for
+    element_smoothing_cell): FEM smoothed tets on the physical displacement, coupled to
+    the coefficients through the functions at the vertices, kernel radius scale x the
+    longest edge, neo-Hookean."""
+    from .rkpm import tet_max_edge_length, two_pass_element_cells
+
+    rng, coords, tets = _box_tets(n, seed, jitter)
+    mat = Material.create("neo_hookean", 1000.0, shear_modulus=3.85e8, bulk_modulus=8.33e8)
+    cells = two_pass_element_cells(coords, tets, mat, scale * tet_max_edge_length(coords, tets),
+                                   max_neighbors=max_neighbors)
+    fixed = mesh.side_sets(coords)["surface_5"]
+    v0 = _initial_velocity(coords, fixed, rng, shear=1.0)
+    dt = 0.5 * float(mesh.tet_char_length(coords, tets).min()) / wave_speed(mat.lam, mat.mu, mat.density)
+    return Problem(f"rkpm_two_pass_box_{n}", coords, [cells.part], [BoundaryCondition.fixed(fixed)], v0, dt, nsteps,
+                   seed, {"mass": cells.mass, "rk": cells.functions(),
+                          "config": f"RKPM two-pass element cells, scale {scale}, cap {max_neighbors}, neo-Hookean"})
+
+
 def tet4_nh_shear_slab(n: int = 70, rank: int = 0, world: int = 1, seed: int = 0, nsteps: int = 1000,
                        jitter: float = 0.2) -> Problem:
     """One rank's slab of the weak-scaled tet4_nh_shear mesh: world slabs of n^3 hexes

@@ -52,8 +52,10 @@ def parse():
     ap.add_argument("--adjoint-n", type=int, default=64)
     ap.add_argument("--box-n", type=int, default=46, help="lattice cells per unit length of the 1x1x2 box workloads")
     ap.add_argument("--hex-n", type=int, default=128, help="hexes per edge of the large Hex8 workload")
+    ap.add_argument("--fbar-n", type=int, default=32, help="lattice cells per unit length of the F-bar RKPM box")
     ap.add_argument("--workload", default="tet4_nh_shear",
-                    choices=["tet4_nh_shear", "hex8_nh_lognormal", "hex8_le_cube", "smoothed_tet4_box", "rkpm_box"],
+                    choices=["tet4_nh_shear", "hex8_nh_lognormal", "hex8_le_cube", "smoothed_tet4_box", "rkpm_box",
+                             "rkpm_fbar_box", "rkpm_two_pass_box"],
                     help="workload of the headline timing (the default is the headline configuration; the others "
                          "exist to profile one kernel at a time)")
     ap.add_argument("--skip-extras", action="store_true")
@@ -294,12 +296,23 @@ def algorithmic_bytes(prob, layout, slot_bytes=12):
     S = layout["used_slots"]
     elem = 48 * N + slot_bytes * S
     node = slot_bytes * S + (8 + 4 + 4 + 96) * N
+    r = slot_bytes // 3
     for p in prob.parts:
         if p.kind == "cells":
             elem += (4 + slot_bytes) * int(p.cell_ptr[-1])
+            if p.cell_groups is not None:
+                # F-bar passes: H and J written and read back, the barred stress written
+                # and replaced, the subcell stress read, and the entries read a second time.
+                elem += 38 * r * p.num_elems + (4 + slot_bytes) * int(p.cell_ptr[-1])
         else:
             elem += 4 * p.conn.size
         elem += 8 * p.num_elems * ((p.mu_field is not None) + (p.kappa_field is not None))
+    rk = prob.meta.get("rk")
+    if rk is not None:
+        # two-pass coupling: the functions read twice (row and transposed, 12 B per entry),
+        # the physical displacement written (32 B), the local force written and read (48 B)
+        # and the generalized force written and read (48 B) per node.
+        elem += 24 * int(rk[0][-1]) + 128 * N
     return {"element": elem, "node": node}
 
 
@@ -352,7 +365,8 @@ def measure_workload(torch, prob, steps, warmup, stream, dev, world, mass=None, 
     out = {"workload": prob.name, "elements": prob.num_elems, "nodes": prob.num_nodes, "steps": steps,
            "dt": prob.dt, "config": prob.meta.get("config")}
     peak, kind = measured_peaks()
-    with ExplicitDynamics(prob.coords, prob.parts, prob.bcs, mass=mass, stream=stream.cuda_stream) as m:
+    with ExplicitDynamics(prob.coords, prob.parts, prob.bcs, mass=mass, stream=stream.cuda_stream,
+                          rk=prob.meta.get("rk")) as m:
         layout = m.layout()
         states = {}
         for prec in precs:
@@ -452,6 +466,10 @@ def make_problem(args, rank=0, world=1):
         return problems.hex8_le_cube(n=20, seed=0, nsteps=args.steps)
     if w == "smoothed_tet4_box":
         return problems.smoothed_tet4_box(n=args.box_n, seed=0, nsteps=args.steps)
+    if w == "rkpm_fbar_box":
+        return problems.rkpm_fbar_box(n=args.fbar_n, seed=0, nsteps=args.steps)
+    if w == "rkpm_two_pass_box":
+        return problems.rkpm_two_pass_box(n=args.box_n, seed=0, nsteps=args.steps)
     return problems.rkpm_box(n=args.box_n, seed=0, nsteps=args.steps)
 
 
@@ -467,7 +485,8 @@ def run_ours(args, rank, world, local):
     stream = torch.cuda.Stream(device=dev)
     res = {}
     mass = decomposed_setup(args, prob, rank, world, dev) if args.decompose else prob.meta.get("mass")
-    model = ExplicitDynamics(prob.coords, prob.parts, prob.bcs, mass=mass, stream=stream.cuda_stream)
+    model = ExplicitDynamics(prob.coords, prob.parts, prob.bcs, mass=mass, stream=stream.cuda_stream,
+                             rk=prob.meta.get("rk"))
     if args.decompose:
         attach_interface(model, prob, rank, world)
     layout = model.layout()
@@ -530,6 +549,19 @@ def run_ours(args, rank, world, local):
         r["setup_s"] = setup_s
         r["entries_per_cell"] = p3b.meta["entries_per_cell"]
         extras["rkpm_box"] = r
+        t0 = time.perf_counter()
+        p3c = problems.rkpm_fbar_box(n=args.fbar_n, seed=0, nsteps=200)
+        setup_s = time.perf_counter() - t0
+        r = measure_workload(torch, p3c, 200, args.warmup, stream, dev, world, mass=p3c.meta["mass"])
+        r["setup_s"] = setup_s
+        r["entries_per_subcell"] = p3c.meta["entries_per_cell"]
+        extras["rkpm_fbar_box"] = r
+        t0 = time.perf_counter()
+        p3d = problems.rkpm_two_pass_box(n=args.box_n, seed=0, nsteps=500)
+        setup_s = time.perf_counter() - t0
+        r = measure_workload(torch, p3d, 500, args.warmup, stream, dev, world, mass=p3d.meta["mass"])
+        r["setup_s"] = setup_s
+        extras["rkpm_two_pass_box"] = r
         p5 = problems.hex8_nh_lognormal(n=args.hex_n, seed=0, nsteps=1000, bulk_field=True)
         extras["hex8_nh_lognormal_large"] = measure_workload(torch, p5, 1000, args.warmup, stream, dev, world)
         if not args.skip_adjoint:
