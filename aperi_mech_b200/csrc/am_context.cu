@@ -103,6 +103,10 @@ struct Block {
     float* grads32 = nullptr;
     double* volumes = nullptr;
     int32_t max_entries = 0;
+    // Updated / semi-Lagrangian state (am_set_formulation): H of the last force evaluation
+    // and the semi formulation's reference H, 9 per element.
+    double* hstate = nullptr;
+    double* href = nullptr;
     // F-bar cells (am_set_cell_groups): the cells are subcells grouped by group_ptr.
     int64_t num_groups = 0;
     int64_t* group_ptr = nullptr;
@@ -135,6 +139,8 @@ struct Block {
         g.patch_nodes = patch_nodes;
         g.patch_local = patch_local;
         g.patch_gather = patch_gather;
+        g.hstate = hstate;
+        g.href = href;
         return g;
     }
     am::CellBlockDev cells() const {
@@ -185,6 +191,8 @@ struct Block {
         dfree(patch_nodes);
         dfree(patch_local);
         dfree(patch_gather);
+        dfree(hstate);
+        dfree(href);
         dfree(group_ptr);
         dfree(fbar64);
         dfree(fbar32);
@@ -311,6 +319,13 @@ struct am_ctx {
     double* pm_fe = nullptr;          // N x 3: F(u + v l eps)
     double* pm_partial = nullptr;     // per-block sums of squares
     bool pm_initialized = false;
+    // Updated / semi-Lagrangian formulation (am_set_formulation).
+    int32_t lagr = 0;                 // 0 total, 1 updated, 2 semi
+    int32_t lagr_interval = 1;        // semi: steps between reference updates
+    int64_t lagr_steps = 0;           // steps completed since the state was set
+    bool lagr_rebased = false;        // the element H of step lagr_steps is already the reference
+    double4* xc = nullptr;            // current (updated) or reference (semi) coordinates
+    double4* lagr_inc = nullptr;      // displacement increment
     // Two-pass reproducing-kernel coupling (am_set_rk_functions).
     int64_t* rk_ptr = nullptr;        // N + 1: rows of Psi
     int32_t* rk_nbr = nullptr;
@@ -342,6 +357,9 @@ struct am_ctx {
             nd.iface_f = iface_buf;
         }
         nd.f_given = rk_f;
+        nd.lagr = lagr;
+        nd.xc = xc;
+        nd.inc = lagr_inc;
         return nd;
     }
 
@@ -369,6 +387,19 @@ struct am_ctx {
     // to the generalized force Psi^T f, which the node kernels then read (f_given).
     void element_forces(int mixed, const double4* U) {
         void* s = slots(mixed);
+        if (lagr) {
+            // The semi formulation's reference configuration moved after the last step
+            // (StepScheduler at update_interval, src/Application.cpp:301-308): the element
+            // kernels take the stored H as the reference gradient first.
+            const int rebase = (lagr == 2 && lagr_steps > 0 && lagr_steps % lagr_interval == 0 && !lagr_rebased) ? 1 : 0;
+            for (auto& b : blocks) {
+                am::launch_gauss_force_lagr(b.gauss(), lagr, rebase, xc, lagr_inc, s, status, stream);
+                ++launches;
+            }
+            if (rebase) lagr_rebased = true;
+            check_launch("element force kernel");
+            return;
+        }
         if (rk_ptr) {
             am::launch_rk_rows4(N, rk_ptr, rk_nbr, rk_val, U, rk_u, stream);
             ++launches;
@@ -419,6 +450,7 @@ struct am_ctx {
                                  int32_t* iterations, int32_t* converged_out) {
         if (!pm_l) fail(AM_ESTATE, "am_set_power_method first");
         if (iface_row_of) fail(AM_ESTATE, "the power method is not available on a decomposed mesh");
+        if (lagr) fail(AM_ESTATE, "the power method is built for the total formulation");
         if (num_iterations < 1 || !(eps > 0.0) || !(tol > 0.0)) fail(AM_EINVAL, "bad power-method parameters");
         if (!pm_initialized) {
             // InitializeEigenvector: the start vector scaled by eps times the node's edge length.
@@ -612,7 +644,10 @@ struct am_ctx {
         const am::NodeDev nd = node_dev();
         void* s = slots(mixed);
         mark(-1, 0);
-        am::launch_prologue(nd, table + n0, U4, V4, A4, u_hist ? u_hist[0] : nullptr, stream);
+        // Semi formulation: a reference update due at the end of the previous run moves the
+        // coordinates in this run's first displacement update.
+        const auto due = [&](int64_t done) { return lagr == 2 && done > 0 && done % lagr_interval == 0; };
+        am::launch_prologue(nd, table + n0, U4, V4, A4, u_hist ? u_hist[0] : nullptr, due(lagr_steps) ? 1 : 0, stream);
         ++launches;
         check_launch("prologue kernel");
         mark(1, 1);
@@ -625,7 +660,12 @@ struct am_ctx {
             }
             const int advance = (n + 1 < n1) ? 1 : 0;
             double4* uc = (u_hist && advance) ? u_hist[n + 1 - n0] : nullptr;
-            am::launch_node_step(nd, mixed, s, table, n, advance, U4, V4, A4, uc, status, stream);
+            if (lagr) {
+                ++lagr_steps;
+                lagr_rebased = false;
+            }
+            am::launch_node_step(nd, mixed, s, table, n, advance, U4, V4, A4, uc, status, stream,
+                                 due(lagr_steps) ? 1 : 0);
             ++launches;
             check_launch("node step kernel");
             mark(1, 1);
@@ -633,11 +673,24 @@ struct am_ctx {
     }
 
     void init_acceleration(int mixed) {
+        if (lagr && mixed) fail(AM_EINVAL, "the updated/semi formulations run in FP64");
         element_forces(mixed, U4);
         exchange(mixed);
         am::launch_init_accel(node_dev(), mixed, slots(mixed), A4, status, stream);
         ++launches;
         check_launch("init acceleration kernel");
+    }
+
+    // Updated / semi state at the undeformed start: coordinates X, no increment, H = 0.
+    void reset_lagrangian() {
+        ck(cudaMemcpyAsync(xc, X4, N * sizeof(double4), cudaMemcpyDeviceToDevice, stream), "copy");
+        ck(cudaMemsetAsync(lagr_inc, 0, N * sizeof(double4), stream), "memset");
+        for (auto& b : blocks) {
+            ck(cudaMemsetAsync(b.hstate, 0, static_cast<size_t>(b.num_elems) * 9 * sizeof(double), stream), "memset");
+            if (b.href) ck(cudaMemsetAsync(b.href, 0, static_cast<size_t>(b.num_elems) * 9 * sizeof(double), stream), "memset");
+        }
+        lagr_steps = 0;
+        lagr_rebased = false;
     }
 
     void require_finalized() const {
@@ -667,6 +720,8 @@ struct am_ctx {
         dfree(pm_fu);
         dfree(pm_fe);
         dfree(pm_partial);
+        dfree(xc);
+        dfree(lagr_inc);
         dfree(rk_ptr);
         dfree(rk_nbr);
         dfree(rk_val);
@@ -748,6 +803,7 @@ void store_nodal(am_ctx* c, am_memory where, const double4* src, double* dst) {
 void run_schedule(am_ctx* c, int prec, const std::vector<double>& dts, double t0) {
     c->require_finalized();
     if (prec != AM_FP64 && prec != AM_MIXED) fail(AM_EINVAL, "unknown precision");
+    if (c->lagr && prec != AM_FP64) fail(AM_EINVAL, "the updated/semi formulations run in FP64");
     for (double d : dts)
         if (!(d >= 0.0) || !std::isfinite(d)) fail(AM_EINVAL, "time increments must be finite and non-negative");
     if (dts.empty()) return;
@@ -877,6 +933,7 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
         const int64_t E = d->num_elems;
         try {
             if (d->kind == AM_SMOOTHED_CELLS) {
+                if (ctx->lagr) fail(AM_EINVAL, "the updated/semi formulations are built for Gauss elements");
                 if (E > 0 && (!d->cell_ptr || !d->cell_nodes || !d->cell_grads || !d->cell_volumes))
                     fail(AM_EINVAL, "cell block needs cell_ptr, cell_nodes, cell_grads and cell_volumes");
                 const int64_t K = E > 0 ? d->cell_ptr[E] : 0;
@@ -928,7 +985,7 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
                     ck(cudaMemcpy(b.conn, d->conn, S * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
                 }
                 b.host_nodes.assign(d->conn, d->conn + S);
-                if (d->kind == AM_TET4_GAUSS && E > 0 && ctx->tet4_patches) {
+                if (d->kind == AM_TET4_GAUSS && E > 0 && ctx->tet4_patches && ctx->lagr == 0) {
                     // Patch the tets when patches hold 2.5 tets or more on average; fewer
                     // would leave most of the eight lanes per patch idle.
                     TetPatches tp = build_tet_patches(d->conn, E);
@@ -1137,6 +1194,16 @@ int am_finalize(am_ctx* ctx) {
             ck(cudaMemcpy(ctx->mass, m.data(), N * sizeof(double), cudaMemcpyHostToDevice), "mass upload");
             ctx->mass_set = true;
         }
+        if (ctx->lagr) {
+            ctx->xc = dalloc<double4>(N, "current coordinates");
+            ctx->lagr_inc = dalloc<double4>(N, "displacement increment");
+            for (auto& b : ctx->blocks) {
+                const size_t n9 = static_cast<size_t>(std::max<int64_t>(b.num_elems, 1)) * 9;
+                b.hstate = dalloc<double>(n9, "element H");
+                if (ctx->lagr == 2) b.href = dalloc<double>(n9, "reference H");
+            }
+            ctx->reset_lagrangian();
+        }
         ctx->finalized = true;
     });
 }
@@ -1155,6 +1222,7 @@ int am_set_state(am_ctx* ctx, am_memory where, const double* u, const double* v,
         load_nodal(ctx, where, u, ctx->U4);
         load_nodal(ctx, where, v, ctx->V4);
         load_nodal(ctx, where, a, ctx->A4);
+        if (u && ctx->lagr) ctx->reset_lagrangian();
         if (where == AM_HOST) ck(cudaStreamSynchronize(ctx->stream), "synchronize");
     });
 }
@@ -1173,6 +1241,7 @@ int am_internal_force(am_ctx* ctx, am_precision prec, am_memory where, const dou
     return guarded(ctx, [&] {
         ctx->require_finalized();
         if (!u || !f) fail(AM_EINVAL, "null u or f");
+        if (ctx->lagr) fail(AM_ESTATE, "am_internal_force evaluates the total formulation");
         const int mixed = prec == AM_MIXED;
         load_nodal(ctx, where, u, ctx->W4);
         ctx->reset_status();
@@ -1303,6 +1372,7 @@ int am_vjp_force(am_ctx* ctx, am_memory where, const double* u, const double* la
         ctx->require_finalized();
         if (ctx->iface_row_of) fail(AM_ESTATE, "the VJP is not available on a decomposed mesh");
         if (ctx->rk_ptr) fail(AM_ESTATE, "the VJP is not available with the two-pass coupling");
+        if (ctx->lagr) fail(AM_ESTATE, "the VJP is built for the total formulation");
         for (const auto& b : ctx->blocks)
             if (b.group_ptr) fail(AM_ESTATE, "the VJP is not available on F-bar cells");
         if (!u || !lam || !gu) fail(AM_EINVAL, "null u, lam or gu");
@@ -1342,6 +1412,7 @@ int am_adjoint(am_ctx* ctx, int64_t nsteps, double dt, int32_t ckpt_every, int32
         ctx->require_finalized();
         if (ctx->iface_row_of) fail(AM_ESTATE, "the adjoint is not available on a decomposed mesh");
         if (ctx->rk_ptr) fail(AM_ESTATE, "the adjoint is not available with the two-pass coupling");
+        if (ctx->lagr) fail(AM_ESTATE, "the adjoint is built for the total formulation");
         for (const auto& b : ctx->blocks)
             if (b.group_ptr) fail(AM_ESTATE, "the adjoint is not available on F-bar cells");
         if (nsteps <= 0 || !(dt > 0.0)) fail(AM_EINVAL, "nsteps and dt must be positive");
@@ -1558,6 +1629,7 @@ int am_set_interface(am_ctx* ctx, int64_t num_local, const int32_t* local_nodes,
             fail(AM_ESTATE, "a decomposed mesh needs the global lumped mass from am_set_mass before am_finalize");
         if (ctx->iface_row_of) fail(AM_ESTATE, "interface already set");
         if (ctx->rk_ptr) fail(AM_ESTATE, "a decomposed mesh with the two-pass coupling is not built");
+        if (ctx->lagr) fail(AM_ESTATE, "a decomposed mesh runs the total formulation");
         if (num_local < 0 || num_global < num_local || (num_local > 0 && (!local_nodes || !rows)))
             fail(AM_EINVAL, "bad interface arrays");
         if (num_global >= (int64_t(1) << 31)) fail(AM_ERANGE, "interface beyond int32 indexing");
@@ -1581,6 +1653,19 @@ int am_set_interface(am_ctx* ctx, int64_t num_local, const int32_t* local_nodes,
             ck(cudaMemcpy(ctx->iface_nodes, local_nodes, num_local * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
             ck(cudaMemcpy(ctx->iface_rows, rows, num_local * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
         }
+    });
+}
+
+int am_set_formulation(am_ctx* ctx, int32_t formulation, int32_t update_interval) {
+    if (!ctx) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        // Before the blocks: the element state is per element, so Tet4 blocks keep one
+        // slot per element node instead of element patches.
+        if (ctx->finalized || !ctx->blocks.empty()) fail(AM_ESTATE, "am_set_formulation comes before am_add_block");
+        if (formulation < 0 || formulation > 2) fail(AM_EINVAL, "formulation: 0 total, 1 updated, 2 semi");
+        if (formulation == 2 && update_interval < 1) fail(AM_EINVAL, "update_interval must be at least 1");
+        ctx->lagr = formulation;
+        ctx->lagr_interval = formulation == 2 ? update_interval : 1;
     });
 }
 

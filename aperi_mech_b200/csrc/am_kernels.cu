@@ -491,6 +491,178 @@ __global__ void __launch_bounds__(sizeof(T) == 8 ? 64 : 128, sizeof(T) == 8 ? 1 
 }
 
 // ---------------------------------------------------------------------------
+// Updated / semi-Lagrangian Gauss elements, FP64 (ComputeInternalForceGaussian.h:57-131 with
+// ComputeInternalForceBase.h:158-174): shape-function gradients on the coordinates xc
+// (current coordinates at the start of the step, or the semi formulation's reference
+// coordinates), dH = inc^T B, H = dH + Href + dH Href, P(H); the force maps back through
+// F_ref = I + Href: B F_ref and w / det F_ref. The element keeps one H (for Hex8 the last
+// Gauss point's, as the reference's element field), which is also every Gauss point's Href.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void lagr_href(const GaussBlockDev& b, int64_t e, int32_t lagr, int rebase, double* hr) {
+    const double* src = (lagr == 1 || rebase) ? b.hstate + 9 * e : b.href + 9 * e;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) hr[k] = src[k];
+    if (lagr == 2 && rebase) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) b.href[9 * e + k] = hr[k];
+    }
+}
+
+// H = dH + Href + dH Href
+__device__ __forceinline__ void lagr_compose(const double* dH, const double* hr, double* H) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            H[i * 3 + j] = dH[i * 3 + j] + hr[i * 3 + j] +
+                           (dH[i * 3 + 0] * hr[0 * 3 + j] + dH[i * 3 + 1] * hr[1 * 3 + j] + dH[i * 3 + 2] * hr[2 * 3 + j]);
+}
+
+// Pm = P F_ref^T / det F_ref, so that B P'^T w = (B F_ref) P^T (w / det F_ref).
+__device__ __forceinline__ void lagr_pull(const double* hr, const double* P, double* Pm) {
+    double Fr[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Fr[k] = hr[k] + ((k % 4 == 0) ? 1.0 : 0.0);
+    const double idet = 1.0 / det3(Fr);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+            Pm[i * 3 + m] = (P[i * 3 + 0] * Fr[m * 3 + 0] + P[i * 3 + 1] * Fr[m * 3 + 1] + P[i * 3 + 2] * Fr[m * 3 + 2]) * idet;
+}
+
+template <int MAT>
+__global__ void __launch_bounds__(128) k_tet4_force_lagr(GaussBlockDev b, int32_t lagr, int rebase,
+                                                          const double4* __restrict__ XC,
+                                                          const double4* __restrict__ INC,
+                                                          double4* __restrict__ slots, int* status) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= b.num_elems) return;
+    const int4 c = reinterpret_cast<const int4*>(b.conn)[e];
+    const double4 x0 = XC[c.x], x1 = XC[c.y], x2 = XC[c.z], x3 = XC[c.w];
+    const double4 u0 = INC[c.x], u1 = INC[c.y], u2 = INC[c.z], u3 = INC[c.w];
+    const double J[9] = {x1.x - x0.x, x2.x - x0.x, x3.x - x0.x, x1.y - x0.y, x2.y - x0.y,
+                         x3.y - x0.y, x1.z - x0.z, x2.z - x0.z, x3.z - x0.z};
+    const double D[9] = {u1.x - u0.x, u2.x - u0.x, u3.x - u0.x, u1.y - u0.y, u2.y - u0.y,
+                         u3.y - u0.y, u1.z - u0.z, u2.z - u0.z, u3.z - u0.z};
+    const double det = det3(J);
+    if (!(det > 0.0)) flag(status, AM_ENONPOS_J, e);
+    double Ji[9];
+    cof_inv3(J, Ji, det);
+    const double w = det / 6.0;
+    double dH[9], hr[9], H[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) dH[i * 3 + j] = D[i * 3 + 0] * Ji[0 * 3 + j] + D[i * 3 + 1] * Ji[1 * 3 + j] + D[i * 3 + 2] * Ji[2 * 3 + j];
+    lagr_href(b, e, lagr, rebase, hr);
+    lagr_compose(dH, hr, H);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) b.hstate[9 * e + k] = H[k];
+    double lam, mu;
+    element_lame(b, e, lam, mu);
+    double P[9], Pm[9];
+    const double Jf = stress<double>(MAT, lam, mu, H, P);
+    if (MAT == kNeoHookean && !(Jf > 0.0)) flag(status, AM_ENONPOS_J, e);
+    lagr_pull(hr, P, Pm);
+    double f[12];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) f[i] = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const double q = w * (Ji[k * 3 + 0] * Pm[i * 3 + 0] + Ji[k * 3 + 1] * Pm[i * 3 + 1] + Ji[k * 3 + 2] * Pm[i * 3 + 2]);
+            f[(k + 1) * 3 + i] = -q;
+            f[i] += q;
+        }
+    slots[b.slot_pos[4 * e]] = make4(f[0], f[1], f[2]);
+    slots[b.slot_pos[4 * e + 1]] = make4(f[3], f[4], f[5]);
+    slots[b.slot_pos[4 * e + 2]] = make4(f[6], f[7], f[8]);
+    slots[b.slot_pos[4 * e + 3]] = make4(f[9], f[10], f[11]);
+}
+
+template <int MAT>
+__global__ void __launch_bounds__(64) k_hex8_force_lagr(GaussBlockDev b, int32_t lagr, int rebase,
+                                                         const double4* __restrict__ XC,
+                                                         const double4* __restrict__ INC,
+                                                         double4* __restrict__ slots, int* status) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= b.num_elems) return;
+    int32_t nd[8];
+    hex_conn(b, e, nd);
+    double X[3][8], U[3][8];
+    hex_load_rel(XC, nd, X);
+    hex_load_rel(INC, nd, U);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        hex_butterfly(X[i]);
+        hex_butterfly(U[i]);
+        hex_scale_coeffs(X[i]);
+        hex_scale_coeffs(U[i]);
+    }
+    double lam, mu;
+    element_lame(b, e, lam, mu);
+    double hr[9];
+    lagr_href(b, e, lagr, rebase, hr);
+    double R[3][8];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int k = 0; k < 8; ++k) R[i][k] = 0.0;
+    bool bad = false;
+    for (int g = 0; g < 8; ++g) {
+        double J[9], G[9], A[9];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                J[i * 3 + j] = hex_dxi(X[i], j, g);
+                G[i * 3 + j] = hex_dxi(U[i], j, g);
+            }
+        adj3(J, A);
+        const double det = J[0] * A[0] + J[1] * A[3] + J[2] * A[6];
+        bad |= !(det > 0.0);
+        const double id = 1.0 / det;
+        double dH[9], H[9], P[9], Pm[9];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+                dH[i * 3 + j] = (G[i * 3 + 0] * A[0 * 3 + j] + G[i * 3 + 1] * A[1 * 3 + j] + G[i * 3 + 2] * A[2 * 3 + j]) * id;
+        lagr_compose(dH, hr, H);
+        // The reference's last Gauss point (its node 7 sign pattern) is corner 6 here.
+        if (g == 6) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) b.hstate[9 * e + k] = H[k];
+        }
+        const double Jf = stress<double>(MAT, lam, mu, H, P);
+        if (MAT == kNeoHookean) bad |= !(Jf > 0.0);
+        lagr_pull(hr, P, Pm);
+        double Q[9];
+#pragma unroll
+        for (int kk = 0; kk < 3; ++kk)
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                Q[kk * 3 + i] = A[kk * 3 + 0] * Pm[i * 3 + 0] + A[kk * 3 + 1] * Pm[i * 3 + 1] + A[kk * 3 + 2] * Pm[i * 3 + 2];
+        hex_accumulate_r(R, Q, g);
+    }
+    if (bad) flag(status, AM_ENONPOS_J, e);
+    int32_t pos[8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) pos[a] = b.slot_pos[8 * e + a];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        R[i][0] = 0.0;
+        hex_scale_coeffs(R[i]);
+        hex_butterfly_t(R[i]);
+    }
+    const double sc = -1.0 / 512.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) slots[pos[hex_node_of_corner(q)]] = make4(sc * R[0][q], sc * R[1][q], sc * R[2][q]);
+}
+
+// ---------------------------------------------------------------------------
 // Smoothed / RKPM cells (ComputeInternalForceSmoothedCell.h:416-442, no F-bar):
 // H = sum_k u_k (x) b_k ; P(H) ; f_k = -V b_k P^T written to the cell's slots.
 // The mixed path subtracts the first entry's displacement (partition of nullity
@@ -1234,9 +1406,40 @@ __global__ void __launch_bounds__(kNodeBlock) k_init_accel(NodeDev nd, const vec
     A4[i] = make_double4(ax, ay, az, 0.0);
 }
 
+// Displacement update d^{n+1} = d^n + dt v^{n+1/2}. Under the updated / semi formulations
+// (UpdateDisplacementsUpdatedFunctor, ExplicitTimeIntegrator.h:141-244) the increment
+// dt v (rounded once) also feeds inc: the updated formulation first moves xc by the last
+// step's increment (the current coordinates advance every step) and replaces inc; the
+// semi formulation accumulates inc, after moving xc by it and clearing it when the
+// reference configuration was just updated (rebase).
+__device__ __forceinline__ void displace(const NodeDev& nd, int64_t i, int rebase, double dt, double vx, double vy,
+                                         double vz, double4& u) {
+    if (nd.lagr == 0) {
+        u.x = u.x + dt * vx;
+        u.y = u.y + dt * vy;
+        u.z = u.z + dt * vz;
+        return;
+    }
+    const double dx = __dmul_rn(dt, vx), dy = __dmul_rn(dt, vy), dz = __dmul_rn(dt, vz);
+    u.x = __dadd_rn(u.x, dx);
+    u.y = __dadd_rn(u.y, dy);
+    u.z = __dadd_rn(u.z, dz);
+    double4 q = nd.inc[i];
+    if (nd.lagr == 1 || rebase) {
+        double4 x = nd.xc[i];
+        x.x = __dadd_rn(x.x, q.x);
+        x.y = __dadd_rn(x.y, q.y);
+        x.z = __dadd_rn(x.z, q.z);
+        nd.xc[i] = x;
+        q = make_double4(0.0, 0.0, 0.0, 0.0);
+    }
+    nd.inc[i] = make_double4(__dadd_rn(q.x, dx), __dadd_rn(q.y, dy), __dadd_rn(q.z, dz), 0.0);
+}
+
 __global__ void __launch_bounds__(256) k_prologue(NodeDev nd, const StepParams* __restrict__ table,
                                                    double4* __restrict__ U4, double4* __restrict__ V4,
-                                                   const double4* __restrict__ A4, double4* __restrict__ u_copy) {
+                                                   const double4* __restrict__ A4, double4* __restrict__ u_copy,
+                                                   int rebase) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= nd.num_nodes) return;
     const StepParams& P = table[0];
@@ -1245,9 +1448,7 @@ __global__ void __launch_bounds__(256) k_prologue(NodeDev nd, const StepParams* 
     const uint32_t w = nd.bcword[i];
     if (w) apply_bc(w, P.vact, P.vscale, nd.bcvalues, vx, vy, vz);
     double4 u = U4[i];
-    u.x = u.x + P.dt * vx;
-    u.y = u.y + P.dt * vy;
-    u.z = u.z + P.dt * vz;
+    displace(nd, i, rebase, P.dt, vx, vy, vz, u);
     U4[i] = u;
     V4[i] = make_double4(vx, vy, vz, 0.0);
     if (u_copy) u_copy[i] = u;
@@ -1258,7 +1459,7 @@ __global__ void __launch_bounds__(kNodeBlock) k_node_step(NodeDev nd, const vec4
                                                            const StepParams* __restrict__ table, int64_t step,
                                                            int advance, double4* __restrict__ U4,
                                                            double4* __restrict__ V4, double4* __restrict__ A4,
-                                                           double4* __restrict__ u_copy, int* status) {
+                                                           double4* __restrict__ u_copy, int* status, int rebase) {
     const int64_t i = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / LPN;
     const bool own = i < nd.num_nodes;
     if (LPN == 1 && !own) return;
@@ -1290,9 +1491,7 @@ __global__ void __launch_bounds__(kNodeBlock) k_node_step(NodeDev nd, const vec4
         double wx = vx + Q.half * ax, wy = vy + Q.half * ay, wz = vz + Q.half * az;
         if (w) apply_bc(w, Q.vact, Q.vscale, nd.bcvalues, wx, wy, wz);
         double4 u = u0;
-        u.x = u.x + Q.dt * wx;
-        u.y = u.y + Q.dt * wy;
-        u.z = u.z + Q.dt * wz;
+        displace(nd, i, rebase, Q.dt, wx, wy, wz, u);
         U4[i] = u;
         V4[i] = make_double4(wx, wy, wz, 0.0);
         if (u_copy) u_copy[i] = u;
@@ -1821,14 +2020,14 @@ void launch_init_accel(const NodeDev& nd, int mixed, const void* slots, double4*
 }
 
 void launch_prologue(const NodeDev& nd, const StepParams* table, double4* U4, double4* V4, const double4* A4,
-                     double4* u_copy, cudaStream_t s) {
-    k_prologue<<<grid_for(nd.num_nodes, 256), 256, 0, s>>>(nd, table, U4, V4, A4, u_copy);
+                     double4* u_copy, int rebase, cudaStream_t s) {
+    k_prologue<<<grid_for(nd.num_nodes, 256), 256, 0, s>>>(nd, table, U4, V4, A4, u_copy, rebase);
 }
 
 void launch_node_step(const NodeDev& nd, int mixed, const void* slots, const StepParams* table, int64_t step,
                       int advance, double4* U4, double4* V4, double4* A4, double4* u_copy, int* status,
-                      cudaStream_t s) {
-    AM_NODE_DISPATCH(k_node_step, table, step, advance, U4, V4, A4, u_copy, status);
+                      cudaStream_t s, int rebase) {
+    AM_NODE_DISPATCH(k_node_step, table, step, advance, U4, V4, A4, u_copy, status, rebase);
 }
 
 void launch_adj_prep(const NodeDev& nd, const StepParams* table, int64_t step, const double4* VB, const double4* AB,
@@ -1858,6 +2057,17 @@ int64_t launch_pm_next(const NodeDev& nd, const double* f_eps, const double* f_u
 }
 void launch_pm_scale(int64_t n, double4* V4, double scale, cudaStream_t s) {
     if (n > 0) k_pm_scale<<<grid_for(n, 256), 256, 0, s>>>(n, V4, scale);
+}
+
+void launch_gauss_force_lagr(const GaussBlockDev& b, int32_t lagr, int rebase, const double4* XC, const double4* INC,
+                             void* slots, int* status, cudaStream_t s) {
+    if (b.num_elems == 0) return;
+    double4* sl = static_cast<double4*>(slots);
+    if (b.kind == AM_HEX8_GAUSS) {
+        AM_DISPATCH_MAT(b.material, (k_hex8_force_lagr<M><<<grid_for(b.num_elems, 64), 64, 0, s>>>(b, lagr, rebase, XC, INC, sl, status)));
+    } else {
+        AM_DISPATCH_MAT(b.material, (k_tet4_force_lagr<M><<<grid_for(b.num_elems, 128), 128, 0, s>>>(b, lagr, rebase, XC, INC, sl, status)));
+    }
 }
 
 void launch_rk_rows4(int64_t n, const int64_t* ptr, const int32_t* nbr, const double* val, const double4* U4,

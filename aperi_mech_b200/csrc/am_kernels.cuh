@@ -46,6 +46,11 @@ struct GaussBlockDev {
     const int32_t* patch_nodes;  // num_patches x 8 (unused entries repeat entry 0)
     const uint32_t* patch_local; // per element: 4 local node ids, one byte each
     const uint32_t* patch_gather;// per patch node: bits 0-7 tets touching it, bits 8+2t: its slot in tet t
+    // Updated / semi-Lagrangian formulations: element displacement gradient of the last
+    // force evaluation (9 per element; for Hex8 the last Gauss point's) and the semi
+    // formulation's reference gradient. null under the total formulation.
+    double* hstate;
+    double* href;
 };
 
 struct CellBlockDev {
@@ -88,6 +93,11 @@ struct NodeDev {
     // Two-pass reproducing-kernel coupling: every node takes its force from this FP64
     // x 3 array (the scattered generalized force) instead of its slots; null otherwise.
     const double* f_given;
+    // Updated (1) / semi (2) Lagrangian formulation, 0 = total: the displacement update
+    // also advances the element kernels' coordinates xc and the increment inc.
+    int32_t lagr;
+    double4* xc;
+    double4* inc;
 };
 
 // ---- launchers (am_kernels.cu) ----
@@ -108,15 +118,22 @@ void launch_gather_force(const NodeDev& nd, int mixed, const void* slots, double
 // exchange buffer (rows of nodes this rank does not hold are left as they are).
 void launch_iface_gather(const NodeDev& nd, int mixed, const void* slots, int64_t num_local,
                          const int32_t* local_nodes, const int32_t* rows, double* buf, cudaStream_t s);
+// Updated / semi-Lagrangian element forces (FP64): coordinates xc, displacement inc, the
+// element's reference gradient (rebase: the semi formulation's reference update takes the
+// last stored H first).
+void launch_gauss_force_lagr(const GaussBlockDev& b, int32_t lagr, int rebase, const double4* XC, const double4* INC,
+                             void* slots, int* status, cudaStream_t s);
 // a = (f + g m) / m with no boundary condition (pre-loop acceleration).
 void launch_init_accel(const NodeDev& nd, int mixed, const void* slots, double4* A4, int* status, cudaStream_t s);
 // First half-step of a run: vh = v + h a ; BC(vh) ; u += dt vh.
+// rebase (semi formulation): the reference configuration moves first (xc += inc, inc = 0);
+// the updated formulation always advances xc by the last increment.
 void launch_prologue(const NodeDev& nd, const StepParams* table, double4* U4, double4* V4, const double4* A4,
-                     double4* u_copy, cudaStream_t s);
+                     double4* u_copy, int rebase, cudaStream_t s);
 // Gather + a = f/m ; BC(a) ; v = vh + h a ; then either advance (next vh, BC, u) or store (v, a).
 void launch_node_step(const NodeDev& nd, int mixed, const void* slots, const StepParams* table, int64_t step,
                       int advance, double4* U4, double4* V4, double4* A4, double4* u_copy, int* status,
-                      cudaStream_t s);
+                      cudaStream_t s, int rebase = 0);
 // Adjoint node kernels.
 void launch_adj_prep(const NodeDev& nd, const StepParams* table, int64_t step, const double4* VB, const double4* AB,
                      double4* L4, cudaStream_t s);

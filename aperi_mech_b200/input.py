@@ -30,7 +30,10 @@ library computes, and builds an ExplicitDynamics model on the GPU:
                                         time_function: {ramp_function | smooth_step_function:
                                                         {abscissa_values, ordinate_values}},
                                         active_time_range: {time_start, time_end}}
-          output: ...                               (ignored: IO is outside this path)
+          output: {file, time_start, time_end, time_increment}
+                                                    (fields at the output times, as an .npz of frames)
+          lagrangian_formulation: {total: ~ | updated: ~ | semi: {update_interval: k}}
+                                                    (IoInputFile.h:188-262; Gauss parts, FP64)
           x_b200: {precision: fp64 | mixed, seed, jitter, velocity_noise, max_steps,
                    fields: {<part set>: {shear_modulus | bulk_modulus: {lognormal_sigma}}}}
 
@@ -88,6 +91,8 @@ class Simulation:
     meta: dict = field(default_factory=dict)
     power_method: tuple | None = None  # (scale_factor, update_interval) of power_method_time_stepper
     rk: tuple | None = None  # (nbr_ptr, nbr, values): two-pass reproducing-kernel coupling
+    output: tuple | None = None  # (file, time_start, time_end, time_increment) of the output block
+    formulation: tuple = ("total", 1)  # lagrangian_formulation and the semi update_interval
 
     @property
     def num_nodes(self) -> int:
@@ -99,7 +104,7 @@ class Simulation:
 
     def model(self, stream=None) -> ExplicitDynamics:
         return ExplicitDynamics(self.coords, self.parts, self.bcs, body_accel=self.body_accel, mass=self.mass,
-                                stream=stream, rk=self.rk)
+                                stream=stream, rk=self.rk, formulation=self.formulation)
 
     def problem(self):
         """The same inputs as a problems.Problem (for the oracle and the benchmark)."""
@@ -115,8 +120,45 @@ class Simulation:
             meta["body_accel"] = self.body_accel
         if self.rk is not None:
             meta["rk"] = self.rk
+        if self.formulation[0] != "total":
+            meta["formulation"] = self.formulation
         return Problem(self.name, self.coords, self.parts, self.bcs, self.v0, self.dt, nsteps,
                        int(self.meta.get("seed", 0)), meta)
+
+
+class TimeIncrementScheduler:
+    """TimeIncrementScheduler (include/Scheduler.h:51-89): an event at time_start, then every
+    time_increment, while the next event point does not pass time_end; a call that finds
+    the event point reached (within 1e-15) moves it past the given time."""
+
+    def __init__(self, time_start: float, time_end: float, time_increment: float):
+        self.time_end = float(time_end)
+        self.increment = float(time_increment)
+        self.next_event = float(time_start)
+
+    def at_next_event(self, time: float) -> bool:
+        at_event = time + 1.0e-15 >= self.next_event
+        if at_event:
+            self.next_event += self.increment
+            self.at_next_event(time)
+            if self.next_event > self.time_end:
+                self.next_event = sys.float_info.max
+        return at_event
+
+
+def output_steps(dts, output) -> list:
+    """Step counts (0 = the initial state) after which ExplicitSolver::Solve writes output
+    (src/Solvers/Explicit.cpp:375,472): the scheduler asked at time 0, then after each step
+    with the accumulated time."""
+    _, t0, t1, inc = output
+    sched = TimeIncrementScheduler(t0, t1, inc)
+    out = [0] if sched.at_next_event(0.0) else []
+    time = 0.0
+    for n, d in enumerate(dts, start=1):
+        time += d
+        if sched.at_next_event(time):
+            out.append(n)
+    return out
 
 
 def direct_time_steps(dt: float, time_end: float, max_steps: int = 1 << 40) -> list:
@@ -463,9 +505,43 @@ def load(source, base_dir: Path | None = None) -> Simulation:
         raise InputError(f"x_b200.precision {precision!r} (fp64 or mixed)")
     name = Path(str(source)).stem if isinstance(source, (str, Path)) and "\n" not in str(source) else "input"
     element_blocks = [blocks[(e.get("part") or {}).get("set")] for e in (geo.get("parts") or [])]
+    formulation = ("total", 1)
+    lnode = proc.get("lagrangian_formulation")
+    if lnode is not None:
+        if not isinstance(lnode, dict):
+            raise InputError("'lagrangian_formulation' must be a map")
+        if "total" in lnode:
+            formulation = ("total", 1)
+        elif "updated" in lnode:
+            formulation = ("updated", 1)
+        elif "semi" in lnode:
+            k = (lnode.get("semi") or {}).get("update_interval")
+            if k is None:
+                raise InputError("lagrangian_formulation.semi needs update_interval")
+            formulation = ("semi", int(k))
+            if formulation[1] < 1:
+                raise InputError("lagrangian_formulation.semi.update_interval must be at least 1")
+        else:
+            raise InputError("lagrangian_formulation must have 'total', 'updated', or 'semi' key")
+    if formulation[0] != "total":
+        if any(p.kind == "cells" for p in parts):
+            raise InputError(f"{formulation[0]} Lagrangian formulation: built for Gauss parts only")
+        if precision != "fp64":
+            raise InputError(f"{formulation[0]} Lagrangian formulation runs in FP64 (x_b200.precision: fp64)")
+        if power is not None:
+            raise InputError(f"{formulation[0]} Lagrangian formulation with the power-method time stepper is not built")
+    output = None
+    onode = proc.get("output")
+    if onode:
+        inc = float(onode.get("time_increment", 0.0))
+        if not inc > 0.0:
+            raise InputError("output.time_increment must be positive")
+        output = (str(onode.get("file", "results.exo")), float(onode.get("time_start", 0.0)),
+                  float(onode.get("time_end", t_end)), inc)
     return Simulation(name, coords, parts, bcs, v0, dt, t_end, precision, body, mass,
                       int(ext.get("max_steps", 1 << 40)), sets,
-                      {"seed": seed, "mesh": mesh_spec, "element_blocks": element_blocks}, power, rk)
+                      {"seed": seed, "mesh": mesh_spec, "element_blocks": element_blocks, "base_dir": str(base_dir)},
+                      power, rk, output, formulation)
 
 
 def power_method_inputs(sim: Simulation):
@@ -478,15 +554,35 @@ def power_method_inputs(sim: Simulation):
 def run(source, stream=None) -> dict:
     """Parse, build the GPU model, and Solve(): the initial acceleration, then the time
     stepper's steps (ExplicitSolver::Solve, src/Solvers/Explicit.cpp:308-483); with the
-    power-method stepper the increment is recomputed on the GPU every update_interval steps."""
+    power-method stepper the increment is recomputed on the GPU every update_interval steps.
+    With an output block and the direct stepper the run stops at the output steps and the
+    result holds the frames (times and nodal fields) the reference would write there."""
     sim = source if isinstance(source, Simulation) else load(source)
     dt = sim.dt
+    frames = None
     with sim.model(stream) as m:
         m.set_state(np.zeros_like(sim.coords), sim.v0)
         if sim.power_method is not None:
             m.set_power_method(*power_method_inputs(sim))
             steps, dt = m.solve_power_method(sim.power_method[0], sim.power_method[1], sim.time_end, sim.precision,
                                              sim.max_steps)
+        elif sim.output is not None:
+            dts = direct_time_steps(sim.dt, sim.time_end, sim.max_steps)
+            at = output_steps(dts, sim.output)
+            m.init_acceleration(sim.precision)
+            frames = {"step": [], "time": [], "displacement": [], "velocity": [], "acceleration": []}
+            done, time = 0, 0.0
+            for n in at + [len(dts)]:
+                if n > done:
+                    m.run_schedule(dts[done:n], sim.precision, t0=time)
+                    for d in dts[done:n]:
+                        time += d
+                    done = n
+                if n in at and (not frames["step"] or frames["step"][-1] != n):
+                    fu, fv, fa = m.get_state()
+                    for k, x in zip(("step", "time", "displacement", "velocity", "acceleration"), (n, time, fu, fv, fa)):
+                        frames[k].append(x)
+            steps = len(dts)
         else:
             steps = m.solve(sim.dt, sim.time_end, sim.precision, sim.max_steps)
         u, v, a = m.get_state()
@@ -497,7 +593,24 @@ def run(source, stream=None) -> dict:
         from .rkpm import apply_functions
 
         out["physical_displacement"] = apply_functions(sim.rk, u)
+    if frames is not None:
+        out["frames"] = {k: np.asarray(x) for k, x in frames.items()}
+        if sim.rk is not None:
+            out["frames"]["physical_displacement"] = np.stack(
+                [apply_functions(sim.rk, fu) for fu in frames["displacement"]]) if frames["displacement"] else \
+                np.zeros((0,) + sim.coords.shape)
     return out
+
+
+def write_output(result: dict, directory: Path | str = ".") -> Path:
+    """The output frames as <output file stem>.npz in `directory`: step, time and the nodal
+    fields (N x 3 per frame) at every output time, with the coordinates."""
+    sim = result["simulation"]
+    if sim.output is None or "frames" not in result:
+        raise InputError("no output block (or the power-method stepper, which writes the final state only)")
+    path = Path(directory) / (Path(sim.output[0]).stem + ".npz")
+    np.savez(path, coordinates=sim.coords, **result["frames"])
+    return path
 
 
 def main(argv=None) -> int:
@@ -506,9 +619,12 @@ def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description="Run an aperi-mech explicit-dynamics input on the GPU.")
     ap.add_argument("input")
     ap.add_argument("--save", help="write the final u, v, a to this .npz")
+    ap.add_argument("--output-dir", default=".", help="where the output block's frames are written (.npz)")
     a = ap.parse_args(argv)
     r = run(a.input)
     sim = r["simulation"]
+    if "frames" in r:
+        write_output(r, a.output_dir)
     if a.save:
         np.savez(a.save, displacement=r["displacement"], velocity=r["velocity"], acceleration=r["acceleration"])
     print(json.dumps({"input": a.input, "nodes": sim.num_nodes, "elements": sim.num_elems, "steps": r["steps"],

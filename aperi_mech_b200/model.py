@@ -110,9 +110,11 @@ class ExplicitDynamics:
     """Device-resident explicit-dynamics model (one am_ctx)."""
 
     def __init__(self, coords: np.ndarray, parts: list[Part], bcs: list[BoundaryCondition] = (),
-                 body_accel=None, mass: np.ndarray | None = None, stream=None, rk=None):
+                 body_accel=None, mass: np.ndarray | None = None, stream=None, rk=None, formulation=None):
         """rk = (nbr_ptr, nbr, values) sets the two-pass reproducing-kernel coupling
-        (set_rk_functions); mass is then the generalized lumped mass."""
+        (set_rk_functions); mass is then the generalized lumped mass. formulation =
+        ('updated', 1) or ('semi', update_interval) selects the updated or semi-Lagrangian
+        formulation of the Gauss blocks (FP64 runs only); None or ('total', ...) the total one."""
         self.lib = capi.load()
         self.coords = np.ascontiguousarray(coords, dtype=np.float64)
         self.N = int(self.coords.shape[0])
@@ -124,6 +126,10 @@ class ExplicitDynamics:
         try:
             if stream is not None:
                 check(self.lib.am_set_stream(self.ctx, stream), self.ctx)
+            if formulation is not None and formulation[0] != "total":
+                code = {"updated": 1, "semi": 2}[formulation[0]]
+                interval = int(formulation[1]) if len(formulation) > 1 else 1
+                check(self.lib.am_set_formulation(self.ctx, code, interval), self.ctx)
             for p in self.parts:
                 self._add_part(p)
             if bcs:

@@ -274,6 +274,24 @@ int am_stable_time_increment(am_ctx* ctx, double previous, int32_t num_iteration
 int am_solve_power_method(am_ctx* ctx, am_precision prec, double scale_factor, int64_t update_interval, double t_end,
                           int64_t max_steps, int64_t* steps_done, double* last_increment);
 
+/* ---- updated / semi-Lagrangian formulations (LagrangianFormulationType; the Gauss force
+ * ComputeInternalForceGaussian.h:57-131 with ComputeInternalForceBase.h:158-174; the displacement
+ * update ExplicitTimeIntegrator.h:141-244,461-551; the reference-configuration schedule
+ * src/Application.cpp:301-308 and src/Solvers/Explicit.cpp:195-214) ----
+ * formulation 0 total (the default), 1 updated, 2 semi with a reference update every
+ * update_interval steps. The element kernels then take shape-function gradients on the
+ * current coordinates (updated: those at the start of the step) or on the reference
+ * coordinates of the last update (semi), the displacement increment of the step (updated)
+ * or since the last update (semi), and compose H = dH + Href + dH Href with the element's
+ * stored reference gradient; forces map back through F_ref = I + Href. As in the reference,
+ * an element keeps one H: for Hex8 the last Gauss point's serves as every Gauss point's
+ * reference (Tet4, with one point, matches the total formulation to round-off). State
+ * starts undeformed and is reset by am_set_state with a displacement (which should be
+ * zero); FP64 only; Gauss blocks only; not with am_internal_force, the VJP, the adjoint,
+ * the power method, the two-pass coupling or a decomposed mesh (AM_ESTATE). Call after
+ * am_create and before am_add_block (Tet4 blocks then keep per-element slots). */
+int am_set_formulation(am_ctx* ctx, int32_t formulation, int32_t update_interval);
+
 /* ---- two-pass reproducing-kernel coupling (the solver's generalized-field path with the
  * two-pass method, src/Solvers/Explicit.cpp:146-186; FunctionEvaluationProcessor::ComputeValues
  * and ScatterValues, include/FunctionEvaluationProcessor.h:70-174) ----

@@ -297,6 +297,68 @@ void gauss_element_force(const ob_block& b, int64_t e, const double* coords, con
     }
 }
 
+// Updated / semi-Lagrangian Gauss element (ComputeInternalForceGaussian.h:57-131 with
+// ComputeInternalForceBase.h:158-174): B and w on the coordinates x (current or reference
+// configuration), dH = inc^T B, H = dH + Href + dH Href stored per element (each Gauss
+// point overwrites it, so the last one remains), P(H), then B F_ref and w / det F_ref with
+// F_ref = I + Href (Href the element's, for every Gauss point).
+void gauss_element_force_lagr(const ob_block& b, int64_t e, const double* coords, const double* inc,
+                              const double* Href, double* Hout, double* fe) {
+    const int nn = nodes_per_elem(b.kind);
+    double X[24], U[24];
+    for (int a = 0; a < nn; ++a) {
+        const int32_t n = b.conn[e * nn + a];
+        for (int i = 0; i < 3; ++i) {
+            X[a * 3 + i] = coords[n * 3 + i];
+            U[a * 3 + i] = inc[n * 3 + i];
+        }
+    }
+    double lambda, mu;
+    block_lame(b, e, &lambda, &mu);
+    for (int k = 0; k < nn * 3; ++k) fe[k] = 0.0;
+    double Fr[9];
+    for (int k = 0; k < 9; ++k) Fr[k] = Href[k] + ((k % 4 == 0) ? 1.0 : 0.0);
+    const double detFr = Fr[0] * (Fr[4] * Fr[8] - Fr[5] * Fr[7]) - Fr[1] * (Fr[3] * Fr[8] - Fr[5] * Fr[6]) +
+                         Fr[2] * (Fr[3] * Fr[7] - Fr[4] * Fr[6]);
+    const int ngp = (b.kind == OB_HEX8_GAUSS) ? 8 : 1;
+    for (int gp = 0; gp < ngp; ++gp) {
+        double B[24], w;
+        if (b.kind == OB_HEX8_GAUSS) {
+            double xi[3], dN[24];
+            hex8_gauss_point(gp, xi);
+            hex8_dN(xi, dN);
+            w = gauss_bw<8>(X, dN, 1.0, B);
+        } else {
+            w = gauss_bw<4>(X, kTet4dN, 1.0 / 6.0, B);
+        }
+        double dH[9], H[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                double t = 0.0;
+                for (int a = 0; a < nn; ++a) t += U[a * 3 + i] * B[a * 3 + j];
+                dH[i * 3 + j] = t;
+            }
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                double t = 0.0;
+                for (int k = 0; k < 3; ++k) t += dH[i * 3 + k] * Href[k * 3 + j];
+                H[i * 3 + j] = dH[i * 3 + j] + Href[i * 3 + j] + t;
+            }
+        for (int k = 0; k < 9; ++k) Hout[k] = H[k];
+        double P[9];
+        stress(b.material, lambda, mu, H, P);
+        const double wr = w / detFr;
+        for (int a = 0; a < nn; ++a) {
+            double Br[3];
+            for (int j = 0; j < 3; ++j) Br[j] = B[a * 3 + 0] * Fr[0 * 3 + j] + B[a * 3 + 1] * Fr[1 * 3 + j] + B[a * 3 + 2] * Fr[2 * 3 + j];
+            for (int i = 0; i < 3; ++i) {
+                const double t = Br[0] * P[i * 3 + 0] + Br[1] * P[i * 3 + 1] + Br[2] * P[i * 3 + 2];
+                fe[a * 3 + i] -= t * wr;
+            }
+        }
+    }
+}
+
 // ComputeInternalForceSmoothedCell.h:86-117 (H gather), :186-224 (stress), :312-351 (force):
 // H = sum_k u_k (x) b_k ; f_k += b_k (-V P^T).
 void cell_force(const ob_block& b, int64_t c, const double* u, double* fk) {
@@ -939,6 +1001,98 @@ int ob_explicit_steps(const ob_problem* p, int64_t nsteps, const double* dts, do
     for (int64_t n = 0; n < nsteps; ++n) {
         cd_step(p, m.data(), dts[n], time, u, v, a, f.data());
         time += dts[n];
+    }
+    return 0;
+}
+
+int ob_lagrangian_force(const ob_problem* p, ob_lagrangian* s, double* f) {
+    const int64_t N = p->num_nodes;
+    std::fill(f, f + N * 3, 0.0);
+    int64_t base = 0;
+    for (int k = 0; k < p->num_blocks; ++k) {
+        const ob_block& b = p->blocks[k];
+        if (b.kind == OB_CELLS) return -1;
+        const int nn = nodes_per_elem(b.kind);
+        std::vector<double> slots(static_cast<size_t>(b.num_elems) * nn * 3);
+        const double* href = s->formulation == OB_SEMI ? s->Href : s->H;
+#pragma omp parallel for schedule(static)
+        for (int64_t e = 0; e < b.num_elems; ++e) {
+            double hr[9];
+            std::copy(href + 9 * (base + e), href + 9 * (base + e) + 9, hr);
+            gauss_element_force_lagr(b, e, s->x, s->inc, hr, s->H + 9 * (base + e), slots.data() + e * nn * 3);
+        }
+        for (int64_t e = 0; e < b.num_elems; ++e)
+            for (int a = 0; a < nn; ++a) {
+                const int32_t n = b.conn[e * nn + a];
+                for (int i = 0; i < 3; ++i) f[n * 3 + i] += slots[(e * nn + a) * 3 + i];
+            }
+        base += b.num_elems;
+    }
+    return 0;
+}
+
+namespace {
+void lagr_acceleration(const ob_problem* p, ob_lagrangian* s, const double* m, double* f, double* a) {
+    const int64_t N = p->num_nodes;
+    ob_lagrangian_force(p, s, f);
+    const double* g = p->body_accel;
+    if (g[0] != 0.0 || g[1] != 0.0 || g[2] != 0.0)
+        for (int64_t n = 0; n < N; ++n)
+            for (int i = 0; i < 3; ++i) f[n * 3 + i] += g[i] * m[n];
+    for (int64_t n = 0; n < N; ++n)
+        for (int i = 0; i < 3; ++i) a[n * 3 + i] = f[n * 3 + i] / m[n];
+}
+}  // namespace
+
+int ob_lagrangian_init(const ob_problem* p, ob_lagrangian* s, double* a) {
+    if (s->formulation != OB_UPDATED && s->formulation != OB_SEMI) return -1;
+    std::vector<double> m = mass_of(p);
+    std::vector<double> f(static_cast<size_t>(p->num_nodes) * 3);
+    lagr_acceleration(p, s, m.data(), f.data(), a);
+    return 0;
+}
+
+// One step of ExplicitSolver::Solve (src/Solvers/Explicit.cpp:383-483) with the updated or
+// semi displacement update (UpdateDisplacementsUpdatedFunctor, ExplicitTimeIntegrator.h:
+// 141-244) and the reference-configuration update at the end of the step (UpdateShapeFunctions
+// :195-214; ExplicitTimeIntegratorSemi::UpdateReferenceConfiguration :511-541; the updated
+// formulation's current coordinates advance every step, :470-478).
+int ob_lagrangian_steps(const ob_problem* p, ob_lagrangian* s, int64_t nsteps, const double* dts, double t0, double* u,
+                        double* v, double* a) {
+    if (s->formulation != OB_UPDATED && s->formulation != OB_SEMI) return -1;
+    if (s->formulation == OB_SEMI && s->update_interval < 1) return -1;
+    const int64_t N = p->num_nodes;
+    std::vector<double> m = mass_of(p);
+    std::vector<double> f(static_cast<size_t>(N) * 3);
+    int64_t E = 0;
+    for (int k = 0; k < p->num_blocks; ++k) E += p->blocks[k].num_elems;
+    double time = t0;
+    for (int64_t k = 0; k < nsteps; ++k) {
+        const double dtn = dts[k], half = 0.5 * dtn;
+        for (int64_t q = 0; q < N * 3; ++q) v[q] = v[q] + half * a[q];
+        apply_bcs(p, 0, time + 0.5 * dtn, v);
+        for (int64_t q = 0; q < N * 3; ++q) {
+            const double d = dtn * v[q];
+            u[q] = u[q] + d;
+            if (s->formulation == OB_SEMI)
+                s->inc[q] += d;
+            else
+                s->inc[q] = d;
+        }
+        lagr_acceleration(p, s, m.data(), f.data(), a);
+        apply_bcs(p, 1, time + dtn, a);
+        for (int64_t q = 0; q < N * 3; ++q) v[q] += half * a[q];
+        time += dtn;
+        s->n += 1;
+        if (s->formulation == OB_UPDATED) {
+            for (int64_t q = 0; q < N * 3; ++q) s->x[q] = s->x[q] + s->inc[q];
+        } else if (s->n % s->update_interval == 0) {
+            for (int64_t q = 0; q < N * 3; ++q) {
+                s->x[q] = s->x[q] + s->inc[q];
+                s->inc[q] = 0.0;
+            }
+            std::copy(s->H, s->H + 9 * E, s->Href);
+        }
     }
     return 0;
 }

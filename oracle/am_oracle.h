@@ -163,6 +163,33 @@ double ob_stable_time_increment(const ob_problem* p, const double* u, double* v,
                                 int32_t num_iterations, double eps, double tol, double vartol, int32_t* iterations,
                                 int32_t* converged);
 
+/* ---- updated / semi-Lagrangian formulations (Gauss blocks) ----
+ * State (ExplicitTimeIntegrator.h:50-90, ComputeInternalForceBase.h:158-174): x holds the
+ * current coordinates at the start of the step (updated) or the reference coordinates
+ * (semi), inc the displacement increment (of the step, or since the last reference
+ * update), H the element displacement gradients of the last force evaluation (one per
+ * element: the last Gauss point's, as the reference's element field) and Href the semi
+ * formulation's reference gradients; n counts completed steps. Start: x = coordinates,
+ * inc = H = Href = 0, n = 0. */
+enum { OB_TOTAL = 0, OB_UPDATED = 1, OB_SEMI = 2 };
+typedef struct {
+    int32_t formulation;
+    int32_t update_interval; /* semi: reference update every update_interval steps */
+    int64_t n;
+    double* x;    /* num_nodes x 3 */
+    double* inc;  /* num_nodes x 3 */
+    double* H;    /* 9 per Gauss element, blocks in order */
+    double* Href; /* 9 per Gauss element (semi) */
+} ob_lagrangian;
+/* Internal force of the formulation at the state (stores H). */
+int ob_lagrangian_force(const ob_problem* p, ob_lagrangian* s, double* f);
+/* Initial acceleration (the force at the state, no acceleration BC). */
+int ob_lagrangian_init(const ob_problem* p, ob_lagrangian* s, double* a);
+/* nsteps central-difference steps in the order of ExplicitSolver::Solve with the
+ * formulation's displacement update and reference-configuration updates. */
+int ob_lagrangian_steps(const ob_problem* p, ob_lagrangian* s, int64_t nsteps, const double* dts, double t0, double* u,
+                        double* v, double* a);
+
 /* ---- threads ---- */
 void ob_set_threads(int n);
 int ob_get_threads(void);

@@ -30,6 +30,31 @@ class OBlock(C.Structure):
                 ("num_groups", C.c_int64), ("group_ptr", _lp)]
 
 
+class OLagrangian(C.Structure):
+    _fields_ = [("formulation", C.c_int32), ("update_interval", C.c_int32), ("n", C.c_int64), ("x", _dp),
+                ("inc", _dp), ("H", _dp), ("Href", _dp)]
+
+
+FORMULATION = {"total": 0, "updated": 1, "semi": 2}
+
+
+class LagrangianState:
+    """Updated / semi-Lagrangian state of the oracle: coordinates x (current or reference),
+    displacement increment, element H and reference H, completed steps."""
+
+    def __init__(self, coords, num_elems, formulation, update_interval=1):
+        self.x = np.array(coords, dtype=np.float64, order="C", copy=True)
+        self.inc = np.zeros_like(self.x)
+        self.H = np.zeros((num_elems, 9))
+        self.Href = np.zeros((num_elems, 9))
+        self.s = OLagrangian(FORMULATION[formulation], int(update_interval), 0, _p(self.x), _p(self.inc), _p(self.H),
+                             _p(self.Href))
+
+    @property
+    def n(self) -> int:
+        return int(self.s.n)
+
+
 class OBC(C.Structure):
     _fields_ = [("num_nodes", C.c_int64), ("nodes", _ip), ("component_mask", C.c_int32), ("kind", C.c_int32),
                 ("time_function", C.c_int32), ("num_points", C.c_int32), ("values", C.c_double * 3),
@@ -81,6 +106,10 @@ def lib() -> C.CDLL:
                                             _lp, _ip, _dp, _lp, _ip, _dp, _dp, _dp]
         L.ob_rkpm_nodal_subcells.argtypes = [C.c_int64, _dp, C.c_int64, _ip, _dp, C.c_int32, C.c_double, _lp, _lp,
                                              _ip, _dp, _dp, _lp]
+        L.ob_lagrangian_force.argtypes = [C.POINTER(OProblem), C.POINTER(OLagrangian), _dp]
+        L.ob_lagrangian_init.argtypes = [C.POINTER(OProblem), C.POINTER(OLagrangian), _dp]
+        L.ob_lagrangian_steps.argtypes = [C.POINTER(OProblem), C.POINTER(OLagrangian), C.c_int64, _dp, C.c_double, _dp,
+                                          _dp, _dp]
         L.ob_stable_time_increment.argtypes = [C.POINTER(OProblem), _dp, _dp, _dp, C.c_double, C.c_int32, C.c_double,
                                                C.c_double, C.c_double, _ip, _ip]
         L.ob_stable_time_increment.restype = C.c_double
@@ -202,6 +231,26 @@ class OracleProblem:
         dt = lib().ob_stable_time_increment(C.byref(self.s), _p(u), _p(v), _p(le), previous, num_iterations, epsilon,
                                             tolerance, variation_tolerance, C.byref(its), C.byref(conv))
         return dt, its.value, bool(conv.value)
+
+    def lagrangian_state(self, formulation, update_interval=1):
+        return LagrangianState(self.coords, self.num_elems, formulation, update_interval)
+
+    def lagrangian_force(self, state):
+        f = np.empty((self.N, 3))
+        assert lib().ob_lagrangian_force(C.byref(self.s), C.byref(state.s), _p(f)) == 0
+        return f
+
+    def lagrangian_init(self, state):
+        a = np.empty((self.N, 3))
+        assert lib().ob_lagrangian_init(C.byref(self.s), C.byref(state.s), _p(a)) == 0
+        return a
+
+    def lagrangian_steps(self, state, u, v, a, dts, t0=0.0):
+        u, v, a = (np.array(x, dtype=np.float64, order="C", copy=True) for x in (u, v, a))
+        dts = np.ascontiguousarray(dts, dtype=np.float64)
+        assert lib().ob_lagrangian_steps(C.byref(self.s), C.byref(state.s), dts.size, _p(dts), t0, _p(u), _p(v),
+                                         _p(a)) == 0
+        return u, v, a
 
     def vjp_force(self, u, lam):
         u = np.ascontiguousarray(u, dtype=np.float64)

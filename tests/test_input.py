@@ -1,4 +1,6 @@
 """The YAML front-end (aperi-mech's input schema) against the array-level set-up and the oracle."""
+import sys
+
 import numpy as np
 import pytest
 
@@ -141,6 +143,25 @@ def test_components_vector_initial_conditions_and_extensions():
     assert np.array_equal(sim.coords[~interior], plain.coords[~interior])  # boundary untouched
 
 
+def test_time_increment_scheduler_known_answers():
+    """SchedulerTest.cpp TimeIncrementSchedulerAtNextEvent (start 0, end 1, increment 0.1)."""
+    sched = inp.TimeIncrementScheduler(0.0, 1.0, 0.1)
+    calls = [(-0.1, False, 0.0), (0.0, True, 0.1), (0.05, False, 0.1), (0.09, False, 0.1), (0.1, True, 0.2),
+             (0.19, False, 0.2), (0.21, True, 0.3), (0.3, True, 0.4), (0.75, True, 0.8), (0.76, False, 0.8),
+             (0.99, True, 1.0)]
+    for t, want, nxt in calls:
+        assert sched.at_next_event(t) == want
+        assert abs(sched.next_event - nxt) < 1e-12
+    assert sched.at_next_event(1.0) and sched.next_event == sys.float_info.max
+    assert not sched.at_next_event(1.1) and not sched.at_next_event(10.1)
+
+
+def test_output_steps_follow_the_solver_loop():
+    dts = inp.direct_time_steps(0.1, 1.0)
+    assert inp.output_steps(dts, ("r.exo", 0.0, 1.0, 0.25)) == [0, 3, 5, 8, 10]
+    assert inp.output_steps(dts, ("r.exo", 0.5, 0.8, 0.1)) == [5, 6, 7, 8]
+
+
 @pytest.mark.parametrize("text, msg", [
     (nh_yaml(stepper="implicit_time_stepper: {time_end: 1.0}"), "time_stepper"),
     (nh_yaml(stepper="power_method_time_stepper: {scale_factor: 0.0, update_interval: 10, time_end: 1.0}"),
@@ -269,6 +290,42 @@ def test_yaml_rkpm_nodal_subcells_match_oracle(oracle_lib, use_f_bar):
     u, v, a, n = prob.solve(np.zeros_like(sim.coords), sim.v0, sim.dt, sim.time_end)
     assert r["steps"] == n
     assert np.linalg.norm(r["displacement"] - u) <= 1e-12 * np.linalg.norm(u)
+
+
+@pytest.mark.gpu
+def test_yaml_output_frames_match_oracle(oracle_lib, tmp_path):
+    """The output block: frames at the scheduler's steps equal the oracle run in the same
+    segments, the last state equals the run without output, and the .npz holds them."""
+    text = nh_yaml(n=4) + """      output:
+        file: results.exo
+        time_start: 0
+        time_end: 4.0e-6
+        time_increment: 1.0e-6
+"""
+    sim = inp.load(text)
+    r = inp.run(sim)
+    fr = r["frames"]
+    dts = inp.direct_time_steps(sim.dt, sim.time_end)
+    assert list(fr["step"]) == inp.output_steps(dts, sim.output) and len(fr["step"]) >= 4
+    prob = oracle_lib.OracleProblem(sim.coords, sim.parts, sim.bcs)
+    u = np.zeros_like(sim.coords)
+    v, a = sim.v0.copy(), prob.init_acceleration(u)
+    done, t = 0, 0.0
+    for k, n in enumerate(fr["step"]):
+        if n > done:
+            u, v, a = prob.steps(u, v, a, np.array(dts[done:n]), t0=t)
+            for d in dts[done:n]:
+                t += d
+            done = n
+        assert abs(fr["time"][k] - t) <= 1e-18
+        for g, w in ((fr["displacement"][k], u), (fr["velocity"][k], v), (fr["acceleration"][k], a)):
+            assert np.linalg.norm(g - w) <= 1e-12 * max(np.linalg.norm(w), 1e-300)
+    plain = inp.run(inp.load(nh_yaml(n=4)))
+    assert np.linalg.norm(r["displacement"] - plain["displacement"]) <= 1e-13 * np.linalg.norm(plain["displacement"])
+    path = inp.write_output(r, tmp_path)
+    with np.load(path) as z:
+        assert z["displacement"].shape == (len(fr["step"]),) + sim.coords.shape
+        assert np.array_equal(z["time"], fr["time"])
 
 
 @pytest.mark.gpu
