@@ -110,6 +110,8 @@ struct Block {
     // F-bar cells (am_set_cell_groups): the cells are subcells grouped by group_ptr.
     int64_t num_groups = 0;
     int64_t* group_ptr = nullptr;
+    int32_t max_group = 0;
+    bool fbar_fused = true;
     double* fbar64 = nullptr;  // kFbarStride per subcell, allocated on first use
     float* fbar32 = nullptr;
     // Tet4 element patches (see GaussBlockDev)
@@ -161,12 +163,14 @@ struct Block {
         c.max_entries = max_entries;
         c.num_groups = num_groups;
         c.group_ptr = group_ptr;
+        c.max_group = max_group;
+        c.fused = fbar_fused && max_group <= 32 ? 1 : 0;  // kFbarMaxSub
         return c;
     }
     // The device view for a force evaluation at the given precision (F-bar scratch attached).
     am::CellBlockDev cells_for(int mixed) {
         am::CellBlockDev c = cells();
-        if (group_ptr) {
+        if (group_ptr && !c.fused) {
             const size_t n = static_cast<size_t>(std::max<int64_t>(num_elems, 1)) * am::kFbarStride;
             if (mixed) {
                 if (!fbar32) fbar32 = dalloc<float>(n, "F-bar scratch (FP32)");
@@ -1117,6 +1121,11 @@ int am_set_cell_groups(am_ctx* ctx, int32_t block_id, int64_t num_cells, const i
         // in total (ForEachCellComputeForce_Impl: num_subcells != num_cells).
         if (num_cells == b.num_elems) return;
         b.num_groups = num_cells;
+        for (int64_t g = 0; g < num_cells; ++g)
+            b.max_group = std::max<int32_t>(b.max_group, static_cast<int32_t>(group_ptr[g + 1] - group_ptr[g]));
+        // APERI_B200_FBAR_PASSES=3 keeps the three-pass form for every cell size.
+        const char* passes = std::getenv("APERI_B200_FBAR_PASSES");
+        b.fbar_fused = !(passes && passes[0] == '3');
         b.group_ptr = dalloc<int64_t>(num_cells + 1, "cell groups");
         ck(cudaMemcpy(b.group_ptr, group_ptr, (num_cells + 1) * sizeof(int64_t), cudaMemcpyHostToDevice), "upload");
     });

@@ -915,6 +915,149 @@ __global__ void __launch_bounds__(256) k_fbar_force(CellBlockDev b, vec4_t<T>* _
     }
 }
 
+// F-bar in one pass for cells of at most 32 subcells: one warp per cell. Eight lanes
+// take one subcell's entries together (coalesced, four subcells at a time) and combine
+// its H by a butterfly; the subcell's H and J go to shared memory. Then one lane per
+// subcell forms J-bar and the dual pressure over the warp (fixed butterflies), the
+// barred and un-barred stresses, back into shared memory; and eight lanes per subcell
+// write its forces. Same formulas as k_fbar_h / k_fbar_cell / k_fbar_force, no global
+// scratch and one launch.
+constexpr int kFbarMaxSub = 32;
+constexpr int kFbarWarps = 4;
+
+__device__ __forceinline__ void warp_sum2(double& x, double& y) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        x += __shfl_xor_sync(kFull, x, off);
+        y += __shfl_xor_sync(kFull, y, off);
+    }
+}
+
+template <typename T, int MAT>
+__global__ void __launch_bounds__(32 * kFbarWarps) k_fbar_fused(CellBlockDev b, const double4* __restrict__ U4,
+                                                                 vec4_t<T>* __restrict__ slots, int* status) {
+    __shared__ T sh_t[kFbarWarps][kFbarMaxSub][18];  // H, then the subcell stress
+    __shared__ double sh_j[kFbarWarps][kFbarMaxSub];
+    const int w = static_cast<int>(threadIdx.x >> 5);
+    const int lane = static_cast<int>(threadIdx.x & 31);
+    const int q = lane >> 3, r8 = lane & 7;
+    const int64_t g = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const bool gvalid = g < b.num_groups;
+    const int64_t s0 = gvalid ? b.group_ptr[g] : 0;
+    const int ns = gvalid ? static_cast<int>(b.group_ptr[g + 1] - s0) : 0;
+    const T* gr = cell_grads<T>(b);
+    const bool diff = sizeof(T) == 4;
+    // H of every subcell, four at a time.
+    for (int base = 0; base < ns; base += 4) {
+        const int k = base + q;
+        const bool has = k < ns;
+        const int64_t s = s0 + k;
+        const int32_t e0 = has ? b.ptr[s] : 0, e1 = has ? b.ptr[s + 1] : 0;
+        const double4 ur = e1 > e0 ? U4[b.nodes[e0]] : make_double4(0.0, 0.0, 0.0, 0.0);
+        T H[9];
+#pragma unroll
+        for (int m = 0; m < 9; ++m) H[m] = T(0);
+        for (int32_t e = e0 + r8; e < e1; e += 8) {
+            const double4 u = U4[b.nodes[e]];
+            const T du[3] = {T(diff ? u.x - ur.x : u.x), T(diff ? u.y - ur.y : u.y), T(diff ? u.z - ur.z : u.z)};
+            const T gg[3] = {gr[3 * e], gr[3 * e + 1], gr[3 * e + 2]};
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) H[i * 3 + j] += du[i] * gg[j];
+        }
+#pragma unroll
+        for (int off = 4; off > 0; off >>= 1)
+#pragma unroll
+            for (int m = 0; m < 9; ++m) H[m] += __shfl_xor_sync(kFull, H[m], off);
+        if (has && r8 == 0) {
+#pragma unroll
+            for (int m = 0; m < 9; ++m) sh_t[w][k][m] = H[m];
+            const double J = det_ap_im1(H) + 1.0;
+            sh_j[w][k] = J;
+            if (!(J > 0.0)) flag(status, AM_ENONPOS_J, s);
+        }
+    }
+    __syncwarp();
+    // J-bar, stresses and the dual pressure: one lane per subcell.
+    const bool own = lane < ns;
+    const int64_t s = s0 + lane;
+    T H[9], Pb[9];
+    double V = 0.0, J = 1.0;
+    if (own) {
+#pragma unroll
+        for (int m = 0; m < 9; ++m) H[m] = sh_t[w][lane][m];
+        J = sh_j[w][lane];
+        V = b.volumes[s];
+    }
+    double jv = own ? J * V : 0.0, vol = own ? V : 0.0;
+    warp_sum2(jv, vol);
+    const double Jbar = ns > 0 ? jv / vol : 1.0;
+    double js = 1.0, pd = 0.0, unused = 0.0;
+    if (own) {
+        const double ratio = Jbar / J;
+        js = cbrt(ratio);
+        T Hb[9];
+        if (fabs(ratio - 1.0) < 3.0 * 2.2204460492503131e-16) {
+#pragma unroll
+            for (int m = 0; m < 9; ++m) Hb[m] = H[m];
+        } else {
+#pragma unroll
+            for (int m = 0; m < 9; ++m) Hb[m] = H[m] * T(js);
+            Hb[0] += T(js - 1.0);
+            Hb[4] += T(js - 1.0);
+            Hb[8] += T(js - 1.0);
+        }
+        double lam, mu;
+        element_lame(b, s, lam, mu);
+        const double Jb = stress<T>(MAT, T(lam), T(mu), Hb, Pb);
+        if (MAT == kNeoHookean && !(Jb > 0.0)) flag(status, AM_ENONPOS_J, s);
+        double pf = static_cast<double>(Pb[0] + Pb[4] + Pb[8]);
+#pragma unroll
+        for (int m = 0; m < 9; ++m) pf += static_cast<double>(Pb[m] * H[m]);
+        pd = js / (3.0 * Jbar) * V * pf;
+    }
+    warp_sum2(pd, unused);
+    if (own) {
+        pd /= vol;
+        T F[9];
+#pragma unroll
+        for (int m = 0; m < 9; ++m) F[m] = H[m];
+        F[0] += T(1);
+        F[4] += T(1);
+        F[8] += T(1);
+        double pf = 0.0;
+#pragma unroll
+        for (int m = 0; m < 9; ++m) pf += static_cast<double>(Pb[m] * F[m]);
+        const T scal = T(pd - js / (3.0 * J) * pf);
+        T A[9];
+        adj3(F, A);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) sh_t[w][lane][9 + i * 3 + j] = Pb[i * 3 + j] * T(js) + scal * A[j * 3 + i];
+    }
+    __syncwarp();
+    // Forces, eight lanes per subcell.
+    for (int base = 0; base < ns; base += 4) {
+        const int k = base + q;
+        if (k >= ns) continue;
+        const int64_t sk = s0 + k;
+        const int32_t e0 = b.ptr[sk], e1 = b.ptr[sk + 1];
+        T P[9];
+#pragma unroll
+        for (int m = 0; m < 9; ++m) P[m] = sh_t[w][k][9 + m];
+        const T Vt = T(b.volumes[sk]);
+        for (int32_t e = e0 + r8; e < e1; e += 8) {
+            const T gg[3] = {gr[3 * e], gr[3 * e + 1], gr[3 * e + 2]};
+            T f[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) f[i] = (gg[0] * P[i * 3 + 0] + gg[1] * P[i * 3 + 1] + gg[2] * P[i * 3 + 2]) * -Vt;
+            slots[b.slot_pos[e]] = make4(f[0], f[1], f[2]);
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // VJP kernels (FP64): slots receive (dF/du)^T lam per element node; gmu/gkappa
 // receive lam^T dF/dmu_e and lam^T dF/dkappa_e (lambda_e = kappa_e - 2/3 mu_e).
@@ -1894,6 +2037,15 @@ void launch_fbar(const CellBlockDev& b, const double4* U4, void* slots, int* sta
 
 int launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void* slots, int* status, cudaStream_t s) {
     if (b.num_cells == 0) return 0;
+    if (b.group_ptr != nullptr && b.fused) {
+        const unsigned grid = grid_for(b.num_groups * 32, 32 * kFbarWarps);
+        if (mixed) {
+            AM_DISPATCH_MAT(b.material, (k_fbar_fused<float, M><<<grid, 32 * kFbarWarps, 0, s>>>(b, U4, static_cast<float4*>(slots), status)));
+        } else {
+            AM_DISPATCH_MAT(b.material, (k_fbar_fused<double, M><<<grid, 32 * kFbarWarps, 0, s>>>(b, U4, static_cast<double4*>(slots), status)));
+        }
+        return 1;
+    }
     if (b.fbar != nullptr) {
         if (mixed)
             launch_fbar<float>(b, U4, slots, status, s);

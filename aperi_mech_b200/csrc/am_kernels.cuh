@@ -73,6 +73,8 @@ struct CellBlockDev {
     int64_t num_groups;
     const int64_t* group_ptr;
     void* fbar;
+    int32_t max_group;          // most subcells in one cell
+    int32_t fused;              // 1: one warp per cell, one lane per subcell (max_group <= 32)
 };
 constexpr int kFbarStride = 20;
 

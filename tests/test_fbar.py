@@ -165,10 +165,15 @@ def test_nodal_subcells_setup_matches_oracle(gpu, oracle_lib):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("passes", ["fused", "three"])
 @pytest.mark.parametrize("kind", ["neo_hookean", "linear_elastic"])
-def test_fbar_force_and_steps_match_oracle(gpu, oracle_lib, kind):
-    """F-bar force (FP64 and mixed) and 20 steps with a held face against the oracle."""
+def test_fbar_force_and_steps_match_oracle(gpu, oracle_lib, kind, passes, monkeypatch):
+    """F-bar force (FP64 and mixed) and 20 steps with a held face against the oracle, with
+    the one-pass kernel (cells of at most 32 subcells) and with the three-pass form."""
     from aperi_mech_b200 import mesh
+
+    if passes == "three":
+        monkeypatch.setenv("APERI_B200_FBAR_PASSES", "3")
     from aperi_mech_b200.model import BoundaryCondition, ExplicitDynamics
     from aperi_mech_b200.rkpm import nodal_subcells
 
