@@ -23,6 +23,27 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
+// Programmatic dependent launch (sm_90+ PTX griddepcontrol): a kernel launched with
+// programmatic stream serialization may start while its predecessor in the stream is
+// still running; it reads only data that no kernel of the step writes (mesh, mass, BC
+// words) before pdl_wait(), which returns once the predecessor has completed and its
+// writes are visible. pdl_trigger() lets the successor start; both are no-ops for a
+// kernel launched without the attribute.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// Load of data the previous kernel in the stream writes (displacements, force slots),
+// through the coherent cached path. Under programmatic dependent launch that kernel may
+// still be running when this one starts, so such data is not read-only for this
+// kernel's lifetime and must not be read through the non-coherent read-only path that
+// const __restrict__ pointers allow.
+__device__ __forceinline__ double4 ld_dep(const double4* p) {
+    const double2 a = __ldca(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldca(reinterpret_cast<const double2*>(p) + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ float4 ld_dep(const float4* p) { return __ldca(p); }
+
 __device__ __forceinline__ void flag(int* status, int code, int64_t idx) {
     if (status == nullptr) return;
     if (atomicCAS(status + kStatusCode, 0, code) == 0) status[kStatusIndex] = static_cast<int>(idx);
@@ -238,21 +259,27 @@ __global__ void __launch_bounds__(hex6_block<T>(), (sizeof(T) == 4 ? 4 : 1)) k_t
     const int r = static_cast<int>(gt % TPH);
     const bool valid = p < b.num_patches;
     const int64_t pp = valid ? p : 0;
-    // Node data relative to patch node 0: X in FP64 then T, u likewise.
-    const int32_t n0 = b.patch_nodes[pp * 8];
-    const double4 x0 = X4[n0], u0 = U4[n0];
-    T dx[8][3], du[8][3];
+    // Node data relative to patch node 0: X in FP64 then T, u likewise. The mesh data
+    // is read before the wait for the previous kernel (which writes u).
+    int32_t nid[8];
 #pragma unroll
-    for (int a = 0; a < 8; ++a) {
-        if (a == 0) {
-            dx[0][0] = dx[0][1] = dx[0][2] = du[0][0] = du[0][1] = du[0][2] = T(0);
-            continue;
-        }
-        const int32_t n = b.patch_nodes[pp * 8 + a];
-        const double4 x = X4[n], u = U4[n];
+    for (int a = 0; a < 8; ++a) nid[a] = b.patch_nodes[pp * 8 + a];
+    const double4 x0 = X4[nid[0]];
+    T dx[8][3], du[8][3];
+    dx[0][0] = dx[0][1] = dx[0][2] = du[0][0] = du[0][1] = du[0][2] = T(0);
+#pragma unroll
+    for (int a = 1; a < 8; ++a) {
+        const double4 x = X4[nid[a]];
         dx[a][0] = T(x.x - x0.x);
         dx[a][1] = T(x.y - x0.y);
         dx[a][2] = T(x.z - x0.z);
+    }
+    pdl_trigger();
+    pdl_wait();
+    const double4 u0 = ld_dep(U4 + nid[0]);
+#pragma unroll
+    for (int a = 1; a < 8; ++a) {
+        const double4 u = ld_dep(U4 + nid[a]);
         du[a][0] = T(u.x - u0.x);
         du[a][1] = T(u.y - u0.y);
         du[a][2] = T(u.z - u0.z);
@@ -398,14 +425,15 @@ __device__ __forceinline__ void hex_accumulate_r(T (*R)[8], const T* Q, int g) {
     }
 }
 
-// Nodal values (corner-bit order) relative to node 0, FP64 difference then T.
-template <typename T>
+// Nodal values (corner-bit order) relative to node 0, FP64 difference then T. DEP: the
+// values come from the previous kernel (coherent loads, see ld_dep).
+template <typename T, bool DEP = false>
 __device__ __forceinline__ void hex_load_rel(const double4* __restrict__ A, const int32_t* nd, T (*V)[8]) {
-    const double4 a0 = A[nd[0]];
+    const double4 a0 = DEP ? ld_dep(A + nd[0]) : A[nd[0]];
     V[0][0] = V[1][0] = V[2][0] = T(0);
 #pragma unroll
     for (int q = 1; q < 8; ++q) {
-        const double4 a = A[nd[hex_node_of_corner(q)]];
+        const double4 a = DEP ? ld_dep(A + nd[hex_node_of_corner(q)]) : A[nd[hex_node_of_corner(q)]];
         V[0][q] = T(a.x - a0.x);
         V[1][q] = T(a.y - a0.y);
         V[2][q] = T(a.z - a0.z);
@@ -430,7 +458,9 @@ __global__ void __launch_bounds__(sizeof(T) == 8 ? 64 : 128, sizeof(T) == 8 ? 1 
     hex_conn(b, e, nd);
     T X[3][8], U[3][8];
     hex_load_rel(X4, nd, X);
-    hex_load_rel(U4, nd, U);
+    pdl_trigger();
+    pdl_wait();
+    hex_load_rel<T, true>(U4, nd, U);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
         hex_butterfly(X[i]);
@@ -678,18 +708,20 @@ __device__ __forceinline__ const float* cell_grads<float>(const CellBlockDev& b)
 template <typename T, int MAT>
 __global__ void __launch_bounds__(256) k_cell_force_thread(CellBlockDev b, const double4* __restrict__ U4,
                                                             vec4_t<T>* __restrict__ slots, int* status) {
+    pdl_trigger();
+    pdl_wait();
     const int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (c >= b.num_cells) return;
     const int32_t s0 = b.ptr[c], s1 = b.ptr[c + 1];
     if (s1 <= s0) return;
     const T* gr = cell_grads<T>(b);
     const bool diff = sizeof(T) == 4;
-    const double4 ur = U4[b.nodes[s0]];
+    const double4 ur = ld_dep(U4 + b.nodes[s0]);
     T H[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) H[k] = T(0);
     for (int32_t s = s0; s < s1; ++s) {
-        const double4 u = U4[b.nodes[s]];
+        const double4 u = ld_dep(U4 + b.nodes[s]);
         const T du[3] = {T(diff ? u.x - ur.x : u.x), T(diff ? u.y - ur.y : u.y), T(diff ? u.z - ur.z : u.z)};
         const T gg[3] = {gr[3 * s], gr[3 * s + 1], gr[3 * s + 2]};
 #pragma unroll
@@ -720,6 +752,8 @@ __global__ void __launch_bounds__(256) k_cell_force_thread(CellBlockDev b, const
 template <typename T, int MAT, int LPC>
 __global__ void __launch_bounds__(256) k_cell_force_group(CellBlockDev b, const double4* __restrict__ U4,
                                                           vec4_t<T>* __restrict__ slots, int* status) {
+    pdl_trigger();
+    pdl_wait();
     const int64_t gt = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const int64_t c = gt / LPC;
     const int r = static_cast<int>(threadIdx.x % LPC);
@@ -728,12 +762,12 @@ __global__ void __launch_bounds__(256) k_cell_force_group(CellBlockDev b, const 
     const int32_t s0 = valid ? b.ptr[c] : 0, s1 = valid ? b.ptr[c + 1] : 0;
     const T* gr = cell_grads<T>(b);
     const bool diff = sizeof(T) == 4;
-    const double4 ur = s1 > s0 ? U4[b.nodes[s0]] : make_double4(0.0, 0.0, 0.0, 0.0);
+    const double4 ur = s1 > s0 ? ld_dep(U4 + b.nodes[s0]) : make_double4(0.0, 0.0, 0.0, 0.0);
     T H[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) H[k] = T(0);
     for (int32_t s = s0 + r; s < s1; s += LPC) {
-        const double4 u = U4[b.nodes[s]];
+        const double4 u = ld_dep(U4 + b.nodes[s]);
         const T du[3] = {T(diff ? u.x - ur.x : u.x), T(diff ? u.y - ur.y : u.y), T(diff ? u.z - ur.z : u.z)};
         const T gg[3] = {gr[3 * s], gr[3 * s + 1], gr[3 * s + 2]};
 #pragma unroll
@@ -786,12 +820,12 @@ __global__ void __launch_bounds__(256) k_fbar_h(CellBlockDev b, const double4* _
     const int32_t s0 = valid ? b.ptr[c] : 0, s1 = valid ? b.ptr[c + 1] : 0;
     const T* gr = cell_grads<T>(b);
     const bool diff = sizeof(T) == 4;
-    const double4 ur = s1 > s0 ? U4[b.nodes[s0]] : make_double4(0.0, 0.0, 0.0, 0.0);
+    const double4 ur = s1 > s0 ? ld_dep(U4 + b.nodes[s0]) : make_double4(0.0, 0.0, 0.0, 0.0);
     T H[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) H[k] = T(0);
     for (int32_t s = s0 + r; s < s1; s += LPC) {
-        const double4 u = U4[b.nodes[s]];
+        const double4 u = ld_dep(U4 + b.nodes[s]);
         const T du[3] = {T(diff ? u.x - ur.x : u.x), T(diff ? u.y - ur.y : u.y), T(diff ? u.z - ur.z : u.z)};
         const T gg[3] = {gr[3 * s], gr[3 * s + 1], gr[3 * s + 2]};
 #pragma unroll
@@ -938,6 +972,8 @@ __global__ void __launch_bounds__(32 * kFbarWarps) k_fbar_fused(CellBlockDev b, 
                                                                  vec4_t<T>* __restrict__ slots, int* status) {
     __shared__ T sh_t[kFbarWarps][kFbarMaxSub][18];  // H, then the subcell stress
     __shared__ double sh_j[kFbarWarps][kFbarMaxSub];
+    pdl_trigger();
+    pdl_wait();
     const int w = static_cast<int>(threadIdx.x >> 5);
     const int lane = static_cast<int>(threadIdx.x & 31);
     const int q = lane >> 3, r8 = lane & 7;
@@ -953,12 +989,12 @@ __global__ void __launch_bounds__(32 * kFbarWarps) k_fbar_fused(CellBlockDev b, 
         const bool has = k < ns;
         const int64_t s = s0 + k;
         const int32_t e0 = has ? b.ptr[s] : 0, e1 = has ? b.ptr[s + 1] : 0;
-        const double4 ur = e1 > e0 ? U4[b.nodes[e0]] : make_double4(0.0, 0.0, 0.0, 0.0);
+        const double4 ur = e1 > e0 ? ld_dep(U4 + b.nodes[e0]) : make_double4(0.0, 0.0, 0.0, 0.0);
         T H[9];
 #pragma unroll
         for (int m = 0; m < 9; ++m) H[m] = T(0);
         for (int32_t e = e0 + r8; e < e1; e += 8) {
-            const double4 u = U4[b.nodes[e]];
+            const double4 u = ld_dep(U4 + b.nodes[e]);
             const T du[3] = {T(diff ? u.x - ur.x : u.x), T(diff ? u.y - ur.y : u.y), T(diff ? u.z - ur.z : u.z)};
             const T gg[3] = {gr[3 * e], gr[3 * e + 1], gr[3 * e + 2]};
 #pragma unroll
@@ -1445,7 +1481,7 @@ __device__ __forceinline__ void gather(const NodeDev& nd, const vec4_t<S>* __res
             vec4_t<S> v[BATCH];
 #pragma unroll
             for (int k = 0; k < BATCH; ++k)
-                if (p + k * LPN < p1) v[k] = slots[p + k * LPN];
+                if (p + k * LPN < p1) v[k] = ld_dep(slots + p + k * LPN);
 #pragma unroll
             for (int k = 0; k < BATCH; ++k)
                 if (p + k * LPN < p1) {
@@ -1605,11 +1641,13 @@ __global__ void __launch_bounds__(kNodeBlock) k_node_step(NodeDev nd, const vec4
                                                            double4* __restrict__ u_copy, int* status, int rebase) {
     const int64_t i = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / LPN;
     const bool own = i < nd.num_nodes;
-    if (LPN == 1 && !own) return;
-    // The node's own data is independent of the gather: issue its loads first.
+    // The node's own data is independent of the gather: issue its loads first (mass
+    // and BC word before the wait for the element kernels, v and u after it).
     const int64_t j = own ? i : 0;
     const double m = nd.mass[j];
     const uint32_t w = nd.bcword[j];
+    pdl_trigger();
+    pdl_wait();
     const double4 vh = V4[j];
     const double4 u0 = advance ? U4[j] : make_double4(0.0, 0.0, 0.0, 0.0);
     double fx, fy, fz;
@@ -1962,6 +2000,23 @@ inline unsigned grid_for(int64_t n, int per_block) { return static_cast<unsigned
 // ---------------------------------------------------------------------------
 // Launchers
 // ---------------------------------------------------------------------------
+// Launch with programmatic stream serialization (the kernel calls pdl_wait before it
+// reads anything its predecessor writes).
+template <typename... KArgs, typename... Args>
+void launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 #define AM_DISPATCH_MAT(MATVAR, CALL)                    \
     switch (MATVAR) {                                    \
         case kLinearElastic: { constexpr int M = 0; CALL; break; } \
@@ -1974,9 +2029,9 @@ void launch_gauss_force(const GaussBlockDev& b, int mixed, const double4* X4, co
     if (b.num_elems == 0) return;
     if (b.kind == AM_TET4_GAUSS && b.patched == 2) {
         if (mixed) {
-            AM_DISPATCH_MAT(b.material, (k_tet4_hex6_force<float, M, 1><<<grid_for(b.num_patches, hex6_block<float>()), hex6_block<float>(), 0, s>>>(b, X4, U4, static_cast<float4*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (launch_pdl(k_tet4_hex6_force<float, M, 1>, grid_for(b.num_patches, hex6_block<float>()), hex6_block<float>(), s, b, X4, U4, static_cast<float4*>(slots), status)));
         } else {
-            AM_DISPATCH_MAT(b.material, (k_tet4_hex6_force<double, M, 1><<<grid_for(b.num_patches, hex6_block<double>()), hex6_block<double>(), 0, s>>>(b, X4, U4, static_cast<double4*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (launch_pdl(k_tet4_hex6_force<double, M, 1>, grid_for(b.num_patches, hex6_block<double>()), hex6_block<double>(), s, b, X4, U4, static_cast<double4*>(slots), status)));
         }
     } else if (b.kind == AM_TET4_GAUSS && b.patched) {
         const unsigned grid = grid_for(b.num_patches, 8 * kPatchesPerWarp);
@@ -1995,9 +2050,9 @@ void launch_gauss_force(const GaussBlockDev& b, int mixed, const double4* X4, co
     } else {
         const unsigned grid = grid_for(b.num_elems, 128);
         if (mixed) {
-            AM_DISPATCH_MAT(b.material, (k_hex8_force<float, M><<<grid, 128, 0, s>>>(b, X4, U4, static_cast<float4*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (launch_pdl(k_hex8_force<float, M>, grid, 128, s, b, X4, U4, static_cast<float4*>(slots), status)));
         } else {
-            AM_DISPATCH_MAT(b.material, (k_hex8_force<double, M><<<grid_for(b.num_elems, 64), 64, 0, s>>>(b, X4, U4, static_cast<double4*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (launch_pdl(k_hex8_force<double, M>, grid_for(b.num_elems, 64), 64, s, b, X4, U4, static_cast<double4*>(slots), status)));
         }
     }
 }
@@ -2010,8 +2065,8 @@ inline int lanes_per_cell(const CellBlockDev& b) {
 }
 
 #define AM_CELL_GROUP(T, LPC)                                                                         \
-    AM_DISPATCH_MAT(b.material, (k_cell_force_group<T, M, LPC><<<grid_for(b.num_cells * LPC, 256), 256, 0, s>>>( \
-                                    b, U4, static_cast<vec4_t<T>*>(slots), status)))
+    AM_DISPATCH_MAT(b.material, (launch_pdl(k_cell_force_group<T, M, LPC>, grid_for(b.num_cells * LPC, 256), 256, s, \
+                                            b, U4, static_cast<vec4_t<T>*>(slots), status)))
 
 template <typename T, int LPC>
 void launch_fbar_lpc(const CellBlockDev& b, const double4* U4, void* slots, int* status, cudaStream_t s) {
@@ -2040,9 +2095,9 @@ int launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void*
     if (b.group_ptr != nullptr && b.fused) {
         const unsigned grid = grid_for(b.num_groups * 32, 32 * kFbarWarps);
         if (mixed) {
-            AM_DISPATCH_MAT(b.material, (k_fbar_fused<float, M><<<grid, 32 * kFbarWarps, 0, s>>>(b, U4, static_cast<float4*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (launch_pdl(k_fbar_fused<float, M>, grid, 32 * kFbarWarps, s, b, U4, static_cast<float4*>(slots), status)));
         } else {
-            AM_DISPATCH_MAT(b.material, (k_fbar_fused<double, M><<<grid, 32 * kFbarWarps, 0, s>>>(b, U4, static_cast<double4*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (launch_pdl(k_fbar_fused<double, M>, grid, 32 * kFbarWarps, s, b, U4, static_cast<double4*>(slots), status)));
         }
         return 1;
     }
@@ -2056,9 +2111,9 @@ int launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void*
     if (b.max_entries <= 8) {
         const unsigned grid = grid_for(b.num_cells, 256);
         if (mixed) {
-            AM_DISPATCH_MAT(b.material, (k_cell_force_thread<float, M><<<grid, 256, 0, s>>>(b, U4, static_cast<float4*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (launch_pdl(k_cell_force_thread<float, M>, grid, 256, s, b, U4, static_cast<float4*>(slots), status)));
         } else {
-            AM_DISPATCH_MAT(b.material, (k_cell_force_thread<double, M><<<grid, 256, 0, s>>>(b, U4, static_cast<double4*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (launch_pdl(k_cell_force_thread<double, M>, grid, 256, s, b, U4, static_cast<double4*>(slots), status)));
         }
         return 1;
     }
@@ -2133,6 +2188,26 @@ inline bool gather_batch8(const NodeDev& nd, int mixed) {
     return bytes <= (int64_t{64} << 20);
 }
 
+#define AM_NODE_DISPATCH_PDL(KERNEL, ...)                                                             \
+    do {                                                                                              \
+        const int lpn = node_lanes(nd);                                                               \
+        const unsigned grid = grid_for(nd.num_nodes * lpn, kNodeBlock);                               \
+        const bool b8 = gather_batch8(nd, mixed);                                                     \
+        if (mixed) {                                                                                  \
+            const float4* sl = static_cast<const float4*>(slots);                                     \
+            if (lpn == 8) launch_pdl(KERNEL<float, 4, 8>, grid, kNodeBlock, s, nd, sl, __VA_ARGS__);   \
+            else if (lpn == 4) launch_pdl(KERNEL<float, 2, 4>, grid, kNodeBlock, s, nd, sl, __VA_ARGS__); \
+            else if (b8) launch_pdl(KERNEL<float, 8, 1>, grid, kNodeBlock, s, nd, sl, __VA_ARGS__);    \
+            else launch_pdl(KERNEL<float, 4, 1>, grid, kNodeBlock, s, nd, sl, __VA_ARGS__);            \
+        } else {                                                                                      \
+            const double4* sl = static_cast<const double4*>(slots);                                   \
+            if (lpn == 8) launch_pdl(KERNEL<double, 4, 8>, grid, kNodeBlock, s, nd, sl, __VA_ARGS__);  \
+            else if (lpn == 4) launch_pdl(KERNEL<double, 2, 4>, grid, kNodeBlock, s, nd, sl, __VA_ARGS__); \
+            else if (b8) launch_pdl(KERNEL<double, 8, 1>, grid, kNodeBlock, s, nd, sl, __VA_ARGS__);   \
+            else launch_pdl(KERNEL<double, 4, 1>, grid, kNodeBlock, s, nd, sl, __VA_ARGS__);           \
+        }                                                                                             \
+    } while (0)
+
 #define AM_NODE_DISPATCH(KERNEL, ...)                                                                 \
     do {                                                                                              \
         const int lpn = node_lanes(nd);                                                               \
@@ -2179,7 +2254,7 @@ void launch_prologue(const NodeDev& nd, const StepParams* table, double4* U4, do
 void launch_node_step(const NodeDev& nd, int mixed, const void* slots, const StepParams* table, int64_t step,
                       int advance, double4* U4, double4* V4, double4* A4, double4* u_copy, int* status,
                       cudaStream_t s, int rebase) {
-    AM_NODE_DISPATCH(k_node_step, table, step, advance, U4, V4, A4, u_copy, status, rebase);
+    AM_NODE_DISPATCH_PDL(k_node_step, table, step, advance, U4, V4, A4, u_copy, status, rebase);
 }
 
 void launch_adj_prep(const NodeDev& nd, const StepParams* table, int64_t step, const double4* VB, const double4* AB,
