@@ -551,19 +551,58 @@ def power_method_inputs(sim: Simulation):
     return rng.uniform(-1.0, 1.0, size=sim.coords.shape), _mesh.max_edge_length(sim.coords, sim.meta["element_blocks"])
 
 
-def run(source, stream=None) -> dict:
+def run(source, stream=None, power_method_start=None) -> dict:
     """Parse, build the GPU model, and Solve(): the initial acceleration, then the time
     stepper's steps (ExplicitSolver::Solve, src/Solvers/Explicit.cpp:308-483); with the
     power-method stepper the increment is recomputed on the GPU every update_interval steps.
     With an output block and the direct stepper the run stops at the output steps and the
-    result holds the frames (times and nodal fields) the reference would write there."""
+    result holds the frames (times and nodal fields) the reference would write there.
+    power_method_start (N x 3) replaces the seeded start vector of the power method."""
     sim = source if isinstance(source, Simulation) else load(source)
     dt = sim.dt
     frames = None
     with sim.model(stream) as m:
         m.set_state(np.zeros_like(sim.coords), sim.v0)
-        if sim.power_method is not None:
-            m.set_power_method(*power_method_inputs(sim))
+        if sim.power_method is not None and sim.output is not None:
+            # The schedule of am_solve_power_method driven from here, so that the run can
+            # stop at the output steps: every update_interval steps the stable increment
+            # is recomputed at the current state and scaled; runs are cut where the output
+            # scheduler fires, with the same time accumulation.
+            start, edges = power_method_inputs(sim)
+            m.set_power_method(start if power_method_start is None else power_method_start, edges)
+            scale, interval = sim.power_method
+            m.init_acceleration(sim.precision)
+            sched = TimeIncrementScheduler(*sim.output[1:])
+            frames = {"step": [], "time": [], "displacement": [], "velocity": [], "acceleration": []}
+
+            def record(n, t):
+                fu, fv, fa = m.get_state()
+                for k, x in zip(("step", "time", "displacement", "velocity", "acceleration"), (n, t, fu, fv, fa)):
+                    frames[k].append(x)
+
+            if sched.at_next_event(0.0):
+                record(0, 0.0)
+            time, dt, steps = 0.0, 0.0, 0
+            while not time >= sim.time_end and steps < sim.max_steps:
+                full, _, _ = m.stable_time_increment(dt / scale)
+                dt = full * scale
+                seg, t_seg = [], time
+                for _ in range(interval):
+                    if time >= sim.time_end or steps >= sim.max_steps:
+                        break
+                    d = dt if time + dt <= sim.time_end else (0.0 if time > sim.time_end else sim.time_end - time)
+                    seg.append(d)
+                    time += d
+                    steps += 1
+                    if sched.at_next_event(time):
+                        m.run_schedule(seg, sim.precision, t0=t_seg)
+                        seg, t_seg = [], time
+                        record(steps, time)
+                if seg:
+                    m.run_schedule(seg, sim.precision, t0=t_seg)
+        elif sim.power_method is not None:
+            start, edges = power_method_inputs(sim)
+            m.set_power_method(start if power_method_start is None else power_method_start, edges)
             steps, dt = m.solve_power_method(sim.power_method[0], sim.power_method[1], sim.time_end, sim.precision,
                                              sim.max_steps)
         elif sim.output is not None:
@@ -607,7 +646,7 @@ def write_output(result: dict, directory: Path | str = ".") -> Path:
     fields (N x 3 per frame) at every output time, with the coordinates."""
     sim = result["simulation"]
     if sim.output is None or "frames" not in result:
-        raise InputError("no output block (or the power-method stepper, which writes the final state only)")
+        raise InputError("no output block")
     path = Path(directory) / (Path(sim.output[0]).stem + ".npz")
     np.savez(path, coordinates=sim.coords, **result["frames"])
     return path
