@@ -107,6 +107,29 @@ __device__ __forceinline__ T tet4_forces(const T* J, const T* D, double lam, dou
     for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j) H[i * 3 + j] = D[i * 3 + 0] * Ji[0 * 3 + j] + D[i * 3 + 1] * Ji[1 * 3 + j] + D[i * 3 + 2] * Ji[2 * 3 + j];
+    if (MAT == kNeoHookean) {
+        // With P = tau F^-T and F = (J + D) J^-1: w J^-1 P^T = w (J + D)^-1 tau
+        // = adj(J + D) tau / (6 det F), det F being the FP64 DetApIm1(H) + 1 the stress uses.
+        T tau[9];
+        const double Jf = nh_kirchhoff<T>(T(lam), T(mu), H, tau);
+        if (!(Jf > 0.0)) flag(status, AM_ENONPOS_J, e);
+        T Jc[9], A[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) Jc[k] = J[k] + D[k];
+        adj3(Jc, A);
+        const T sc = T(1.0 / (6.0 * Jf));
+#pragma unroll
+        for (int i = 0; i < 3; ++i) f[i] = T(0);
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const T q = sc * (A[k * 3 + 0] * tau[0 * 3 + i] + A[k * 3 + 1] * tau[1 * 3 + i] + A[k * 3 + 2] * tau[2 * 3 + i]);
+                f[(k + 1) * 3 + i] = -q;
+                f[i] += q;
+            }
+        return det;
+    }
     T P[9];
     const double Jf = stress<T>(MAT, T(lam), T(mu), H, P);
     if (MAT == kNeoHookean && !(Jf > 0.0)) flag(status, AM_ENONPOS_J, e);

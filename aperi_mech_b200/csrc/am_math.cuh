@@ -87,6 +87,22 @@ __device__ __forceinline__ double log1p_nh(double x) {
 //   linear elastic  (LinearElastic.h:79-87): P = lambda tr(eps) I + 2 mu eps, eps = sym(H)
 //   neo-Hookean     (NeoHooke.h:79-91):      tau = lambda log1p(J-1) I + mu (H H^T + H + H^T), P = tau F^-T
 //   St-Venant-K.    (Elastic.h:70-78):       E = (H + H^T + H^T H)/2, S = lambda tr(E) I + 2 mu E, P = F S
+// Neo-Hookean Kirchhoff stress tau = lambda log1p(J-1) I + mu (H H^T + H + H^T)
+// (NeoHooke.h:79-91); returns J = det F (FP64).
+template <typename T>
+__device__ __forceinline__ double nh_kirchhoff(T lambda, T mu, const T* H, T* tau) {
+    const double Jm1 = det_ap_im1(H);
+    const T lam_lnJ = T((double)lambda * log1p_nh(Jm1));
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const T hh = H[i * 3 + 0] * H[j * 3 + 0] + H[i * 3 + 1] * H[j * 3 + 1] + H[i * 3 + 2] * H[j * 3 + 2];
+            tau[i * 3 + j] = mu * (hh + H[j * 3 + i] + H[i * 3 + j]) + (i == j ? lam_lnJ : T(0));
+        }
+    return 1.0 + Jm1;
+}
+
 template <typename T>
 __device__ __forceinline__ double stress(int32_t mat, T lambda, T mu, const T* H, T* P) {
     if (mat == kLinearElastic) {
@@ -104,19 +120,10 @@ __device__ __forceinline__ double stress(int32_t mat, T lambda, T mu, const T* H
     F[4] += T(1);
     F[8] += T(1);
     if (mat == kNeoHookean) {
-        const double Jm1 = det_ap_im1(H);
-        const double J = 1.0 + Jm1;
-        const T lam_lnJ = T((double)lambda * log1p_nh(Jm1));
+        T tau[9];
+        const double J = nh_kirchhoff(lambda, mu, H, tau);
         T Fi[9];
         cof_inv3(F, Fi, T(J));
-        T tau[9];
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                const T hh = H[i * 3 + 0] * H[j * 3 + 0] + H[i * 3 + 1] * H[j * 3 + 1] + H[i * 3 + 2] * H[j * 3 + 2];
-                tau[i * 3 + j] = mu * (hh + H[j * 3 + i] + H[i * 3 + j]) + (i == j ? lam_lnJ : T(0));
-            }
         // P = tau F^-T : P_ij = sum_k tau_ik Fi_jk
 #pragma unroll
         for (int i = 0; i < 3; ++i)
