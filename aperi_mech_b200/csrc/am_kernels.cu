@@ -2037,7 +2037,12 @@ void launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, cudaStr
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+    if (cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...) != cudaSuccess) {
+        // Clear the error and launch in the ordinary way (the kernel's wait is then a no-op);
+        // a failure of that launch is what the caller's error check reports.
+        (void)cudaGetLastError();
+        kernel<<<grid, block, 0, s>>>(static_cast<KArgs>(args)...);
+    }
 }
 
 #define AM_DISPATCH_MAT(MATVAR, CALL)                    \
