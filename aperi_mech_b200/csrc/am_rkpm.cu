@@ -532,8 +532,13 @@ int am_rkpm_nodal_subcells(int64_t N, const double* X, int64_t T, const int32_t*
     return nodal_cells(N, X, T, tets, R, max_neighbors, density, true, out);
 }
 
-int am_rkpm_element_cells(int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R,
-                          int32_t max_neighbors, double density, am_cells** out) {
+}  // extern "C"
+
+namespace {
+
+// Element cells of Tet4 (nn = 4) or Hex8 (nn = 8) elements.
+int element_cells(int nn, int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R,
+                  int32_t max_neighbors, double density, am_cells** out) {
     am::set_free_error("");
     if (!out) return AM_EINVAL;
     *out = nullptr;
@@ -541,8 +546,8 @@ int am_rkpm_element_cells(int64_t N, const double* X, int64_t T, const int32_t* 
         if (N <= 0 || T <= 0 || !X || !tets || !R) throw Fail{AM_EINVAL, "empty mesh or null array"};
         if (max_neighbors <= 0) throw Fail{AM_EINVAL, "max_neighbors must be positive"};
         if (!(density > 0.0)) throw Fail{AM_EINVAL, "density must be positive"};
-        for (int64_t i = 0; i < 4 * T; ++i)
-            if (tets[i] < 0 || tets[i] >= N) throw Fail{AM_EINVAL, "tet node index out of range"};
+        for (int64_t i = 0; i < nn * T; ++i)
+            if (tets[i] < 0 || tets[i] >= N) throw Fail{AM_EINVAL, "element node index out of range"};
         double rmax = 0.0;
         for (int64_t j = 0; j < N; ++j) {
             if (!(R[j] > 0.0)) throw Fail{AM_EINVAL, "kernel radii must be positive"};
@@ -554,14 +559,26 @@ int am_rkpm_element_cells(int64_t N, const double* X, int64_t T, const int32_t* 
         // The functions are needed at the vertices only.
         c->points.assign(X, X + 3 * N);
         rk_functions(c, N, X, R, rmax, max_neighbors);
-        // One cell per tet: entries = union of the four vertices' neighbours (vertex order,
-        // then neighbour order); b_{t,j} = sum_k B_{t,k} V_t psi_k(j) / V_t.
+        // One cell per element: entries = union of the vertices' neighbours (vertex order,
+        // then neighbour order); b_{t,j} = sum_k B_{t,k} V_t psi_k(j) / V_t, B the smoothed
+        // gradients (for a tet the exact linear ones; for a hex QuadratureSmoothed.h:97-142).
         std::vector<std::vector<int32_t>> cn(T);
         std::vector<std::vector<double>> cg(T);
         c->cell_volumes.assign(T, 0.0);
         std::atomic<int> bad(0);
         parallel_for(T, [&](int64_t t) {
-            const int32_t* v = tets + 4 * t;
+            const int32_t* v = tets + nn * t;
+            double B[24], V;
+            if (nn == 8) {
+                double hx[24];
+                for (int k = 0; k < 8; ++k)
+                    for (int d = 0; d < 3; ++d) hx[k * 3 + d] = X[v[k] * 3 + d];
+                hex_smoothed(hx, B, &V);
+                if (!(V > 0.0)) {
+                    bad = 1;
+                    return;
+                }
+            } else {
             double J[9];  // J[i][a] = x_{a+1,i} - x_{0,i}
             for (int i = 0; i < 3; ++i)
                 for (int a = 0; a < 3; ++a) J[i * 3 + a] = X[v[a + 1] * 3 + i] - X[v[0] * 3 + i];
@@ -578,16 +595,16 @@ int am_rkpm_element_cells(int64_t N, const double* X, int64_t T, const int32_t* 
                                   (J[0] * J[8] - J[2] * J[6]) * id, (J[2] * J[3] - J[0] * J[5]) * id,
                                   (J[3] * J[7] - J[4] * J[6]) * id, (J[1] * J[6] - J[0] * J[7]) * id,
                                   (J[0] * J[4] - J[1] * J[3]) * id};
-            double B[12];
             for (int i = 0; i < 3; ++i) {
                 B[3 + i] = Ji[0 * 3 + i];
                 B[6 + i] = Ji[1 * 3 + i];
                 B[9 + i] = Ji[2 * 3 + i];
                 B[i] = -(B[3 + i] + B[6 + i] + B[9 + i]);
             }
-            const double V = det / 6.0;
+            V = det / 6.0;
+            }
             c->cell_volumes[t] = V;
-            for (int k = 0; k < 4; ++k)
+            for (int k = 0; k < nn; ++k)
                 for (int64_t e = c->nbr_ptr[v[k]]; e < c->nbr_ptr[v[k] + 1]; ++e) {
                     const int32_t j = c->nbr[e];
                     size_t idx = std::find(cn[t].begin(), cn[t].end(), j) - cn[t].begin();
@@ -599,7 +616,7 @@ int am_rkpm_element_cells(int64_t N, const double* X, int64_t T, const int32_t* 
                 }
             for (double& g : cg[t]) g /= V;
         });
-        if (bad) throw Fail{AM_ENONPOS_J, "a tet has non-positive volume"};
+        if (bad) throw Fail{AM_ENONPOS_J, "an element has non-positive volume"};
         c->cell_ptr.assign(T + 1, 0);
         for (int64_t t = 0; t < T; ++t) c->cell_ptr[t + 1] = c->cell_ptr[t] + static_cast<int64_t>(cn[t].size());
         const int64_t K = c->cell_ptr[T];
@@ -610,10 +627,10 @@ int am_rkpm_element_cells(int64_t N, const double* X, int64_t T, const int32_t* 
             std::copy(cn[t].begin(), cn[t].end(), c->cell_nodes.begin() + c->cell_ptr[t]);
             std::copy(cg[t].begin(), cg[t].end(), c->cell_grads.begin() + 3 * c->cell_ptr[t]);
         });
-        // Lumped mass: rho V_t / 4 to the vertices, scattered through the functions.
+        // Lumped mass: rho V_t / nn to the vertices, scattered through the functions.
         std::vector<double> mfe(N, 0.0);
         for (int64_t t = 0; t < T; ++t)
-            for (int k = 0; k < 4; ++k) mfe[tets[4 * t + k]] += density * c->cell_volumes[t] / 4;
+            for (int k = 0; k < nn; ++k) mfe[tets[nn * t + k]] += density * c->cell_volumes[t] / nn;
         c->mass.assign(N, 0.0);
         for (int64_t q = 0; q < N; ++q)
             for (int64_t e = c->nbr_ptr[q]; e < c->nbr_ptr[q + 1]; ++e) c->mass[c->nbr[e]] += mfe[q] * c->psi[e];
@@ -629,6 +646,20 @@ int am_rkpm_element_cells(int64_t N, const double* X, int64_t T, const int32_t* 
         am::set_free_error(e.what());
         return AM_EINVAL;
     }
+}
+
+}  // namespace
+
+extern "C" {
+
+int am_rkpm_element_cells(int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R,
+                          int32_t max_neighbors, double density, am_cells** out) {
+    return element_cells(4, N, X, T, tets, R, max_neighbors, density, out);
+}
+
+int am_rkpm_hex8_element_cells(int64_t N, const double* X, int64_t E, const int32_t* hexes, const double* R,
+                               int32_t max_neighbors, double density, am_cells** out) {
+    return element_cells(8, N, X, E, hexes, R, max_neighbors, density, out);
 }
 
 int am_cells_sizes(const am_cells* c, int64_t* num_cells, int64_t* num_entries, int64_t* num_points,

@@ -328,8 +328,6 @@ def _part(pnode: dict, blocks: dict, coords, ext: dict, rng):
     if force_one and force_two:
         raise InputError("Cannot force both one pass and two pass methods")
     one_pass = force_one or (not force_two and "element_smoothing_cell" not in snode)
-    if conn.shape[1] != 4:
-        raise InputError(f"strain_smoothing on block {name}: Tet4 meshes only")
     cell = "nodal_smoothing_cell" if "nodal_smoothing_cell" in snode else "element_smoothing_cell"
     sub = int(((snode.get(cell) or {}).get("subdomains", 1)))
     # MeshLabelerProcessor.h:832-870: element cells always hold one subcell (other values
@@ -339,6 +337,15 @@ def _part(pnode: dict, blocks: dict, coords, ext: dict, rng):
         raise InputError(f"nodal_smoothing_cell.subdomains = {sub}: num_subcells > 1 is not implemented")
     if cell == "element_smoothing_cell":
         sub = 1
+    # include/Element.h:32-86: Hex8 blocks take strain smoothing only with the
+    # reproducing-kernel space; nodal cells are built here from a tet mesh's thex refinement.
+    if conn.shape[1] not in (4, 8):
+        raise InputError(f"block {name}: {conn.shape[1]}-node elements (Tet4 or Hex8 only)")
+    if conn.shape[1] == 8 and space == "finite_element":
+        raise InputError("Strain Smoothing is not supported for finite elements and Hexahedron8")
+    if conn.shape[1] == 8 and cell == "nodal_smoothing_cell":
+        raise InputError(f"nodal_smoothing_cell on the Hex8 block {name}: nodal cells are built from the tet mesh "
+                         "(its thex refinement is formed here)")
     if space == "finite_element" and cell == "element_smoothing_cell":
         from .smoothing import element_smoothing_part
 

@@ -91,9 +91,11 @@ def nodal_subcells(coords: np.ndarray, tets: np.ndarray, material: Material, ker
 def element_cells(coords: np.ndarray, tets: np.ndarray, material: Material, kernel_radius: np.ndarray,
                   max_neighbors: int = 40, keep_points: bool = False, mu_field=None, kappa_field=None,
                   name: str = "block_1") -> RKPMCells:
-    """One cell per tet (element_smoothing_cell with the reproducing_kernel space)."""
-    return _cells("am_rkpm_element_cells", coords, tets, material, kernel_radius, max_neighbors, keep_points,
-                  mu_field, kappa_field, name)
+    """One cell per element (element_smoothing_cell with the reproducing_kernel space):
+    Tet4 (4 columns) or Hex8 (8 columns, reference node order) connectivity."""
+    entry = "am_rkpm_hex8_element_cells" if np.asarray(tets).shape[1] == 8 else "am_rkpm_element_cells"
+    return _cells(entry, coords, tets, material, kernel_radius, max_neighbors, keep_points, mu_field, kappa_field,
+                  name)
 
 
 def two_pass_element_cells(coords: np.ndarray, tets: np.ndarray, material: Material, kernel_radius: np.ndarray,

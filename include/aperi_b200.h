@@ -199,6 +199,12 @@ int am_rkpm_nodal_subcells(int64_t num_nodes, const double* coords, int64_t num_
 int am_cells_groups(const am_cells* cells, int64_t* num_groups, int64_t* group_ptr);
 int am_rkpm_element_cells(int64_t num_nodes, const double* coords, int64_t num_tets, const int32_t* tets,
                           const double* kernel_radius, int32_t max_neighbors, double density, am_cells** out);
+/* The same for Hex8 elements (ElementReproducingKernelHex8 with element_smoothing_cell, the
+ * reference's rkpm_hex inputs): one cell per hex (reference node order), gradients from the
+ * smoothed Hex8 quadrature (QuadratureSmoothed.h:97-142) through the vertices' functions,
+ * mass rho V / 8 to the vertices scattered through the functions. */
+int am_rkpm_hex8_element_cells(int64_t num_nodes, const double* coords, int64_t num_hexes, const int32_t* hexes,
+                               const double* kernel_radius, int32_t max_neighbors, double density, am_cells** out);
 int am_cells_sizes(const am_cells* cells, int64_t* num_cells, int64_t* num_entries, int64_t* num_points,
                    int64_t* num_nbr_entries);
 /* cell_ptr (num_cells+1), cell_nodes/cell_grads (entries, x3), cell_volumes (num_cells)

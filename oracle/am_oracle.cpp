@@ -1522,11 +1522,11 @@ extern "C" int ob_rkpm_nodal_subcells(int64_t N, const double* X, int64_t T, con
 // (src/MassUtils.cpp:17-46, FunctionEvaluationProcessor.h:130-176).
 // Two calls: sizes first (outputs NULL), then the arrays.
 // ---------------------------------------------------------------------------
-extern "C" int ob_rkpm_element_cells(int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R,
-                                     int32_t max_neighbors, double density, int64_t* num_nbr_entries,
-                                     int64_t* num_cell_entries, int64_t* nbr_ptr, int32_t* nbr, double* values,
-                                     int64_t* cell_ptr, int32_t* cell_nodes, double* cell_grads, double* cell_volumes,
-                                     double* mass) {
+namespace {
+int element_cells_impl(int nn, int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R,
+                       int32_t max_neighbors, double density, int64_t* num_nbr_entries, int64_t* num_cell_entries,
+                       int64_t* nbr_ptr, int32_t* nbr, double* values, int64_t* cell_ptr, int32_t* cell_nodes,
+                       double* cell_grads, double* cell_volumes, double* mass) {
     std::vector<std::vector<int32_t>> nb(N);
 #pragma omp parallel for schedule(dynamic, 64)
     for (int64_t p = 0; p < N; ++p) {
@@ -1553,15 +1553,17 @@ extern "C" int ob_rkpm_element_cells(int64_t N, const double* X, int64_t T, cons
     std::vector<std::vector<double>> cg(T);
     std::vector<double> cv(T, 0.0), mfe(N, 0.0);
     for (int64_t t = 0; t < T; ++t) {
-        const int32_t* v = tets + 4 * t;
-        double xt[12], B[12], V;
-        for (int k = 0; k < 4; ++k)
+        const int32_t* v = tets + nn * t;
+        double xt[24], B[24], V;
+        for (int k = 0; k < nn; ++k)
             for (int c = 0; c < 3; ++c) xt[k * 3 + c] = X[v[k] * 3 + c];
-        ob_tet4_smoothed_bw(xt, B, &V);
+        if (nn == 8)
+            ob_hex8_smoothed_bw(xt, B, &V);
+        else
+            ob_tet4_smoothed_bw(xt, B, &V);
         cv[t] = V;
-        std::vector<int32_t> seen;
-        for (int k = 0; k < 4; ++k) {
-            mfe[v[k]] += density * V / 4;
+        for (int k = 0; k < nn; ++k) {
+            mfe[v[k]] += density * V / nn;
             for (int64_t s = ptr[v[k]]; s < ptr[v[k] + 1]; ++s) {
                 const int32_t j = flat[s];
                 int64_t idx = std::find(cn[t].begin(), cn[t].end(), j) - cn[t].begin();
@@ -1598,6 +1600,27 @@ extern "C" int ob_rkpm_element_cells(int64_t N, const double* X, int64_t T, cons
             for (int64_t s = ptr[p]; s < ptr[p + 1]; ++s) mass[flat[s]] += mfe[p] * psi[s];
     }
     return 0;
+}
+}  // namespace
+
+extern "C" int ob_rkpm_element_cells(int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R,
+                                     int32_t max_neighbors, double density, int64_t* num_nbr_entries,
+                                     int64_t* num_cell_entries, int64_t* nbr_ptr, int32_t* nbr, double* values,
+                                     int64_t* cell_ptr, int32_t* cell_nodes, double* cell_grads, double* cell_volumes,
+                                     double* mass) {
+    return element_cells_impl(4, N, X, T, tets, R, max_neighbors, density, num_nbr_entries, num_cell_entries, nbr_ptr,
+                              nbr, values, cell_ptr, cell_nodes, cell_grads, cell_volumes, mass);
+}
+
+// The same for Hex8 elements (ElementReproducingKernelHex8 with element cells): the smoothed
+// Hex8 gradients (QuadratureSmoothed.h:97-142), mass rho V / 8 to the vertices.
+extern "C" int ob_rkpm_hex8_element_cells(int64_t N, const double* X, int64_t E, const int32_t* hexes, const double* R,
+                                          int32_t max_neighbors, double density, int64_t* num_nbr_entries,
+                                          int64_t* num_cell_entries, int64_t* nbr_ptr, int32_t* nbr, double* values,
+                                          int64_t* cell_ptr, int32_t* cell_nodes, double* cell_grads,
+                                          double* cell_volumes, double* mass) {
+    return element_cells_impl(8, N, X, E, hexes, R, max_neighbors, density, num_nbr_entries, num_cell_entries, nbr_ptr,
+                              nbr, values, cell_ptr, cell_nodes, cell_grads, cell_volumes, mass);
 }
 
 // ---------------------------------------------------------------------------

@@ -156,6 +156,13 @@ int ob_rkpm_element_cells(int64_t num_nodes, const double* coords, int64_t num_t
                           double* values, int64_t* cell_ptr, int32_t* cell_nodes, double* cell_grads,
                           double* cell_volumes, double* mass);
 
+/* The same for Hex8 elements: smoothed Hex8 gradients, mass rho V / 8 to the vertices. */
+int ob_rkpm_hex8_element_cells(int64_t num_nodes, const double* coords, int64_t num_hexes, const int32_t* hexes,
+                               const double* kernel_radius, int32_t max_neighbors, double density,
+                               int64_t* num_nbr_entries, int64_t* num_cell_entries, int64_t* nbr_ptr, int32_t* nbr,
+                               double* values, int64_t* cell_ptr, int32_t* cell_nodes, double* cell_grads,
+                               double* cell_volumes, double* mass);
+
 /* Stable time increment by the power method (PowerMethodProcessor.h:331-480) at the
  * displacement u; v (num_nodes x 3) is the eigenvector estimate, updated in place; l is
  * each node's longest edge. Returns the increment. */

@@ -110,6 +110,8 @@ def lib() -> C.CDLL:
         L.ob_lagrangian_init.argtypes = [C.POINTER(OProblem), C.POINTER(OLagrangian), _dp]
         L.ob_lagrangian_steps.argtypes = [C.POINTER(OProblem), C.POINTER(OLagrangian), C.c_int64, _dp, C.c_double, _dp,
                                           _dp, _dp]
+        L.ob_rkpm_hex8_element_cells.argtypes = [C.c_int64, _dp, C.c_int64, _ip, _dp, C.c_int32, C.c_double, _lp,
+                                                 _lp, _lp, _ip, _dp, _lp, _ip, _dp, _dp, _dp]
         L.ob_stable_time_increment.argtypes = [C.POINTER(OProblem), _dp, _dp, _dp, C.c_double, C.c_int32, C.c_double,
                                                C.c_double, C.c_double, _ip, _ip]
         L.ob_stable_time_increment.restype = C.c_double
@@ -340,20 +342,22 @@ def rkpm_nodal_cells(coords, tets, kernel_radius, max_neighbors=40, density=1000
 
 
 def rkpm_element_cells(coords, tets, kernel_radius, max_neighbors=40, density=1000.0):
-    """Oracle RKPM element cells: dict with nbr_ptr, nbr, values (at the vertices),
-    cell_ptr, cell_nodes, cell_grads, cell_volumes, mass."""
+    """Oracle RKPM element cells (Tet4 or Hex8 elements, from the connectivity's width):
+    dict with nbr_ptr, nbr, values (at the vertices), cell_ptr, cell_nodes, cell_grads,
+    cell_volumes, mass."""
     X = np.ascontiguousarray(coords, dtype=np.float64)
     T = np.ascontiguousarray(tets, dtype=np.int32)
     R = np.ascontiguousarray(kernel_radius, dtype=np.float64)
+    fn = lib().ob_rkpm_hex8_element_cells if T.shape[1] == 8 else lib().ob_rkpm_element_cells
     S, K = C.c_int64(), C.c_int64()
     args = (X.shape[0], _p(X), T.shape[0], _p(T, C.c_int32), _p(R), int(max_neighbors), float(density))
-    lib().ob_rkpm_element_cells(*args, C.byref(S), C.byref(K), *([None] * 8))
+    fn(*args, C.byref(S), C.byref(K), *([None] * 8))
     N, E = X.shape[0], T.shape[0]
     out = {"nbr_ptr": np.empty(N + 1, dtype=np.int64), "nbr": np.empty(S.value, dtype=np.int32),
            "values": np.empty(S.value), "cell_ptr": np.empty(E + 1, dtype=np.int64),
            "cell_nodes": np.empty(K.value, dtype=np.int32), "cell_grads": np.empty((K.value, 3)),
            "cell_volumes": np.empty(E), "mass": np.empty(N)}
-    lib().ob_rkpm_element_cells(*args, None, None, _p(out["nbr_ptr"], C.c_int64), _p(out["nbr"], C.c_int32),
+    fn(*args, None, None, _p(out["nbr_ptr"], C.c_int64), _p(out["nbr"], C.c_int32),
                                 _p(out["values"]), _p(out["cell_ptr"], C.c_int64), _p(out["cell_nodes"], C.c_int32),
                                 _p(out["cell_grads"]), _p(out["cell_volumes"]), _p(out["mass"]))
     return out

@@ -175,6 +175,12 @@ def test_output_steps_follow_the_solver_loop():
                        "strain_smoothing: {nodal_smoothing_cell: {subdomains: 2}, use_f_bar: true}").replace(
         "finite_element: ~", "reproducing_kernel: {kernel_radius_scale_factor: 1.1}"), "num_subcells > 1"),
     (nh_yaml().replace("components: {X: 1.0, Z: -0.5}", "components: {W: 1.0}"), "component"),
+    (nh_yaml(mesh_opts="|sideset:z").replace("gauss_quadrature: {integration_order: 1}",
+                                             "strain_smoothing: {element_smoothing_cell: {subdomains: 1}}"),
+     "finite elements and Hexahedron8"),
+    (nh_yaml(mesh_opts="|sideset:z").replace("gauss_quadrature: {integration_order: 1}",
+                                             "strain_smoothing: {nodal_smoothing_cell: {subdomains: 1}}").replace(
+        "finite_element: ~", "reproducing_kernel: {kernel_radius_scale_factor: 1.1}"), "Hex8 block"),
     (nh_yaml().replace("gauss_quadrature: {integration_order: 1}",
                        "strain_smoothing: {element_smoothing_cell: {subdomains: 1}, force_one_pass_method: true, "
                        "force_two_pass_method: true}"), "Cannot force both"),
@@ -326,6 +332,25 @@ def test_yaml_output_frames_match_oracle(oracle_lib, tmp_path):
     with np.load(path) as z:
         assert z["displacement"].shape == (len(fr["step"]),) + sim.coords.shape
         assert np.array_equal(z["time"], fr["time"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("one_pass", [True, False])
+def test_yaml_rkpm_hex8_element_cells_match_oracle(oracle_lib, one_pass):
+    """element_smoothing_cell with reproducing_kernel on a Hex8 block (the reference's
+    rkpm_hex inputs), one-pass or the two-pass default."""
+    flag = ", force_one_pass_method: true" if one_pass else ""
+    text = nh_yaml(n=3, mesh_opts="|sideset:z").replace(
+        "gauss_quadrature: {integration_order: 1}",
+        f"strain_smoothing: {{element_smoothing_cell: {{subdomains: 1}}{flag}}}").replace(
+        "finite_element: ~", "reproducing_kernel: {kernel_radius_scale_factor: 1.0}")
+    sim = inp.load(text)
+    assert sim.parts[0].num_elems == 27 and (sim.rk is None) == one_pass
+    r = inp.run(sim)
+    prob = oracle_lib.OracleProblem(sim.coords, sim.parts, sim.bcs, mass=sim.mass, rk=sim.rk)
+    u, v, a, n = prob.solve(np.zeros_like(sim.coords), sim.v0, sim.dt, sim.time_end)
+    assert r["steps"] == n
+    assert np.linalg.norm(r["displacement"] - u) <= 1e-12 * np.linalg.norm(u)
 
 
 @pytest.mark.gpu

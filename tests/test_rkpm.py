@@ -311,3 +311,84 @@ def test_rkpm_two_pass_force_and_steps_match_oracle(gpu, oracle_lib):
     # the physical displacement reproduces a linear field of the coefficients
     A = 1e-3 * rng.standard_normal((3, 3))
     assert np.abs(apply_functions(cells.functions(), X @ A.T) - X @ A.T).max() < 1e-12
+
+
+# ---- RKPM element cells on Hex8 meshes (ElementReproducingKernelHex8) ------------------
+def _hex_box(n=3, seed=4, jitter=0.15):
+    from aperi_mech_b200 import mesh
+
+    coords, conn = mesh.box_hex(n, n, 2 * n, 1.0, 1.0, 2.0)
+    return mesh.jitter_interior(coords, jitter / n, np.random.default_rng(seed)), conn
+
+
+def test_oracle_rk_hex8_element_cells(oracle_lib):
+    """Hex cells: partition of unity and linear completeness of the vertex functions,
+    partition of nullity and exact linear-field gradients per cell, volume and mass."""
+    from aperi_mech_b200.rkpm import tet_max_edge_length
+
+    X, E = _hex_box()
+    r = oracle_lib.rkpm_element_cells(X, E, 1.1 * tet_max_edge_length(X, E), max_neighbors=40, density=1000.0)
+    ptr, nb, v = r["nbr_ptr"], r["nbr"], r["values"]
+    rows = _rows(ptr)
+    assert np.abs(np.bincount(rows, weights=v, minlength=X.shape[0]) - 1.0).max() < 4e-12
+    lc = np.zeros_like(X)
+    np.add.at(lc, rows, v[:, None] * X[nb])
+    assert np.abs(lc - X).max() < 4e-11
+    g, cp, cn = r["cell_grads"], r["cell_ptr"], r["cell_nodes"]
+    assert len(cp) == E.shape[0] + 1
+    crow = _rows(cp)
+    nul = np.zeros((E.shape[0], 3))
+    np.add.at(nul, crow, g)
+    assert np.abs(nul).max() < 1e-9
+    A = np.random.default_rng(2).standard_normal((3, 3))
+    H = np.zeros((E.shape[0], 3, 3))
+    np.add.at(H, crow, (X[cn] @ A.T)[:, :, None] * g[:, None, :])
+    assert np.abs(H - A).max() < 1e-9
+    assert abs(r["cell_volumes"].sum() - 2.0) < 1e-12
+    assert abs(r["mass"].sum() - 2000.0) < 1e-9
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("method", ["one_pass", "two_pass"])
+def test_rk_hex8_element_cells_match_oracle(gpu, oracle_lib, method):
+    """Set-up against the oracle, then force and 20 steps (one-pass cells, or the two-pass
+    coupling of the smoothed hexes) at 1e-12."""
+    from aperi_mech_b200 import mesh
+    from aperi_mech_b200.model import BoundaryCondition, ExplicitDynamics, Material
+    from aperi_mech_b200.rkpm import element_cells, tet_max_edge_length, two_pass_element_cells
+
+    X, E = _hex_box(seed=6)
+    R = 1.1 * tet_max_edge_length(X, E)
+    mat = Material.create("neo_hookean", 1000.0, shear_modulus=3.85e8, bulk_modulus=8.33e8)
+    want = oracle_lib.rkpm_element_cells(X, E, R, max_neighbors=40, density=1000.0)
+    if method == "one_pass":
+        cells = element_cells(X, E, mat, R, keep_points=True)
+        p = cells.part
+        assert np.array_equal(p.cell_ptr, want["cell_ptr"]) and np.array_equal(p.cell_nodes, want["cell_nodes"])
+        assert rel_err(p.cell_grads, want["cell_grads"]) < 1e-12
+        rk = None
+    else:
+        cells = two_pass_element_cells(X, E, mat, R)
+        rk = cells.functions()
+    assert np.array_equal(cells.nbr_ptr, want["nbr_ptr"]) and np.array_equal(cells.nbr, want["nbr"])
+    assert rel_err(cells.values, want["values"]) < 1e-12
+    assert rel_err(cells.mass, want["mass"]) < 1e-12
+    fixed = mesh.side_sets(X)["surface_5"]
+    bcs = [BoundaryCondition.fixed(fixed)]
+    rng = np.random.default_rng(8)
+    v0 = rng.uniform(-0.01, 0.01, size=X.shape)
+    v0[:, 0] += X[:, 2]
+    v0[fixed] = 0.0
+    u = 1e-3 * rng.standard_normal(X.shape)
+    op = oracle_lib.OracleProblem(X, [cells.part], bcs, mass=cells.mass, rk=rk)
+    dt = 0.3 * (1.0 / 3.0) / np.sqrt((mat.lam + 2 * mat.mu) / mat.density)
+    zero = np.zeros_like(X)
+    want_state = op.steps(zero, v0, op.init_acceleration(zero), np.full(20, dt))
+    with ExplicitDynamics(X, [cells.part], bcs, mass=cells.mass, rk=rk) as m:
+        assert rel_err(m.internal_force(u), op.internal_force(u)) < 1e-12
+        m.set_state(None, v0)
+        m.init_acceleration()
+        m.run(20, dt)
+        got = m.get_state()
+    for g, w in zip(got, want_state):
+        assert rel_err(g, w) < 1e-12
