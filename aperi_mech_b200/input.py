@@ -33,7 +33,8 @@ library computes, and builds an ExplicitDynamics model on the GPU:
           output: {file, time_start, time_end, time_increment}
                                                     (fields at the output times, as an .npz of frames)
           lagrangian_formulation: {total: ~ | updated: ~ | semi: {update_interval: k}}
-                                                    (IoInputFile.h:188-262; Gauss parts, FP64)
+                                                    (IoInputFile.h:188-262; Gauss parts and Tet4
+                                                    finite-element element cells, FP64)
           x_b200: {precision: fp64 | mixed, seed, jitter, velocity_noise, max_steps,
                    fields: {<part set>: {shear_modulus | bulk_modulus: {lognormal_sigma}}}}
 
@@ -285,7 +286,29 @@ def _material(node: dict) -> Material:
         raise InputError(f"material {kind}: {e}") from None
 
 
-def _part(pnode: dict, blocks: dict, coords, ext: dict, rng):
+def _lagrangian_formulation(proc: dict) -> tuple:
+    """lagrangian_formulation (IoInputFile.h:195-252): ("total", 1),
+    ("updated", 1) or ("semi", update_interval)."""
+    lnode = proc.get("lagrangian_formulation")
+    if lnode is None:
+        return ("total", 1)
+    if not isinstance(lnode, dict):
+        raise InputError("'lagrangian_formulation' must be a map")
+    if "total" in lnode:
+        return ("total", 1)
+    if "updated" in lnode:
+        return ("updated", 1)
+    if "semi" in lnode:
+        k = (lnode.get("semi") or {}).get("update_interval")
+        if k is None:
+            raise InputError("lagrangian_formulation.semi needs update_interval")
+        if int(k) < 1:
+            raise InputError("lagrangian_formulation.semi.update_interval must be at least 1")
+        return ("semi", int(k))
+    raise InputError("lagrangian_formulation must have 'total', 'updated', or 'semi' key")
+
+
+def _part(pnode: dict, blocks: dict, coords, ext: dict, rng, formulation=("total", 1)):
     """One InternalForceContribution: block connectivity + formulation + material.
     Returns (part, lumped mass or None, two-pass functions or None)."""
     name = pnode.get("set")
@@ -346,6 +369,18 @@ def _part(pnode: dict, blocks: dict, coords, ext: dict, rng):
     if conn.shape[1] == 8 and cell == "nodal_smoothing_cell":
         raise InputError(f"nodal_smoothing_cell on the Hex8 block {name}: nodal cells are built from the tet mesh "
                          "(its thex refinement is formed here)")
+    if space == "finite_element" and cell == "element_smoothing_cell" and formulation[0] != "total":
+        # Updated / semi (ElementSmoothedTetrahedron4.h:73-122, ComputeInternalForceSmoothedCell.h:
+        # 326-350): the cell gradients and volume are rebuilt on the reference configuration of
+        # each update, H composes with the stored reference gradient and the force maps back by
+        # F_ref / det F_ref, as for a Gauss element. A Tet4 cell's divergence-theorem gradients
+        # are the tet's exact constant gradients and its volume the tet's, so the cell is the
+        # one-point Gauss tet in every configuration and runs as one.
+        part = Part("tet4", mat, conn=conn, mu_field=mu_f, kappa_field=kappa_f, name=name)
+        return part, None, None
+    if formulation[0] != "total":
+        raise InputError(f"{formulation[0]} Lagrangian formulation: built for Gauss parts and Tet4 "
+                         "finite-element element cells only")
     if space == "finite_element" and cell == "element_smoothing_cell":
         from .smoothing import element_smoothing_part
 
@@ -427,10 +462,11 @@ def load(source, base_dir: Path | None = None) -> Simulation:
     for b, conn in blocks.items():
         sets.setdefault(b, np.unique(conn).astype(np.int32))
 
+    formulation = _lagrangian_formulation(proc)
     parts, masses, rk = [], [], None
     for entry in geo.get("parts") or []:
         _, pnode = _one_key(entry, "parts entry")
-        part, mass, functions = _part(pnode, blocks, coords, ext, rng)
+        part, mass, functions = _part(pnode, blocks, coords, ext, rng, formulation)
         parts.append(part)
         masses.append(mass)
         if functions is not None:
@@ -512,27 +548,7 @@ def load(source, base_dir: Path | None = None) -> Simulation:
         raise InputError(f"x_b200.precision {precision!r} (fp64 or mixed)")
     name = Path(str(source)).stem if isinstance(source, (str, Path)) and "\n" not in str(source) else "input"
     element_blocks = [blocks[(e.get("part") or {}).get("set")] for e in (geo.get("parts") or [])]
-    formulation = ("total", 1)
-    lnode = proc.get("lagrangian_formulation")
-    if lnode is not None:
-        if not isinstance(lnode, dict):
-            raise InputError("'lagrangian_formulation' must be a map")
-        if "total" in lnode:
-            formulation = ("total", 1)
-        elif "updated" in lnode:
-            formulation = ("updated", 1)
-        elif "semi" in lnode:
-            k = (lnode.get("semi") or {}).get("update_interval")
-            if k is None:
-                raise InputError("lagrangian_formulation.semi needs update_interval")
-            formulation = ("semi", int(k))
-            if formulation[1] < 1:
-                raise InputError("lagrangian_formulation.semi.update_interval must be at least 1")
-        else:
-            raise InputError("lagrangian_formulation must have 'total', 'updated', or 'semi' key")
     if formulation[0] != "total":
-        if any(p.kind == "cells" for p in parts):
-            raise InputError(f"{formulation[0]} Lagrangian formulation: built for Gauss parts only")
         if precision != "fp64":
             raise InputError(f"{formulation[0]} Lagrangian formulation runs in FP64 (x_b200.precision: fp64)")
         if power is not None:

@@ -178,3 +178,95 @@ procedures:
     u, v, a = prob.lagrangian_steps(st, z, sim.v0, prob.lagrangian_init(st), dts)
     assert r["steps"] == len(dts)
     assert np.linalg.norm(r["displacement"] - u) <= 1e-12 * np.linalg.norm(u)
+
+
+def test_oracle_tet4_element_cell_is_the_gauss_tet(oracle_lib):
+    """A Tet4 element smoothing cell (divergence-theorem gradients, QuadratureSmoothed.h:
+    32-63) holds the tet's exact constant gradients and volume in any configuration, so its
+    force equals the one-point Gauss tet's: on the mesh and on a deformed copy of it (the
+    configuration an updated or semi reference update rebuilds the cells on)."""
+    from aperi_mech_b200.model import Part
+    from aperi_mech_b200.smoothing import element_smoothing_part
+
+    p = _tet_problem()
+    mat = p.parts[0].material
+    T = p.parts[0].conn
+    rng = np.random.default_rng(3)
+    h = float(np.ptp(p.coords, axis=0).max()) / 4.0
+    for X in (p.coords, p.coords + 0.05 * h * rng.standard_normal(p.coords.shape)):
+        cells, mass = element_smoothing_part(X, T, mat)
+        u = 1e-2 * h * rng.standard_normal(X.shape)
+        f_cell = oracle_lib.OracleProblem(X, [cells]).internal_force(u)
+        gauss = oracle_lib.OracleProblem(X, [Part("tet4", mat, conn=T)])
+        assert rel_err(f_cell, gauss.internal_force(u)) < 1e-12
+        assert rel_err(mass, gauss.lumped_mass()) < 1e-13
+
+
+SMOOTHING_SEMI = """
+procedures:
+  - explicit_dynamics_procedure:
+{lagr}      geometry:
+        mesh: generated:3x3x6|sideset:z|tets|bbox:0,0,0,0.01,0.01,0.02
+        parts:
+          - part:
+              set: block_1
+              formulation:
+                integration_scheme:
+                  strain_smoothing:
+                    element_smoothing_cell:
+                      subdomains: 1
+                approximation_space:
+                  finite_element: ~
+              material:
+                elastic: {{density: 2700.0, youngs_modulus: 78.2e8, poissons_ratio: 0.3}}
+      initial_conditions:
+        - velocity:
+            sets: [block_1]
+            components: {{Z: -373.0}}
+      time_stepper:
+        direct_time_stepper: {{time_increment: 1.0e-7, time_end: 6.0e-6}}
+      boundary_conditions:
+        - displacement:
+            sets: [surface_1]
+            components: {{Z: 0.0}}
+            time_function:
+              ramp_function: {{abscissa_values: [0, 1], ordinate_values: [0, 1]}}
+      x_b200: {{jitter: 0.15}}
+"""
+
+
+def test_yaml_element_smoothing_semi_runs_as_gauss_tets():
+    """The reference's fem_strain_smoothing_semi form (element cells, finite elements,
+    semi update_interval 10) loads as a Tet4 Gauss part under updated / semi and as
+    element cells under the total formulation; reproducing-kernel cells stay refused."""
+    from aperi_mech_b200 import input as inp
+
+    semi = inp.load(SMOOTHING_SEMI.format(lagr="      lagrangian_formulation: {semi: {update_interval: 10}}\n"))
+    assert semi.formulation == ("semi", 10) and semi.parts[0].kind == "tet4" and semi.mass is None
+    total = inp.load(SMOOTHING_SEMI.format(lagr=""))
+    assert total.formulation == ("total", 1) and total.parts[0].kind == "cells"
+    assert np.array_equal(total.coords, semi.coords)
+    rk = SMOOTHING_SEMI.format(lagr="      lagrangian_formulation: {updated: ~}\n").replace(
+        "finite_element: ~", "reproducing_kernel: {kernel_radius_scale_factor: 0.03}")
+    with pytest.raises(inp.InputError, match="Tet4 finite-element element cells only"):
+        inp.load(rk)
+
+
+@pytest.mark.gpu
+def test_yaml_element_smoothing_semi_matches_oracle_and_total(oracle_lib):
+    """The semi run (every tenth step a reference update) against the oracle's semi run of
+    the same tets at 1e-12, and against the total formulation's element-cell run (the cell
+    kernel) at 1e-10: on tets the formulations agree to round-off."""
+    from aperi_mech_b200 import input as inp
+
+    sim = inp.load(SMOOTHING_SEMI.format(lagr="      lagrangian_formulation: {semi: {update_interval: 10}}\n"))
+    r = inp.run(sim)
+    prob = oracle_lib.OracleProblem(sim.coords, sim.parts, sim.bcs)
+    st = prob.lagrangian_state(*sim.formulation)
+    z = np.zeros_like(sim.coords)
+    dts = inp.direct_time_steps(sim.dt, sim.time_end)
+    u, v, a = prob.lagrangian_steps(st, z, sim.v0, prob.lagrangian_init(st), dts)
+    assert r["steps"] == len(dts) == 60 and st.n == 60
+    assert np.linalg.norm(r["displacement"] - u) <= 1e-12 * np.linalg.norm(u)
+    total = inp.run(inp.load(SMOOTHING_SEMI.format(lagr="")))
+    assert np.linalg.norm(total["displacement"] - r["displacement"]) <= 1e-10 * np.linalg.norm(u)
