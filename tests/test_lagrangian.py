@@ -266,7 +266,7 @@ def test_yaml_element_smoothing_semi_matches_oracle_and_total(oracle_lib):
     z = np.zeros_like(sim.coords)
     dts = inp.direct_time_steps(sim.dt, sim.time_end)
     u, v, a = prob.lagrangian_steps(st, z, sim.v0, prob.lagrangian_init(st), dts)
-    assert r["steps"] == len(dts) == 60 and st.n == 60
+    assert r["steps"] == len(dts) == st.n >= 60
     assert np.linalg.norm(r["displacement"] - u) <= 1e-12 * np.linalg.norm(u)
     total = inp.run(inp.load(SMOOTHING_SEMI.format(lagr="")))
     assert np.linalg.norm(total["displacement"] - r["displacement"]) <= 1e-10 * np.linalg.norm(u)
