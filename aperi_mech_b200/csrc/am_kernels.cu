@@ -256,105 +256,123 @@ __global__ void __launch_bounds__(256) k_tet4_patch_force(GaussBlockDev b, const
 }
 
 // ---------------------------------------------------------------------------
-// Tet4 patches that are split hexes (the six tets around the 0-6 diagonal, in the
-// patch-local node order the patch builder produces): the local connectivity is a
-// compile-time table, so each thread keeps its patch's 8 nodes and force sums in
-// registers. TPH threads share one patch (6/TPH tets each) and combine their sums
-// with one butterfly step; no shared memory, no divergence.
+// Tet4 patches that are split hexes: the six tets around the hex diagonal, which is
+// patch-local nodes 0 and 3 in the order the patch builder produces; tet t = (0, a_t, b_t, 3) with
+// (a_t, b_t) running round the ring 1-2-4-5-6-7-1. Two threads share a patch:
+// thread r takes tets 3r..3r+2, the three around ring nodes R_r = (1, 2, 4, 5) for
+// r = 0 and (5, 6, 7, 1) for r = 1, so its tet k is (0, R_r[k], R_r[k+1], 3) and
+// both threads run the same code on six of the eight nodes. The pair's sums meet
+// with three shuffles: node 0 and node 3 from both threads, and each thread's
+// first ring node (1 or 5) from the other thread's last. Per thread this halves
+// the unrolled code and holds 6 nodes' data and sums instead of 8, which is what
+// lets the FP32 kernel run five 128-thread blocks per SM in 96 registers; on B200
+// that ran the element kernel 12% faster (mixed and FP64) than one thread per patch.
 // ---------------------------------------------------------------------------
-__host__ __device__ constexpr int hex6_local(int t, int k) {
-    // patch-local ids of tet t's 4 nodes: (0, a_t, b_t, 3), a = 1,2,4,5,6,7 ; b = 2,4,5,6,7,1
-    return k == 0 ? 0 : k == 3 ? 3 : k == 1 ? (t == 0 ? 1 : t == 1 ? 2 : t + 2) : (t == 0 ? 2 : t == 5 ? 1 : t + 3);
-}
-
-// Small blocks: on B200 the FP32 kernel (held to 128 registers, four 128-thread blocks
-// per SM) ran 3% faster than with 256-thread blocks, and the FP64 kernel (about 190
-// registers, 64-thread blocks) 20% faster, from the finer granularity at equal occupancy.
 template <typename T>
-constexpr int hex6_block() { return sizeof(T) == 4 ? 128 : 64; }
+constexpr int hex6_min_blocks() { return sizeof(T) == 4 ? 5 : 3; }
+constexpr int kHex6Block = 128;
 
-template <typename T, int MAT, int TPH>
-__global__ void __launch_bounds__(hex6_block<T>(), (sizeof(T) == 4 ? 4 : 1)) k_tet4_hex6_force(GaussBlockDev b, const double4* __restrict__ X4,
+template <typename T, int MAT>
+__global__ void __launch_bounds__(kHex6Block, hex6_min_blocks<T>()) k_tet4_hex6_force(GaussBlockDev b, const double4* __restrict__ X4,
                                                           const double4* __restrict__ U4,
                                                           vec4_t<T>* __restrict__ slots, int* status) {
     const int64_t gt = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const int64_t p = gt / TPH;
-    const int r = static_cast<int>(gt % TPH);
+    const int64_t p = gt >> 1;
+    const int r = static_cast<int>(gt & 1);
     const bool valid = p < b.num_patches;
     const int64_t pp = valid ? p : 0;
     // Node data relative to patch node 0: X in FP64 then T, u likewise. The mesh data
-    // is read before the wait for the previous kernel (which writes u).
-    int32_t nid[8];
+    // is read before the wait for the previous kernel (which writes u), and the slot
+    // positions, needed only at the end, are sent to L2 now (on B200 that took 2% off
+    // the FP32 kernel and 5% off the FP64 one).
+    const int4* pn4 = reinterpret_cast<const int4*>(b.patch_nodes + pp * 8);
+    const int4 lo = pn4[0], hi = pn4[1];  // patch-local nodes 0-3 and 4-7
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(b.slot_pos + pp * 8));
+    const int32_t n0 = lo.x, n3 = lo.w;
+    int32_t nr[4];
+    nr[0] = r ? hi.y : lo.y;
+    nr[1] = r ? hi.z : lo.z;
+    nr[2] = r ? hi.w : hi.x;
+    nr[3] = r ? lo.y : hi.y;
+    const double4 x0 = X4[n0];
+    T dx3[3], dxr[4][3], du3[3], dur[4][3];
+    {
+        const double4 x = X4[n3];
+        dx3[0] = T(x.x - x0.x);
+        dx3[1] = T(x.y - x0.y);
+        dx3[2] = T(x.z - x0.z);
+    }
 #pragma unroll
-    for (int a = 0; a < 8; ++a) nid[a] = b.patch_nodes[pp * 8 + a];
-    const double4 x0 = X4[nid[0]];
-    T dx[8][3], du[8][3];
-    dx[0][0] = dx[0][1] = dx[0][2] = du[0][0] = du[0][1] = du[0][2] = T(0);
-#pragma unroll
-    for (int a = 1; a < 8; ++a) {
-        const double4 x = X4[nid[a]];
-        dx[a][0] = T(x.x - x0.x);
-        dx[a][1] = T(x.y - x0.y);
-        dx[a][2] = T(x.z - x0.z);
+    for (int k = 0; k < 4; ++k) {
+        const double4 x = X4[nr[k]];
+        dxr[k][0] = T(x.x - x0.x);
+        dxr[k][1] = T(x.y - x0.y);
+        dxr[k][2] = T(x.z - x0.z);
     }
     pdl_trigger();
     pdl_wait();
-    const double4 u0 = ld_dep(U4 + nid[0]);
-#pragma unroll
-    for (int a = 1; a < 8; ++a) {
-        const double4 u = ld_dep(U4 + nid[a]);
-        du[a][0] = T(u.x - u0.x);
-        du[a][1] = T(u.y - u0.y);
-        du[a][2] = T(u.z - u0.z);
+    const double4 u0 = ld_dep(U4 + n0);
+    {
+        const double4 u = ld_dep(U4 + n3);
+        du3[0] = T(u.x - u0.x);
+        du3[1] = T(u.y - u0.y);
+        du3[2] = T(u.z - u0.z);
     }
-    T acc[8][3];
 #pragma unroll
-    for (int a = 0; a < 8; ++a) acc[a][0] = acc[a][1] = acc[a][2] = T(0);
-    const int64_t e0 = static_cast<int64_t>(b.patch_first[pp]);
+    for (int k = 0; k < 4; ++k) {
+        const double4 u = ld_dep(U4 + nr[k]);
+        dur[k][0] = T(u.x - u0.x);
+        dur[k][1] = T(u.y - u0.y);
+        dur[k][2] = T(u.z - u0.z);
+    }
+    T acc0[3] = {T(0), T(0), T(0)}, acc3[3] = {T(0), T(0), T(0)}, accr[4][3];
 #pragma unroll
-    for (int tt = 0; tt < 6 / TPH; ++tt) {
-        const int t = r * (6 / TPH) + tt;
+    for (int k = 0; k < 4; ++k) accr[k][0] = accr[k][1] = accr[k][2] = T(0);
+    const int64_t e0 = static_cast<int64_t>(b.patch_first[pp]) + 3 * r;
 #pragma unroll
-        for (int tc = 0; tc < 6; ++tc) {
-            if (tc != t) continue;  // compile-time local connectivity for the selected tet
-            const int l0 = hex6_local(tc, 0), l1 = hex6_local(tc, 1), l2 = hex6_local(tc, 2), l3 = hex6_local(tc, 3);
-            T J[9], D[9];
+    for (int k = 0; k < 3; ++k) {
+        // columns of J and D: X_l - X_0 and u_l - u_0 for l = R_r[k], R_r[k+1], 3
+        T J[9], D[9];
 #pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                J[i * 3 + 0] = dx[l1][i] - dx[l0][i];
-                J[i * 3 + 1] = dx[l2][i] - dx[l0][i];
-                J[i * 3 + 2] = dx[l3][i] - dx[l0][i];
-                D[i * 3 + 0] = du[l1][i] - du[l0][i];
-                D[i * 3 + 1] = du[l2][i] - du[l0][i];
-                D[i * 3 + 2] = du[l3][i] - du[l0][i];
-            }
-            const int64_t e = e0 + tc;
-            double lam, mu;
-            element_lame(b, e, lam, mu);
-            T f[12];
-            tet4_forces<T, MAT>(J, D, lam, mu, f, valid ? e : 0, valid ? status : nullptr);
+        for (int i = 0; i < 3; ++i) {
+            J[i * 3 + 0] = dxr[k][i];
+            J[i * 3 + 1] = dxr[k + 1][i];
+            J[i * 3 + 2] = dx3[i];
+            D[i * 3 + 0] = dur[k][i];
+            D[i * 3 + 1] = dur[k + 1][i];
+            D[i * 3 + 2] = du3[i];
+        }
+        const int64_t e = e0 + k;
+        double lam, mu;
+        element_lame(b, e, lam, mu);
+        T f[12];
+        tet4_forces<T, MAT>(J, D, lam, mu, f, valid ? e : 0, valid ? status : nullptr);
 #pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                acc[l0][i] += f[i];
-                acc[l1][i] += f[3 + i];
-                acc[l2][i] += f[6 + i];
-                acc[l3][i] += f[9 + i];
-            }
+        for (int i = 0; i < 3; ++i) {
+            acc0[i] += f[i];
+            accr[k][i] += f[3 + i];
+            accr[k + 1][i] += f[6 + i];
+            acc3[i] += f[9 + i];
         }
     }
-    if (TPH > 1) {
+    // Both threads of a pair are in one warp (even lane first) and share `valid`.
 #pragma unroll
-        for (int a = 0; a < 8; ++a)
-#pragma unroll
-            for (int i = 0; i < 3; ++i) acc[a][i] += __shfl_xor_sync(kFull, acc[a][i], 1);
+    for (int i = 0; i < 3; ++i) {
+        acc0[i] += __shfl_xor_sync(kFull, acc0[i], 1);
+        acc3[i] += __shfl_xor_sync(kFull, acc3[i], 1);
+        accr[0][i] += __shfl_xor_sync(kFull, accr[3][i], 1);
     }
     if (!valid) return;
-#pragma unroll
-    for (int a = 0; a < 8; ++a) {
-        if (a % TPH != r) continue;
-        const int32_t pos = b.slot_pos[p * 8 + a];
-        if (pos >= 0) slots[pos] = make4(acc[a][0], acc[a][1], acc[a][2]);
-    }
+    // thread 0 writes nodes 1, 2, 4 and 0; thread 1 nodes 5, 6, 7 and 3
+    const int32_t* sp = b.slot_pos + p * 8;
+    int32_t pos = sp[r ? 5 : 1];
+    if (pos >= 0) slots[pos] = make4(accr[0][0], accr[0][1], accr[0][2]);
+    pos = sp[r ? 6 : 2];
+    if (pos >= 0) slots[pos] = make4(accr[1][0], accr[1][1], accr[1][2]);
+    pos = sp[r ? 7 : 4];
+    if (pos >= 0) slots[pos] = make4(accr[2][0], accr[2][1], accr[2][2]);
+    pos = sp[r ? 3 : 0];
+    if (pos >= 0) slots[pos] = r ? make4(acc3[0], acc3[1], acc3[2]) : make4(acc0[0], acc0[1], acc0[2]);
 }
 
 // ---------------------------------------------------------------------------
@@ -2057,9 +2075,9 @@ void launch_gauss_force(const GaussBlockDev& b, int mixed, const double4* X4, co
     if (b.num_elems == 0) return;
     if (b.kind == AM_TET4_GAUSS && b.patched == 2) {
         if (mixed) {
-            AM_DISPATCH_MAT(b.material, (launch_pdl(k_tet4_hex6_force<float, M, 1>, grid_for(b.num_patches, hex6_block<float>()), hex6_block<float>(), s, b, X4, U4, static_cast<float4*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (launch_pdl(k_tet4_hex6_force<float, M>, grid_for(2 * b.num_patches, kHex6Block), kHex6Block, s, b, X4, U4, static_cast<float4*>(slots), status)));
         } else {
-            AM_DISPATCH_MAT(b.material, (launch_pdl(k_tet4_hex6_force<double, M, 1>, grid_for(b.num_patches, hex6_block<double>()), hex6_block<double>(), s, b, X4, U4, static_cast<double4*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (launch_pdl(k_tet4_hex6_force<double, M>, grid_for(2 * b.num_patches, kHex6Block), kHex6Block, s, b, X4, U4, static_cast<double4*>(slots), status)));
         }
     } else if (b.kind == AM_TET4_GAUSS && b.patched) {
         const unsigned grid = grid_for(b.num_patches, 8 * kPatchesPerWarp);
