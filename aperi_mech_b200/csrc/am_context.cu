@@ -121,6 +121,8 @@ struct Block {
     int32_t* patch_nodes = nullptr;
     uint32_t* patch_local = nullptr;
     uint32_t* patch_gather = nullptr;
+    float* patch_dx32 = nullptr;
+    double* patch_dx64 = nullptr;
     const int32_t* slot_pos = nullptr;  // block-local view into the context's position array
     std::vector<int32_t> host_nodes;    // node of each logical slot (-1: unused), for the node CSR
 
@@ -141,6 +143,8 @@ struct Block {
         g.patch_nodes = patch_nodes;
         g.patch_local = patch_local;
         g.patch_gather = patch_gather;
+        g.patch_dx32 = patch_dx32;
+        g.patch_dx64 = patch_dx64;
         g.hstate = hstate;
         g.href = href;
         return g;
@@ -195,6 +199,8 @@ struct Block {
         dfree(patch_nodes);
         dfree(patch_local);
         dfree(patch_gather);
+        dfree(patch_dx32);
+        dfree(patch_dx64);
         dfree(hstate);
         dfree(href);
         dfree(group_ptr);
@@ -1015,6 +1021,12 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
                         ck(cudaMemcpy(b.patch_first, tp.first.data(), (P + 1) * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
                         ck(cudaMemcpy(b.patch_nodes, tp.nodes.data(), 8 * P * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
                         ck(cudaMemcpy(b.patch_local, tp.local.data(), E * sizeof(uint32_t), cudaMemcpyHostToDevice), "upload");
+                        if (hex6) {
+                            b.patch_dx32 = dalloc<float>(21 * P, "patch coordinate differences");
+                            b.patch_dx64 = dalloc<double>(21 * P, "patch coordinate differences");
+                            am::launch_hex6_patch_dx(b.patch_nodes, P, ctx->X4, b.patch_dx32, b.patch_dx64, ctx->stream);
+                            ck(cudaGetLastError(), "patch coordinate differences");
+                        }
                         b.host_nodes.assign(8 * P, -1);
                         for (int64_t q = 0; q < P; ++q)
                             for (int a = 0; a < tp.used[q]; ++a) b.host_nodes[8 * q + a] = tp.nodes[8 * q + a];

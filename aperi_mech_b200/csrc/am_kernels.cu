@@ -263,13 +263,16 @@ __global__ void __launch_bounds__(256) k_tet4_patch_force(GaussBlockDev b, const
 // r = 0 and (5, 6, 7, 1) for r = 1, so its tet k is (0, R_r[k], R_r[k+1], 3) and
 // both threads run the same code on six of the eight nodes. The pair's sums meet
 // with three shuffles: node 0 and node 3 from both threads, and each thread's
-// first ring node (1 or 5) from the other thread's last. Per thread this halves
-// the unrolled code and holds 6 nodes' data and sums instead of 8, which is what
-// lets the FP32 kernel run five 128-thread blocks per SM in 96 registers; on B200
-// that ran the element kernel 12% faster (mixed and FP64) than one thread per patch.
+// first ring node (1 or 5) from the other thread's last. The reference differences
+// X_a - X_0 come from a per-patch table formed at set-up (coalesced loads in place of
+// coordinate gathers, and no FP64 subtractions per step). Per thread this halves the
+// unrolled code and holds 6 nodes' data and sums instead of 8; that is what fits the
+// FP32 kernel in 72 registers at seven 128-thread blocks per SM and the FP64 one in
+// 128 at four. On B200, against one thread per patch with gathered coordinates, the
+// element kernel ran 55.8 -> 42.4 us (FP32) and 81.9 -> 57.3 us (FP64) per launch.
 // ---------------------------------------------------------------------------
 template <typename T>
-constexpr int hex6_min_blocks() { return sizeof(T) == 4 ? 5 : 3; }
+constexpr int hex6_min_blocks() { return sizeof(T) == 4 ? 7 : 4; }
 constexpr int kHex6Block = 128;
 
 template <typename T, int MAT>
@@ -281,10 +284,11 @@ __global__ void __launch_bounds__(kHex6Block, hex6_min_blocks<T>()) k_tet4_hex6_
     const int r = static_cast<int>(gt & 1);
     const bool valid = p < b.num_patches;
     const int64_t pp = valid ? p : 0;
-    // Node data relative to patch node 0: X in FP64 then T, u likewise. The mesh data
-    // is read before the wait for the previous kernel (which writes u), and the slot
-    // positions, needed only at the end, are sent to L2 now (on B200 that took 2% off
-    // the FP32 kernel and 5% off the FP64 one).
+    // Node data relative to patch node 0: X from the set-up table, u gathered in FP64
+    // and differenced before the cast to T. The mesh data is read before the wait for
+    // the previous kernel (which writes u), and the slot positions, needed only at the
+    // end, are sent to L2 now (on B200 that took 2% off the FP32 kernel and 5% off the
+    // FP64 one).
     const int4* pn4 = reinterpret_cast<const int4*>(b.patch_nodes + pp * 8);
     const int4 lo = pn4[0], hi = pn4[1];  // patch-local nodes 0-3 and 4-7
     asm volatile("prefetch.global.L2 [%0];" ::"l"(b.slot_pos + pp * 8));
@@ -294,20 +298,19 @@ __global__ void __launch_bounds__(kHex6Block, hex6_min_blocks<T>()) k_tet4_hex6_
     nr[1] = r ? hi.z : lo.z;
     nr[2] = r ? hi.w : hi.x;
     nr[3] = r ? lo.y : hi.y;
-    const double4 x0 = X4[n0];
     T dx3[3], dxr[4][3], du3[3], dur[4][3];
     {
-        const double4 x = X4[n3];
-        dx3[0] = T(x.x - x0.x);
-        dx3[1] = T(x.y - x0.y);
-        dx3[2] = T(x.z - x0.z);
-    }
+        // X_a - X_0, formed in FP64 (and rounded to T) once at set-up
+        const T* dxp = (sizeof(T) == 4 ? reinterpret_cast<const T*>(b.patch_dx32)
+                                       : reinterpret_cast<const T*>(b.patch_dx64)) + pp;
+        const int64_t P = b.num_patches;
+        const int ra[4] = {r ? 5 : 1, r ? 6 : 2, r ? 7 : 4, r ? 1 : 5};
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const double4 x = X4[nr[k]];
-        dxr[k][0] = T(x.x - x0.x);
-        dxr[k][1] = T(x.y - x0.y);
-        dxr[k][2] = T(x.z - x0.z);
+        for (int i = 0; i < 3; ++i) dx3[i] = dxp[(6 + i) * P];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) dxr[k][i] = dxp[(3 * (ra[k] - 1) + i) * P];
     }
     pdl_trigger();
     pdl_wait();
@@ -373,6 +376,24 @@ __global__ void __launch_bounds__(kHex6Block, hex6_min_blocks<T>()) k_tet4_hex6_
     if (pos >= 0) slots[pos] = make4(accr[2][0], accr[2][1], accr[2][2]);
     pos = sp[r ? 3 : 0];
     if (pos >= 0) slots[pos] = r ? make4(acc3[0], acc3[1], acc3[2]) : make4(acc0[0], acc0[1], acc0[2]);
+}
+
+// Set-up for the split-hex kernels: X_a - X_0 in FP64 (and rounded to FP32) for
+// patch-local nodes a = 1..7 of every patch (component-major).
+__global__ void __launch_bounds__(256) k_hex6_patch_dx(const int32_t* __restrict__ patch_nodes, int64_t num_patches,
+                                                       const double4* __restrict__ X4, float* __restrict__ dx32,
+                                                       double* __restrict__ dx64) {
+    const int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= num_patches) return;
+    const double4 x0 = X4[patch_nodes[p * 8]];
+    for (int a = 1; a < 8; ++a) {
+        const double4 x = X4[patch_nodes[p * 8 + a]];
+        const double d[3] = {x.x - x0.x, x.y - x0.y, x.z - x0.z};
+        for (int i = 0; i < 3; ++i) {
+            dx64[(3 * (a - 1) + i) * num_patches + p] = d[i];
+            dx32[(3 * (a - 1) + i) * num_patches + p] = static_cast<float>(d[i]);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -2073,7 +2094,7 @@ void launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, cudaStr
 void launch_gauss_force(const GaussBlockDev& b, int mixed, const double4* X4, const double4* U4, void* slots,
                         int* status, cudaStream_t s) {
     if (b.num_elems == 0) return;
-    if (b.kind == AM_TET4_GAUSS && b.patched == 2) {
+    if (b.kind == AM_TET4_GAUSS && b.patched == 2 && b.patch_dx32 != nullptr && b.patch_dx64 != nullptr) {
         if (mixed) {
             AM_DISPATCH_MAT(b.material, (launch_pdl(k_tet4_hex6_force<float, M>, grid_for(2 * b.num_patches, kHex6Block), kHex6Block, s, b, X4, U4, static_cast<float4*>(slots), status)));
         } else {
@@ -2208,6 +2229,12 @@ void launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4
     if (b.num_cells == 0) return;
     const unsigned grid = grid_for(b.num_cells * 32, 256);
     AM_DISPATCH_MAT(b.material, (k_cell_vjp<M><<<grid, 256, 0, s>>>(b, U4, L4, slots, gmu, gkappa, accumulate)));
+}
+
+void launch_hex6_patch_dx(const int32_t* patch_nodes, int64_t num_patches, const double4* X4, float* dx32,
+                          double* dx64, cudaStream_t stream) {
+    if (num_patches <= 0) return;
+    k_hex6_patch_dx<<<grid_for(num_patches, 256), 256, 0, stream>>>(patch_nodes, num_patches, X4, dx32, dx64);
 }
 
 void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const double4* X4, double4* slots,

@@ -46,6 +46,12 @@ struct GaussBlockDev {
     const int32_t* patch_nodes;  // num_patches x 8 (unused entries repeat entry 0)
     const uint32_t* patch_local; // per element: 4 local node ids, one byte each
     const uint32_t* patch_gather;// per patch node: bits 0-7 tets touching it, bits 8+2t: its slot in tet t
+    // Split-hex patches: reference differences X_a - X_0 of patch-local nodes a = 1..7
+    // (formed in FP64; rounded once to FP32 for the mixed path), component-major:
+    // entry (3 (a - 1) + i) * num_patches + patch. Run-invariant; read by the kernels
+    // in place of the coordinate gathers. null where not built.
+    const float* patch_dx32;
+    const double* patch_dx64;
     // Updated / semi-Lagrangian formulations: element displacement gradient of the last
     // force evaluation (9 per element; for Hex8 the last Gauss point's) and the semi
     // formulation's reference gradient. null under the total formulation.
@@ -111,6 +117,8 @@ void launch_gauss_vjp(const GaussBlockDev& b, const double4* X4, const double4* 
                       double* gmu, double* gkappa, int accumulate, cudaStream_t s);
 void launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double4* slots, double* gmu,
                      double* gkappa, int accumulate, cudaStream_t s);
+void launch_hex6_patch_dx(const int32_t* patch_nodes, int64_t num_patches, const double4* X4, float* dx32,
+                          double* dx64, cudaStream_t stream);
 void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const double4* X4, double4* slots,
                                cudaStream_t s);
 
