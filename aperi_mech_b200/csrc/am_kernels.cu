@@ -117,7 +117,9 @@ __device__ __forceinline__ T tet4_forces(const T* J, const T* D, double lam, dou
 #pragma unroll
         for (int k = 0; k < 9; ++k) Jc[k] = J[k] + D[k];
         adj3(Jc, A);
-        const T sc = T(1.0 / (6.0 * Jf));
+        // det F stays FP64; the FP32 path takes its scale from an FP32 reciprocal of
+        // 6 det F (on B200 1.7% off the kernel against the FP64 division).
+        const T sc = sizeof(T) == 4 ? T(__frcp_rn(static_cast<float>(6.0 * Jf))) : T(1.0 / (6.0 * Jf));
 #pragma unroll
         for (int i = 0; i < 3; ++i) f[i] = T(0);
 #pragma unroll
@@ -1514,15 +1516,32 @@ constexpr int kNodeBlock = 128;  // 7-8% faster node kernels than 256-thread blo
 // takes every slot in one round; that wins when the slot array sits in L2 (the
 // loads are latency-bound), while BATCH = 4 keeps more warps resident, which wins
 // when the slots stream from HBM (see gather_batch8).
+// The run-invariant part of a node's gather: its slot range and interface row, which
+// a kernel can read before it waits for the kernels that write the slots.
+struct NodeSlots {
+    int32_t p0, p1, row;
+};
+__device__ __forceinline__ NodeSlots node_slots(const NodeDev& nd, int64_t i, bool own) {
+    NodeSlots q{0, 0, -1};
+    if (own) {
+        q.row = nd.iface_row != nullptr ? nd.iface_row[i] : -1;
+        if (nd.f_given == nullptr && q.row < 0) {
+            q.p0 = nd.node_ptr[i];
+            q.p1 = nd.node_ptr[i + 1];
+        }
+    }
+    return q;
+}
+
 template <typename S, int BATCH, int LPN>
 __device__ __forceinline__ void gather(const NodeDev& nd, const vec4_t<S>* __restrict__ slots, int64_t i, bool own,
-                                       double& fx, double& fy, double& fz) {
+                                       const NodeSlots& q, double& fx, double& fy, double& fz) {
     // LPN lanes per node: lane r takes every LPN-th slot from r (the group reads the
     // node's contiguous range with coalesced loads), then the partial sums combine by
     // a fixed butterfly, so every lane holds the same total and the order is fixed.
     const int r = LPN == 1 ? 0 : static_cast<int>(threadIdx.x % LPN);
     fx = fy = fz = 0.0;
-    const int32_t row = (own && nd.iface_row != nullptr) ? nd.iface_row[i] : -1;
+    const int32_t row = q.row;
     if (own && nd.f_given != nullptr) {
         // Two-pass coupling: the node's generalized force, already summed.
         if (r == 0) {
@@ -1538,8 +1557,8 @@ __device__ __forceinline__ void gather(const NodeDev& nd, const vec4_t<S>* __res
             fz = nd.iface_f[3 * static_cast<int64_t>(row) + 2];
         }
     } else if (own) {
-        const int32_t p0 = nd.node_ptr[i], p1 = nd.node_ptr[i + 1];
-        for (int32_t p = p0 + r; p < p1; p += BATCH * LPN) {
+        const int32_t p1 = q.p1;
+        for (int32_t p = q.p0 + r; p < p1; p += BATCH * LPN) {
             vec4_t<S> v[BATCH];
 #pragma unroll
             for (int k = 0; k < BATCH; ++k)
@@ -1562,6 +1581,12 @@ __device__ __forceinline__ void gather(const NodeDev& nd, const vec4_t<S>* __res
             fz += __shfl_xor_sync(gmask, fz, off);
         }
     }
+}
+
+template <typename S, int BATCH, int LPN>
+__device__ __forceinline__ void gather(const NodeDev& nd, const vec4_t<S>* __restrict__ slots, int64_t i, bool own,
+                                       double& fx, double& fy, double& fz) {
+    gather<S, BATCH, LPN>(nd, slots, i, own, node_slots(nd, i, own), fx, fy, fz);
 }
 
 // BoundaryCondition::ApplyVelocity / ApplyAcceleration: for each component the
@@ -1703,17 +1728,18 @@ __global__ void __launch_bounds__(kNodeBlock) k_node_step(NodeDev nd, const vec4
                                                            double4* __restrict__ u_copy, int* status, int rebase) {
     const int64_t i = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / LPN;
     const bool own = i < nd.num_nodes;
-    // The node's own data is independent of the gather: issue its loads first (mass
-    // and BC word before the wait for the element kernels, v and u after it).
+    // The node's own data is independent of the gather: issue its loads first (mass,
+    // BC word and slot range before the wait for the element kernels, v and u after it).
     const int64_t j = own ? i : 0;
     const double m = nd.mass[j];
     const uint32_t w = nd.bcword[j];
+    const NodeSlots q = node_slots(nd, i, own);
     pdl_trigger();
     pdl_wait();
     const double4 vh = V4[j];
     const double4 u0 = advance ? U4[j] : make_double4(0.0, 0.0, 0.0, 0.0);
     double fx, fy, fz;
-    gather<S, BATCH, LPN>(nd, slots, i, own, fx, fy, fz);
+    gather<S, BATCH, LPN>(nd, slots, i, own, q, fx, fy, fz);
     if (!own || threadIdx.x % LPN != 0) return;
     if (nd.has_g) {
         fx += nd.g[0] * m;
