@@ -392,7 +392,9 @@ def run_adjoint(torch, pa, ckpt, stream, dev):
 
     with ExplicitDynamics(pa.coords, pa.parts, pa.bcs, stream=stream.cuda_stream) as ma:
         times = {}
-        for rep in range(2):
+        # rep 0 warms up (the adjoint allocates its checkpoint buffers), rep 1 is timed,
+        # rep 2 records the per-kernel breakdown (its events between kernels slow it down)
+        for rep in range(3):
             ma.set_state(None, pa.v0)
             torch.cuda.synchronize(dev)
             a0, a1 = _events(torch)
@@ -401,15 +403,17 @@ def run_adjoint(torch, pa, ckpt, stream, dev):
             ma.run(pa.nsteps, pa.dt)
             a1.record(stream)
             torch.cuda.synchronize(dev)
-            times["forward"] = a0.elapsed_time(a1)
+            if rep == 1:
+                times["forward"] = a0.elapsed_time(a1)
             ma.set_state(None, pa.v0)
             torch.cuda.synchronize(dev)
-            ma.profile(rep == 1)
+            ma.profile(rep == 2)
             a0.record(stream)
             loss, gm, gk = ma.adjoint(pa.nsteps, pa.dt, ckpt, pa.meta["sensors"])
             a1.record(stream)
             torch.cuda.synchronize(dev)
-            times["adjoint"] = a0.elapsed_time(a1)
+            if rep == 1:
+                times["adjoint"] = a0.elapsed_time(a1)
         pms, pn = ma.profile_read()
         ma.profile(False)
     return {"workload": pa.name, "elements": pa.num_elems, "steps": pa.nsteps, "ckpt_every": ckpt,
