@@ -94,6 +94,7 @@ struct Block {
     int64_t num_elems = 0;
     int64_t num_entries = 0;  // slots of this block
     int64_t slot_base = 0;
+    int64_t slot_count = -1;  // logical slots when they differ from num_entries (patched cells)
     int32_t* conn = nullptr;
     double* mu_field = nullptr;
     double* kappa_field = nullptr;
@@ -165,6 +166,10 @@ struct Block {
         c.slot_pos = slot_pos;
         c.num_entries = num_entries;
         c.max_entries = max_entries;
+        c.patched = patched;
+        c.num_patches = num_patches;
+        c.patch_first = patch_first;
+        c.patch_nodes = patch_nodes;
         c.num_groups = num_groups;
         c.group_ptr = group_ptr;
         c.max_group = max_group;
@@ -268,6 +273,19 @@ TetPatches build_tet_patches(const int32_t* conn, int64_t E) {
             }
         }
     return tp;
+}
+
+// True when every patch is exactly one hex's six-tet split in the canonical local
+// order (tet t on local nodes 0, a_t, b_t, 3 with a = 1,2,4,5,6,7 and b = 2,4,5,6,7,1).
+bool hex6_patches(const TetPatches& tp) {
+    static const uint32_t kHex6[6] = {0x03020100u, 0x03040200u, 0x03050400u, 0x03060500u, 0x03070600u, 0x03010700u};
+    const int64_t P = static_cast<int64_t>(tp.used.size());
+    for (int64_t q = 0; q < P; ++q) {
+        if (tp.first[q + 1] - tp.first[q] != 6 || tp.used[q] != 8) return false;
+        for (int t = 0; t < 6; ++t)
+            if (tp.local[tp.first[q] + t] != kHex6[t]) return false;
+    }
+    return true;
 }
 
 }  // namespace
@@ -982,6 +1000,24 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
                     ck(cudaMemcpy(b.volumes, d->cell_volumes, E * sizeof(double), cudaMemcpyHostToDevice), "upload");
                 }
                 b.host_nodes.assign(d->cell_nodes, d->cell_nodes + K);
+                // Cells of four entries that group into split hexes (a tet mesh's element
+                // cells) run as patches like the Gauss tets: one slot per patch node.
+                bool four = E > 0 && ctx->tet4_patches;
+                for (int64_t c = 0; c < E && four; ++c) four = ptr[c + 1] - ptr[c] == 4;
+                if (four) {
+                    TetPatches tp = build_tet_patches(d->cell_nodes, E);
+                    const int64_t P = static_cast<int64_t>(tp.used.size());
+                    if (static_cast<double>(E) >= 2.5 * static_cast<double>(P) && hex6_patches(tp)) {
+                        b.patched = 2;
+                        b.num_patches = P;
+                        b.slot_count = 8 * P;
+                        b.patch_first = dalloc<int32_t>(P + 1, "patch offsets");
+                        b.patch_nodes = dalloc<int32_t>(8 * P, "patch nodes");
+                        ck(cudaMemcpy(b.patch_first, tp.first.data(), (P + 1) * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+                        ck(cudaMemcpy(b.patch_nodes, tp.nodes.data(), 8 * P * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+                        b.host_nodes.assign(tp.nodes.begin(), tp.nodes.begin() + 8 * P);
+                    }
+                }
             } else {
                 const int nn = d->kind == AM_HEX8_GAUSS ? 8 : 4;
                 if (E > 0 && !d->conn) fail(AM_EINVAL, "null connectivity");
@@ -1003,13 +1039,7 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
                     if (static_cast<double>(E) >= 2.5 * static_cast<double>(P)) {
                         // Split-hex patches (six tets in the canonical local order) get the
                         // register-resident kernel; any other patching the generic one.
-                        static const uint32_t kHex6[6] = {0x03020100u, 0x03040200u, 0x03050400u,
-                                                          0x03060500u, 0x03070600u, 0x03010700u};
-                        bool hex6 = true;
-                        for (int64_t q = 0; q < P && hex6; ++q) {
-                            hex6 = (tp.first[q + 1] - tp.first[q] == 6) && tp.used[q] == 8;
-                            for (int t = 0; t < 6 && hex6; ++t) hex6 = tp.local[tp.first[q] + t] == kHex6[t];
-                        }
+                        const bool hex6 = hex6_patches(tp);
                         b.patched = hex6 ? 2 : 1;
                         b.num_patches = P;
                         b.num_entries = 8 * P;
@@ -1050,7 +1080,7 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
             b.release();
             throw;
         }
-        ctx->num_slots += b.num_entries;
+        ctx->num_slots += b.slot_count >= 0 ? b.slot_count : b.num_entries;
         ctx->blocks.push_back(std::move(b));
         if (block_id) *block_id = static_cast<int32_t>(ctx->blocks.size() - 1);
     });
@@ -1124,6 +1154,8 @@ int am_set_cell_groups(am_ctx* ctx, int32_t block_id, int64_t num_cells, const i
         Block& b = ctx->blocks[block_id];
         if (b.kind != AM_SMOOTHED_CELLS) fail(AM_EINVAL, "cell groups need a smoothed-cell block");
         if (b.group_ptr) fail(AM_ESTATE, "cell groups already set");
+        if (b.patched)
+            fail(AM_ESTATE, "cell groups on four-entry cells grouped as split hexes (APERI_B200_TET4_PATCHES=0 keeps them ungrouped)");
         if (num_cells < 0 || !group_ptr) fail(AM_EINVAL, "null cell groups");
         if (group_ptr[0] != 0 || group_ptr[num_cells] != b.num_elems)
             fail(AM_EINVAL, "group_ptr must run from 0 to the block's subcell count");

@@ -861,6 +861,125 @@ __global__ void __launch_bounds__(256) k_cell_force_group(CellBlockDev b, const 
 }
 
 // ---------------------------------------------------------------------------
+// Four-entry cells grouped as split hexes (a tet mesh's element smoothing cells):
+// the split-hex Tet4 kernel's pair split, with each cell's stored gradients b_e and
+// volume V in place of the tet's own geometry. Entry e of the patch's tet t sits on
+// local node (0, a_t, b_t, 3)[e]; H = sum_e (u_e - u_0) (x) b_e, P(H), and the entry
+// forces -V b_e P^T are summed per patch node and written to its slot.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void load_cell12(const T* p, T* g);
+template <>
+__device__ __forceinline__ void load_cell12<float>(const float* p, float* g) {
+    const float4* q = reinterpret_cast<const float4*>(p);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float4 v = __ldg(q + k);
+        g[4 * k] = v.x;
+        g[4 * k + 1] = v.y;
+        g[4 * k + 2] = v.z;
+        g[4 * k + 3] = v.w;
+    }
+}
+template <>
+__device__ __forceinline__ void load_cell12<double>(const double* p, double* g) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const double2 v = __ldg(q + k);
+        g[2 * k] = v.x;
+        g[2 * k + 1] = v.y;
+    }
+}
+
+template <typename T, int MAT>
+__global__ void __launch_bounds__(kHex6Block, hex6_min_blocks<T>()) k_cell_hex6_force(CellBlockDev b, const double4* U4,
+                                                                                    vec4_t<T>* slots, int* status) {
+    const int64_t gt = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t p = gt >> 1;
+    const int r = static_cast<int>(gt & 1);
+    const bool valid = p < b.num_patches;
+    const int64_t pp = valid ? p : 0;
+    const int4* pn4 = reinterpret_cast<const int4*>(b.patch_nodes + pp * 8);
+    const int4 lo = pn4[0], hi = pn4[1];
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(b.slot_pos + pp * 8));
+    const int32_t n0 = lo.x, n3 = lo.w;
+    int32_t nr[4];
+    nr[0] = r ? hi.y : lo.y;
+    nr[1] = r ? hi.z : lo.z;
+    nr[2] = r ? hi.w : hi.x;
+    nr[3] = r ? lo.y : hi.y;
+    const int64_t c0 = static_cast<int64_t>(b.patch_first[pp]) + 3 * r;
+    pdl_trigger();
+    pdl_wait();
+    T du3[3], dur[4][3];
+    const double4 u0 = ld_dep(U4 + n0);
+    {
+        const double4 u = ld_dep(U4 + n3);
+        du3[0] = T(u.x - u0.x);
+        du3[1] = T(u.y - u0.y);
+        du3[2] = T(u.z - u0.z);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const double4 u = ld_dep(U4 + nr[k]);
+        dur[k][0] = T(u.x - u0.x);
+        dur[k][1] = T(u.y - u0.y);
+        dur[k][2] = T(u.z - u0.z);
+    }
+    T acc0[3] = {T(0), T(0), T(0)}, acc3[3] = {T(0), T(0), T(0)}, accr[4][3];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) accr[k][0] = accr[k][1] = accr[k][2] = T(0);
+    const T* gr = cell_grads<T>(b);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int64_t c = c0 + k;
+        T g[12];  // b_e for the entries on local nodes 0, R_r[k], R_r[k+1], 3
+        load_cell12<T>(gr + 12 * c, g);
+        T H[9];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) H[i * 3 + j] = dur[k][i] * g[3 + j] + dur[k + 1][i] * g[6 + j] + du3[i] * g[9 + j];
+        double lam, mu;
+        element_lame(b, c, lam, mu);
+        T P[9];
+        const double Jf = stress<T>(MAT, T(lam), T(mu), H, P);
+        if (valid && MAT == kNeoHookean && !(Jf > 0.0)) flag(status, AM_ENONPOS_J, c);
+        const T V = T(b.volumes[c]);
+        T f[4][3];
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                f[e][i] = (g[3 * e] * P[i * 3 + 0] + g[3 * e + 1] * P[i * 3 + 1] + g[3 * e + 2] * P[i * 3 + 2]) * -V;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            acc0[i] += f[0][i];
+            accr[k][i] += f[1][i];
+            accr[k + 1][i] += f[2][i];
+            acc3[i] += f[3][i];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        acc0[i] += __shfl_xor_sync(kFull, acc0[i], 1);
+        acc3[i] += __shfl_xor_sync(kFull, acc3[i], 1);
+        accr[0][i] += __shfl_xor_sync(kFull, accr[3][i], 1);
+    }
+    if (!valid) return;
+    const int32_t* sp = b.slot_pos + p * 8;
+    int32_t pos = sp[r ? 5 : 1];
+    if (pos >= 0) slots[pos] = make4(accr[0][0], accr[0][1], accr[0][2]);
+    pos = sp[r ? 6 : 2];
+    if (pos >= 0) slots[pos] = make4(accr[1][0], accr[1][1], accr[1][2]);
+    pos = sp[r ? 7 : 4];
+    if (pos >= 0) slots[pos] = make4(accr[2][0], accr[2][1], accr[2][2]);
+    pos = sp[r ? 3 : 0];
+    if (pos >= 0) slots[pos] = r ? make4(acc3[0], acc3[1], acc3[2]) : make4(acc0[0], acc0[1], acc0[2]);
+}
+
+// ---------------------------------------------------------------------------
 // F-bar smoothed cells (ForEachCellComputeForceFbar, ComputeInternalForceSmoothedCell.h:
 // 354-413) in three passes over the scratch fb (kFbarStride values per subcell):
 //   k_fbar_h     per subcell: H_s = sum_k u_k (x) b_k, J_s = DetApIm1(H_s) + 1 -> fb[0..9]
@@ -1427,6 +1546,60 @@ __global__ void __launch_bounds__(256) k_cell_vjp(CellBlockDev b, const double4*
         slots[b.slot_pos[s]] = make4(f[0], f[1], f[2]);
     }
     if (lane == 0) store_theta(gmu, gk, c, -V * (ldm - 2.0 / 3.0 * ldl), -V * ldl, accumulate);
+}
+
+// VJP of the split-hex-grouped cells (FP64, one thread per patch): the cell VJP above
+// for the patch's six cells, summed per patch node.
+template <int MAT>
+__global__ void __launch_bounds__(64) k_cell_hex6_vjp(CellBlockDev b, const double4* __restrict__ U4,
+                                                       const double4* __restrict__ L4, double4* __restrict__ slots,
+                                                       double* gmu, double* gk, int accumulate) {
+    const int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= b.num_patches) return;
+    constexpr int kRing[7] = {1, 2, 4, 5, 6, 7, 1};
+    double acc[8][3];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) acc[a][0] = acc[a][1] = acc[a][2] = 0.0;
+    const int64_t c0 = b.patch_first[p];
+#pragma unroll 1
+    for (int t = 0; t < 6; ++t) {
+        const int64_t c = c0 + t;
+        const int ln[4] = {0, kRing[t], kRing[t + 1], 3};
+        double g[12];
+        load_cell12<double>(b.grads64 + 12 * c, g);
+        double H[9], L[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) H[k] = L[k] = 0.0;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int32_t n = b.patch_nodes[p * 8 + ln[e]];
+            const double4 u = U4[n], l = L4[n];
+            const double uu[3] = {u.x, u.y, u.z}, ll[3] = {l.x, l.y, l.z};
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    H[i * 3 + j] += uu[i] * g[3 * e + j];
+                    L[i * 3 + j] += ll[i] * g[3 * e + j];
+                }
+        }
+        double lam, mu;
+        element_lame(b, c, lam, mu);
+        double dP[9], ldl, ldm;
+        stress_vjp(MAT, lam, mu, H, L, dP, &ldl, &ldm);
+        const double V = b.volumes[c];
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                acc[ln[e]][i] += (g[3 * e] * dP[i * 3 + 0] + g[3 * e + 1] * dP[i * 3 + 1] + g[3 * e + 2] * dP[i * 3 + 2]) * -V;
+        store_theta(gmu, gk, c, -V * (ldm - 2.0 / 3.0 * ldl), -V * ldl, accumulate);
+    }
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        const int32_t pos = b.slot_pos[p * 8 + a];
+        if (pos >= 0) slots[pos] = make4(acc[a][0], acc[a][1], acc[a][2]);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -2185,6 +2358,15 @@ void launch_fbar(const CellBlockDev& b, const double4* U4, void* slots, int* sta
 
 int launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void* slots, int* status, cudaStream_t s) {
     if (b.num_cells == 0) return 0;
+    if (b.patched == 2) {
+        const unsigned grid = grid_for(2 * b.num_patches, kHex6Block);
+        if (mixed) {
+            AM_DISPATCH_MAT(b.material, (launch_pdl(k_cell_hex6_force<float, M>, grid, kHex6Block, s, b, U4, static_cast<float4*>(slots), status)));
+        } else {
+            AM_DISPATCH_MAT(b.material, (launch_pdl(k_cell_hex6_force<double, M>, grid, kHex6Block, s, b, U4, static_cast<double4*>(slots), status)));
+        }
+        return 1;
+    }
     if (b.group_ptr != nullptr && b.fused) {
         const unsigned grid = grid_for(b.num_groups * 32, 32 * kFbarWarps);
         if (mixed) {
@@ -2253,6 +2435,10 @@ void launch_gauss_vjp(const GaussBlockDev& b, const double4* X4, const double4* 
 void launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double4* slots, double* gmu,
                      double* gkappa, int accumulate, cudaStream_t s) {
     if (b.num_cells == 0) return;
+    if (b.patched == 2) {
+        AM_DISPATCH_MAT(b.material, (k_cell_hex6_vjp<M><<<grid_for(b.num_patches, 64), 64, 0, s>>>(b, U4, L4, slots, gmu, gkappa, accumulate)));
+        return;
+    }
     const unsigned grid = grid_for(b.num_cells * 32, 256);
     AM_DISPATCH_MAT(b.material, (k_cell_vjp<M><<<grid, 256, 0, s>>>(b, U4, L4, slots, gmu, gkappa, accumulate)));
 }

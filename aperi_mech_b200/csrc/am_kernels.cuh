@@ -73,6 +73,12 @@ struct CellBlockDev {
     const int32_t* slot_pos;    // entry -> node-major position
     int64_t num_entries;        // ptr[num_cells]
     int32_t max_entries;        // longest cell (selects thread- or group-per-cell)
+    // Four-entry cells grouped as split hexes (patched == 2, see GaussBlockDev): cell
+    // patch_first[q] + t holds tet t of patch q; one slot per patch node.
+    int32_t patched;
+    int64_t num_patches;
+    const int32_t* patch_first;
+    const int32_t* patch_nodes;
     // F-bar (ComputeInternalForceSmoothedCell.h:354-413): the cells above are subcells,
     // grouped into num_groups cells by group_ptr; fbar is the per-subcell scratch
     // (kFbarStride values of the slot precision: H, J, then the stress). null: no F-bar.

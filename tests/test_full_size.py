@@ -1,6 +1,6 @@
 """Parity at the benchmark sizes. The FP64 internal force of the library against the
 oracle on the full workloads: 70^3 split-hex Tet4, 128^3 Hex8 with lognormal fields, the
-RKPM nodal-cell box at h = 1/46 and the F-bar subcell box at h = 1/32 (for the cell
+element-cell and RKPM nodal-cell boxes at h = 1/46 and the F-bar subcell box at h = 1/32 (for the cell
 workloads the oracle takes the cells the library built; their set-up is pinned against the
 oracle at smaller sizes, since the oracle's full-size RKPM set-up takes minutes). The mixed
 force against the same at the mixed-precision bar; size-independent properties (the nodal
@@ -108,13 +108,17 @@ def test_hex8_128_force_matches_oracle(gpu, oracle_lib):
     _check(f, oracle_lib.OracleProblem(p.coords, p.parts, p.bcs).internal_force(u))
 
 
-@pytest.mark.parametrize("workload", ["rkpm_box_46", "rkpm_fbar_box_32"])
-def test_rkpm_cells_force_matches_oracle(gpu, oracle_lib, workload):
-    """The one-pass RKPM nodal cells (205,437 cells, 13.5 M entries) and the F-bar corner-hex
-    subcells (1,572,864 subcells) built by the library, forces against the oracle's."""
+@pytest.mark.parametrize("workload", ["smoothed_tet4_box_46", "rkpm_box_46", "rkpm_fbar_box_32"])
+def test_cells_force_matches_oracle(gpu, oracle_lib, workload):
+    """The element smoothing cells of the h = 1/46 box (1,168,032 tets, grouped as split
+    hexes), the one-pass RKPM nodal cells (205,437 cells, 13.5 M entries) and the F-bar
+    corner-hex subcells (1,572,864 subcells) built by the library, forces against the
+    oracle's."""
     from aperi_mech_b200 import problems
 
-    p = problems.rkpm_box(n=46, nsteps=1) if workload == "rkpm_box_46" else problems.rkpm_fbar_box(n=32, nsteps=1)
+    p = {"smoothed_tet4_box_46": lambda: problems.smoothed_tet4_box(n=46, nsteps=1),
+         "rkpm_box_46": lambda: problems.rkpm_box(n=46, nsteps=1),
+         "rkpm_fbar_box_32": lambda: problems.rkpm_fbar_box(n=32, nsteps=1)}[workload]()
     u = _displacement(p, 1e-3, 4)
     f, _ = _forces(p, u, mass=p.meta["mass"])
     _check(f, oracle_lib.OracleProblem(p.coords, p.parts, p.bcs, mass=p.meta["mass"]).internal_force(u))

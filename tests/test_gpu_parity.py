@@ -165,6 +165,48 @@ def test_smoothed_cells_parity(gpu, oracle_lib):
         assert rel_err(m.internal_force(u, "mixed"), want) < MIXED_FORCE_TOL
 
 
+@pytest.mark.parametrize("material", ["neo_hookean", "elastic", "linear_elastic"])
+def test_element_cells_grouped_as_split_hexes(gpu, oracle_lib, monkeypatch, material):
+    """Element smoothing cells of a split-hex tet mesh run as patches (one slot per patch
+    node, a third of the slots): the force (FP64 and mixed), the VJP and 30 steps with
+    per-cell moduli against the oracle, grouped and with patching off."""
+    from aperi_mech_b200 import mesh
+    from aperi_mech_b200.model import BoundaryCondition, ExplicitDynamics
+    from aperi_mech_b200.smoothing import element_smoothing_part
+
+    coords, conn = _mesh("tet4", 5, seed=11)
+    mu_f, k_f = _fields(conn.shape[0], 7, True)
+    mat = _material(material)
+    part, mass = element_smoothing_part(coords, conn, mat, mu_field=mu_f, kappa_field=k_f)
+    bcs = [BoundaryCondition.fixed(mesh.side_sets(coords)["surface_5"])]
+    rng = np.random.default_rng(12)
+    u = 1e-3 * rng.standard_normal(coords.shape)
+    lam = rng.standard_normal(coords.shape)
+    v0 = rng.uniform(-0.01, 0.01, size=coords.shape)
+    v0[bcs[0].nodes] = 0.0
+    cmax = np.sqrt((k_f.max() + 4.0 / 3.0 * mu_f.max()) / mat.density)
+    dt = 0.2 * float(mesh.tet_char_length(coords, conn).min()) / cmax
+    op = oracle_lib.OracleProblem(coords, [part], bcs, mass=mass)
+    want_f, want_v = op.internal_force(u), op.vjp_force(u, lam)
+    zero = np.zeros_like(coords)
+    want_s = op.steps(zero, v0, op.init_acceleration(zero), np.full(30, dt))
+    slots = {}
+    for patches in ("1", "0"):
+        monkeypatch.setenv("APERI_B200_TET4_PATCHES", patches)
+        with ExplicitDynamics(coords, [part], bcs, mass=mass) as m:
+            slots[patches] = m.layout()["used_slots"]
+            assert rel_err(m.internal_force(u), want_f) < FP64_TOL
+            assert rel_err(m.internal_force(u, "mixed"), want_f) < MIXED_FORCE_TOL
+            for g, w in zip(m.vjp_force(u, lam), want_v):
+                assert rel_err(g, w) < 1e-11
+            m.set_state(None, v0)
+            m.init_acceleration()
+            m.run(30, dt)
+            for g, w in zip(m.get_state(), want_s):
+                assert rel_err(g, w) < FP64_TOL
+    assert 3 * slots["1"] == slots["0"] == 4 * conn.shape[0]
+
+
 # ---- time integration ----------------------------------------------------------------
 def _small_problem(name):
     from aperi_mech_b200 import problems
