@@ -37,10 +37,12 @@ __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;"
 // still be running when this one starts, so such data is not read-only for this
 // kernel's lifetime and must not be read through the non-coherent read-only path that
 // const __restrict__ pointers allow.
+// A double4 is one 32-byte load (sm_100 vector width; the arrays are 32-byte aligned),
+// volatile so that it stays after the wait that orders it.
 __device__ __forceinline__ double4 ld_dep(const double4* p) {
-    const double2 a = __ldca(reinterpret_cast<const double2*>(p));
-    const double2 b = __ldca(reinterpret_cast<const double2*>(p) + 1);
-    return make_double4(a.x, a.y, b.x, b.y);
+    double4 r;
+    asm volatile("ld.global.ca.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(r.x), "=d"(r.y), "=d"(r.z), "=d"(r.w) : "l"(p));
+    return r;
 }
 __device__ __forceinline__ float4 ld_dep(const float4* p) { return __ldca(p); }
 
