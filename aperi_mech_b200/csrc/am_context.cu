@@ -362,7 +362,7 @@ struct am_ctx {
     int32_t* rkt_src = nullptr;
     double* rkt_val = nullptr;
     double4* rk_u = nullptr;          // physical displacement Psi U
-    double* rk_f_local = nullptr;     // N x 3: element forces at the nodes
+    double4* rk_f_local = nullptr;    // element forces at the nodes
     double* rk_f = nullptr;           // N x 3: generalized force Psi^T f_local
     std::vector<cudaEvent_t> events;
     std::vector<std::pair<int, int64_t>> mark_slot;
@@ -445,7 +445,7 @@ struct am_ctx {
         if (rk_ptr) {
             am::NodeDev nd = node_dev();
             nd.f_given = nullptr;
-            am::launch_gather_force(nd, mixed, s, rk_f_local, 0, stream);
+            am::launch_gather_force4(nd, mixed, s, rk_f_local, stream);
             am::launch_rk_cols3(N, rkt_ptr, rkt_src, rkt_val, rk_f_local, rk_f, stream);
             launches += 2;
         }
@@ -1772,7 +1772,7 @@ int am_set_rk_functions(am_ctx* ctx, const int64_t* nbr_ptr, const int32_t* nbr,
         up(ctx->rkt_src, tsrc.data(), T, "transposed sources");
         up(ctx->rkt_val, tval.data(), T, "transposed values");
         ctx->rk_u = dalloc<double4>(N, "physical displacement");
-        ctx->rk_f_local = dalloc<double>(3 * N, "local force");
+        ctx->rk_f_local = dalloc<double4>(N, "local force");
         ctx->rk_f = dalloc<double>(3 * N, "generalized force");
     });
 }

@@ -45,6 +45,13 @@ __device__ __forceinline__ double4 ld_dep(const double4* p) {
     return r;
 }
 __device__ __forceinline__ float4 ld_dep(const float4* p) { return __ldca(p); }
+// One 32-byte load through the read-only path, for data that no kernel still running
+// writes (kernels launched without programmatic overlap, on arrays finished before).
+__device__ __forceinline__ double4 ld_ro4(const double4* p) {
+    double4 r;
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(r.x), "=d"(r.y), "=d"(r.z), "=d"(r.w) : "l"(p));
+    return r;
+}
 
 __device__ __forceinline__ void flag(int* status, int code, int64_t idx) {
     if (status == nullptr) return;
@@ -1811,6 +1818,20 @@ __global__ void __launch_bounds__(kNodeBlock) k_gather_force(NodeDev nd, const v
     }
 }
 
+// The node-summed force as one double4 per node (for the transposed coupling's
+// 32-byte gathers).
+template <typename S, int BATCH, int LPN>
+__global__ void __launch_bounds__(kNodeBlock) k_gather_force4(NodeDev nd, const vec4_t<S>* __restrict__ slots,
+                                                               double4* __restrict__ f) {
+    const int64_t i = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / LPN;
+    const bool own = i < nd.num_nodes;
+    if (LPN == 1 && !own) return;
+    double fx, fy, fz;
+    gather<S, BATCH, LPN>(nd, slots, i, own, fx, fy, fz);
+    if (!own || threadIdx.x % LPN != 0) return;
+    f[i] = make_double4(fx, fy, fz, 0.0);
+}
+
 // One thread per local interface node: its own slots summed (no interface override).
 template <typename S>
 __global__ void __launch_bounds__(kNodeBlock) k_iface_gather(NodeDev nd, const vec4_t<S>* __restrict__ slots,
@@ -2101,7 +2122,7 @@ __global__ void __launch_bounds__(128) k_rk_rows4(int64_t n, const int64_t* __re
         b = ptr[i];
         e = ptr[i + 1];
         for (int64_t k = e - 1 - r; k >= b; k -= kRkLanes) {
-            const double4 u = U4[nbr[k]];
+            const double4 u = ld_ro4(U4 + nbr[k]);
             const double w = val[k];
             x += w * u.x;
             y += w * u.y;
@@ -2117,7 +2138,7 @@ __global__ void __launch_bounds__(128) k_rk_rows4(int64_t n, const int64_t* __re
 // functions, no atomics).
 __global__ void __launch_bounds__(128) k_rk_cols3(int64_t n, const int64_t* __restrict__ tptr,
                                                  const int32_t* __restrict__ tsrc, const double* __restrict__ tval,
-                                                 const double* __restrict__ fl, double* __restrict__ f) {
+                                                 const double4* __restrict__ fl, double* __restrict__ f) {
     const int64_t j = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / kRkLanes;
     const int r = static_cast<int>(threadIdx.x % kRkLanes);
     const bool own = j < n;
@@ -2125,11 +2146,11 @@ __global__ void __launch_bounds__(128) k_rk_cols3(int64_t n, const int64_t* __re
     if (own) {
         const int64_t e = tptr[j + 1];
         for (int64_t k = tptr[j] + r; k < e; k += kRkLanes) {
-            const int64_t i = tsrc[k];
+            const double4 g = ld_ro4(fl + tsrc[k]);
             const double w = tval[k];
-            x += w * fl[3 * i];
-            y += w * fl[3 * i + 1];
-            z += w * fl[3 * i + 2];
+            x += w * g.x;
+            y += w * g.y;
+            z += w * g.z;
         }
     }
     rk_combine(x, y, z);
@@ -2518,6 +2539,9 @@ inline bool gather_batch8(const NodeDev& nd, int mixed) {
 void launch_gather_force(const NodeDev& nd, int mixed, const void* slots, double* f, int accumulate, cudaStream_t s) {
     AM_NODE_DISPATCH(k_gather_force, f, accumulate);
 }
+void launch_gather_force4(const NodeDev& nd, int mixed, const void* slots, double4* f, cudaStream_t s) {
+    AM_NODE_DISPATCH(k_gather_force4, f);
+}
 
 void launch_iface_gather(const NodeDev& nd, int mixed, const void* slots, int64_t num_local,
                          const int32_t* local_nodes, const int32_t* rows, double* buf, cudaStream_t s) {
@@ -2588,7 +2612,7 @@ void launch_rk_rows4(int64_t n, const int64_t* ptr, const int32_t* nbr, const do
                      double4* P4, cudaStream_t s) {
     if (n > 0) k_rk_rows4<<<grid_for(n * kRkLanes, 128), 128, 0, s>>>(n, ptr, nbr, val, U4, P4);
 }
-void launch_rk_cols3(int64_t n, const int64_t* tptr, const int32_t* tsrc, const double* tval, const double* f_local,
+void launch_rk_cols3(int64_t n, const int64_t* tptr, const int32_t* tsrc, const double* tval, const double4* f_local,
                      double* f, cudaStream_t s) {
     if (n > 0) k_rk_cols3<<<grid_for(n * kRkLanes, 128), 128, 0, s>>>(n, tptr, tsrc, tval, f_local, f);
 }

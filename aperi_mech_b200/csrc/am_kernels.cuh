@@ -130,6 +130,7 @@ void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const dou
 
 // f (N x 3, row-major) = gather of the slots (FP64 or FP32 slots), overwrite or accumulate.
 void launch_gather_force(const NodeDev& nd, int mixed, const void* slots, double* f, int accumulate, cudaStream_t s);
+void launch_gather_force4(const NodeDev& nd, int mixed, const void* slots, double4* f, cudaStream_t s);
 // Partial force of each local interface node (own slots only) into its row of the
 // exchange buffer (rows of nodes this rank does not hold are left as they are).
 void launch_iface_gather(const NodeDev& nd, int mixed, const void* slots, int64_t num_local,
@@ -170,7 +171,7 @@ void launch_pm_scale(int64_t n, double4* V4, double scale, cudaStream_t s);
 // the rows i that hold j, ascending i, with a unit entry for each empty row).
 void launch_rk_rows4(int64_t n, const int64_t* ptr, const int32_t* nbr, const double* val, const double4* U4,
                      double4* P4, cudaStream_t s);
-void launch_rk_cols3(int64_t n, const int64_t* tptr, const int32_t* tsrc, const double* tval, const double* f_local,
+void launch_rk_cols3(int64_t n, const int64_t* tptr, const int32_t* tsrc, const double* tval, const double4* f_local,
                      double* f, cudaStream_t s);
 void launch_sensor_seed(const double4* U4, int32_t num_sensors, const int32_t* sensors, double4* UB, double* loss,
                         cudaStream_t s);
