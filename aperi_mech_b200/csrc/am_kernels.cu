@@ -45,6 +45,10 @@ __device__ __forceinline__ double4 ld_dep(const double4* p) {
     return r;
 }
 __device__ __forceinline__ float4 ld_dep(const float4* p) { return __ldca(p); }
+// One 32-byte store (the arrays are 32-byte aligned).
+__device__ __forceinline__ void st4(double4* p, const double4& v) {
+    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(v.x), "d"(v.y), "d"(v.z), "d"(v.w) : "memory");
+}
 // One 32-byte load through the read-only path, for data that no kernel still running
 // writes (kernels launched without programmatic overlap, on arrays finished before).
 __device__ __forceinline__ double4 ld_ro4(const double4* p) {
@@ -1932,8 +1936,8 @@ __global__ void __launch_bounds__(kNodeBlock) k_node_step(NodeDev nd, const vec4
     const NodeSlots q = node_slots(nd, i, own);
     pdl_trigger();
     pdl_wait();
-    const double4 vh = V4[j];
-    const double4 u0 = advance ? U4[j] : make_double4(0.0, 0.0, 0.0, 0.0);
+    const double4 vh = ld_dep(V4 + j);
+    const double4 u0 = advance ? ld_dep(U4 + j) : make_double4(0.0, 0.0, 0.0, 0.0);
     double fx, fy, fz;
     gather<S, BATCH, LPN>(nd, slots, i, own, q, fx, fy, fz);
     if (!own || threadIdx.x % LPN != 0) return;
@@ -1957,12 +1961,12 @@ __global__ void __launch_bounds__(kNodeBlock) k_node_step(NodeDev nd, const vec4
         if (w) apply_bc(w, Q.vact, Q.vscale, nd.bcvalues, wx, wy, wz);
         double4 u = u0;
         displace(nd, i, rebase, Q.dt, wx, wy, wz, u);
-        U4[i] = u;
-        V4[i] = make_double4(wx, wy, wz, 0.0);
-        if (u_copy) u_copy[i] = u;
+        st4(U4 + i, u);
+        st4(V4 + i, make_double4(wx, wy, wz, 0.0));
+        if (u_copy) st4(u_copy + i, u);
     } else {
-        V4[i] = make_double4(vx, vy, vz, 0.0);
-        A4[i] = make_double4(ax, ay, az, 0.0);
+        st4(V4 + i, make_double4(vx, vy, vz, 0.0));
+        st4(A4 + i, make_double4(ax, ay, az, 0.0));
     }
 }
 
