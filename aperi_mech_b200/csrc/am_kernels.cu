@@ -506,11 +506,11 @@ __device__ __forceinline__ void hex_accumulate_r(T (*R)[8], const T* Q, int g) {
 // values come from the previous kernel (coherent loads, see ld_dep).
 template <typename T, bool DEP = false>
 __device__ __forceinline__ void hex_load_rel(const double4* __restrict__ A, const int32_t* nd, T (*V)[8]) {
-    const double4 a0 = DEP ? ld_dep(A + nd[0]) : A[nd[0]];
+    const double4 a0 = DEP ? ld_dep(A + nd[0]) : ld_ro4(A + nd[0]);
     V[0][0] = V[1][0] = V[2][0] = T(0);
 #pragma unroll
     for (int q = 1; q < 8; ++q) {
-        const double4 a = DEP ? ld_dep(A + nd[hex_node_of_corner(q)]) : A[nd[hex_node_of_corner(q)]];
+        const double4 a = DEP ? ld_dep(A + nd[hex_node_of_corner(q)]) : ld_ro4(A + nd[hex_node_of_corner(q)]);
         V[0][q] = T(a.x - a0.x);
         V[1][q] = T(a.y - a0.y);
         V[2][q] = T(a.z - a0.z);
