@@ -31,8 +31,12 @@ EXPORTED = [
     "am_cells_get_points", "am_cells_destroy", "am_get_layout", "am_rkpm_element_cells", "am_set_power_method",
     "am_stable_time_increment", "am_solve_power_method", "am_set_interface", "am_nccl_unique_id",
     "am_set_nccl", "am_set_rk_functions", "am_set_cell_groups", "am_rkpm_nodal_subcells", "am_cells_groups",
-    "am_set_formulation", "am_rkpm_hex8_element_cells",
+    "am_set_formulation", "am_rkpm_hex8_element_cells", "am_noalloc_status",
+    "am_measure_fma_peak",
 ]
+
+# Tets per call of am_tet4_internal_force_noalloc (AM_NOALLOC_MAX_TETS in include/aperi_b200.h).
+AM_NOALLOC_MAX_TETS = 174762
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -133,6 +137,8 @@ def load(build_if_missing: bool = False) -> C.CDLL:
         "am_set_formulation": (C.c_int, [vp, C.c_int32, C.c_int32]),
         "am_rkpm_hex8_element_cells": (C.c_int, [C.c_int64, _dp, C.c_int64, _ip, _dp, C.c_int32, C.c_double,
                                                  C.POINTER(vp)]),
+        "am_noalloc_status": (C.c_int, [vp, _ip, _lp]),
+        "am_measure_fma_peak": (C.c_int, [C.c_int32, vp, _dp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -226,16 +226,32 @@ void am_cells_destroy(am_cells* cells);
  * larger inputs return AM_ERANGE with the reason in am_last_error(NULL).
  *   coords, u, f : num_nodes x 3 row-major FP64;  conn : num_elems x 4 (reference node order)
  *   node_ptr (num_nodes+1) / node_slots (4 num_elems): for each node, the slots
- *   4e+a (element e, local node a) that touch it, ascending.
- * The first call on a device looks up the scratch array's device address (so make
- * that call before any stream capture). All calls share the array: each call
- * overwrites the slots it reads, so nothing needs clearing, but calls that overlap
- * on the GPU race on it and must be ordered by the caller. Stream-ordered on
- * cuda_stream (NULL = legacy default stream); nothing is synchronized. */
+ *   4e+a (element e, local node a) that touch it, ascending. node_ptr[num_nodes]
+ *   must equal 4 num_elems and every slot id must be below it: only those slots
+ *   are written by this call, so a range or id beyond them would read what an
+ *   earlier call left in the shared array. Such entries are skipped and reported
+ *   as AM_EINVAL through am_noalloc_status (index = the node).
+ * The first call on a device, and the first after a device reset, looks up the
+ * scratch array's device address (so make that call before any stream capture).
+ * All calls share the array: each call overwrites the slots it reads, so nothing
+ * needs clearing, but calls that overlap on the GPU race on it and must be ordered
+ * by the caller. Stream-ordered on cuda_stream (NULL = legacy default stream);
+ * nothing is synchronized, and device-side checks do not change the return code:
+ * read them with am_noalloc_status. */
 #define AM_NOALLOC_MAX_TETS 174762
 int am_tet4_internal_force_noalloc(int32_t material, double lambda, double mu, int64_t num_nodes, int64_t num_elems,
                                    const double* coords, const double* u, const int32_t* conn,
                                    const int32_t* node_ptr, const int32_t* node_slots, double* f, void* cuda_stream);
+/* Device-side status of the most recent am_tet4_internal_force_noalloc call on the
+ * current device (no counterpart in the reference; the context path reports the same
+ * checks through its own return codes): *status = AM_OK, AM_ENONPOS_J (a tet with
+ * det J <= 0, or J <= 0 for neo-Hookean; *index = the tet) or AM_EINVAL (a node ->
+ * slot CSR entry outside the call's slots; *index = the node, or num_nodes when
+ * node_ptr[num_nodes] != 4 num_elems). The first error of a call wins. The word lives
+ * beside the scratch array, in fixed device memory shared by every caller, and each
+ * force call clears it before its kernels run; so read it on the same stream, after
+ * the call and before the next one. Synchronizes cuda_stream; allocates nothing. */
+int am_noalloc_status(void* cuda_stream, int32_t* status, int64_t* index);
 
 /* LinearElasticProperties::CompleteProperties (Materials/Base.h:47-158): props =
  * {youngs_modulus, poissons_ratio, shear_modulus, lambda, bulk_modulus} with NaN for
@@ -259,6 +275,12 @@ int64_t am_launch_count(const am_ctx* ctx);
  * Milliseconds and launch counts accumulate until am_profile_enable is called again. */
 int am_profile_enable(am_ctx* ctx, int enable);
 int am_profile_read(am_ctx* ctx, double ms[5], int64_t launches[5]);
+/* Measured FMA throughput of the current device (no counterpart in the reference): FP64
+ * (fp64 != 0) or FP32 fused multiply-adds in independent chains over the whole GPU,
+ * one launch timed with CUDA events on cuda_stream after a warm-up launch; writes
+ * flop/s (an FMA counts 2). The compute-roofline denominator for the element kernels,
+ * which FP32 issue or the FP64 pipe bind rather than HBM. Synchronizes cuda_stream. */
+int am_measure_fma_peak(int32_t fp64, void* cuda_stream, double* flops_per_s);
 
 /* ---- stable time increment by the power method (PowerMethodProcessor,
  * include/PowerMethodProcessor.h:87-480, and PowerMethodTimeStepper, TimeStepper.h:138-221) ----

@@ -70,3 +70,13 @@ def test_create_rejects_bad_input(capi_lib):
     assert capi_lib.am_create(0, None, C.byref(h)) == 1
     X = np.array([[0.0, math.nan, 0.0]])
     assert capi_lib.am_create(1, X.ctypes.data_as(C.POINTER(C.c_double)), C.byref(h)) == 1
+
+
+def test_noalloc_limit_mirrors_header():
+    """The Python constant the no-alloc tests size against is the header's #define."""
+    from aperi_mech_b200 import capi
+
+    text = (ROOT / "include" / "aperi_b200.h").read_text()
+    m = re.search(r"#define\s+AM_NOALLOC_MAX_TETS\s+(\d+)", text)
+    assert m is not None
+    assert int(m.group(1)) == capi.AM_NOALLOC_MAX_TETS
