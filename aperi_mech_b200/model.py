@@ -54,10 +54,14 @@ class Material:
     mu: float
 
     @classmethod
-    def create(cls, kind: str, density: float, **props) -> "Material":
+    def create(cls, kind: str, density: float, complete=None, **props) -> "Material":
+        """CreateMaterial: kind, density and two elastic constants. `complete` replaces the
+        library's property completion (a callable taking the constants as keywords and
+        returning all five), for callers that build problems without loading the CUDA
+        library."""
         if kind not in MATERIAL_KINDS:
             raise ValueError(f"unknown material {kind!r}")
-        p = complete_properties(**props)
+        p = (complete or complete_properties)(**props)
         return cls(kind, float(density), p["lambda"], p["shear_modulus"])
 
     @property

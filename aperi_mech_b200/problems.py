@@ -67,14 +67,15 @@ def hex8_le_cube(n: int = 20, seed: int = 0, nsteps: int = 100) -> Problem:
                    v0, dt, nsteps, seed, {"config": "Hex8 2x2x2 Gauss, linear elastic"})
 
 
-def tet4_nh_shear(n: int = 70, seed: int = 0, nsteps: int = 1000, jitter: float = 0.2) -> Problem:
+def tet4_nh_shear(n: int = 70, seed: int = 0, nsteps: int = 1000, jitter: float = 0.2, complete=None) -> Problem:
+    """complete: property completion to use instead of the library's (Material.create)."""
     rng = np.random.default_rng(seed)
     coords, conn_hex = mesh.box_hex(n, n, n)
     h = 1.0 / n
     coords = mesh.jitter_interior(coords, jitter * h, rng)
     conn = mesh.hex_to_tets(conn_hex)
     mesh.check_orientation(coords, conn)
-    mat = Material.create("neo_hookean", 1000.0, shear_modulus=3.85e8, bulk_modulus=8.33e8)
+    mat = Material.create("neo_hookean", 1000.0, complete=complete, shear_modulus=3.85e8, bulk_modulus=8.33e8)
     fixed = mesh.side_sets(coords)["surface_5"]
     v0 = _initial_velocity(coords, fixed, rng, shear=1.0)
     c = wave_speed(mat.lam, mat.mu, mat.density)

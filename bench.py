@@ -285,46 +285,50 @@ def time_run(torch, model, prob, steps, warmup, prec, stream, dev, world, sample
 
 
 def algorithmic_bytes(prob, layout, slot_bytes=12):
-    """Compulsory HBM bytes per launch of the element and node kernels; slot_bytes is
-    three reals (12 B mixed, 24 B FP64). Element kernels: coordinates and displacement
-    read once per node (48 B), connectivity (4 B per element node) or, for cell blocks,
-    each entry's node id and gradient (4 B + three reals), per-element moduli (8 B
-    per field), and the node-major force slots written once. Node kernel: the slots
-    read once, and per node mass 8 B, BC word 4 B, slot range 4 B, displacement and
-    half-step velocity read and written (96 B)."""
+    """Compulsory HBM bytes per launch (every array touched once, FP64 state) of the
+    element and node kernels, and apart from them the bytes this implementation's
+    layout adds (`*_impl`: the node-major force slots written by the element kernel and
+    read back by the node kernel, 12 B mixed / 24 B FP64 per slot, plus the node
+    kernel's BC word and slot range).
+    Element kernels: per node X and u read (48 B) and f written (24 B); per Gauss
+    element its connectivity (4 B per element node) and 8 B per modulus field; per
+    cell entry its node id and gradient (4 B + three reals) and per cell its volume.
+    Node kernel (the fused central-difference update): per node u, v, f read (24 B
+    each), the mass (8 B), u and v written (24 B each): 128 B."""
     N = prob.num_nodes
     S = layout["used_slots"]
-    elem = 48 * N + slot_bytes * S
-    node = slot_bytes * S + (8 + 4 + 4 + 96) * N
     r = slot_bytes // 3
+    elem = 48 * N + (24 * N if any(p.kind != "cells" for p in prob.parts) else 0)
     for p in prob.parts:
         if p.kind == "cells":
-            elem += (4 + slot_bytes) * int(p.cell_ptr[-1])
-            if p.cell_groups is not None:
-                # F-bar passes: H and J written and read back, the barred stress written
-                # and replaced, the subcell stress read, and the entries read a second time.
-                elem += 38 * r * p.num_elems + (4 + slot_bytes) * int(p.cell_ptr[-1])
+            elem += (4 + 3 * r) * int(p.cell_ptr[-1]) + 8 * p.num_elems
         else:
             elem += 4 * p.conn.size
         elem += 8 * p.num_elems * ((p.mu_field is not None) + (p.kappa_field is not None))
     rk = prob.meta.get("rk")
     if rk is not None:
-        # two-pass coupling: the functions read twice (row and transposed, 12 B per entry),
-        # the physical displacement written (32 B), the local force written and read (48 B)
-        # and the generalized force written and read (48 B) per node.
-        elem += 24 * int(rk[0][-1]) + 128 * N
-    return {"element": elem, "node": node}
+        # two-pass coupling: the functions read once (index + FP64 value per entry) and
+        # the physical displacement written and read once per node
+        elem += 12 * int(rk[0][-1]) + 48 * N
+    node = 128 * N
+    return {"element": elem, "node": node,
+            "element_impl": elem + slot_bytes * S - 24 * N,
+            "node_impl": node + slot_bytes * S + 8 * N - 24 * N}
 
 
-def profiled_traffic(workload: str, role: str, prec: str):
-    """DRAM bytes (read + write) per launch of a kernel from the committed ncu
-    summaries under profiles/ (lines 'traffic workload=W role=R prec=P bytes=B');
-    None when no capture of that kernel on that workload is recorded."""
+def profiled(workload: str, role: str, prec: str, key: str):
+    """A value recorded from an ncu capture in the committed summaries under profiles/
+    (lines 'traffic workload=W role=R prec=P bytes=B' for DRAM bytes read + written per
+    launch, 'bound workload=W role=R prec=P bound=B' for the binding resource); None when
+    no capture of that kernel on that workload is recorded."""
+    tag = "traffic " if key == "bytes" else "bound "
     for f in sorted((ROOT / "profiles").glob("*.md")):
         for line in f.read_text().splitlines():
-            t = dict(kv.split("=", 1) for kv in line.split()[1:] if "=" in kv) if line.strip().startswith("traffic ") else {}
-            if t.get("workload") == workload and t.get("role") == role and t.get("prec") == prec:
-                return int(t["bytes"])
+            if not line.strip().startswith(tag):
+                continue
+            t = dict(kv.split("=", 1) for kv in line.split()[1:] if "=" in kv)
+            if t.get("workload") == workload and t.get("role") == role and t.get("prec") == prec and key in t:
+                return int(t[key]) if key == "bytes" else t[key]
     return None
 
 
@@ -345,21 +349,71 @@ def algorithmic_flop(prob):
     return total
 
 
-def roofline_for(kernels, alg, peak, peak_kind, workload=None, prec="mixed", flop=None):
+def roofline_for(kernels, alg, peak, peak_kind, workload=None, prec="mixed", flop=None, fma=None):
+    """Roofline of the kernel that takes the larger share of the step. `achieved` is its
+    compulsory bytes per launch over its CUDA-event launch time, against the measured
+    HBM copy bandwidth; `bound` is the resource that ncu showed binding it (from the
+    committed capture of that kernel on this workload: 'issue', 'fp64_pipe', 'hbm',
+    'latency'), 'hbm' where none is recorded. For element kernels `compute` gives the
+    algorithmic flop rate against the measured FMA peak of the precision the kernel
+    computes in (FP32 for the mixed path)."""
     dominant = "node" if kernels["node_total_ms"] >= kernels["element_total_ms"] else "element"
     ms = kernels[f"{dominant}_ms"]
     achieved = alg[dominant] / (ms * 1e-3) / 1e9
-    out = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
-           "frac": achieved / peak, "peak_source": peak_kind,
-           "traffic": profiled_traffic(workload, dominant, prec) if workload else None,
-           "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/",
-           "algorithmic_bytes_per_launch": alg[dominant], "ms_per_launch": ms}
+    traffic = profiled(workload, dominant, prec, "bytes") if workload else None
+    out = {"bound": (profiled(workload, dominant, prec, "bound") if workload else None) or "hbm",
+           "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+           "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, copy)"
+           if peak_kind == "measured" else peak_kind,
+           "traffic": traffic,
+           "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, profiles/",
+           "algorithmic_bytes_per_launch": alg[dominant],
+           "implementation_bytes_per_launch": alg[f"{dominant}_impl"],
+           "traffic_over_algorithmic": traffic / alg[dominant] if traffic else None,
+           "ms_per_launch": ms}
     if flop and dominant == "element":
-        out["compute"] = {"algorithmic_flop_per_launch": flop, "achieved_tflops": flop / (ms * 1e-3) / 1e12}
+        tf = flop / (ms * 1e-3) / 1e12
+        c = {"algorithmic_flop_per_launch": flop, "achieved_tflops": tf}
+        key = "fp64" if prec == "fp64" else "fp32"
+        if fma and fma.get(key):
+            c.update({"peak_tflops": fma[key], "frac": tf / fma[key],
+                      "peak_source": f"{key.upper()} FMA throughput measured in this run (am_measure_fma_peak)"})
+        out["compute"] = c
     return out
 
 
-def measure_workload(torch, prob, steps, warmup, stream, dev, world, mass=None, precs=("fp64", "mixed")):
+def fma_peaks(stream):
+    """FP32 and FP64 FMA throughput of this GPU, measured once (TFLOP/s)."""
+    import ctypes as C
+
+    from aperi_mech_b200 import capi
+
+    lib = capi.load()
+    out = {}
+    for key, fp64 in (("fp32", 0), ("fp64", 1)):
+        v = C.c_double(0.0)
+        if lib.am_measure_fma_peak(fp64, stream.cuda_stream, C.byref(v)) == capi.AM_OK:
+            out[key] = v.value / 1e12
+    return out
+
+
+def mixed_errors(prob, steps_total, s64, sm, f64=None, fm=None):
+    """Mixed-vs-FP64 errors: the displacement after the run (relative to the FP64 one),
+    the same against the part of the displacement the internal forces produced
+    (u - v0 t, v0 t being the force-free drift both paths integrate in FP64), the
+    acceleration at the last step, and the internal force at the FP64 displacement."""
+    u64, _, a64 = s64
+    um, _, am = sm
+    ukin = prob.v0 * (steps_total * prob.dt)
+    out = {"rel_disp_err_l2": float(np.linalg.norm(um - u64) / np.linalg.norm(u64)),
+           "rel_disp_err_l2_force_part": float(np.linalg.norm(um - u64) / max(np.linalg.norm(u64 - ukin), 1e-300)),
+           "rel_accel_err_l2": float(np.linalg.norm(am - a64) / max(np.linalg.norm(a64), 1e-300))}
+    if f64 is not None:
+        out["rel_force_err_l2"] = float(np.linalg.norm(fm - f64) / np.linalg.norm(f64))
+    return out
+
+
+def measure_workload(torch, prob, steps, warmup, stream, dev, world, mass=None, precs=("fp64", "mixed"), fma=None):
     from aperi_mech_b200.model import ExplicitDynamics
 
     out = {"workload": prob.name, "elements": prob.num_elems, "nodes": prob.num_nodes, "steps": steps,
@@ -371,19 +425,22 @@ def measure_workload(torch, prob, steps, warmup, stream, dev, world, mass=None, 
         states = {}
         for prec in precs:
             r = time_run(torch, m, prob, steps, warmup, prec, stream, dev, world)
-            states[prec] = r["state"][0]
+            states[prec] = r["state"]
             out[prec] = {"value": r["value"], "ms_per_step": r["ms"] / steps, "kernels": r["kernels"]}
         if "fp64" in states and "mixed" in states:
-            u64 = states["fp64"]
-            out["mixed_rel_disp_err_l2"] = float(np.linalg.norm(states["mixed"] - u64) / np.linalg.norm(u64))
+            u64 = states["fp64"][0]
             f64 = m.internal_force(u64, "fp64")
-            out["mixed_rel_force_err_l2"] = float(np.linalg.norm(m.internal_force(u64, "mixed") - f64) / np.linalg.norm(f64))
+            err = mixed_errors(prob, warmup + steps, states["fp64"], states["mixed"], f64,
+                               m.internal_force(u64, "mixed"))
+            out["mixed_vs_fp64"] = err
+            out["mixed_rel_disp_err_l2"] = err["rel_disp_err_l2"]
+            out["mixed_rel_force_err_l2"] = err["rel_force_err_l2"]
         if "mixed" in precs:
             out["roofline_mixed"] = roofline_for(out["mixed"]["kernels"], algorithmic_bytes(prob, layout), peak, kind,
-                                                 prob.name, "mixed", algorithmic_flop(prob))
+                                                 prob.name, "mixed", algorithmic_flop(prob), fma)
         if "fp64" in precs:
             out["roofline_fp64"] = roofline_for(out["fp64"]["kernels"], algorithmic_bytes(prob, layout, 24), peak, kind,
-                                                prob.name, "fp64", algorithmic_flop(prob))
+                                                prob.name, "fp64", algorithmic_flop(prob), fma)
     return out
 
 
@@ -495,15 +552,14 @@ def run_ours(args, rank, world, local):
         attach_interface(model, prob, rank, world)
     layout = model.layout()
     hbm_peak, peak_kind = measured_peaks()
+    fma = fma_peaks(stream)
     for prec in ("fp64", "mixed"):
         res[prec] = time_run(torch, model, prob, args.steps, args.warmup, prec, stream, dev, world,
                              sampler_index=local if prec == "mixed" else None)
     # accuracy of the mixed path against the FP64 path (itself 1e-12 from the oracle)
-    u64, um = res["fp64"]["state"][0], res["mixed"]["state"][0]
-    disp_err = float(np.linalg.norm(um - u64) / np.linalg.norm(u64))
-    f64 = model.internal_force(u64, "fp64")
-    f32 = model.internal_force(u64, "mixed")
-    force_err = float(np.linalg.norm(f32 - f64) / np.linalg.norm(f64))
+    u64 = res["fp64"]["state"][0]
+    errors = mixed_errors(prob, args.warmup + args.steps, res["fp64"]["state"], res["mixed"]["state"],
+                          model.internal_force(u64, "fp64"), model.internal_force(u64, "mixed"))
 
     # end to end through the public API: pinned host state in, K steps, host state out
     e2e = None
@@ -531,10 +587,12 @@ def run_ours(args, rank, world, local):
     model.close()
 
     roofline = roofline_for(res["mixed"]["kernels"], algorithmic_bytes(prob, layout), hbm_peak, peak_kind,
-                            prob.name, "mixed", algorithmic_flop(prob))
+                            prob.name, "mixed", algorithmic_flop(prob), fma)
     roofline["layout"] = layout
     roofline_fp64 = roofline_for(res["fp64"]["kernels"], algorithmic_bytes(prob, layout, 24), hbm_peak, peak_kind,
-                                 prob.name, "fp64", algorithmic_flop(prob))
+                                 prob.name, "fp64", algorithmic_flop(prob), fma)
+    # the CPU oracle on the same mesh (rank 0 at N = 1), while the problem is at hand
+    cpu = None if (args.skip_cpu or rank != 0 or world != 1) else cpu_baseline(prob)
 
     # the other configurations, each on its own context
     extras = {}
@@ -542,32 +600,32 @@ def run_ours(args, rank, world, local):
         args.skip_extras = args.skip_adjoint = True  # the adjoint is single-domain
     if not args.skip_extras:
         p1 = problems.hex8_le_cube(n=20, seed=0, nsteps=100)
-        extras["hex8_le_cube_20"] = measure_workload(torch, p1, 100, args.warmup, stream, dev, world)
+        extras["hex8_le_cube_20"] = measure_workload(torch, p1, 100, args.warmup, stream, dev, world, fma=fma)
         p3a = problems.smoothed_tet4_box(n=args.box_n, seed=0, nsteps=500)
         extras["smoothed_tet4_box"] = measure_workload(torch, p3a, 500, args.warmup, stream, dev, world,
-                                                       mass=p3a.meta["mass"])
+                                                       mass=p3a.meta["mass"], fma=fma)
         t0 = time.perf_counter()
         p3b = problems.rkpm_box(n=args.box_n, seed=0, nsteps=500)
         setup_s = time.perf_counter() - t0
-        r = measure_workload(torch, p3b, 500, args.warmup, stream, dev, world, mass=p3b.meta["mass"])
+        r = measure_workload(torch, p3b, 500, args.warmup, stream, dev, world, mass=p3b.meta["mass"], fma=fma)
         r["setup_s"] = setup_s
         r["entries_per_cell"] = p3b.meta["entries_per_cell"]
         extras["rkpm_box"] = r
         t0 = time.perf_counter()
         p3c = problems.rkpm_fbar_box(n=args.fbar_n, seed=0, nsteps=200)
         setup_s = time.perf_counter() - t0
-        r = measure_workload(torch, p3c, 200, args.warmup, stream, dev, world, mass=p3c.meta["mass"])
+        r = measure_workload(torch, p3c, 200, args.warmup, stream, dev, world, mass=p3c.meta["mass"], fma=fma)
         r["setup_s"] = setup_s
         r["entries_per_subcell"] = p3c.meta["entries_per_cell"]
         extras["rkpm_fbar_box"] = r
         t0 = time.perf_counter()
         p3d = problems.rkpm_two_pass_box(n=args.box_n, seed=0, nsteps=500)
         setup_s = time.perf_counter() - t0
-        r = measure_workload(torch, p3d, 500, args.warmup, stream, dev, world, mass=p3d.meta["mass"])
+        r = measure_workload(torch, p3d, 500, args.warmup, stream, dev, world, mass=p3d.meta["mass"], fma=fma)
         r["setup_s"] = setup_s
         extras["rkpm_two_pass_box"] = r
         p5 = problems.hex8_nh_lognormal(n=args.hex_n, seed=0, nsteps=1000, bulk_field=True)
-        extras["hex8_nh_lognormal_large"] = measure_workload(torch, p5, 1000, args.warmup, stream, dev, world)
+        extras["hex8_nh_lognormal_large"] = measure_workload(torch, p5, 1000, args.warmup, stream, dev, world, fma=fma)
         if not args.skip_adjoint:
             extras["hex8_nh_lognormal_large"]["adjoint"] = run_adjoint(torch, p5, 50, stream, dev)
 
@@ -576,43 +634,57 @@ def run_ours(args, rank, world, local):
         adj = run_adjoint(torch, problems.hex8_nh_lognormal(n=args.adjoint_n, seed=0, nsteps=200), 20, stream, dev)
     kernel_ms = {p: res[p]["kernels"] for p in ("fp64", "mixed")}
     launches = {p: res[p]["launches"] for p in ("fp64", "mixed")}
-    return (prob, res, disp_err, force_err, e2e, adj, roofline, roofline_fp64, kernel_ms, launches,
-            res["mixed"]["clocks"], extras)
+    return (prob, res, errors, e2e, adj, roofline, roofline_fp64, kernel_ms, launches,
+            res["mixed"]["clocks"], extras, cpu, fma)
 
 
-def cpu_baseline(target_s=10.0, n=24):
-    """The oracle (C++ FP64 restatement, all host threads) on a bounded sample of the
-    same workload family: the neo-Hookean Tet4 shear mesh at n^3 x 6 tets."""
-    from aperi_mech_b200 import problems
+def workload_config(prob, world, decompose):
+    """The `config` of the JSON line, the same for both arms on the same workload."""
+    return {"workload": prob.name, "elements": prob.num_elems, "nodes": prob.num_nodes,
+            "description": prob.meta.get("config"), "material": "neo-Hookean mu=3.85e8 kappa=8.33e8"
+            if "nh" in prob.name or "box" in prob.name else "linear elastic E=1e9 nu=0.3",
+            "dt": prob.dt, "seed": prob.seed,
+            "l2_flush": "inputs larger than L2 (state + slots + connectivity ~ 230 MB per step)",
+            "parallelism": (f"z-slab domain decomposition x{world}, interface forces summed over NCCL "
+                            f"({prob.meta['num_iface']} interface nodes)" if decompose else
+                            f"replicas x{world}" if world > 1 else "single GPU")}
+
+
+def cpu_baseline(prob, target_s=10.0):
+    """The oracle (C++ FP64 restatement, all host threads) on the benchmark's own mesh:
+    central-difference steps from the same initial state, as many as take about
+    target_s seconds (a two-step probe sizes the sample)."""
     from oracle import oracle
 
-    p = problems.tet4_nh_shear(n=n, seed=0, nsteps=1)
-    op = oracle.OracleProblem.from_problem(p)
-    u = np.zeros_like(p.coords)
+    op = oracle.OracleProblem.from_problem(prob)
+    u = np.zeros_like(prob.coords)
     a = op.init_acceleration(u)
     t0 = time.perf_counter()
-    u1, v1, a1 = op.steps(u, p.v0, a, np.full(2, p.dt))
+    op.steps(u, prob.v0, a, np.full(2, prob.dt))
     t1 = (time.perf_counter() - t0) / 2
     steps = max(2, int(target_s / max(t1, 1e-6)))
     t0 = time.perf_counter()
-    op.steps(u, p.v0, a, np.full(steps, p.dt))
+    op.steps(u, prob.v0, a, np.full(steps, prob.dt))
     dt = time.perf_counter() - t0
-    return {"value": p.num_elems * steps / dt / 1e6, "unit": UNIT, "cores": oracle.get_threads(), "kind": "port",
-            "sample": f"tet4_nh_shear_{n} ({p.num_elems} tets), {steps} central-difference steps, FP64, "
-                      f"{oracle.get_threads()} OpenMP threads"}
+    return {"value": prob.num_elems * steps / dt / 1e6, "unit": UNIT, "cores": oracle.get_threads(), "kind": "port",
+            "sample": f"{prob.name} ({prob.num_elems} tets, the benchmark mesh), {steps} of its central-difference "
+                      f"steps, FP64, {oracle.get_threads()} OpenMP threads; the reference CPU build is unavailable "
+                      f"(Kokkos/Trilinos/Eigen/MPI missing), so the oracle restatement stands in for it"}
 
 
 def run_reference(args, rank, world):
     """Reference arm: the reference's CPU implementation cannot be built here (Kokkos,
-    Trilinos/STK, Eigen, yaml-cpp, MPI absent), so its CPU restatement (oracle) runs on
-    the host cores; each step is one central-difference step of a bounded sample mesh."""
+    Trilinos/STK, Eigen, yaml-cpp, MPI absent), so its CPU restatement (the oracle, FP64,
+    all host threads) runs the benchmark's own workload: the same seeded mesh, initial
+    state and dt, `warmup` untimed and `steps` timed central-difference steps. The
+    problem is built without the CUDA library (the oracle completes the material
+    properties), so this process loads only the oracle."""
     if rank != 0:
         return
     from aperi_mech_b200 import problems
     from oracle import oracle
 
-    n = 24
-    p = problems.tet4_nh_shear(n=n, seed=0, nsteps=1)
+    p = problems.tet4_nh_shear(n=args.n, seed=0, nsteps=args.steps, complete=oracle.complete_properties)
     op = oracle.OracleProblem.from_problem(p)
     u = np.zeros_like(p.coords)
     a = op.init_acceleration(u)
@@ -621,12 +693,13 @@ def run_reference(args, rank, world):
     op.steps(u, v, a, np.full(args.steps, p.dt), t0=args.warmup * p.dt)
     dt = time.perf_counter() - t0
     value = p.num_elems * args.steps / dt / 1e6
-    sample = (f"tet4_nh_shear_{n} ({p.num_elems} tets) per step, FP64 oracle restatement (reference CPU build "
-              f"unavailable: missing Kokkos/Trilinos/Eigen/MPI)")
+    sample = (f"{p.name} ({p.num_elems} tets, the benchmark workload itself), {args.steps} timed FP64 "
+              f"central-difference steps after {args.warmup} untimed; oracle restatement of the reference's CPU "
+              f"path (reference CPU build unavailable: missing Kokkos/Trilinos/Eigen/MPI)")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sample_workload": f"tet4_nh_shear_{n}"},
+            "config": workload_config(p, world, False),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": oracle.get_threads(), "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -639,27 +712,21 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
-    (prob, res, disp_err, force_err, e2e, adj, roofline, roofline_fp64, kernel_ms, launches, clocks,
-     extras) = run_ours(args, rank, world, local)
+    (prob, res, errors, e2e, adj, roofline, roofline_fp64, kernel_ms, launches, clocks,
+     extras, cpu, fma) = run_ours(args, rank, world, local)
     if rank != 0:
         return
-    cpu = None if args.skip_cpu else cpu_baseline()
     ms_step = res["mixed"]["ms"] / args.steps
     line = {
         "metric": METRIC, "value": res["mixed"]["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-        "config": {"workload": prob.name, "elements": prob.num_elems, "nodes": prob.num_nodes,
-                   "description": prob.meta.get("config"), "material": "neo-Hookean mu=3.85e8 kappa=8.33e8"
-                   if "nh" in prob.name or "box" in prob.name else "linear elastic E=1e9 nu=0.3",
-                   "dt": prob.dt, "seed": prob.seed,
-                   "l2_flush": "inputs larger than L2 (state + slots + connectivity ~ 230 MB per step)",
-                   "parallelism": (f"z-slab domain decomposition x{world}, interface forces summed over NCCL "
-                                   f"({prob.meta['num_iface']} interface nodes)" if args.decompose else
-                                   f"replicas x{world}" if world > 1 else "single GPU")},
-        "fp64": {"value": res["fp64"]["value"], "ms_per_step": res["fp64"]["ms"] / args.steps},
-        "mixed_vs_fp64": {"rel_disp_err_l2": disp_err, "rel_force_err_l2": force_err,
-                          "speedup": res["mixed"]["value"] / res["fp64"]["value"]},
+        "config": workload_config(prob, world, args.decompose),
+        "value_fp64": res["fp64"]["value"],
+        "fp64": {"value": res["fp64"]["value"], "ms_per_step": res["fp64"]["ms"] / args.steps,
+                 "note": "the plain FP64 path, the reference's precision"},
+        "mixed_vs_fp64": dict(errors, speedup=res["mixed"]["value"] / res["fp64"]["value"]),
+        "fma_peak_tflops": fma,
         "adjoint": adj,
         "roofline": roofline,
         "roofline_fp64": roofline_fp64,
