@@ -5,6 +5,7 @@
 #include <nccl.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -17,6 +18,7 @@
 
 #include "../../include/aperi_b200.h"
 #include "am_host.hpp"
+#include "am_order.hpp"
 #include "am_kernels.cuh"
 
 namespace {
@@ -126,6 +128,25 @@ struct Block {
     double* patch_dx64 = nullptr;
     const int32_t* slot_pos = nullptr;  // block-local view into the context's position array
     std::vector<int32_t> host_nodes;    // node of each logical slot (-1: unused), for the node CSR
+    // Processing order of a Gauss block's elements: order[k] is the caller's index of the
+    // block's k-th element as stored and run here (empty: the caller's order). Per-element
+    // inputs are permuted into it and per-element outputs back out of it.
+    std::vector<int32_t> order;
+    int32_t* order_dev = nullptr;
+
+    // A per-element array given in the caller's order, in the processing order.
+    std::vector<double> to_order(const double* v) const {
+        if (order.empty()) return std::vector<double>(v, v + num_elems);
+        std::vector<double> out(num_elems);
+        for (int64_t k = 0; k < num_elems; ++k) out[k] = v[order[k]];
+        return out;
+    }
+    // A per-element host array in the processing order, back into the caller's order.
+    void from_order(double* v) const {
+        if (order.empty()) return;
+        std::vector<double> tmp(v, v + num_elems);
+        for (int64_t k = 0; k < num_elems; ++k) v[order[k]] = tmp[k];
+    }
 
     am::GaussBlockDev gauss() const {
         am::GaussBlockDev g{};
@@ -206,6 +227,7 @@ struct Block {
         dfree(patch_gather);
         dfree(patch_dx32);
         dfree(patch_dx64);
+        dfree(order_dev);
         dfree(hstate);
         dfree(href);
         dfree(group_ptr);
@@ -315,7 +337,14 @@ struct am_ctx {
     int64_t num_used_slots = 0;    // slots referenced by a node
     std::vector<double4*> adj_bufs;  // cached adjoint checkpoint / segment buffers
     int64_t adj_key[3] = {0, 0, 0};
-    bool tet4_patches = true;  // APERI_B200_TET4_PATCHES=0 turns element patching off
+    // Tet4 element patches: 2 (default) split-hex patches where every tet lies on a
+    // six-tet ring, else generic patches; APERI_B200_TET4_PATCHES=1 generic patches only,
+    // =0 one thread per tet.
+    int32_t tet4_patches = 2;
+    // Element processing order of Gauss blocks: the locality order chosen from the mesh
+    // (element_order, the default) or, with APERI_B200_ELEMENT_ORDER=input, the caller's.
+    bool locality_order = true;
+    std::vector<double> host_X;  // coordinates (N x 3), for the element order at am_add_block
     am::StepParams* table = nullptr;
     int64_t table_cap = 0;
     am::StepParams* table_host = nullptr;  // pinned staging
@@ -577,13 +606,45 @@ struct am_ctx {
         check_launch("vjp kernel");
     }
 
+    // Per-element arrays over all blocks (block after block), from the processing order
+    // back into the caller's: on the host in place, on the device through a scratch copy.
+    void elems_to_caller_host(double* v) const {
+        if (!v) return;
+        int64_t off = 0;
+        for (const auto& b : blocks) {
+            b.from_order(v + off);
+            off += b.num_elems;
+        }
+    }
+    void elems_to_caller_device(double* v) {
+        if (!v) return;
+        int64_t off = 0;
+        for (const auto& b : blocks) {
+            if (b.order_dev) {
+                double* tmp = dalloc<double>(b.num_elems, "element scratch");
+                std::unique_ptr<double, void (*)(double*)> hold(tmp, [](double* p) { cudaFree(p); });
+                ck(cudaMemcpyAsync(tmp, v + off, b.num_elems * sizeof(double), cudaMemcpyDeviceToDevice, stream), "copy");
+                am::launch_scatter_elems(b.order_dev, b.num_elems, tmp, v + off, stream);
+                ++launches;
+                ck(cudaStreamSynchronize(stream), "synchronize");
+            }
+            off += b.num_elems;
+        }
+    }
+
     void reset_status() { ck(cudaMemsetAsync(status, 0, 2 * sizeof(int), stream), "reset status"); }
 
     void check_status() {
         int h[2] = {0, 0};
         ck(cudaMemcpyAsync(h, status, sizeof(h), cudaMemcpyDeviceToHost, stream), "read status");
         ck(cudaStreamSynchronize(stream), "synchronize");
-        if (h[0] == AM_ENONPOS_J) fail(AM_ENONPOS_J, "non-positive Jacobian determinant at element/cell " + std::to_string(h[1]));
+        if (h[0] == AM_ENONPOS_J) {
+            // Gauss elements are counted in the processing order; with one block it maps back.
+            int64_t idx = h[1];
+            if (blocks.size() == 1 && !blocks[0].order.empty() && idx >= 0 && idx < blocks[0].num_elems)
+                idx = blocks[0].order[idx];
+            fail(AM_ENONPOS_J, "non-positive Jacobian determinant at element/cell " + std::to_string(idx));
+        }
         if (h[0] == AM_ENAN) fail(AM_ENAN, "non-finite acceleration at node " + std::to_string(h[1]));
         if (h[0] != 0) fail(h[0], "device status " + std::to_string(h[0]));
     }
@@ -881,7 +942,7 @@ int am_create(int64_t num_nodes, const double* coords, am_ctx** out) {
         ck(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream create");
         c->own_stream = true;
         const char* patches = std::getenv("APERI_B200_TET4_PATCHES");
-        c->tet4_patches = !(patches && patches[0] == '0');
+        c->tet4_patches = patches && patches[0] == '0' ? 0 : patches && patches[0] == '1' ? 1 : 2;
         c->N = num_nodes;
         const size_t N = static_cast<size_t>(num_nodes);
         c->X4 = dalloc<double4>(N, "coordinates");
@@ -896,6 +957,9 @@ int am_create(int64_t num_nodes, const double* coords, am_ctx** out) {
         c->status = dalloc<int>(2, "status");
         c->f_scratch = dalloc<double>(N * 3, "force scratch");
         c->io_scratch = dalloc<double>(N * 3, "io scratch");
+        const char* order = std::getenv("APERI_B200_ELEMENT_ORDER");
+        c->locality_order = !(order && std::strcmp(order, "input") == 0);
+        c->host_X.assign(coords, coords + 3 * N);
         std::vector<double4> x(N);
         for (size_t i = 0; i < N; ++i) x[i] = make_double4(coords[3 * i], coords[3 * i + 1], coords[3 * i + 2], 0.0);
         ck(cudaMemcpy(c->X4, x.data(), N * sizeof(double4), cudaMemcpyHostToDevice), "coords upload");
@@ -1002,7 +1066,7 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
                 b.host_nodes.assign(d->cell_nodes, d->cell_nodes + K);
                 // Cells of four entries that group into split hexes (a tet mesh's element
                 // cells) run as patches like the Gauss tets: one slot per patch node.
-                bool four = E > 0 && ctx->tet4_patches;
+                bool four = E > 0 && ctx->tet4_patches == 2;
                 for (int64_t c = 0; c < E && four; ++c) four = ptr[c + 1] - ptr[c] == 4;
                 if (four) {
                     TetPatches tp = build_tet_patches(d->cell_nodes, E);
@@ -1026,20 +1090,36 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
                 for (int64_t s = 0; s < S; ++s)
                     if (d->conn[s] < 0 || d->conn[s] >= ctx->N) fail(AM_EINVAL, "connectivity index out of range");
                 b.num_entries = S;
+                // The elements run in the locality order (element_order); the block keeps
+                // that order's connectivity, and per-element data are permuted through it.
+                const int32_t* conn = d->conn;
+                std::vector<int32_t> conn_ordered;
+                if (ctx->locality_order && E > 1) {
+                    am::ElementOrder eo = am::element_order(d->conn, E, nn, ctx->host_X,
+                                                    d->kind == AM_TET4_GAUSS && ctx->tet4_patches == 2 && ctx->lagr == 0);
+                    conn_ordered.resize(S);
+                    for (int64_t k = 0; k < E; ++k)
+                        std::copy(d->conn + nn * static_cast<int64_t>(eo.order[k]), d->conn + nn * static_cast<int64_t>(eo.order[k]) + nn,
+                                  conn_ordered.begin() + nn * k);
+                    conn = conn_ordered.data();
+                    b.order = std::move(eo.order);
+                    b.order_dev = dalloc<int32_t>(E, "element order");
+                    ck(cudaMemcpy(b.order_dev, b.order.data(), E * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+                }
                 if (S > 0) {
                     b.conn = dalloc<int32_t>(S, "connectivity");
-                    ck(cudaMemcpy(b.conn, d->conn, S * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+                    ck(cudaMemcpy(b.conn, conn, S * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
                 }
-                b.host_nodes.assign(d->conn, d->conn + S);
+                b.host_nodes.assign(conn, conn + S);
                 if (d->kind == AM_TET4_GAUSS && E > 0 && ctx->tet4_patches && ctx->lagr == 0) {
                     // Patch the tets when patches hold 2.5 tets or more on average; fewer
                     // would leave most of the eight lanes per patch idle.
-                    TetPatches tp = build_tet_patches(d->conn, E);
+                    TetPatches tp = build_tet_patches(conn, E);
                     const int64_t P = static_cast<int64_t>(tp.used.size());
                     if (static_cast<double>(E) >= 2.5 * static_cast<double>(P)) {
                         // Split-hex patches (six tets in the canonical local order) get the
                         // register-resident kernel; any other patching the generic one.
-                        const bool hex6 = hex6_patches(tp);
+                        const bool hex6 = ctx->tet4_patches == 2 && hex6_patches(tp);
                         b.patched = hex6 ? 2 : 1;
                         b.num_patches = P;
                         b.num_entries = 8 * P;
@@ -1068,13 +1148,15 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
                 for (int64_t e = 0; e < E; ++e)
                     if (!(d->mu_field[e] > 0.0)) fail(AM_EINVAL, "shear modulus field must be positive");
                 b.mu_field = dalloc<double>(E, "mu field");
-                ck(cudaMemcpy(b.mu_field, d->mu_field, E * sizeof(double), cudaMemcpyHostToDevice), "upload");
+                const std::vector<double> v = b.to_order(d->mu_field);
+                ck(cudaMemcpy(b.mu_field, v.data(), E * sizeof(double), cudaMemcpyHostToDevice), "upload");
             }
             if (d->kappa_field && E > 0) {
                 for (int64_t e = 0; e < E; ++e)
                     if (!(d->kappa_field[e] > 0.0)) fail(AM_EINVAL, "bulk modulus field must be positive");
                 b.kappa_field = dalloc<double>(E, "kappa field");
-                ck(cudaMemcpy(b.kappa_field, d->kappa_field, E * sizeof(double), cudaMemcpyHostToDevice), "upload");
+                const std::vector<double> v = b.to_order(d->kappa_field);
+                ck(cudaMemcpy(b.kappa_field, v.data(), E * sizeof(double), cudaMemcpyHostToDevice), "upload");
             }
         } catch (...) {
             b.release();
@@ -1138,7 +1220,8 @@ int am_set_block_fields(am_ctx* ctx, int32_t block_id, const double* mu_field, c
             for (int64_t e = 0; e < E; ++e)
                 if (!(src[e] > 0.0)) fail(AM_EINVAL, std::string(what) + " field must be positive");
             if (!dst) dst = dalloc<double>(E, what);
-            ck(cudaMemcpyAsync(dst, src, E * sizeof(double), cudaMemcpyHostToDevice, ctx->stream), "field upload");
+            const std::vector<double> v = b.to_order(src);
+            ck(cudaMemcpyAsync(dst, v.data(), E * sizeof(double), cudaMemcpyHostToDevice, ctx->stream), "field upload");
             ck(cudaStreamSynchronize(ctx->stream), "synchronize");
         };
         upload(mu_field, b.mu_field, "shear modulus");
@@ -1453,6 +1536,12 @@ int am_vjp_force(am_ctx* ctx, am_memory where, const double* u, const double* la
             ck(cudaMemcpyAsync(gu, out, ctx->N * 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
             if (gmu) ck(cudaMemcpyAsync(gmu, gm, E * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
             if (gkappa) ck(cudaMemcpyAsync(gkappa, gk, E * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+            ck(cudaStreamSynchronize(ctx->stream), "synchronize");
+            ctx->elems_to_caller_host(gmu);
+            ctx->elems_to_caller_host(gkappa);
+        } else {
+            ctx->elems_to_caller_device(gm);
+            ctx->elems_to_caller_device(gk);
         }
         ck(cudaStreamSynchronize(ctx->stream), "synchronize");
     });
@@ -1570,6 +1659,8 @@ int am_adjoint(am_ctx* ctx, int64_t nsteps, double dt, int32_t ckpt_every, int32
         if (gmu) ck(cudaMemcpyAsync(gmu, gm, E * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
         if (gkappa) ck(cudaMemcpyAsync(gkappa, gk, E * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
         ctx->check_status();
+        ctx->elems_to_caller_host(gmu);
+        ctx->elems_to_caller_host(gkappa);
     });
 }
 
@@ -1657,6 +1748,31 @@ int am_complete_properties(double props[5], char* msg, int msg_len) {
     } catch (const std::exception& e) {
         if (msg && msg_len > 0) std::snprintf(msg, static_cast<size_t>(msg_len), "%s", e.what());
         return AM_EINVAL;
+    }
+}
+
+int am_element_order(int64_t num_nodes, const double* coords, int64_t num_elems, int32_t nodes_per_elem,
+                     const int32_t* conn, int32_t try_rings, int32_t* order, int32_t* rings) {
+    am::set_free_error("");
+    if (num_nodes <= 0 || !coords || num_elems < 0 || (nodes_per_elem != 4 && nodes_per_elem != 8) ||
+        (num_elems > 0 && (!conn || !order))) {
+        am::set_free_error("am_element_order: bad arguments");
+        return AM_EINVAL;
+    }
+    try {
+        for (int64_t s = 0; s < num_elems * nodes_per_elem; ++s)
+            if (conn[s] < 0 || conn[s] >= num_nodes) {
+                am::set_free_error("am_element_order: connectivity index out of range");
+                return AM_EINVAL;
+            }
+        const std::vector<double> X(coords, coords + 3 * num_nodes);
+        am::ElementOrder eo = am::element_order(conn, num_elems, nodes_per_elem, X, try_rings != 0);
+        std::copy(eo.order.begin(), eo.order.end(), order);
+        if (rings) *rings = eo.rings ? 1 : 0;
+        return AM_OK;
+    } catch (const std::bad_alloc&) {
+        am::set_free_error("am_element_order: host allocation failed");
+        return AM_ENOMEM;
     }
 }
 

@@ -829,8 +829,13 @@ __global__ void __launch_bounds__(256) k_cell_force_thread(CellBlockDev b, const
 template <typename T, int MAT, int LPC>
 __global__ void __launch_bounds__(256) k_cell_force_group(CellBlockDev b, const double4* __restrict__ U4,
                                                           vec4_t<T>* __restrict__ slots, int* status) {
-    pdl_trigger();
-    pdl_wait();
+    // Entries go in rounds of kCellBatch per lane: a round's node ids and gradients (set-up
+    // data) are loaded a round ahead, and its displacement gathers are all issued before
+    // the first is used, so a lane has kCellBatch gathers in flight instead of one
+    // dependent id -> displacement chain per entry. The first round's ids and gradients
+    // load before the wait for the kernel that writes the displacements. Each lane still
+    // sums its entries in ascending order.
+    constexpr int kCellBatch = 4;
     const int64_t gt = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const int64_t c = gt / LPC;
     const int r = static_cast<int>(threadIdx.x % LPC);
@@ -839,18 +844,52 @@ __global__ void __launch_bounds__(256) k_cell_force_group(CellBlockDev b, const 
     const int32_t s0 = valid ? b.ptr[c] : 0, s1 = valid ? b.ptr[c + 1] : 0;
     const T* gr = cell_grads<T>(b);
     const bool diff = sizeof(T) == 4;
-    const double4 ur = s1 > s0 ? ld_dep(U4 + b.nodes[s0]) : make_double4(0.0, 0.0, 0.0, 0.0);
+    int32_t nid[kCellBatch];
+    T gg[kCellBatch][3];
+#pragma unroll
+    for (int k = 0; k < kCellBatch; ++k) {
+        const int32_t s = s0 + r + k * LPC;
+        nid[k] = s < s1 ? b.nodes[s] : 0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) gg[k][i] = s < s1 ? gr[3 * s + i] : T(0);
+    }
+    const int32_t n_ref = s1 > s0 ? b.nodes[s0] : 0;
+    pdl_trigger();
+    pdl_wait();
+    const double4 ur = s1 > s0 ? ld_dep(U4 + n_ref) : make_double4(0.0, 0.0, 0.0, 0.0);
     T H[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) H[k] = T(0);
-    for (int32_t s = s0 + r; s < s1; s += LPC) {
-        const double4 u = ld_dep(U4 + b.nodes[s]);
-        const T du[3] = {T(diff ? u.x - ur.x : u.x), T(diff ? u.y - ur.y : u.y), T(diff ? u.z - ur.z : u.z)};
-        const T gg[3] = {gr[3 * s], gr[3 * s + 1], gr[3 * s + 2]};
+    for (int32_t base = s0 + r; base < s1; base += kCellBatch * LPC) {
+        double4 u[kCellBatch];
 #pragma unroll
-        for (int i = 0; i < 3; ++i)
+        for (int k = 0; k < kCellBatch; ++k)
+            if (base + k * LPC < s1) u[k] = ld_dep(U4 + nid[k]);
+        int32_t nid2[kCellBatch];
+        T gg2[kCellBatch][3];
 #pragma unroll
-            for (int j = 0; j < 3; ++j) H[i * 3 + j] += du[i] * gg[j];
+        for (int k = 0; k < kCellBatch; ++k) {
+            const int32_t s = base + (kCellBatch + k) * LPC;
+            nid2[k] = s < s1 ? b.nodes[s] : 0;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) gg2[k][i] = s < s1 ? gr[3 * s + i] : T(0);
+        }
+#pragma unroll
+        for (int k = 0; k < kCellBatch; ++k)
+            if (base + k * LPC < s1) {
+                const T du[3] = {T(diff ? u[k].x - ur.x : u[k].x), T(diff ? u[k].y - ur.y : u[k].y),
+                                 T(diff ? u[k].z - ur.z : u[k].z)};
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) H[i * 3 + j] += du[i] * gg[k][j];
+            }
+#pragma unroll
+        for (int k = 0; k < kCellBatch; ++k) {
+            nid[k] = nid2[k];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) gg[k][i] = gg2[k][i];
+        }
     }
     // Butterfly over the group: fixed pairing, identical result on every lane.
 #pragma unroll
@@ -864,12 +903,25 @@ __global__ void __launch_bounds__(256) k_cell_force_group(CellBlockDev b, const 
     const double Jf = stress<T>(MAT, T(lam), T(mu), H, P);
     if (r == 0 && MAT == kNeoHookean && !(Jf > 0.0)) flag(status, AM_ENONPOS_J, c);
     const T V = T(b.volumes[c]);
-    for (int32_t s = s0 + r; s < s1; s += LPC) {
-        const T gg[3] = {gr[3 * s], gr[3 * s + 1], gr[3 * s + 2]};
-        T f[3];
+    for (int32_t base = s0 + r; base < s1; base += kCellBatch * LPC) {
+        T g[kCellBatch][3];
+        int32_t pos[kCellBatch];
 #pragma unroll
-        for (int i = 0; i < 3; ++i) f[i] = (gg[0] * P[i * 3 + 0] + gg[1] * P[i * 3 + 1] + gg[2] * P[i * 3 + 2]) * -V;
-        slots[b.slot_pos[s]] = make4(f[0], f[1], f[2]);
+        for (int k = 0; k < kCellBatch; ++k) {
+            const int32_t s = base + k * LPC;
+            pos[k] = s < s1 ? b.slot_pos[s] : -1;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) g[k][i] = s < s1 ? gr[3 * s + i] : T(0);
+        }
+#pragma unroll
+        for (int k = 0; k < kCellBatch; ++k)
+            if (pos[k] >= 0) {
+                T f[3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    f[i] = (g[k][0] * P[i * 3 + 0] + g[k][1] * P[i * 3 + 1] + g[k][2] * P[i * 3 + 2]) * -V;
+                slots[pos[k]] = make4(f[0], f[1], f[2]);
+            }
     }
 }
 
@@ -2177,6 +2229,12 @@ __global__ void k_unpack4(const double4* __restrict__ in, double* __restrict__ o
     out[3 * i + 1] = v.y;
     out[3 * i + 2] = v.z;
 }
+__global__ void k_scatter_elems(const int32_t* __restrict__ order, int64_t n, const double* __restrict__ src,
+                                double* __restrict__ dst) {
+    const int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k < n) dst[order[k]] = src[k];
+}
+
 __global__ void k_zero4(double4* __restrict__ out, int64_t n) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i < n) out[i] = make_double4(0.0, 0.0, 0.0, 0.0);
@@ -2639,6 +2697,10 @@ void launch_stress_batch(int32_t mat, double lambda, double mu, int64_t n, const
 void launch_quadrature_batch(int32_t kind, int32_t smoothed, int64_t n, const double* X, double* B, double* w,
                              cudaStream_t s) {
     if (n > 0) k_quadrature_batch<<<grid_for(n, 64), 64, 0, s>>>(kind, smoothed, n, X, B, w);
+}
+
+void launch_scatter_elems(const int32_t* order, int64_t n, const double* src, double* dst, cudaStream_t s) {
+    if (n > 0) k_scatter_elems<<<grid_for(n, 256), 256, 0, s>>>(order, n, src, dst);
 }
 
 }  // namespace am

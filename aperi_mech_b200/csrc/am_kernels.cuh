@@ -187,4 +187,7 @@ void launch_stress_batch(int32_t mat, double lambda, double mu, int64_t n, const
 void launch_quadrature_batch(int32_t kind, int32_t smoothed, int64_t n, const double* X, double* B, double* w,
                              cudaStream_t s);
 
+// dst[order[k]] = src[k] for k < n (per-element results back into the caller's order).
+void launch_scatter_elems(const int32_t* order, int64_t n, const double* src, double* dst, cudaStream_t s);
+
 }  // namespace am

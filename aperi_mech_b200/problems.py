@@ -236,3 +236,32 @@ def tet4_nh_shear_slab(n: int = 70, rank: int = 0, world: int = 1, seed: int = 0
             "slab_mass": mesh.lumped_mass(coords, conn, mat.density)}
     return Problem(f"tet4_nh_shear_{n}_slab{rank}of{world}", coords, [Part("tet4", mat, conn=conn)],
                    [BoundaryCondition.fixed(fixed)], v0, dt, nsteps, seed, meta)
+
+
+def renumbered(p: Problem, seed: int = 1) -> tuple[Problem, np.ndarray, list]:
+    """The same workload with its nodes and its elements renumbered at random (seeded):
+    an unstructured mesh's numbering carries no locality. Returns the problem, pn (new
+    node k is old node pn[k]) and per part pe (new element k of the part is old element
+    pe[k]). Gauss parts only."""
+    rng = np.random.default_rng(seed)
+    pn = rng.permutation(p.num_nodes)
+    inv = np.empty_like(pn)
+    inv[pn] = np.arange(pn.size)
+    parts, pes = [], []
+    for q in p.parts:
+        if q.kind == "cells":
+            raise ValueError("renumbered() takes Gauss parts only")
+        pe = rng.permutation(q.num_elems)
+        pes.append(pe)
+        parts.append(Part(q.kind, q.material, conn=inv[q.conn[pe]].astype(np.int32),
+                          mu_field=None if q.mu_field is None else q.mu_field[pe],
+                          kappa_field=None if q.kappa_field is None else q.kappa_field[pe], name=q.name))
+    bcs = [BoundaryCondition(nodes=np.sort(inv[b.nodes]).astype(np.int32), values=b.values,
+                             component_mask=b.component_mask, kind=b.kind, time_function=b.time_function,
+                             abscissa=b.abscissa, ordinate=b.ordinate, active_range=b.active_range) for b in p.bcs]
+    meta = dict(p.meta)
+    if "sensors" in meta:
+        meta["sensors"] = inv[meta["sensors"]].astype(np.int32)
+    meta["config"] = f"{p.meta.get('config')}, nodes and elements renumbered at random (seed {seed})"
+    return (Problem(f"{p.name}_renumbered", p.coords[pn].copy(), parts, bcs, p.v0[pn].copy(), p.dt, p.nsteps, p.seed,
+                    meta), pn, pes)

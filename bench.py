@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--fbar-n", type=int, default=32, help="lattice cells per unit length of the F-bar RKPM box")
     ap.add_argument("--workload", default="tet4_nh_shear",
                     choices=["tet4_nh_shear", "hex8_nh_lognormal", "hex8_le_cube", "smoothed_tet4_box", "rkpm_box",
-                             "rkpm_fbar_box", "rkpm_two_pass_box"],
+                             "rkpm_fbar_box", "rkpm_two_pass_box", "tet4_nh_shear_renumbered"],
                     help="workload of the headline timing (the default is the headline configuration; the others "
                          "exist to profile one kernel at a time)")
     ap.add_argument("--skip-extras", action="store_true")
@@ -531,6 +531,8 @@ def make_problem(args, rank=0, world=1):
         return problems.rkpm_fbar_box(n=args.fbar_n, seed=0, nsteps=args.steps)
     if w == "rkpm_two_pass_box":
         return problems.rkpm_two_pass_box(n=args.box_n, seed=0, nsteps=args.steps)
+    if w == "tet4_nh_shear_renumbered":
+        return problems.renumbered(problems.tet4_nh_shear(n=args.n, seed=0, nsteps=args.steps), seed=1)[0]
     return problems.rkpm_box(n=args.box_n, seed=0, nsteps=args.steps)
 
 
@@ -624,6 +626,24 @@ def run_ours(args, rank, world, local):
         r = measure_workload(torch, p3d, 500, args.warmup, stream, dev, world, mass=p3d.meta["mass"], fma=fma)
         r["setup_s"] = setup_s
         extras["rkpm_two_pass_box"] = r
+        # The headline mesh renumbered at random (an unstructured mesh's numbering): with the
+        # split-hex rings found by topology, with generic patches only, and one thread per tet.
+        pr, _, _ = problems.renumbered(problems.tet4_nh_shear(n=args.n, seed=0, nsteps=args.steps), seed=1)
+        for label, patches in (("split_hex", None), ("generic_patches", "1"), ("per_tet", "0")):
+            old_env = os.environ.get("APERI_B200_TET4_PATCHES")
+            if patches is not None:
+                os.environ["APERI_B200_TET4_PATCHES"] = patches
+            try:
+                r = measure_workload(torch, pr, args.steps, args.warmup, stream, dev, world, fma=fma)
+            finally:
+                if old_env is None:
+                    os.environ.pop("APERI_B200_TET4_PATCHES", None)
+                else:
+                    os.environ["APERI_B200_TET4_PATCHES"] = old_env
+            r["kernel_path"] = label
+            r["vs_structured_mixed"] = r["mixed"]["value"] / res["mixed"]["value"]
+            r["vs_structured_fp64"] = r["fp64"]["value"] / res["fp64"]["value"]
+            extras[f"tet4_nh_shear_renumbered_{label}"] = r
         p5 = problems.hex8_nh_lognormal(n=args.hex_n, seed=0, nsteps=1000, bulk_field=True)
         extras["hex8_nh_lognormal_large"] = measure_workload(torch, p5, 1000, args.warmup, stream, dev, world, fma=fma)
         if not args.skip_adjoint:

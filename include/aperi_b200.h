@@ -205,6 +205,15 @@ int am_rkpm_element_cells(int64_t num_nodes, const double* coords, int64_t num_t
  * mass rho V / 8 to the vertices scattered through the functions. */
 int am_rkpm_hex8_element_cells(int64_t num_nodes, const double* coords, int64_t num_hexes, const int32_t* hexes,
                                const double* kernel_radius, int32_t max_neighbors, double density, am_cells** out);
+/* Finite-element strain smoothing with element cells (element_smoothing_cell with
+ * finite_element, subdomains 1; ElementSmoothedTetrahedron4, include/Element.h:45-47):
+ * one cell per Tet4 or Hex8 element holding its own nodes, with the smoothed gradients
+ * of QuadratureSmoothed.h:32-63 (Tet4) / :97-142 (Hex8) and the element volume, and the
+ * lumped mass rho V / nodes_per_elem to the vertices (src/MassUtils.cpp:17-46). Host
+ * only. Read it with am_cells_sizes / am_cells_get, add it with am_add_block
+ * (AM_SMOOTHED_CELLS) and pass the mass to am_set_mass. */
+int am_smoothed_element_cells(int64_t num_nodes, const double* coords, int64_t num_elems, int32_t nodes_per_elem,
+                              const int32_t* conn, double density, am_cells** out);
 int am_cells_sizes(const am_cells* cells, int64_t* num_cells, int64_t* num_entries, int64_t* num_points,
                    int64_t* num_nbr_entries);
 /* cell_ptr (num_cells+1), cell_nodes/cell_grads (entries, x3), cell_volumes (num_cells)
@@ -258,6 +267,20 @@ int am_noalloc_status(void* cuda_stream, int32_t* status, int64_t* index);
  * the undefined ones; exactly two must be defined. Fills the rest, checks the physical
  * bounds; on failure returns AM_EINVAL and writes the reason to msg. Host only. */
 int am_complete_properties(double props[5], char* msg, int msg_len);
+
+/* The order in which the library runs a Gauss block's elements (no counterpart in the
+ * reference, whose Kokkos loops run elements in mesh order). Host only. order[k] = the
+ * caller's index of the k-th element run. Chosen from the mesh alone, so every
+ * numbering of one mesh gets the same order (and bitwise the same results): with
+ * try_rings, Tet4 blocks whose tets all lie on six-tet rings around an edge (a tet
+ * (c0, a, b, c3) on the ring of the tets sharing its first and last node, as in the
+ * six-tet split of a hex) run ring by ring in the Morton order of the ring axes, each
+ * ring in its chain order (*rings = 1: the split-hex patches); otherwise the elements
+ * run in the Morton order of their centroids (*rings = 0). am_add_block applies it
+ * unless APERI_B200_ELEMENT_ORDER=input; per-element inputs and outputs of the ABI stay
+ * in the caller's order. */
+int am_element_order(int64_t num_nodes, const double* coords, int64_t num_elems, int32_t nodes_per_elem,
+                     const int32_t* conn, int32_t try_rings, int32_t* order, int32_t* rings);
 
 /* ---- diagnostics ---- */
 const char* am_last_error(const am_ctx* ctx);

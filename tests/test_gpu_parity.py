@@ -191,7 +191,7 @@ def test_element_cells_grouped_as_split_hexes(gpu, oracle_lib, monkeypatch, mate
     zero = np.zeros_like(coords)
     want_s = op.steps(zero, v0, op.init_acceleration(zero), np.full(30, dt))
     slots = {}
-    for patches in ("1", "0"):
+    for patches in ("2", "0"):  # split-hex grouping (the default), and no grouping
         monkeypatch.setenv("APERI_B200_TET4_PATCHES", patches)
         with ExplicitDynamics(coords, [part], bcs, mass=mass) as m:
             slots[patches] = m.layout()["used_slots"]
@@ -204,7 +204,7 @@ def test_element_cells_grouped_as_split_hexes(gpu, oracle_lib, monkeypatch, mate
             m.run(30, dt)
             for g, w in zip(m.get_state(), want_s):
                 assert rel_err(g, w) < FP64_TOL
-    assert 3 * slots["1"] == slots["0"] == 4 * conn.shape[0]
+    assert 3 * slots["2"] == slots["0"] == 4 * conn.shape[0]
 
 
 # ---- time integration ----------------------------------------------------------------
