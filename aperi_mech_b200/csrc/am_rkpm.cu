@@ -210,6 +210,30 @@ void hex_smoothed(const double* X, double* B, double* vol) {
     *vol = V;
 }
 
+// Tet4 smoothed quadrature (QuadratureSmoothed.h:32-63): the four faces' area normals,
+// each shared equally by its three nodes, over the volume from the divergence theorem.
+// For a tet these are the exact gradients of the linear shape functions.
+void tet_smoothed(const double* X, double* B, double* vol) {
+    static const int faces[4][3] = {{0, 1, 3}, {1, 2, 3}, {0, 3, 2}, {0, 2, 1}};
+    for (int k = 0; k < 12; ++k) B[k] = 0.0;
+    double V = 0.0;
+    for (int f = 0; f < 4; ++f) {
+        const double* p0 = X + 3 * faces[f][0];
+        const double* p1 = X + 3 * faces[f][1];
+        const double* p2 = X + 3 * faces[f][2];
+        const double e1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+        const double e2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
+        const double n[3] = {(e1[1] * e2[2] - e1[2] * e2[1]) / 2.0, (e1[2] * e2[0] - e1[0] * e2[2]) / 2.0,
+                             (e1[0] * e2[1] - e1[1] * e2[0]) / 2.0};
+        V += p0[0] * n[0] + p0[1] * n[1] + p0[2] * n[2];
+        for (int l = 0; l < 3; ++l)
+            for (int i = 0; i < 3; ++i) B[faces[f][l] * 3 + i] += n[i] / 3.0;
+    }
+    V /= 3.0;
+    for (int k = 0; k < 12; ++k) B[k] /= V;
+    *vol = V;
+}
+
 // Neighbours of every point of c->points (ball search with the neighbour's kernel
 // radius on a uniform grid of cell size rmax, sorted by the tweaked squared distance,
 // truncated to max_neighbors) and the reproducing-kernel function values there (FP64,
@@ -660,6 +684,63 @@ int am_rkpm_element_cells(int64_t N, const double* X, int64_t T, const int32_t* 
 int am_rkpm_hex8_element_cells(int64_t N, const double* X, int64_t E, const int32_t* hexes, const double* R,
                                int32_t max_neighbors, double density, am_cells** out) {
     return element_cells(8, N, X, E, hexes, R, max_neighbors, density, out);
+}
+
+int am_smoothed_element_cells(int64_t N, const double* X, int64_t E, int32_t nodes_per_elem, const int32_t* conn,
+                              double density, am_cells** out) {
+    am::set_free_error("");
+    if (!out) return AM_EINVAL;
+    *out = nullptr;
+    const int nn = nodes_per_elem;
+    if (N <= 0 || !X || E < 0 || (nn != 4 && nn != 8) || (E > 0 && !conn) || !(density > 0.0)) {
+        am::set_free_error("am_smoothed_element_cells: bad arguments");
+        return AM_EINVAL;
+    }
+    if (E * nn >= (int64_t(1) << 31)) {
+        am::set_free_error("cell entry count beyond int32 indexing");
+        return AM_ERANGE;
+    }
+    try {
+        for (int64_t k = 0; k < E * nn; ++k)
+            if (conn[k] < 0 || conn[k] >= N) throw Fail{AM_EINVAL, "connectivity index out of range"};
+        std::unique_ptr<am_cells> hold(new am_cells());
+        am_cells* c = hold.get();
+        c->num_nodes = N;
+        c->cell_ptr.resize(E + 1);
+        for (int64_t e = 0; e <= E; ++e) c->cell_ptr[e] = nn * e;
+        c->cell_nodes.assign(conn, conn + nn * E);
+        c->cell_grads.assign(3 * nn * E, 0.0);
+        c->cell_volumes.assign(E, 0.0);
+        std::atomic<int> bad(0);
+        parallel_for(E, [&](int64_t e) {
+            double x[24], B[24], V = 0.0;
+            for (int k = 0; k < nn; ++k)
+                for (int i = 0; i < 3; ++i) x[3 * k + i] = X[3 * static_cast<int64_t>(conn[nn * e + k]) + i];
+            if (nn == 8)
+                hex_smoothed(x, B, &V);
+            else
+                tet_smoothed(x, B, &V);
+            if (!(V > 0.0)) {
+                bad = 1;
+                return;
+            }
+            std::copy(B, B + 3 * nn, c->cell_grads.begin() + 3 * nn * e);
+            c->cell_volumes[e] = V;
+        });
+        if (bad) throw Fail{AM_ENONPOS_J, "an element has non-positive volume"};
+        // Lumped mass rho V / nn to each vertex, in element order (src/MassUtils.cpp:17-46).
+        c->mass.assign(N, 0.0);
+        for (int64_t e = 0; e < E; ++e)
+            for (int k = 0; k < nn; ++k) c->mass[conn[nn * e + k]] += c->cell_volumes[e] * density / nn;
+        *out = hold.release();
+        return AM_OK;
+    } catch (const Fail& f) {
+        am::set_free_error(f.msg);
+        return f.code;
+    } catch (const std::bad_alloc&) {
+        am::set_free_error("host allocation failed");
+        return AM_ENOMEM;
+    }
 }
 
 int am_cells_sizes(const am_cells* c, int64_t* num_cells, int64_t* num_entries, int64_t* num_points,

@@ -56,3 +56,35 @@ def element_smoothing_part(coords: np.ndarray, conn: np.ndarray, material: Mater
     mass = np.zeros(coords.shape[0])
     np.add.at(mass, conn.reshape(-1), np.repeat(vol * material.density / nn, nn))
     return part, mass
+
+
+def element_smoothing_part_library(coords: np.ndarray, conn: np.ndarray, material: Material, mu_field=None,
+                                   kappa_field=None, name: str = "block_1"):
+    """The same cells and mass from the library's host set-up (am_smoothed_element_cells),
+    the call a C++ host makes without Python."""
+    import ctypes as C
+
+    from . import capi
+    from .capi import check
+
+    lib = capi.load()
+    X = np.ascontiguousarray(coords, dtype=np.float64)
+    T = np.ascontiguousarray(conn, dtype=np.int32)
+    h = C.c_void_p()
+    check(lib.am_smoothed_element_cells(X.shape[0], capi._ptr(X), T.shape[0], T.shape[1], capi._ptr(T, C.c_int32),
+                                        float(material.density), C.byref(h)))
+    try:
+        nc, ne = C.c_int64(), C.c_int64()
+        check(lib.am_cells_sizes(h, C.byref(nc), C.byref(ne), None, None))
+        ptr = np.empty(nc.value + 1, dtype=np.int64)
+        nodes = np.empty(ne.value, dtype=np.int32)
+        grads = np.empty((ne.value, 3))
+        vols = np.empty(nc.value)
+        mass = np.empty(X.shape[0])
+        check(lib.am_cells_get(h, capi._ptr(ptr, C.c_int64), capi._ptr(nodes, C.c_int32), capi._ptr(grads),
+                               capi._ptr(vols), capi._ptr(mass)))
+    finally:
+        lib.am_cells_destroy(h)
+    part = Part("cells", material, cell_ptr=ptr, cell_nodes=nodes, cell_grads=grads, cell_volumes=vols,
+                mu_field=mu_field, kappa_field=kappa_field, name=name)
+    return part, mass
