@@ -38,6 +38,12 @@ class Subdomain:
     num_iface: int            # interface nodes of the whole mesh
     owned: np.ndarray         # per local node: this rank is the lowest rank holding it
     elements: list = field(default_factory=list)  # per part: global element (cell) ids held here
+    # Neighbour exchange: the ranks sharing interface nodes with this one (ascending) and,
+    # per neighbour, the local ids of the shared nodes in ascending global id, the order
+    # both sides of the pair agree on.
+    neighbors: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    shared_ptr: np.ndarray = field(default_factory=lambda: np.zeros(1, np.int64))
+    shared_nodes: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
 
     @property
     def num_nodes(self) -> int:
@@ -130,11 +136,46 @@ def decompose(coords: np.ndarray, parts: list, bcs: list, v0: np.ndarray, world:
                                              time_function=bc.time_function, abscissa=bc.abscissa,
                                              ordinate=bc.ordinate, active_range=bc.active_range))
         il = np.nonzero(iface_index[gnodes] >= 0)[0]
+        nbrs, ptr, shared = [], [0], []
+        for q in range(world):
+            if q == k:
+                continue
+            common = np.nonzero(touch[k] & touch[q])[0]  # ascending global ids
+            if common.size:
+                nbrs.append(q)
+                shared.append(g2l[common])
+                ptr.append(ptr[-1] + common.size)
         subs.append(Subdomain(k, world, gnodes, np.ascontiguousarray(coords[gnodes]), sub_parts, sub_bcs,
                               np.ascontiguousarray(np.asarray(v0)[gnodes]), np.ascontiguousarray(mass[gnodes]),
                               il.astype(np.int32), iface_index[gnodes[il]].astype(np.int32), int(iface_global.size),
-                              owner[gnodes] == k, elems))
+                              owner[gnodes] == k, elems, np.asarray(nbrs, dtype=np.int32),
+                              np.asarray(ptr, dtype=np.int64),
+                              np.concatenate(shared).astype(np.int32) if shared else np.zeros(0, np.int32)))
     return subs
+
+
+def neighbor_sum(sub: Subdomain, own: np.ndarray, received: list) -> np.ndarray:
+    """The interface nodes' summed force after a neighbour exchange, as every holder
+    forms it: own is this rank's partial force (local nodes x 3), received[j] the partial
+    forces neighbour j sent for the nodes it shares with this rank (in the shared order).
+    Each interface node sums its holders' partials in ascending rank order (this rank's
+    own partial at its place), so all holders of a node get the same bits. Returns the
+    local array with the interface rows replaced."""
+    out = np.array(own, dtype=np.float64, copy=True)
+    parts = {}  # local node -> [(rank, partial)]
+    for i in sub.iface_local:
+        parts[int(i)] = [(sub.rank, own[i])]
+    for j, q in enumerate(sub.neighbors):
+        nodes = sub.shared_nodes[sub.shared_ptr[j]:sub.shared_ptr[j + 1]]
+        for t, i in enumerate(nodes):
+            parts[int(i)].append((int(q), received[j][t]))
+    for i, lst in parts.items():
+        lst.sort(key=lambda x: x[0])
+        acc = np.zeros(3)
+        for _, v in lst:
+            acc = acc + v
+        out[i] = acc
+    return out
 
 
 def assemble(subs: list, arrays: list, num_nodes: int) -> np.ndarray:
