@@ -32,7 +32,7 @@ EXPORTED = [
     "am_stable_time_increment", "am_solve_power_method", "am_set_interface", "am_nccl_unique_id",
     "am_set_nccl", "am_set_rk_functions", "am_set_cell_groups", "am_rkpm_nodal_subcells", "am_cells_groups",
     "am_set_formulation", "am_rkpm_hex8_element_cells", "am_noalloc_status",
-    "am_measure_fma_peak", "am_element_order", "am_smoothed_element_cells",
+    "am_measure_fma_peak", "am_element_order", "am_smoothed_element_cells", "am_set_neighbors",
 ]
 
 # Tets per call of am_tet4_internal_force_noalloc (AM_NOALLOC_MAX_TETS in include/aperi_b200.h).
@@ -142,6 +142,7 @@ def load(build_if_missing: bool = False) -> C.CDLL:
         "am_element_order": (C.c_int, [C.c_int64, _dp, C.c_int64, C.c_int32, _ip, C.c_int32, _ip, _ip]),
         "am_smoothed_element_cells": (C.c_int, [C.c_int64, _dp, C.c_int64, C.c_int32, _ip, C.c_double,
                                                 C.POINTER(vp)]),
+        "am_set_neighbors": (C.c_int, [vp, C.c_int32, C.c_int32, _ip, _lp, _ip]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -63,6 +63,10 @@ struct NcclApi {
     ncclResult_t (*all_reduce)(const void*, void*, size_t, ncclDataType_t, ncclRedOp_t, ncclComm_t, cudaStream_t) = nullptr;
     ncclResult_t (*comm_destroy)(ncclComm_t) = nullptr;
     const char* (*error_string)(ncclResult_t) = nullptr;
+    ncclResult_t (*group_start)() = nullptr;
+    ncclResult_t (*group_end)() = nullptr;
+    ncclResult_t (*send)(const void*, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t) = nullptr;
+    ncclResult_t (*recv)(void*, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t) = nullptr;
 };
 
 const NcclApi& nccl() {
@@ -75,6 +79,10 @@ const NcclApi& nccl() {
         a.all_reduce = reinterpret_cast<decltype(a.all_reduce)>(dlsym(a.handle, "ncclAllReduce"));
         a.comm_destroy = reinterpret_cast<decltype(a.comm_destroy)>(dlsym(a.handle, "ncclCommDestroy"));
         a.error_string = reinterpret_cast<decltype(a.error_string)>(dlsym(a.handle, "ncclGetErrorString"));
+        a.group_start = reinterpret_cast<decltype(a.group_start)>(dlsym(a.handle, "ncclGroupStart"));
+        a.group_end = reinterpret_cast<decltype(a.group_end)>(dlsym(a.handle, "ncclGroupEnd"));
+        a.send = reinterpret_cast<decltype(a.send)>(dlsym(a.handle, "ncclSend"));
+        a.recv = reinterpret_cast<decltype(a.recv)>(dlsym(a.handle, "ncclRecv"));
         return a;
     }();
     if (!api.handle || !api.get_unique_id || !api.comm_init_rank || !api.all_reduce || !api.comm_destroy)
@@ -126,6 +134,10 @@ struct Block {
     uint32_t* patch_gather = nullptr;
     float* patch_dx32 = nullptr;
     double* patch_dx64 = nullptr;
+    // Hex8 element groups (see GaussBlockDev)
+    int64_t hex_groups = 0;
+    int32_t* hex_group_ptr = nullptr;
+    uint32_t* hex_group_mask = nullptr;
     const int32_t* slot_pos = nullptr;  // block-local view into the context's position array
     std::vector<int32_t> host_nodes;    // node of each logical slot (-1: unused), for the node CSR
     // Processing order of a Gauss block's elements: order[k] is the caller's index of the
@@ -167,6 +179,9 @@ struct Block {
         g.patch_gather = patch_gather;
         g.patch_dx32 = patch_dx32;
         g.patch_dx64 = patch_dx64;
+        g.num_groups = hex_groups;
+        g.group_ptr = hex_group_ptr;
+        g.group_mask = hex_group_mask;
         g.hstate = hstate;
         g.href = href;
         return g;
@@ -228,6 +243,8 @@ struct Block {
         dfree(patch_dx32);
         dfree(patch_dx64);
         dfree(order_dev);
+        dfree(hex_group_ptr);
+        dfree(hex_group_mask);
         dfree(hstate);
         dfree(href);
         dfree(group_ptr);
@@ -297,6 +314,36 @@ TetPatches build_tet_patches(const int32_t* conn, int64_t E) {
     return tp;
 }
 
+// Hex8 element groups: elements 8g .. 8g+7 form group g; its distinct nodes in order of
+// first appearance are its logical slots, each with the mask of the group's elements that
+// touch it (bits 0-7) and the element-local node there (3 bits per element from bit 8).
+struct HexGroups {
+    std::vector<int32_t> ptr;     // groups + 1
+    std::vector<int32_t> nodes;   // per logical slot
+    std::vector<uint32_t> mask;   // per logical slot
+};
+
+HexGroups build_hex_groups(const int32_t* conn, int64_t E) {
+    HexGroups hg;
+    hg.ptr.push_back(0);
+    for (int64_t g0 = 0; g0 < E; g0 += 8) {
+        const int64_t first = static_cast<int64_t>(hg.nodes.size());
+        for (int l = 0; l < 8 && g0 + l < E; ++l)
+            for (int a = 0; a < 8; ++a) {
+                const int32_t n = conn[8 * (g0 + l) + a];
+                int64_t d = first;
+                while (d < static_cast<int64_t>(hg.nodes.size()) && hg.nodes[d] != n) ++d;
+                if (d == static_cast<int64_t>(hg.nodes.size())) {
+                    hg.nodes.push_back(n);
+                    hg.mask.push_back(0u);
+                }
+                hg.mask[d] |= (1u << l) | (static_cast<uint32_t>(a) << (8 + 3 * l));
+            }
+        hg.ptr.push_back(static_cast<int32_t>(hg.nodes.size()));
+    }
+    return hg;
+}
+
 // True when every patch is exactly one hex's six-tet split in the canonical local
 // order (tet t on local nodes 0, a_t, b_t, 3 with a = 1,2,4,5,6,7 and b = 2,4,5,6,7,1).
 bool hex6_patches(const TetPatches& tp) {
@@ -344,6 +391,9 @@ struct am_ctx {
     // Element processing order of Gauss blocks: the locality order chosen from the mesh
     // (element_order, the default) or, with APERI_B200_ELEMENT_ORDER=input, the caller's.
     bool locality_order = true;
+    // Hex8 element groups of eight (the default; APERI_B200_HEX8_GROUPS=0: one slot per
+    // element node).
+    bool hex8_groups = true;
     std::vector<double> host_X;  // coordinates (N x 3), for the element order at am_add_block
     am::StepParams* table = nullptr;
     int64_t table_cap = 0;
@@ -368,6 +418,23 @@ struct am_ctx {
     int32_t* iface_row_of = nullptr;  // per local node: row or -1
     double* iface_buf = nullptr;      // iface_global x 3
     ncclComm_t comm = nullptr;
+    // Neighbour exchange (am_set_neighbors), in place of the all-rank sum of every row:
+    // the rows are this rank's interface nodes; each neighbour gets the partial forces of
+    // the nodes it shares, and every row sums its holders' partials in ascending rank.
+    int32_t my_rank = -1;
+    std::vector<int32_t> nbr_ranks;
+    std::vector<int64_t> nbr_off;     // per neighbour: offset of its entries (num_nbr + 1)
+    int32_t* nbr_send_rows = nullptr; // per shared entry: its row
+    double* nbr_own = nullptr;        // rows x 3: this rank's partial forces
+    double* nbr_send = nullptr;       // shared entries x 3
+    double* nbr_recv = nullptr;       // shared entries x 3
+    int32_t* comb_ptr = nullptr;      // rows + 1
+    int32_t* comb_idx = nullptr;      // sources in ascending holder rank (row, or rows + entry)
+    // Overlap of the exchange with the interior nodes' update (APERI_B200_EXCHANGE_OVERLAP=0
+    // keeps exchange and update in sequence): a second stream carries the exchange.
+    bool overlap = true;
+    cudaStream_t xstream = nullptr;
+    cudaEvent_t ev_ready = nullptr, ev_done = nullptr;
     // Power method for the stable time increment (am_set_power_method).
     std::vector<double> pm_start;     // N x 3 start vector, scaled by eps l on first use
     double* pm_l = nullptr;           // N: max edge length per node
@@ -485,6 +552,11 @@ struct am_ctx {
     // partial interface forces into their rows, the rows summed over ranks.
     void exchange(int mixed) {
         if (!iface_row_of) return;
+        if (!nbr_ranks.empty()) {
+            exchange_send(mixed);
+            exchange_finish(stream);
+            return;
+        }
         ck(cudaMemsetAsync(iface_buf, 0, static_cast<size_t>(iface_global) * 3 * sizeof(double), stream), "memset");
         am::NodeDev nd = node_dev();
         am::launch_iface_gather(nd, mixed, slots(mixed), iface_local, iface_nodes, iface_rows, iface_buf, stream);
@@ -494,6 +566,32 @@ struct am_ctx {
             nccl_check(nccl().all_reduce(iface_buf, iface_buf, static_cast<size_t>(iface_global) * 3, ncclDouble, ncclSum,
                                          comm, stream),
                        "interface all-reduce");
+    }
+
+    // Neighbour exchange, first half (context stream): this rank's partial forces of its
+    // interface nodes into their rows, then into the per-neighbour send buffer.
+    void exchange_send(int mixed) {
+        am::NodeDev nd = node_dev();
+        am::launch_iface_gather(nd, mixed, slots(mixed), iface_local, iface_nodes, iface_rows, nbr_own, stream);
+        am::launch_iface_pack(nbr_off.back(), nbr_send_rows, nbr_own, nbr_send, stream);
+        launches += 2;
+        check_launch("interface gather kernels");
+    }
+    // Second half, on stream s: the grouped sends and receives with each neighbour, then
+    // every row's sum in ascending holder rank into the rows the node kernels read.
+    void exchange_finish(cudaStream_t s) {
+        if (!comm) fail(AM_ESTATE, "the neighbour exchange needs am_set_nccl");
+        const NcclApi& a = nccl();
+        nccl_check(a.group_start(), "ncclGroupStart");
+        for (size_t j = 0; j < nbr_ranks.size(); ++j) {
+            const size_t n = static_cast<size_t>(nbr_off[j + 1] - nbr_off[j]) * 3;
+            nccl_check(a.send(nbr_send + 3 * nbr_off[j], n, ncclDouble, nbr_ranks[j], comm, s), "ncclSend");
+            nccl_check(a.recv(nbr_recv + 3 * nbr_off[j], n, ncclDouble, nbr_ranks[j], comm, s), "ncclRecv");
+        }
+        nccl_check(a.group_end(), "ncclGroupEnd");
+        am::launch_iface_combine(iface_local, comb_ptr, comb_idx, iface_local, nbr_own, nbr_recv, iface_buf, s);
+        ++launches;
+        check_launch("interface combine kernel");
     }
 
     // PowerMethodProcessor::ComputeStableTimeIncrement (include/PowerMethodProcessor.h:331-480)
@@ -740,18 +838,40 @@ struct am_ctx {
         ++launches;
         check_launch("prologue kernel");
         mark(1, 1);
+        const bool split = !nbr_ranks.empty() && overlap && comm && xstream;
         for (int64_t n = n0; n < n1; ++n) {
             element_forces(mixed, U4);
             mark(0, static_cast<int64_t>(blocks.size()));
-            if (iface_row_of) {
-                exchange(mixed);
-                mark(4, 1);
-            }
             const int advance = (n + 1 < n1) ? 1 : 0;
             double4* uc = (u_hist && advance) ? u_hist[n + 1 - n0] : nullptr;
             if (lagr) {
                 ++lagr_steps;
                 lagr_rebased = false;
+            }
+            if (split) {
+                // The exchange runs on the second stream while the interior nodes update on
+                // the context stream; the interface nodes update once it has landed.
+                exchange_send(mixed);
+                ck(cudaEventRecord(ev_ready, stream), "event record");
+                ck(cudaStreamWaitEvent(xstream, ev_ready, 0), "stream wait");
+                exchange_finish(xstream);
+                ck(cudaEventRecord(ev_done, xstream), "event record");
+                am::NodeDev interior = nd;
+                interior.skip_iface = 1;
+                am::launch_node_step(interior, mixed, s, table, n, advance, U4, V4, A4, uc, status, stream, 0);
+                ck(cudaStreamWaitEvent(stream, ev_done, 0), "stream wait");
+                am::NodeDev rim = nd;
+                rim.subset_nodes = iface_nodes;
+                rim.subset_count = iface_local;
+                am::launch_node_step(rim, mixed, s, table, n, advance, U4, V4, A4, uc, status, stream, 0);
+                launches += 2;
+                check_launch("node step kernels");
+                mark(1, 2);
+                continue;
+            }
+            if (iface_row_of) {
+                exchange(mixed);
+                mark(4, 1);
             }
             am::launch_node_step(nd, mixed, s, table, n, advance, U4, V4, A4, uc, status, stream,
                                  due(lagr_steps) ? 1 : 0);
@@ -824,6 +944,15 @@ struct am_ctx {
         dfree(iface_rows);
         dfree(iface_row_of);
         dfree(iface_buf);
+        dfree(nbr_send_rows);
+        dfree(nbr_own);
+        dfree(nbr_send);
+        dfree(nbr_recv);
+        dfree(comb_ptr);
+        dfree(comb_idx);
+        if (ev_ready) cudaEventDestroy(ev_ready);
+        if (ev_done) cudaEventDestroy(ev_done);
+        if (xstream) cudaStreamDestroy(xstream);
         if (comm) nccl().comm_destroy(comm);
         comm = nullptr;
         for (auto& pbuf : adj_bufs) dfree(pbuf);
@@ -959,6 +1088,8 @@ int am_create(int64_t num_nodes, const double* coords, am_ctx** out) {
         c->io_scratch = dalloc<double>(N * 3, "io scratch");
         const char* order = std::getenv("APERI_B200_ELEMENT_ORDER");
         c->locality_order = !(order && std::strcmp(order, "input") == 0);
+        const char* groups = std::getenv("APERI_B200_HEX8_GROUPS");
+        c->hex8_groups = !(groups && groups[0] == '0');
         c->host_X.assign(coords, coords + 3 * N);
         std::vector<double4> x(N);
         for (size_t i = 0; i < N; ++i) x[i] = make_double4(coords[3 * i], coords[3 * i + 1], coords[3 * i + 2], 0.0);
@@ -1111,15 +1242,31 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
                     ck(cudaMemcpy(b.conn, conn, S * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
                 }
                 b.host_nodes.assign(conn, conn + S);
+                if (d->kind == AM_HEX8_GAUSS && E > 0 && ctx->hex8_groups && ctx->lagr == 0) {
+                    // Groups of eight consecutive elements (in the locality order a 2x2x2
+                    // block of a structured mesh): one logical slot per distinct node of a
+                    // group, in order of first appearance (element, then node).
+                    HexGroups hg = build_hex_groups(conn, E);
+                    b.hex_groups = static_cast<int64_t>(hg.ptr.size()) - 1;
+                    b.num_entries = hg.ptr.back();
+                    b.hex_group_ptr = dalloc<int32_t>(hg.ptr.size(), "group offsets");
+                    b.hex_group_mask = dalloc<uint32_t>(std::max<size_t>(hg.mask.size(), 1), "group masks");
+                    ck(cudaMemcpy(b.hex_group_ptr, hg.ptr.data(), hg.ptr.size() * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+                    ck(cudaMemcpy(b.hex_group_mask, hg.mask.data(), hg.mask.size() * sizeof(uint32_t), cudaMemcpyHostToDevice), "upload");
+                    b.host_nodes = std::move(hg.nodes);
+                }
                 if (d->kind == AM_TET4_GAUSS && E > 0 && ctx->tet4_patches && ctx->lagr == 0) {
                     // Patch the tets when patches hold 2.5 tets or more on average; fewer
                     // would leave most of the eight lanes per patch idle.
                     TetPatches tp = build_tet_patches(conn, E);
                     const int64_t P = static_cast<int64_t>(tp.used.size());
-                    if (static_cast<double>(E) >= 2.5 * static_cast<double>(P)) {
-                        // Split-hex patches (six tets in the canonical local order) get the
-                        // register-resident kernel; any other patching the generic one.
-                        const bool hex6 = ctx->tet4_patches == 2 && hex6_patches(tp);
+                    // Split-hex patches (six tets in the canonical local order) get the
+                    // register-resident kernel. Other tets run one thread per tet unless
+                    // generic patches are asked for (APERI_B200_TET4_PATCHES=1): on a
+                    // renumbered 70^3 mesh in Morton order (3.9 tets per patch) the generic
+                    // patch kernel took 170 us against 82 us for one thread per tet (mixed).
+                    const bool hex6 = ctx->tet4_patches == 2 && hex6_patches(tp);
+                    if ((hex6 || ctx->tet4_patches == 1) && static_cast<double>(E) >= 2.5 * static_cast<double>(P)) {
                         b.patched = hex6 ? 2 : 1;
                         b.num_patches = P;
                         b.num_entries = 8 * P;
@@ -1825,6 +1972,91 @@ int am_set_interface(am_ctx* ctx, int64_t num_local, const int32_t* local_nodes,
     });
 }
 
+int am_set_neighbors(am_ctx* ctx, int32_t rank, int32_t num_neighbors, const int32_t* neighbor_ranks,
+                     const int64_t* shared_ptr, const int32_t* shared_nodes) {
+    if (!ctx) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        ctx->require_finalized();
+        if (!ctx->mass_from_caller)
+            fail(AM_ESTATE, "a decomposed mesh needs the global lumped mass from am_set_mass before am_finalize");
+        if (ctx->iface_row_of) fail(AM_ESTATE, "interface already set");
+        if (ctx->rk_ptr) fail(AM_ESTATE, "a decomposed mesh with the two-pass coupling is not built");
+        if (ctx->lagr) fail(AM_ESTATE, "a decomposed mesh runs the total formulation");
+        if (rank < 0 || num_neighbors < 1 || !neighbor_ranks || !shared_ptr || !shared_nodes || shared_ptr[0] != 0)
+            fail(AM_EINVAL, "bad neighbour arrays");
+        const int64_t S = shared_ptr[num_neighbors];
+        if (S >= (int64_t(1) << 31)) fail(AM_ERANGE, "shared entries beyond int32 indexing");
+        // Rows: this rank's interface nodes (every node shared with a neighbour), ascending.
+        std::vector<int32_t> row_of(ctx->N, -1), nodes;
+        for (int32_t j = 0; j < num_neighbors; ++j) {
+            if (shared_ptr[j + 1] < shared_ptr[j]) fail(AM_EINVAL, "shared_ptr must not decrease");
+            if (j > 0 && neighbor_ranks[j] <= neighbor_ranks[j - 1]) fail(AM_EINVAL, "neighbour ranks must ascend");
+            for (int64_t k = shared_ptr[j]; k < shared_ptr[j + 1]; ++k) {
+                const int32_t i = shared_nodes[k];
+                if (i < 0 || i >= ctx->N) fail(AM_EINVAL, "shared node out of range");
+                if (row_of[i] < 0) {
+                    row_of[i] = 0;
+                    nodes.push_back(i);
+                }
+            }
+        }
+        std::sort(nodes.begin(), nodes.end());
+        const int64_t R = static_cast<int64_t>(nodes.size());
+        for (int64_t r = 0; r < R; ++r) row_of[nodes[r]] = static_cast<int32_t>(r);
+        // Per row: its sources in ascending holder rank; this rank's own partial (index r)
+        // at its place, a neighbour's entry k as R + k.
+        std::vector<std::vector<std::pair<int32_t, int32_t>>> src(R);
+        std::vector<int32_t> send_rows(S);
+        for (int64_t r = 0; r < R; ++r) src[r].emplace_back(rank, static_cast<int32_t>(r));
+        for (int32_t j = 0; j < num_neighbors; ++j)
+            for (int64_t k = shared_ptr[j]; k < shared_ptr[j + 1]; ++k) {
+                const int32_t r = row_of[shared_nodes[k]];
+                send_rows[k] = r;
+                src[r].emplace_back(neighbor_ranks[j], static_cast<int32_t>(R + k));
+            }
+        std::vector<int32_t> cptr(R + 1, 0), cidx;
+        for (int64_t r = 0; r < R; ++r) {
+            std::stable_sort(src[r].begin(), src[r].end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+            for (const auto& e : src[r]) cidx.push_back(e.second);
+            cptr[r + 1] = static_cast<int32_t>(cidx.size());
+        }
+        std::vector<int32_t> rows(R);
+        for (int64_t r = 0; r < R; ++r) rows[r] = static_cast<int32_t>(r);
+        ctx->my_rank = rank;
+        ctx->nbr_ranks.assign(neighbor_ranks, neighbor_ranks + num_neighbors);
+        ctx->nbr_off.assign(shared_ptr, shared_ptr + num_neighbors + 1);
+        ctx->iface_local = R;
+        ctx->iface_global = R;
+        ctx->iface_row_of = dalloc<int32_t>(ctx->N, "interface rows");
+        ck(cudaMemcpy(ctx->iface_row_of, row_of.data(), ctx->N * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+        const size_t R1 = static_cast<size_t>(std::max<int64_t>(R, 1)), S1 = static_cast<size_t>(std::max<int64_t>(S, 1));
+        ctx->iface_buf = dalloc<double>(R1 * 3, "interface buffer");
+        ctx->nbr_own = dalloc<double>(R1 * 3, "interface partials");
+        ctx->nbr_send = dalloc<double>(S1 * 3, "send buffer");
+        ctx->nbr_recv = dalloc<double>(S1 * 3, "receive buffer");
+        ctx->nbr_send_rows = dalloc<int32_t>(S1, "send rows");
+        ctx->comb_ptr = dalloc<int32_t>(R + 1, "combine offsets");
+        ctx->comb_idx = dalloc<int32_t>(std::max<size_t>(cidx.size(), 1), "combine sources");
+        ctx->iface_nodes = dalloc<int32_t>(R1, "interface nodes");
+        ctx->iface_rows = dalloc<int32_t>(R1, "interface rows");
+        if (S > 0) ck(cudaMemcpy(ctx->nbr_send_rows, send_rows.data(), S * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+        ck(cudaMemcpy(ctx->comb_ptr, cptr.data(), (R + 1) * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+        if (!cidx.empty())
+            ck(cudaMemcpy(ctx->comb_idx, cidx.data(), cidx.size() * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+        if (R > 0) {
+            ck(cudaMemcpy(ctx->iface_nodes, nodes.data(), R * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+            ck(cudaMemcpy(ctx->iface_rows, rows.data(), R * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+        }
+        const char* ov = std::getenv("APERI_B200_EXCHANGE_OVERLAP");
+        ctx->overlap = !(ov && ov[0] == '0');
+        if (ctx->overlap) {
+            ck(cudaStreamCreateWithFlags(&ctx->xstream, cudaStreamNonBlocking), "stream create");
+            ck(cudaEventCreateWithFlags(&ctx->ev_ready, cudaEventDisableTiming), "event create");
+            ck(cudaEventCreateWithFlags(&ctx->ev_done, cudaEventDisableTiming), "event create");
+        }
+    });
+}
+
 int am_set_formulation(am_ctx* ctx, int32_t formulation, int32_t update_interval) {
     if (!ctx) return AM_EINVAL;
     return guarded(ctx, [&] {
@@ -1909,7 +2141,14 @@ int am_set_nccl(am_ctx* ctx, const unsigned char id[128], int32_t rank, int32_t 
     if (!ctx) return AM_EINVAL;
     return guarded(ctx, [&] {
         if (!id || nranks < 1 || rank < 0 || rank >= nranks) fail(AM_EINVAL, "bad NCCL rank or id");
-        if (!ctx->iface_row_of) fail(AM_ESTATE, "am_set_interface first");
+        if (!ctx->iface_row_of) fail(AM_ESTATE, "am_set_interface or am_set_neighbors first");
+        if (!ctx->nbr_ranks.empty()) {
+            if (rank != ctx->my_rank) fail(AM_EINVAL, "rank differs from the one given to am_set_neighbors");
+            for (int32_t q : ctx->nbr_ranks)
+                if (q >= nranks) fail(AM_EINVAL, "neighbour rank beyond the communicator");
+            if (!nccl().group_start || !nccl().group_end || !nccl().send || !nccl().recv)
+                fail(AM_ESTATE, "libnccl.so.2 lacks the point-to-point calls");
+        }
         if (ctx->comm) fail(AM_ESTATE, "communicator already set");
         ncclUniqueId u;
         std::memcpy(&u, id, sizeof(u));

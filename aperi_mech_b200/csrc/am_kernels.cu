@@ -13,6 +13,7 @@
 // accumulates nodal forces and the state in FP64.
 #include <cuda_runtime.h>
 #include <math_constants.h>
+#include <stdlib.h>
 
 #include "am_kernels.cuh"
 #include "am_math.cuh"
@@ -522,6 +523,45 @@ __device__ __forceinline__ void hex_conn(const GaussBlockDev& b, int64_t e, int3
     nd[0] = c0.x, nd[1] = c0.y, nd[2] = c0.z, nd[3] = c0.w, nd[4] = c1.x, nd[5] = c1.y, nd[6] = c1.z, nd[7] = c1.w;
 }
 
+// Hex8 element groups (GaussBlockDev::num_groups > 0): the elements run in a locality
+// order, and the eight elements of a group sit on lanes 8k .. 8k+7 of one warp. Each
+// element leaves its eight nodal vectors in shared memory (hex_group_put); the group's
+// lanes then write one slot per distinct node of the group, the sum over the elements
+// touching it in ascending element order (hex_group_write). A 2x2x2 block of hexes
+// writes 27 slots instead of 64, which the node kernel then reads. Lanes past the last
+// element compute a copy of it and write nothing, so every lane reaches the warp sync.
+constexpr int kHexGroupStride = 25;  // 24 values per element, padded: odd stride, no bank conflicts
+
+template <typename T>
+__device__ __forceinline__ void hex_group_put(T* sm, int a, T x, T y, T z) {
+    T* p = sm + threadIdx.x * kHexGroupStride + 3 * a;
+    p[0] = x;
+    p[1] = y;
+    p[2] = z;
+}
+
+template <typename T, typename S>
+__device__ __forceinline__ void hex_group_write(const GaussBlockDev& b, int64_t e, const T* sm, S* slots) {
+    __syncwarp();
+    const int64_t g = e >> 3;
+    if (g >= b.num_groups) return;
+    const int r = static_cast<int>(threadIdx.x & 7);
+    const T* base = sm + (threadIdx.x & ~7u) * kHexGroupStride;
+    const int32_t d1 = b.group_ptr[g + 1];
+    for (int32_t d = b.group_ptr[g] + r; d < d1; d += 8) {
+        const uint32_t m = b.group_mask[d];
+        T x = T(0), y = T(0), z = T(0);
+        for (uint32_t lm = m & 0xFFu; lm; lm &= lm - 1) {
+            const int l = __ffs(lm) - 1;
+            const T* q = base + l * kHexGroupStride + 3 * ((m >> (8 + 3 * l)) & 7u);
+            x += q[0];
+            y += q[1];
+            z += q[2];
+        }
+        slots[b.slot_pos[d]] = make4(x, y, z);
+    }
+}
+
 // The FP32 kernel is held to 128 registers (four 128-thread blocks per SM); the
 // FP64 one keeps its ~250 registers (forcing three blocks per SM spills and was
 // slower on B200) and runs in 64-thread blocks.
@@ -529,8 +569,12 @@ template <typename T, int MAT>
 __global__ void __launch_bounds__(sizeof(T) == 8 ? 64 : 128, sizeof(T) == 8 ? 1 : 4) k_hex8_force(GaussBlockDev b, const double4* __restrict__ X4,
                                                          const double4* __restrict__ U4,
                                                          vec4_t<T>* __restrict__ slots, int* status) {
-    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (e >= b.num_elems) return;
+    constexpr int kBlock = sizeof(T) == 8 ? 64 : 128;
+    __shared__ T sm[kBlock * kHexGroupStride];
+    const int64_t e_thread = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const bool valid = e_thread < b.num_elems;
+    if (!valid && b.num_groups == 0) return;
+    const int64_t e = valid ? e_thread : b.num_elems - 1;
     int32_t nd[8];
     hex_conn(b, e, nd);
     T X[3][8], U[3][8];
@@ -583,9 +627,7 @@ __global__ void __launch_bounds__(sizeof(T) == 8 ? 64 : 128, sizeof(T) == 8 ? 1 
                 Q[k * 3 + i] = A[k * 3 + 0] * P[i * 3 + 0] + A[k * 3 + 1] * P[i * 3 + 1] + A[k * 3 + 2] * P[i * 3 + 2];
         hex_accumulate_r(R, Q, g);
     }
-    if (bad) flag(status, AM_ENONPOS_J, e);
-    const int4 p0 = reinterpret_cast<const int4*>(b.slot_pos)[2 * e], p1 = reinterpret_cast<const int4*>(b.slot_pos)[2 * e + 1];
-    const int32_t pos[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
+    if (bad && valid) flag(status, AM_ENONPOS_J, e);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
         R[i][0] = T(0);
@@ -593,6 +635,14 @@ __global__ void __launch_bounds__(sizeof(T) == 8 ? 64 : 128, sizeof(T) == 8 ? 1 
         hex_butterfly_t(R[i]);
     }
     const T s = T(-1.0 / 512.0);
+    if (b.num_groups > 0) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) hex_group_put(sm, hex_node_of_corner(q), s * R[0][q], s * R[1][q], s * R[2][q]);
+        hex_group_write(b, e_thread, sm, slots);
+        return;
+    }
+    const int4 p0 = reinterpret_cast<const int4*>(b.slot_pos)[2 * e], p1 = reinterpret_cast<const int4*>(b.slot_pos)[2 * e + 1];
+    const int32_t pos[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
 #pragma unroll
     for (int q = 0; q < 8; ++q) slots[pos[hex_node_of_corner(q)]] = make4(s * R[0][q], s * R[1][q], s * R[2][q]);
 }
@@ -826,7 +876,7 @@ __global__ void __launch_bounds__(256) k_cell_force_thread(CellBlockDev b, const
 // holds the same H and P), and each lane writes the forces of its own entries.
 // Narrow groups keep the lanes busy on cells of a few tens of entries and repeat
 // the stress update on fewer lanes.
-template <typename T, int MAT, int LPC>
+template <typename T, int MAT, int LPC, int kCellBatch>
 __global__ void __launch_bounds__(256) k_cell_force_group(CellBlockDev b, const double4* __restrict__ U4,
                                                           vec4_t<T>* __restrict__ slots, int* status) {
     // Entries go in rounds of kCellBatch per lane: a round's node ids and gradients (set-up
@@ -835,7 +885,6 @@ __global__ void __launch_bounds__(256) k_cell_force_group(CellBlockDev b, const 
     // dependent id -> displacement chain per entry. The first round's ids and gradients
     // load before the wait for the kernel that writes the displacements. Each lane still
     // sums its entries in ascending order.
-    constexpr int kCellBatch = 4;
     const int64_t gt = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const int64_t c = gt / LPC;
     const int r = static_cast<int>(threadIdx.x % LPC);
@@ -1495,8 +1544,11 @@ __global__ void __launch_bounds__(64) k_hex8_vjp(GaussBlockDev b, const double4*
                                                        const double4* __restrict__ U4, const double4* __restrict__ L4,
                                                        double4* __restrict__ slots, double* gmu, double* gk,
                                                        int accumulate) {
-    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (e >= b.num_elems) return;
+    __shared__ double sm[64 * kHexGroupStride];
+    const int64_t e_thread = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const bool valid = e_thread < b.num_elems;
+    if (!valid && b.num_groups == 0) return;
+    const int64_t e = valid ? e_thread : b.num_elems - 1;
     int32_t nd[8];
     hex_conn(b, e, nd);
     double X[3][8], U[3][8], W[3][8];
@@ -1553,8 +1605,6 @@ __global__ void __launch_bounds__(64) k_hex8_vjp(GaussBlockDev b, const double4*
                 Q[k * 3 + i] = A[k * 3 + 0] * dP[i * 3 + 0] + A[k * 3 + 1] * dP[i * 3 + 1] + A[k * 3 + 2] * dP[i * 3 + 2];
         hex_accumulate_r(R, Q, g);
     }
-    const int4 p0 = reinterpret_cast<const int4*>(b.slot_pos)[2 * e], p1 = reinterpret_cast<const int4*>(b.slot_pos)[2 * e + 1];
-    const int32_t pos[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
         R[i][0] = 0.0;
@@ -1562,9 +1612,17 @@ __global__ void __launch_bounds__(64) k_hex8_vjp(GaussBlockDev b, const double4*
         hex_butterfly_t(R[i]);
     }
     const double s = -1.0 / 512.0;
+    if (valid) store_theta(gmu, gk, e, tm, tk, accumulate);
+    if (b.num_groups > 0) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) hex_group_put(sm, hex_node_of_corner(q), s * R[0][q], s * R[1][q], s * R[2][q]);
+        hex_group_write(b, e_thread, sm, slots);
+        return;
+    }
+    const int4 p0 = reinterpret_cast<const int4*>(b.slot_pos)[2 * e], p1 = reinterpret_cast<const int4*>(b.slot_pos)[2 * e + 1];
+    const int32_t pos[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
 #pragma unroll
     for (int q = 0; q < 8; ++q) slots[pos[hex_node_of_corner(q)]] = make4(s * R[0][q], s * R[1][q], s * R[2][q]);
-    store_theta(gmu, gk, e, tm, tk, accumulate);
 }
 
 template <int MAT>
@@ -1725,10 +1783,14 @@ __global__ void k_tet4_patch_volume_slots(GaussBlockDev b, double density, const
     }
 }
 
-__global__ void k_gauss_volume_slots(GaussBlockDev b, double density, const double4* __restrict__ X4,
-                                     double4* __restrict__ slots) {
-    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (e >= b.num_elems) return;
+__global__ void __launch_bounds__(128) k_gauss_volume_slots(GaussBlockDev b, double density,
+                                                             const double4* __restrict__ X4,
+                                                             double4* __restrict__ slots) {
+    __shared__ double sm[128 * kHexGroupStride];
+    const int64_t e_thread = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const bool valid = e_thread < b.num_elems;
+    if (!valid && b.num_groups == 0) return;
+    const int64_t e = valid ? e_thread : b.num_elems - 1;
     const int nn = b.kind == AM_HEX8_GAUSS ? 8 : 4;
     double X[24];
     for (int a = 0; a < nn; ++a) {
@@ -1738,6 +1800,11 @@ __global__ void k_gauss_volume_slots(GaussBlockDev b, double density, const doub
         X[a * 3 + 2] = x.z;
     }
     const double me = element_volume(nn, X) * density / nn;
+    if (b.num_groups > 0) {
+        for (int a = 0; a < 8; ++a) hex_group_put(sm, a, me, 0.0, 0.0);
+        hex_group_write(b, e_thread, sm, slots);
+        return;
+    }
     for (int a = 0; a < nn; ++a) slots[b.slot_pos[e * nn + a]] = make_double4(me, 0.0, 0.0, 0.0);
 }
 
@@ -1978,8 +2045,16 @@ __global__ void __launch_bounds__(kNodeBlock) k_node_step(NodeDev nd, const vec4
                                                            int advance, double4* __restrict__ U4,
                                                            double4* __restrict__ V4, double4* __restrict__ A4,
                                                            double4* __restrict__ u_copy, int* status, int rebase) {
-    const int64_t i = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / LPN;
-    const bool own = i < nd.num_nodes;
+    const int64_t t = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / LPN;
+    bool own;
+    int64_t i;
+    if (nd.subset_nodes != nullptr) {
+        own = t < nd.subset_count;
+        i = own ? nd.subset_nodes[t] : 0;
+    } else {
+        i = t;
+        own = t < nd.num_nodes && !(nd.skip_iface && nd.iface_row[t] >= 0);
+    }
     // The node's own data is independent of the gather: issue its loads first (mass,
     // BC word and slot range before the wait for the element kernels, v and u after it).
     const int64_t j = own ? i : 0;
@@ -2235,6 +2310,34 @@ __global__ void k_scatter_elems(const int32_t* __restrict__ order, int64_t n, co
     if (k < n) dst[order[k]] = src[k];
 }
 
+__global__ void k_iface_pack(int64_t n, const int32_t* __restrict__ rows, const double* __restrict__ own,
+                             double* __restrict__ send) {
+    const int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int64_t r = rows[k];
+    send[3 * k] = own[3 * r];
+    send[3 * k + 1] = own[3 * r + 1];
+    send[3 * k + 2] = own[3 * r + 2];
+}
+
+__global__ void k_iface_combine(int64_t rows, const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                                int64_t num_own, const double* __restrict__ own, const double* __restrict__ recv,
+                                double* __restrict__ out) {
+    const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    double x = 0.0, y = 0.0, z = 0.0;
+    for (int32_t e = ptr[r]; e < ptr[r + 1]; ++e) {
+        const int64_t j = idx[e];
+        const double* src = j < num_own ? own + 3 * j : recv + 3 * (j - num_own);
+        x += src[0];
+        y += src[1];
+        z += src[2];
+    }
+    out[3 * r] = x;
+    out[3 * r + 1] = y;
+    out[3 * r + 2] = z;
+}
+
 __global__ void k_zero4(double4* __restrict__ out, int64_t n) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i < n) out[i] = make_double4(0.0, 0.0, 0.0, 0.0);
@@ -2415,9 +2518,26 @@ inline int lanes_per_cell(const CellBlockDev& b) {
     return mean <= 16.0 ? 4 : mean <= 96.0 ? 8 : mean <= 192.0 ? 16 : 32;
 }
 
-#define AM_CELL_GROUP(T, LPC)                                                                         \
-    AM_DISPATCH_MAT(b.material, (launch_pdl(k_cell_force_group<T, M, LPC>, grid_for(b.num_cells * LPC, 256), 256, s, \
+inline int cell_batch() {
+    static const int v = [] {
+        const char* e = getenv("APERI_B200_CELL_BATCH");
+        return e ? atoi(e) : 1;
+    }();
+    return v;
+}
+#define AM_CELL_GROUP_B(T, LPC, NB)                                                                   \
+    AM_DISPATCH_MAT(b.material, (launch_pdl(k_cell_force_group<T, M, LPC, NB>, grid_for(b.num_cells * LPC, 256), 256, s, \
                                             b, U4, static_cast<vec4_t<T>*>(slots), status)))
+#define AM_CELL_GROUP(T, LPC)                                                                         \
+    do {                                                                                              \
+        if (cell_batch() == 4) {                                                                      \
+            AM_CELL_GROUP_B(T, LPC, 4);                                                               \
+        } else if (cell_batch() == 2) {                                                               \
+            AM_CELL_GROUP_B(T, LPC, 2);                                                               \
+        } else {                                                                                      \
+            AM_CELL_GROUP_B(T, LPC, 1);                                                               \
+        }                                                                                             \
+    } while (0)
 
 template <typename T, int LPC>
 void launch_fbar_lpc(const CellBlockDev& b, const double4* U4, void* slots, int* status, cudaStream_t s) {
@@ -2561,7 +2681,7 @@ inline bool gather_batch8(const NodeDev& nd, int mixed) {
 #define AM_NODE_DISPATCH_PDL(KERNEL, ...)                                                             \
     do {                                                                                              \
         const int lpn = node_lanes(nd);                                                               \
-        const unsigned grid = grid_for(nd.num_nodes * lpn, kNodeBlock);                               \
+        const unsigned grid = grid_for((nd.subset_nodes ? nd.subset_count : nd.num_nodes) * lpn, kNodeBlock); \
         const bool b8 = gather_batch8(nd, mixed);                                                     \
         if (mixed) {                                                                                  \
             const float4* sl = static_cast<const float4*>(slots);                                     \
@@ -2697,6 +2817,15 @@ void launch_stress_batch(int32_t mat, double lambda, double mu, int64_t n, const
 void launch_quadrature_batch(int32_t kind, int32_t smoothed, int64_t n, const double* X, double* B, double* w,
                              cudaStream_t s) {
     if (n > 0) k_quadrature_batch<<<grid_for(n, 64), 64, 0, s>>>(kind, smoothed, n, X, B, w);
+}
+
+void launch_iface_pack(int64_t n, const int32_t* rows, const double* own, double* send, cudaStream_t s) {
+    if (n > 0) k_iface_pack<<<grid_for(n, 256), 256, 0, s>>>(n, rows, own, send);
+}
+
+void launch_iface_combine(int64_t rows, const int32_t* ptr, const int32_t* idx, int64_t num_own, const double* own,
+                          const double* recv, double* out, cudaStream_t s) {
+    if (rows > 0) k_iface_combine<<<grid_for(rows, 256), 256, 0, s>>>(rows, ptr, idx, num_own, own, recv, out);
 }
 
 void launch_scatter_elems(const int32_t* order, int64_t n, const double* src, double* dst, cudaStream_t s) {

@@ -52,6 +52,14 @@ struct GaussBlockDev {
     // in place of the coordinate gathers. null where not built.
     const float* patch_dx32;
     const double* patch_dx64;
+    // Hex8 element groups: elements 8g .. 8g+7 form group g; the group's distinct nodes
+    // are its logical slots group_ptr[g] .. group_ptr[g+1]-1 (slot_pos indexes them), and
+    // group_mask[d] tells which of the group's elements touch distinct node d (bits 0-7)
+    // and at which of their nodes (3 bits per element from bit 8). num_groups = 0: one
+    // slot per (element, node).
+    int64_t num_groups;
+    const int32_t* group_ptr;
+    const uint32_t* group_mask;
     // Updated / semi-Lagrangian formulations: element displacement gradient of the last
     // force evaluation (9 per element; for Hex8 the last Gauss point's) and the semi
     // formulation's reference gradient. null under the total formulation.
@@ -112,6 +120,12 @@ struct NodeDev {
     int32_t lagr;
     double4* xc;
     double4* inc;
+    // Node subset of a k_node_step launch, for overlapping the interface exchange: with
+    // subset_nodes the launch runs those nodes (thread t takes subset_nodes[t]); with
+    // skip_iface it runs every node except the interface ones. Neither: every node.
+    const int32_t* subset_nodes;
+    int64_t subset_count;
+    int32_t skip_iface;
 };
 
 // ---- launchers (am_kernels.cu) ----
@@ -189,5 +203,12 @@ void launch_quadrature_batch(int32_t kind, int32_t smoothed, int64_t n, const do
 
 // dst[order[k]] = src[k] for k < n (per-element results back into the caller's order).
 void launch_scatter_elems(const int32_t* order, int64_t n, const double* src, double* dst, cudaStream_t s);
+// Neighbour exchange: send[k] = own[rows[k]] (3 doubles each) for k < n.
+void launch_iface_pack(int64_t n, const int32_t* rows, const double* own, double* send, cudaStream_t s);
+// out[r] = sum over e in [ptr[r], ptr[r+1]) of src(idx[e]) in that order, src(j) = own[j]
+// for j < num_own and recv[j - num_own] after: each interface node's partial forces
+// summed in ascending rank of their holders.
+void launch_iface_combine(int64_t rows, const int32_t* ptr, const int32_t* idx, int64_t num_own, const double* own,
+                          const double* recv, double* out, cudaStream_t s);
 
 }  // namespace am

@@ -315,6 +315,15 @@ class ExplicitDynamics:
         check(self.lib.am_set_interface(self.ctx, ln.size, capi._ptr(ln, C.c_int32), capi._ptr(rw, C.c_int32),
                                         int(num_global)), self.ctx)
 
+    def set_neighbors(self, rank: int, neighbors: np.ndarray, shared_ptr: np.ndarray, shared_nodes: np.ndarray) -> None:
+        """am_set_neighbors: neighbour exchange of the shared nodes' partial forces (the
+        lists of partition.Subdomain: neighbors, shared_ptr, shared_nodes)."""
+        nb = np.ascontiguousarray(neighbors, dtype=np.int32)
+        sp = np.ascontiguousarray(shared_ptr, dtype=np.int64)
+        sn = np.ascontiguousarray(shared_nodes, dtype=np.int32)
+        check(self.lib.am_set_neighbors(self.ctx, int(rank), int(nb.size), capi._ptr(nb, C.c_int32),
+                                        capi._ptr(sp, C.c_int64), capi._ptr(sn, C.c_int32)), self.ctx)
+
     def set_rk_functions(self, nbr_ptr: np.ndarray, nbr: np.ndarray, values: np.ndarray) -> None:
         """Two-pass reproducing-kernel coupling: the state holds generalized coefficients,
         the blocks run on the physical displacement Psi u and their forces reach the

@@ -231,9 +231,16 @@ def tet4_nh_shear_slab(n: int = 70, rank: int = 0, world: int = 1, seed: int = 0
         rows.append(rank * m1 * m1 + np.arange(m1 * m1))
     iface_local = np.concatenate(local).astype(np.int32) if local else np.zeros(0, np.int32)
     iface_rows = np.concatenate(rows).astype(np.int32) if rows else np.zeros(0, np.int32)
+    # neighbour exchange: the bottom plane is shared with rank - 1, the top with rank + 1,
+    # both listed in ascending global id (the order the neighbour lists them in too)
+    neighbors = [q for q in (rank - 1, rank + 1) if 0 <= q < world]
+    planes = [np.arange(m1 * m1) if q < rank else n * m1 * m1 + np.arange(m1 * m1) for q in neighbors]
     meta = {"config": f"Tet4 1-pt Gauss, neo-Hookean, slab {rank} of {world}", "iface_local": iface_local,
             "iface_rows": iface_rows, "num_iface": (world - 1) * m1 * m1,
-            "slab_mass": mesh.lumped_mass(coords, conn, mat.density)}
+            "slab_mass": mesh.lumped_mass(coords, conn, mat.density),
+            "neighbors": np.asarray(neighbors, dtype=np.int32),
+            "shared_ptr": np.arange(len(neighbors) + 1, dtype=np.int64) * m1 * m1,
+            "shared_nodes": (np.concatenate(planes) if planes else np.zeros(0)).astype(np.int32)}
     return Problem(f"tet4_nh_shear_{n}_slab{rank}of{world}", coords, [Part("tet4", mat, conn=conn)],
                    [BoundaryCondition.fixed(fixed)], v0, dt, nsteps, seed, meta)
 

@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--decompose", action="store_true",
                     help="N > 1: one z-slab of the Tet4 shear mesh per rank (weak scaling) with the interface "
                          "forces summed over NCCL every step, instead of N independent replicas")
+    ap.add_argument("--exchange", choices=["neighbor", "allreduce"], default="neighbor",
+                    help="--decompose: interface forces sent to the neighbouring slabs (overlapped with the interior "
+                         "nodes' update) or summed over all ranks")
     ap.add_argument("--skip-adjoint", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
@@ -501,10 +504,15 @@ def decomposed_setup(args, prob, rank, world, dev):
     return mass
 
 
-def attach_interface(model, prob, rank, world):
+def attach_interface(model, prob, rank, world, exchange="neighbor"):
+    """The slab's interface: a neighbour exchange with the slabs above and below (the
+    default), or the all-rank sum of every interface row."""
     from aperi_mech_b200.model import nccl_unique_id
 
-    model.set_interface(prob.meta["iface_local"], prob.meta["iface_rows"], prob.meta["num_iface"])
+    if exchange == "neighbor" and world > 1:
+        model.set_neighbors(rank, prob.meta["neighbors"], prob.meta["shared_ptr"], prob.meta["shared_nodes"])
+    else:
+        model.set_interface(prob.meta["iface_local"], prob.meta["iface_rows"], prob.meta["num_iface"])
     if world > 1:
         import torch.distributed as dist
 
@@ -551,7 +559,7 @@ def run_ours(args, rank, world, local):
     model = ExplicitDynamics(prob.coords, prob.parts, prob.bcs, mass=mass, stream=stream.cuda_stream,
                              rk=prob.meta.get("rk"))
     if args.decompose:
-        attach_interface(model, prob, rank, world)
+        attach_interface(model, prob, rank, world, args.exchange)
     layout = model.layout()
     hbm_peak, peak_kind = measured_peaks()
     fma = fma_peaks(stream)

@@ -371,6 +371,20 @@ int am_set_rk_functions(am_ctx* ctx, const int64_t* nbr_ptr, const int32_t* nbr,
  * not available on a decomposed mesh (AM_ESTATE). */
 int am_set_interface(am_ctx* ctx, int64_t num_local, const int32_t* local_nodes, const int32_t* rows,
                      int64_t num_global);
+/* The same decomposition with a neighbour exchange in place of the all-rank sum: this
+ * context is rank `rank`; it shares nodes with num_neighbors ranks neighbor_ranks
+ * (ascending), the nodes shared with neighbour j being shared_nodes[shared_ptr[j] ..
+ * shared_ptr[j+1]) (this context's node ids, in the order both ranks of the pair use,
+ * e.g. ascending global id). Each step this rank's partial forces of the shared nodes go
+ * to the neighbours that hold them (grouped ncclSend / ncclRecv, payload a few MB at
+ * most for slabs), and every interface node sums its holders' partials in ascending rank
+ * (its own at its place), so all holders of a node get the same bits. In am_run /
+ * am_solve the exchange runs on a second stream while the interior nodes update, and the
+ * interface nodes update once it lands (APERI_B200_EXCHANGE_OVERLAP=0 runs the two in
+ * sequence on the context stream, with bitwise the same result). Call after am_finalize
+ * instead of am_set_interface, then am_set_nccl with the same rank. */
+int am_set_neighbors(am_ctx* ctx, int32_t rank, int32_t num_neighbors, const int32_t* neighbor_ranks,
+                     const int64_t* shared_ptr, const int32_t* shared_nodes);
 /* ncclGetUniqueId (libnccl.so.2 is opened at run time): rank 0 makes the id, the host
  * sends it to the other ranks, every rank passes it to am_set_nccl. */
 int am_nccl_unique_id(unsigned char id[128]);

@@ -507,3 +507,42 @@ def test_interface_exchange_single_rank_is_exact(gpu, use_nccl):
         for a, b in zip(out[(False, key)], out[(True, key)]):
             assert np.array_equal(a, b), key
     assert np.array_equal(out[(False, "f")], out[(True, "f")])
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_neighbor_exchange_single_rank_self_neighbor(gpu, prec, monkeypatch):
+    """The neighbour exchange on one GPU, with the rank as its own neighbour for a subset
+    S of the nodes (NCCL sends to self): each node of S then sums its own partial twice
+    (own, then the received copy), so the internal force doubles exactly on S and stays
+    bitwise equal elsewhere; and the step with the exchange on a second stream under the
+    interior nodes' update equals the same step run in sequence, bit for bit."""
+    import os
+
+    from aperi_mech_b200 import mesh, problems
+    from aperi_mech_b200.model import ExplicitDynamics, nccl_unique_id
+
+    p = problems.tet4_nh_shear(n=8, seed=5, nsteps=20)
+    mass = mesh.lumped_mass(p.coords, p.parts[0].conn, p.parts[0].material.density)
+    rng = np.random.default_rng(3)
+    shared = np.sort(rng.choice(p.num_nodes, size=p.num_nodes // 4, replace=False)).astype(np.int32)
+    u = 1e-4 * rng.standard_normal(p.coords.shape)
+    os.environ.setdefault("NCCL_SOCKET_IFNAME", "lo")
+    with ExplicitDynamics(p.coords, p.parts, p.bcs, mass=mass) as m:
+        f_plain = m.internal_force(u, prec)
+    runs = {}
+    for overlap in ("1", "0"):
+        monkeypatch.setenv("APERI_B200_EXCHANGE_OVERLAP", overlap)
+        with ExplicitDynamics(p.coords, p.parts, p.bcs, mass=mass) as m:
+            m.set_neighbors(0, np.array([0]), np.array([0, shared.size]), shared)
+            m.set_nccl(nccl_unique_id(), 0, 1)
+            f = m.internal_force(u, prec)
+            m.set_state(None, p.v0)
+            m.init_acceleration(prec)
+            m.run(p.nsteps, p.dt, prec)
+            runs[overlap] = m.get_state()
+        mask = np.zeros(p.num_nodes, dtype=bool)
+        mask[shared] = True
+        assert np.array_equal(f[mask], 2.0 * f_plain[mask])
+        assert np.array_equal(f[~mask], f_plain[~mask])
+    for a, b in zip(runs["1"], runs["0"]):
+        assert np.array_equal(a, b)

@@ -294,3 +294,21 @@ def test_three_rank_neighbor_exchange_matches_single_domain(oracle_lib, tmp_path
             for key in ("u", "v", "a"):
                 assert np.array_equal(data[r][key][ia], data[q][key][ib])
     assert np.linalg.norm(u - u_ref) <= 1e-12 * np.linalg.norm(u_ref)
+
+
+def test_slab_neighbor_lists_pair_up():
+    """The weak-scaled slabs' neighbour lists: rank r's top plane and rank r+1's bottom
+    plane are the same global nodes in the same order."""
+    n, world = 3, 3
+    slabs = [problems.tet4_nh_shear_slab(n=n, rank=r, world=world, seed=1, nsteps=1) for r in range(world)]
+    for r, s in enumerate(slabs):
+        nb = list(s.meta["neighbors"])
+        assert nb == [q for q in (r - 1, r + 1) if 0 <= q < world]
+        gid = _slab_global_ids(s, n, r)
+        ptr, nodes = s.meta["shared_ptr"], s.meta["shared_nodes"]
+        for j, q in enumerate(nb):
+            mine = gid[nodes[ptr[j]:ptr[j + 1]]]
+            t = slabs[q]
+            jq = list(t.meta["neighbors"]).index(r)
+            theirs = _slab_global_ids(t, n, q)[t.meta["shared_nodes"][t.meta["shared_ptr"][jq]:t.meta["shared_ptr"][jq + 1]]]
+            assert np.array_equal(mine, theirs) and np.all(np.diff(mine) > 0)
