@@ -134,10 +134,6 @@ struct Block {
     uint32_t* patch_gather = nullptr;
     float* patch_dx32 = nullptr;
     double* patch_dx64 = nullptr;
-    // Hex8 element groups (see GaussBlockDev)
-    int64_t hex_groups = 0;
-    int32_t* hex_group_ptr = nullptr;
-    uint32_t* hex_group_mask = nullptr;
     const int32_t* slot_pos = nullptr;  // block-local view into the context's position array
     std::vector<int32_t> host_nodes;    // node of each logical slot (-1: unused), for the node CSR
     // Processing order of a Gauss block's elements: order[k] is the caller's index of the
@@ -179,9 +175,6 @@ struct Block {
         g.patch_gather = patch_gather;
         g.patch_dx32 = patch_dx32;
         g.patch_dx64 = patch_dx64;
-        g.num_groups = hex_groups;
-        g.group_ptr = hex_group_ptr;
-        g.group_mask = hex_group_mask;
         g.hstate = hstate;
         g.href = href;
         return g;
@@ -243,8 +236,6 @@ struct Block {
         dfree(patch_dx32);
         dfree(patch_dx64);
         dfree(order_dev);
-        dfree(hex_group_ptr);
-        dfree(hex_group_mask);
         dfree(hstate);
         dfree(href);
         dfree(group_ptr);
@@ -314,36 +305,6 @@ TetPatches build_tet_patches(const int32_t* conn, int64_t E) {
     return tp;
 }
 
-// Hex8 element groups: elements 8g .. 8g+7 form group g; its distinct nodes in order of
-// first appearance are its logical slots, each with the mask of the group's elements that
-// touch it (bits 0-7) and the element-local node there (3 bits per element from bit 8).
-struct HexGroups {
-    std::vector<int32_t> ptr;     // groups + 1
-    std::vector<int32_t> nodes;   // per logical slot
-    std::vector<uint32_t> mask;   // per logical slot
-};
-
-HexGroups build_hex_groups(const int32_t* conn, int64_t E) {
-    HexGroups hg;
-    hg.ptr.push_back(0);
-    for (int64_t g0 = 0; g0 < E; g0 += 8) {
-        const int64_t first = static_cast<int64_t>(hg.nodes.size());
-        for (int l = 0; l < 8 && g0 + l < E; ++l)
-            for (int a = 0; a < 8; ++a) {
-                const int32_t n = conn[8 * (g0 + l) + a];
-                int64_t d = first;
-                while (d < static_cast<int64_t>(hg.nodes.size()) && hg.nodes[d] != n) ++d;
-                if (d == static_cast<int64_t>(hg.nodes.size())) {
-                    hg.nodes.push_back(n);
-                    hg.mask.push_back(0u);
-                }
-                hg.mask[d] |= (1u << l) | (static_cast<uint32_t>(a) << (8 + 3 * l));
-            }
-        hg.ptr.push_back(static_cast<int32_t>(hg.nodes.size()));
-    }
-    return hg;
-}
-
 // True when every patch is exactly one hex's six-tet split in the canonical local
 // order (tet t on local nodes 0, a_t, b_t, 3 with a = 1,2,4,5,6,7 and b = 2,4,5,6,7,1).
 bool hex6_patches(const TetPatches& tp) {
@@ -391,9 +352,6 @@ struct am_ctx {
     // Element processing order of Gauss blocks: the locality order chosen from the mesh
     // (element_order, the default) or, with APERI_B200_ELEMENT_ORDER=input, the caller's.
     bool locality_order = true;
-    // Hex8 element groups of eight (the default; APERI_B200_HEX8_GROUPS=0: one slot per
-    // element node).
-    bool hex8_groups = true;
     std::vector<double> host_X;  // coordinates (N x 3), for the element order at am_add_block
     am::StepParams* table = nullptr;
     int64_t table_cap = 0;
@@ -1088,8 +1046,6 @@ int am_create(int64_t num_nodes, const double* coords, am_ctx** out) {
         c->io_scratch = dalloc<double>(N * 3, "io scratch");
         const char* order = std::getenv("APERI_B200_ELEMENT_ORDER");
         c->locality_order = !(order && std::strcmp(order, "input") == 0);
-        const char* groups = std::getenv("APERI_B200_HEX8_GROUPS");
-        c->hex8_groups = !(groups && groups[0] == '0');
         c->host_X.assign(coords, coords + 3 * N);
         std::vector<double4> x(N);
         for (size_t i = 0; i < N; ++i) x[i] = make_double4(coords[3 * i], coords[3 * i + 1], coords[3 * i + 2], 0.0);
@@ -1242,19 +1198,6 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
                     ck(cudaMemcpy(b.conn, conn, S * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
                 }
                 b.host_nodes.assign(conn, conn + S);
-                if (d->kind == AM_HEX8_GAUSS && E > 0 && ctx->hex8_groups && ctx->lagr == 0) {
-                    // Groups of eight consecutive elements (in the locality order a 2x2x2
-                    // block of a structured mesh): one logical slot per distinct node of a
-                    // group, in order of first appearance (element, then node).
-                    HexGroups hg = build_hex_groups(conn, E);
-                    b.hex_groups = static_cast<int64_t>(hg.ptr.size()) - 1;
-                    b.num_entries = hg.ptr.back();
-                    b.hex_group_ptr = dalloc<int32_t>(hg.ptr.size(), "group offsets");
-                    b.hex_group_mask = dalloc<uint32_t>(std::max<size_t>(hg.mask.size(), 1), "group masks");
-                    ck(cudaMemcpy(b.hex_group_ptr, hg.ptr.data(), hg.ptr.size() * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
-                    ck(cudaMemcpy(b.hex_group_mask, hg.mask.data(), hg.mask.size() * sizeof(uint32_t), cudaMemcpyHostToDevice), "upload");
-                    b.host_nodes = std::move(hg.nodes);
-                }
                 if (d->kind == AM_TET4_GAUSS && E > 0 && ctx->tet4_patches && ctx->lagr == 0) {
                     // Patch the tets when patches hold 2.5 tets or more on average; fewer
                     // would leave most of the eight lanes per patch idle.

@@ -523,45 +523,6 @@ __device__ __forceinline__ void hex_conn(const GaussBlockDev& b, int64_t e, int3
     nd[0] = c0.x, nd[1] = c0.y, nd[2] = c0.z, nd[3] = c0.w, nd[4] = c1.x, nd[5] = c1.y, nd[6] = c1.z, nd[7] = c1.w;
 }
 
-// Hex8 element groups (GaussBlockDev::num_groups > 0): the elements run in a locality
-// order, and the eight elements of a group sit on lanes 8k .. 8k+7 of one warp. Each
-// element leaves its eight nodal vectors in shared memory (hex_group_put); the group's
-// lanes then write one slot per distinct node of the group, the sum over the elements
-// touching it in ascending element order (hex_group_write). A 2x2x2 block of hexes
-// writes 27 slots instead of 64, which the node kernel then reads. Lanes past the last
-// element compute a copy of it and write nothing, so every lane reaches the warp sync.
-constexpr int kHexGroupStride = 25;  // 24 values per element, padded: odd stride, no bank conflicts
-
-template <typename T>
-__device__ __forceinline__ void hex_group_put(T* sm, int a, T x, T y, T z) {
-    T* p = sm + threadIdx.x * kHexGroupStride + 3 * a;
-    p[0] = x;
-    p[1] = y;
-    p[2] = z;
-}
-
-template <typename T, typename S>
-__device__ __forceinline__ void hex_group_write(const GaussBlockDev& b, int64_t e, const T* sm, S* slots) {
-    __syncwarp();
-    const int64_t g = e >> 3;
-    if (g >= b.num_groups) return;
-    const int r = static_cast<int>(threadIdx.x & 7);
-    const T* base = sm + (threadIdx.x & ~7u) * kHexGroupStride;
-    const int32_t d1 = b.group_ptr[g + 1];
-    for (int32_t d = b.group_ptr[g] + r; d < d1; d += 8) {
-        const uint32_t m = b.group_mask[d];
-        T x = T(0), y = T(0), z = T(0);
-        for (uint32_t lm = m & 0xFFu; lm; lm &= lm - 1) {
-            const int l = __ffs(lm) - 1;
-            const T* q = base + l * kHexGroupStride + 3 * ((m >> (8 + 3 * l)) & 7u);
-            x += q[0];
-            y += q[1];
-            z += q[2];
-        }
-        slots[b.slot_pos[d]] = make4(x, y, z);
-    }
-}
-
 // The FP32 kernel is held to 128 registers (four 128-thread blocks per SM); the
 // FP64 one keeps its ~250 registers (forcing three blocks per SM spills and was
 // slower on B200) and runs in 64-thread blocks.
@@ -569,12 +530,8 @@ template <typename T, int MAT>
 __global__ void __launch_bounds__(sizeof(T) == 8 ? 64 : 128, sizeof(T) == 8 ? 1 : 4) k_hex8_force(GaussBlockDev b, const double4* __restrict__ X4,
                                                          const double4* __restrict__ U4,
                                                          vec4_t<T>* __restrict__ slots, int* status) {
-    constexpr int kBlock = sizeof(T) == 8 ? 64 : 128;
-    __shared__ T sm[kBlock * kHexGroupStride];
-    const int64_t e_thread = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const bool valid = e_thread < b.num_elems;
-    if (!valid && b.num_groups == 0) return;
-    const int64_t e = valid ? e_thread : b.num_elems - 1;
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= b.num_elems) return;
     int32_t nd[8];
     hex_conn(b, e, nd);
     T X[3][8], U[3][8];
@@ -617,17 +574,34 @@ __global__ void __launch_bounds__(sizeof(T) == 8 ? 64 : 128, sizeof(T) == 8 ? 1 
 #pragma unroll
             for (int j = 0; j < 3; ++j)
                 H[i * 3 + j] = (G[i * 3 + 0] * A[0 * 3 + j] + G[i * 3 + 1] * A[1 * 3 + j] + G[i * 3 + 2] * A[2 * 3 + j]) * id;
-        const double Jf = stress<T>(MAT, T(lam), T(mu), H, P);
-        if (MAT == kNeoHookean) bad |= !(Jf > 0.0);
         T Q[9];
+        if (MAT == kNeoHookean) {
+            // Q = adj(J) P^T with P = tau F^-T and F = (J + G) J^-1 is adj(J + G) tau / det F
+            // (the 8x scale of J and G cancels): no F^-1 and no P.
+            T tau[9];
+            const double Jf = nh_kirchhoff<T>(T(lam), T(mu), H, tau);
+            bad |= !(Jf > 0.0);
+            T Jc[9], Ac[9];
 #pragma unroll
-        for (int k = 0; k < 3; ++k)
+            for (int k = 0; k < 9; ++k) Jc[k] = J[k] + G[k];
+            adj3(Jc, Ac);
+            const T sc = sizeof(T) == 4 ? T(__frcp_rn(static_cast<float>(Jf))) : T(1.0 / Jf);
 #pragma unroll
-            for (int i = 0; i < 3; ++i)
-                Q[k * 3 + i] = A[k * 3 + 0] * P[i * 3 + 0] + A[k * 3 + 1] * P[i * 3 + 1] + A[k * 3 + 2] * P[i * 3 + 2];
+            for (int k = 0; k < 3; ++k)
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    Q[k * 3 + i] = sc * (Ac[k * 3 + 0] * tau[0 * 3 + i] + Ac[k * 3 + 1] * tau[1 * 3 + i] + Ac[k * 3 + 2] * tau[2 * 3 + i]);
+        } else {
+            stress<T>(MAT, T(lam), T(mu), H, P);
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    Q[k * 3 + i] = A[k * 3 + 0] * P[i * 3 + 0] + A[k * 3 + 1] * P[i * 3 + 1] + A[k * 3 + 2] * P[i * 3 + 2];
+        }
         hex_accumulate_r(R, Q, g);
     }
-    if (bad && valid) flag(status, AM_ENONPOS_J, e);
+    if (bad) flag(status, AM_ENONPOS_J, e);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
         R[i][0] = T(0);
@@ -635,12 +609,6 @@ __global__ void __launch_bounds__(sizeof(T) == 8 ? 64 : 128, sizeof(T) == 8 ? 1 
         hex_butterfly_t(R[i]);
     }
     const T s = T(-1.0 / 512.0);
-    if (b.num_groups > 0) {
-#pragma unroll
-        for (int q = 0; q < 8; ++q) hex_group_put(sm, hex_node_of_corner(q), s * R[0][q], s * R[1][q], s * R[2][q]);
-        hex_group_write(b, e_thread, sm, slots);
-        return;
-    }
     const int4 p0 = reinterpret_cast<const int4*>(b.slot_pos)[2 * e], p1 = reinterpret_cast<const int4*>(b.slot_pos)[2 * e + 1];
     const int32_t pos[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
 #pragma unroll
@@ -876,15 +844,11 @@ __global__ void __launch_bounds__(256) k_cell_force_thread(CellBlockDev b, const
 // holds the same H and P), and each lane writes the forces of its own entries.
 // Narrow groups keep the lanes busy on cells of a few tens of entries and repeat
 // the stress update on fewer lanes.
-template <typename T, int MAT, int LPC, int kCellBatch>
+template <typename T, int MAT, int LPC>
 __global__ void __launch_bounds__(256) k_cell_force_group(CellBlockDev b, const double4* __restrict__ U4,
                                                           vec4_t<T>* __restrict__ slots, int* status) {
-    // Entries go in rounds of kCellBatch per lane: a round's node ids and gradients (set-up
-    // data) are loaded a round ahead, and its displacement gathers are all issued before
-    // the first is used, so a lane has kCellBatch gathers in flight instead of one
-    // dependent id -> displacement chain per entry. The first round's ids and gradients
-    // load before the wait for the kernel that writes the displacements. Each lane still
-    // sums its entries in ascending order.
+    pdl_trigger();
+    pdl_wait();
     const int64_t gt = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const int64_t c = gt / LPC;
     const int r = static_cast<int>(threadIdx.x % LPC);
@@ -893,52 +857,18 @@ __global__ void __launch_bounds__(256) k_cell_force_group(CellBlockDev b, const 
     const int32_t s0 = valid ? b.ptr[c] : 0, s1 = valid ? b.ptr[c + 1] : 0;
     const T* gr = cell_grads<T>(b);
     const bool diff = sizeof(T) == 4;
-    int32_t nid[kCellBatch];
-    T gg[kCellBatch][3];
-#pragma unroll
-    for (int k = 0; k < kCellBatch; ++k) {
-        const int32_t s = s0 + r + k * LPC;
-        nid[k] = s < s1 ? b.nodes[s] : 0;
-#pragma unroll
-        for (int i = 0; i < 3; ++i) gg[k][i] = s < s1 ? gr[3 * s + i] : T(0);
-    }
-    const int32_t n_ref = s1 > s0 ? b.nodes[s0] : 0;
-    pdl_trigger();
-    pdl_wait();
-    const double4 ur = s1 > s0 ? ld_dep(U4 + n_ref) : make_double4(0.0, 0.0, 0.0, 0.0);
+    const double4 ur = s1 > s0 ? ld_dep(U4 + b.nodes[s0]) : make_double4(0.0, 0.0, 0.0, 0.0);
     T H[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) H[k] = T(0);
-    for (int32_t base = s0 + r; base < s1; base += kCellBatch * LPC) {
-        double4 u[kCellBatch];
+    for (int32_t s = s0 + r; s < s1; s += LPC) {
+        const double4 u = ld_dep(U4 + b.nodes[s]);
+        const T du[3] = {T(diff ? u.x - ur.x : u.x), T(diff ? u.y - ur.y : u.y), T(diff ? u.z - ur.z : u.z)};
+        const T gg[3] = {gr[3 * s], gr[3 * s + 1], gr[3 * s + 2]};
 #pragma unroll
-        for (int k = 0; k < kCellBatch; ++k)
-            if (base + k * LPC < s1) u[k] = ld_dep(U4 + nid[k]);
-        int32_t nid2[kCellBatch];
-        T gg2[kCellBatch][3];
+        for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int k = 0; k < kCellBatch; ++k) {
-            const int32_t s = base + (kCellBatch + k) * LPC;
-            nid2[k] = s < s1 ? b.nodes[s] : 0;
-#pragma unroll
-            for (int i = 0; i < 3; ++i) gg2[k][i] = s < s1 ? gr[3 * s + i] : T(0);
-        }
-#pragma unroll
-        for (int k = 0; k < kCellBatch; ++k)
-            if (base + k * LPC < s1) {
-                const T du[3] = {T(diff ? u[k].x - ur.x : u[k].x), T(diff ? u[k].y - ur.y : u[k].y),
-                                 T(diff ? u[k].z - ur.z : u[k].z)};
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) H[i * 3 + j] += du[i] * gg[k][j];
-            }
-#pragma unroll
-        for (int k = 0; k < kCellBatch; ++k) {
-            nid[k] = nid2[k];
-#pragma unroll
-            for (int i = 0; i < 3; ++i) gg[k][i] = gg2[k][i];
-        }
+            for (int j = 0; j < 3; ++j) H[i * 3 + j] += du[i] * gg[j];
     }
     // Butterfly over the group: fixed pairing, identical result on every lane.
 #pragma unroll
@@ -952,25 +882,12 @@ __global__ void __launch_bounds__(256) k_cell_force_group(CellBlockDev b, const 
     const double Jf = stress<T>(MAT, T(lam), T(mu), H, P);
     if (r == 0 && MAT == kNeoHookean && !(Jf > 0.0)) flag(status, AM_ENONPOS_J, c);
     const T V = T(b.volumes[c]);
-    for (int32_t base = s0 + r; base < s1; base += kCellBatch * LPC) {
-        T g[kCellBatch][3];
-        int32_t pos[kCellBatch];
+    for (int32_t s = s0 + r; s < s1; s += LPC) {
+        const T gg[3] = {gr[3 * s], gr[3 * s + 1], gr[3 * s + 2]};
+        T f[3];
 #pragma unroll
-        for (int k = 0; k < kCellBatch; ++k) {
-            const int32_t s = base + k * LPC;
-            pos[k] = s < s1 ? b.slot_pos[s] : -1;
-#pragma unroll
-            for (int i = 0; i < 3; ++i) g[k][i] = s < s1 ? gr[3 * s + i] : T(0);
-        }
-#pragma unroll
-        for (int k = 0; k < kCellBatch; ++k)
-            if (pos[k] >= 0) {
-                T f[3];
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-                    f[i] = (g[k][0] * P[i * 3 + 0] + g[k][1] * P[i * 3 + 1] + g[k][2] * P[i * 3 + 2]) * -V;
-                slots[pos[k]] = make4(f[0], f[1], f[2]);
-            }
+        for (int i = 0; i < 3; ++i) f[i] = (gg[0] * P[i * 3 + 0] + gg[1] * P[i * 3 + 1] + gg[2] * P[i * 3 + 2]) * -V;
+        slots[b.slot_pos[s]] = make4(f[0], f[1], f[2]);
     }
 }
 
@@ -1544,11 +1461,8 @@ __global__ void __launch_bounds__(64) k_hex8_vjp(GaussBlockDev b, const double4*
                                                        const double4* __restrict__ U4, const double4* __restrict__ L4,
                                                        double4* __restrict__ slots, double* gmu, double* gk,
                                                        int accumulate) {
-    __shared__ double sm[64 * kHexGroupStride];
-    const int64_t e_thread = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const bool valid = e_thread < b.num_elems;
-    if (!valid && b.num_groups == 0) return;
-    const int64_t e = valid ? e_thread : b.num_elems - 1;
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= b.num_elems) return;
     int32_t nd[8];
     hex_conn(b, e, nd);
     double X[3][8], U[3][8], W[3][8];
@@ -1612,17 +1526,11 @@ __global__ void __launch_bounds__(64) k_hex8_vjp(GaussBlockDev b, const double4*
         hex_butterfly_t(R[i]);
     }
     const double s = -1.0 / 512.0;
-    if (valid) store_theta(gmu, gk, e, tm, tk, accumulate);
-    if (b.num_groups > 0) {
-#pragma unroll
-        for (int q = 0; q < 8; ++q) hex_group_put(sm, hex_node_of_corner(q), s * R[0][q], s * R[1][q], s * R[2][q]);
-        hex_group_write(b, e_thread, sm, slots);
-        return;
-    }
     const int4 p0 = reinterpret_cast<const int4*>(b.slot_pos)[2 * e], p1 = reinterpret_cast<const int4*>(b.slot_pos)[2 * e + 1];
     const int32_t pos[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
 #pragma unroll
     for (int q = 0; q < 8; ++q) slots[pos[hex_node_of_corner(q)]] = make4(s * R[0][q], s * R[1][q], s * R[2][q]);
+    store_theta(gmu, gk, e, tm, tk, accumulate);
 }
 
 template <int MAT>
@@ -1783,14 +1691,10 @@ __global__ void k_tet4_patch_volume_slots(GaussBlockDev b, double density, const
     }
 }
 
-__global__ void __launch_bounds__(128) k_gauss_volume_slots(GaussBlockDev b, double density,
-                                                             const double4* __restrict__ X4,
-                                                             double4* __restrict__ slots) {
-    __shared__ double sm[128 * kHexGroupStride];
-    const int64_t e_thread = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const bool valid = e_thread < b.num_elems;
-    if (!valid && b.num_groups == 0) return;
-    const int64_t e = valid ? e_thread : b.num_elems - 1;
+__global__ void k_gauss_volume_slots(GaussBlockDev b, double density, const double4* __restrict__ X4,
+                                     double4* __restrict__ slots) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= b.num_elems) return;
     const int nn = b.kind == AM_HEX8_GAUSS ? 8 : 4;
     double X[24];
     for (int a = 0; a < nn; ++a) {
@@ -1800,11 +1704,6 @@ __global__ void __launch_bounds__(128) k_gauss_volume_slots(GaussBlockDev b, dou
         X[a * 3 + 2] = x.z;
     }
     const double me = element_volume(nn, X) * density / nn;
-    if (b.num_groups > 0) {
-        for (int a = 0; a < 8; ++a) hex_group_put(sm, a, me, 0.0, 0.0);
-        hex_group_write(b, e_thread, sm, slots);
-        return;
-    }
     for (int a = 0; a < nn; ++a) slots[b.slot_pos[e * nn + a]] = make_double4(me, 0.0, 0.0, 0.0);
 }
 
@@ -1956,15 +1855,19 @@ __global__ void __launch_bounds__(kNodeBlock) k_gather_force4(NodeDev nd, const 
 }
 
 // One thread per local interface node: its own slots summed (no interface override).
-template <typename S>
+template <typename S, int LPN>
 __global__ void __launch_bounds__(kNodeBlock) k_iface_gather(NodeDev nd, const vec4_t<S>* __restrict__ slots,
                                                               int64_t num_local, const int32_t* __restrict__ local_nodes,
                                                               const int32_t* __restrict__ rows, double* __restrict__ buf) {
-    const int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (k >= num_local) return;
+    // LPN lanes per node, as the node kernels take them: the same summation order, so a
+    // decomposed step on one rank reproduces the plain step bit for bit.
+    const int64_t k = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / LPN;
+    const bool own = k < num_local;
+    if (LPN == 1 && !own) return;
     nd.iface_row = nullptr;
     double fx, fy, fz;
-    gather<S, 4, 1>(nd, slots, local_nodes[k], true, fx, fy, fz);
+    gather<S, 4, LPN>(nd, slots, own ? local_nodes[k] : 0, own, fx, fy, fz);
+    if (!own || threadIdx.x % LPN != 0) return;
     const int64_t r = rows[k];
     buf[3 * r] = fx;
     buf[3 * r + 1] = fy;
@@ -2518,26 +2421,9 @@ inline int lanes_per_cell(const CellBlockDev& b) {
     return mean <= 16.0 ? 4 : mean <= 96.0 ? 8 : mean <= 192.0 ? 16 : 32;
 }
 
-inline int cell_batch() {
-    static const int v = [] {
-        const char* e = getenv("APERI_B200_CELL_BATCH");
-        return e ? atoi(e) : 1;
-    }();
-    return v;
-}
-#define AM_CELL_GROUP_B(T, LPC, NB)                                                                   \
-    AM_DISPATCH_MAT(b.material, (launch_pdl(k_cell_force_group<T, M, LPC, NB>, grid_for(b.num_cells * LPC, 256), 256, s, \
-                                            b, U4, static_cast<vec4_t<T>*>(slots), status)))
 #define AM_CELL_GROUP(T, LPC)                                                                         \
-    do {                                                                                              \
-        if (cell_batch() == 4) {                                                                      \
-            AM_CELL_GROUP_B(T, LPC, 4);                                                               \
-        } else if (cell_batch() == 2) {                                                               \
-            AM_CELL_GROUP_B(T, LPC, 2);                                                               \
-        } else {                                                                                      \
-            AM_CELL_GROUP_B(T, LPC, 1);                                                               \
-        }                                                                                             \
-    } while (0)
+    AM_DISPATCH_MAT(b.material, (launch_pdl(k_cell_force_group<T, M, LPC>, grid_for(b.num_cells * LPC, 256), 256, s, \
+                                            b, U4, static_cast<vec4_t<T>*>(slots), status)))
 
 template <typename T, int LPC>
 void launch_fbar_lpc(const CellBlockDev& b, const double4* U4, void* slots, int* status, cudaStream_t s) {
@@ -2669,9 +2555,17 @@ void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const dou
 // in L2 (126 MB on B200), else 4: on B200 the eight-deep batch was ~10% faster for
 // the 70^3 Tet4 mesh's 44 MB of FP32 slots and ~5-10% slower for the 128^3 Hex8
 // mesh's 268 MB.
-inline int node_lanes(const NodeDev& nd) {
+// Lanes per node. Meshes of Gauss elements (at most a dozen slots per node) take two lanes
+// (each reads every other slot of the node's contiguous range, so a warp's loads cover
+// whole lines, and a butterfly adds the halves) for FP64 slots, and for FP32 slots when
+// the slot array sits in L2; FP32 slots streaming from HBM keep one lane per node. On
+// B200: 70^3 Tet4 node kernel 23.1 -> 21.3 us mixed and 32.0 -> 28.8 us FP64, 128^3
+// Hex8 153.9 -> 133.8 us FP64, but 95.2 -> 103.5 us mixed. Cell meshes with tens of
+// slots per node take four or eight lanes.
+inline int node_lanes(const NodeDev& nd, int mixed) {
     const double per_node = static_cast<double>(nd.num_slots) / static_cast<double>(nd.num_nodes);
-    return per_node <= 12.0 ? 1 : per_node <= 40.0 ? 4 : 8;
+    if (per_node <= 12.0) return (!mixed || nd.num_slots * 16 <= (int64_t{64} << 20)) ? 2 : 1;
+    return per_node <= 40.0 ? 4 : 8;
 }
 inline bool gather_batch8(const NodeDev& nd, int mixed) {
     const int64_t bytes = nd.num_slots * (mixed ? 16 : 32);
@@ -2680,19 +2574,21 @@ inline bool gather_batch8(const NodeDev& nd, int mixed) {
 
 #define AM_NODE_DISPATCH_PDL(KERNEL, ...)                                                             \
     do {                                                                                              \
-        const int lpn = node_lanes(nd);                                                               \
+        const int lpn = node_lanes(nd, mixed);                                                               \
         const unsigned grid = grid_for((nd.subset_nodes ? nd.subset_count : nd.num_nodes) * lpn, kNodeBlock); \
         const bool b8 = gather_batch8(nd, mixed);                                                     \
         if (mixed) {                                                                                  \
             const float4* sl = static_cast<const float4*>(slots);                                     \
             if (lpn == 8) launch_pdl(KERNEL<float, 4, 8>, grid, kNodeBlock, s, nd, sl, __VA_ARGS__);   \
             else if (lpn == 4) launch_pdl(KERNEL<float, 2, 4>, grid, kNodeBlock, s, nd, sl, __VA_ARGS__); \
+            else if (lpn == 2) launch_pdl(KERNEL<float, 4, 2>, grid, kNodeBlock, s, nd, sl, __VA_ARGS__); \
             else if (b8) launch_pdl(KERNEL<float, 8, 1>, grid, kNodeBlock, s, nd, sl, __VA_ARGS__);    \
             else launch_pdl(KERNEL<float, 4, 1>, grid, kNodeBlock, s, nd, sl, __VA_ARGS__);            \
         } else {                                                                                      \
             const double4* sl = static_cast<const double4*>(slots);                                   \
             if (lpn == 8) launch_pdl(KERNEL<double, 4, 8>, grid, kNodeBlock, s, nd, sl, __VA_ARGS__);  \
             else if (lpn == 4) launch_pdl(KERNEL<double, 2, 4>, grid, kNodeBlock, s, nd, sl, __VA_ARGS__); \
+            else if (lpn == 2) launch_pdl(KERNEL<double, 4, 2>, grid, kNodeBlock, s, nd, sl, __VA_ARGS__); \
             else if (b8) launch_pdl(KERNEL<double, 8, 1>, grid, kNodeBlock, s, nd, sl, __VA_ARGS__);   \
             else launch_pdl(KERNEL<double, 4, 1>, grid, kNodeBlock, s, nd, sl, __VA_ARGS__);           \
         }                                                                                             \
@@ -2700,19 +2596,21 @@ inline bool gather_batch8(const NodeDev& nd, int mixed) {
 
 #define AM_NODE_DISPATCH(KERNEL, ...)                                                                 \
     do {                                                                                              \
-        const int lpn = node_lanes(nd);                                                               \
+        const int lpn = node_lanes(nd, mixed);                                                               \
         const unsigned grid = grid_for(nd.num_nodes * lpn, kNodeBlock);                               \
         const bool b8 = gather_batch8(nd, mixed);                                                     \
         if (mixed) {                                                                                  \
             const float4* sl = static_cast<const float4*>(slots);                                     \
             if (lpn == 8) KERNEL<float, 4, 8><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);        \
             else if (lpn == 4) KERNEL<float, 2, 4><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);   \
+            else if (lpn == 2) KERNEL<float, 4, 2><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);   \
             else if (b8) KERNEL<float, 8, 1><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);         \
             else KERNEL<float, 4, 1><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);                 \
         } else {                                                                                      \
             const double4* sl = static_cast<const double4*>(slots);                                   \
             if (lpn == 8) KERNEL<double, 4, 8><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);       \
             else if (lpn == 4) KERNEL<double, 2, 4><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);  \
+            else if (lpn == 2) KERNEL<double, 4, 2><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);  \
             else if (b8) KERNEL<double, 8, 1><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);        \
             else KERNEL<double, 4, 1><<<grid, kNodeBlock, 0, s>>>(nd, sl, __VA_ARGS__);                \
         }                                                                                             \
@@ -2728,11 +2626,21 @@ void launch_gather_force4(const NodeDev& nd, int mixed, const void* slots, doubl
 void launch_iface_gather(const NodeDev& nd, int mixed, const void* slots, int64_t num_local,
                          const int32_t* local_nodes, const int32_t* rows, double* buf, cudaStream_t s) {
     if (num_local == 0) return;
-    const unsigned grid = grid_for(num_local, kNodeBlock);
-    if (mixed)
-        k_iface_gather<float><<<grid, kNodeBlock, 0, s>>>(nd, static_cast<const float4*>(slots), num_local, local_nodes, rows, buf);
-    else
-        k_iface_gather<double><<<grid, kNodeBlock, 0, s>>>(nd, static_cast<const double4*>(slots), num_local, local_nodes, rows, buf);
+    const int lpn = node_lanes(nd, mixed);
+    const unsigned grid = grid_for(num_local * lpn, kNodeBlock);
+#define AM_IFACE(S, V, L) k_iface_gather<S, L><<<grid, kNodeBlock, 0, s>>>(nd, static_cast<const V*>(slots), num_local, local_nodes, rows, buf)
+    if (mixed) {
+        if (lpn == 8) AM_IFACE(float, float4, 8);
+        else if (lpn == 4) AM_IFACE(float, float4, 4);
+        else if (lpn == 2) AM_IFACE(float, float4, 2);
+        else AM_IFACE(float, float4, 1);
+    } else {
+        if (lpn == 8) AM_IFACE(double, double4, 8);
+        else if (lpn == 4) AM_IFACE(double, double4, 4);
+        else if (lpn == 2) AM_IFACE(double, double4, 2);
+        else AM_IFACE(double, double4, 1);
+    }
+#undef AM_IFACE
 }
 
 void launch_init_accel(const NodeDev& nd, int mixed, const void* slots, double4* A4, int* status, cudaStream_t s) {

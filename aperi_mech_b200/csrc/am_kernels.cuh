@@ -52,14 +52,6 @@ struct GaussBlockDev {
     // in place of the coordinate gathers. null where not built.
     const float* patch_dx32;
     const double* patch_dx64;
-    // Hex8 element groups: elements 8g .. 8g+7 form group g; the group's distinct nodes
-    // are its logical slots group_ptr[g] .. group_ptr[g+1]-1 (slot_pos indexes them), and
-    // group_mask[d] tells which of the group's elements touch distinct node d (bits 0-7)
-    // and at which of their nodes (3 bits per element from bit 8). num_groups = 0: one
-    // slot per (element, node).
-    int64_t num_groups;
-    const int32_t* group_ptr;
-    const uint32_t* group_mask;
     // Updated / semi-Lagrangian formulations: element displacement gradient of the last
     // force evaluation (9 per element; for Hex8 the last Gauss point's) and the semi
     // formulation's reference gradient. null under the total formulation.

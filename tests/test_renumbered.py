@@ -117,36 +117,3 @@ def test_caller_order_option_matches_locality_order(gpu, monkeypatch):
     f1, _, _ = _run(p, "fp64", u)
     assert rel_err(f1, f0) < 1e-13
 
-
-def test_hex8_groups_match_per_element_slots(gpu, monkeypatch):
-    """Hex8 element groups (eight consecutive elements sum their shared nodes in shared
-    memory and write one slot per distinct node) against one slot per element node
-    (APERI_B200_HEX8_GROUPS=0): the same forces, VJP, lumped mass and trajectory to
-    round-off, with far fewer slots (27 per 2x2x2 block instead of 64)."""
-    from aperi_mech_b200.model import ExplicitDynamics
-
-    p = _problem("hex8")
-    rng = np.random.default_rng(8)
-    u = 1e-4 * rng.standard_normal(p.coords.shape)
-    lam = rng.standard_normal(p.coords.shape)
-    out = {}
-    for groups in ("1", "0"):
-        monkeypatch.setenv("APERI_B200_HEX8_GROUPS", groups)
-        with ExplicitDynamics(p.coords, p.parts, p.bcs) as m:
-            f = m.internal_force(u)
-            fm = m.internal_force(u, "mixed")
-            v = m.vjp_force(u, lam)
-            mass = m.mass()
-            m.set_state(None, p.v0)
-            m.init_acceleration()
-            m.run(p.nsteps, p.dt)
-            out[groups] = (f, fm, v, mass, m.get_state(), m.layout()["used_slots"])
-    g, n = out["1"], out["0"]
-    assert rel_err(g[0], n[0]) < 1e-13
-    assert rel_err(g[1], n[1]) < 1e-6
-    for a, b in zip(g[2], n[2]):
-        assert rel_err(a, b) < 1e-13
-    assert rel_err(g[3], n[3]) < 1e-14
-    for a, b in zip(g[4], n[4]):
-        assert l2_rel(a, b) < 1e-13
-    assert g[5] < 0.5 * n[5]
