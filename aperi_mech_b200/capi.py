@@ -33,6 +33,7 @@ EXPORTED = [
     "am_set_nccl", "am_set_rk_functions", "am_set_cell_groups", "am_rkpm_nodal_subcells", "am_cells_groups",
     "am_set_formulation", "am_rkpm_hex8_element_cells", "am_noalloc_status",
     "am_measure_fma_peak", "am_element_order", "am_smoothed_element_cells", "am_set_neighbors",
+    "am_rkpm_nodal_cells_two_pass", "am_set_rk_points",
 ]
 
 # Tets per call of am_tet4_internal_force_noalloc (AM_NOALLOC_MAX_TETS in include/aperi_b200.h).
@@ -143,6 +144,9 @@ def load(build_if_missing: bool = False) -> C.CDLL:
         "am_smoothed_element_cells": (C.c_int, [C.c_int64, _dp, C.c_int64, C.c_int32, _ip, C.c_double,
                                                 C.POINTER(vp)]),
         "am_set_neighbors": (C.c_int, [vp, C.c_int32, C.c_int32, _ip, _lp, _ip]),
+        "am_rkpm_nodal_cells_two_pass": (C.c_int, [C.c_int64, _dp, C.c_int64, _ip, _dp, C.c_int32, C.c_double,
+                                                   C.POINTER(vp)]),
+        "am_set_rk_points": (C.c_int, [vp, C.c_int64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

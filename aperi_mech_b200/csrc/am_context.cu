@@ -355,6 +355,15 @@ struct am_ctx {
     std::vector<double> host_X;  // coordinates (N x 3), for the element order at am_add_block
     am::StepParams* table = nullptr;
     int64_t table_cap = 0;
+    // CUDA graphs of the step loop: kGraphSteps steps (element and node kernels, with their
+    // programmatic launch edges) captured once per precision and replayed for every full
+    // chunk of a run, the chunk's rows of the step table first copied to a fixed chunk table
+    // that the graph reads. Captured at the end of a precision's first run, after it made any
+    // lazily allocated buffers. APERI_B200_GRAPHS=0 launches every kernel on the stream.
+    static constexpr int64_t kGraphSteps = 32;
+    bool use_graphs = true;
+    am::StepParams* chunk_table = nullptr;
+    cudaGraphExec_t step_graph[2] = {nullptr, nullptr};
     am::StepParams* table_host = nullptr;  // pinned staging
     cudaEvent_t table_copied = nullptr;    // the last upload out of table_host has executed
     std::vector<Block> blocks;
@@ -408,8 +417,12 @@ struct am_ctx {
     bool lagr_rebased = false;        // the element H of step lagr_steps is already the reference
     double4* xc = nullptr;            // current (updated) or reference (semi) coordinates
     double4* lagr_inc = nullptr;      // displacement increment
+    // Points the cell entries index (am_set_rk_points): the nodes, then the refinement
+    // points of two-pass nodal cells. 0: the nodes alone.
+    int64_t num_points = 0;
+    int64_t points() const { return num_points > N ? num_points : N; }
     // Two-pass reproducing-kernel coupling (am_set_rk_functions).
-    int64_t* rk_ptr = nullptr;        // N + 1: rows of Psi
+    int64_t* rk_ptr = nullptr;        // points + 1: rows of Psi
     int32_t* rk_nbr = nullptr;
     double* rk_val = nullptr;
     int64_t* rkt_ptr = nullptr;       // N + 1: columns of Psi (transposed CSR)
@@ -482,8 +495,9 @@ struct am_ctx {
             check_launch("element force kernel");
             return;
         }
+        if (num_points > N && !rk_ptr) fail(AM_ESTATE, "cells on refinement points run after am_set_rk_functions");
         if (rk_ptr) {
-            am::launch_rk_rows4(N, rk_ptr, rk_nbr, rk_val, U, rk_u, stream);
+            am::launch_rk_rows4(points(), N, rk_ptr, rk_nbr, rk_val, U, rk_u, stream);
             ++launches;
             U = rk_u;
         }
@@ -499,6 +513,7 @@ struct am_ctx {
         if (rk_ptr) {
             am::NodeDev nd = node_dev();
             nd.f_given = nullptr;
+            nd.num_nodes = points();  // the local force lives on the points
             am::launch_gather_force4(nd, mixed, s, rk_f_local, stream);
             am::launch_rk_cols3(N, rkt_ptr, rkt_src, rkt_val, rk_f_local, rk_f, stream);
             launches += 2;
@@ -781,6 +796,46 @@ struct am_ctx {
         ck(cudaEventRecord(table_copied, stream), "event record");
     }
 
+    // A setter that changes what the step kernels are given (conditions, fields, mass, body
+    // acceleration, functions, exchange) drops the captured graphs; the next run captures anew.
+    // An executable graph still in flight is freed once it completes.
+    void drop_graphs() {
+        for (auto& g : step_graph) {
+            if (g) cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    }
+
+    // Captures kGraphSteps advancing steps (element kernels, node kernel) reading the chunk
+    // table, on the context stream.
+    int64_t graph_step_launches = 0;
+    void capture_step_graph(int mixed) {
+        if (!chunk_table) chunk_table = dalloc<am::StepParams>(kGraphSteps + 1, "chunk step table");
+        const am::NodeDev nd = node_dev();
+        void* s = slots(mixed);
+        const int64_t before = launches;
+        ck(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        cudaGraph_t g = nullptr;
+        try {
+            for (int64_t k = 0; k < kGraphSteps; ++k) {
+                element_forces(mixed, U4);
+                am::launch_node_step(nd, mixed, s, chunk_table, k, 1, U4, V4, A4, nullptr, status, stream, 0);
+                ++launches;
+            }
+        } catch (...) {
+            cudaStreamEndCapture(stream, &g);
+            if (g) cudaGraphDestroy(g);
+            launches = before;
+            throw;
+        }
+        ck(cudaStreamEndCapture(stream, &g), "end capture");
+        graph_step_launches = (launches - before) / kGraphSteps;
+        launches = before;
+        const cudaError_t e = cudaGraphInstantiate(&step_graph[mixed], g, 0);
+        cudaGraphDestroy(g);
+        ck(e, "graph instantiate");
+    }
+
     // Steps [n0, n1) of the uploaded table, from a consistent (U4, V4, A4). u_hist[k]
     // (optional) receives the displacement the element kernels use at step n0+k.
     void run_range(int mixed, int64_t n0, int64_t n1, double4* const* u_hist) {
@@ -797,7 +852,19 @@ struct am_ctx {
         check_launch("prologue kernel");
         mark(1, 1);
         const bool split = !nbr_ranks.empty() && overlap && comm && xstream;
-        for (int64_t n = n0; n < n1; ++n) {
+        int64_t n = n0;
+        // Full chunks by graph replay (forward runs on a single domain, total formulation, no
+        // per-kernel marks). The run's last step (which does not advance) stays on the stream.
+        const bool graphs = use_graphs && !u_hist && !lagr && !iface_row_of && !profiling;
+        if (graphs && step_graph[mixed] && n1 - n0 - 1 >= kGraphSteps) {
+            for (; n1 - n - 1 >= kGraphSteps; n += kGraphSteps) {
+                ck(cudaMemcpyAsync(chunk_table, table + n, (kGraphSteps + 1) * sizeof(am::StepParams),
+                                   cudaMemcpyDeviceToDevice, stream), "chunk table");
+                ck(cudaGraphLaunch(step_graph[mixed], stream), "graph launch");
+                launches += kGraphSteps * graph_step_launches;
+            }
+        }
+        for (; n < n1; ++n) {
             element_forces(mixed, U4);
             mark(0, static_cast<int64_t>(blocks.size()));
             const int advance = (n + 1 < n1) ? 1 : 0;
@@ -837,6 +904,9 @@ struct am_ctx {
             check_launch("node step kernel");
             mark(1, 1);
         }
+        // The graph is captured at the end of a precision's first run (after that run made any
+        // lazily allocated buffers), so that later runs replay it without a capture of their own.
+        if (graphs && !step_graph[mixed]) capture_step_graph(mixed);
     }
 
     void init_acceleration(int mixed) {
@@ -908,6 +978,9 @@ struct am_ctx {
         dfree(nbr_recv);
         dfree(comb_ptr);
         dfree(comb_idx);
+        for (auto& g : step_graph)
+            if (g) cudaGraphExecDestroy(g);
+        dfree(chunk_table);
         if (ev_ready) cudaEventDestroy(ev_ready);
         if (ev_done) cudaEventDestroy(ev_done);
         if (xstream) cudaStreamDestroy(xstream);
@@ -1044,6 +1117,8 @@ int am_create(int64_t num_nodes, const double* coords, am_ctx** out) {
         c->status = dalloc<int>(2, "status");
         c->f_scratch = dalloc<double>(N * 3, "force scratch");
         c->io_scratch = dalloc<double>(N * 3, "io scratch");
+        const char* graphs = std::getenv("APERI_B200_GRAPHS");
+        c->use_graphs = !(graphs && graphs[0] == '0');
         const char* order = std::getenv("APERI_B200_ELEMENT_ORDER");
         c->locality_order = !(order && std::strcmp(order, "input") == 0);
         c->host_X.assign(coords, coords + 3 * N);
@@ -1126,7 +1201,7 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
                     if (c > 0) maxlen = std::max<int32_t>(maxlen, ptr[c] - ptr[c - 1]);
                 }
                 for (int64_t s = 0; s < K; ++s)
-                    if (d->cell_nodes[s] < 0 || d->cell_nodes[s] >= ctx->N) fail(AM_EINVAL, "cell node index out of range");
+                    if (d->cell_nodes[s] < 0 || d->cell_nodes[s] >= ctx->points()) fail(AM_EINVAL, "cell node index out of range");
                 std::vector<float> g32(K * 3);
                 for (int64_t s = 0; s < K * 3; ++s) {
                     if (!std::isfinite(d->cell_grads[s])) fail(AM_EINVAL, "non-finite cell gradient");
@@ -1261,6 +1336,7 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
 int am_set_boundary_conditions(am_ctx* ctx, int32_t num_bcs, const am_bc_desc* bcs) {
     if (!ctx) return AM_EINVAL;
     return guarded(ctx, [&] {
+        ctx->drop_graphs();
         if (num_bcs < 0 || num_bcs > AM_MAX_BCS) fail(AM_ERANGE, "at most AM_MAX_BCS boundary conditions");
         if (num_bcs > 0 && !bcs) fail(AM_EINVAL, "null boundary-condition array");
         std::vector<am::host::BoundaryCondition> list;
@@ -1302,6 +1378,7 @@ int am_set_boundary_conditions(am_ctx* ctx, int32_t num_bcs, const am_bc_desc* b
 int am_set_block_fields(am_ctx* ctx, int32_t block_id, const double* mu_field, const double* kappa_field) {
     if (!ctx) return AM_EINVAL;
     return guarded(ctx, [&] {
+        ctx->drop_graphs();
         if (block_id < 0 || block_id >= static_cast<int32_t>(ctx->blocks.size())) fail(AM_EINVAL, "no such block");
         Block& b = ctx->blocks[block_id];
         const int64_t E = b.num_elems;
@@ -1322,6 +1399,7 @@ int am_set_block_fields(am_ctx* ctx, int32_t block_id, const double* mu_field, c
 int am_set_cell_groups(am_ctx* ctx, int32_t block_id, int64_t num_cells, const int64_t* group_ptr) {
     if (!ctx) return AM_EINVAL;
     return guarded(ctx, [&] {
+        ctx->drop_graphs();
         if (ctx->finalized) fail(AM_ESTATE, "am_set_cell_groups after am_finalize");
         if (block_id < 0 || block_id >= static_cast<int32_t>(ctx->blocks.size())) fail(AM_EINVAL, "bad block id");
         Block& b = ctx->blocks[block_id];
@@ -1351,6 +1429,7 @@ int am_set_cell_groups(am_ctx* ctx, int32_t block_id, int64_t num_cells, const i
 int am_set_body_acceleration(am_ctx* ctx, const double g[3]) {
     if (!ctx || !g) return AM_EINVAL;
     return guarded(ctx, [&] {
+        ctx->drop_graphs();
         for (int i = 0; i < 3; ++i) {
             if (!std::isfinite(g[i])) fail(AM_EINVAL, "non-finite body acceleration");
             ctx->g[i] = g[i];
@@ -1361,6 +1440,7 @@ int am_set_body_acceleration(am_ctx* ctx, const double g[3]) {
 int am_set_mass(am_ctx* ctx, const double* mass) {
     if (!ctx || !mass) return AM_EINVAL;
     return guarded(ctx, [&] {
+        ctx->drop_graphs();
         for (int64_t i = 0; i < ctx->N; ++i)
             if (!(mass[i] > 0.0)) fail(AM_EINVAL, "nodal masses must be positive");
         ck(cudaMemcpy(ctx->mass, mass, ctx->N * sizeof(double), cudaMemcpyHostToDevice), "mass upload");
@@ -1374,21 +1454,22 @@ int am_finalize(am_ctx* ctx) {
     return guarded(ctx, [&] {
         if (ctx->finalized) fail(AM_ESTATE, "am_finalize called twice");
         if (ctx->blocks.empty()) fail(AM_EINVAL, "no blocks");
-        const int64_t N = ctx->N, S = ctx->num_slots;
-        // Node-major slot layout: node i owns positions [ptr[i], ptr[i+1]); within a node
-        // the positions follow ascending logical slot (block order, then element order).
-        std::vector<int32_t> ptr(N + 1, 0), pos(S, -1);
+        const int64_t N = ctx->N, S = ctx->num_slots, NP = ctx->points();
+        if (NP > N && !ctx->mass_set) fail(AM_ESTATE, "cells on refinement points need the generalized mass (am_set_mass)");
+        // Node-major slot layout: node (or point) i owns positions [ptr[i], ptr[i+1]); within
+        // a node the positions follow ascending logical slot (block order, then element order).
+        std::vector<int32_t> ptr(NP + 1, 0), pos(S, -1);
         for (const auto& b : ctx->blocks)
             for (int32_t n : b.host_nodes)
                 if (n >= 0) ++ptr[n + 1];
-        for (int64_t i = 0; i < N; ++i) ptr[i + 1] += ptr[i];
+        for (int64_t i = 0; i < NP; ++i) ptr[i + 1] += ptr[i];
         std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
         for (const auto& b : ctx->blocks)
             for (int64_t k = 0; k < static_cast<int64_t>(b.host_nodes.size()); ++k)
                 if (b.host_nodes[k] >= 0) pos[b.slot_base + k] = fill[b.host_nodes[k]]++;
-        ctx->num_used_slots = ptr[N];
-        ctx->node_ptr = dalloc<int32_t>(N + 1, "node ptr");
-        ck(cudaMemcpy(ctx->node_ptr, ptr.data(), (N + 1) * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+        ctx->num_used_slots = ptr[NP];
+        ctx->node_ptr = dalloc<int32_t>(NP + 1, "node ptr");
+        ck(cudaMemcpy(ctx->node_ptr, ptr.data(), (NP + 1) * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
         if (S > 0) {
             ctx->slot_pos = dalloc<int32_t>(S, "slot positions");
             ck(cudaMemcpy(ctx->slot_pos, pos.data(), S * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
@@ -1528,6 +1609,7 @@ int am_solve(am_ctx* ctx, am_precision prec, double dt, double t_end, int64_t ma
 int am_set_power_method(am_ctx* ctx, const double* start, const double* max_edge_length) {
     if (!ctx) return AM_EINVAL;
     return guarded(ctx, [&] {
+        ctx->drop_graphs();
         ctx->require_finalized();
         if (!start || !max_edge_length) fail(AM_EINVAL, "null start vector or edge lengths");
         for (int64_t i = 0; i < ctx->N; ++i)
@@ -1883,6 +1965,7 @@ int am_set_interface(am_ctx* ctx, int64_t num_local, const int32_t* local_nodes,
                      int64_t num_global) {
     if (!ctx) return AM_EINVAL;
     return guarded(ctx, [&] {
+        ctx->drop_graphs();
         ctx->require_finalized();
         if (!ctx->mass_from_caller)
             fail(AM_ESTATE, "a decomposed mesh needs the global lumped mass from am_set_mass before am_finalize");
@@ -1919,6 +2002,7 @@ int am_set_neighbors(am_ctx* ctx, int32_t rank, int32_t num_neighbors, const int
                      const int64_t* shared_ptr, const int32_t* shared_nodes) {
     if (!ctx) return AM_EINVAL;
     return guarded(ctx, [&] {
+        ctx->drop_graphs();
         ctx->require_finalized();
         if (!ctx->mass_from_caller)
             fail(AM_ESTATE, "a decomposed mesh needs the global lumped mass from am_set_mass before am_finalize");
@@ -2003,6 +2087,7 @@ int am_set_neighbors(am_ctx* ctx, int32_t rank, int32_t num_neighbors, const int
 int am_set_formulation(am_ctx* ctx, int32_t formulation, int32_t update_interval) {
     if (!ctx) return AM_EINVAL;
     return guarded(ctx, [&] {
+        ctx->drop_graphs();
         // Before the blocks: the element state is per element, so Tet4 blocks keep one
         // slot per element node instead of element patches.
         if (ctx->finalized || !ctx->blocks.empty()) fail(AM_ESTATE, "am_set_formulation comes before am_add_block");
@@ -2013,26 +2098,40 @@ int am_set_formulation(am_ctx* ctx, int32_t formulation, int32_t update_interval
     });
 }
 
+int am_set_rk_points(am_ctx* ctx, int64_t num_points) {
+    if (!ctx) return AM_EINVAL;
+    return guarded(ctx, [&] {
+        if (ctx->finalized || !ctx->blocks.empty()) fail(AM_ESTATE, "am_set_rk_points comes before am_add_block");
+        if (num_points < ctx->N) fail(AM_EINVAL, "the points start with the nodes: num_points >= num_nodes");
+        if (num_points >= (int64_t(1) << 31)) fail(AM_ERANGE, "point count beyond int32 indexing");
+        if (ctx->lagr) fail(AM_ESTATE, "refinement points are built for the total formulation");
+        ctx->num_points = num_points;
+    });
+}
+
 int am_set_rk_functions(am_ctx* ctx, const int64_t* nbr_ptr, const int32_t* nbr, const double* values) {
     if (!ctx) return AM_EINVAL;
     return guarded(ctx, [&] {
+        ctx->drop_graphs();
         ctx->require_finalized();
         if (ctx->rk_ptr) fail(AM_ESTATE, "reproducing-kernel functions already set");
         if (ctx->iface_row_of) fail(AM_ESTATE, "a decomposed mesh with the two-pass coupling is not built");
         if (!ctx->mass_from_caller)
             fail(AM_ESTATE, "the two-pass coupling needs the generalized lumped mass from am_set_mass before am_finalize");
         if (!nbr_ptr) fail(AM_EINVAL, "null neighbour offsets");
-        const int64_t N = ctx->N, K = nbr_ptr[N];
+        // One row per point: the nodes, then any refinement points (am_set_rk_points).
+        const int64_t N = ctx->N, NP = ctx->points(), K = nbr_ptr[NP];
         if (nbr_ptr[0] != 0 || K < 0 || (K > 0 && (!nbr || !values))) fail(AM_EINVAL, "bad neighbour arrays");
-        for (int64_t i = 0; i < N; ++i)
+        for (int64_t i = 0; i < NP; ++i)
             if (nbr_ptr[i + 1] < nbr_ptr[i]) fail(AM_EINVAL, "neighbour offsets must not decrease");
         for (int64_t k = 0; k < K; ++k)
             if (nbr[k] < 0 || nbr[k] >= N) fail(AM_EINVAL, "neighbour out of range");
-        // Transposed functions: column j lists (i, psi_j(x_i)) for ascending i; a row
-        // without neighbours contributes a unit entry to its own column.
+        // Transposed functions: column j lists (i, psi_j(x_i)) for ascending i; a node row
+        // without neighbours contributes a unit entry to its own column (a refinement point
+        // without neighbours contributes nothing).
         std::vector<int64_t> tptr(N + 1, 0);
-        for (int64_t i = 0; i < N; ++i) {
-            if (nbr_ptr[i] == nbr_ptr[i + 1]) ++tptr[i + 1];
+        for (int64_t i = 0; i < NP; ++i) {
+            if (nbr_ptr[i] == nbr_ptr[i + 1] && i < N) ++tptr[i + 1];
             for (int64_t k = nbr_ptr[i]; k < nbr_ptr[i + 1]; ++k) ++tptr[nbr[k] + 1];
         }
         for (int64_t j = 0; j < N; ++j) tptr[j + 1] += tptr[j];
@@ -2041,8 +2140,8 @@ int am_set_rk_functions(am_ctx* ctx, const int64_t* nbr_ptr, const int32_t* nbr,
         std::vector<int32_t> tsrc(static_cast<size_t>(T));
         std::vector<double> tval(static_cast<size_t>(T));
         std::vector<int64_t> fill(tptr.begin(), tptr.end() - 1);
-        for (int64_t i = 0; i < N; ++i) {
-            if (nbr_ptr[i] == nbr_ptr[i + 1]) {
+        for (int64_t i = 0; i < NP; ++i) {
+            if (nbr_ptr[i] == nbr_ptr[i + 1] && i < N) {
                 tsrc[fill[i]] = static_cast<int32_t>(i);
                 tval[fill[i]++] = 1.0;
             }
@@ -2056,14 +2155,14 @@ int am_set_rk_functions(am_ctx* ctx, const int64_t* nbr_ptr, const int32_t* nbr,
             dst = dalloc<T0>(static_cast<size_t>(std::max<int64_t>(n, 1)), what);
             if (n > 0) ck(cudaMemcpy(dst, src, n * sizeof(T0), cudaMemcpyHostToDevice), "upload");
         };
-        up(ctx->rk_ptr, nbr_ptr, N + 1, "function offsets");
+        up(ctx->rk_ptr, nbr_ptr, NP + 1, "function offsets");
         up(ctx->rk_nbr, nbr, K, "function neighbours");
         up(ctx->rk_val, values, K, "function values");
         up(ctx->rkt_ptr, tptr.data(), N + 1, "transposed offsets");
         up(ctx->rkt_src, tsrc.data(), T, "transposed sources");
         up(ctx->rkt_val, tval.data(), T, "transposed values");
-        ctx->rk_u = dalloc<double4>(N, "physical displacement");
-        ctx->rk_f_local = dalloc<double4>(N, "local force");
+        ctx->rk_u = dalloc<double4>(NP, "physical displacement");
+        ctx->rk_f_local = dalloc<double4>(NP, "local force");
         ctx->rk_f = dalloc<double>(3 * N, "generalized force");
     });
 }
@@ -2083,6 +2182,7 @@ int am_nccl_unique_id(unsigned char id[128]) {
 int am_set_nccl(am_ctx* ctx, const unsigned char id[128], int32_t rank, int32_t nranks) {
     if (!ctx) return AM_EINVAL;
     return guarded(ctx, [&] {
+        ctx->drop_graphs();
         if (!id || nranks < 1 || rank < 0 || rank >= nranks) fail(AM_EINVAL, "bad NCCL rank or id");
         if (!ctx->iface_row_of) fail(AM_ESTATE, "am_set_interface or am_set_neighbors first");
         if (!ctx->nbr_ranks.empty()) {

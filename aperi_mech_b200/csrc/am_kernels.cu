@@ -2144,7 +2144,7 @@ __device__ __forceinline__ void rk_combine(double& x, double& y, double& z) {
 
 // Physical displacement P = Psi U (ComputeValues: neighbours taken from the last; a
 // row without neighbours copies the coefficient).
-__global__ void __launch_bounds__(128) k_rk_rows4(int64_t n, const int64_t* __restrict__ ptr,
+__global__ void __launch_bounds__(128) k_rk_rows4(int64_t n, int64_t num_nodes, const int64_t* __restrict__ ptr,
                                                  const int32_t* __restrict__ nbr, const double* __restrict__ val,
                                                  const double4* __restrict__ U4, double4* __restrict__ P4) {
     const int64_t i = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / kRkLanes;
@@ -2165,7 +2165,9 @@ __global__ void __launch_bounds__(128) k_rk_rows4(int64_t n, const int64_t* __re
     }
     rk_combine(x, y, z);
     if (!own || r != 0) return;
-    P4[i] = b == e ? U4[i] : make_double4(x, y, z, 0.0);
+    // A row without neighbours copies its node's coefficient; a refinement point past the
+    // nodes has none and stays at zero.
+    P4[i] = b != e ? make_double4(x, y, z, 0.0) : i < num_nodes ? U4[i] : make_double4(0.0, 0.0, 0.0, 0.0);
 }
 
 // Generalized force f = Psi^T f_local (ScatterValues as a gather over the transposed
@@ -2698,9 +2700,9 @@ void launch_gauss_force_lagr(const GaussBlockDev& b, int32_t lagr, int rebase, c
     }
 }
 
-void launch_rk_rows4(int64_t n, const int64_t* ptr, const int32_t* nbr, const double* val, const double4* U4,
-                     double4* P4, cudaStream_t s) {
-    if (n > 0) k_rk_rows4<<<grid_for(n * kRkLanes, 128), 128, 0, s>>>(n, ptr, nbr, val, U4, P4);
+void launch_rk_rows4(int64_t n, int64_t num_nodes, const int64_t* ptr, const int32_t* nbr, const double* val,
+                     const double4* U4, double4* P4, cudaStream_t s) {
+    if (n > 0) k_rk_rows4<<<grid_for(n * kRkLanes, 128), 128, 0, s>>>(n, num_nodes, ptr, nbr, val, U4, P4);
 }
 void launch_rk_cols3(int64_t n, const int64_t* tptr, const int32_t* tsrc, const double* tval, const double4* f_local,
                      double* f, cudaStream_t s) {

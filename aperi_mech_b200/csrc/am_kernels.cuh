@@ -172,11 +172,12 @@ int64_t launch_pm_next(const NodeDev& nd, const double* f_eps, const double* f_u
                        double4* V4, double* partial, cudaStream_t s);
 void launch_pm_scale(int64_t n, double4* V4, double scale, cudaStream_t s);
 // Two-pass reproducing-kernel coupling (FunctionEvaluationProcessor): Psi in CSR rows
-// (row i: psi_j(x_i) for the neighbours j of node i). rows4: P = Psi U, a row without
-// neighbours copying U[i]; cols3: f = Psi^T f_local from the transposed CSR (column j:
-// the rows i that hold j, ascending i, with a unit entry for each empty row).
-void launch_rk_rows4(int64_t n, const int64_t* ptr, const int32_t* nbr, const double* val, const double4* U4,
-                     double4* P4, cudaStream_t s);
+// (row i: psi_j(x_i) for the neighbours j of node i, n rows: one per node, or one per
+// refinement point with the nodes first). rows4: P = Psi U, a row without neighbours
+// copying U[i] (zero past the nodes); cols3: f = Psi^T f_local from the transposed CSR
+// (column j: the rows i that hold j, ascending i, with a unit entry for each empty node row).
+void launch_rk_rows4(int64_t n, int64_t num_nodes, const int64_t* ptr, const int32_t* nbr, const double* val,
+                     const double4* U4, double4* P4, cudaStream_t s);
 void launch_rk_cols3(int64_t n, const int64_t* tptr, const int32_t* tsrc, const double* tval, const double4* f_local,
                      double* f, cudaStream_t s);
 void launch_sensor_seed(const double4* U4, int32_t num_sensors, const int32_t* sensors, double4* UB, double* loss,

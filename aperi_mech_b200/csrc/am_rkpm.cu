@@ -335,8 +335,15 @@ void rk_functions(am_cells* c, int64_t N, const double* X, const double* R, doub
 
 // Nodal cells on the thex corner hexes; with subcells every corner hex is its own
 // subcell and group_ptr collects the hexes of each vertex.
+// mode: kOnePass (vertex cells, one-pass gradients), kSubcells (one subcell per corner hex),
+// kTwoPass (vertex cells whose entries are the corner-hex points themselves, with the
+// hexes' smoothed gradients b_p = sum_hex B_hex,k(p) V_hex / V_cell; the functions
+// couple the points to the vertices at run time).
+enum NodalMode { kOnePass = 0, kSubcells = 1, kTwoPass = 2 };
+
 int nodal_cells(int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R, int32_t max_neighbors,
-                double density, bool subcells, am_cells** out) {
+                double density, int mode, am_cells** out) {
+    const bool subcells = mode == kSubcells;
     am::set_free_error("");
     if (!out) return AM_EINVAL;
     *out = nullptr;
@@ -478,9 +485,11 @@ int nodal_cells(int64_t N, const double* X, int64_t T, const int32_t* tets, cons
             });
             c->group_ptr = vptr;
         } else {
+        const bool two_pass = mode == kTwoPass;
+        const int64_t W = two_pass ? P : N;  // entry ids: points (two-pass) or nodes
         parallel_for(N, [&](int64_t vtx) {
-            thread_local std::vector<int32_t> where;  // node -> entry of the current cell, -1 if none
-            if (static_cast<int64_t>(where.size()) < N) where.assign(N, -1);
+            thread_local std::vector<int32_t> where;  // node (point) -> entry of the current cell, -1 if none
+            if (static_cast<int64_t>(where.size()) < W) where.assign(W, -1);
             double Vc = 0.0;
             for (int64_t s = vptr[vtx]; s < vptr[vtx + 1]; ++s) {
                 const int64_t h = vcorner[s];
@@ -492,6 +501,20 @@ int nodal_cells(int64_t N, const double* X, int64_t T, const int32_t* tets, cons
                 if (!(V > 0.0)) bad = 1;
                 hexvol[h] = V;
                 Vc += V;
+                if (two_pass) {
+                    for (int k = 0; k < 8; ++k) {
+                        const int32_t q8 = static_cast<int32_t>(hp[k]);
+                        int32_t idx = where[q8];
+                        if (idx < 0) {
+                            idx = static_cast<int32_t>(cn[vtx].size());
+                            where[q8] = idx;
+                            cn[vtx].push_back(q8);
+                            cg[vtx].insert(cg[vtx].end(), {0.0, 0.0, 0.0});
+                        }
+                        for (int q = 0; q < 3; ++q) cg[vtx][idx * 3 + q] += B[k * 3 + q] * V;
+                    }
+                    continue;
+                }
                 for (int k = 0; k < 8; ++k)
                     for (int64_t e = c->nbr_ptr[hp[k]]; e < c->nbr_ptr[hp[k] + 1]; ++e) {
                         const int32_t j = c->nbr[e];
@@ -548,12 +571,17 @@ extern "C" {
 
 int am_rkpm_nodal_cells(int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R,
                         int32_t max_neighbors, double density, am_cells** out) {
-    return nodal_cells(N, X, T, tets, R, max_neighbors, density, false, out);
+    return nodal_cells(N, X, T, tets, R, max_neighbors, density, kOnePass, out);
 }
 
 int am_rkpm_nodal_subcells(int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R,
                            int32_t max_neighbors, double density, am_cells** out) {
-    return nodal_cells(N, X, T, tets, R, max_neighbors, density, true, out);
+    return nodal_cells(N, X, T, tets, R, max_neighbors, density, kSubcells, out);
+}
+
+int am_rkpm_nodal_cells_two_pass(int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R,
+                                 int32_t max_neighbors, double density, am_cells** out) {
+    return nodal_cells(N, X, T, tets, R, max_neighbors, density, kTwoPass, out);
 }
 
 }  // extern "C"

@@ -45,11 +45,12 @@ X = max-x face, ...), and "|tets" splits each hex into six tets (this library's 
 split; STK's own split is not available here). An .npz mesh holds `coords` (N x 3),
 `block_<name>` (E x 4 or E x 8, zero-based) and `set_<name>` (zero-based node ids).
 Element cells with the reproducing_kernel space use the two-pass method unless
-force_one_pass_method is set, nodal cells the one-pass method (the reference's defaults).
+force_one_pass_method is set, nodal cells the one-pass method unless force_two_pass_method is
+set (the reference's defaults and switches).
 Nodal cells with subdomains 0 split into one subcell per corner hex, and use_f_bar then
 applies F-bar over each vertex's subcells; with one subcell per cell (subdomains 1, or
 element cells) use_f_bar changes nothing, as in the reference. Anything else (Exodus
-meshes, two-pass nodal cells, other materials) raises InputError naming the key.
+meshes, two-pass nodal cells split into subcells, other materials) raises InputError naming the key.
 """
 from __future__ import annotations
 
@@ -388,14 +389,21 @@ def _part(pnode: dict, blocks: dict, coords, ext: dict, rng, formulation=("total
         part.name = name
         return part, mass, None
     if space == "reproducing_kernel" and cell == "nodal_smoothing_cell":
-        if not one_pass:
-            raise InputError("force_two_pass_method on nodal_smoothing_cell: two-pass nodal cells are not built")
         if mu_f is not None or kappa_f is not None:
             raise InputError("x_b200.fields on RKPM nodal cells: per-cell fields are not supported")
-        from .rkpm import nodal_cells, nodal_subcells, thex_max_edge_length
+        from .rkpm import nodal_cells, nodal_subcells, thex_max_edge_length, two_pass_nodal_cells
 
         scale = float((spnode or {}).get("kernel_radius_scale_factor", 1.0))
         radius = scale * thex_max_edge_length(coords, conn)
+        if not one_pass:
+            # force_two_pass_method: the vertex cells hold their corner-hex points, coupled to
+            # the vertices by the functions at every point of the thex refinement.
+            if sub < 1:
+                raise InputError("force_two_pass_method with nodal_smoothing_cell.subdomains 0: not built "
+                                 "(two-pass nodal cells integrate whole vertex cells)")
+            cells = two_pass_nodal_cells(coords, conn, mat, radius, max_neighbors=int(ext.get("max_neighbors", 40)),
+                                         name=name)
+            return cells.part, cells.mass, cells.functions()
         if sub < 1:
             cells = nodal_subcells(coords, conn, mat, radius, max_neighbors=int(ext.get("max_neighbors", 40)),
                                    fbar=use_f_bar)

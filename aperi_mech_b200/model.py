@@ -116,7 +116,9 @@ class ExplicitDynamics:
     def __init__(self, coords: np.ndarray, parts: list[Part], bcs: list[BoundaryCondition] = (),
                  body_accel=None, mass: np.ndarray | None = None, stream=None, rk=None, formulation=None):
         """rk = (nbr_ptr, nbr, values) sets the two-pass reproducing-kernel coupling
-        (set_rk_functions); mass is then the generalized lumped mass. formulation =
+        (set_rk_functions); mass is then the generalized lumped mass. With more rows than
+        nodes (two-pass nodal cells: one row per refinement point, the nodes first) the
+        cells index the points (am_set_rk_points). formulation =
         ('updated', 1) or ('semi', update_interval) selects the updated or semi-Lagrangian
         formulation of the Gauss blocks (FP64 runs only); None or ('total', ...) the total one."""
         self.lib = capi.load()
@@ -134,6 +136,9 @@ class ExplicitDynamics:
                 code = {"updated": 1, "semi": 2}[formulation[0]]
                 interval = int(formulation[1]) if len(formulation) > 1 else 1
                 check(self.lib.am_set_formulation(self.ctx, code, interval), self.ctx)
+            if rk is not None and len(rk[0]) - 1 > self.N:
+                # functions with a row per refinement point: the cells index the points
+                check(self.lib.am_set_rk_points(self.ctx, len(rk[0]) - 1), self.ctx)
             for p in self.parts:
                 self._add_part(p)
             if bcs:
@@ -328,12 +333,14 @@ class ExplicitDynamics:
         """Two-pass reproducing-kernel coupling: the state holds generalized coefficients,
         the blocks run on the physical displacement Psi u and their forces reach the
         coefficients as Psi^T f. Row i of Psi: values[nbr_ptr[i]:nbr_ptr[i+1]] at the
-        neighbours nbr[...] of node i (rkpm.RKPMCells.functions())."""
+        neighbours nbr[...] of point i, one row per node or, for two-pass nodal cells, per
+        refinement point with the nodes first (rkpm.RKPMCells.functions())."""
         ptr = np.ascontiguousarray(nbr_ptr, dtype=np.int64)
         nb = np.ascontiguousarray(nbr, dtype=np.int32)
         val = np.ascontiguousarray(values, dtype=np.float64)
-        if ptr.size != self.N + 1 or nb.size != val.size or nb.size != ptr[-1]:
-            raise ValueError("nbr_ptr needs num_nodes + 1 offsets and nbr/values nbr_ptr[-1] entries")
+        if ptr.size < self.N + 1 or nb.size != val.size or nb.size != ptr[-1]:
+            raise ValueError("nbr_ptr needs one offset per point plus one (the nodes first) and nbr/values "
+                             "nbr_ptr[-1] entries")
         check(self.lib.am_set_rk_functions(self.ctx, capi._ptr(ptr, C.c_int64), capi._ptr(nb, C.c_int32),
                                            capi._ptr(val)), self.ctx)
 

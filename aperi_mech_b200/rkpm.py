@@ -36,8 +36,9 @@ class RKPMCells:
         coupling (element cells: the points are the vertices)."""
         if self.nbr_ptr is None:
             raise ValueError("built without keep_points")
-        if self.points is not None and self.points.shape[0] != self.mass.shape[0]:
-            raise ValueError("the functions live on refinement points, not on the mesh nodes")
+        if self.points is not None and self.points.shape[0] != self.mass.shape[0] and \
+                int(self.part.cell_nodes.max()) < self.mass.shape[0]:
+            raise ValueError("the functions live on refinement points the cells do not use")
         return self.nbr_ptr, self.nbr, self.values
 
 
@@ -88,6 +89,17 @@ def nodal_subcells(coords: np.ndarray, tets: np.ndarray, material: Material, ker
                   mu_field, kappa_field, name, groups=fbar)
 
 
+def two_pass_nodal_cells(coords: np.ndarray, tets: np.ndarray, material: Material, kernel_radius: np.ndarray,
+                         max_neighbors: int = 40, mu_field=None, kappa_field=None,
+                         name: str = "block_1") -> RKPMCells:
+    """Two-pass nodal cells (nodal_smoothing_cell with force_two_pass_method): the vertex
+    cells' entries are their corner-hex points with the hexes' own smoothed gradients;
+    functions() then returns one row per point (the vertices first), which
+    ExplicitDynamics(..., rk=cells.functions()) takes as the coupling."""
+    return _cells("am_rkpm_nodal_cells_two_pass", coords, tets, material, kernel_radius, max_neighbors, True,
+                  mu_field, kappa_field, name)
+
+
 def element_cells(coords: np.ndarray, tets: np.ndarray, material: Material, kernel_radius: np.ndarray,
                   max_neighbors: int = 40, keep_points: bool = False, mu_field=None, kappa_field=None,
                   name: str = "block_1") -> RKPMCells:
@@ -113,14 +125,15 @@ def two_pass_element_cells(coords: np.ndarray, tets: np.ndarray, material: Mater
 
 
 def apply_functions(functions, d: np.ndarray) -> np.ndarray:
-    """Physical field Psi d at the nodes from generalized coefficients d (N x 3): row i
-    sums psi_j(x_i) d_j over its neighbours; a row without neighbours copies d_i."""
+    """Physical field Psi d at the points (the nodes, or the refinement points with the
+    nodes first) from generalized coefficients d (N x 3): row i sums psi_j(x_i) d_j over
+    its neighbours; a node row without neighbours copies d_i, any other empty row is 0."""
     ptr, nbr, val = (np.asarray(a) for a in functions)
     d = np.asarray(d, dtype=np.float64)
     counts = np.diff(ptr)
-    out = np.zeros_like(d)
+    out = np.zeros((counts.size,) + d.shape[1:])
     np.add.at(out, np.repeat(np.arange(counts.size), counts), val[:, None] * d[nbr])
-    empty = counts == 0
+    empty = np.nonzero(counts[: d.shape[0]] == 0)[0]
     out[empty] = d[empty]
     return out
 

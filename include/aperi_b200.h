@@ -199,6 +199,17 @@ int am_rkpm_nodal_subcells(int64_t num_nodes, const double* coords, int64_t num_
 int am_cells_groups(const am_cells* cells, int64_t* num_groups, int64_t* group_ptr);
 int am_rkpm_element_cells(int64_t num_nodes, const double* coords, int64_t num_tets, const int32_t* tets,
                           const double* kernel_radius, int32_t max_neighbors, double density, am_cells** out);
+/* Two-pass nodal cells (nodal_smoothing_cell with force_two_pass_method,
+ * InternalForceContributionParameters.h:164-194; ExplicitSolver::ComputeForce's two
+ * passes, src/Solvers/Explicit.cpp:146-186): the vertex cells of am_rkpm_nodal_cells,
+ * whose entries are now their corner-hex points (point ids; the first num_nodes points
+ * are the vertices) with the hexes' own smoothed gradients b_p = sum_hex B_hex(p) V_hex /
+ * V_cell (SmoothedCellDataProcessor.h:541-675 without the functions). The functions at
+ * all points (am_cells_get_points) couple them to the vertices at run time: declare the
+ * points with am_set_rk_points before am_add_block, add the cells, pass the mass (as
+ * above) to am_set_mass, finalize, then hand the functions to am_set_rk_functions. */
+int am_rkpm_nodal_cells_two_pass(int64_t num_nodes, const double* coords, int64_t num_tets, const int32_t* tets,
+                                 const double* kernel_radius, int32_t max_neighbors, double density, am_cells** out);
 /* The same for Hex8 elements (ElementReproducingKernelHex8 with element_smoothing_cell, the
  * reference's rkpm_hex inputs): one cell per hex (reference node order), gradients from the
  * smoothed Hex8 quadrature (QuadratureSmoothed.h:97-142) through the vertices' functions,
@@ -357,6 +368,12 @@ int am_set_formulation(am_ctx* ctx, int32_t formulation, int32_t update_interval
  * am_cells_get returns it) from am_set_mass before am_finalize; call once after
  * am_finalize. Not available with the VJP, the adjoint or a decomposed mesh (AM_ESTATE). */
 int am_set_rk_functions(am_ctx* ctx, const int64_t* nbr_ptr, const int32_t* nbr, const double* values);
+/* Points for cells coupled through the functions (two-pass nodal cells): the cell entries
+ * of this context then index num_points points, the first num_nodes being the nodes and
+ * the rest refinement points. The functions of am_set_rk_functions then have one row per
+ * point (nbr_ptr of num_points + 1), the physical displacement lives on the points and
+ * the cells' forces reach the nodes through the functions' transpose. Before am_add_block. */
+int am_set_rk_points(am_ctx* ctx, int64_t num_points);
 
 /* ---- domain decomposition (replaces the reference's ParallelSum of the force field
  * after the element loop, src/Solvers/Explicit.cpp:190-193) ----

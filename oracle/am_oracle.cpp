@@ -895,12 +895,15 @@ void ob_internal_force(const ob_problem* p, const double* u, double* f) {
     // Physical displacement from the coefficients (FunctionEvaluationProcessor::ComputeValues,
     // include/FunctionEvaluationProcessor.h:86-121): a row without neighbours copies its
     // coefficient, others sum psi * coefficient over the neighbours in reverse order.
-    std::vector<double> up(N * 3), fl(N * 3, 0.0);
-    for (int64_t i = 0; i < N; ++i) {
+    // With more points than nodes (two-pass nodal cells) a point without neighbours past
+    // the nodes has no coefficient to copy: it stays at zero and its force is dropped.
+    const int64_t P = p->rk_rows > 0 ? p->rk_rows : N;
+    std::vector<double> up(P * 3), fl(P * 3, 0.0);
+    for (int64_t i = 0; i < P; ++i) {
         const int64_t b = p->rk_ptr[i], e = p->rk_ptr[i + 1];
         for (int c = 0; c < 3; ++c) {
             if (b == e) {
-                up[i * 3 + c] = u[i * 3 + c];
+                up[i * 3 + c] = i < N ? u[i * 3 + c] : 0.0;
                 continue;
             }
             double s = 0.0;
@@ -912,10 +915,11 @@ void ob_internal_force(const ob_problem* p, const double* u, double* f) {
     // Local forces scattered to the coefficients (ScatterValues, :130-174): psi_j(x_i) f_i
     // added to node j; a row without neighbours passes its force through. The reference
     // adds with atomics in no fixed order; here the sum for each node runs over i ascending.
-    for (int64_t i = 0; i < N; ++i) {
+    for (int64_t i = 0; i < P; ++i) {
         const int64_t b = p->rk_ptr[i], e = p->rk_ptr[i + 1];
         if (b == e) {
-            for (int c = 0; c < 3; ++c) f[i * 3 + c] += fl[i * 3 + c];
+            if (i < N)
+                for (int c = 0; c < 3; ++c) f[i * 3 + c] += fl[i * 3 + c];
             continue;
         }
         for (int64_t k = b; k < e; ++k)
@@ -1382,11 +1386,17 @@ void thex_functions(int64_t N, const double* X, const double* R, int32_t max_nei
 
 }  // namespace
 
-extern "C" int ob_rkpm_nodal_cells(int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R,
-                                   int32_t max_neighbors, double density, int64_t* num_points, int64_t* num_nbr_entries,
-                                   int64_t* num_cell_entries, double* points, int64_t* nbr_ptr, int32_t* nbr,
-                                   double* values, int64_t* cell_ptr, int32_t* cell_nodes, double* cell_grads,
-                                   double* cell_volumes, double* mass) {
+namespace {
+
+// Nodal cells of the thex refinement, one-pass or two-pass. One-pass: a vertex cell's
+// entries are the union of its corner-hex points' neighbours, b_j = sum_hex sum_k B_hex,k
+// V_hex psi_k(j) / V_cell. Two-pass (SmoothedCellDataProcessor.h:541-675 without the
+// functions): the entries are the corner-hex points themselves, b_p = sum_hex B_hex,k(p)
+// V_hex / V_cell, and the functions couple the points to the vertices at run time.
+int nodal_cells(bool two_pass, int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R,
+                int32_t max_neighbors, double density, int64_t* num_points, int64_t* num_nbr_entries,
+                int64_t* num_cell_entries, double* points, int64_t* nbr_ptr, int32_t* nbr, double* values,
+                int64_t* cell_ptr, int32_t* cell_nodes, double* cell_grads, double* cell_volumes, double* mass) {
     const ThexPoints tp = thex_points(N, X, T, tets);
     const int64_t P = static_cast<int64_t>(tp.xyz.size() / 3);
     std::vector<int64_t> ptr;
@@ -1401,7 +1411,7 @@ extern "C" int ob_rkpm_nodal_cells(int64_t N, const double* X, int64_t T, const 
     std::vector<std::vector<double>> cg(N);
     std::vector<double> cv(N, 0.0), mfe(P, 0.0);
     for (int32_t v = 0; v < N; ++v) {
-        std::vector<int32_t> where(N, -1);
+        std::vector<int32_t> where(two_pass ? P : N, -1);
         for (const auto& ti : corners[v]) {
             int64_t hp[8];
             corner_hex(tp, X, tets + 4 * ti.first, ti.first, ti.second, hp);
@@ -1411,6 +1421,18 @@ extern "C" int ob_rkpm_nodal_cells(int64_t N, const double* X, int64_t T, const 
             ob_hex8_smoothed_bw(hx, B, &V);
             cv[v] += V;
             for (int k = 0; k < 8; ++k) mfe[hp[k]] += V * density / 8;
+            if (two_pass) {
+                for (int k = 0; k < 8; ++k) {
+                    const int32_t q = static_cast<int32_t>(hp[k]);
+                    if (where[q] < 0) {
+                        where[q] = static_cast<int32_t>(cn[v].size());
+                        cn[v].push_back(q);
+                        cg[v].insert(cg[v].end(), {0.0, 0.0, 0.0});
+                    }
+                    for (int c = 0; c < 3; ++c) cg[v][where[q] * 3 + c] += B[k * 3 + c] * V;
+                }
+                continue;
+            }
             for (int k = 0; k < 8; ++k)
                 for (int64_t s = ptr[hp[k]]; s < ptr[hp[k] + 1]; ++s) {
                     const int32_t j = flat[s];
@@ -1450,6 +1472,27 @@ extern "C" int ob_rkpm_nodal_cells(int64_t N, const double* X, int64_t T, const 
             for (int64_t s = ptr[p]; s < ptr[p + 1]; ++s) mass[flat[s]] += mfe[p] * psi[s];
     }
     return 0;
+}
+
+}  // namespace
+
+extern "C" int ob_rkpm_nodal_cells(int64_t N, const double* X, int64_t T, const int32_t* tets, const double* R,
+                                   int32_t max_neighbors, double density, int64_t* num_points, int64_t* num_nbr_entries,
+                                   int64_t* num_cell_entries, double* points, int64_t* nbr_ptr, int32_t* nbr,
+                                   double* values, int64_t* cell_ptr, int32_t* cell_nodes, double* cell_grads,
+                                   double* cell_volumes, double* mass) {
+    return nodal_cells(false, N, X, T, tets, R, max_neighbors, density, num_points, num_nbr_entries, num_cell_entries,
+                       points, nbr_ptr, nbr, values, cell_ptr, cell_nodes, cell_grads, cell_volumes, mass);
+}
+
+extern "C" int ob_rkpm_nodal_cells_two_pass(int64_t N, const double* X, int64_t T, const int32_t* tets,
+                                            const double* R, int32_t max_neighbors, double density,
+                                            int64_t* num_points, int64_t* num_nbr_entries, int64_t* num_cell_entries,
+                                            double* points, int64_t* nbr_ptr, int32_t* nbr, double* values,
+                                            int64_t* cell_ptr, int32_t* cell_nodes, double* cell_grads,
+                                            double* cell_volumes, double* mass) {
+    return nodal_cells(true, N, X, T, tets, R, max_neighbors, density, num_points, num_nbr_entries, num_cell_entries,
+                       points, nbr_ptr, nbr, values, cell_ptr, cell_nodes, cell_grads, cell_volumes, mass);
 }
 
 // Nodal cells split into subcells (subdomains 0): each corner hex keeps its own entries

@@ -77,12 +77,16 @@ typedef struct {
     const ob_bc* bcs;
     const double* mass;    /* lumped nodal mass, or NULL = from Gauss blocks */
     double body_accel[3];  /* gravity vector (ExternalForceContributionGravity) */
-    /* Two-pass reproducing-kernel coupling, or NULL: row i of Psi (rk_ptr num_nodes+1,
-     * rk_nbr / rk_values) holds the functions psi_j(x_i). The blocks then see the
-     * physical displacement Psi u and their forces reach the nodes as Psi^T f. */
+    /* Two-pass reproducing-kernel coupling, or NULL: row i of Psi (rk_ptr rk_rows+1,
+     * rk_nbr / rk_values) holds the functions psi_j(x_i) at point i. The blocks then see
+     * the physical displacement Psi u at the points and their forces reach the nodes as
+     * Psi^T f. rk_rows = 0 means one point per node (element cells: the points are the
+     * nodes); more points than nodes are the thex refinement points of two-pass nodal
+     * cells, the first num_nodes of them the nodes. Cell entries index the points. */
     const int64_t* rk_ptr;
     const int32_t* rk_nbr;
     const double* rk_values;
+    int64_t rk_rows;
 } ob_problem;
 
 /* ---- quadrature (QuadratureGaussian.h, QuadratureSmoothed.h) ---- */
@@ -134,6 +138,17 @@ int ob_rkpm_nodal_cells(int64_t num_nodes, const double* coords, int64_t num_tet
                         double* points, int64_t* nbr_ptr, int32_t* nbr, double* values,
                         int64_t* cell_ptr, int32_t* cell_nodes, double* cell_grads, double* cell_volumes,
                         double* mass);
+
+/* The two-pass form of the same cells (force_two_pass_method with nodal_smoothing_cell):
+ * a vertex cell's entries are its corner-hex points (point ids, the first num_nodes
+ * points being the vertices) with the hexes' own smoothed gradients b_p = sum_hex
+ * B_hex,k(p) V_hex / V_cell; points, functions and mass as above. */
+int ob_rkpm_nodal_cells_two_pass(int64_t num_nodes, const double* coords, int64_t num_tets, const int32_t* tets,
+                                 const double* kernel_radius, int32_t max_neighbors, double density,
+                                 int64_t* num_points, int64_t* num_nbr_entries, int64_t* num_cell_entries,
+                                 double* points, int64_t* nbr_ptr, int32_t* nbr, double* values,
+                                 int64_t* cell_ptr, int32_t* cell_nodes, double* cell_grads, double* cell_volumes,
+                                 double* mass);
 
 /* RKPM one-pass element smoothing cells (each tet a cell; functions at the vertices).
  * Two calls: sizes first (outputs NULL), then the arrays: the vertices' neighbour CSR

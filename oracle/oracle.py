@@ -64,7 +64,7 @@ class OBC(C.Structure):
 class OProblem(C.Structure):
     _fields_ = [("num_nodes", C.c_int64), ("coords", _dp), ("num_blocks", C.c_int32), ("blocks", C.POINTER(OBlock)),
                 ("num_bcs", C.c_int32), ("bcs", C.POINTER(OBC)), ("mass", _dp), ("body_accel", C.c_double * 3),
-                ("rk_ptr", _lp), ("rk_nbr", _ip), ("rk_values", _dp)]
+                ("rk_ptr", _lp), ("rk_nbr", _ip), ("rk_values", _dp), ("rk_rows", C.c_int64)]
 
 
 def build() -> Path:
@@ -102,6 +102,8 @@ def lib() -> C.CDLL:
         L.ob_rk_function_values.argtypes = [C.c_int64, _dp, _dp, _dp, _lp, _ip, _dp]
         L.ob_rkpm_nodal_cells.argtypes = [C.c_int64, _dp, C.c_int64, _ip, _dp, C.c_int32, C.c_double, _lp, _lp, _lp,
                                           _dp, _lp, _ip, _dp, _lp, _ip, _dp, _dp, _dp]
+        L.ob_rkpm_nodal_cells_two_pass.argtypes = [C.c_int64, _dp, C.c_int64, _ip, _dp, C.c_int32, C.c_double, _lp,
+                                                   _lp, _lp, _dp, _lp, _ip, _dp, _lp, _ip, _dp, _dp, _dp]
         L.ob_rkpm_element_cells.argtypes = [C.c_int64, _dp, C.c_int64, _ip, _dp, C.c_int32, C.c_double, _lp, _lp,
                                             _lp, _ip, _dp, _lp, _ip, _dp, _dp, _dp]
         L.ob_rkpm_nodal_subcells.argtypes = [C.c_int64, _dp, C.c_int64, _ip, _dp, C.c_int32, C.c_double, _lp, _lp,
@@ -175,8 +177,9 @@ class OracleProblem:
                           (C.c_double * 3)(*body_accel))
         if rk is not None:
             ptr, nbr, val = (self._arr(a, t) for a, t in zip(rk, (np.int64, np.int32, np.float64)))
-            assert ptr.size == self.N + 1 and nbr.size == val.size == ptr[-1]
+            assert ptr.size >= self.N + 1 and nbr.size == val.size == ptr[-1]
             self.s.rk_ptr, self.s.rk_nbr, self.s.rk_values = _p(ptr, C.c_int64), _p(nbr, C.c_int32), _p(val)
+            self.s.rk_rows = ptr.size - 1
 
     def _arr(self, a, dt):
         if a is None:
@@ -320,24 +323,25 @@ def smoothed_bw(kind: str, X):
     return B, w.value
 
 
-def rkpm_nodal_cells(coords, tets, kernel_radius, max_neighbors=40, density=1000.0):
+def rkpm_nodal_cells(coords, tets, kernel_radius, max_neighbors=40, density=1000.0, two_pass=False):
     """Oracle RKPM nodal cells: dict with points, nbr_ptr, nbr, values, cell_ptr, cell_nodes,
-    cell_grads, cell_volumes, mass."""
+    cell_grads, cell_volumes, mass. two_pass: the cells hold the corner-hex points with
+    their own smoothed gradients (the entries index the points)."""
     X = np.ascontiguousarray(coords, dtype=np.float64)
     T = np.ascontiguousarray(tets, dtype=np.int32)
     R = np.ascontiguousarray(kernel_radius, dtype=np.float64)
     P, S, K = C.c_int64(), C.c_int64(), C.c_int64()
     args = (X.shape[0], _p(X), T.shape[0], _p(T, C.c_int32), _p(R), int(max_neighbors), float(density))
-    lib().ob_rkpm_nodal_cells(*args, C.byref(P), C.byref(S), C.byref(K), *([None] * 9))
+    fn = lib().ob_rkpm_nodal_cells_two_pass if two_pass else lib().ob_rkpm_nodal_cells
+    fn(*args, C.byref(P), C.byref(S), C.byref(K), *([None] * 9))
     N = X.shape[0]
     out = {"points": np.empty((P.value, 3)), "nbr_ptr": np.empty(P.value + 1, dtype=np.int64),
            "nbr": np.empty(S.value, dtype=np.int32), "values": np.empty(S.value),
            "cell_ptr": np.empty(N + 1, dtype=np.int64), "cell_nodes": np.empty(K.value, dtype=np.int32),
            "cell_grads": np.empty((K.value, 3)), "cell_volumes": np.empty(N), "mass": np.empty(N)}
-    lib().ob_rkpm_nodal_cells(*args, None, None, None, _p(out["points"]), _p(out["nbr_ptr"], C.c_int64),
-                              _p(out["nbr"], C.c_int32), _p(out["values"]), _p(out["cell_ptr"], C.c_int64),
-                              _p(out["cell_nodes"], C.c_int32), _p(out["cell_grads"]), _p(out["cell_volumes"]),
-                              _p(out["mass"]))
+    fn(*args, None, None, None, _p(out["points"]), _p(out["nbr_ptr"], C.c_int64), _p(out["nbr"], C.c_int32),
+       _p(out["values"]), _p(out["cell_ptr"], C.c_int64), _p(out["cell_nodes"], C.c_int32), _p(out["cell_grads"]),
+       _p(out["cell_volumes"]), _p(out["mass"]))
     return out
 
 

@@ -546,3 +546,42 @@ def test_neighbor_exchange_single_rank_self_neighbor(gpu, prec, monkeypatch):
         assert np.array_equal(f[~mask], f_plain[~mask])
     for a, b in zip(runs["1"], runs["0"]):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("name", ["tet4_nh", "hex8_le", "cells"])
+def test_graph_replay_is_bitwise_identical(gpu, monkeypatch, name):
+    """The step loop replayed from captured CUDA graphs (chunks of 32 steps, captured at
+    the end of a precision's first run and replayed from its second) gives bitwise the
+    same states as the same runs launched kernel by kernel (APERI_B200_GRAPHS=0). A body
+    acceleration set between runs (a kernel argument of the node kernel) reaches the
+    replayed steps: the setter drops the captured graphs."""
+    import ctypes as C
+
+    from aperi_mech_b200 import problems
+    from aperi_mech_b200.model import ExplicitDynamics
+
+    p = _small_problem(name) if name != "cells" else problems.smoothed_tet4_box(n=4, seed=2, nsteps=80)
+    mass = p.meta.get("mass")
+    g = np.array([0.0, -3.0e2, 1.0e2])
+    out = {}
+    for graphs in ("1", "0"):
+        monkeypatch.setenv("APERI_B200_GRAPHS", graphs)
+        res = []
+        with ExplicitDynamics(p.coords, p.parts, p.bcs, mass=mass) as m:
+            for prec in ("fp64", "mixed"):
+                for k in range(3):  # the second and third runs of a precision replay a graph
+                    if k == 2:
+                        rc = m.lib.am_set_body_acceleration(m.ctx, g.ctypes.data_as(C.POINTER(C.c_double)))
+                        assert rc == 0
+                    m.set_state(None, p.v0)
+                    m.init_acceleration(prec)
+                    m.run(75, p.dt, prec)
+                    res.append(m.get_state())
+                rc = m.lib.am_set_body_acceleration(m.ctx, np.zeros(3).ctypes.data_as(C.POINTER(C.c_double)))
+                assert rc == 0
+        out[graphs] = res
+    # the body acceleration changed the third run's state
+    assert not np.array_equal(out["0"][1][0], out["0"][2][0])
+    for a, b in zip(out["1"], out["0"]):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)

@@ -185,7 +185,7 @@ def test_output_steps_follow_the_solver_loop():
                        "strain_smoothing: {element_smoothing_cell: {subdomains: 1}, force_one_pass_method: true, "
                        "force_two_pass_method: true}"), "Cannot force both"),
     (nh_yaml().replace("gauss_quadrature: {integration_order: 1}",
-                       "strain_smoothing: {nodal_smoothing_cell: {subdomains: 1}, force_two_pass_method: true}").replace(
+                       "strain_smoothing: {nodal_smoothing_cell: {subdomains: 0}, force_two_pass_method: true}").replace(
         "finite_element: ~", "reproducing_kernel: {kernel_radius_scale_factor: 1.1}"), "two-pass nodal"),
 ])
 def test_rejected_inputs(text, msg):
@@ -277,6 +277,30 @@ def test_yaml_rkpm_two_pass_default_matches_oracle(oracle_lib, precision):
 
     up = apply_functions(sim.rk, u)
     assert np.linalg.norm(r["physical_displacement"] - up) <= tol * np.linalg.norm(up)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_yaml_rkpm_two_pass_nodal_cells_match_oracle(oracle_lib, precision):
+    """nodal_smoothing_cell with reproducing_kernel and force_two_pass_method: the vertex
+    cells of the thex refinement hold their corner-hex points, coupled to the coefficients
+    through the functions at every point (one row per point), against the oracle given them."""
+    text = nh_yaml(n=3, extra=f"""      x_b200:
+        precision: {precision}
+""").replace(
+        "gauss_quadrature: {integration_order: 1}",
+        "strain_smoothing: {nodal_smoothing_cell: {subdomains: 1}, force_two_pass_method: true}").replace(
+        "finite_element: ~", "reproducing_kernel: {kernel_radius_scale_factor: 1.1}")
+    sim = inp.load(text)
+    N = sim.coords.shape[0]
+    assert sim.rk is not None and len(sim.rk[0]) - 1 > N and sim.parts[0].num_elems == N
+    r = inp.run(sim)
+    prob = oracle_lib.OracleProblem(sim.coords, sim.parts, sim.bcs, mass=sim.mass, rk=sim.rk)
+    u, v, a, n = prob.solve(np.zeros_like(sim.coords), sim.v0, sim.dt, sim.time_end)
+    assert r["steps"] == n
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    assert np.linalg.norm(r["displacement"] - u) <= tol * np.linalg.norm(u)
+    assert r["physical_displacement"].shape[0] == len(sim.rk[0]) - 1
 
 
 @pytest.mark.gpu

@@ -392,3 +392,100 @@ def test_rk_hex8_element_cells_match_oracle(gpu, oracle_lib, method):
         got = m.get_state()
     for g, w in zip(got, want_state):
         assert rel_err(g, w) < 1e-12
+
+
+# ---- two-pass method on nodal cells (force_two_pass_method with nodal_smoothing_cell) ---
+def _two_pass_nodal(oracle_lib, X, T, mat, R):
+    """Oracle two-pass nodal cells: the cells over the thex points, the functions at the
+    points (P rows), the generalized mass at the vertices."""
+    from aperi_mech_b200.model import Part
+
+    r = oracle_lib.rkpm_nodal_cells(X, T, R, max_neighbors=40, density=mat.density, two_pass=True)
+    part = Part("cells", mat, cell_ptr=r["cell_ptr"], cell_nodes=r["cell_nodes"], cell_grads=r["cell_grads"],
+                cell_volumes=r["cell_volumes"])
+    return part, r["mass"], (r["nbr_ptr"], r["nbr"], r["values"]), r["points"]
+
+
+def _dense_rect(rk, P, N):
+    ptr, nb, v = rk
+    Psi = np.zeros((P, N))
+    np.add.at(Psi, (_rows(ptr), nb), v)
+    return Psi
+
+
+def test_oracle_two_pass_nodal_cells(oracle_lib):
+    """Two-pass nodal cells: each vertex cell holds its corner-hex points with the hexes'
+    smoothed gradients (partition of nullity: they sum to zero; a linear field gives its
+    gradient exactly), the first N points are the vertices, and f = Psi^T F_fem(Psi d)
+    with Psi the P x N functions at the points; the work identity d . f = (Psi d) . F_fem."""
+    from aperi_mech_b200.model import Material
+
+    X, T = _box(n=3, seed=8)
+    N = X.shape[0]
+    R = np.full(N, 1.8 / 3)
+    mat = Material.create("neo_hookean", 1000.0, shear_modulus=3.85e8, bulk_modulus=8.33e8)
+    part, mass, rk, points = _two_pass_nodal(oracle_lib, X, T, mat, R)
+    P = points.shape[0]
+    assert P > N and np.array_equal(points[:N], X)
+    assert part.cell_nodes.max() < P
+    ptr, g = part.cell_ptr, part.cell_grads
+    A = np.array([[0.3, -0.1, 0.2], [0.05, 0.4, -0.3], [0.1, 0.2, -0.2]])
+    for c in range(N):
+        s = slice(ptr[c], ptr[c + 1])
+        assert np.abs(g[s].sum(axis=0)).max() < 1e-9 * np.abs(g[s]).max()
+        H = (points[part.cell_nodes[s]] @ A.T).T @ g[s]
+        assert np.abs(H - A).max() < 1e-11
+    Psi = _dense_rect(rk, P, N)
+    d = 1e-3 * np.random.default_rng(4).standard_normal(X.shape)
+    fem = oracle_lib.OracleProblem(points, [part]).internal_force(Psi @ d)
+    got = oracle_lib.OracleProblem(X, [part], mass=mass, rk=rk).internal_force(d)
+    assert rel_err(got, Psi.T @ fem) < 1e-13
+    assert abs(np.sum(got * d) - np.sum(fem * (Psi @ d))) < 1e-12 * np.abs(fem).max() * np.abs(d).max() * d.size
+    one = oracle_lib.rkpm_nodal_cells(X, T, R, max_neighbors=40, density=mat.density)
+    assert rel_err(mass, one["mass"]) < 1e-14
+
+
+@pytest.mark.gpu
+def test_rkpm_two_pass_nodal_force_and_steps_match_oracle(gpu, oracle_lib):
+    """Two-pass nodal cells through the library (set-up, P-row coupling, force, 20 steps
+    in FP64 and mixed) against the oracle at 1e-12 (FP64) and 1e-5 (mixed)."""
+    from aperi_mech_b200 import mesh
+    from aperi_mech_b200.model import BoundaryCondition, ExplicitDynamics, Material
+    from aperi_mech_b200.rkpm import two_pass_nodal_cells
+
+    X, T = _box(n=3, seed=9)
+    N = X.shape[0]
+    R = np.full(N, 1.8 / 3)
+    mat = Material.create("neo_hookean", 1000.0, shear_modulus=3.85e8, bulk_modulus=8.33e8)
+    cells = two_pass_nodal_cells(X, T, mat, R)
+    part, mass, rk, points = _two_pass_nodal(oracle_lib, X, T, mat, R)
+    assert np.array_equal(cells.points, points)
+    assert np.array_equal(cells.nbr_ptr, rk[0]) and np.array_equal(cells.nbr, rk[1])
+    assert rel_err(cells.values, rk[2]) < 1e-12
+    assert np.array_equal(cells.part.cell_ptr, part.cell_ptr) and np.array_equal(cells.part.cell_nodes, part.cell_nodes)
+    assert rel_err(cells.part.cell_grads, part.cell_grads) < 1e-12
+    assert rel_err(cells.part.cell_volumes, part.cell_volumes) < 1e-13
+    assert rel_err(cells.mass, mass) < 1e-12
+    bcs = [BoundaryCondition.fixed(mesh.side_sets(X)["surface_5"])]
+    op = oracle_lib.OracleProblem(X, [cells.part], bcs, mass=cells.mass, rk=cells.functions())
+    rng = np.random.default_rng(10)
+    d = 1e-4 * rng.standard_normal(X.shape)
+    v0 = rng.uniform(-0.01, 0.01, size=X.shape)
+    v0[bcs[0].nodes] = 0.0
+    dt = 2e-7
+    z = np.zeros_like(X)
+    want = op.steps(z, v0, op.init_acceleration(z), np.full(20, dt))
+    with ExplicitDynamics(X, [cells.part], bcs, mass=cells.mass, rk=cells.functions()) as m:
+        assert rel_err(m.internal_force(d), op.internal_force(d)) < 1e-12
+        assert rel_err(m.internal_force(d, "mixed"), op.internal_force(d)) < 1e-5
+        m.set_state(None, v0)
+        m.init_acceleration()
+        m.run(20, dt)
+        got = m.get_state()
+        m.set_state(None, v0)
+        m.init_acceleration("mixed")
+        m.run(20, dt, "mixed")
+        mixed = m.get_state()
+    for g, w in zip(got, want):
+        assert rel_err(g, w) < 1e-12
+    assert rel_err(mixed[0], want[0]) < 1e-5
