@@ -97,6 +97,78 @@ void nccl_check(ncclResult_t r, const char* what) {
     }
 }
 
+// Octet rows of the cell-stress form: items 8o .. 8o + 7 (cells, or nodes), item j with
+// entries ptr[j] .. ptr[j+1] whose partners (node, or cell) ascend. Rows are aligned by
+// offset (partner minus item: on a locality-numbered mesh consecutive items see the same
+// offsets, so a row's eight partners are consecutive) when that pads by at most 35% over
+// the octet's entries; otherwise each item's entries fill rows from the first. src holds,
+// per (row, item) at 8 row + item, the entry or -1 (padding).
+struct OctetRows {
+    std::vector<int32_t> ptr;
+    std::vector<int32_t> src;
+};
+
+OctetRows octet_rows(int64_t count, const std::vector<int32_t>& ptr, const std::vector<int32_t>& partner) {
+    OctetRows o;
+    const int64_t O = (count + 7) / 8;
+    o.ptr.reserve(O + 1);
+    o.ptr.push_back(0);
+    std::vector<int32_t> rowsrc;
+    for (int64_t q = 0; q < O; ++q) {
+        int32_t at[8], end[8];
+        int64_t total = 0, longest = 0;
+        for (int j = 0; j < 8; ++j) {
+            const int64_t item = 8 * q + j;
+            at[j] = item < count ? ptr[item] : 0;
+            end[j] = item < count ? ptr[item + 1] : 0;
+            total += end[j] - at[j];
+            longest = std::max<int64_t>(longest, end[j] - at[j]);
+        }
+        // aligned rows: merge the offset lists, a row per offset (times its largest multiplicity)
+        rowsrc.clear();
+        int32_t p[8];
+        std::copy(at, at + 8, p);
+        while (true) {
+            int64_t off = INT64_MAX;
+            for (int j = 0; j < 8; ++j)
+                if (p[j] < end[j]) off = std::min<int64_t>(off, int64_t(partner[p[j]]) - (8 * q + j));
+            if (off == INT64_MAX) break;
+            int32_t run[8], mult = 0;
+            for (int j = 0; j < 8; ++j) {
+                run[j] = 0;
+                while (p[j] + run[j] < end[j] && int64_t(partner[p[j] + run[j]]) - (8 * q + j) == off) ++run[j];
+                mult = std::max(mult, run[j]);
+            }
+            for (int32_t t = 0; t < mult; ++t)
+                for (int j = 0; j < 8; ++j) rowsrc.push_back(t < run[j] ? p[j] + t : -1);
+            for (int j = 0; j < 8; ++j) p[j] += run[j];
+        }
+        const int64_t aligned = static_cast<int64_t>(rowsrc.size()) / 8;
+        if (8 * aligned * 100 <= 135 * total) {
+            o.src.insert(o.src.end(), rowsrc.begin(), rowsrc.end());
+            o.ptr.push_back(o.ptr.back() + static_cast<int32_t>(aligned));
+        } else {
+            for (int64_t r = 0; r < longest; ++r)
+                for (int j = 0; j < 8; ++j) o.src.push_back(at[j] + r < end[j] ? static_cast<int32_t>(at[j] + r) : -1);
+            o.ptr.push_back(o.ptr.back() + static_cast<int32_t>(longest));
+        }
+        if (static_cast<int64_t>(o.src.size()) >= (int64_t(1) << 31)) fail(AM_ERANGE, "octet rows beyond int32 indexing");
+    }
+    return o;
+}
+
+float bits32(int32_t v) {
+    float f;
+    std::memcpy(&f, &v, sizeof f);
+    return f;
+}
+double bits64(int32_t v) {
+    const int64_t w = v;
+    double d;
+    std::memcpy(&d, &w, sizeof d);
+    return d;
+}
+
 struct Block {
     int32_t kind = 0;
     int32_t material = 0;
@@ -134,6 +206,24 @@ struct Block {
     uint32_t* patch_gather = nullptr;
     float* patch_dx32 = nullptr;
     double* patch_dx64 = nullptr;
+    // Cell-stress form of a generic cell block (no patches, no F-bar groups, cells of more
+    // than eight entries): octet row records of the cells and of the nodes the block
+    // touches (one logical slot each), a node of each cell, and the per-cell matrices
+    // M = -V P of each precision.
+    bool gather = false;
+    int32_t unroll[2][2] = {{4, 2}, {4, 4}};  // [FP64, mixed][cell kernel, gather kernel]
+    int64_t num_octets = 0, num_node_octets = 0, t_count = 0;
+    int32_t* o_ptr = nullptr;
+    int32_t* n_ptr = nullptr;
+    int32_t* c_ref = nullptr;
+    float4* orec32 = nullptr;
+    double4* orec64 = nullptr;
+    float4* nrec32 = nullptr;
+    double4* nrec64 = nullptr;
+    float* cmat32 = nullptr;
+    double* cmat64 = nullptr;
+    std::vector<int32_t> host_cell_ptr;  // until am_finalize: the CSR and gradients the records
+    std::vector<double> host_grads;      // are built from
     const int32_t* slot_pos = nullptr;  // block-local view into the context's position array
     std::vector<int32_t> host_nodes;    // node of each logical slot (-1: unused), for the node CSR
     // Processing order of a Gauss block's elements: order[k] is the caller's index of the
@@ -203,11 +293,30 @@ struct Block {
         c.group_ptr = group_ptr;
         c.max_group = max_group;
         c.fused = fbar_fused && max_group <= 32 ? 1 : 0;  // kFbarMaxSub
+        c.gather = gather ? 1 : 0;
+        c.num_octets = num_octets;
+        c.o_ptr = o_ptr;
+        c.orec32 = orec32;
+        c.orec64 = orec64;
+        c.c_ref = c_ref;
+        c.t_count = t_count;
+        c.num_node_octets = num_node_octets;
+        c.n_ptr = n_ptr;
+        c.nrec32 = nrec32;
+        c.nrec64 = nrec64;
+        c.cmat = cmat64;
+        c.unroll[0] = unroll[0][0];
+        c.unroll[1] = unroll[0][1];
         return c;
     }
     // The device view for a force evaluation at the given precision (F-bar scratch attached).
     am::CellBlockDev cells_for(int mixed) {
         am::CellBlockDev c = cells();
+        if (gather) {
+            c.cmat = mixed ? static_cast<void*>(cmat32) : static_cast<void*>(cmat64);
+            c.unroll[0] = unroll[mixed ? 1 : 0][0];
+            c.unroll[1] = unroll[mixed ? 1 : 0][1];
+        }
         if (group_ptr && !c.fused) {
             const size_t n = static_cast<size_t>(std::max<int64_t>(num_elems, 1)) * am::kFbarStride;
             if (mixed) {
@@ -241,6 +350,93 @@ struct Block {
         dfree(group_ptr);
         dfree(fbar64);
         dfree(fbar32);
+        dfree(o_ptr);
+        dfree(n_ptr);
+        dfree(c_ref);
+        dfree(orec32);
+        dfree(orec64);
+        dfree(nrec32);
+        dfree(nrec64);
+        dfree(cmat32);
+        dfree(cmat64);
+    }
+
+    // The cell-stress form's records (see above), built at am_finalize once the block is
+    // known to take no F-bar groups. A cell's entries run in ascending node, a node's in
+    // ascending cell; the block's logical slots become its nodes in ascending order.
+    void build_gather(int64_t num_points) {
+        const int64_t E = num_elems, K = num_entries;
+        std::vector<int32_t> cnt(num_points + 1, 0);
+        for (int64_t s = 0; s < K; ++s) ++cnt[host_nodes[s] + 1];
+        std::vector<int32_t> local(num_points, -1), nodes;
+        for (int64_t n = 0; n < num_points; ++n)
+            if (cnt[n + 1] > 0) {
+                local[n] = static_cast<int32_t>(nodes.size());
+                nodes.push_back(static_cast<int32_t>(n));
+            }
+        const int64_t T = static_cast<int64_t>(nodes.size());
+        // cell-major entries sorted by node (cperm: original entry of each sorted position)
+        std::vector<int32_t> cperm(K), cpart(K);
+        for (int64_t c = 0; c < E; ++c) {
+            const int32_t a = host_cell_ptr[c], z = host_cell_ptr[c + 1];
+            for (int32_t q = a; q < z; ++q) cperm[q] = q;
+            std::stable_sort(cperm.begin() + a, cperm.begin() + z,
+                             [&](int32_t x, int32_t y) { return host_nodes[x] < host_nodes[y]; });
+            for (int32_t q = a; q < z; ++q) cpart[q] = host_nodes[cperm[q]];
+        }
+        // node-major entries in ascending cell (tperm: original entry; tpart: cell)
+        std::vector<int32_t> tptr(T + 1, 0);
+        for (int64_t i = 0; i < T; ++i) tptr[i + 1] = tptr[i] + cnt[nodes[i] + 1];
+        std::vector<int32_t> fill(tptr.begin(), tptr.end() - 1), tperm(K), tpart(K);
+        for (int64_t c = 0; c < E; ++c)
+            for (int32_t s = host_cell_ptr[c]; s < host_cell_ptr[c + 1]; ++s) {
+                const int32_t k = fill[local[host_nodes[s]]]++;
+                tperm[k] = s;
+                tpart[k] = static_cast<int32_t>(c);
+            }
+        const OctetRows co = octet_rows(E, host_cell_ptr, cpart);
+        const OctetRows no = octet_rows(T, tptr, tpart);
+        auto records = [&](const OctetRows& o, const std::vector<int32_t>& perm, const std::vector<int32_t>& part,
+                           float4*& r32, double4*& r64, const char* what) {
+            const size_t R = o.src.size();
+            std::vector<float4> h32(R);
+            std::vector<double4> h64(R);
+            for (size_t q = 0; q < R; ++q) {
+                const int32_t e = o.src[q];
+                if (e < 0) {
+                    h32[q] = make_float4(0.f, 0.f, 0.f, bits32(-1));
+                    h64[q] = make_double4(0.0, 0.0, 0.0, bits64(-1));
+                    continue;
+                }
+                const double* g = host_grads.data() + 3 * static_cast<int64_t>(perm[e]);
+                h32[q] = make_float4(static_cast<float>(g[0]), static_cast<float>(g[1]), static_cast<float>(g[2]), bits32(part[e]));
+                h64[q] = make_double4(g[0], g[1], g[2], bits64(part[e]));
+            }
+            r32 = dalloc<float4>(std::max<size_t>(R, 1), what);
+            r64 = dalloc<double4>(std::max<size_t>(R, 1), what);
+            ck(cudaMemcpy(r32, h32.data(), R * sizeof(float4), cudaMemcpyHostToDevice), "upload");
+            ck(cudaMemcpy(r64, h64.data(), R * sizeof(double4), cudaMemcpyHostToDevice), "upload");
+        };
+        records(co, cperm, cpart, orec32, orec64, "cell octet records");
+        records(no, tperm, tpart, nrec32, nrec64, "node octet records");
+        // The mixed path's differences are taken against the cell's first entry as given
+        // (for nodal cells a node next to the cell's own), which keeps them small.
+        std::vector<int32_t> ref(E, -1);
+        for (int64_t c = 0; c < E; ++c)
+            if (host_cell_ptr[c + 1] > host_cell_ptr[c]) ref[c] = host_nodes[host_cell_ptr[c]];
+        num_octets = static_cast<int64_t>(co.ptr.size()) - 1;
+        num_node_octets = static_cast<int64_t>(no.ptr.size()) - 1;
+        o_ptr = dalloc<int32_t>(co.ptr.size(), "cell octet rows");
+        n_ptr = dalloc<int32_t>(no.ptr.size(), "node octet rows");
+        c_ref = dalloc<int32_t>(std::max<int64_t>(E, 1), "cell reference nodes");
+        cmat32 = dalloc<float>(std::max<int64_t>(9 * E, 1), "cell matrices (FP32)");
+        cmat64 = dalloc<double>(std::max<int64_t>(9 * E, 1), "cell matrices");
+        ck(cudaMemcpy(o_ptr, co.ptr.data(), co.ptr.size() * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+        ck(cudaMemcpy(n_ptr, no.ptr.data(), no.ptr.size() * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+        ck(cudaMemcpy(c_ref, ref.data(), E * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+        t_count = T;
+        host_nodes = std::move(nodes);
+        gather = true;
     }
 };
 
@@ -352,6 +548,13 @@ struct am_ctx {
     // Element processing order of Gauss blocks: the locality order chosen from the mesh
     // (element_order, the default) or, with APERI_B200_ELEMENT_ORDER=input, the caller's.
     bool locality_order = true;
+    // Generic cell blocks in the cell-stress form (per-cell M, node-major gather; the
+    // default) or, with APERI_B200_CELL_GATHER=0, with one force slot per entry.
+    // APERI_B200_CELL_UNROLL: rows per lane in flight in its kernels (see am_create).
+    bool cell_gather = true;
+    // The defaults measured fastest on the RKPM nodal cells of the h = 1/46 box: FP64 4 and
+    // 2 (the FP64 gather at 4 holds 128 registers), mixed 4 and 4.
+    int32_t cell_unroll[2][2] = {{4, 2}, {4, 4}};
     std::vector<double> host_X;  // coordinates (N x 3), for the element order at am_add_block
     am::StepParams* table = nullptr;
     int64_t table_cap = 0;
@@ -667,11 +870,12 @@ struct am_ctx {
         for (const auto& b : blocks) {
             double* gm = gmu ? gmu + off : nullptr;
             double* gk = gkappa ? gkappa + off : nullptr;
-            if (b.kind == AM_SMOOTHED_CELLS)
-                am::launch_cell_vjp(b.cells(), U, L, slots64, gm, gk, accumulate, stream);
-            else
+            if (b.kind == AM_SMOOTHED_CELLS) {
+                launches += am::launch_cell_vjp(b.cells(), U, L, slots64, gm, gk, accumulate, stream);
+            } else {
                 am::launch_gauss_vjp(b.gauss(), X4, U, L, slots64, gm, gk, accumulate, stream);
-            ++launches;
+                ++launches;
+            }
             off += b.num_elems;
         }
         check_launch("vjp kernel");
@@ -1119,6 +1323,12 @@ int am_create(int64_t num_nodes, const double* coords, am_ctx** out) {
         c->io_scratch = dalloc<double>(N * 3, "io scratch");
         const char* graphs = std::getenv("APERI_B200_GRAPHS");
         c->use_graphs = !(graphs && graphs[0] == '0');
+        const char* cg = std::getenv("APERI_B200_CELL_GATHER");
+        c->cell_gather = !(cg && cg[0] == '0');
+        // four digits: FP64 cell, FP64 gather, mixed cell, mixed gather kernel (1, 2 or 4)
+        const char* cu = std::getenv("APERI_B200_CELL_UNROLL");
+        for (int q = 0; cu && q < 4 && cu[q]; ++q)
+            c->cell_unroll[q / 2][q % 2] = cu[q] == '1' ? 1 : cu[q] == '2' ? 2 : 4;
         const char* order = std::getenv("APERI_B200_ELEMENT_ORDER");
         c->locality_order = !(order && std::strcmp(order, "input") == 0);
         c->host_X.assign(coords, coords + 3 * N);
@@ -1226,6 +1436,10 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
                     ck(cudaMemcpy(b.volumes, d->cell_volumes, E * sizeof(double), cudaMemcpyHostToDevice), "upload");
                 }
                 b.host_nodes.assign(d->cell_nodes, d->cell_nodes + K);
+                if (maxlen > 8 && ctx->cell_gather) {
+                    b.host_cell_ptr = ptr;
+                    b.host_grads.assign(d->cell_grads, d->cell_grads + 3 * K);
+                }
                 // Cells of four entries that group into split hexes (a tet mesh's element
                 // cells) run as patches like the Gauss tets: one slot per patch node.
                 bool four = E > 0 && ctx->tet4_patches == 2;
@@ -1454,8 +1668,23 @@ int am_finalize(am_ctx* ctx) {
     return guarded(ctx, [&] {
         if (ctx->finalized) fail(AM_ESTATE, "am_finalize called twice");
         if (ctx->blocks.empty()) fail(AM_EINVAL, "no blocks");
-        const int64_t N = ctx->N, S = ctx->num_slots, NP = ctx->points();
+        const int64_t N = ctx->N, NP = ctx->points();
         if (NP > N && !ctx->mass_set) fail(AM_ESTATE, "cells on refinement points need the generalized mass (am_set_mass)");
+        // Generic cell blocks without F-bar groups take the cell-stress form: one logical
+        // slot per node they touch instead of one per entry.
+        int64_t base = 0;
+        for (auto& b : ctx->blocks) {
+            if (!b.host_grads.empty() && b.patched == 0 && !b.group_ptr) {
+                std::memcpy(b.unroll, ctx->cell_unroll, sizeof b.unroll);
+                b.build_gather(NP);
+            }
+            std::vector<double>().swap(b.host_grads);
+            std::vector<int32_t>().swap(b.host_cell_ptr);
+            b.slot_base = base;
+            base += static_cast<int64_t>(b.host_nodes.size());
+        }
+        ctx->num_slots = base;
+        const int64_t S = ctx->num_slots;
         // Node-major slot layout: node (or point) i owns positions [ptr[i], ptr[i+1]); within
         // a node the positions follow ascending logical slot (block order, then element order).
         std::vector<int32_t> ptr(NP + 1, 0), pos(S, -1);

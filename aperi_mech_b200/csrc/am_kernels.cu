@@ -892,6 +892,198 @@ __global__ void __launch_bounds__(256) k_cell_force_group(CellBlockDev b, const 
 }
 
 // ---------------------------------------------------------------------------
+// Cell-stress form of the generic cell path (ComputeInternalForceSmoothedCell.h:416-442
+// with the scatter turned into a gather). The cell kernel writes per cell the nine values
+// M_c = -V_c P_c; the gather kernel then forms, for every node the block touches,
+// f_n = sum over its entries (c, b) of M_c b, in a fixed order, into the node's one slot.
+//
+// Both kernels run a warp per octet of eight consecutive items (cells, or nodes): lane
+// 8k + j takes item j of the octet and rows k, k + 4, ... of the octet's row list, so a
+// quarter-warp (the eight lanes the load unit serves together) reads one row of all eight
+// items. Set-up aligns the rows by offset (partner index minus item index) where that
+// pads little, so that on a locality-numbered mesh a quarter-warp's eight gathers hit
+// eight consecutive nodes or cells; rows hold packed records (gradient in x, y, z; the
+// partner index in w, -1 for padding), one 16-byte (FP32) or 32-byte (FP64) load each.
+// Per entry this reads a record twice (32 B mixed) instead of a record, a slot position
+// and a slot written and read back (52 B), and the per-node sums need no slot per entry.
+// M is stored as three component arrays (values 0-3, 4-7 and 8 of every cell), so that
+// the eight lanes of a quarter-warp read contiguous pieces.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int32_t rec_index(const float4& r) { return __float_as_int(r.w); }
+__device__ __forceinline__ int32_t rec_index(const double4& r) { return static_cast<int32_t>(__double_as_longlong(r.w)); }
+// Records are written once at set-up: the read-only path.
+__device__ __forceinline__ float4 ld_rec(const float4* p) { return __ldg(p); }
+__device__ __forceinline__ double4 ld_rec(const double4* p) { return ld_ro4(p); }
+template <typename T>
+__device__ __forceinline__ vec4_t<T> pad_rec() {
+    vec4_t<T> z;
+    z.x = z.y = z.z = T(0);
+    if constexpr (sizeof(T) == 4) {
+        z.w = __int_as_float(-1);
+    } else {
+        z.w = __longlong_as_double(-1LL);
+    }
+    return z;
+}
+template <typename T>
+__device__ __forceinline__ const vec4_t<T>* cell_recs(const CellBlockDev& b);
+template <>
+__device__ __forceinline__ const float4* cell_recs<float>(const CellBlockDev& b) { return b.orec32; }
+template <>
+__device__ __forceinline__ const double4* cell_recs<double>(const CellBlockDev& b) { return b.orec64; }
+template <typename T>
+__device__ __forceinline__ const vec4_t<T>* node_recs(const CellBlockDev& b);
+template <>
+__device__ __forceinline__ const float4* node_recs<float>(const CellBlockDev& b) { return b.nrec32; }
+template <>
+__device__ __forceinline__ const double4* node_recs<double>(const CellBlockDev& b) { return b.nrec64; }
+
+// Part k (0, 1, 2) of M_c in the component arrays of a block of E cells.
+template <typename T>
+__device__ __forceinline__ void store_cell_matrix(T* M, int64_t E, int64_t c, int k, const T (&m)[9]) {
+    if (k == 0) {
+        vec4_t<T> v;
+        v.x = m[0], v.y = m[1], v.z = m[2], v.w = m[3];
+        reinterpret_cast<vec4_t<T>*>(M)[c] = v;
+    } else if (k == 1) {
+        vec4_t<T> v;
+        v.x = m[4], v.y = m[5], v.z = m[6], v.w = m[7];
+        reinterpret_cast<vec4_t<T>*>(M + 4 * E)[c] = v;
+    } else if (k == 2) {
+        M[8 * E + c] = m[8];
+    }
+}
+template <typename T>
+__device__ __forceinline__ void load_cell_matrix(const T* M, int64_t E, int32_t c, T (&m)[9]) {
+    const vec4_t<T> a = ld_dep(reinterpret_cast<const vec4_t<T>*>(M) + c);
+    const vec4_t<T> b = ld_dep(reinterpret_cast<const vec4_t<T>*>(M + 4 * E) + c);
+    m[0] = a.x, m[1] = a.y, m[2] = a.z, m[3] = a.w, m[4] = b.x, m[5] = b.y, m[6] = b.z, m[7] = b.w;
+    m[8] = __ldca(M + 8 * E + c);
+}
+
+// Cell octets: H over the rows (UNR rows per lane in flight: the batch's displacement
+// gathers issued together, the next batch's records loaded while they are in flight),
+// combined over the four lanes of a cell, P(H), and M_c written by lanes k = 0, 1, 2.
+template <typename T, int MAT, int UNR>
+__global__ void __launch_bounds__(256) k_cell_stress(CellBlockDev b, const double4* __restrict__ U4, T* __restrict__ M,
+                                                     int* status) {
+    pdl_trigger();
+    const int64_t o = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = static_cast<int>(threadIdx.x & 31), j = lane & 7, k = lane >> 3;
+    const int64_t c = 8 * o + j;
+    const bool valid = c < b.num_cells;
+    const bool live = o < b.num_octets;
+    const int32_t r0 = live ? b.o_ptr[o] : 0, rows = live ? b.o_ptr[o + 1] - r0 : 0;
+    const vec4_t<T>* rec = cell_recs<T>(b) + 8 * static_cast<int64_t>(r0) + j;
+    const int32_t ref = valid ? b.c_ref[c] : -1;
+    const bool diff = sizeof(T) == 4;
+    vec4_t<T> rr[UNR];
+#pragma unroll
+    for (int u = 0; u < UNR; ++u) rr[u] = k + 4 * u < rows ? ld_rec(rec + 8 * (k + 4 * u)) : pad_rec<T>();
+    pdl_wait();
+    const double4 ur = ref >= 0 ? ld_dep(U4 + ref) : make_double4(0.0, 0.0, 0.0, 0.0);
+    T H[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) H[q] = T(0);
+#pragma unroll 1
+    for (int32_t r = k; r < rows; r += 4 * UNR) {
+        double4 uu[UNR];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const int32_t n = rec_index(rr[u]);
+            uu[u] = n >= 0 ? ld_dep(U4 + n) : ur;
+        }
+        vec4_t<T> nx[UNR];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const int32_t rn = r + 4 * (UNR + u);
+            nx[u] = rn < rows ? ld_rec(rec + 8 * rn) : pad_rec<T>();
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const T du[3] = {T(diff ? uu[u].x - ur.x : uu[u].x), T(diff ? uu[u].y - ur.y : uu[u].y),
+                             T(diff ? uu[u].z - ur.z : uu[u].z)};
+            const T gg[3] = {rr[u].x, rr[u].y, rr[u].z};
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) H[a * 3 + d] += du[a] * gg[d];
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) rr[u] = nx[u];
+    }
+    // the four lanes of a cell (j, j + 8, j + 16, j + 24): fixed pairing, same H on each
+#pragma unroll
+    for (int off = 8; off < 32; off <<= 1)
+#pragma unroll
+        for (int q = 0; q < 9; ++q) H[q] += __shfl_xor_sync(kFull, H[q], off);
+    if (!valid || ref < 0) return;
+    double lam, mu;
+    element_lame(b, c, lam, mu);
+    T P[9];
+    const double Jf = stress<T>(MAT, T(lam), T(mu), H, P);
+    if (k == 0 && MAT == kNeoHookean && !(Jf > 0.0)) flag(status, AM_ENONPOS_J, c);
+    const T V = T(b.volumes[c]);
+    T m[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) m[q] = -V * P[q];
+    store_cell_matrix<T>(M, b.num_cells, c, k, m);
+}
+
+// Node octets: f = sum of M_c b over the rows in FP64 (products in the slot precision),
+// combined over the node's four lanes, written to the node's slot by lane k = 0.
+template <typename T, int UNR>
+__global__ void __launch_bounds__(256) k_cell_gather(CellBlockDev b, const T* __restrict__ M, vec4_t<T>* __restrict__ slots) {
+    pdl_trigger();
+    const int64_t o = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = static_cast<int>(threadIdx.x & 31), j = lane & 7, k = lane >> 3;
+    const int64_t i = 8 * o + j;
+    const bool valid = i < b.t_count;
+    const bool live = o < b.num_node_octets;
+    const int32_t r0 = live ? b.n_ptr[o] : 0, rows = live ? b.n_ptr[o + 1] - r0 : 0;
+    const int32_t pos = valid && k == 0 ? b.slot_pos[i] : 0;
+    const vec4_t<T>* rec = node_recs<T>(b) + 8 * static_cast<int64_t>(r0) + j;
+    vec4_t<T> rr[UNR];
+#pragma unroll
+    for (int u = 0; u < UNR; ++u) rr[u] = k + 4 * u < rows ? ld_rec(rec + 8 * (k + 4 * u)) : pad_rec<T>();
+    pdl_wait();
+    double f[3] = {0.0, 0.0, 0.0};
+#pragma unroll 1
+    for (int32_t r = k; r < rows; r += 4 * UNR) {
+        T mm[UNR][9];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const int32_t c = rec_index(rr[u]);
+            if (c >= 0) {
+                load_cell_matrix(M, b.num_cells, c, mm[u]);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 9; ++q) mm[u][q] = T(0);
+            }
+        }
+        vec4_t<T> nx[UNR];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const int32_t rn = r + 4 * (UNR + u);
+            nx[u] = rn < rows ? ld_rec(rec + 8 * rn) : pad_rec<T>();
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+                f[a] += static_cast<double>(mm[u][3 * a] * rr[u].x + mm[u][3 * a + 1] * rr[u].y + mm[u][3 * a + 2] * rr[u].z);
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) rr[u] = nx[u];
+    }
+#pragma unroll
+    for (int off = 8; off < 32; off <<= 1)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) f[a] += __shfl_xor_sync(kFull, f[a], off);
+    if (valid && k == 0) slots[pos] = make4(T(f[0]), T(f[1]), T(f[2]));
+}
+
+// ---------------------------------------------------------------------------
 // Four-entry cells grouped as split hexes (a tet mesh's element smoothing cells):
 // the split-hex Tet4 kernel's pair split, with each cell's stored gradients b_e and
 // volume V in place of the tet's own geometry. Entry e of the patch's tet t sits on
@@ -1569,12 +1761,20 @@ __global__ void __launch_bounds__(256) k_cell_vjp(CellBlockDev b, const double4*
     double dP[9], ldl, ldm;
     stress_vjp(MAT, lam, mu, H, L, dP, &ldl, &ldm);
     const double V = b.volumes[c];
-    for (int32_t s = s0 + lane; s < s1; s += 32) {
-        const double gg[3] = {b.grads64[3 * s], b.grads64[3 * s + 1], b.grads64[3 * s + 2]};
-        double f[3];
+    if (b.gather) {
+        // cell-stress form: -V dP per cell, summed per node by the gather kernel
+        double m[9];
 #pragma unroll
-        for (int i = 0; i < 3; ++i) f[i] = (gg[0] * dP[i * 3 + 0] + gg[1] * dP[i * 3 + 1] + gg[2] * dP[i * 3 + 2]) * -V;
-        slots[b.slot_pos[s]] = make4(f[0], f[1], f[2]);
+        for (int k = 0; k < 9; ++k) m[k] = -V * dP[k];
+        store_cell_matrix<double>(static_cast<double*>(b.cmat), b.num_cells, c, lane, m);
+    } else {
+        for (int32_t s = s0 + lane; s < s1; s += 32) {
+            const double gg[3] = {b.grads64[3 * s], b.grads64[3 * s + 1], b.grads64[3 * s + 2]};
+            double f[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) f[i] = (gg[0] * dP[i * 3 + 0] + gg[1] * dP[i * 3 + 1] + gg[2] * dP[i * 3 + 2]) * -V;
+            slots[b.slot_pos[s]] = make4(f[0], f[1], f[2]);
+        }
     }
     if (lane == 0) store_theta(gmu, gk, c, -V * (ldm - 2.0 / 3.0 * ldl), -V * ldl, accumulate);
 }
@@ -2449,8 +2649,44 @@ void launch_fbar(const CellBlockDev& b, const double4* U4, void* slots, int* sta
     }
 }
 
+template <typename T, int UNR>
+void launch_cell_stress_unr(const CellBlockDev& b, const double4* U4, int* status, cudaStream_t s) {
+    AM_DISPATCH_MAT(b.material, (launch_pdl(k_cell_stress<T, M, UNR>, grid_for(b.num_octets * 32, 256), 256, s, b, U4,
+                                            static_cast<T*>(b.cmat), status)));
+}
+template <typename T, int UNR>
+void launch_cell_gather_unr(const CellBlockDev& b, void* slots, cudaStream_t s) {
+    launch_pdl(k_cell_gather<T, UNR>, grid_for(b.num_node_octets * 32, 256), 256, s, b, static_cast<const T*>(b.cmat),
+               static_cast<vec4_t<T>*>(slots));
+}
+// Rows in flight per lane: unroll[0] (cell kernel) and unroll[1] (gather kernel), 1, 2 or 4.
+template <typename T>
+void launch_cell_gather_form(const CellBlockDev& b, const double4* U4, void* slots, int* status, cudaStream_t s) {
+    if (b.unroll[0] == 1) {
+        launch_cell_stress_unr<T, 1>(b, U4, status, s);
+    } else if (b.unroll[0] == 2) {
+        launch_cell_stress_unr<T, 2>(b, U4, status, s);
+    } else {
+        launch_cell_stress_unr<T, 4>(b, U4, status, s);
+    }
+    if (b.unroll[1] == 1) {
+        launch_cell_gather_unr<T, 1>(b, slots, s);
+    } else if (b.unroll[1] == 2) {
+        launch_cell_gather_unr<T, 2>(b, slots, s);
+    } else {
+        launch_cell_gather_unr<T, 4>(b, slots, s);
+    }
+}
+
 int launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void* slots, int* status, cudaStream_t s) {
     if (b.num_cells == 0) return 0;
+    if (b.gather) {
+        if (mixed)
+            launch_cell_gather_form<float>(b, U4, slots, status, s);
+        else
+            launch_cell_gather_form<double>(b, U4, slots, status, s);
+        return 2;
+    }
     if (b.patched == 2) {
         const unsigned grid = grid_for(2 * b.num_patches, kHex6Block);
         if (mixed) {
@@ -2525,15 +2761,24 @@ void launch_gauss_vjp(const GaussBlockDev& b, const double4* X4, const double4* 
     }
 }
 
-void launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double4* slots, double* gmu,
-                     double* gkappa, int accumulate, cudaStream_t s) {
-    if (b.num_cells == 0) return;
+int launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double4* slots, double* gmu,
+                    double* gkappa, int accumulate, cudaStream_t s) {
+    if (b.num_cells == 0) return 0;
     if (b.patched == 2) {
         AM_DISPATCH_MAT(b.material, (k_cell_hex6_vjp<M><<<grid_for(b.num_patches, 64), 64, 0, s>>>(b, U4, L4, slots, gmu, gkappa, accumulate)));
-        return;
+        return 1;
     }
     const unsigned grid = grid_for(b.num_cells * 32, 256);
     AM_DISPATCH_MAT(b.material, (k_cell_vjp<M><<<grid, 256, 0, s>>>(b, U4, L4, slots, gmu, gkappa, accumulate)));
+    if (!b.gather) return 1;
+    if (b.unroll[1] == 1) {
+        launch_cell_gather_unr<double, 1>(b, slots, s);
+    } else if (b.unroll[1] == 2) {
+        launch_cell_gather_unr<double, 2>(b, slots, s);
+    } else {
+        launch_cell_gather_unr<double, 4>(b, slots, s);
+    }
+    return 2;
 }
 
 void launch_hex6_patch_dx(const int32_t* patch_nodes, int64_t num_patches, const double4* X4, float* dx32,

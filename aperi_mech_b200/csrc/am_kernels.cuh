@@ -87,6 +87,25 @@ struct CellBlockDev {
     void* fbar;
     int32_t max_group;          // most subcells in one cell
     int32_t fused;              // 1: one warp per cell, one lane per subcell (max_group <= 32)
+    // Cell-stress form (gather = 1): per-cell M = -V P into cmat (three component arrays:
+    // values 0-3, 4-7 and 8 of the num_cells cells, slot precision), then per node the block
+    // touches (t_count of them, logical slot i) the sum of M b over its entries. Both
+    // kernels walk octets of eight items: octet o's rows are o_ptr[o] .. o_ptr[o+1] (cells)
+    // or n_ptr (nodes), row r of item j at record 8 r + j: gradient in x, y, z, the partner
+    // index (node, or cell) in w, -1 for padding. c_ref: a node of each cell (-1: empty).
+    int32_t gather;
+    int64_t num_octets;
+    const int32_t* o_ptr;
+    const float4* orec32;
+    const double4* orec64;
+    const int32_t* c_ref;
+    int64_t t_count;
+    int64_t num_node_octets;
+    const int32_t* n_ptr;
+    const float4* nrec32;
+    const double4* nrec64;
+    void* cmat;
+    int32_t unroll[2];  // rows per lane in flight (1, 2 or 4): cell kernel, gather kernel
 };
 constexpr int kFbarStride = 20;
 
@@ -127,7 +146,7 @@ void launch_gauss_force(const GaussBlockDev& b, int mixed, const double4* X4, co
 int launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void* slots, int* status, cudaStream_t s);
 void launch_gauss_vjp(const GaussBlockDev& b, const double4* X4, const double4* U4, const double4* L4, double4* slots,
                       double* gmu, double* gkappa, int accumulate, cudaStream_t s);
-void launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double4* slots, double* gmu,
+int launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double4* slots, double* gmu,
                      double* gkappa, int accumulate, cudaStream_t s);
 void launch_hex6_patch_dx(const int32_t* patch_nodes, int64_t num_patches, const double4* X4, float* dx32,
                           double* dx64, cudaStream_t stream);

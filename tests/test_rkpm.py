@@ -96,6 +96,44 @@ def test_rkpm_force_and_steps_match_oracle(gpu, oracle_lib):
 
 
 @pytest.mark.gpu
+def test_rkpm_cell_stress_form(gpu, oracle_lib, monkeypatch):
+    """The generic cell path runs in the cell-stress form by default (per cell -V P, then a
+    node-major gather into one slot per node). With one, two or four rows per lane in flight
+    (APERI_B200_CELL_UNROLL) every lane sums its rows in the same order, so the
+    forces, gradients and states are bitwise equal; the per-entry slot form
+    (APERI_B200_CELL_GATHER=0) sums in another order and agrees with the oracle as closely."""
+    from aperi_mech_b200 import problems
+    from aperi_mech_b200.model import ExplicitDynamics
+
+    p = problems.rkpm_box(n=4, seed=5, nsteps=30)
+    mass = p.meta["mass"]
+    op = oracle_lib.OracleProblem(p.coords, p.parts, p.bcs, mass=mass)
+    rng = np.random.default_rng(3)
+    u = 1e-3 * rng.standard_normal(p.coords.shape)
+    lam = rng.standard_normal(p.coords.shape)
+    want_f = op.internal_force(u)
+    out = {}
+    for gather, unroll in (("1", "1111"), ("1", "2222"), ("1", "4444"), ("0", "4444")):
+        monkeypatch.setenv("APERI_B200_CELL_GATHER", gather)
+        monkeypatch.setenv("APERI_B200_CELL_UNROLL", unroll)
+        with ExplicitDynamics(p.coords, p.parts, p.bcs, mass=mass) as m:
+            f = m.internal_force(u)
+            fm = m.internal_force(u, "mixed")
+            g = m.vjp_force(u, lam)
+            m.set_state(None, p.v0)
+            m.init_acceleration("mixed")
+            m.run(p.nsteps, p.dt, "mixed")
+            out[gather, unroll] = (f, fm, *g, *m.get_state())
+        assert rel_err(f, want_f) < 1e-12
+        assert rel_err(fm, want_f) < 5e-5
+    for key in (("1", "1111"), ("1", "2222")):
+        for a, b in zip(out[key], out["1", "4444"]):
+            assert np.array_equal(a, b)
+    for a, b in zip(out["0", "4444"][2:5], out["1", "4444"][2:5]):
+        assert rel_err(a, b) < 1e-11
+
+
+@pytest.mark.gpu
 def test_rkpm_linear_field_patch(gpu):
     """Linear displacement -> every nodal cell's displacement gradient is exact, so the
     forces of a linear-elastic body in constant stress vanish away from the boundary."""
