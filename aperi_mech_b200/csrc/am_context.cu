@@ -206,6 +206,8 @@ struct Block {
     uint32_t* patch_gather = nullptr;
     float* patch_dx32 = nullptr;
     double* patch_dx64 = nullptr;
+    float* geo32 = nullptr;  // per-tet J^-1 and w (see GaussBlockDev)
+    double* geo64 = nullptr;
     // Cell-stress form of a generic cell block (no patches, no F-bar groups, cells of more
     // than eight entries): octet row records of the cells and of the nodes the block
     // touches (one logical slot each), a node of each cell, and the per-cell matrices
@@ -265,6 +267,8 @@ struct Block {
         g.patch_gather = patch_gather;
         g.patch_dx32 = patch_dx32;
         g.patch_dx64 = patch_dx64;
+        g.geo32 = geo32;
+        g.geo64 = geo64;
         g.hstate = hstate;
         g.href = href;
         return g;
@@ -344,6 +348,8 @@ struct Block {
         dfree(patch_gather);
         dfree(patch_dx32);
         dfree(patch_dx64);
+        dfree(geo32);
+        dfree(geo64);
         dfree(order_dev);
         dfree(hstate);
         dfree(href);
@@ -551,6 +557,10 @@ struct am_ctx {
     // Generic cell blocks in the cell-stress form (per-cell M, node-major gather; the
     // default) or, with APERI_B200_CELL_GATHER=0, with one force slot per entry.
     // APERI_B200_CELL_UNROLL: rows per lane in flight in its kernels (see am_create).
+    // Tet4 blocks run one thread per tet stream their reference J^-1 and weight from a
+    // table built at am_add_block (the default) or, with APERI_B200_TET4_GEOMETRY=0,
+    // gather the coordinates and invert J every step.
+    bool tet_geometry = true;
     bool cell_gather = true;
     // The defaults measured fastest on the RKPM nodal cells of the h = 1/46 box: FP64 4 and
     // 2 (the FP64 gather at 4 holds 128 registers), mixed 4 and 4.
@@ -1323,6 +1333,8 @@ int am_create(int64_t num_nodes, const double* coords, am_ctx** out) {
         c->io_scratch = dalloc<double>(N * 3, "io scratch");
         const char* graphs = std::getenv("APERI_B200_GRAPHS");
         c->use_graphs = !(graphs && graphs[0] == '0');
+        const char* tg = std::getenv("APERI_B200_TET4_GEOMETRY");
+        c->tet_geometry = !(tg && tg[0] == '0');
         const char* cg = std::getenv("APERI_B200_CELL_GATHER");
         c->cell_gather = !(cg && cg[0] == '0');
         // four digits: FP64 cell, FP64 gather, mixed cell, mixed gather kernel (1, 2 or 4)
@@ -1520,6 +1532,13 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
                         for (int64_t q = 0; q < P; ++q)
                             for (int a = 0; a < tp.used[q]; ++a) b.host_nodes[8 * q + a] = tp.nodes[8 * q + a];
                     }
+                }
+                if (d->kind == AM_TET4_GAUSS && E > 0 && b.patched == 0 && ctx->lagr == 0 && ctx->tet_geometry) {
+                    // one thread per tet: the reference geometry is set up once
+                    b.geo32 = dalloc<float>(10 * E, "tet geometry (FP32)");
+                    b.geo64 = dalloc<double>(10 * E, "tet geometry");
+                    am::launch_tet4_geometry(b.conn, E, ctx->X4, b.geo32, b.geo64, ctx->stream);
+                    ck(cudaGetLastError(), "tet geometry");
                 }
             }
             if (ctx->num_slots + b.num_entries >= (int64_t(1) << 31)) fail(AM_ERANGE, "slot count beyond int32 indexing");

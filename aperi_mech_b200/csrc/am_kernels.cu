@@ -189,6 +189,119 @@ __global__ void __launch_bounds__(256) k_tet4_force(GaussBlockDev b, const doubl
 }
 
 // ---------------------------------------------------------------------------
+// Tet4 one thread per tet with the geometry set up once: J^-1 and w = det J / 6 of the
+// reference configuration (constant under the total formulation) are streamed from a
+// table in place of four coordinate gathers and a 3x3 inverse per step. H = D J^-1;
+// for the neo-Hookean material w J^-1 P^T = w J^-1 adj(F) tau / det F (adj(J + D) =
+// adj(F J) = adj(J) adj(F) = 6 w J^-1 adj(F)), otherwise w J^-1 P^T from P.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct Vec2Of;
+template <>
+struct Vec2Of<float> {
+    using type = float2;
+};
+template <>
+struct Vec2Of<double> {
+    using type = double2;
+};
+template <typename T>
+__device__ __forceinline__ const T* tet_geo(const GaussBlockDev& b);
+template <>
+__device__ __forceinline__ const float* tet_geo<float>(const GaussBlockDev& b) { return b.geo32; }
+template <>
+__device__ __forceinline__ const double* tet_geo<double>(const GaussBlockDev& b) { return b.geo64; }
+__device__ __forceinline__ float4 ld_geo4(const float4* p) { return __ldg(p); }
+__device__ __forceinline__ double4 ld_geo4(const double4* p) { return ld_ro4(p); }
+
+__global__ void __launch_bounds__(256) k_tet4_geometry(const int32_t* __restrict__ conn, int64_t E,
+                                                        const double4* __restrict__ X4, float* __restrict__ g32,
+                                                        double* __restrict__ g64) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    const int4 c = reinterpret_cast<const int4*>(conn)[e];
+    const double4 x0 = X4[c.x], x1 = X4[c.y], x2 = X4[c.z], x3 = X4[c.w];
+    const double J[9] = {x1.x - x0.x, x2.x - x0.x, x3.x - x0.x, x1.y - x0.y, x2.y - x0.y,
+                         x3.y - x0.y, x1.z - x0.z, x2.z - x0.z, x3.z - x0.z};
+    const double det = det3(J);
+    double Ji[9];
+    cof_inv3(J, Ji, det);
+    const double w = det / 6.0;
+    reinterpret_cast<double4*>(g64)[e] = make_double4(Ji[0], Ji[1], Ji[2], Ji[3]);
+    reinterpret_cast<double4*>(g64 + 4 * E)[e] = make_double4(Ji[4], Ji[5], Ji[6], Ji[7]);
+    reinterpret_cast<double2*>(g64 + 8 * E)[e] = make_double2(Ji[8], w);
+    reinterpret_cast<float4*>(g32)[e] = make_float4(float(Ji[0]), float(Ji[1]), float(Ji[2]), float(Ji[3]));
+    reinterpret_cast<float4*>(g32 + 4 * E)[e] = make_float4(float(Ji[4]), float(Ji[5]), float(Ji[6]), float(Ji[7]));
+    reinterpret_cast<float2*>(g32 + 8 * E)[e] = make_float2(float(Ji[8]), float(w));
+}
+
+template <typename T, int MAT>
+__global__ void __launch_bounds__(256) k_tet4_force_geo(GaussBlockDev b, const double4* __restrict__ U4,
+                                                         vec4_t<T>* __restrict__ slots, int* status) {
+    pdl_trigger();
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= b.num_elems) return;
+    const int64_t E = b.num_elems;
+    const int4 c = reinterpret_cast<const int4*>(b.conn)[e];
+    const T* geo = tet_geo<T>(b);
+    const vec4_t<T> g0 = ld_geo4(reinterpret_cast<const vec4_t<T>*>(geo) + e);
+    const vec4_t<T> g1 = ld_geo4(reinterpret_cast<const vec4_t<T>*>(geo + 4 * E) + e);
+    const typename Vec2Of<T>::type g2 = __ldg(reinterpret_cast<const typename Vec2Of<T>::type*>(geo + 8 * E) + e);
+    const int32_t pos[4] = {b.slot_pos[4 * e], b.slot_pos[4 * e + 1], b.slot_pos[4 * e + 2], b.slot_pos[4 * e + 3]};
+    double lam, mu;
+    element_lame(b, e, lam, mu);
+    pdl_wait();
+    const double4 u0 = ld_dep(U4 + c.x), u1 = ld_dep(U4 + c.y), u2 = ld_dep(U4 + c.z), u3 = ld_dep(U4 + c.w);
+    const T D[9] = {T(u1.x - u0.x), T(u2.x - u0.x), T(u3.x - u0.x), T(u1.y - u0.y), T(u2.y - u0.y),
+                    T(u3.y - u0.y), T(u1.z - u0.z), T(u2.z - u0.z), T(u3.z - u0.z)};
+    const T Ji[9] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w, g2.x};
+    const T w = g2.y;
+    if (!(w > T(0))) flag(status, AM_ENONPOS_J, e);
+    T H[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) H[i * 3 + j] = D[i * 3 + 0] * Ji[0 * 3 + j] + D[i * 3 + 1] * Ji[1 * 3 + j] + D[i * 3 + 2] * Ji[2 * 3 + j];
+    T Q[9];
+    if (MAT == kNeoHookean) {
+        T tau[9];
+        const double Jf = nh_kirchhoff<T>(T(lam), T(mu), H, tau);
+        if (!(Jf > 0.0)) flag(status, AM_ENONPOS_J, e);
+        T F[9], AF[9], K[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) F[k] = H[k] + ((k % 4 == 0) ? T(1) : T(0));
+        adj3(F, AF);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) K[i * 3 + j] = Ji[i * 3 + 0] * AF[0 * 3 + j] + Ji[i * 3 + 1] * AF[1 * 3 + j] + Ji[i * 3 + 2] * AF[2 * 3 + j];
+        const T sc = sizeof(T) == 4 ? T(w * __frcp_rn(static_cast<float>(Jf))) : T(w / Jf);
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                Q[k * 3 + i] = sc * (K[k * 3 + 0] * tau[0 * 3 + i] + K[k * 3 + 1] * tau[1 * 3 + i] + K[k * 3 + 2] * tau[2 * 3 + i]);
+    } else {
+        T P[9];
+        stress<T>(MAT, T(lam), T(mu), H, P);
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                Q[k * 3 + i] = w * (Ji[k * 3 + 0] * P[i * 3 + 0] + Ji[k * 3 + 1] * P[i * 3 + 1] + Ji[k * 3 + 2] * P[i * 3 + 2]);
+    }
+    // f_{k+1} = -Q_k ; f_0 = Q_0 + Q_1 + Q_2
+    T f0[3] = {T(0), T(0), T(0)};
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) f0[i] += Q[k * 3 + i];
+    slots[pos[0]] = make4(f0[0], f0[1], f0[2]);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) slots[pos[k + 1]] = make4(-Q[k * 3 + 0], -Q[k * 3 + 1], -Q[k * 3 + 2]);
+}
+
+// ---------------------------------------------------------------------------
 // Tet4 element patches (at most 6 tets on at most 8 nodes, e.g. the six tets of a
 // split hex): one warp serves 5 patches. The warp first loads the 40 patch nodes
 // into shared memory (FP64), then lane 6q+t computes tet t of patch q (30 busy
@@ -2599,6 +2712,13 @@ void launch_gauss_force(const GaussBlockDev& b, int mixed, const double4* X4, co
         } else {
             AM_DISPATCH_MAT(b.material, (k_tet4_patch_force<double, M><<<grid, 256, 0, s>>>(b, X4, U4, static_cast<double4*>(slots), status)));
         }
+    } else if (b.kind == AM_TET4_GAUSS && b.geo64 != nullptr) {
+        const unsigned grid = grid_for(b.num_elems, 256);
+        if (mixed) {
+            AM_DISPATCH_MAT(b.material, (launch_pdl(k_tet4_force_geo<float, M>, grid, 256, s, b, U4, static_cast<float4*>(slots), status)));
+        } else {
+            AM_DISPATCH_MAT(b.material, (launch_pdl(k_tet4_force_geo<double, M>, grid, 256, s, b, U4, static_cast<double4*>(slots), status)));
+        }
     } else if (b.kind == AM_TET4_GAUSS) {
         const unsigned grid = grid_for(b.num_elems, 256);
         if (mixed) {
@@ -2779,6 +2899,12 @@ int launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4,
         launch_cell_gather_unr<double, 4>(b, slots, s);
     }
     return 2;
+}
+
+void launch_tet4_geometry(const int32_t* conn, int64_t num_elems, const double4* X4, float* geo32, double* geo64,
+                          cudaStream_t s) {
+    if (num_elems == 0) return;
+    k_tet4_geometry<<<grid_for(num_elems, 256), 256, 0, s>>>(conn, num_elems, X4, geo32, geo64);
 }
 
 void launch_hex6_patch_dx(const int32_t* patch_nodes, int64_t num_patches, const double4* X4, float* dx32,

@@ -52,6 +52,13 @@ struct GaussBlockDev {
     // in place of the coordinate gathers. null where not built.
     const float* patch_dx32;
     const double* patch_dx64;
+    // Per-tet geometry of a Tet4 block run one thread per tet under the total formulation:
+    // J^-1 (row-major) and w = det J / 6 of every tet, formed in FP64 at set-up (an FP32 copy
+    // for the mixed path), in three component blocks: values 0-3 and 4-7 of J^-1 (a vec4
+    // each, num_elems apiece), then (J^-1[8], w) pairs. Read in place of the coordinate
+    // gathers. null where not built.
+    const float* geo32;
+    const double* geo64;
     // Updated / semi-Lagrangian formulations: element displacement gradient of the last
     // force evaluation (9 per element; for Hex8 the last Gauss point's) and the semi
     // formulation's reference gradient. null under the total formulation.
@@ -144,6 +151,8 @@ void launch_gauss_force(const GaussBlockDev& b, int mixed, const double4* X4, co
                         int* status, cudaStream_t s);
 // Returns the number of kernels launched (3 for an F-bar block).
 int launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void* slots, int* status, cudaStream_t s);
+void launch_tet4_geometry(const int32_t* conn, int64_t num_elems, const double4* X4, float* geo32, double* geo64,
+                          cudaStream_t s);
 void launch_gauss_vjp(const GaussBlockDev& b, const double4* X4, const double4* U4, const double4* L4, double4* slots,
                       double* gmu, double* gkappa, int accumulate, cudaStream_t s);
 int launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double4* slots, double* gmu,

@@ -443,6 +443,43 @@ def test_adjoint_finite_differences_hex8_64(gpu):
     assert max(errs) <= 1e-4, max(errs)
 
 
+# ---- Tet4 one thread per tet: reference geometry table ------------------------------------
+@pytest.mark.parametrize("material", ["neo_hookean", "elastic", "linear_elastic"])
+def test_tet4_geometry_table(gpu, oracle_lib, monkeypatch, material):
+    """One thread per tet with the reference J^-1 and weight set up once (the default) and
+    with the coordinates gathered and J inverted every step (APERI_B200_TET4_GEOMETRY=0):
+    both match the oracle, FP64 forces and 30 steps, and agree with each other to
+    round-off; mixed forces within the mixed bar."""
+    from aperi_mech_b200.model import ExplicitDynamics, Part
+
+    monkeypatch.setenv("APERI_B200_TET4_PATCHES", "0")
+    coords, conn = _mesh("tet4", 5, seed=9)
+    conn = conn[np.random.default_rng(1).permutation(conn.shape[0])]
+    parts = [Part("tet4", _material(material), conn=conn)]
+    rng = np.random.default_rng(4)
+    u = 1e-3 * rng.standard_normal(coords.shape)
+    v0 = 10.0 * rng.standard_normal(coords.shape)
+    op = oracle_lib.OracleProblem(coords, parts)
+    want_f = op.internal_force(u)
+    out = {}
+    for geo in ("1", "0"):
+        monkeypatch.setenv("APERI_B200_TET4_GEOMETRY", geo)
+        with ExplicitDynamics(coords, parts) as m:
+            f = m.internal_force(u)
+            assert rel_err(f, want_f) < FP64_TOL
+            assert rel_err(m.internal_force(u, "mixed"), want_f) < MIXED_FORCE_TOL
+            dt = 1e-7
+            m.set_state(None, v0)
+            m.init_acceleration()
+            m.run(30, dt)
+            out[geo] = (f, m.get_state())
+    z = np.zeros_like(coords)
+    want = op.steps(z, v0, op.init_acceleration(z), np.full(30, 1e-7))
+    for g, w in zip(out["1"][1], want):
+        assert rel_err(g, w) < 1e-12
+    assert rel_err(out["1"][0], out["0"][0]) < 1e-13
+
+
 # ---- Tet4 element patches ----------------------------------------------------------------
 @pytest.mark.parametrize("layout", ["unpatched", "irregular_patches", "shuffled"])
 def test_tet4_patch_layouts(gpu, oracle_lib, monkeypatch, layout):
