@@ -561,6 +561,7 @@ struct am_ctx {
     // table built at am_add_block (the default) or, with APERI_B200_TET4_GEOMETRY=0,
     // gather the coordinates and invert J every step.
     bool tet_geometry = true;
+    int32_t node_lanes = 0;  // APERI_B200_NODE_LANES (1, 2, 4, 8): lanes per node; 0 chosen per mesh
     bool cell_gather = true;
     // The defaults measured fastest on the RKPM nodal cells of the h = 1/46 box: FP64 4 and
     // 2 (the FP64 gather at 4 holds 128 registers), mixed 4 and 4.
@@ -668,6 +669,7 @@ struct am_ctx {
         nd.lagr = lagr;
         nd.xc = xc;
         nd.inc = lagr_inc;
+        nd.lanes = node_lanes;
         return nd;
     }
 
@@ -1333,6 +1335,8 @@ int am_create(int64_t num_nodes, const double* coords, am_ctx** out) {
         c->io_scratch = dalloc<double>(N * 3, "io scratch");
         const char* graphs = std::getenv("APERI_B200_GRAPHS");
         c->use_graphs = !(graphs && graphs[0] == '0');
+        const char* nl = std::getenv("APERI_B200_NODE_LANES");
+        c->node_lanes = nl ? std::atoi(nl) : 0;
         const char* tg = std::getenv("APERI_B200_TET4_GEOMETRY");
         c->tet_geometry = !(tg && tg[0] == '0');
         const char* cg = std::getenv("APERI_B200_CELL_GATHER");

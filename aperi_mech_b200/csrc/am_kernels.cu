@@ -2936,8 +2936,12 @@ void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const dou
 // Hex8 153.9 -> 133.8 us FP64, but 95.2 -> 103.5 us mixed. Cell meshes with tens of
 // slots per node take four or eight lanes.
 inline int node_lanes(const NodeDev& nd, int mixed) {
+    if (nd.lanes == 1 || nd.lanes == 2 || nd.lanes == 4 || nd.lanes == 8) return nd.lanes;
     const double per_node = static_cast<double>(nd.num_slots) / static_cast<double>(nd.num_nodes);
     if (per_node <= 12.0) return (!mixed || nd.num_slots * 16 <= (int64_t{64} << 20)) ? 2 : 1;
+    // one thread per tet on a tet mesh (about 23 slots per node): 2 lanes ran the node
+    // kernel in 40.9 us against 49.8 (1), 47.6 (4) and 60.2 (8) on the renumbered 70^3 mesh
+    if (per_node <= 32.0) return 2;
     return per_node <= 40.0 ? 4 : 8;
 }
 inline bool gather_batch8(const NodeDev& nd, int mixed) {

@@ -144,6 +144,7 @@ struct NodeDev {
     const int32_t* subset_nodes;
     int64_t subset_count;
     int32_t skip_iface;
+    int32_t lanes;              // lanes per node in the node kernels; 0: chosen from the slots per node
 };
 
 // ---- launchers (am_kernels.cu) ----
