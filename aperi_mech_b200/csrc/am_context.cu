@@ -99,16 +99,31 @@ void nccl_check(ncclResult_t r, const char* what) {
 
 // Octet rows of the cell-stress form: items 8o .. 8o + 7 (cells, or nodes), item j with
 // entries ptr[j] .. ptr[j+1] whose partners (node, or cell) ascend. Rows are aligned by
-// offset (partner minus item: on a locality-numbered mesh consecutive items see the same
-// offsets, so a row's eight partners are consecutive) when that pads by at most 35% over
-// the octet's entries; otherwise each item's entries fill rows from the first. src holds,
-// per (row, item) at 8 row + item, the entry or -1 (padding).
+// offset (partner minus item, or their anchors': on a locality-numbered mesh consecutive
+// items see the same offsets, so a row's eight partners are consecutive) when that pads by
+// at most 35% over the octet's entries; otherwise each item's entries fill rows from the
+// first. src holds, per (row, item) at 8 row + item, the entry or -1 (padding).
 struct OctetRows {
     std::vector<int32_t> ptr;
     std::vector<int32_t> src;
 };
 
-OctetRows octet_rows(int64_t count, const std::vector<int32_t>& ptr, const std::vector<int32_t>& partner) {
+OctetRows octet_rows(int64_t count, const std::vector<int32_t>& ptr, const std::vector<int32_t>& partner,
+                     const int32_t* item_anchor = nullptr, const int32_t* partner_anchor = nullptr, int items = 8) {
+    if (items == 1) {
+        // a warp per item: its rows are its entries
+        OctetRows o;
+        o.ptr.assign(ptr.begin(), ptr.begin() + count + 1);
+        o.src.resize(static_cast<size_t>(ptr[count]));
+        for (size_t e = 0; e < o.src.size(); ++e) o.src[e] = static_cast<int32_t>(e);
+        return o;
+    }
+    // the alignment key of an entry: its partner's anchor minus its item's (anchors default to
+    // the indices themselves; F-bar subcells are anchored at their vertex)
+    auto key = [&](int64_t item, int32_t e) {
+        const int64_t pa = partner_anchor ? partner_anchor[partner[e]] : partner[e];
+        return pa - (item_anchor ? item_anchor[item] : item);
+    };
     OctetRows o;
     const int64_t O = (count + 7) / 8;
     o.ptr.reserve(O + 1);
@@ -131,12 +146,12 @@ OctetRows octet_rows(int64_t count, const std::vector<int32_t>& ptr, const std::
         while (true) {
             int64_t off = INT64_MAX;
             for (int j = 0; j < 8; ++j)
-                if (p[j] < end[j]) off = std::min<int64_t>(off, int64_t(partner[p[j]]) - (8 * q + j));
+                if (p[j] < end[j]) off = std::min<int64_t>(off, key(8 * q + j, p[j]));
             if (off == INT64_MAX) break;
             int32_t run[8], mult = 0;
             for (int j = 0; j < 8; ++j) {
                 run[j] = 0;
-                while (p[j] + run[j] < end[j] && int64_t(partner[p[j] + run[j]]) - (8 * q + j) == off) ++run[j];
+                while (p[j] + run[j] < end[j] && key(8 * q + j, p[j] + run[j]) == off) ++run[j];
                 mult = std::max(mult, run[j]);
             }
             for (int32_t t = 0; t < mult; ++t)
@@ -208,12 +223,13 @@ struct Block {
     double* patch_dx64 = nullptr;
     float* geo32 = nullptr;  // per-tet J^-1 and w (see GaussBlockDev)
     double* geo64 = nullptr;
-    // Cell-stress form of a generic cell block (no patches, no F-bar groups, cells of more
-    // than eight entries): octet row records of the cells and of the nodes the block
+    // Cell-stress form of a generic cell block (no patches, cells of more than eight entries,
+    // no F-bar groups or groups of at most 32 subcells): octet row records of the cells and of the nodes the block
     // touches (one logical slot each), a node of each cell, and the per-cell matrices
     // M = -V P of each precision.
     bool gather = false;
     int32_t unroll[2][2] = {{4, 2}, {4, 4}};  // [FP64, mixed][cell kernel, gather kernel]
+    int32_t group_items[2] = {8, 8};          // items per warp: cell side, node side
     int64_t num_octets = 0, num_node_octets = 0, t_count = 0;
     int32_t* o_ptr = nullptr;
     int32_t* n_ptr = nullptr;
@@ -225,7 +241,8 @@ struct Block {
     float* cmat32 = nullptr;
     double* cmat64 = nullptr;
     std::vector<int32_t> host_cell_ptr;  // until am_finalize: the CSR and gradients the records
-    std::vector<double> host_grads;      // are built from
+    std::vector<double> host_grads;      // are built from, and the F-bar groups
+    std::vector<int64_t> host_group_ptr;
     const int32_t* slot_pos = nullptr;  // block-local view into the context's position array
     std::vector<int32_t> host_nodes;    // node of each logical slot (-1: unused), for the node CSR
     // Processing order of a Gauss block's elements: order[k] is the caller's index of the
@@ -305,6 +322,8 @@ struct Block {
         c.c_ref = c_ref;
         c.t_count = t_count;
         c.num_node_octets = num_node_octets;
+        c.group_items[0] = group_items[0];
+        c.group_items[1] = group_items[1];
         c.n_ptr = n_ptr;
         c.nrec32 = nrec32;
         c.nrec64 = nrec64;
@@ -400,8 +419,21 @@ struct Block {
                 tperm[k] = s;
                 tpart[k] = static_cast<int32_t>(c);
             }
-        const OctetRows co = octet_rows(E, host_cell_ptr, cpart);
-        const OctetRows no = octet_rows(T, tptr, tpart);
+        // F-bar subcells are anchored at their group (the vertex of a nodal cell), so that the
+        // subcells of a vertex line up on the nodes they share
+        std::vector<int32_t> canc;
+        if (!host_group_ptr.empty()) {
+            canc.resize(E);
+            for (size_t g = 0; g + 1 < host_group_ptr.size(); ++g)
+                for (int64_t c = host_group_ptr[g]; c < host_group_ptr[g + 1]; ++c) canc[c] = static_cast<int32_t>(g);
+        }
+        const int32_t* anc = canc.empty() ? nullptr : canc.data();
+        // Items of many entries (more than 160 on average: the nodes of F-bar subcells, about
+        // 840 each on the h = 1/32 box) take a warp each; 32 lanes then read consecutive rows.
+        group_items[0] = E > 0 && K > 160 * E ? 1 : 8;
+        group_items[1] = T > 0 && K > 160 * T ? 1 : 8;
+        const OctetRows co = octet_rows(E, host_cell_ptr, cpart, anc, nullptr, group_items[0]);
+        const OctetRows no = octet_rows(T, tptr, tpart, nullptr, anc, group_items[1]);
         auto records = [&](const OctetRows& o, const std::vector<int32_t>& perm, const std::vector<int32_t>& part,
                            float4*& r32, double4*& r64, const char* what) {
             const size_t R = o.src.size();
@@ -1660,6 +1692,7 @@ int am_set_cell_groups(am_ctx* ctx, int32_t block_id, int64_t num_cells, const i
         b.fbar_fused = !(passes && passes[0] == '3');
         b.group_ptr = dalloc<int64_t>(num_cells + 1, "cell groups");
         ck(cudaMemcpy(b.group_ptr, group_ptr, (num_cells + 1) * sizeof(int64_t), cudaMemcpyHostToDevice), "upload");
+        if (!b.host_grads.empty()) b.host_group_ptr.assign(group_ptr, group_ptr + num_cells + 1);
     });
 }
 
@@ -1693,16 +1726,18 @@ int am_finalize(am_ctx* ctx) {
         if (ctx->blocks.empty()) fail(AM_EINVAL, "no blocks");
         const int64_t N = ctx->N, NP = ctx->points();
         if (NP > N && !ctx->mass_set) fail(AM_ESTATE, "cells on refinement points need the generalized mass (am_set_mass)");
-        // Generic cell blocks without F-bar groups take the cell-stress form: one logical
-        // slot per node they touch instead of one per entry.
+        // Generic cell blocks (without F-bar groups, or with groups of at most 32 subcells)
+        // take the cell-stress form: one logical slot per node they touch instead of one per
+        // entry.
         int64_t base = 0;
         for (auto& b : ctx->blocks) {
-            if (!b.host_grads.empty() && b.patched == 0 && !b.group_ptr) {
+            if (!b.host_grads.empty() && b.patched == 0 && (!b.group_ptr || b.cells().fused)) {
                 std::memcpy(b.unroll, ctx->cell_unroll, sizeof b.unroll);
                 b.build_gather(NP);
             }
             std::vector<double>().swap(b.host_grads);
             std::vector<int32_t>().swap(b.host_cell_ptr);
+            std::vector<int64_t>().swap(b.host_group_ptr);
             b.slot_base = base;
             base += static_cast<int64_t>(b.host_nodes.size());
         }

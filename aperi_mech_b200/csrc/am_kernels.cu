@@ -1004,6 +1004,14 @@ __global__ void __launch_bounds__(256) k_cell_force_group(CellBlockDev b, const 
     }
 }
 
+__device__ __forceinline__ void warp_sum2(double& x, double& y) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        x += __shfl_xor_sync(kFull, x, off);
+        y += __shfl_xor_sync(kFull, y, off);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Cell-stress form of the generic cell path (ComputeInternalForceSmoothedCell.h:416-442
 // with the scatter turned into a gather). The cell kernel writes per cell the nine values
@@ -1077,29 +1085,30 @@ __device__ __forceinline__ void load_cell_matrix(const T* M, int64_t E, int32_t 
 // Cell octets: H over the rows (UNR rows per lane in flight: the batch's displacement
 // gathers issued together, the next batch's records loaded while they are in flight),
 // combined over the four lanes of a cell, P(H), and M_c written by lanes k = 0, 1, 2.
-template <typename T, int MAT, int UNR>
+template <typename T, int MAT, int UNR, bool FBAR, int G>
 __global__ void __launch_bounds__(256) k_cell_stress(CellBlockDev b, const double4* __restrict__ U4, T* __restrict__ M,
                                                      int* status) {
+    constexpr int L = 32 / G;  // lanes per cell
     pdl_trigger();
     const int64_t o = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    const int lane = static_cast<int>(threadIdx.x & 31), j = lane & 7, k = lane >> 3;
-    const int64_t c = 8 * o + j;
+    const int lane = static_cast<int>(threadIdx.x & 31), j = lane % G, k = lane / G;
+    const int64_t c = G * o + j;
     const bool valid = c < b.num_cells;
     const bool live = o < b.num_octets;
     const int32_t r0 = live ? b.o_ptr[o] : 0, rows = live ? b.o_ptr[o + 1] - r0 : 0;
-    const vec4_t<T>* rec = cell_recs<T>(b) + 8 * static_cast<int64_t>(r0) + j;
+    const vec4_t<T>* rec = cell_recs<T>(b) + G * static_cast<int64_t>(r0) + j;
     const int32_t ref = valid ? b.c_ref[c] : -1;
     const bool diff = sizeof(T) == 4;
     vec4_t<T> rr[UNR];
 #pragma unroll
-    for (int u = 0; u < UNR; ++u) rr[u] = k + 4 * u < rows ? ld_rec(rec + 8 * (k + 4 * u)) : pad_rec<T>();
+    for (int u = 0; u < UNR; ++u) rr[u] = k + L * u < rows ? ld_rec(rec + G * (k + L * u)) : pad_rec<T>();
     pdl_wait();
     const double4 ur = ref >= 0 ? ld_dep(U4 + ref) : make_double4(0.0, 0.0, 0.0, 0.0);
     T H[9];
 #pragma unroll
     for (int q = 0; q < 9; ++q) H[q] = T(0);
 #pragma unroll 1
-    for (int32_t r = k; r < rows; r += 4 * UNR) {
+    for (int32_t r = k; r < rows; r += L * UNR) {
         double4 uu[UNR];
 #pragma unroll
         for (int u = 0; u < UNR; ++u) {
@@ -1109,8 +1118,8 @@ __global__ void __launch_bounds__(256) k_cell_stress(CellBlockDev b, const doubl
         vec4_t<T> nx[UNR];
 #pragma unroll
         for (int u = 0; u < UNR; ++u) {
-            const int32_t rn = r + 4 * (UNR + u);
-            nx[u] = rn < rows ? ld_rec(rec + 8 * rn) : pad_rec<T>();
+            const int32_t rn = r + L * (UNR + u);
+            nx[u] = rn < rows ? ld_rec(rec + G * rn) : pad_rec<T>();
         }
 #pragma unroll
         for (int u = 0; u < UNR; ++u) {
@@ -1125,12 +1134,17 @@ __global__ void __launch_bounds__(256) k_cell_stress(CellBlockDev b, const doubl
 #pragma unroll
         for (int u = 0; u < UNR; ++u) rr[u] = nx[u];
     }
-    // the four lanes of a cell (j, j + 8, j + 16, j + 24): fixed pairing, same H on each
+    // the L lanes of a cell (j, j + G, ...): fixed pairing, same H on each
 #pragma unroll
-    for (int off = 8; off < 32; off <<= 1)
+    for (int off = G; off < 32; off <<= 1)
 #pragma unroll
         for (int q = 0; q < 9; ++q) H[q] += __shfl_xor_sync(kFull, H[q], off);
     if (!valid || ref < 0) return;
+    if constexpr (FBAR) {
+        // F-bar subcells: H goes to the matrix array; the per-vertex kernel forms M from it
+        store_cell_matrix<T>(M, b.num_cells, c, k, H);
+        return;
+    }
     double lam, mu;
     element_lame(b, c, lam, mu);
     T P[9];
@@ -1143,26 +1157,104 @@ __global__ void __launch_bounds__(256) k_cell_stress(CellBlockDev b, const doubl
     store_cell_matrix<T>(M, b.num_cells, c, k, m);
 }
 
+// F-bar in the cell-stress form (ComputeInternalForceSmoothedCell.h:354-413): a warp per
+// cell (group of at most 32 subcells), a lane per subcell. H of each subcell comes from the
+// octet kernel; J-bar = sum J V / sum V over the cell, the subcell's F-bar stress and the
+// dual pressure as in k_fbar_fused, and M = -V P replaces H in the matrix array for the
+// node-major gather.
+template <typename T, int MAT>
+__global__ void __launch_bounds__(256) k_fbar_cell_stress(CellBlockDev b, T* __restrict__ M, int* status) {
+    pdl_trigger();
+    const int lane = static_cast<int>(threadIdx.x & 31);
+    const int64_t g = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const bool gvalid = g < b.num_groups;
+    const int64_t s0 = gvalid ? b.group_ptr[g] : 0;
+    const int ns = gvalid ? static_cast<int>(b.group_ptr[g + 1] - s0) : 0;
+    const bool own = lane < ns;
+    const int64_t s = s0 + lane;
+    const double V = own ? b.volumes[s] : 0.0;
+    double lam = 0.0, mu = 0.0;
+    if (own) element_lame(b, s, lam, mu);
+    pdl_wait();
+    T H[9];
+    double J = 1.0;
+    if (own) {
+        load_cell_matrix(M, b.num_cells, static_cast<int32_t>(s), H);
+        J = det_ap_im1(H) + 1.0;
+        if (!(J > 0.0)) flag(status, AM_ENONPOS_J, s);
+    }
+    double jv = own ? J * V : 0.0, vol = own ? V : 0.0;
+    warp_sum2(jv, vol);
+    const double Jbar = ns > 0 ? jv / vol : 1.0;
+    double js = 1.0, pd = 0.0, unused = 0.0;
+    T Pb[9];
+    if (own) {
+        const double ratio = Jbar / J;
+        js = cbrt(ratio);
+        T Hb[9];
+        if (fabs(ratio - 1.0) < 3.0 * 2.2204460492503131e-16) {
+#pragma unroll
+            for (int m = 0; m < 9; ++m) Hb[m] = H[m];
+        } else {
+#pragma unroll
+            for (int m = 0; m < 9; ++m) Hb[m] = H[m] * T(js);
+            Hb[0] += T(js - 1.0);
+            Hb[4] += T(js - 1.0);
+            Hb[8] += T(js - 1.0);
+        }
+        const double Jb = stress<T>(MAT, T(lam), T(mu), Hb, Pb);
+        if (MAT == kNeoHookean && !(Jb > 0.0)) flag(status, AM_ENONPOS_J, s);
+        double pf = static_cast<double>(Pb[0] + Pb[4] + Pb[8]);
+#pragma unroll
+        for (int m = 0; m < 9; ++m) pf += static_cast<double>(Pb[m] * H[m]);
+        pd = js / (3.0 * Jbar) * V * pf;
+    }
+    warp_sum2(pd, unused);
+    if (!own) return;
+    pd /= vol;
+    T F[9];
+#pragma unroll
+    for (int m = 0; m < 9; ++m) F[m] = H[m];
+    F[0] += T(1);
+    F[4] += T(1);
+    F[8] += T(1);
+    double pf = 0.0;
+#pragma unroll
+    for (int m = 0; m < 9; ++m) pf += static_cast<double>(Pb[m] * F[m]);
+    const T scal = T(pd - js / (3.0 * J) * pf);
+    T A[9];
+    adj3(F, A);
+    const T Vt = T(V);
+    T m[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) m[i * 3 + j] = -Vt * (Pb[i * 3 + j] * T(js) + scal * A[j * 3 + i]);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) store_cell_matrix<T>(M, b.num_cells, s, k, m);
+}
+
 // Node octets: f = sum of M_c b over the rows in FP64 (products in the slot precision),
 // combined over the node's four lanes, written to the node's slot by lane k = 0.
-template <typename T, int UNR>
+template <typename T, int UNR, int G>
 __global__ void __launch_bounds__(256) k_cell_gather(CellBlockDev b, const T* __restrict__ M, vec4_t<T>* __restrict__ slots) {
+    constexpr int L = 32 / G;  // lanes per node
     pdl_trigger();
     const int64_t o = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    const int lane = static_cast<int>(threadIdx.x & 31), j = lane & 7, k = lane >> 3;
-    const int64_t i = 8 * o + j;
+    const int lane = static_cast<int>(threadIdx.x & 31), j = lane % G, k = lane / G;
+    const int64_t i = G * o + j;
     const bool valid = i < b.t_count;
     const bool live = o < b.num_node_octets;
     const int32_t r0 = live ? b.n_ptr[o] : 0, rows = live ? b.n_ptr[o + 1] - r0 : 0;
     const int32_t pos = valid && k == 0 ? b.slot_pos[i] : 0;
-    const vec4_t<T>* rec = node_recs<T>(b) + 8 * static_cast<int64_t>(r0) + j;
+    const vec4_t<T>* rec = node_recs<T>(b) + G * static_cast<int64_t>(r0) + j;
     vec4_t<T> rr[UNR];
 #pragma unroll
-    for (int u = 0; u < UNR; ++u) rr[u] = k + 4 * u < rows ? ld_rec(rec + 8 * (k + 4 * u)) : pad_rec<T>();
+    for (int u = 0; u < UNR; ++u) rr[u] = k + L * u < rows ? ld_rec(rec + G * (k + L * u)) : pad_rec<T>();
     pdl_wait();
     double f[3] = {0.0, 0.0, 0.0};
 #pragma unroll 1
-    for (int32_t r = k; r < rows; r += 4 * UNR) {
+    for (int32_t r = k; r < rows; r += L * UNR) {
         T mm[UNR][9];
 #pragma unroll
         for (int u = 0; u < UNR; ++u) {
@@ -1177,8 +1269,8 @@ __global__ void __launch_bounds__(256) k_cell_gather(CellBlockDev b, const T* __
         vec4_t<T> nx[UNR];
 #pragma unroll
         for (int u = 0; u < UNR; ++u) {
-            const int32_t rn = r + 4 * (UNR + u);
-            nx[u] = rn < rows ? ld_rec(rec + 8 * rn) : pad_rec<T>();
+            const int32_t rn = r + L * (UNR + u);
+            nx[u] = rn < rows ? ld_rec(rec + G * rn) : pad_rec<T>();
         }
 #pragma unroll
         for (int u = 0; u < UNR; ++u) {
@@ -1190,7 +1282,7 @@ __global__ void __launch_bounds__(256) k_cell_gather(CellBlockDev b, const T* __
         for (int u = 0; u < UNR; ++u) rr[u] = nx[u];
     }
 #pragma unroll
-    for (int off = 8; off < 32; off <<= 1)
+    for (int off = G; off < 32; off <<= 1)
 #pragma unroll
         for (int a = 0; a < 3; ++a) f[a] += __shfl_xor_sync(kFull, f[a], off);
     if (valid && k == 0) slots[pos] = make4(T(f[0]), T(f[1]), T(f[2]));
@@ -1478,13 +1570,6 @@ __global__ void __launch_bounds__(256) k_fbar_force(CellBlockDev b, vec4_t<T>* _
 constexpr int kFbarMaxSub = 32;
 constexpr int kFbarWarps = 4;
 
-__device__ __forceinline__ void warp_sum2(double& x, double& y) {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        x += __shfl_xor_sync(kFull, x, off);
-        y += __shfl_xor_sync(kFull, y, off);
-    }
-}
 
 template <typename T, int MAT>
 __global__ void __launch_bounds__(32 * kFbarWarps) k_fbar_fused(CellBlockDev b, const double4* __restrict__ U4,
@@ -2769,15 +2854,34 @@ void launch_fbar(const CellBlockDev& b, const double4* U4, void* slots, int* sta
     }
 }
 
+template <typename T, int UNR, int G>
+void launch_cell_stress_g(const CellBlockDev& b, const double4* U4, int* status, cudaStream_t s) {
+    if (b.group_ptr != nullptr) {
+        // F-bar: H per subcell, then M per cell of subcells
+        launch_pdl(k_cell_stress<T, kLinearElastic, UNR, true, G>, grid_for(b.num_octets * 32, 256), 256, s, b, U4,
+                   static_cast<T*>(b.cmat), status);
+        AM_DISPATCH_MAT(b.material, (launch_pdl(k_fbar_cell_stress<T, M>, grid_for(b.num_groups * 32, 256), 256, s, b,
+                                                static_cast<T*>(b.cmat), status)));
+        return;
+    }
+    AM_DISPATCH_MAT(b.material, (launch_pdl(k_cell_stress<T, M, UNR, false, G>, grid_for(b.num_octets * 32, 256), 256, s, b,
+                                            U4, static_cast<T*>(b.cmat), status)));
+}
 template <typename T, int UNR>
 void launch_cell_stress_unr(const CellBlockDev& b, const double4* U4, int* status, cudaStream_t s) {
-    AM_DISPATCH_MAT(b.material, (launch_pdl(k_cell_stress<T, M, UNR>, grid_for(b.num_octets * 32, 256), 256, s, b, U4,
-                                            static_cast<T*>(b.cmat), status)));
+    if (b.group_items[0] == 1)
+        launch_cell_stress_g<T, UNR, 1>(b, U4, status, s);
+    else
+        launch_cell_stress_g<T, UNR, 8>(b, U4, status, s);
 }
 template <typename T, int UNR>
 void launch_cell_gather_unr(const CellBlockDev& b, void* slots, cudaStream_t s) {
-    launch_pdl(k_cell_gather<T, UNR>, grid_for(b.num_node_octets * 32, 256), 256, s, b, static_cast<const T*>(b.cmat),
-               static_cast<vec4_t<T>*>(slots));
+    if (b.group_items[1] == 1)
+        launch_pdl(k_cell_gather<T, UNR, 1>, grid_for(b.num_node_octets * 32, 256), 256, s, b, static_cast<const T*>(b.cmat),
+                   static_cast<vec4_t<T>*>(slots));
+    else
+        launch_pdl(k_cell_gather<T, UNR, 8>, grid_for(b.num_node_octets * 32, 256), 256, s, b, static_cast<const T*>(b.cmat),
+                   static_cast<vec4_t<T>*>(slots));
 }
 // Rows in flight per lane: unroll[0] (cell kernel) and unroll[1] (gather kernel), 1, 2 or 4.
 template <typename T>
@@ -2805,7 +2909,7 @@ int launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void*
             launch_cell_gather_form<float>(b, U4, slots, status, s);
         else
             launch_cell_gather_form<double>(b, U4, slots, status, s);
-        return 2;
+        return b.group_ptr != nullptr ? 3 : 2;
     }
     if (b.patched == 2) {
         const unsigned grid = grid_for(2 * b.num_patches, kHex6Block);

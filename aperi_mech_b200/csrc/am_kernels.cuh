@@ -100,6 +100,7 @@ struct CellBlockDev {
     // kernels walk octets of eight items: octet o's rows are o_ptr[o] .. o_ptr[o+1] (cells)
     // or n_ptr (nodes), row r of item j at record 8 r + j: gradient in x, y, z, the partner
     // index (node, or cell) in w, -1 for padding. c_ref: a node of each cell (-1: empty).
+    // With group_items 1 instead of 8 a side's warps take one item each (rows = its entries).
     int32_t gather;
     int64_t num_octets;
     const int32_t* o_ptr;
@@ -112,6 +113,7 @@ struct CellBlockDev {
     const float4* nrec32;
     const double4* nrec64;
     void* cmat;
+    int32_t group_items[2];  // items per warp (8, or 1 for items of many entries): cell side, node side
     int32_t unroll[2];  // rows per lane in flight (1, 2 or 4): cell kernel, gather kernel
 };
 constexpr int kFbarStride = 20;

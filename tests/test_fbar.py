@@ -165,15 +165,19 @@ def test_nodal_subcells_setup_matches_oracle(gpu, oracle_lib):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("passes", ["fused", "three"])
+@pytest.mark.parametrize("passes", ["cell_stress", "fused", "three"])
 @pytest.mark.parametrize("kind", ["neo_hookean", "linear_elastic"])
 def test_fbar_force_and_steps_match_oracle(gpu, oracle_lib, kind, passes, monkeypatch):
-    """F-bar force (FP64 and mixed) and 20 steps with a held face against the oracle, with
-    the one-pass kernel (cells of at most 32 subcells) and with the three-pass form."""
+    """F-bar force (FP64 and mixed) and 20 steps with a held face against the oracle: in the
+    cell-stress form (the default for cells of at most 32 subcells: H per subcell, M per
+    cell, node-major gather), with the one-pass kernel writing per-entry slots
+    (APERI_B200_CELL_GATHER=0) and with the three-pass form."""
     from aperi_mech_b200 import mesh
 
     if passes == "three":
         monkeypatch.setenv("APERI_B200_FBAR_PASSES", "3")
+    if passes == "fused":
+        monkeypatch.setenv("APERI_B200_CELL_GATHER", "0")
     from aperi_mech_b200.model import BoundaryCondition, ExplicitDynamics
     from aperi_mech_b200.rkpm import nodal_subcells
 
