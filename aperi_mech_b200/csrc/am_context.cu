@@ -674,6 +674,14 @@ struct am_ctx {
     int64_t* rkt_ptr = nullptr;       // N + 1: columns of Psi (transposed CSR)
     int32_t* rkt_src = nullptr;
     double* rkt_val = nullptr;
+    // The same rows and columns in warp octets (APERI_B200_RK_OCTETS=0 keeps the CSR kernels):
+    // octet row offsets and (value, index) records.
+    bool rk_octets = true;
+    int64_t rko_count = 0, rkto_count = 0;
+    int32_t* rko_ptr = nullptr;
+    int32_t* rkto_ptr = nullptr;
+    double2* rko_rec = nullptr;
+    double2* rkto_rec = nullptr;
     double4* rk_u = nullptr;          // physical displacement Psi U
     double4* rk_f_local = nullptr;    // element forces at the nodes
     double* rk_f = nullptr;           // N x 3: generalized force Psi^T f_local
@@ -744,7 +752,10 @@ struct am_ctx {
         }
         if (num_points > N && !rk_ptr) fail(AM_ESTATE, "cells on refinement points run after am_set_rk_functions");
         if (rk_ptr) {
-            am::launch_rk_rows4(points(), N, rk_ptr, rk_nbr, rk_val, U, rk_u, stream);
+            if (rko_rec)
+                am::launch_rk_octets(points(), rko_count, rko_ptr, rko_rec, U, rk_ptr, N, rk_u, nullptr, stream);
+            else
+                am::launch_rk_rows4(points(), N, rk_ptr, rk_nbr, rk_val, U, rk_u, stream);
             ++launches;
             U = rk_u;
         }
@@ -762,7 +773,10 @@ struct am_ctx {
             nd.f_given = nullptr;
             nd.num_nodes = points();  // the local force lives on the points
             am::launch_gather_force4(nd, mixed, s, rk_f_local, stream);
-            am::launch_rk_cols3(N, rkt_ptr, rkt_src, rkt_val, rk_f_local, rk_f, stream);
+            if (rkto_rec)
+                am::launch_rk_octets(N, rkto_count, rkto_ptr, rkto_rec, rk_f_local, nullptr, N, nullptr, rk_f, stream);
+            else
+                am::launch_rk_cols3(N, rkt_ptr, rkt_src, rkt_val, rk_f_local, rk_f, stream);
             launches += 2;
         }
         check_launch("element force kernel");
@@ -1213,6 +1227,10 @@ struct am_ctx {
         dfree(rkt_ptr);
         dfree(rkt_src);
         dfree(rkt_val);
+        dfree(rko_ptr);
+        dfree(rkto_ptr);
+        dfree(rko_rec);
+        dfree(rkto_rec);
         dfree(rk_u);
         dfree(rk_f_local);
         dfree(rk_f);
@@ -1369,6 +1387,8 @@ int am_create(int64_t num_nodes, const double* coords, am_ctx** out) {
         c->use_graphs = !(graphs && graphs[0] == '0');
         const char* nl = std::getenv("APERI_B200_NODE_LANES");
         c->node_lanes = nl ? std::atoi(nl) : 0;
+        const char* ro = std::getenv("APERI_B200_RK_OCTETS");
+        c->rk_octets = !(ro && ro[0] == '0');
         const char* tg = std::getenv("APERI_B200_TET4_GEOMETRY");
         c->tet_geometry = !(tg && tg[0] == '0');
         const char* cg = std::getenv("APERI_B200_CELL_GATHER");
@@ -2442,6 +2462,38 @@ int am_set_rk_functions(am_ctx* ctx, const int64_t* nbr_ptr, const int32_t* nbr,
             dst = dalloc<T0>(static_cast<size_t>(std::max<int64_t>(n, 1)), what);
             if (n > 0) ck(cudaMemcpy(dst, src, n * sizeof(T0), cudaMemcpyHostToDevice), "upload");
         };
+        if (ctx->rk_octets) {
+            // rows sorted by node and columns (ascending point already) in warp octets
+            auto octets = [&](int64_t count, const std::vector<int32_t>& ptr, const std::vector<int32_t>& part,
+                              const std::vector<double>& w, int32_t*& optr, double2*& rec, int64_t& n_oct) {
+                const OctetRows o = octet_rows(count, ptr, part);
+                std::vector<double2> h(o.src.size());
+                for (size_t q = 0; q < h.size(); ++q) {
+                    const int32_t e = o.src[q];
+                    h[q] = e < 0 ? make_double2(0.0, bits64(-1)) : make_double2(w[e], bits64(part[e]));
+                }
+                n_oct = static_cast<int64_t>(o.ptr.size()) - 1;
+                up(optr, o.ptr.data(), static_cast<int64_t>(o.ptr.size()), "function octet rows");
+                up(rec, h.data(), static_cast<int64_t>(h.size()), "function octet records");
+            };
+            std::vector<int32_t> rptr(NP + 1), rpart(static_cast<size_t>(K));
+            std::vector<double> rval(static_cast<size_t>(K));
+            std::vector<int64_t> perm;
+            for (int64_t i = 0; i < NP; ++i) {
+                rptr[i] = static_cast<int32_t>(nbr_ptr[i]);
+                perm.resize(static_cast<size_t>(nbr_ptr[i + 1] - nbr_ptr[i]));
+                for (size_t q = 0; q < perm.size(); ++q) perm[q] = nbr_ptr[i] + static_cast<int64_t>(q);
+                std::stable_sort(perm.begin(), perm.end(), [&](int64_t a, int64_t b) { return nbr[a] < nbr[b]; });
+                for (size_t q = 0; q < perm.size(); ++q) {
+                    rpart[nbr_ptr[i] + q] = nbr[perm[q]];
+                    rval[nbr_ptr[i] + q] = values[perm[q]];
+                }
+            }
+            rptr[NP] = static_cast<int32_t>(K);
+            std::vector<int32_t> cptr(tptr.begin(), tptr.end());
+            octets(NP, rptr, rpart, rval, ctx->rko_ptr, ctx->rko_rec, ctx->rko_count);
+            octets(N, cptr, tsrc, tval, ctx->rkto_ptr, ctx->rkto_rec, ctx->rkto_count);
+        }
         up(ctx->rk_ptr, nbr_ptr, NP + 1, "function offsets");
         up(ctx->rk_nbr, nbr, K, "function neighbours");
         up(ctx->rk_val, values, K, "function values");

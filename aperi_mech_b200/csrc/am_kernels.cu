@@ -2594,6 +2594,70 @@ __global__ void __launch_bounds__(128) k_rk_cols3(int64_t n, const int64_t* __re
     f[3 * j + 2] = z;
 }
 
+// The coupling in warp octets (the row layout of the cell-stress form): item i (a point for
+// the rows of Psi, a node for its columns) sums w * in[idx] over its rows, lane 8k + j taking
+// item j of the octet and rows k, k + 4, ...; records are (w, idx) pairs in one 16-byte load,
+// idx -1 for padding. Rows are aligned by offset where that pads little, so a quarter-warp's
+// eight gathers read consecutive nodes or points. Rows of Psi without neighbours copy the
+// node's coefficient (out4 set, row_ptr the original offsets); columns write out3.
+template <int UNR>
+__global__ void __launch_bounds__(256) k_rk_octets(int64_t count, int64_t num_octets, const int32_t* __restrict__ optr,
+                                                   const double2* __restrict__ rec, const double4* __restrict__ in,
+                                                   const int64_t* __restrict__ row_ptr, int64_t num_nodes,
+                                                   double4* __restrict__ out4, double* __restrict__ out3) {
+    const int64_t o = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = static_cast<int>(threadIdx.x & 31), j = lane & 7, k = lane >> 3;
+    const int64_t i = 8 * o + j;
+    const bool valid = i < count;
+    const bool live = o < num_octets;
+    const int32_t r0 = live ? optr[o] : 0, rows = live ? optr[o + 1] - r0 : 0;
+    const double2* rp = rec + 8 * static_cast<int64_t>(r0) + j;
+    const double2 pad = make_double2(0.0, __longlong_as_double(-1LL));
+    double2 rr[UNR];
+#pragma unroll
+    for (int u = 0; u < UNR; ++u) rr[u] = k + 4 * u < rows ? __ldg(rp + 8 * (k + 4 * u)) : pad;
+    double x = 0.0, y = 0.0, z = 0.0;
+#pragma unroll 1
+    for (int32_t r = k; r < rows; r += 4 * UNR) {
+        double4 g[UNR];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const int32_t idx = static_cast<int32_t>(__double_as_longlong(rr[u].y));
+            g[u] = idx >= 0 ? ld_ro4(in + idx) : make_double4(0.0, 0.0, 0.0, 0.0);
+        }
+        double2 nx[UNR];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const int32_t rn = r + 4 * (UNR + u);
+            nx[u] = rn < rows ? __ldg(rp + 8 * rn) : pad;
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            x += rr[u].x * g[u].x;
+            y += rr[u].x * g[u].y;
+            z += rr[u].x * g[u].z;
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) rr[u] = nx[u];
+    }
+#pragma unroll
+    for (int off = 8; off < 32; off <<= 1) {
+        x += __shfl_xor_sync(kFull, x, off);
+        y += __shfl_xor_sync(kFull, y, off);
+        z += __shfl_xor_sync(kFull, z, off);
+    }
+    if (!valid || k != 0) return;
+    if (out4 != nullptr) {
+        out4[i] = row_ptr[i + 1] != row_ptr[i] ? make_double4(x, y, z, 0.0)
+                  : i < num_nodes              ? in[i]
+                                               : make_double4(0.0, 0.0, 0.0, 0.0);
+    } else {
+        out3[3 * i] = x;
+        out3[3 * i + 1] = y;
+        out3[3 * i + 2] = z;
+    }
+}
+
 __global__ void k_pack4(const double* __restrict__ in, double4* __restrict__ out, int64_t n) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -3186,6 +3250,12 @@ void launch_rk_rows4(int64_t n, int64_t num_nodes, const int64_t* ptr, const int
 void launch_rk_cols3(int64_t n, const int64_t* tptr, const int32_t* tsrc, const double* tval, const double4* f_local,
                      double* f, cudaStream_t s) {
     if (n > 0) k_rk_cols3<<<grid_for(n * kRkLanes, 128), 128, 0, s>>>(n, tptr, tsrc, tval, f_local, f);
+}
+
+void launch_rk_octets(int64_t count, int64_t num_octets, const int32_t* optr, const double2* rec, const double4* in,
+                      const int64_t* row_ptr, int64_t num_nodes, double4* out4, double* out3, cudaStream_t s) {
+    if (count > 0) k_rk_octets<4><<<grid_for(num_octets * 32, 256), 256, 0, s>>>(count, num_octets, optr, rec, in, row_ptr,
+                                                                                num_nodes, out4, out3);
 }
 
 void launch_pack4(const double* aos3, double4* out, int64_t n, cudaStream_t s) {

@@ -215,6 +215,8 @@ void launch_sensor_seed(const double4* U4, int32_t num_sensors, const int32_t* s
                         cudaStream_t s);
 
 // Layout conversion.
+void launch_rk_octets(int64_t count, int64_t num_octets, const int32_t* optr, const double2* rec, const double4* in,
+                      const int64_t* row_ptr, int64_t num_nodes, double4* out4, double* out3, cudaStream_t s);
 void launch_pack4(const double* aos3, double4* out, int64_t n, cudaStream_t s);
 void launch_unpack4(const double4* in, double* aos3, int64_t n, cudaStream_t s);
 void launch_zero4(double4* out, int64_t n, cudaStream_t s);
