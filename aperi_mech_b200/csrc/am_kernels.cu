@@ -134,13 +134,19 @@ __device__ __forceinline__ T tet4_forces(const T* J, const T* D, double lam, dou
         // det F stays FP64; the FP32 path takes its scale from an FP32 reciprocal of
         // 6 det F (on B200 1.7% off the kernel against the FP64 division).
         const T sc = sizeof(T) == 4 ? T(__frcp_rn(static_cast<float>(6.0 * Jf))) : T(1.0 / (6.0 * Jf));
+        // the scale folded into tau (six distinct entries)
+        T ts[9];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = i; j < 3; ++j) ts[i * 3 + j] = ts[j * 3 + i] = sc * tau[i * 3 + j];
 #pragma unroll
         for (int i = 0; i < 3; ++i) f[i] = T(0);
 #pragma unroll
         for (int k = 0; k < 3; ++k)
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
-                const T q = sc * (A[k * 3 + 0] * tau[0 * 3 + i] + A[k * 3 + 1] * tau[1 * 3 + i] + A[k * 3 + 2] * tau[2 * 3 + i]);
+                const T q = A[k * 3 + 0] * ts[0 * 3 + i] + A[k * 3 + 1] * ts[1 * 3 + i] + A[k * 3 + 2] * ts[2 * 3 + i];
                 f[(k + 1) * 3 + i] = -q;
                 f[i] += q;
             }
@@ -276,11 +282,16 @@ __global__ void __launch_bounds__(256) k_tet4_force_geo(GaussBlockDev b, const d
 #pragma unroll
             for (int j = 0; j < 3; ++j) K[i * 3 + j] = Ji[i * 3 + 0] * AF[0 * 3 + j] + Ji[i * 3 + 1] * AF[1 * 3 + j] + Ji[i * 3 + 2] * AF[2 * 3 + j];
         const T sc = sizeof(T) == 4 ? T(w * __frcp_rn(static_cast<float>(Jf))) : T(w / Jf);
+        T ts[9];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = i; j < 3; ++j) ts[i * 3 + j] = ts[j * 3 + i] = sc * tau[i * 3 + j];
 #pragma unroll
         for (int k = 0; k < 3; ++k)
 #pragma unroll
             for (int i = 0; i < 3; ++i)
-                Q[k * 3 + i] = sc * (K[k * 3 + 0] * tau[0 * 3 + i] + K[k * 3 + 1] * tau[1 * 3 + i] + K[k * 3 + 2] * tau[2 * 3 + i]);
+                Q[k * 3 + i] = K[k * 3 + 0] * ts[0 * 3 + i] + K[k * 3 + 1] * ts[1 * 3 + i] + K[k * 3 + 2] * ts[2 * 3 + i];
     } else {
         T P[9];
         stress<T>(MAT, T(lam), T(mu), H, P);
@@ -699,11 +710,16 @@ __global__ void __launch_bounds__(sizeof(T) == 8 ? 64 : 128, sizeof(T) == 8 ? 1 
             for (int k = 0; k < 9; ++k) Jc[k] = J[k] + G[k];
             adj3(Jc, Ac);
             const T sc = sizeof(T) == 4 ? T(__frcp_rn(static_cast<float>(Jf))) : T(1.0 / Jf);
+            T ts[9];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = i; j < 3; ++j) ts[i * 3 + j] = ts[j * 3 + i] = sc * tau[i * 3 + j];
 #pragma unroll
             for (int k = 0; k < 3; ++k)
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
-                    Q[k * 3 + i] = sc * (Ac[k * 3 + 0] * tau[0 * 3 + i] + Ac[k * 3 + 1] * tau[1 * 3 + i] + Ac[k * 3 + 2] * tau[2 * 3 + i]);
+                    Q[k * 3 + i] = Ac[k * 3 + 0] * ts[0 * 3 + i] + Ac[k * 3 + 1] * ts[1 * 3 + i] + Ac[k * 3 + 2] * ts[2 * 3 + i];
         } else {
             stress<T>(MAT, T(lam), T(mu), H, P);
 #pragma unroll

@@ -89,6 +89,7 @@ __device__ __forceinline__ double log1p_nh(double x) {
 //   St-Venant-K.    (Elastic.h:70-78):       E = (H + H^T + H^T H)/2, S = lambda tr(E) I + 2 mu E, P = F S
 // Neo-Hookean Kirchhoff stress tau = lambda log1p(J-1) I + mu (H H^T + H + H^T)
 // (NeoHooke.h:79-91); returns J = det F (FP64).
+// tau is symmetric: the upper triangle is formed and mirrored.
 template <typename T>
 __device__ __forceinline__ double nh_kirchhoff(T lambda, T mu, const T* H, T* tau) {
     const double Jm1 = det_ap_im1(H);
@@ -96,9 +97,10 @@ __device__ __forceinline__ double nh_kirchhoff(T lambda, T mu, const T* H, T* ta
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) {
+        for (int j = i; j < 3; ++j) {
             const T hh = H[i * 3 + 0] * H[j * 3 + 0] + H[i * 3 + 1] * H[j * 3 + 1] + H[i * 3 + 2] * H[j * 3 + 2];
             tau[i * 3 + j] = mu * (hh + H[j * 3 + i] + H[i * 3 + j]) + (i == j ? lam_lnJ : T(0));
+            if (j != i) tau[j * 3 + i] = tau[i * 3 + j];
         }
     return 1.0 + Jm1;
 }
