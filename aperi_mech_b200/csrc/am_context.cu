@@ -1836,7 +1836,9 @@ int am_set_state(am_ctx* ctx, am_memory where, const double* u, const double* v,
         load_nodal(ctx, where, u, ctx->U4);
         load_nodal(ctx, where, v, ctx->V4);
         load_nodal(ctx, where, a, ctx->A4);
-        if (u && ctx->lagr) ctx->reset_lagrangian();
+        // The displacement is always set (null: zero), so the updated / semi state restarts
+        // from the undeformed configuration with it.
+        if (ctx->lagr) ctx->reset_lagrangian();
         if (where == AM_HOST) ck(cudaStreamSynchronize(ctx->stream), "synchronize");
     });
 }

@@ -416,14 +416,17 @@ def mixed_errors(prob, steps_total, s64, sm, f64=None, fm=None):
     return out
 
 
-def measure_workload(torch, prob, steps, warmup, stream, dev, world, mass=None, precs=("fp64", "mixed"), fma=None):
+def measure_workload(torch, prob, steps, warmup, stream, dev, world, mass=None, precs=("fp64", "mixed"), fma=None,
+                     formulation=None):
     from aperi_mech_b200.model import ExplicitDynamics
 
     out = {"workload": prob.name, "elements": prob.num_elems, "nodes": prob.num_nodes, "steps": steps,
            "dt": prob.dt, "config": prob.meta.get("config")}
+    if formulation is not None:
+        out["formulation"] = list(formulation)
     peak, kind = measured_peaks()
     with ExplicitDynamics(prob.coords, prob.parts, prob.bcs, mass=mass, stream=stream.cuda_stream,
-                          rk=prob.meta.get("rk")) as m:
+                          rk=prob.meta.get("rk"), formulation=formulation) as m:
         layout = m.layout()
         states = {}
         for prec in precs:
@@ -652,6 +655,13 @@ def run_ours(args, rank, world, local):
             r["vs_structured_mixed"] = r["mixed"]["value"] / res["mixed"]["value"]
             r["vs_structured_fp64"] = r["fp64"]["value"] / res["fp64"]["value"]
             extras[f"tet4_nh_shear_renumbered_{label}"] = r
+        # The updated and semi-Lagrangian formulations (FP64) on the headline mesh: the current
+        # (or last reference) coordinates, the displacement increment and the element H on the
+        # device, the reference update every 10 steps (semi) or every step (updated).
+        pl = problems.tet4_nh_shear(n=args.n, seed=0, nsteps=200)
+        for label, form in (("semi_10", ("semi", 10)), ("updated", ("updated", 1))):
+            extras[f"tet4_nh_shear_{label}"] = measure_workload(torch, pl, 200, args.warmup, stream, dev, world,
+                                                              precs=("fp64",), fma=fma, formulation=form)
         p5 = problems.hex8_nh_lognormal(n=args.hex_n, seed=0, nsteps=1000, bulk_field=True)
         extras["hex8_nh_lognormal_large"] = measure_workload(torch, p5, 1000, args.warmup, stream, dev, world, fma=fma)
         if not args.skip_adjoint:

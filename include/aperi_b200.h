@@ -348,8 +348,8 @@ int am_solve_power_method(am_ctx* ctx, am_precision prec, double scale_factor, i
  * stored reference gradient; forces map back through F_ref = I + Href. As in the reference,
  * an element keeps one H: for Hex8 the last Gauss point's serves as every Gauss point's
  * reference (Tet4, with one point, matches the total formulation to round-off). State
- * starts undeformed and is reset by am_set_state with a displacement (which should be
- * zero); FP64 only; Gauss blocks only; not with am_internal_force, the VJP, the adjoint,
+ * starts undeformed and is reset by every am_set_state (whose displacement, null meaning
+ * zero, should be zero); FP64 only; Gauss blocks only; not with am_internal_force, the VJP, the adjoint,
  * the power method, the two-pass coupling or a decomposed mesh (AM_ESTATE). Call after
  * am_create and before am_add_block (Tet4 blocks then keep per-element slots). */
 int am_set_formulation(am_ctx* ctx, int32_t formulation, int32_t update_interval);

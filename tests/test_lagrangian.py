@@ -136,8 +136,17 @@ def test_lagrangian_steps_match_oracle(gpu, oracle_lib, kind, form, k):
             m.internal_force(z)
         with pytest.raises(Exception):
             m.run(1, p.dt, "mixed")
+        # a second run from rest (the displacement given as null, i.e. zero) restarts the
+        # formulation's state too: bitwise the first run
+        m.set_state(None, p.v0)
+        m.init_acceleration()
+        m.run(9, p.dt)
+        m.run(21, p.dt, t0=9 * p.dt)
+        again = m.get_state()
     for g, w in zip(got, want):
         assert rel_err(g, w) < 1e-12
+    for g, h in zip(got, again):
+        assert np.array_equal(g, h)
 
 
 @pytest.mark.gpu
