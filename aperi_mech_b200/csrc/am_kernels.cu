@@ -752,14 +752,22 @@ __global__ void __launch_bounds__(sizeof(T) == 8 ? 64 : 128, sizeof(T) == 8 ? 1 
 // F_ref = I + Href: B F_ref and w / det F_ref. The element keeps one H (for Hex8 the last
 // Gauss point's, as the reference's element field), which is also every Gauss point's Href.
 // ---------------------------------------------------------------------------
+// The element H arrays are component-major (component k of element e at k E + e), so that a
+// warp's nine loads and stores are coalesced. They are written by the element kernel of the
+// previous step: read after the wait for the predecessor, with coherent loads.
 __device__ __forceinline__ void lagr_href(const GaussBlockDev& b, int64_t e, int32_t lagr, int rebase, double* hr) {
-    const double* src = (lagr == 1 || rebase) ? b.hstate + 9 * e : b.href + 9 * e;
+    const int64_t E = b.num_elems;
+    const double* src = (lagr == 1 || rebase) ? b.hstate : b.href;
 #pragma unroll
-    for (int k = 0; k < 9; ++k) hr[k] = src[k];
+    for (int k = 0; k < 9; ++k) hr[k] = __ldcg(src + k * E + e);
     if (lagr == 2 && rebase) {
 #pragma unroll
-        for (int k = 0; k < 9; ++k) b.href[9 * e + k] = hr[k];
+        for (int k = 0; k < 9; ++k) b.href[k * E + e] = hr[k];
     }
+}
+__device__ __forceinline__ void lagr_store_h(const GaussBlockDev& b, int64_t e, const double* H) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) b.hstate[k * b.num_elems + e] = H[k];
 }
 
 // H = dH + Href + dH Href
@@ -790,11 +798,14 @@ __global__ void __launch_bounds__(128) k_tet4_force_lagr(GaussBlockDev b, int32_
                                                           const double4* __restrict__ XC,
                                                           const double4* __restrict__ INC,
                                                           double4* __restrict__ slots, int* status) {
+    pdl_trigger();
     const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (e >= b.num_elems) return;
     const int4 c = reinterpret_cast<const int4*>(b.conn)[e];
-    const double4 x0 = XC[c.x], x1 = XC[c.y], x2 = XC[c.z], x3 = XC[c.w];
-    const double4 u0 = INC[c.x], u1 = INC[c.y], u2 = INC[c.z], u3 = INC[c.w];
+    const int32_t pos[4] = {b.slot_pos[4 * e], b.slot_pos[4 * e + 1], b.slot_pos[4 * e + 2], b.slot_pos[4 * e + 3]};
+    pdl_wait();
+    const double4 x0 = ld_dep(XC + c.x), x1 = ld_dep(XC + c.y), x2 = ld_dep(XC + c.z), x3 = ld_dep(XC + c.w);
+    const double4 u0 = ld_dep(INC + c.x), u1 = ld_dep(INC + c.y), u2 = ld_dep(INC + c.z), u3 = ld_dep(INC + c.w);
     const double J[9] = {x1.x - x0.x, x2.x - x0.x, x3.x - x0.x, x1.y - x0.y, x2.y - x0.y,
                          x3.y - x0.y, x1.z - x0.z, x2.z - x0.z, x3.z - x0.z};
     const double D[9] = {u1.x - u0.x, u2.x - u0.x, u3.x - u0.x, u1.y - u0.y, u2.y - u0.y,
@@ -811,8 +822,7 @@ __global__ void __launch_bounds__(128) k_tet4_force_lagr(GaussBlockDev b, int32_
         for (int j = 0; j < 3; ++j) dH[i * 3 + j] = D[i * 3 + 0] * Ji[0 * 3 + j] + D[i * 3 + 1] * Ji[1 * 3 + j] + D[i * 3 + 2] * Ji[2 * 3 + j];
     lagr_href(b, e, lagr, rebase, hr);
     lagr_compose(dH, hr, H);
-#pragma unroll
-    for (int k = 0; k < 9; ++k) b.hstate[9 * e + k] = H[k];
+    lagr_store_h(b, e, H);
     double lam, mu;
     element_lame(b, e, lam, mu);
     double P[9], Pm[9];
@@ -830,10 +840,10 @@ __global__ void __launch_bounds__(128) k_tet4_force_lagr(GaussBlockDev b, int32_
             f[(k + 1) * 3 + i] = -q;
             f[i] += q;
         }
-    slots[b.slot_pos[4 * e]] = make4(f[0], f[1], f[2]);
-    slots[b.slot_pos[4 * e + 1]] = make4(f[3], f[4], f[5]);
-    slots[b.slot_pos[4 * e + 2]] = make4(f[6], f[7], f[8]);
-    slots[b.slot_pos[4 * e + 3]] = make4(f[9], f[10], f[11]);
+    slots[pos[0]] = make4(f[0], f[1], f[2]);
+    slots[pos[1]] = make4(f[3], f[4], f[5]);
+    slots[pos[2]] = make4(f[6], f[7], f[8]);
+    slots[pos[3]] = make4(f[9], f[10], f[11]);
 }
 
 template <int MAT>
@@ -841,13 +851,15 @@ __global__ void __launch_bounds__(64) k_hex8_force_lagr(GaussBlockDev b, int32_t
                                                          const double4* __restrict__ XC,
                                                          const double4* __restrict__ INC,
                                                          double4* __restrict__ slots, int* status) {
+    pdl_trigger();
     const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (e >= b.num_elems) return;
     int32_t nd[8];
     hex_conn(b, e, nd);
     double X[3][8], U[3][8];
-    hex_load_rel(XC, nd, X);
-    hex_load_rel(INC, nd, U);
+    pdl_wait();
+    hex_load_rel<double, true>(XC, nd, X);
+    hex_load_rel<double, true>(INC, nd, U);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
         hex_butterfly(X[i]);
@@ -886,10 +898,7 @@ __global__ void __launch_bounds__(64) k_hex8_force_lagr(GaussBlockDev b, int32_t
                 dH[i * 3 + j] = (G[i * 3 + 0] * A[0 * 3 + j] + G[i * 3 + 1] * A[1 * 3 + j] + G[i * 3 + 2] * A[2 * 3 + j]) * id;
         lagr_compose(dH, hr, H);
         // The reference's last Gauss point (its node 7 sign pattern) is corner 6 here.
-        if (g == 6) {
-#pragma unroll
-            for (int k = 0; k < 9; ++k) b.hstate[9 * e + k] = H[k];
-        }
+        if (g == 6) lagr_store_h(b, e, H);
         const double Jf = stress<double>(MAT, lam, mu, H, P);
         if (MAT == kNeoHookean) bad |= !(Jf > 0.0);
         lagr_pull(hr, P, Pm);
@@ -3253,9 +3262,9 @@ void launch_gauss_force_lagr(const GaussBlockDev& b, int32_t lagr, int rebase, c
     if (b.num_elems == 0) return;
     double4* sl = static_cast<double4*>(slots);
     if (b.kind == AM_HEX8_GAUSS) {
-        AM_DISPATCH_MAT(b.material, (k_hex8_force_lagr<M><<<grid_for(b.num_elems, 64), 64, 0, s>>>(b, lagr, rebase, XC, INC, sl, status)));
+        AM_DISPATCH_MAT(b.material, (launch_pdl(k_hex8_force_lagr<M>, grid_for(b.num_elems, 64), 64, s, b, lagr, rebase, XC, INC, sl, status)));
     } else {
-        AM_DISPATCH_MAT(b.material, (k_tet4_force_lagr<M><<<grid_for(b.num_elems, 128), 128, 0, s>>>(b, lagr, rebase, XC, INC, sl, status)));
+        AM_DISPATCH_MAT(b.material, (launch_pdl(k_tet4_force_lagr<M>, grid_for(b.num_elems, 128), 128, s, b, lagr, rebase, XC, INC, sl, status)));
     }
 }
 
