@@ -1164,12 +1164,14 @@ __global__ void __launch_bounds__(256) k_cell_stress(CellBlockDev b, const doubl
     for (int off = G; off < 32; off <<= 1)
 #pragma unroll
         for (int q = 0; q < 9; ++q) H[q] += __shfl_xor_sync(kFull, H[q], off);
-    if (!valid || ref < 0) return;
+    if (!valid) return;
     if constexpr (FBAR) {
-        // F-bar subcells: H goes to the matrix array; the per-vertex kernel forms M from it
+        // F-bar subcells: H goes to the matrix array (zero for a subcell without entries);
+        // the per-vertex kernel forms M from it
         store_cell_matrix<T>(M, b.num_cells, c, k, H);
         return;
     }
+    if (ref < 0) return;
     double lam, mu;
     element_lame(b, c, lam, mu);
     T P[9];

@@ -208,3 +208,32 @@ def test_fbar_force_and_steps_match_oracle(gpu, oracle_lib, kind, passes, monkey
     # after 20 steps the acceleration differs by about 1e-12 of its size.
     for g, w in zip(got, want):
         assert rel_err(g, w) < 1e-11
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form", ["cell_stress", "fused"])
+def test_fbar_empty_subcell_counts_in_jbar(gpu, oracle_lib, form, monkeypatch):
+    """A subcell without entries (H = 0, J = 1) still enters its cell's J-bar with its volume:
+    an empty subcell inserted at the front of one cell, both F-bar forms against the oracle."""
+    from aperi_mech_b200.model import ExplicitDynamics, Part
+    from aperi_mech_b200.rkpm import nodal_subcells
+
+    if form == "fused":
+        monkeypatch.setenv("APERI_B200_CELL_GATHER", "0")
+    n = 3
+    X, T = _box(n, seed=8)
+    mat = _material("neo_hookean")
+    cells = nodal_subcells(X, T, mat, np.full(X.shape[0], RADIUS / n))
+    p0 = cells.part
+    s = int(p0.cell_groups[1])
+    ptr = np.insert(p0.cell_ptr, s, p0.cell_ptr[s])
+    vols = np.insert(p0.cell_volumes, s, p0.cell_volumes[s])
+    groups = np.array(p0.cell_groups, dtype=np.int64)
+    groups[2:] += 1
+    part = Part("cells", mat, cell_ptr=ptr, cell_nodes=p0.cell_nodes, cell_grads=p0.cell_grads, cell_volumes=vols,
+                cell_groups=groups)
+    u = 2e-3 * np.random.default_rng(4).standard_normal(X.shape)
+    want = oracle_lib.OracleProblem(X, [part], mass=cells.mass).internal_force(u)
+    with ExplicitDynamics(X, [part], mass=cells.mass) as m:
+        assert rel_err(m.internal_force(u), want) < 1e-12
+        assert rel_err(m.internal_force(u, "mixed"), want) < 1e-4
