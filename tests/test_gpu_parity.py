@@ -585,7 +585,7 @@ def test_neighbor_exchange_single_rank_self_neighbor(gpu, prec, monkeypatch):
         assert np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("name", ["tet4_nh", "hex8_le", "cells"])
+@pytest.mark.parametrize("name", ["tet4_nh", "hex8_le", "cells", "rkpm", "fbar"])
 def test_graph_replay_is_bitwise_identical(gpu, monkeypatch, name):
     """The step loop replayed from captured CUDA graphs (chunks of 32 steps, captured at
     the end of a precision's first run and replayed from its second) gives bitwise the
@@ -597,7 +597,9 @@ def test_graph_replay_is_bitwise_identical(gpu, monkeypatch, name):
     from aperi_mech_b200 import problems
     from aperi_mech_b200.model import ExplicitDynamics
 
-    p = _small_problem(name) if name != "cells" else problems.smoothed_tet4_box(n=4, seed=2, nsteps=80)
+    p = {"cells": lambda: problems.smoothed_tet4_box(n=4, seed=2, nsteps=80),
+         "rkpm": lambda: problems.rkpm_box(n=4, seed=2, nsteps=80),
+         "fbar": lambda: problems.rkpm_fbar_box(n=3, seed=2, nsteps=80)}.get(name, lambda: _small_problem(name))()
     mass = p.meta.get("mass")
     g = np.array([0.0, -3.0e2, 1.0e2])
     out = {}
