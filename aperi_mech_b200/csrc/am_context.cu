@@ -683,7 +683,8 @@ struct am_ctx {
     double2* rko_rec = nullptr;
     double2* rkto_rec = nullptr;
     double4* rk_u = nullptr;          // physical displacement Psi U
-    double4* rk_f_local = nullptr;    // element forces at the nodes
+    double4* rk_f_local = nullptr;
+    double4* rk_l = nullptr;  // the cotangent at the points (VJP with the two-pass coupling)    // element forces at the nodes
     double* rk_f = nullptr;           // N x 3: generalized force Psi^T f_local
     std::vector<cudaEvent_t> events;
     std::vector<std::pair<int, int64_t>> mark_slot;
@@ -735,6 +736,22 @@ struct am_ctx {
     // coupling (ExplicitSolver::ComputeForce, src/Solvers/Explicit.cpp:146-186) the blocks
     // see the physical displacement Psi U, their forces are gathered per node and scattered
     // to the generalized force Psi^T f, which the node kernels then read (f_given).
+    // The two-pass functions: Psi in (nodes) -> out (points); Psi^T in (points) -> out (nodes, N x 3).
+    void rk_rows(const double4* in, double4* out) {
+        if (rko_rec)
+            am::launch_rk_octets(points(), rko_count, rko_ptr, rko_rec, in, rk_ptr, N, out, nullptr, stream);
+        else
+            am::launch_rk_rows4(points(), N, rk_ptr, rk_nbr, rk_val, in, out, stream);
+        ++launches;
+    }
+    void rk_cols(const double4* in, double* out) {
+        if (rkto_rec)
+            am::launch_rk_octets(N, rkto_count, rkto_ptr, rkto_rec, in, nullptr, N, nullptr, out, stream);
+        else
+            am::launch_rk_cols3(N, rkt_ptr, rkt_src, rkt_val, in, out, stream);
+        ++launches;
+    }
+
     void element_forces(int mixed, const double4* U) {
         void* s = slots(mixed);
         if (lagr) {
@@ -752,11 +769,7 @@ struct am_ctx {
         }
         if (num_points > N && !rk_ptr) fail(AM_ESTATE, "cells on refinement points run after am_set_rk_functions");
         if (rk_ptr) {
-            if (rko_rec)
-                am::launch_rk_octets(points(), rko_count, rko_ptr, rko_rec, U, rk_ptr, N, rk_u, nullptr, stream);
-            else
-                am::launch_rk_rows4(points(), N, rk_ptr, rk_nbr, rk_val, U, rk_u, stream);
-            ++launches;
+            rk_rows(U, rk_u);
             U = rk_u;
         }
         for (auto& b : blocks) {
@@ -773,11 +786,8 @@ struct am_ctx {
             nd.f_given = nullptr;
             nd.num_nodes = points();  // the local force lives on the points
             am::launch_gather_force4(nd, mixed, s, rk_f_local, stream);
-            if (rkto_rec)
-                am::launch_rk_octets(N, rkto_count, rkto_ptr, rkto_rec, rk_f_local, nullptr, N, nullptr, rk_f, stream);
-            else
-                am::launch_rk_cols3(N, rkt_ptr, rkt_src, rkt_val, rk_f_local, rk_f, stream);
-            launches += 2;
+            ++launches;
+            rk_cols(rk_f_local, rk_f);
         }
         check_launch("element force kernel");
     }
@@ -923,7 +933,15 @@ struct am_ctx {
         return result;
     }
 
+    // With the two-pass coupling (f = Psi^T F(Psi u)) the VJP runs at (Psi u, Psi lam) and its
+    // point values are gathered and mapped back by Psi^T into rk_f, the node kernels' force.
     void vjp(const double4* U, const double4* L, double* gmu, double* gkappa, int accumulate) {
+        if (rk_ptr) {
+            rk_rows(U, rk_u);
+            rk_rows(L, rk_l);
+            U = rk_u;
+            L = rk_l;
+        }
         int64_t off = 0;
         for (const auto& b : blocks) {
             double* gm = gmu ? gmu + off : nullptr;
@@ -935,6 +953,14 @@ struct am_ctx {
                 ++launches;
             }
             off += b.num_elems;
+        }
+        if (rk_ptr) {
+            am::NodeDev nd = node_dev();
+            nd.f_given = nullptr;
+            nd.num_nodes = points();
+            am::launch_gather_force4(nd, 0, slots64, rk_f_local, stream);
+            ++launches;
+            rk_cols(rk_f_local, rk_f);
         }
         check_launch("vjp kernel");
     }
@@ -1233,6 +1259,7 @@ struct am_ctx {
         dfree(rkto_rec);
         dfree(rk_u);
         dfree(rk_f_local);
+        dfree(rk_l);
         dfree(rk_f);
         dfree(iface_nodes);
         dfree(iface_rows);
@@ -1988,7 +2015,6 @@ int am_vjp_force(am_ctx* ctx, am_memory where, const double* u, const double* la
     return guarded(ctx, [&] {
         ctx->require_finalized();
         if (ctx->iface_row_of) fail(AM_ESTATE, "the VJP is not available on a decomposed mesh");
-        if (ctx->rk_ptr) fail(AM_ESTATE, "the VJP is not available with the two-pass coupling");
         if (ctx->lagr) fail(AM_ESTATE, "the VJP is built for the total formulation");
         for (const auto& b : ctx->blocks)
             if (b.group_ptr) fail(AM_ESTATE, "the VJP is not available on F-bar cells");
@@ -2010,8 +2036,12 @@ int am_vjp_force(am_ctx* ctx, am_memory where, const double* u, const double* la
         }
         ctx->vjp(ctx->W4, ctx->L4, gm, gk, 0);
         double* out = where == AM_DEVICE ? gu : ctx->f_scratch;
-        am::launch_gather_force(ctx->node_dev(), 0, ctx->slots64, out, 0, ctx->stream);
-        ++ctx->launches;
+        if (ctx->rk_ptr) {
+            ck(cudaMemcpyAsync(out, ctx->rk_f, ctx->N * 3 * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+        } else {
+            am::launch_gather_force(ctx->node_dev(), 0, ctx->slots64, out, 0, ctx->stream);
+            ++ctx->launches;
+        }
         ck(cudaGetLastError(), "gather kernel");
         if (where == AM_HOST) {
             ck(cudaMemcpyAsync(gu, out, ctx->N * 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
@@ -2034,7 +2064,6 @@ int am_adjoint(am_ctx* ctx, int64_t nsteps, double dt, int32_t ckpt_every, int32
     return guarded(ctx, [&] {
         ctx->require_finalized();
         if (ctx->iface_row_of) fail(AM_ESTATE, "the adjoint is not available on a decomposed mesh");
-        if (ctx->rk_ptr) fail(AM_ESTATE, "the adjoint is not available with the two-pass coupling");
         if (ctx->lagr) fail(AM_ESTATE, "the adjoint is built for the total formulation");
         for (const auto& b : ctx->blocks)
             if (b.group_ptr) fail(AM_ESTATE, "the adjoint is not available on F-bar cells");
@@ -2504,6 +2533,7 @@ int am_set_rk_functions(am_ctx* ctx, const int64_t* nbr_ptr, const int32_t* nbr,
         up(ctx->rkt_val, tval.data(), T, "transposed values");
         ctx->rk_u = dalloc<double4>(NP, "physical displacement");
         ctx->rk_f_local = dalloc<double4>(NP, "local force");
+        ctx->rk_l = dalloc<double4>(NP, "cotangent at the points");
         ctx->rk_f = dalloc<double>(3 * N, "generalized force");
     });
 }

@@ -366,7 +366,9 @@ int am_set_formulation(am_ctx* ctx, int32_t formulation, int32_t update_interval
  * force through), summed in a fixed order instead of the reference's atomics. Needs the
  * generalized lumped mass (the element mass scattered through the functions, as
  * am_cells_get returns it) from am_set_mass before am_finalize; call once after
- * am_finalize. Not available with the VJP, the adjoint or a decomposed mesh (AM_ESTATE). */
+ * am_finalize. am_vjp_force and am_adjoint then apply Psi^T VJP(Psi u, Psi lam) (the VJP of
+ * the composed force; the modulus gradients are the blocks' at the physical fields). Not
+ * available on a decomposed mesh (AM_ESTATE). */
 int am_set_rk_functions(am_ctx* ctx, const int64_t* nbr_ptr, const int32_t* nbr, const double* values);
 /* Points for cells coupled through the functions (two-pass nodal cells): the cell entries
  * of this context then index num_points points, the first num_nodes being the nodes and

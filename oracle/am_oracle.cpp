@@ -882,6 +882,45 @@ void ob_stress(int material, double lambda, double mu, int64_t n, const double* 
     for (int64_t k = 0; k < n; ++k) stress(material, lambda, mu, H + 9 * k, P + 9 * k);
 }
 
+// The two-pass functions applied to a nodal field x (N x 3) at the P points
+// (FunctionEvaluationProcessor::ComputeValues, include/FunctionEvaluationProcessor.h:86-121):
+// a row without neighbours copies its coefficient, others sum psi * coefficient over the
+// neighbours in reverse order. With more points than nodes (two-pass nodal cells) a point
+// without neighbours past the nodes has no coefficient to copy: it stays at zero.
+static void rk_apply_rows(const ob_problem* p, const double* x, double* out) {
+    const int64_t N = p->num_nodes, P = p->rk_rows > 0 ? p->rk_rows : N;
+    for (int64_t i = 0; i < P; ++i) {
+        const int64_t b = p->rk_ptr[i], e = p->rk_ptr[i + 1];
+        for (int c = 0; c < 3; ++c) {
+            if (b == e) {
+                out[i * 3 + c] = i < N ? x[i * 3 + c] : 0.0;
+                continue;
+            }
+            double s = 0.0;
+            for (int64_t k = e; k-- > b;) s += x[p->rk_nbr[k] * 3 + c] * p->rk_values[k];
+            out[i * 3 + c] = s;
+        }
+    }
+}
+
+// Point values scattered to the coefficients (ScatterValues, :130-174): psi_j(x_i) v_i added
+// to node j of f; a row without neighbours passes its value through (a point past the nodes
+// drops it). The reference adds with atomics in no fixed order; here the sum for each node
+// runs over i ascending.
+static void rk_scatter(const ob_problem* p, const double* v, double* f) {
+    const int64_t N = p->num_nodes, P = p->rk_rows > 0 ? p->rk_rows : N;
+    for (int64_t i = 0; i < P; ++i) {
+        const int64_t b = p->rk_ptr[i], e = p->rk_ptr[i + 1];
+        if (b == e) {
+            if (i < N)
+                for (int c = 0; c < 3; ++c) f[i * 3 + c] += v[i * 3 + c];
+            continue;
+        }
+        for (int64_t k = b; k < e; ++k)
+            for (int c = 0; c < 3; ++c) f[p->rk_nbr[k] * 3 + c] += p->rk_values[k] * v[i * 3 + c];
+    }
+}
+
 // Internal force over all parts, overwriting f (the solver zeroes the force field
 // before the contributions accumulate, src/Solvers/Explicit.cpp:157-163).
 void ob_internal_force(const ob_problem* p, const double* u, double* f) {
@@ -891,40 +930,13 @@ void ob_internal_force(const ob_problem* p, const double* u, double* f) {
         for (int k = 0; k < p->num_blocks; ++k) add_block_forces(p, p->blocks[k], u, f);
         return;
     }
-    // Two-pass method (ExplicitSolver::ComputeForce, src/Solvers/Explicit.cpp:146-186).
-    // Physical displacement from the coefficients (FunctionEvaluationProcessor::ComputeValues,
-    // include/FunctionEvaluationProcessor.h:86-121): a row without neighbours copies its
-    // coefficient, others sum psi * coefficient over the neighbours in reverse order.
-    // With more points than nodes (two-pass nodal cells) a point without neighbours past
-    // the nodes has no coefficient to copy: it stays at zero and its force is dropped.
+    // Two-pass method (ExplicitSolver::ComputeForce, src/Solvers/Explicit.cpp:146-186): the
+    // blocks on the physical displacement at the points, their forces scattered back.
     const int64_t P = p->rk_rows > 0 ? p->rk_rows : N;
     std::vector<double> up(P * 3), fl(P * 3, 0.0);
-    for (int64_t i = 0; i < P; ++i) {
-        const int64_t b = p->rk_ptr[i], e = p->rk_ptr[i + 1];
-        for (int c = 0; c < 3; ++c) {
-            if (b == e) {
-                up[i * 3 + c] = i < N ? u[i * 3 + c] : 0.0;
-                continue;
-            }
-            double s = 0.0;
-            for (int64_t k = e; k-- > b;) s += u[p->rk_nbr[k] * 3 + c] * p->rk_values[k];
-            up[i * 3 + c] = s;
-        }
-    }
+    rk_apply_rows(p, u, up.data());
     for (int k = 0; k < p->num_blocks; ++k) add_block_forces(p, p->blocks[k], up.data(), fl.data());
-    // Local forces scattered to the coefficients (ScatterValues, :130-174): psi_j(x_i) f_i
-    // added to node j; a row without neighbours passes its force through. The reference
-    // adds with atomics in no fixed order; here the sum for each node runs over i ascending.
-    for (int64_t i = 0; i < P; ++i) {
-        const int64_t b = p->rk_ptr[i], e = p->rk_ptr[i + 1];
-        if (b == e) {
-            if (i < N)
-                for (int c = 0; c < 3; ++c) f[i * 3 + c] += fl[i * 3 + c];
-            continue;
-        }
-        for (int64_t k = b; k < e; ++k)
-            for (int c = 0; c < 3; ++c) f[p->rk_nbr[k] * 3 + c] += p->rk_values[k] * fl[i * 3 + c];
-    }
+    rk_scatter(p, fl.data(), f);
 }
 
 // ComputeElementVolumeFunctor.h:20-79: V_e = sum_gp w_gp.
@@ -1120,13 +1132,31 @@ int ob_explicit_solve(const ob_problem* p, double dt, double t_end, int64_t max_
     return 0;
 }
 
+// With the two-pass coupling the force is f = Psi^T F(Psi u): its VJP with cotangent lam is
+// Psi^T VJP_F(Psi u, Psi lam), and the modulus gradients are F's at (Psi u, Psi lam).
 void ob_vjp_force(const ob_problem* p, const double* u, const double* lam, double* gu, double* gmu, double* gkappa) {
     std::fill(gu, gu + p->num_nodes * 3, 0.0);
+    const double* uu = u;
+    const double* ll = lam;
+    double* g = gu;
+    std::vector<double> up, lp, gl;
+    if (p->rk_ptr) {
+        const int64_t P = p->rk_rows > 0 ? p->rk_rows : p->num_nodes;
+        up.resize(P * 3);
+        lp.resize(P * 3);
+        gl.assign(P * 3, 0.0);
+        rk_apply_rows(p, u, up.data());
+        rk_apply_rows(p, lam, lp.data());
+        uu = up.data();
+        ll = lp.data();
+        g = gl.data();
+    }
     int64_t off = 0;
     for (int k = 0; k < p->num_blocks; ++k) {
-        add_block_vjp(p, p->blocks[k], u, lam, gu, gmu ? gmu + off : nullptr, gkappa ? gkappa + off : nullptr);
+        add_block_vjp(p, p->blocks[k], uu, ll, g, gmu ? gmu + off : nullptr, gkappa ? gkappa + off : nullptr);
         off += p->blocks[k].num_elems;
     }
+    if (p->rk_ptr) rk_scatter(p, gl.data(), gu);
 }
 
 // Discrete adjoint of the central-difference trajectory (new capability): the

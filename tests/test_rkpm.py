@@ -263,6 +263,29 @@ def test_oracle_two_pass_is_psi_transpose_fem_psi(oracle_lib):
     assert abs(mass.sum() - 2000.0) < 1e-9
 
 
+def test_oracle_two_pass_vjp_is_psi_transpose_fem_vjp(oracle_lib):
+    """The VJP of the composed force f = Psi^T F(Psi d): Psi^T VJP_F(Psi d, Psi lam), with the
+    modulus gradients of F at (Psi d, Psi lam); and lam . f against central differences."""
+    from aperi_mech_b200.model import Material
+
+    X, T = _box(n=3, seed=7)
+    mat = Material.create("neo_hookean", 1000.0, shear_modulus=3.85e8, bulk_modulus=8.33e8)
+    part, mass, rk = _two_pass_inputs(oracle_lib, X, T, mat)
+    Psi = _dense(rk, X.shape[0])
+    rng = np.random.default_rng(5)
+    d = 1e-3 * rng.standard_normal(X.shape)
+    lam = rng.standard_normal(X.shape)
+    op = oracle_lib.OracleProblem(X, [part], mass=mass, rk=rk)
+    gu, gm, gk = op.vjp_force(d, lam)
+    fu, fm, fk = oracle_lib.OracleProblem(X, [part]).vjp_force(Psi @ d, Psi @ lam)
+    assert rel_err(gu, Psi.T @ fu) < 1e-13
+    assert rel_err(gm, fm) < 1e-13 and rel_err(gk, fk) < 1e-13
+    dirn = rng.standard_normal(X.shape)
+    h = 1e-6
+    fd = (np.sum(lam * op.internal_force(d + h * dirn)) - np.sum(lam * op.internal_force(d - h * dirn))) / (2 * h)
+    assert abs(np.sum(gu * dirn) - fd) < 1e-5 * abs(fd)
+
+
 SHEAR = [(1, 0), (2, 0), (0, 1), (2, 1), (0, 2), (1, 2)]
 
 
@@ -302,6 +325,31 @@ def test_oracle_two_pass_shear_patch(oracle_lib, direction, surface):
     dd[direction] = mag
     assert np.abs(u[s_hi] - dd).max() < 1e-9 and np.abs(u[s_lo] + dd).max() < 1e-9
     assert np.abs(vp[s_hi] - 1.875 * dd / 10.0).max() < 1e-4
+
+
+@pytest.mark.gpu
+def test_rkpm_two_pass_vjp_and_adjoint_match_oracle(gpu, oracle_lib):
+    """The library's VJP and checkpointed adjoint with the two-pass coupling against the
+    oracle's (its reverse pass stores every state): u-VJP at 1e-11, loss at 1e-12, modulus
+    gradients at 1e-10."""
+    from aperi_mech_b200 import problems
+    from aperi_mech_b200.model import ExplicitDynamics
+
+    p = problems.rkpm_two_pass_box(n=4, seed=2, nsteps=20)
+    mass, rk = p.meta["mass"], p.meta["rk"]
+    op = oracle_lib.OracleProblem(p.coords, p.parts, p.bcs, mass=mass, rk=rk)
+    rng = np.random.default_rng(8)
+    u = 1e-3 * rng.standard_normal(p.coords.shape)
+    lam = rng.standard_normal(p.coords.shape)
+    sens = np.arange(0, p.coords.shape[0], 7, dtype=np.int32)[:16]
+    with ExplicitDynamics(p.coords, p.parts, p.bcs, mass=mass, rk=rk) as m:
+        for g, w in zip(m.vjp_force(u, lam), op.vjp_force(u, lam)):
+            assert rel_err(g, w) < 1e-11
+        m.set_state(None, p.v0)
+        loss, gm, gk = m.adjoint(p.nsteps, p.dt, 5, sens)
+    wl, wm, wk = op.adjoint(p.nsteps, p.dt, np.zeros_like(p.coords), p.v0, sens)
+    assert abs(loss - wl) < 1e-12 * abs(wl)
+    assert rel_err(gm, wm) < 1e-10 and rel_err(gk, wk) < 1e-10
 
 
 @pytest.mark.gpu
