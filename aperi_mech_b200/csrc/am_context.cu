@@ -240,6 +240,7 @@ struct Block {
     double4* nrec64 = nullptr;
     float* cmat32 = nullptr;
     double* cmat64 = nullptr;
+    double* vjp_lmat = nullptr;  // F-bar VJP: L_s per subcell (component arrays), allocated on first use
     std::vector<int32_t> host_cell_ptr;  // until am_finalize: the CSR and gradients the records
     std::vector<double> host_grads;      // are built from, and the F-bar groups
     std::vector<int64_t> host_group_ptr;
@@ -384,6 +385,7 @@ struct Block {
         dfree(nrec64);
         dfree(cmat32);
         dfree(cmat64);
+        dfree(vjp_lmat);
     }
 
     // The cell-stress form's records (see above), built at am_finalize once the block is
@@ -947,7 +949,7 @@ struct am_ctx {
             double* gm = gmu ? gmu + off : nullptr;
             double* gk = gkappa ? gkappa + off : nullptr;
             if (b.kind == AM_SMOOTHED_CELLS) {
-                launches += am::launch_cell_vjp(b.cells(), U, L, slots64, gm, gk, accumulate, stream);
+                launches += am::launch_cell_vjp(b.cells(), U, L, b.vjp_lmat, slots64, gm, gk, accumulate, stream);
             } else {
                 am::launch_gauss_vjp(b.gauss(), X4, U, L, slots64, gm, gk, accumulate, stream);
                 ++launches;
@@ -963,6 +965,16 @@ struct am_ctx {
             rk_cols(rk_f_local, rk_f);
         }
         check_launch("vjp kernel");
+    }
+
+    // The VJP's refusals and scratch: F-bar cells only in the cell-stress form (cells of at
+    // most 32 subcells), which keeps L_s per subcell beside H_s.
+    void prepare_vjp(const char* what) {
+        for (auto& b : blocks) {
+            if (!b.group_ptr) continue;
+            if (!b.gather) fail(AM_ESTATE, std::string(what) + " on F-bar cells needs the cell-stress form (cells of at most 32 subcells)");
+            if (!b.vjp_lmat) b.vjp_lmat = dalloc<double>(std::max<int64_t>(9 * b.num_elems, 1), "F-bar VJP scratch");
+        }
     }
 
     // Per-element arrays over all blocks (block after block), from the processing order
@@ -2016,8 +2028,7 @@ int am_vjp_force(am_ctx* ctx, am_memory where, const double* u, const double* la
         ctx->require_finalized();
         if (ctx->iface_row_of) fail(AM_ESTATE, "the VJP is not available on a decomposed mesh");
         if (ctx->lagr) fail(AM_ESTATE, "the VJP is built for the total formulation");
-        for (const auto& b : ctx->blocks)
-            if (b.group_ptr) fail(AM_ESTATE, "the VJP is not available on F-bar cells");
+        ctx->prepare_vjp("the VJP");
         if (!u || !lam || !gu) fail(AM_EINVAL, "null u, lam or gu");
         load_nodal(ctx, where, u, ctx->W4);
         load_nodal(ctx, where, lam, ctx->L4);
@@ -2065,8 +2076,7 @@ int am_adjoint(am_ctx* ctx, int64_t nsteps, double dt, int32_t ckpt_every, int32
         ctx->require_finalized();
         if (ctx->iface_row_of) fail(AM_ESTATE, "the adjoint is not available on a decomposed mesh");
         if (ctx->lagr) fail(AM_ESTATE, "the adjoint is built for the total formulation");
-        for (const auto& b : ctx->blocks)
-            if (b.group_ptr) fail(AM_ESTATE, "the adjoint is not available on F-bar cells");
+        ctx->prepare_vjp("the adjoint");
         if (nsteps <= 0 || !(dt > 0.0)) fail(AM_EINVAL, "nsteps and dt must be positive");
         if (ckpt_every <= 0) fail(AM_EINVAL, "ckpt_every must be positive");
         if (num_sensors < 0 || (num_sensors > 0 && !sensors)) fail(AM_EINVAL, "bad sensor list");

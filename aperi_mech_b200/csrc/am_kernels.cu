@@ -2004,6 +2004,108 @@ __global__ void __launch_bounds__(256) k_cell_vjp(CellBlockDev b, const double4*
     if (lane == 0) store_theta(gmu, gk, c, -V * (ldm - 2.0 / 3.0 * ldl), -V * ldl, accumulate);
 }
 
+// VJP of F-bar cells in the cell-stress form (a warp per cell of at most 32 subcells, a lane
+// per subcell; FP64). The F-bar force is f = -dW/du of W = sum_s V_s psi(Fbar_s), so its VJP
+// with lam is the derivative along L_s = sum_k lam_k (x) b_k (W's Hessian is symmetric):
+//   dJ_s = cof(F_s) : L_s, dJbar = sum V_s dJ_s / V, djs = js / 3 (dJbar / Jbar - dJ_s / J_s),
+//   dFbar = djs F + js L, dPbar = dP/dF(Hbar)[dFbar], pf = Pbar : F, dpf = dPbar : F + Pbar : L,
+//   dP = djs Pbar + js dPbar + dscal cof(F) + scal dcof(F)[L]
+// with scal = p - js pf / (3 J) and its derivative dscal. H_s (in M) and L_s (in Lm) come
+// from the octet kernel; M = -V_s dP_s replaces H_s for the node-major gather. The moduli of
+// subcell s enter lam^T f = -sum_s V_s Pbar_s : dFbar_s only through Pbar_s.
+template <int MAT>
+__global__ void __launch_bounds__(256) k_fbar_cell_vjp(CellBlockDev b, double* __restrict__ M,
+                                                        const double* __restrict__ Lm, double* gmu, double* gk,
+                                                        int accumulate) {
+    pdl_trigger();
+    const int lane = static_cast<int>(threadIdx.x & 31);
+    const int64_t g = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const bool gvalid = g < b.num_groups;
+    const int64_t s0 = gvalid ? b.group_ptr[g] : 0;
+    const int ns = gvalid ? static_cast<int>(b.group_ptr[g + 1] - s0) : 0;
+    if (ns == 0) return;  // the whole warp
+    const bool own = lane < ns;
+    const int64_t s = s0 + lane;
+    const double V = own ? b.volumes[s] : 0.0;
+    double lam = 0.0, mu = 0.0;
+    if (own) element_lame(b, s, lam, mu);
+    pdl_wait();
+    double H[9], L[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) H[q] = L[q] = 0.0;
+    if (own) {
+        load_cell_matrix(M, b.num_cells, static_cast<int32_t>(s), H);
+        load_cell_matrix(Lm, b.num_cells, static_cast<int32_t>(s), L);
+    }
+    double F[9], A[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) F[q] = H[q];
+    F[0] += 1.0;
+    F[4] += 1.0;
+    F[8] += 1.0;
+    adj3(F, A);  // cof(F)_ij = A_ji
+    const double J = det_ap_im1(H) + 1.0;
+    double dJ = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) dJ += A[j * 3 + i] * L[i * 3 + j];
+    double jv = own ? J * V : 0.0, vol = V, djv = own ? dJ * V : 0.0, unused = 0.0;
+    warp_sum2(jv, vol);
+    warp_sum2(djv, unused);
+    const double Jbar = jv / vol, dJbar = djv / vol;
+    const double ratio = Jbar / J;
+    const double js = cbrt(ratio);
+    const double djs = js / 3.0 * (dJbar / Jbar - dJ / J);
+    double Hb[9], dFb[9];
+    if (fabs(ratio - 1.0) < 3.0 * 2.2204460492503131e-16) {
+#pragma unroll
+        for (int q = 0; q < 9; ++q) Hb[q] = H[q];
+    } else {
+#pragma unroll
+        for (int q = 0; q < 9; ++q) Hb[q] = H[q] * js;
+        Hb[0] += js - 1.0;
+        Hb[4] += js - 1.0;
+        Hb[8] += js - 1.0;
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) dFb[q] = djs * F[q] + js * L[q];
+    double Pb[9], dPb[9], ldl = 0.0, ldm = 0.0;
+    stress<double>(MAT, lam, mu, Hb, Pb);
+    stress_vjp(MAT, lam, mu, Hb, dFb, dPb, &ldl, &ldm);
+    double pf = 0.0, dpf = 0.0;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        pf += Pb[q] * F[q];
+        dpf += dPb[q] * F[q] + Pb[q] * L[q];
+    }
+    double pd = own ? V * js * pf / (3.0 * Jbar) : 0.0;
+    double dpd = own ? V * (djs * pf + js * dpf - js * pf * dJbar / Jbar) / (3.0 * Jbar) : 0.0;
+    warp_sum2(pd, dpd);
+    if (!own) return;
+    pd /= vol;
+    dpd /= vol;
+    const double scal = pd - js * pf / (3.0 * J);
+    const double dscal = dpd - (djs * pf + js * dpf) / (3.0 * J) + js * pf * dJ / (3.0 * J * J);
+    double m[9];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        // row r of cof(F) is F_a x F_c (rows a = r + 1, c = r + 2): its derivative along L
+        const int a = (r + 1) % 3, c = (r + 2) % 3;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const int i1 = (i + 1) % 3, i2 = (i + 2) % 3;
+            const double dG = L[a * 3 + i1] * F[c * 3 + i2] - L[a * 3 + i2] * F[c * 3 + i1] + F[a * 3 + i1] * L[c * 3 + i2] -
+                              F[a * 3 + i2] * L[c * 3 + i1];
+            const int q = r * 3 + i;
+            m[q] = -V * (djs * Pb[q] + js * dPb[q] + dscal * A[i * 3 + r] + scal * dG);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) store_cell_matrix<double>(M, b.num_cells, s, k, m);
+    store_theta(gmu, gk, s, -V * (ldm - 2.0 / 3.0 * ldl), -V * ldl, accumulate);
+}
+
 // VJP of the split-hex-grouped cells (FP64, one thread per patch): the cell VJP above
 // for the patch's six cells, summed per patch node.
 template <int MAT>
@@ -3076,16 +3178,48 @@ void launch_gauss_vjp(const GaussBlockDev& b, const double4* X4, const double4* 
     }
 }
 
-int launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double4* slots, double* gmu,
-                    double* gkappa, int accumulate, cudaStream_t s) {
+// F-bar cells in the cell-stress form: H_s on u into M, L_s on lam into Lm (the octet
+// kernel of the force, FP64), the per-cell VJP writing M = -V_s dP_s, then the gather.
+template <int UNR, int G>
+void launch_fbar_vjp_g(const CellBlockDev& b, const double4* U4, const double4* L4, double* Lm, double* gmu,
+                       double* gkappa, int accumulate, cudaStream_t s) {
+    const unsigned grid = grid_for(b.num_octets * 32, 256);
+    double* Hm = static_cast<double*>(b.cmat);
+    // the H-only instance returns before any status flag
+    launch_pdl(k_cell_stress<double, kLinearElastic, UNR, true, G>, grid, 256, s, b, U4, Hm, static_cast<int*>(nullptr));
+    launch_pdl(k_cell_stress<double, kLinearElastic, UNR, true, G>, grid, 256, s, b, L4, Lm, static_cast<int*>(nullptr));
+    AM_DISPATCH_MAT(b.material, (launch_pdl(k_fbar_cell_vjp<M>, grid_for(b.num_groups * 32, 256), 256, s, b, Hm,
+                                            static_cast<const double*>(Lm), gmu, gkappa, accumulate)));
+}
+template <int UNR>
+void launch_fbar_vjp_unr(const CellBlockDev& b, const double4* U4, const double4* L4, double* Lm, double* gmu,
+                         double* gkappa, int accumulate, cudaStream_t s) {
+    if (b.group_items[0] == 1)
+        launch_fbar_vjp_g<UNR, 1>(b, U4, L4, Lm, gmu, gkappa, accumulate, s);
+    else
+        launch_fbar_vjp_g<UNR, 8>(b, U4, L4, Lm, gmu, gkappa, accumulate, s);
+}
+
+int launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double* Lm, double4* slots,
+                    double* gmu, double* gkappa, int accumulate, cudaStream_t s) {
     if (b.num_cells == 0) return 0;
-    if (b.patched == 2) {
+    int count = 2;
+    if (b.group_ptr != nullptr) {
+        if (b.unroll[0] == 1)
+            launch_fbar_vjp_unr<1>(b, U4, L4, Lm, gmu, gkappa, accumulate, s);
+        else if (b.unroll[0] == 2)
+            launch_fbar_vjp_unr<2>(b, U4, L4, Lm, gmu, gkappa, accumulate, s);
+        else
+            launch_fbar_vjp_unr<4>(b, U4, L4, Lm, gmu, gkappa, accumulate, s);
+        count = 4;
+    } else if (b.patched == 2) {
         AM_DISPATCH_MAT(b.material, (k_cell_hex6_vjp<M><<<grid_for(b.num_patches, 64), 64, 0, s>>>(b, U4, L4, slots, gmu, gkappa, accumulate)));
         return 1;
+    } else {
+        const unsigned grid = grid_for(b.num_cells * 32, 256);
+        AM_DISPATCH_MAT(b.material, (k_cell_vjp<M><<<grid, 256, 0, s>>>(b, U4, L4, slots, gmu, gkappa, accumulate)));
+        if (!b.gather) return 1;
     }
-    const unsigned grid = grid_for(b.num_cells * 32, 256);
-    AM_DISPATCH_MAT(b.material, (k_cell_vjp<M><<<grid, 256, 0, s>>>(b, U4, L4, slots, gmu, gkappa, accumulate)));
-    if (!b.gather) return 1;
     if (b.unroll[1] == 1) {
         launch_cell_gather_unr<double, 1>(b, slots, s);
     } else if (b.unroll[1] == 2) {
@@ -3093,7 +3227,7 @@ int launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4,
     } else {
         launch_cell_gather_unr<double, 4>(b, slots, s);
     }
-    return 2;
+    return count;
 }
 
 void launch_tet4_geometry(const int32_t* conn, int64_t num_elems, const double4* X4, float* geo32, double* geo64,

@@ -158,8 +158,9 @@ void launch_tet4_geometry(const int32_t* conn, int64_t num_elems, const double4*
                           cudaStream_t s);
 void launch_gauss_vjp(const GaussBlockDev& b, const double4* X4, const double4* U4, const double4* L4, double4* slots,
                       double* gmu, double* gkappa, int accumulate, cudaStream_t s);
-int launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double4* slots, double* gmu,
-                     double* gkappa, int accumulate, cudaStream_t s);
+// Lm: scratch of 9 doubles per cell for F-bar blocks (null otherwise). Returns the launch count.
+int launch_cell_vjp(const CellBlockDev& b, const double4* U4, const double4* L4, double* Lm, double4* slots,
+                    double* gmu, double* gkappa, int accumulate, cudaStream_t s);
 void launch_hex6_patch_dx(const int32_t* patch_nodes, int64_t num_patches, const double4* X4, float* dx32,
                           double* dx64, cudaStream_t stream);
 void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const double4* X4, double4* slots,

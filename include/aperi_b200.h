@@ -113,8 +113,10 @@ int am_set_block_fields(am_ctx* ctx, int32_t block_id, const double* mu_field, c
  * subcell, Jbar = sum J_s V_s / V_cell per cell, the subcells' stresses at
  * Fbar = (Jbar / J_s)^(1/3) F, the cell's dual pressure, the un-barred stresses, and the
  * subcell forces -V_s b P^T. As in the reference, when num_cells equals the subcell
- * count the call changes nothing. Before am_finalize; not available with the VJP or
- * the adjoint (AM_ESTATE). */
+ * count the call changes nothing. Before am_finalize. am_vjp_force and am_adjoint take
+ * F-bar blocks in the cell-stress form (every cell of at most 32 subcells, the default
+ * layout; AM_ESTATE otherwise): the VJP is the F-bar force's derivative along lam, the
+ * force being the gradient of sum_s V_s psi(Fbar_s). */
 int am_set_cell_groups(am_ctx* ctx, int32_t block_id, int64_t num_cells, const int64_t* group_ptr);
 int am_set_body_acceleration(am_ctx* ctx, const double g[3]);
 int am_set_mass(am_ctx* ctx, const double* mass);

@@ -67,6 +67,17 @@ inline double det_ap_im1(const double* A) {
            a12 * a21 * (1 + a00) + a00 * a22 + a11 * a22 + a01 * a12 * a20 + a02 * a10 * a21;
 }
 
+// Cofactor matrix det(F) F^-T: rows r1 x r2, r2 x r0, r0 x r1 of F's rows r0, r1, r2.
+inline void cof3(const double* F, double* C) {
+    for (int r = 0; r < 3; ++r) {
+        const int a = (r + 1) % 3, c = (r + 2) % 3;
+        for (int i = 0; i < 3; ++i) {
+            const int i1 = (i + 1) % 3, i2 = (i + 2) % 3;
+            C[r * 3 + i] = F[a * 3 + i1] * F[c * 3 + i2] - F[a * 3 + i2] * F[c * 3 + i1];
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Shape functions and Gauss quadrature
 // ---------------------------------------------------------------------------
@@ -463,6 +474,132 @@ void fbar_cell_forces(const ob_block& b, int64_t g, const double* u, double* slo
     }
 }
 
+// VJP of the F-bar cell forces of one cell g (the adjoint extension; the reference has
+// none). The forces above are f = -dW/du of W = sum_s V_s psi(Fbar_s), with
+// Fbar_s = js F_s, js = cbrt(Jbar / J_s): P_s above is dW/dF_s / V_s. The Hessian of W
+// is symmetric, so lam^T df/du is the derivative of f along L_s = sum_k lam_k (x) b_k:
+//   dJ_s = cof(F_s) : L_s, dJbar = sum_s V_s dJ_s / V_g,
+//   djs = js / 3 (dJbar / Jbar - dJ_s / J_s), dFbar = djs F + js L,
+//   dPbar = dP/dF(Hbar)[dFbar], pf = Pbar : F, dpf = dPbar : F + Pbar : L,
+//   dp = sum_s V_s (djs pf + js dpf - js pf dJbar / Jbar) / (3 Jbar) / V_g,
+//   dscal = dp - (djs pf + js dpf) / (3 J) + js pf dJ / (3 J^2),
+//   dP = djs Pbar + js dPbar + dscal cof(F) + scal dcof(F)[L]
+// and slots get -V_s b_k dP^T. lam^T f = -dW[L] = -sum_s V_s Pbar_s : dFbar_s, so the
+// moduli of subcell s enter only through Pbar_s: d(lam^T f)/dtheta_s = -V_s dPbar/dtheta : dFbar.
+void fbar_cell_vjp(const ob_block& b, int64_t g, const double* u, const double* lam, double* slots, double* gmu,
+                   double* gkappa) {
+    const int64_t s0 = b.group_ptr[g], s1 = b.group_ptr[g + 1];
+    if (s1 <= s0) return;
+    const int64_t n = s1 - s0;
+    std::vector<double> H(9 * n), L(9 * n), J(n), dJ(n), G(9 * n);
+    double Vg = 0.0, jv = 0.0, djv = 0.0;
+    for (int64_t s = s0; s < s1; ++s) {
+        const int64_t q = s - s0;
+        double* h = &H[9 * q];
+        double* l = &L[9 * q];
+        std::fill(h, h + 9, 0.0);
+        std::fill(l, l + 9, 0.0);
+        for (int64_t e = b.cell_ptr[s]; e < b.cell_ptr[s + 1]; ++e) {
+            const int32_t nd = b.cell_nodes[e];
+            const double* gr = b.cell_grads + 3 * e;
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    h[i * 3 + j] += u[nd * 3 + i] * gr[j];
+                    l[i * 3 + j] += lam[nd * 3 + i] * gr[j];
+                }
+        }
+        double F[9];
+        std::copy(h, h + 9, F);
+        F[0] += 1.0;
+        F[4] += 1.0;
+        F[8] += 1.0;
+        cof3(F, &G[9 * q]);
+        J[q] = det_ap_im1(h) + 1.0;
+        dJ[q] = 0.0;
+        for (int k = 0; k < 9; ++k) dJ[q] += G[9 * q + k] * l[k];
+        jv += J[q] * b.cell_volumes[s];
+        djv += dJ[q] * b.cell_volumes[s];
+        Vg += b.cell_volumes[s];
+    }
+    const double Jbar = jv / Vg, dJbar = djv / Vg;
+    std::vector<double> js(n), djs(n), Pb(9 * n), dPb(9 * n), pf(n), dpf(n);
+    double p = 0.0, dp = 0.0;
+    for (int64_t s = s0; s < s1; ++s) {
+        const int64_t q = s - s0;
+        const double* h = &H[9 * q];
+        const double* l = &L[9 * q];
+        const double ratio = Jbar / J[q];
+        js[q] = std::cbrt(ratio);
+        djs[q] = js[q] / 3.0 * (dJbar / Jbar - dJ[q] / J[q]);
+        double hb[9];
+        if (std::abs(ratio - 1.0) < 3.0 * 2.2204460492503131e-16) {
+            std::copy(h, h + 9, hb);
+        } else {
+            for (int k = 0; k < 9; ++k) hb[k] = h[k] * js[q];
+            for (int i = 0; i < 3; ++i) hb[i * 4] += js[q] - 1.0;
+        }
+        double F[9], dFb[9];
+        std::copy(h, h + 9, F);
+        F[0] += 1.0;
+        F[4] += 1.0;
+        F[8] += 1.0;
+        for (int k = 0; k < 9; ++k) dFb[k] = djs[q] * F[k] + js[q] * l[k];
+        double lambda, mu;
+        block_lame(b, s, &lambda, &mu);
+        double dPl[9], dPm[9];
+        stress(b.material, lambda, mu, hb, &Pb[9 * q]);
+        stress_tangent(b.material, lambda, mu, hb, dFb, &dPb[9 * q], dPl, dPm);
+        double sl = 0.0, sm = 0.0;
+        pf[q] = dpf[q] = 0.0;
+        for (int k = 0; k < 9; ++k) {
+            sl += dFb[k] * dPl[k];
+            sm += dFb[k] * dPm[k];
+            pf[q] += Pb[9 * q + k] * F[k];
+            dpf[q] += dPb[9 * q + k] * F[k] + Pb[9 * q + k] * l[k];
+        }
+        const double V = b.cell_volumes[s];
+        // lambda = kappa - 2/3 mu, as in add_block_vjp
+        if (gmu) gmu[s] = -V * (sm - 2.0 / 3.0 * sl);
+        if (gkappa) gkappa[s] = -V * sl;
+        p += V * js[q] * pf[q] / (3.0 * Jbar);
+        dp += V * (djs[q] * pf[q] + js[q] * dpf[q] - js[q] * pf[q] * dJbar / Jbar) / (3.0 * Jbar);
+    }
+    p /= Vg;
+    dp /= Vg;
+    for (int64_t s = s0; s < s1; ++s) {
+        const int64_t q = s - s0;
+        const double* h = &H[9 * q];
+        const double* l = &L[9 * q];
+        double F[9];
+        std::copy(h, h + 9, F);
+        F[0] += 1.0;
+        F[4] += 1.0;
+        F[8] += 1.0;
+        const double scal = p - js[q] * pf[q] / (3.0 * J[q]);
+        const double dscal = dp - (djs[q] * pf[q] + js[q] * dpf[q]) / (3.0 * J[q]) +
+                             js[q] * pf[q] * dJ[q] / (3.0 * J[q] * J[q]);
+        // cof(F) rows are r1 x r2, r2 x r0, r0 x r1 of F's rows: its derivative along L
+        double dG[9];
+        for (int r = 0; r < 3; ++r) {
+            const int a = (r + 1) % 3, c = (r + 2) % 3;
+            for (int i = 0; i < 3; ++i) {
+                const int i1 = (i + 1) % 3, i2 = (i + 2) % 3;
+                dG[r * 3 + i] = l[a * 3 + i1] * F[c * 3 + i2] - l[a * 3 + i2] * F[c * 3 + i1] +
+                                F[a * 3 + i1] * l[c * 3 + i2] - F[a * 3 + i2] * l[c * 3 + i1];
+            }
+        }
+        double dP[9];
+        for (int k = 0; k < 9; ++k)
+            dP[k] = djs[q] * Pb[9 * q + k] + js[q] * dPb[9 * q + k] + dscal * G[9 * q + k] + scal * dG[k];
+        const double V = b.cell_volumes[s];
+        for (int64_t e = b.cell_ptr[s]; e < b.cell_ptr[s + 1]; ++e) {
+            const double* gr = b.cell_grads + 3 * e;
+            for (int i = 0; i < 3; ++i)
+                slots[e * 3 + i] = (gr[0] * dP[i * 3 + 0] + gr[1] * dP[i * 3 + 1] + gr[2] * dP[i * 3 + 2]) * -V;
+        }
+    }
+}
+
 void add_block_forces(const ob_problem* p, const ob_block& b, const double* u, double* f) {
     if (b.kind == OB_CELLS) {
         const int64_t K = b.cell_ptr[b.num_elems];
@@ -630,6 +767,15 @@ std::vector<double> mass_of(const ob_problem* p) {
 void add_block_vjp(const ob_problem* p, const ob_block& b, const double* u, const double* lam, double* gu,
                    double* gmu, double* gkappa) {
     const bool cells = b.kind == OB_CELLS;
+    if (cells && b.group_ptr) {
+        std::vector<double> slots(static_cast<size_t>(b.cell_ptr[b.num_elems]) * 3, 0.0);
+#pragma omp parallel for schedule(dynamic, 64)
+        for (int64_t g = 0; g < b.num_groups; ++g) fbar_cell_vjp(b, g, u, lam, slots.data(), gmu, gkappa);
+        for (int64_t s = 0; s < b.num_elems; ++s)
+            for (int64_t e = b.cell_ptr[s]; e < b.cell_ptr[s + 1]; ++e)
+                for (int i = 0; i < 3; ++i) gu[b.cell_nodes[e] * 3 + i] += slots[e * 3 + i];
+        return;
+    }
     const int nn = cells ? 0 : nodes_per_elem(b.kind);
     std::vector<int64_t> start(b.num_elems + 1);
     for (int64_t e = 0; e <= b.num_elems; ++e) start[e] = cells ? b.cell_ptr[e] : e * nn;

@@ -145,6 +145,67 @@ def test_oracle_fbar_force_is_the_energy_gradient(oracle_lib, kind):
         assert abs(fd + np.sum(f * d)) < 1e-6 * abs(fd)
 
 
+def _with_empty_subcell(p0, mat, mu_field=None, kappa_field=None):
+    """The part with an empty subcell (no entries, the next subcell's volume) inserted at
+    the front of the second cell."""
+    from aperi_mech_b200.model import Part
+
+    s = int(p0.cell_groups[1])
+    ptr = np.insert(p0.cell_ptr, s, p0.cell_ptr[s])
+    vols = np.insert(p0.cell_volumes, s, p0.cell_volumes[s])
+    groups = np.array(p0.cell_groups, dtype=np.int64)
+    groups[2:] += 1
+    return Part("cells", mat, cell_ptr=ptr, cell_nodes=p0.cell_nodes, cell_grads=p0.cell_grads, cell_volumes=vols,
+                cell_groups=groups, mu_field=mu_field, kappa_field=kappa_field), s
+
+
+def _fields(mat, n, seed):
+    rng = np.random.default_rng(seed)
+    kappa = mat.lam + 2.0 * mat.mu / 3.0
+    return mat.mu * np.exp(0.2 * rng.standard_normal(n)), kappa * np.exp(0.2 * rng.standard_normal(n))
+
+
+@pytest.mark.parametrize("kind", ["neo_hookean", "linear_elastic", "elastic"])
+def test_oracle_fbar_vjp_matches_finite_differences(oracle_lib, kind):
+    """VJP of the F-bar force (the adjoint extension): lam . (df/du) d and the per-subcell
+    shear and bulk modulus gradients of lam . f against central differences, on a part with
+    modulus fields and an empty subcell (which still enters J-bar, so its moduli matter)."""
+    n = 3
+    X, T = _box(n, seed=10)
+    mat = _material(kind)
+    fb, _, _ = _oracle_parts(oracle_lib, X, T, mat, n)
+    mu_f, k_f = _fields(mat, fb.cell_volumes.size + 1, 11)
+    part, empty = _with_empty_subcell(fb, mat, mu_f, k_f)
+    rng = np.random.default_rng(12)
+    u = 1e-2 * rng.standard_normal(X.shape)
+    lam = rng.standard_normal(X.shape)
+    gu, gm, gk = oracle_lib.OracleProblem(X, [part]).vjp_force(u, lam)
+
+    def lam_f(uu):
+        return float(np.sum(lam * oracle_lib.OracleProblem(X, [part]).internal_force(uu)))
+
+    h = 1e-6
+    for _ in range(2):
+        d = rng.standard_normal(X.shape)
+        fd = (lam_f(u + h * d) - lam_f(u - h * d)) / (2 * h)
+        assert abs(np.sum(gu * d) - fd) < 1e-6 * abs(fd)
+    base = {"mu_field": mu_f, "kappa_field": k_f}
+    for e in [0, empty, 37, mu_f.size - 1]:
+        for field, g in (("mu_field", gm), ("kappa_field", gk)):
+            step = 1e-6 * base[field][e]
+            vals = []
+            for sgn in (1, -1):
+                arr = base[field].copy()
+                arr[e] += sgn * step
+                setattr(part, field, arr)
+                vals.append(lam_f(u))
+            setattr(part, field, base[field])
+            fd = (vals[0] - vals[1]) / (2 * step)
+            # roundoff of the differences floors the check at ~1e-9 of the largest gradient
+            assert abs(g[e] - fd) < 1e-6 * abs(fd) + 1e-8 * abs(g).max(), (field, e)
+    assert gm[empty] != 0.0 and gk[empty] != 0.0
+
+
 @pytest.mark.gpu
 def test_nodal_subcells_setup_matches_oracle(gpu, oracle_lib):
     from aperi_mech_b200.rkpm import nodal_cells, nodal_subcells
@@ -237,3 +298,71 @@ def test_fbar_empty_subcell_counts_in_jbar(gpu, oracle_lib, form, monkeypatch):
     with ExplicitDynamics(X, [part], mass=cells.mass) as m:
         assert rel_err(m.internal_force(u), want) < 1e-12
         assert rel_err(m.internal_force(u, "mixed"), want) < 1e-4
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["neo_hookean", "linear_elastic", "elastic"])
+def test_fbar_vjp_and_adjoint_match_oracle(gpu, oracle_lib, kind):
+    """The library's F-bar VJP (H and L per subcell by the octet kernel, the per-cell
+    derivative, the node-major gather) and the checkpointed adjoint over 20 steps with a
+    held face, against the oracle, on a part with modulus fields and an empty subcell:
+    u-VJP and modulus VJP at 1e-11, loss at 1e-12, modulus gradients at 1e-10 (the linear
+    material's bulk gradient at 1e-9)."""
+    from aperi_mech_b200 import mesh
+    from aperi_mech_b200.model import BoundaryCondition, ExplicitDynamics
+    from aperi_mech_b200.rkpm import nodal_subcells
+
+    n = 3
+    X, T = _box(n, seed=13)
+    mat = _material(kind)
+    cells = nodal_subcells(X, T, mat, np.full(X.shape[0], RADIUS / n))
+    mu_f, k_f = _fields(mat, cells.part.cell_volumes.size + 1, 14)
+    part, _ = _with_empty_subcell(cells.part, mat, mu_f, k_f)
+    fixed = mesh.side_sets(X)["surface_5"]
+    bcs = [BoundaryCondition.fixed(fixed)]
+    rng = np.random.default_rng(15)
+    u = 2e-3 * rng.standard_normal(X.shape)
+    lam = rng.standard_normal(X.shape)
+    v0 = rng.uniform(-0.01, 0.01, size=X.shape)
+    v0[:, 0] += X[:, 2]
+    v0[fixed] = 0.0
+    dt = 0.3 * float(mesh.tet_char_length(X, T).min()) / np.sqrt(1.8 * (mat.lam + 2 * mat.mu) / mat.density)
+    sens = np.arange(0, X.shape[0], 5, dtype=np.int32)[:16]
+    op = oracle_lib.OracleProblem(X, [part], bcs, mass=cells.mass)
+    with ExplicitDynamics(X, [part], bcs, mass=cells.mass) as m:
+        for g, w in zip(m.vjp_force(u, lam), op.vjp_force(u, lam)):
+            assert rel_err(g, w) < 1e-11
+        m.set_state(None, v0)
+        loss, gm, gk = m.adjoint(20, dt, 5, sens)
+    wl, wm, wk = op.adjoint(20, dt, np.zeros_like(X), v0, sens)
+    assert abs(loss - wl) < 1e-12 * abs(wl)
+    assert rel_err(gm, wm) < 1e-10
+    # F-bar takes the volumetric response from J-bar, so the bulk gradient is what is left of
+    # the subcells' volumetric terms after they cancel: for the linear material ~1e-2 of the
+    # shear gradient, with the trajectory's last bits (~1e-12) amplified into ~1e-10 of it.
+    assert rel_err(gk, wk) < (1e-9 if kind == "linear_elastic" else 1e-10)
+
+
+@pytest.mark.gpu
+def test_fbar_vjp_refused_outside_the_cell_stress_form(gpu, oracle_lib, monkeypatch):
+    """The three-pass F-bar form keeps no per-subcell L beside H: the VJP and the adjoint
+    refuse it (AM_ESTATE) and the context stays usable."""
+    from aperi_mech_b200.capi import AM_ESTATE, AmError
+    from aperi_mech_b200.model import ExplicitDynamics
+    from aperi_mech_b200.rkpm import nodal_subcells
+
+    monkeypatch.setenv("APERI_B200_FBAR_PASSES", "3")
+    n = 3
+    X, T = _box(n, seed=8)
+    mat = _material("neo_hookean")
+    cells = nodal_subcells(X, T, mat, np.full(X.shape[0], RADIUS / n))
+    u = 2e-3 * np.random.default_rng(4).standard_normal(X.shape)
+    with ExplicitDynamics(X, [cells.part], mass=cells.mass) as m:
+        with pytest.raises(AmError) as e:
+            m.vjp_force(u, u)
+        assert e.value.code == AM_ESTATE
+        with pytest.raises(AmError) as e:
+            m.adjoint(4, 1e-7, 2, np.arange(4, dtype=np.int32))
+        assert e.value.code == AM_ESTATE
+        want = oracle_lib.OracleProblem(X, [cells.part], mass=cells.mass).internal_force(u)
+        assert rel_err(m.internal_force(u), want) < 1e-12
