@@ -223,6 +223,11 @@ struct Block {
     double* patch_dx64 = nullptr;
     float* geo32 = nullptr;  // per-tet J^-1 and w (see GaussBlockDev)
     double* geo64 = nullptr;
+    int32_t* chunk_ptr = nullptr;  // warp chunks of such a block (see GaussBlockDev)
+    uint32_t* chunk_code = nullptr;
+    uint32_t* chunk_rank = nullptr;
+    int32_t* chunk_ident = nullptr;      // 0 .. 4E - 1: per-corner positions into chunk_scratch
+    double4* chunk_scratch = nullptr;    // 4E per-corner values (VJP, lumped mass), on first use
     // Cell-stress form of a generic cell block (no patches, cells of more than eight entries,
     // no F-bar groups or groups of at most 32 subcells): octet row records of the cells and of the nodes the block
     // touches (one logical slot each), a node of each cell, and the per-cell matrices
@@ -287,8 +292,26 @@ struct Block {
         g.patch_dx64 = patch_dx64;
         g.geo32 = geo32;
         g.geo64 = geo64;
+        g.chunk_ptr = chunk_ptr;
+        g.chunk_code = chunk_code;
+        g.chunk_rank = chunk_rank;
         g.hstate = hstate;
         g.href = href;
+        return g;
+    }
+    // A chunked block's per-corner view for the kernels that write four values per tet: the
+    // identity positions into the scratch array (allocated on first use).
+    am::GaussBlockDev gauss_corners() {
+        const size_t n = static_cast<size_t>(4 * std::max<int64_t>(num_elems, 1));
+        if (!chunk_ident) {
+            std::vector<int32_t> id(n);
+            for (size_t k = 0; k < n; ++k) id[k] = static_cast<int32_t>(k);
+            chunk_ident = dalloc<int32_t>(n, "chunk corner positions");
+            ck(cudaMemcpy(chunk_ident, id.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+        }
+        if (!chunk_scratch) chunk_scratch = dalloc<double4>(n, "chunk corner values");
+        am::GaussBlockDev g = gauss();
+        g.slot_pos = chunk_ident;
         return g;
     }
     am::CellBlockDev cells() const {
@@ -370,6 +393,11 @@ struct Block {
         dfree(patch_dx64);
         dfree(geo32);
         dfree(geo64);
+        dfree(chunk_ptr);
+        dfree(chunk_code);
+        dfree(chunk_rank);
+        dfree(chunk_ident);
+        dfree(chunk_scratch);
         dfree(order_dev);
         dfree(hstate);
         dfree(href);
@@ -479,6 +507,55 @@ struct Block {
         gather = true;
     }
 };
+
+// Warp chunks of a Tet4 block run one thread per tet: chunk c holds tets [32c, 32c + 32) in
+// the processing order. Its distinct nodes, ranked by first appearance over the entry codes
+// q = 32 a + lane (corner a of the chunk's tet lane), take logical slots ptr[c] + rank. The
+// chunk's entries sorted by (rank, code) go four to a lane: word 32 c + l of code / rank
+// holds sorted entries 4 l .. 4 l + 3, a byte each, 0xFF past the chunk's last tet. All of
+// it follows from the element order and the corner order, not from the node numbers.
+struct TetChunks {
+    std::vector<int32_t> ptr, nodes;
+    std::vector<uint32_t> code, rank;
+};
+TetChunks build_tet_chunks(const int32_t* conn, int64_t E) {
+    TetChunks t;
+    const int64_t C = (E + 31) / 32;
+    t.ptr.assign(C + 1, 0);
+    t.code.assign(static_cast<size_t>(32 * C), 0xFFFFFFFFu);
+    t.rank.assign(static_cast<size_t>(32 * C), 0xFFFFFFFFu);
+    for (int64_t c = 0; c < C; ++c) {
+        const int64_t e0 = 32 * c;
+        const int n = static_cast<int>(std::min<int64_t>(32, E - e0));
+        int32_t node[128];
+        int which[128], count[129] = {0};
+        int nd = 0;
+        for (int q = 0; q < 128; ++q) {
+            which[q] = -1;
+            if ((q & 31) >= n) continue;
+            const int32_t v = conn[4 * (e0 + (q & 31)) + (q >> 5)];
+            int k = 0;
+            while (k < nd && node[k] != v) ++k;
+            if (k == nd) node[nd++] = v;
+            which[q] = k;
+            ++count[k + 1];
+        }
+        for (int k = 0; k < nd; ++k) count[k + 1] += count[k];
+        int fill[128];
+        for (int k = 0; k < nd; ++k) fill[k] = count[k];
+        for (int q = 0; q < 128; ++q) {
+            if (which[q] < 0) continue;
+            const int j = fill[which[q]]++;  // sorted position
+            const size_t w = static_cast<size_t>(32 * c + j / 4);
+            const int sh = 8 * (j % 4);
+            t.code[w] = (t.code[w] & ~(0xFFu << sh)) | (static_cast<uint32_t>(q) << sh);
+            t.rank[w] = (t.rank[w] & ~(0xFFu << sh)) | (static_cast<uint32_t>(which[q]) << sh);
+        }
+        for (int k = 0; k < nd; ++k) t.nodes.push_back(node[k]);
+        t.ptr[c + 1] = t.ptr[c] + nd;
+    }
+    return t;
+}
 
 // Greedy element patches: consecutive tets are grouped while the patch has at most
 // 6 tets on at most 8 distinct nodes (the six tets of a split hex form one patch).
@@ -595,6 +672,9 @@ struct am_ctx {
     // table built at am_add_block (the default) or, with APERI_B200_TET4_GEOMETRY=0,
     // gather the coordinates and invert J every step.
     bool tet_geometry = true;
+    // Such blocks write one slot per distinct node of each warp's 32 tets (the default) or,
+    // with APERI_B200_TET4_CHUNKS=0, four per tet.
+    bool tet_chunks = true;
     int32_t node_lanes = 0;  // APERI_B200_NODE_LANES (1, 2, 4, 8): lanes per node; 0 chosen per mesh
     bool cell_gather = true;
     // The defaults measured fastest on the RKPM nodal cells of the h = 1/46 box: FP64 4 and
@@ -950,6 +1030,13 @@ struct am_ctx {
             double* gk = gkappa ? gkappa + off : nullptr;
             if (b.kind == AM_SMOOTHED_CELLS) {
                 launches += am::launch_cell_vjp(b.cells(), U, L, b.vjp_lmat, slots64, gm, gk, accumulate, stream);
+            } else if (b.chunk_ptr) {
+                // per-corner values, then the chunk sums (scratch allocated by prepare_vjp)
+                am::GaussBlockDev g = b.gauss();
+                g.slot_pos = b.chunk_ident;
+                am::launch_gauss_vjp(g, X4, U, L, b.chunk_scratch, gm, gk, accumulate, stream);
+                am::launch_chunk_sum(b.gauss(), b.chunk_scratch, slots64, stream);
+                launches += 2;
             } else {
                 am::launch_gauss_vjp(b.gauss(), X4, U, L, slots64, gm, gk, accumulate, stream);
                 ++launches;
@@ -971,6 +1058,7 @@ struct am_ctx {
     // most 32 subcells), which keeps L_s per subcell beside H_s.
     void prepare_vjp(const char* what) {
         for (auto& b : blocks) {
+            if (b.chunk_ptr) (void)b.gauss_corners();
             if (!b.group_ptr) continue;
             if (!b.gather) fail(AM_ESTATE, std::string(what) + " on F-bar cells needs the cell-stress form (cells of at most 32 subcells)");
             if (!b.vjp_lmat) b.vjp_lmat = dalloc<double>(std::max<int64_t>(9 * b.num_elems, 1), "F-bar VJP scratch");
@@ -1430,6 +1518,8 @@ int am_create(int64_t num_nodes, const double* coords, am_ctx** out) {
         c->rk_octets = !(ro && ro[0] == '0');
         const char* tg = std::getenv("APERI_B200_TET4_GEOMETRY");
         c->tet_geometry = !(tg && tg[0] == '0');
+        const char* tc = std::getenv("APERI_B200_TET4_CHUNKS");
+        c->tet_chunks = !(tc && tc[0] == '0');
         const char* cg = std::getenv("APERI_B200_CELL_GATHER");
         c->cell_gather = !(cg && cg[0] == '0');
         // four digits: FP64 cell, FP64 gather, mixed cell, mixed gather kernel (1, 2 or 4)
@@ -1634,6 +1724,19 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
                     b.geo64 = dalloc<double>(10 * E, "tet geometry");
                     am::launch_tet4_geometry(b.conn, E, ctx->X4, b.geo32, b.geo64, ctx->stream);
                     ck(cudaGetLastError(), "tet geometry");
+                    if (ctx->tet_chunks) {
+                        TetChunks tc = build_tet_chunks(conn, E);
+                        const int64_t C = static_cast<int64_t>(tc.ptr.size()) - 1;
+                        const int64_t G = static_cast<int64_t>(tc.nodes.size());
+                        b.chunk_ptr = dalloc<int32_t>(C + 1, "chunk offsets");
+                        b.chunk_code = dalloc<uint32_t>(32 * C, "chunk entry codes");
+                        b.chunk_rank = dalloc<uint32_t>(32 * C, "chunk entry ranks");
+                        ck(cudaMemcpy(b.chunk_ptr, tc.ptr.data(), (C + 1) * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+                        ck(cudaMemcpy(b.chunk_code, tc.code.data(), 32 * C * sizeof(uint32_t), cudaMemcpyHostToDevice), "upload");
+                        ck(cudaMemcpy(b.chunk_rank, tc.rank.data(), 32 * C * sizeof(uint32_t), cudaMemcpyHostToDevice), "upload");
+                        b.host_nodes = std::move(tc.nodes);
+                        b.slot_count = G;
+                    }
                 }
             }
             if (ctx->num_slots + b.num_entries >= (int64_t(1) << 31)) fail(AM_ERANGE, "slot count beyond int32 indexing");
@@ -1830,9 +1933,17 @@ int am_finalize(am_ctx* ctx) {
         if (!ctx->mass_set) {
             if (has_cells) fail(AM_EINVAL, "smoothed-cell blocks need an explicit lumped mass (am_set_mass)");
             // Lumped mass (src/MassUtils.cpp:17-112) on the device, summed in element order.
-            for (const auto& b : ctx->blocks) {
-                am::launch_gauss_volume_slots(b.gauss(), b.density, ctx->X4, ctx->slots64, ctx->stream);
-                ++ctx->launches;
+            for (auto& b : ctx->blocks) {
+                if (b.chunk_ptr) {
+                    // allocates the scratch first: it is an argument of the launch below
+                    const am::GaussBlockDev corners = b.gauss_corners();
+                    am::launch_gauss_volume_slots(corners, b.density, ctx->X4, b.chunk_scratch, ctx->stream);
+                    am::launch_chunk_sum(b.gauss(), b.chunk_scratch, ctx->slots64, ctx->stream);
+                    ctx->launches += 2;
+                } else {
+                    am::launch_gauss_volume_slots(b.gauss(), b.density, ctx->X4, ctx->slots64, ctx->stream);
+                    ++ctx->launches;
+                }
             }
             am::launch_gather_force(ctx->node_dev(), 0, ctx->slots64, ctx->f_scratch, 0, ctx->stream);
             ++ctx->launches;

@@ -241,19 +241,122 @@ __global__ void __launch_bounds__(256) k_tet4_geometry(const int32_t* __restrict
     reinterpret_cast<float2*>(g32 + 8 * E)[e] = make_float2(float(Ji[8]), float(w));
 }
 
-template <typename T, int MAT>
-__global__ void __launch_bounds__(256) k_tet4_force_geo(GaussBlockDev b, const double4* __restrict__ U4,
+// A lane's share of a warp chunk (see GaussBlockDev): its four sorted entries (code and
+// node-rank bytes) and, for each entry that is the last of its node's run, the node's slot.
+struct ChunkLane {
+    uint32_t cw, rw;
+    int32_t pos[4];
+};
+__device__ __forceinline__ int chunk_byte(uint32_t w, int j) { return static_cast<int>((w >> (8 * j)) & 0xFFu); }
+// All 32 lanes call it (live is uniform over the warp).
+__device__ __forceinline__ ChunkLane chunk_lane(const GaussBlockDev& b, int64_t ch, int lane, bool live) {
+    ChunkLane L{0xFFFFFFFFu, 0xFFFFFFFFu, {-1, -1, -1, -1}};
+    int32_t n0 = 0;
+    if (live) {
+        L.cw = b.chunk_code[32 * ch + lane];
+        L.rw = b.chunk_rank[32 * ch + lane];
+        n0 = b.chunk_ptr[ch];
+    }
+    const uint32_t nw = __shfl_down_sync(kFull, L.rw, 1);
+    const int rnext = lane == 31 ? 0x100 : chunk_byte(nw, 0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int r = chunk_byte(L.rw, j), after = j < 3 ? chunk_byte(L.rw, j + 1) : rnext;
+        if (r != after && r != 0xFF) L.pos[j] = b.slot_pos[n0 + r];
+    }
+    return L;
+}
+// Sums the chunk's entries per node and writes each node's slot once: a lane sums the runs
+// of its four sorted entries, a segmented inclusive scan over the lanes (fixed shuffle tree)
+// carries a run across lane boundaries, and the lane holding a node's last entry writes it.
+// value(q, v) gives entry q's three components. All 32 lanes call it.
+template <typename T, typename Value>
+__device__ __forceinline__ void chunk_reduce(const ChunkLane& L, int lane, Value value, vec4_t<T>* __restrict__ slots) {
+    T run[3] = {T(0), T(0), T(0)}, head[3] = {T(0), T(0), T(0)};
+    bool split = false;  // the lane's first run ends inside the lane
+    int32_t posh = -1;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int r = chunk_byte(L.rw, j);
+        if (j > 0 && r != chunk_byte(L.rw, j - 1)) {
+            if (!split) {
+                // the first run may continue one from the lanes before: written after the scan
+#pragma unroll
+                for (int i = 0; i < 3; ++i) head[i] = run[i];
+                split = true;
+                posh = L.pos[j - 1];
+            } else if (chunk_byte(L.rw, j - 1) != 0xFF) {
+                slots[L.pos[j - 1]] = make4(run[0], run[1], run[2]);  // a run wholly inside the lane
+            }
+#pragma unroll
+            for (int i = 0; i < 3; ++i) run[i] = T(0);
+        }
+        const int q = chunk_byte(L.cw, j);
+        if (q != 0xFF) {
+            T v[3];
+            value(q, v);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) run[i] += v[i];
+        }
+    }
+    // the last run's sum over the lanes it spans: (value, starts here) scanned with
+    // (a, fa) + (b, fb) = (fb ? b : a + b, fa | fb)
+    const int r0 = chunk_byte(L.rw, 0);
+    const int rprev = __shfl_up_sync(kFull, chunk_byte(L.rw, 3), 1);
+    bool F = split || lane == 0 || r0 != rprev;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        T u[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) u[i] = __shfl_up_sync(kFull, run[i], d);
+        const bool fu = __shfl_up_sync(kFull, static_cast<int>(F), d) != 0;
+        if (lane >= d) {
+            if (!F) {
+#pragma unroll
+                for (int i = 0; i < 3; ++i) run[i] = u[i] + run[i];
+            }
+            F = F || fu;
+        }
+    }
+    T carry[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) carry[i] = __shfl_up_sync(kFull, run[i], 1);
+    if (split && r0 != 0xFF) {
+        const bool cont = lane > 0 && r0 == rprev;
+        slots[posh] = make4(cont ? carry[0] + head[0] : head[0], cont ? carry[1] + head[1] : head[1],
+                            cont ? carry[2] + head[2] : head[2]);
+    }
+    if (L.pos[3] >= 0) slots[L.pos[3]] = make4(run[0], run[1], run[2]);
+}
+
+// One thread per tet. CHUNKS: the warp's 32 tets (a chunk) stage their corner forces in
+// shared memory and sum them per distinct node (about 32 for 128 corners on a Morton-ordered
+// tet mesh), a quarter of the slots of four per tet for the node kernel to read.
+template <typename T, int MAT, bool CHUNKS>
+__global__ void __launch_bounds__(256, CHUNKS && sizeof(T) == 8 ? 3 : 0) k_tet4_force_geo(GaussBlockDev b, const double4* __restrict__ U4,
                                                          vec4_t<T>* __restrict__ slots, int* status) {
     pdl_trigger();
-    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (e >= b.num_elems) return;
     const int64_t E = b.num_elems;
+    const int64_t et = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    // chunked: lanes past the last tet run a copy of it (never summed) to reach the warp sum
+    if (!CHUNKS && et >= E) return;
+    const int64_t e = et < E ? et : E - 1;
     const int4 c = reinterpret_cast<const int4*>(b.conn)[e];
     const T* geo = tet_geo<T>(b);
     const vec4_t<T> g0 = ld_geo4(reinterpret_cast<const vec4_t<T>*>(geo) + e);
     const vec4_t<T> g1 = ld_geo4(reinterpret_cast<const vec4_t<T>*>(geo + 4 * E) + e);
     const typename Vec2Of<T>::type g2 = __ldg(reinterpret_cast<const typename Vec2Of<T>::type*>(geo + 8 * E) + e);
-    const int32_t pos[4] = {b.slot_pos[4 * e], b.slot_pos[4 * e + 1], b.slot_pos[4 * e + 2], b.slot_pos[4 * e + 3]};
+    int32_t pos[4] = {0, 0, 0, 0};
+    const int64_t ch = et >> 5;
+    const int lane = static_cast<int>(threadIdx.x & 31);
+    const bool live = 32 * ch < E;
+    ChunkLane L{};
+    if (!CHUNKS) {
+#pragma unroll
+        for (int a = 0; a < 4; ++a) pos[a] = b.slot_pos[4 * e + a];
+    } else {
+        L = chunk_lane(b, ch, lane, live);
+    }
     double lam, mu;
     element_lame(b, e, lam, mu);
     pdl_wait();
@@ -307,9 +410,45 @@ __global__ void __launch_bounds__(256) k_tet4_force_geo(GaussBlockDev b, const d
     for (int k = 0; k < 3; ++k)
 #pragma unroll
         for (int i = 0; i < 3; ++i) f0[i] += Q[k * 3 + i];
-    slots[pos[0]] = make4(f0[0], f0[1], f0[2]);
+    if constexpr (!CHUNKS) {
+        slots[pos[0]] = make4(f0[0], f0[1], f0[2]);
 #pragma unroll
-    for (int k = 0; k < 3; ++k) slots[pos[k + 1]] = make4(-Q[k * 3 + 0], -Q[k * 3 + 1], -Q[k * 3 + 2]);
+        for (int k = 0; k < 3; ++k) slots[pos[k + 1]] = make4(-Q[k * 3 + 0], -Q[k * 3 + 1], -Q[k * 3 + 2]);
+    } else {
+        // entry q = 32 a + lane, one component plane per coordinate
+        __shared__ T ent[256 / 32][3][128];
+        T(&st)[3][128] = ent[threadIdx.x >> 5];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            st[i][lane] = f0[i];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) st[i][32 * (k + 1) + lane] = -Q[k * 3 + i];
+        }
+        __syncwarp();
+        if (!live) return;  // the whole warp
+        chunk_reduce<T>(L, lane, [&](int q, T(&v)[3]) {
+            v[0] = st[0][q];
+            v[1] = st[1][q];
+            v[2] = st[2][q];
+        }, slots);
+    }
+}
+
+// Chunked Tet4 blocks outside the force (VJP, lumped mass): the per-tet kernels write
+// corner values to scratch[4 e + a], and a warp per chunk sums them per distinct node in
+// the chunk's entry order into the block's slots.
+__global__ void __launch_bounds__(256) k_chunk_sum(GaussBlockDev b, const double4* __restrict__ scratch,
+                                                    double4* __restrict__ slots) {
+    const int64_t ch = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = static_cast<int>(threadIdx.x & 31);
+    if (32 * ch >= b.num_elems) return;  // the whole warp
+    const ChunkLane L = chunk_lane(b, ch, lane, true);
+    chunk_reduce<double>(L, lane, [&](int q, double(&v)[3]) {
+        const double4 x = scratch[4 * (32 * ch + (q & 31)) + (q >> 5)];
+        v[0] = x.x;
+        v[1] = x.y;
+        v[2] = x.z;
+    }, slots);
 }
 
 // ---------------------------------------------------------------------------
@@ -2992,10 +3131,16 @@ void launch_gauss_force(const GaussBlockDev& b, int mixed, const double4* X4, co
         }
     } else if (b.kind == AM_TET4_GAUSS && b.geo64 != nullptr) {
         const unsigned grid = grid_for(b.num_elems, 256);
-        if (mixed) {
-            AM_DISPATCH_MAT(b.material, (launch_pdl(k_tet4_force_geo<float, M>, grid, 256, s, b, U4, static_cast<float4*>(slots), status)));
+        if (b.chunk_ptr != nullptr) {
+            if (mixed) {
+                AM_DISPATCH_MAT(b.material, (launch_pdl(k_tet4_force_geo<float, M, true>, grid, 256, s, b, U4, static_cast<float4*>(slots), status)));
+            } else {
+                AM_DISPATCH_MAT(b.material, (launch_pdl(k_tet4_force_geo<double, M, true>, grid, 256, s, b, U4, static_cast<double4*>(slots), status)));
+            }
+        } else if (mixed) {
+            AM_DISPATCH_MAT(b.material, (launch_pdl(k_tet4_force_geo<float, M, false>, grid, 256, s, b, U4, static_cast<float4*>(slots), status)));
         } else {
-            AM_DISPATCH_MAT(b.material, (launch_pdl(k_tet4_force_geo<double, M>, grid, 256, s, b, U4, static_cast<double4*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (launch_pdl(k_tet4_force_geo<double, M, false>, grid, 256, s, b, U4, static_cast<double4*>(slots), status)));
         }
     } else if (b.kind == AM_TET4_GAUSS) {
         const unsigned grid = grid_for(b.num_elems, 256);
@@ -3240,6 +3385,11 @@ void launch_hex6_patch_dx(const int32_t* patch_nodes, int64_t num_patches, const
                           double* dx64, cudaStream_t stream) {
     if (num_patches <= 0) return;
     k_hex6_patch_dx<<<grid_for(num_patches, 256), 256, 0, stream>>>(patch_nodes, num_patches, X4, dx32, dx64);
+}
+
+void launch_chunk_sum(const GaussBlockDev& b, const double4* scratch, double4* slots, cudaStream_t s) {
+    if (b.num_elems == 0) return;
+    k_chunk_sum<<<grid_for(b.num_elems, 256), 256, 0, s>>>(b, scratch, slots);
 }
 
 void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const double4* X4, double4* slots,
