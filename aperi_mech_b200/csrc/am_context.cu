@@ -226,8 +226,9 @@ struct Block {
     int32_t* chunk_ptr = nullptr;  // warp chunks of such a block (see GaussBlockDev)
     uint32_t* chunk_code = nullptr;
     uint32_t* chunk_rank = nullptr;
-    int32_t* chunk_ident = nullptr;      // 0 .. 4E - 1: per-corner positions into chunk_scratch
-    double4* chunk_scratch = nullptr;    // 4E per-corner values (VJP, lumped mass), on first use
+    int32_t* chunk_pos = nullptr;
+    int32_t* chunk_ident = nullptr;      // 0 .. nn E - 1: per-corner positions into chunk_scratch
+    double4* chunk_scratch = nullptr;    // nn E per-corner values (VJP, lumped mass), on first use
     // Cell-stress form of a generic cell block (no patches, cells of more than eight entries,
     // no F-bar groups or groups of at most 32 subcells): octet row records of the cells and of the nodes the block
     // touches (one logical slot each), a node of each cell, and the per-cell matrices
@@ -295,6 +296,7 @@ struct Block {
         g.chunk_ptr = chunk_ptr;
         g.chunk_code = chunk_code;
         g.chunk_rank = chunk_rank;
+        g.chunk_pos = chunk_pos;
         g.hstate = hstate;
         g.href = href;
         return g;
@@ -302,7 +304,8 @@ struct Block {
     // A chunked block's per-corner view for the kernels that write four values per tet: the
     // identity positions into the scratch array (allocated on first use).
     am::GaussBlockDev gauss_corners() {
-        const size_t n = static_cast<size_t>(4 * std::max<int64_t>(num_elems, 1));
+        const int nn = kind == AM_HEX8_GAUSS ? 8 : 4;
+        const size_t n = static_cast<size_t>(nn * std::max<int64_t>(num_elems, 1));
         if (!chunk_ident) {
             std::vector<int32_t> id(n);
             for (size_t k = 0; k < n; ++k) id[k] = static_cast<int32_t>(k);
@@ -396,6 +399,7 @@ struct Block {
         dfree(chunk_ptr);
         dfree(chunk_code);
         dfree(chunk_rank);
+        dfree(chunk_pos);
         dfree(chunk_ident);
         dfree(chunk_scratch);
         dfree(order_dev);
@@ -508,53 +512,57 @@ struct Block {
     }
 };
 
-// Warp chunks of a Tet4 block run one thread per tet: chunk c holds tets [32c, 32c + 32) in
-// the processing order. Its distinct nodes, ranked by first appearance over the entry codes
-// q = 32 a + lane (corner a of the chunk's tet lane), take logical slots ptr[c] + rank. The
-// chunk's entries sorted by (rank, code) go four to a lane: word 32 c + l of code / rank
-// holds sorted entries 4 l .. 4 l + 3, a byte each, 0xFF past the chunk's last tet. All of
-// it follows from the element order and the corner order, not from the node numbers.
-struct TetChunks {
+// Warp chunks of a Gauss block of nn-node elements run one thread per element: chunk c
+// holds elements [32c, 32c + 32) in the processing order. Its distinct nodes, ranked by first
+// appearance over the entry codes q = 32 a + lane (connectivity node a of the chunk's element
+// lane), take logical slots ptr[c] + rank. The chunk's entries sorted by (rank, code) go nn to
+// a lane, a byte each: words (32 c + l) nn/4 .. (32 c + l + 1) nn/4 - 1 of code / rank hold
+// lane l's, rank 0xFF past the chunk's last element. All of it follows from the element order
+// and the corner order, not from the node numbers. Fails (false) when a chunk has more than
+// 254 distinct nodes, which the rank bytes cannot hold.
+struct WarpChunks {
     std::vector<int32_t> ptr, nodes;
     std::vector<uint32_t> code, rank;
 };
-TetChunks build_tet_chunks(const int32_t* conn, int64_t E) {
-    TetChunks t;
+bool build_warp_chunks(const int32_t* conn, int64_t E, int nn, WarpChunks& t) {
     const int64_t C = (E + 31) / 32;
+    const int W = nn / 4, Q = 32 * nn;
     t.ptr.assign(C + 1, 0);
-    t.code.assign(static_cast<size_t>(32 * C), 0xFFFFFFFFu);
-    t.rank.assign(static_cast<size_t>(32 * C), 0xFFFFFFFFu);
+    t.nodes.clear();
+    t.code.assign(static_cast<size_t>(32 * W * C), 0xFFFFFFFFu);
+    t.rank.assign(static_cast<size_t>(32 * W * C), 0xFFFFFFFFu);
+    std::vector<int32_t> node(Q);
+    std::vector<int> which(Q), count(Q + 1), fill(Q);
     for (int64_t c = 0; c < C; ++c) {
         const int64_t e0 = 32 * c;
         const int n = static_cast<int>(std::min<int64_t>(32, E - e0));
-        int32_t node[128];
-        int which[128], count[129] = {0};
+        std::fill(count.begin(), count.end(), 0);
         int nd = 0;
-        for (int q = 0; q < 128; ++q) {
+        for (int q = 0; q < Q; ++q) {
             which[q] = -1;
             if ((q & 31) >= n) continue;
-            const int32_t v = conn[4 * (e0 + (q & 31)) + (q >> 5)];
+            const int32_t v = conn[nn * (e0 + (q & 31)) + (q >> 5)];
             int k = 0;
             while (k < nd && node[k] != v) ++k;
             if (k == nd) node[nd++] = v;
             which[q] = k;
             ++count[k + 1];
         }
+        if (nd > 254) return false;
         for (int k = 0; k < nd; ++k) count[k + 1] += count[k];
-        int fill[128];
         for (int k = 0; k < nd; ++k) fill[k] = count[k];
-        for (int q = 0; q < 128; ++q) {
+        for (int q = 0; q < Q; ++q) {
             if (which[q] < 0) continue;
-            const int j = fill[which[q]]++;  // sorted position
-            const size_t w = static_cast<size_t>(32 * c + j / 4);
+            const int j = fill[which[q]]++;  // sorted position: lane j / nn, entry j % nn of it
+            const size_t w = static_cast<size_t>((32 * c + j / nn) * W + (j % nn) / 4);
             const int sh = 8 * (j % 4);
-            t.code[w] = (t.code[w] & ~(0xFFu << sh)) | (static_cast<uint32_t>(q) << sh);
+            t.code[w] = (t.code[w] & ~(0xFFu << sh)) | (static_cast<uint32_t>(q & 0xFF) << sh);
             t.rank[w] = (t.rank[w] & ~(0xFFu << sh)) | (static_cast<uint32_t>(which[q]) << sh);
         }
         for (int k = 0; k < nd; ++k) t.nodes.push_back(node[k]);
         t.ptr[c + 1] = t.ptr[c] + nd;
     }
-    return t;
+    return true;
 }
 
 // Greedy element patches: consecutive tets are grouped while the patch has at most
@@ -672,9 +680,10 @@ struct am_ctx {
     // table built at am_add_block (the default) or, with APERI_B200_TET4_GEOMETRY=0,
     // gather the coordinates and invert J every step.
     bool tet_geometry = true;
-    // Such blocks write one slot per distinct node of each warp's 32 tets (the default) or,
-    // with APERI_B200_TET4_CHUNKS=0, four per tet.
-    bool tet_chunks = true;
+    // One-thread-per-tet blocks (total formulation, geometry table) write one slot per
+    // distinct node of each warp's 32 tets (the default) or, with APERI_B200_WARP_CHUNKS=0,
+    // four per tet.
+    bool warp_chunks = true;
     int32_t node_lanes = 0;  // APERI_B200_NODE_LANES (1, 2, 4, 8): lanes per node; 0 chosen per mesh
     bool cell_gather = true;
     // The defaults measured fastest on the RKPM nodal cells of the h = 1/46 box: FP64 4 and
@@ -1518,8 +1527,8 @@ int am_create(int64_t num_nodes, const double* coords, am_ctx** out) {
         c->rk_octets = !(ro && ro[0] == '0');
         const char* tg = std::getenv("APERI_B200_TET4_GEOMETRY");
         c->tet_geometry = !(tg && tg[0] == '0');
-        const char* tc = std::getenv("APERI_B200_TET4_CHUNKS");
-        c->tet_chunks = !(tc && tc[0] == '0');
+        const char* wch = std::getenv("APERI_B200_WARP_CHUNKS");
+        c->warp_chunks = !(wch && wch[0] == '0');
         const char* cg = std::getenv("APERI_B200_CELL_GATHER");
         c->cell_gather = !(cg && cg[0] == '0');
         // four digits: FP64 cell, FP64 gather, mixed cell, mixed gather kernel (1, 2 or 4)
@@ -1724,19 +1733,22 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
                     b.geo64 = dalloc<double>(10 * E, "tet geometry");
                     am::launch_tet4_geometry(b.conn, E, ctx->X4, b.geo32, b.geo64, ctx->stream);
                     ck(cudaGetLastError(), "tet geometry");
-                    if (ctx->tet_chunks) {
-                        TetChunks tc = build_tet_chunks(conn, E);
-                        const int64_t C = static_cast<int64_t>(tc.ptr.size()) - 1;
-                        const int64_t G = static_cast<int64_t>(tc.nodes.size());
-                        b.chunk_ptr = dalloc<int32_t>(C + 1, "chunk offsets");
-                        b.chunk_code = dalloc<uint32_t>(32 * C, "chunk entry codes");
-                        b.chunk_rank = dalloc<uint32_t>(32 * C, "chunk entry ranks");
-                        ck(cudaMemcpy(b.chunk_ptr, tc.ptr.data(), (C + 1) * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
-                        ck(cudaMemcpy(b.chunk_code, tc.code.data(), 32 * C * sizeof(uint32_t), cudaMemcpyHostToDevice), "upload");
-                        ck(cudaMemcpy(b.chunk_rank, tc.rank.data(), 32 * C * sizeof(uint32_t), cudaMemcpyHostToDevice), "upload");
-                        b.host_nodes = std::move(tc.nodes);
-                        b.slot_count = G;
-                    }
+                }
+                // Warp chunks for the one-thread-per-tet kernel (Hex8 measured no gain: its
+                // issue-bound element kernel paid for the warp sums what its node kernel saved).
+                WarpChunks wc;
+                if (ctx->warp_chunks && E > 0 && d->kind == AM_TET4_GAUSS && b.geo64 && build_warp_chunks(conn, E, nn, wc)) {
+                    const int64_t C = static_cast<int64_t>(wc.ptr.size()) - 1;
+                    const int64_t G = static_cast<int64_t>(wc.nodes.size());
+                    const size_t words = wc.code.size();
+                    b.chunk_ptr = dalloc<int32_t>(C + 1, "chunk offsets");
+                    b.chunk_code = dalloc<uint32_t>(words, "chunk entry codes");
+                    b.chunk_rank = dalloc<uint32_t>(words, "chunk entry ranks");
+                    ck(cudaMemcpy(b.chunk_ptr, wc.ptr.data(), (C + 1) * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+                    ck(cudaMemcpy(b.chunk_code, wc.code.data(), words * sizeof(uint32_t), cudaMemcpyHostToDevice), "upload");
+                    ck(cudaMemcpy(b.chunk_rank, wc.rank.data(), words * sizeof(uint32_t), cudaMemcpyHostToDevice), "upload");
+                    b.host_nodes = std::move(wc.nodes);
+                    b.slot_count = G;
                 }
             }
             if (ctx->num_slots + b.num_entries >= (int64_t(1) << 31)) fail(AM_ERANGE, "slot count beyond int32 indexing");
@@ -1927,6 +1939,13 @@ int am_finalize(am_ctx* ctx) {
         for (auto& b : ctx->blocks) {
             b.slot_pos = ctx->slot_pos + b.slot_base;
             std::vector<int32_t>().swap(b.host_nodes);
+            if (b.chunk_ptr) {
+                const int nn = b.kind == AM_HEX8_GAUSS ? 8 : 4;
+                b.chunk_pos = dalloc<int32_t>(static_cast<size_t>(32 * nn * ((b.num_elems + 31) / 32)), "chunk positions");
+                am::launch_chunk_positions(b.gauss(), b.chunk_pos, ctx->stream);
+                ++ctx->launches;
+                ck(cudaGetLastError(), "chunk positions");
+            }
         }
         bool has_cells = false;
         for (const auto& b : ctx->blocks) has_cells |= b.kind == AM_SMOOTHED_CELLS;
@@ -1951,6 +1970,11 @@ int am_finalize(am_ctx* ctx) {
             std::vector<double> f(N * 3), m(N);
             ck(cudaMemcpyAsync(f.data(), ctx->f_scratch, N * 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
             ck(cudaStreamSynchronize(ctx->stream), "synchronize");
+            for (auto& b : ctx->blocks) {
+                // the per-corner scratch of the chunked mass comes back on first use (VJP)
+                dfree(b.chunk_ident);
+                dfree(b.chunk_scratch);
+            }
             for (int64_t i = 0; i < N; ++i) {
                 m[i] = f[3 * i];
                 if (!(m[i] > 0.0)) fail(AM_EINVAL, "node " + std::to_string(i) + " has no mass (not connected to an element)");

@@ -241,42 +241,73 @@ __global__ void __launch_bounds__(256) k_tet4_geometry(const int32_t* __restrict
     reinterpret_cast<float2*>(g32 + 8 * E)[e] = make_float2(float(Ji[8]), float(w));
 }
 
-// A lane's share of a warp chunk (see GaussBlockDev): its four sorted entries (code and
-// node-rank bytes) and, for each entry that is the last of its node's run, the node's slot.
+// A lane's share of a warp chunk (see GaussBlockDev): its K sorted entries (K / 4 words of
+// code bytes and of node-rank bytes; rank 0xFF past the chunk's last element) and, for each
+// entry that is the last of its node's run, the node's slot.
+template <int K>
 struct ChunkLane {
-    uint32_t cw, rw;
-    int32_t pos[4];
+    uint32_t cw[K / 4], rw[K / 4];
+    int32_t pos[K];
 };
-__device__ __forceinline__ int chunk_byte(uint32_t w, int j) { return static_cast<int>((w >> (8 * j)) & 0xFFu); }
-// All 32 lanes call it (live is uniform over the warp).
-__device__ __forceinline__ ChunkLane chunk_lane(const GaussBlockDev& b, int64_t ch, int lane, bool live) {
-    ChunkLane L{0xFFFFFFFFu, 0xFFFFFFFFu, {-1, -1, -1, -1}};
-    int32_t n0 = 0;
-    if (live) {
-        L.cw = b.chunk_code[32 * ch + lane];
-        L.rw = b.chunk_rank[32 * ch + lane];
-        n0 = b.chunk_ptr[ch];
-    }
-    const uint32_t nw = __shfl_down_sync(kFull, L.rw, 1);
-    const int rnext = lane == 31 ? 0x100 : chunk_byte(nw, 0);
+__device__ __forceinline__ int chunk_byte(const uint32_t* w, int j) {
+    return static_cast<int>((w[j >> 2] >> (8 * (j & 3))) & 0xFFu);
+}
+// The lane's plan: its words and its run-end slot positions (resolved once by
+// k_chunk_positions), independent loads.
+template <int K>
+__device__ __forceinline__ ChunkLane<K> chunk_lane(const GaussBlockDev& b, int64_t ch, int lane, bool live) {
+    constexpr int W = K / 4;
+    ChunkLane<K> L;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const int r = chunk_byte(L.rw, j), after = j < 3 ? chunk_byte(L.rw, j + 1) : rnext;
-        if (r != after && r != 0xFF) L.pos[j] = b.slot_pos[n0 + r];
+    for (int w = 0; w < W; ++w) L.cw[w] = L.rw[w] = 0xFFFFFFFFu;
+#pragma unroll
+    for (int j = 0; j < K; ++j) L.pos[j] = -1;
+    if (live) {
+        const int64_t l = 32 * ch + lane;
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            L.cw[w] = b.chunk_code[l * W + w];
+            L.rw[w] = b.chunk_rank[l * W + w];
+            const int4 p = reinterpret_cast<const int4*>(b.chunk_pos)[l * W + w];
+            L.pos[4 * w] = p.x, L.pos[4 * w + 1] = p.y, L.pos[4 * w + 2] = p.z, L.pos[4 * w + 3] = p.w;
+        }
     }
     return L;
 }
+
+// Set-up, a warp per chunk: the slot position of each lane entry that ends its node's run
+// (the next sorted entry, in this lane or the next, has another rank), else -1.
+template <int K>
+__global__ void __launch_bounds__(256) k_chunk_positions(GaussBlockDev b, int32_t* __restrict__ out) {
+    constexpr int W = K / 4;
+    const int64_t ch = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = static_cast<int>(threadIdx.x & 31);
+    if (32 * ch >= b.num_elems) return;  // the whole warp
+    const int64_t l = 32 * ch + lane;
+    uint32_t rw[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) rw[w] = b.chunk_rank[l * W + w];
+    const int32_t n0 = b.chunk_ptr[ch];
+    const uint32_t nw = __shfl_down_sync(kFull, rw[0], 1);
+    const int rnext = lane == 31 ? 0x100 : static_cast<int>(nw & 0xFFu);
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        const int r = chunk_byte(rw, j), after = j < K - 1 ? chunk_byte(rw, j + 1) : rnext;
+        out[l * K + j] = (r != after && r != 0xFF) ? b.slot_pos[n0 + r] : -1;
+    }
+}
+
 // Sums the chunk's entries per node and writes each node's slot once: a lane sums the runs
-// of its four sorted entries, a segmented inclusive scan over the lanes (fixed shuffle tree)
+// of its K sorted entries, a segmented inclusive scan over the lanes (fixed shuffle tree)
 // carries a run across lane boundaries, and the lane holding a node's last entry writes it.
 // value(q, v) gives entry q's three components. All 32 lanes call it.
-template <typename T, typename Value>
-__device__ __forceinline__ void chunk_reduce(const ChunkLane& L, int lane, Value value, vec4_t<T>* __restrict__ slots) {
+template <typename T, int K, typename Value>
+__device__ __forceinline__ void chunk_reduce(const ChunkLane<K>& L, int lane, Value value, vec4_t<T>* __restrict__ slots) {
     T run[3] = {T(0), T(0), T(0)}, head[3] = {T(0), T(0), T(0)};
     bool split = false;  // the lane's first run ends inside the lane
     int32_t posh = -1;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+    for (int j = 0; j < K; ++j) {
         const int r = chunk_byte(L.rw, j);
         if (j > 0 && r != chunk_byte(L.rw, j - 1)) {
             if (!split) {
@@ -291,10 +322,9 @@ __device__ __forceinline__ void chunk_reduce(const ChunkLane& L, int lane, Value
 #pragma unroll
             for (int i = 0; i < 3; ++i) run[i] = T(0);
         }
-        const int q = chunk_byte(L.cw, j);
-        if (q != 0xFF) {
+        if (r != 0xFF) {
             T v[3];
-            value(q, v);
+            value(chunk_byte(L.cw, j), v);
 #pragma unroll
             for (int i = 0; i < 3; ++i) run[i] += v[i];
         }
@@ -302,7 +332,7 @@ __device__ __forceinline__ void chunk_reduce(const ChunkLane& L, int lane, Value
     // the last run's sum over the lanes it spans: (value, starts here) scanned with
     // (a, fa) + (b, fb) = (fb ? b : a + b, fa | fb)
     const int r0 = chunk_byte(L.rw, 0);
-    const int rprev = __shfl_up_sync(kFull, chunk_byte(L.rw, 3), 1);
+    const int rprev = __shfl_up_sync(kFull, chunk_byte(L.rw, K - 1), 1);
     bool F = split || lane == 0 || r0 != rprev;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
@@ -326,7 +356,7 @@ __device__ __forceinline__ void chunk_reduce(const ChunkLane& L, int lane, Value
         slots[posh] = make4(cont ? carry[0] + head[0] : head[0], cont ? carry[1] + head[1] : head[1],
                             cont ? carry[2] + head[2] : head[2]);
     }
-    if (L.pos[3] >= 0) slots[L.pos[3]] = make4(run[0], run[1], run[2]);
+    if (L.pos[K - 1] >= 0) slots[L.pos[K - 1]] = make4(run[0], run[1], run[2]);
 }
 
 // One thread per tet. CHUNKS: the warp's 32 tets (a chunk) stage their corner forces in
@@ -350,12 +380,12 @@ __global__ void __launch_bounds__(256, CHUNKS && sizeof(T) == 8 ? 3 : 0) k_tet4_
     const int64_t ch = et >> 5;
     const int lane = static_cast<int>(threadIdx.x & 31);
     const bool live = 32 * ch < E;
-    ChunkLane L{};
+    ChunkLane<4> L{};
     if (!CHUNKS) {
 #pragma unroll
         for (int a = 0; a < 4; ++a) pos[a] = b.slot_pos[4 * e + a];
     } else {
-        L = chunk_lane(b, ch, lane, live);
+        L = chunk_lane<4>(b, ch, lane, live);
     }
     double lam, mu;
     element_lame(b, e, lam, mu);
@@ -426,7 +456,7 @@ __global__ void __launch_bounds__(256, CHUNKS && sizeof(T) == 8 ? 3 : 0) k_tet4_
         }
         __syncwarp();
         if (!live) return;  // the whole warp
-        chunk_reduce<T>(L, lane, [&](int q, T(&v)[3]) {
+        chunk_reduce<T, 4>(L, lane, [&](int q, T(&v)[3]) {
             v[0] = st[0][q];
             v[1] = st[1][q];
             v[2] = st[2][q];
@@ -434,17 +464,18 @@ __global__ void __launch_bounds__(256, CHUNKS && sizeof(T) == 8 ? 3 : 0) k_tet4_
     }
 }
 
-// Chunked Tet4 blocks outside the force (VJP, lumped mass): the per-tet kernels write
-// corner values to scratch[4 e + a], and a warp per chunk sums them per distinct node in
-// the chunk's entry order into the block's slots.
+// Chunked blocks outside the force (VJP, lumped mass): the per-element kernels write corner
+// values to scratch[NN e + a], and a warp per chunk sums them per distinct node with the
+// chunk's plan into the block's slots.
+template <int NN>
 __global__ void __launch_bounds__(256) k_chunk_sum(GaussBlockDev b, const double4* __restrict__ scratch,
                                                     double4* __restrict__ slots) {
     const int64_t ch = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const int lane = static_cast<int>(threadIdx.x & 31);
     if (32 * ch >= b.num_elems) return;  // the whole warp
-    const ChunkLane L = chunk_lane(b, ch, lane, true);
-    chunk_reduce<double>(L, lane, [&](int q, double(&v)[3]) {
-        const double4 x = scratch[4 * (32 * ch + (q & 31)) + (q >> 5)];
+    const ChunkLane<NN> L = chunk_lane<NN>(b, ch, lane, true);
+    chunk_reduce<double, NN>(L, lane, [&](int q, double(&v)[3]) {
+        const double4 x = scratch[NN * (32 * ch + (q & 31)) + (q >> 5)];
         v[0] = x.x;
         v[1] = x.y;
         v[2] = x.z;
@@ -3387,9 +3418,14 @@ void launch_hex6_patch_dx(const int32_t* patch_nodes, int64_t num_patches, const
     k_hex6_patch_dx<<<grid_for(num_patches, 256), 256, 0, stream>>>(patch_nodes, num_patches, X4, dx32, dx64);
 }
 
+void launch_chunk_positions(const GaussBlockDev& b, int32_t* out, cudaStream_t s) {
+    if (b.num_elems == 0) return;
+    k_chunk_positions<4><<<grid_for(b.num_elems, 256), 256, 0, s>>>(b, out);
+}
+
 void launch_chunk_sum(const GaussBlockDev& b, const double4* scratch, double4* slots, cudaStream_t s) {
     if (b.num_elems == 0) return;
-    k_chunk_sum<<<grid_for(b.num_elems, 256), 256, 0, s>>>(b, scratch, slots);
+    k_chunk_sum<4><<<grid_for(b.num_elems, 256), 256, 0, s>>>(b, scratch, slots);
 }
 
 void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const double4* X4, double4* slots,

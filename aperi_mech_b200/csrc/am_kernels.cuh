@@ -59,15 +59,20 @@ struct GaussBlockDev {
     // gathers. null where not built.
     const float* geo32;
     const double* geo64;
-    // Warp chunks of such a block: the 32 tets [32c, 32c + 32) of chunk c sum their forces on
-    // each node they share and write one slot per distinct node; the node of rank k (order
-    // of first appearance over the entry codes q = 32 a + lane, corner a of the chunk's tet
-    // lane) has logical slot chunk_ptr[c] + k. The chunk's 128 entries sorted by (rank,
-    // code): word 32 c + l of chunk_code / chunk_rank holds sorted entries 4 l .. 4 l + 3,
-    // one byte each (0xFF past the chunk's last tet). null: four slots per tet.
+    // Warp chunks (such Tet4 blocks and Hex8 blocks under the total formulation): the 32
+    // elements [32c, 32c + 32) of chunk c sum their forces on each node they share and write
+    // one slot per distinct node; the node of rank k (order of first appearance over the entry
+    // codes q = 32 a + lane, connectivity node a of the chunk's element lane) has logical slot
+    // chunk_ptr[c] + k. The chunk's 32 nn entries (nn nodes per element) sorted by (rank,
+    // code), nn to a lane: words (32 c + l) nn/4 .. (32 c + l + 1) nn/4 - 1 of chunk_code /
+    // chunk_rank hold lane l's, one byte each (rank 0xFF past the chunk's last element).
+    // null: one slot per element node.
     const int32_t* chunk_ptr;
     const uint32_t* chunk_code;
     const uint32_t* chunk_rank;
+    // nn per lane (the lane's word order): the slot position of each entry that ends its
+    // node's run, else -1; resolved at am_finalize
+    const int32_t* chunk_pos;
     // Updated / semi-Lagrangian formulations: element displacement gradient of the last
     // force evaluation (9 per element; for Hex8 the last Gauss point's) and the semi
     // formulation's reference gradient. null under the total formulation.
@@ -174,8 +179,10 @@ void launch_hex6_patch_dx(const int32_t* patch_nodes, int64_t num_patches, const
                           double* dx64, cudaStream_t stream);
 void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const double4* X4, double4* slots,
                                cudaStream_t s);
-// Chunked Tet4 blocks: per-corner values (scratch[4 e + a]) summed into the block's slots.
+// Chunked blocks: per-corner values (scratch[nn e + a]) summed into the block's slots.
 void launch_chunk_sum(const GaussBlockDev& b, const double4* scratch, double4* slots, cudaStream_t s);
+// Chunked blocks: the run-end slot positions of every lane (at am_finalize, after the layout).
+void launch_chunk_positions(const GaussBlockDev& b, int32_t* out, cudaStream_t s);
 
 // f (N x 3, row-major) = gather of the slots (FP64 or FP32 slots), overwrite or accumulate.
 void launch_gather_force(const NodeDev& nd, int mixed, const void* slots, double* f, int accumulate, cudaStream_t s);

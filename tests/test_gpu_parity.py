@@ -481,16 +481,17 @@ def test_tet4_geometry_table(gpu, oracle_lib, monkeypatch, material):
 
 
 @pytest.mark.parametrize("material", ["neo_hookean", "elastic", "linear_elastic"])
-def test_tet4_warp_chunks(gpu, oracle_lib, monkeypatch, material):
+def test_warp_chunks(gpu, oracle_lib, monkeypatch, material):
     """One thread per tet with each warp's 32 tets summing their forces on shared nodes
     before writing one slot per distinct node (the default) and with four slots per tet
-    (APERI_B200_TET4_CHUNKS=0): FP64 and mixed forces, the lumped mass, the VJP with modulus
-    fields and 30 steps against the oracle, on 750 tets (a partial last chunk); the chunked
-    layout writes fewer slots and repeats bit for bit."""
+    (APERI_B200_WARP_CHUNKS=0): FP64 and mixed forces, the lumped mass, the VJP with
+    modulus fields and 30 steps against the oracle, on 750 tets (a partial last chunk); the
+    chunked layout writes fewer slots and repeats bit for bit."""
     from aperi_mech_b200.model import ExplicitDynamics, Part
 
     monkeypatch.setenv("APERI_B200_TET4_PATCHES", "0")
     coords, conn = _mesh("tet4", 5, seed=13)
+    nn = conn.shape[1]
     assert conn.shape[0] % 32 != 0
     mu_f, k_f = _fields(conn.shape[0], 8, True)
     parts = [Part("tet4", _material(material), conn=conn, mu_field=mu_f, kappa_field=k_f)]
@@ -504,7 +505,7 @@ def test_tet4_warp_chunks(gpu, oracle_lib, monkeypatch, material):
     want_s = op.steps(z, v0, op.init_acceleration(z), np.full(30, 1e-7))
     slots = {}
     for chunks in ("1", "0"):
-        monkeypatch.setenv("APERI_B200_TET4_CHUNKS", chunks)
+        monkeypatch.setenv("APERI_B200_WARP_CHUNKS", chunks)
         with ExplicitDynamics(coords, parts) as m:
             slots[chunks] = m.layout()["used_slots"]
             f = m.internal_force(u)
@@ -519,7 +520,7 @@ def test_tet4_warp_chunks(gpu, oracle_lib, monkeypatch, material):
             m.run(30, 1e-7)
             for g, w in zip(m.get_state(), want_s):
                 assert rel_err(g, w) < 1e-12
-    assert slots["0"] == 4 * conn.shape[0] and slots["1"] < slots["0"] // 2
+    assert slots["0"] == nn * conn.shape[0] and slots["1"] < slots["0"] // 2
 
 
 # ---- Tet4 element patches ----------------------------------------------------------------
