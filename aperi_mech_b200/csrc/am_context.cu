@@ -227,6 +227,7 @@ struct Block {
     uint32_t* chunk_code = nullptr;
     uint32_t* chunk_rank = nullptr;
     int32_t* chunk_pos = nullptr;
+    int64_t chunk_units = 0;             // tets, or split-hex half patches (see GaussBlockDev)
     int32_t* chunk_ident = nullptr;      // 0 .. nn E - 1: per-corner positions into chunk_scratch
     double4* chunk_scratch = nullptr;    // nn E per-corner values (VJP, lumped mass), on first use
     // Cell-stress form of a generic cell block (no patches, cells of more than eight entries,
@@ -297,18 +298,26 @@ struct Block {
         g.chunk_code = chunk_code;
         g.chunk_rank = chunk_rank;
         g.chunk_pos = chunk_pos;
+        g.chunk_units = chunk_units;
         g.hstate = hstate;
         g.href = href;
         return g;
     }
-    // A chunked block's per-corner view for the kernels that write four values per tet: the
-    // identity positions into the scratch array (allocated on first use).
+    // A chunked block's per-corner view for the kernels that write one value per element (or
+    // patch) node: positions into the scratch array (allocated on first use) at 4 u + a, unit
+    // u and corner a. Per tet the identity; a split-hex patch p's node k is corner a of half
+    // patch 2p + r (thread r writes nodes 1, 2, 4, 0 or 5, 6, 7, 3).
     am::GaussBlockDev gauss_corners() {
-        const int nn = kind == AM_HEX8_GAUSS ? 8 : 4;
-        const size_t n = static_cast<size_t>(nn * std::max<int64_t>(num_elems, 1));
+        const size_t n = static_cast<size_t>(4 * std::max<int64_t>(chunk_units, 1));
         if (!chunk_ident) {
             std::vector<int32_t> id(n);
-            for (size_t k = 0; k < n; ++k) id[k] = static_cast<int32_t>(k);
+            if (patched == 2) {
+                constexpr int kR[8] = {0, 0, 0, 1, 0, 1, 1, 1}, kA[8] = {3, 0, 1, 3, 2, 0, 1, 2};
+                for (int64_t p = 0; p < num_patches; ++p)
+                    for (int k = 0; k < 8; ++k) id[8 * p + k] = static_cast<int32_t>(4 * (2 * p + kR[k]) + kA[k]);
+            } else {
+                for (size_t k = 0; k < n; ++k) id[k] = static_cast<int32_t>(k);
+            }
             chunk_ident = dalloc<int32_t>(n, "chunk corner positions");
             ck(cudaMemcpy(chunk_ident, id.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
         }
@@ -565,6 +574,21 @@ bool build_warp_chunks(const int32_t* conn, int64_t E, int nn, WarpChunks& t) {
     return true;
 }
 
+// The plan's device arrays; the block's logical slots become the chunks' distinct nodes.
+void upload_warp_chunks(Block& b, WarpChunks& wc, int64_t units) {
+    const int64_t C = static_cast<int64_t>(wc.ptr.size()) - 1;
+    const size_t words = wc.code.size();
+    b.chunk_ptr = dalloc<int32_t>(C + 1, "chunk offsets");
+    b.chunk_code = dalloc<uint32_t>(words, "chunk entry codes");
+    b.chunk_rank = dalloc<uint32_t>(words, "chunk entry ranks");
+    ck(cudaMemcpy(b.chunk_ptr, wc.ptr.data(), (C + 1) * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+    ck(cudaMemcpy(b.chunk_code, wc.code.data(), words * sizeof(uint32_t), cudaMemcpyHostToDevice), "upload");
+    ck(cudaMemcpy(b.chunk_rank, wc.rank.data(), words * sizeof(uint32_t), cudaMemcpyHostToDevice), "upload");
+    b.slot_count = static_cast<int64_t>(wc.nodes.size());
+    b.host_nodes = std::move(wc.nodes);
+    b.chunk_units = units;
+}
+
 // Greedy element patches: consecutive tets are grouped while the patch has at most
 // 6 tets on at most 8 distinct nodes (the six tets of a split hex form one patch).
 struct TetPatches {
@@ -680,9 +704,9 @@ struct am_ctx {
     // table built at am_add_block (the default) or, with APERI_B200_TET4_GEOMETRY=0,
     // gather the coordinates and invert J every step.
     bool tet_geometry = true;
-    // One-thread-per-tet blocks (total formulation, geometry table) write one slot per
-    // distinct node of each warp's 32 tets (the default) or, with APERI_B200_WARP_CHUNKS=0,
-    // four per tet.
+    // One-thread-per-tet blocks (total formulation, geometry table) and split-hex patches
+    // write one slot per distinct node of each warp's 32 tets (16 patches) (the default) or,
+    // with APERI_B200_WARP_CHUNKS=0, one per tet or patch node.
     bool warp_chunks = true;
     int32_t node_lanes = 0;  // APERI_B200_NODE_LANES (1, 2, 4, 8): lanes per node; 0 chosen per mesh
     bool cell_gather = true;
@@ -1725,6 +1749,17 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
                         b.host_nodes.assign(8 * P, -1);
                         for (int64_t q = 0; q < P; ++q)
                             for (int a = 0; a < tp.used[q]; ++a) b.host_nodes[8 * q + a] = tp.nodes[8 * q + a];
+                        if (hex6 && ctx->warp_chunks) {
+                            // warp chunks over the half patches: thread r of patch p writes
+                            // patch nodes 1, 2, 4, 0 (r = 0) or 5, 6, 7, 3 (r = 1)
+                            constexpr int kNode[2][4] = {{1, 2, 4, 0}, {5, 6, 7, 3}};
+                            std::vector<int32_t> half(8 * P);
+                            for (int64_t q = 0; q < P; ++q)
+                                for (int r = 0; r < 2; ++r)
+                                    for (int a = 0; a < 4; ++a) half[4 * (2 * q + r) + a] = tp.nodes[8 * q + kNode[r][a]];
+                            WarpChunks wc;
+                            if (build_warp_chunks(half.data(), 2 * P, 4, wc)) upload_warp_chunks(b, wc, 2 * P);
+                        }
                     }
                 }
                 if (d->kind == AM_TET4_GAUSS && E > 0 && b.patched == 0 && ctx->lagr == 0 && ctx->tet_geometry) {
@@ -1737,19 +1772,8 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
                 // Warp chunks for the one-thread-per-tet kernel (Hex8 measured no gain: its
                 // issue-bound element kernel paid for the warp sums what its node kernel saved).
                 WarpChunks wc;
-                if (ctx->warp_chunks && E > 0 && d->kind == AM_TET4_GAUSS && b.geo64 && build_warp_chunks(conn, E, nn, wc)) {
-                    const int64_t C = static_cast<int64_t>(wc.ptr.size()) - 1;
-                    const int64_t G = static_cast<int64_t>(wc.nodes.size());
-                    const size_t words = wc.code.size();
-                    b.chunk_ptr = dalloc<int32_t>(C + 1, "chunk offsets");
-                    b.chunk_code = dalloc<uint32_t>(words, "chunk entry codes");
-                    b.chunk_rank = dalloc<uint32_t>(words, "chunk entry ranks");
-                    ck(cudaMemcpy(b.chunk_ptr, wc.ptr.data(), (C + 1) * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
-                    ck(cudaMemcpy(b.chunk_code, wc.code.data(), words * sizeof(uint32_t), cudaMemcpyHostToDevice), "upload");
-                    ck(cudaMemcpy(b.chunk_rank, wc.rank.data(), words * sizeof(uint32_t), cudaMemcpyHostToDevice), "upload");
-                    b.host_nodes = std::move(wc.nodes);
-                    b.slot_count = G;
-                }
+                if (ctx->warp_chunks && E > 0 && d->kind == AM_TET4_GAUSS && b.geo64 && build_warp_chunks(conn, E, nn, wc))
+                    upload_warp_chunks(b, wc, E);
             }
             if (ctx->num_slots + b.num_entries >= (int64_t(1) << 31)) fail(AM_ERANGE, "slot count beyond int32 indexing");
             if (d->mu_field && E > 0) {
@@ -1940,8 +1964,7 @@ int am_finalize(am_ctx* ctx) {
             b.slot_pos = ctx->slot_pos + b.slot_base;
             std::vector<int32_t>().swap(b.host_nodes);
             if (b.chunk_ptr) {
-                const int nn = b.kind == AM_HEX8_GAUSS ? 8 : 4;
-                b.chunk_pos = dalloc<int32_t>(static_cast<size_t>(32 * nn * ((b.num_elems + 31) / 32)), "chunk positions");
+                b.chunk_pos = dalloc<int32_t>(static_cast<size_t>(128 * ((b.chunk_units + 31) / 32)), "chunk positions");
                 am::launch_chunk_positions(b.gauss(), b.chunk_pos, ctx->stream);
                 ++ctx->launches;
                 ck(cudaGetLastError(), "chunk positions");

@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(256) k_chunk_positions(GaussBlockDev b, int32_
     constexpr int W = K / 4;
     const int64_t ch = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const int lane = static_cast<int>(threadIdx.x & 31);
-    if (32 * ch >= b.num_elems) return;  // the whole warp
+    if (32 * ch >= b.chunk_units) return;  // the whole warp
     const int64_t l = 32 * ch + lane;
     uint32_t rw[W];
 #pragma unroll
@@ -464,15 +464,15 @@ __global__ void __launch_bounds__(256, CHUNKS && sizeof(T) == 8 ? 3 : 0) k_tet4_
     }
 }
 
-// Chunked blocks outside the force (VJP, lumped mass): the per-element kernels write corner
-// values to scratch[NN e + a], and a warp per chunk sums them per distinct node with the
-// chunk's plan into the block's slots.
+// Chunked blocks outside the force (VJP, lumped mass): the per-element (per-patch) kernels
+// write corner values to scratch[NN u + a] (unit u, corner a), and a warp per chunk sums
+// them per distinct node with the chunk's plan into the block's slots.
 template <int NN>
 __global__ void __launch_bounds__(256) k_chunk_sum(GaussBlockDev b, const double4* __restrict__ scratch,
                                                     double4* __restrict__ slots) {
     const int64_t ch = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const int lane = static_cast<int>(threadIdx.x & 31);
-    if (32 * ch >= b.num_elems) return;  // the whole warp
+    if (32 * ch >= b.chunk_units) return;  // the whole warp
     const ChunkLane<NN> L = chunk_lane<NN>(b, ch, lane, true);
     chunk_reduce<double, NN>(L, lane, [&](int q, double(&v)[3]) {
         const double4 x = scratch[NN * (32 * ch + (q & 31)) + (q >> 5)];
@@ -585,7 +585,7 @@ template <typename T>
 constexpr int hex6_min_blocks() { return sizeof(T) == 4 ? 7 : 4; }
 constexpr int kHex6Block = 128;
 
-template <typename T, int MAT>
+template <typename T, int MAT, bool CHUNKS>
 __global__ void __launch_bounds__(kHex6Block, hex6_min_blocks<T>()) k_tet4_hex6_force(GaussBlockDev b, const double4* __restrict__ X4,
                                                           const double4* __restrict__ U4,
                                                           vec4_t<T>* __restrict__ slots, int* status) {
@@ -601,7 +601,15 @@ __global__ void __launch_bounds__(kHex6Block, hex6_min_blocks<T>()) k_tet4_hex6_
     // FP64 one).
     const int4* pn4 = reinterpret_cast<const int4*>(b.patch_nodes + pp * 8);
     const int4 lo = pn4[0], hi = pn4[1];  // patch-local nodes 0-3 and 4-7
-    asm volatile("prefetch.global.L2 [%0];" ::"l"(b.slot_pos + pp * 8));
+    if (CHUNKS) {
+        // the lane's chunk plan (warp chunks over the half patches gt)
+        const int64_t gu = gt < 2 * b.num_patches ? gt : 0;
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(b.chunk_code + gu));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(b.chunk_rank + gu));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(b.chunk_pos + 4 * gu));
+    } else {
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(b.slot_pos + pp * 8));
+    }
     const int32_t n0 = lo.x, n3 = lo.w;
     int32_t nr[4];
     nr[0] = r ? hi.y : lo.y;
@@ -675,17 +683,41 @@ __global__ void __launch_bounds__(kHex6Block, hex6_min_blocks<T>()) k_tet4_hex6_
         acc3[i] += __shfl_xor_sync(kFull, acc3[i], 1);
         accr[0][i] += __shfl_xor_sync(kFull, accr[3][i], 1);
     }
-    if (!valid) return;
-    // thread 0 writes nodes 1, 2, 4 and 0; thread 1 nodes 5, 6, 7 and 3
-    const int32_t* sp = b.slot_pos + p * 8;
-    int32_t pos = sp[r ? 5 : 1];
-    if (pos >= 0) slots[pos] = make4(accr[0][0], accr[0][1], accr[0][2]);
-    pos = sp[r ? 6 : 2];
-    if (pos >= 0) slots[pos] = make4(accr[1][0], accr[1][1], accr[1][2]);
-    pos = sp[r ? 7 : 4];
-    if (pos >= 0) slots[pos] = make4(accr[2][0], accr[2][1], accr[2][2]);
-    pos = sp[r ? 3 : 0];
-    if (pos >= 0) slots[pos] = r ? make4(acc3[0], acc3[1], acc3[2]) : make4(acc0[0], acc0[1], acc0[2]);
+    if constexpr (!CHUNKS) {
+        if (!valid) return;
+        // thread 0 writes nodes 1, 2, 4 and 0; thread 1 nodes 5, 6, 7 and 3
+        const int32_t* sp = b.slot_pos + p * 8;
+        int32_t pos = sp[r ? 5 : 1];
+        if (pos >= 0) slots[pos] = make4(accr[0][0], accr[0][1], accr[0][2]);
+        pos = sp[r ? 6 : 2];
+        if (pos >= 0) slots[pos] = make4(accr[1][0], accr[1][1], accr[1][2]);
+        pos = sp[r ? 7 : 4];
+        if (pos >= 0) slots[pos] = make4(accr[2][0], accr[2][1], accr[2][2]);
+        pos = sp[r ? 3 : 0];
+        if (pos >= 0) slots[pos] = r ? make4(acc3[0], acc3[1], acc3[2]) : make4(acc0[0], acc0[1], acc0[2]);
+    } else {
+        // the same four node sums as entries 32 a + lane (a: nodes 1, 2, 4, 0 or 5, 6, 7, 3),
+        // summed per distinct node over the warp's 16 patches
+        __shared__ T ent[kHex6Block / 32][3][128];
+        T(&st)[3][128] = ent[threadIdx.x >> 5];
+        const int lane = static_cast<int>(threadIdx.x & 31);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            st[i][lane] = accr[0][i];
+            st[i][32 + lane] = accr[1][i];
+            st[i][64 + lane] = accr[2][i];
+            st[i][96 + lane] = r ? acc3[i] : acc0[i];
+        }
+        __syncwarp();
+        const int64_t ch = gt >> 5;
+        if (32 * ch >= 2 * b.num_patches) return;  // the whole warp
+        const ChunkLane<4> L = chunk_lane<4>(b, ch, lane, true);
+        chunk_reduce<T, 4>(L, lane, [&](int q, T(&v)[3]) {
+            v[0] = st[0][q];
+            v[1] = st[1][q];
+            v[2] = st[2][q];
+        }, slots);
+    }
 }
 
 // Set-up for the split-hex kernels: X_a - X_0 in FP64 (and rounded to FP32) for
@@ -3148,10 +3180,17 @@ void launch_gauss_force(const GaussBlockDev& b, int mixed, const double4* X4, co
                         int* status, cudaStream_t s) {
     if (b.num_elems == 0) return;
     if (b.kind == AM_TET4_GAUSS && b.patched == 2 && b.patch_dx32 != nullptr && b.patch_dx64 != nullptr) {
-        if (mixed) {
-            AM_DISPATCH_MAT(b.material, (launch_pdl(k_tet4_hex6_force<float, M>, grid_for(2 * b.num_patches, kHex6Block), kHex6Block, s, b, X4, U4, static_cast<float4*>(slots), status)));
+        const unsigned grid = grid_for(2 * b.num_patches, kHex6Block);
+        if (b.chunk_ptr != nullptr) {
+            if (mixed) {
+                AM_DISPATCH_MAT(b.material, (launch_pdl(k_tet4_hex6_force<float, M, true>, grid, kHex6Block, s, b, X4, U4, static_cast<float4*>(slots), status)));
+            } else {
+                AM_DISPATCH_MAT(b.material, (launch_pdl(k_tet4_hex6_force<double, M, true>, grid, kHex6Block, s, b, X4, U4, static_cast<double4*>(slots), status)));
+            }
+        } else if (mixed) {
+            AM_DISPATCH_MAT(b.material, (launch_pdl(k_tet4_hex6_force<float, M, false>, grid, kHex6Block, s, b, X4, U4, static_cast<float4*>(slots), status)));
         } else {
-            AM_DISPATCH_MAT(b.material, (launch_pdl(k_tet4_hex6_force<double, M>, grid_for(2 * b.num_patches, kHex6Block), kHex6Block, s, b, X4, U4, static_cast<double4*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (launch_pdl(k_tet4_hex6_force<double, M, false>, grid, kHex6Block, s, b, X4, U4, static_cast<double4*>(slots), status)));
         }
     } else if (b.kind == AM_TET4_GAUSS && b.patched) {
         const unsigned grid = grid_for(b.num_patches, 8 * kPatchesPerWarp);
@@ -3419,13 +3458,13 @@ void launch_hex6_patch_dx(const int32_t* patch_nodes, int64_t num_patches, const
 }
 
 void launch_chunk_positions(const GaussBlockDev& b, int32_t* out, cudaStream_t s) {
-    if (b.num_elems == 0) return;
-    k_chunk_positions<4><<<grid_for(b.num_elems, 256), 256, 0, s>>>(b, out);
+    if (b.chunk_units == 0) return;
+    k_chunk_positions<4><<<grid_for(b.chunk_units, 256), 256, 0, s>>>(b, out);
 }
 
 void launch_chunk_sum(const GaussBlockDev& b, const double4* scratch, double4* slots, cudaStream_t s) {
-    if (b.num_elems == 0) return;
-    k_chunk_sum<4><<<grid_for(b.num_elems, 256), 256, 0, s>>>(b, scratch, slots);
+    if (b.chunk_units == 0) return;
+    k_chunk_sum<4><<<grid_for(b.chunk_units, 256), 256, 0, s>>>(b, scratch, slots);
 }
 
 void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const double4* X4, double4* slots,

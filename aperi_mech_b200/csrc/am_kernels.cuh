@@ -59,17 +59,18 @@ struct GaussBlockDev {
     // gathers. null where not built.
     const float* geo32;
     const double* geo64;
-    // Warp chunks (such Tet4 blocks and Hex8 blocks under the total formulation): the 32
-    // elements [32c, 32c + 32) of chunk c sum their forces on each node they share and write
-    // one slot per distinct node; the node of rank k (order of first appearance over the entry
-    // codes q = 32 a + lane, connectivity node a of the chunk's element lane) has logical slot
-    // chunk_ptr[c] + k. The chunk's 32 nn entries (nn nodes per element) sorted by (rank,
-    // code), nn to a lane: words (32 c + l) nn/4 .. (32 c + l + 1) nn/4 - 1 of chunk_code /
-    // chunk_rank hold lane l's, one byte each (rank 0xFF past the chunk's last element).
-    // null: one slot per element node.
+    // Warp chunks (such Tet4 blocks, and split-hex patches, whose thread r of patch p, unit
+    // 2p + r, writes patch nodes 1, 2, 4, 0 or 5, 6, 7, 3): the 32 units [32c, 32c + 32) of
+    // chunk c sum their four nodal forces on each node they share and write one slot per
+    // distinct node; the node of rank k (order of first appearance over the entry codes
+    // q = 32 a + lane, corner a of the chunk's unit lane) has logical slot chunk_ptr[c] + k.
+    // The chunk's 128 entries sorted by (rank, code), four to a lane: word 32 c + l of
+    // chunk_code / chunk_rank holds lane l's, one byte each (rank 0xFF past the last unit).
+    // null: one slot per element (or patch) node.
     const int32_t* chunk_ptr;
     const uint32_t* chunk_code;
     const uint32_t* chunk_rank;
+    int64_t chunk_units;  // the units chunked: tets, or split-hex half patches (two per patch)
     // nn per lane (the lane's word order): the slot position of each entry that ends its
     // node's run, else -1; resolved at am_finalize
     const int32_t* chunk_pos;

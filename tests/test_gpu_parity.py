@@ -480,19 +480,20 @@ def test_tet4_geometry_table(gpu, oracle_lib, monkeypatch, material):
     assert rel_err(out["1"][0], out["0"][0]) < 1e-13
 
 
+@pytest.mark.parametrize("path", ["per_tet", "split_hex"])
 @pytest.mark.parametrize("material", ["neo_hookean", "elastic", "linear_elastic"])
-def test_warp_chunks(gpu, oracle_lib, monkeypatch, material):
-    """One thread per tet with each warp's 32 tets summing their forces on shared nodes
-    before writing one slot per distinct node (the default) and with four slots per tet
-    (APERI_B200_WARP_CHUNKS=0): FP64 and mixed forces, the lumped mass, the VJP with
-    modulus fields and 30 steps against the oracle, on 750 tets (a partial last chunk); the
-    chunked layout writes fewer slots and repeats bit for bit."""
+def test_warp_chunks(gpu, oracle_lib, monkeypatch, material, path):
+    """Warp chunks, where each warp sums its nodal forces on shared nodes before writing one
+    slot per distinct node (the default), against one slot per tet or patch node
+    (APERI_B200_WARP_CHUNKS=0), on one thread per tet (32 tets a warp) and on the split-hex
+    patches (16 patches a warp): FP64 and mixed forces, the lumped mass, the VJP with
+    modulus fields and 30 steps against the oracle, on 750 tets (125 patches: partial last
+    chunks); the chunked layout writes fewer slots and repeats bit for bit."""
     from aperi_mech_b200.model import ExplicitDynamics, Part
 
-    monkeypatch.setenv("APERI_B200_TET4_PATCHES", "0")
+    monkeypatch.setenv("APERI_B200_TET4_PATCHES", "0" if path == "per_tet" else "2")
     coords, conn = _mesh("tet4", 5, seed=13)
-    nn = conn.shape[1]
-    assert conn.shape[0] % 32 != 0
+    assert conn.shape[0] % 32 != 0 and (conn.shape[0] // 3) % 32 != 0
     mu_f, k_f = _fields(conn.shape[0], 8, True)
     parts = [Part("tet4", _material(material), conn=conn, mu_field=mu_f, kappa_field=k_f)]
     rng = np.random.default_rng(5)
@@ -508,6 +509,7 @@ def test_warp_chunks(gpu, oracle_lib, monkeypatch, material):
         monkeypatch.setenv("APERI_B200_WARP_CHUNKS", chunks)
         with ExplicitDynamics(coords, parts) as m:
             slots[chunks] = m.layout()["used_slots"]
+            assert m.layout()["patched_tet4_blocks"] == (path == "split_hex")
             f = m.internal_force(u)
             assert rel_err(f, want_f) < FP64_TOL
             assert np.array_equal(f, m.internal_force(u))
@@ -520,7 +522,8 @@ def test_warp_chunks(gpu, oracle_lib, monkeypatch, material):
             m.run(30, 1e-7)
             for g, w in zip(m.get_state(), want_s):
                 assert rel_err(g, w) < 1e-12
-    assert slots["0"] == nn * conn.shape[0] and slots["1"] < slots["0"] // 2
+    per_node = 4 if path == "per_tet" else 8 / 6
+    assert slots["0"] == per_node * conn.shape[0] and slots["1"] < slots["0"] // 2
 
 
 # ---- Tet4 element patches ----------------------------------------------------------------

@@ -51,15 +51,19 @@ def test_renumbered_mesh_is_bitwise_identical(gpu, kind, prec):
         assert np.array_equal(a, b[pn])
 
 
-def test_renumbered_tet4_runs_split_hex_patches(gpu):
-    """The rings of the six-tet split are found in the renumbered mesh too."""
+def test_renumbered_tet4_runs_split_hex_patches(gpu, monkeypatch):
+    """The rings of the six-tet split are found in the renumbered mesh too: one slot per
+    patch node (8 per 6 tets) without warp chunks, fewer with them (the default)."""
     from aperi_mech_b200 import problems
 
     p = _problem("tet4")
     q, _, _ = problems.renumbered(p, seed=3)
+    _, _, chunked = _run(q, "fp64", np.zeros_like(q.coords))
+    monkeypatch.setenv("APERI_B200_WARP_CHUNKS", "0")
     _, _, layout = _run(q, "fp64", np.zeros_like(q.coords))
-    assert layout["patched_tet4_blocks"] == 1
+    assert layout["patched_tet4_blocks"] == 1 and chunked["patched_tet4_blocks"] == 1
     assert layout["used_slots"] == 8 * q.num_elems // 6
+    assert chunked["used_slots"] < layout["used_slots"] // 2
 
 
 def test_renumbered_vjp_and_adjoint_map_back(gpu):
