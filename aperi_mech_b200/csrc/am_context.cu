@@ -305,9 +305,9 @@ struct Block {
     }
     // A chunked block's per-corner view for the kernels that write one value per element (or
     // patch) node: positions into the scratch array (allocated on first use) at 4 u + a, unit
-    // u and corner a. Per tet the identity; a split-hex patch p's node k is corner a of half
-    // patch 2p + r (thread r writes nodes 1, 2, 4, 0 or 5, 6, 7, 3).
-    am::GaussBlockDev gauss_corners() {
+    // u and corner a. Per tet the identity; a split-hex patch p's node k (tets or cells) is
+    // corner a of half patch 2p + r (thread r writes nodes 1, 2, 4, 0 or 5, 6, 7, 3).
+    void ensure_corners() {
         const size_t n = static_cast<size_t>(4 * std::max<int64_t>(chunk_units, 1));
         if (!chunk_ident) {
             std::vector<int32_t> id(n);
@@ -322,6 +322,9 @@ struct Block {
             ck(cudaMemcpy(chunk_ident, id.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
         }
         if (!chunk_scratch) chunk_scratch = dalloc<double4>(n, "chunk corner values");
+    }
+    am::GaussBlockDev gauss_corners() {
+        ensure_corners();
         am::GaussBlockDev g = gauss();
         g.slot_pos = chunk_ident;
         return g;
@@ -366,6 +369,11 @@ struct Block {
         c.cmat = cmat64;
         c.unroll[0] = unroll[0][0];
         c.unroll[1] = unroll[0][1];
+        c.chunk_ptr = chunk_ptr;
+        c.chunk_code = chunk_code;
+        c.chunk_rank = chunk_rank;
+        c.chunk_pos = chunk_pos;
+        c.chunk_units = chunk_units;
         return c;
     }
     // The device view for a force evaluation at the given precision (F-bar scratch attached).
@@ -1061,7 +1069,14 @@ struct am_ctx {
         for (const auto& b : blocks) {
             double* gm = gmu ? gmu + off : nullptr;
             double* gk = gkappa ? gkappa + off : nullptr;
-            if (b.kind == AM_SMOOTHED_CELLS) {
+            if (b.kind == AM_SMOOTHED_CELLS && b.chunk_ptr) {
+                // per-corner values, then the chunk sums (scratch allocated by prepare_vjp)
+                am::CellBlockDev c = b.cells();
+                c.slot_pos = b.chunk_ident;
+                launches += am::launch_cell_vjp(c, U, L, b.vjp_lmat, b.chunk_scratch, gm, gk, accumulate, stream);
+                am::launch_chunk_sum(b.cells(), b.chunk_scratch, slots64, stream);
+                ++launches;
+            } else if (b.kind == AM_SMOOTHED_CELLS) {
                 launches += am::launch_cell_vjp(b.cells(), U, L, b.vjp_lmat, slots64, gm, gk, accumulate, stream);
             } else if (b.chunk_ptr) {
                 // per-corner values, then the chunk sums (scratch allocated by prepare_vjp)
@@ -1091,7 +1106,7 @@ struct am_ctx {
     // most 32 subcells), which keeps L_s per subcell beside H_s.
     void prepare_vjp(const char* what) {
         for (auto& b : blocks) {
-            if (b.chunk_ptr) (void)b.gauss_corners();
+            if (b.chunk_ptr) b.ensure_corners();
             if (!b.group_ptr) continue;
             if (!b.gather) fail(AM_ESTATE, std::string(what) + " on F-bar cells needs the cell-stress form (cells of at most 32 subcells)");
             if (!b.vjp_lmat) b.vjp_lmat = dalloc<double>(std::max<int64_t>(9 * b.num_elems, 1), "F-bar VJP scratch");
@@ -1686,6 +1701,16 @@ int am_add_block(am_ctx* ctx, const am_block_desc* d, int32_t* block_id) {
                         ck(cudaMemcpy(b.patch_first, tp.first.data(), (P + 1) * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
                         ck(cudaMemcpy(b.patch_nodes, tp.nodes.data(), 8 * P * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
                         b.host_nodes.assign(tp.nodes.begin(), tp.nodes.begin() + 8 * P);
+                        if (ctx->warp_chunks && ctx->lagr == 0) {
+                            // warp chunks over the half patches, as for the split-hex tets
+                            constexpr int kNode[2][4] = {{1, 2, 4, 0}, {5, 6, 7, 3}};
+                            std::vector<int32_t> half(8 * P);
+                            for (int64_t q = 0; q < P; ++q)
+                                for (int r = 0; r < 2; ++r)
+                                    for (int a = 0; a < 4; ++a) half[4 * (2 * q + r) + a] = tp.nodes[8 * q + kNode[r][a]];
+                            WarpChunks wc;
+                            if (build_warp_chunks(half.data(), 2 * P, 4, wc)) upload_warp_chunks(b, wc, 2 * P);
+                        }
                     }
                 }
             } else {
@@ -1965,7 +1990,10 @@ int am_finalize(am_ctx* ctx) {
             std::vector<int32_t>().swap(b.host_nodes);
             if (b.chunk_ptr) {
                 b.chunk_pos = dalloc<int32_t>(static_cast<size_t>(128 * ((b.chunk_units + 31) / 32)), "chunk positions");
-                am::launch_chunk_positions(b.gauss(), b.chunk_pos, ctx->stream);
+                if (b.kind == AM_SMOOTHED_CELLS)
+                    am::launch_chunk_positions(b.cells(), b.chunk_pos, ctx->stream);
+                else
+                    am::launch_chunk_positions(b.gauss(), b.chunk_pos, ctx->stream);
                 ++ctx->launches;
                 ck(cudaGetLastError(), "chunk positions");
             }

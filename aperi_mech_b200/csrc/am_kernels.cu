@@ -254,8 +254,8 @@ __device__ __forceinline__ int chunk_byte(const uint32_t* w, int j) {
 }
 // The lane's plan: its words and its run-end slot positions (resolved once by
 // k_chunk_positions), independent loads.
-template <int K>
-__device__ __forceinline__ ChunkLane<K> chunk_lane(const GaussBlockDev& b, int64_t ch, int lane, bool live) {
+template <int K, typename B>
+__device__ __forceinline__ ChunkLane<K> chunk_lane(const B& b, int64_t ch, int lane, bool live) {
     constexpr int W = K / 4;
     ChunkLane<K> L;
 #pragma unroll
@@ -277,8 +277,8 @@ __device__ __forceinline__ ChunkLane<K> chunk_lane(const GaussBlockDev& b, int64
 
 // Set-up, a warp per chunk: the slot position of each lane entry that ends its node's run
 // (the next sorted entry, in this lane or the next, has another rank), else -1.
-template <int K>
-__global__ void __launch_bounds__(256) k_chunk_positions(GaussBlockDev b, int32_t* __restrict__ out) {
+template <int K, typename B>
+__global__ void __launch_bounds__(256) k_chunk_positions(B b, int32_t* __restrict__ out) {
     constexpr int W = K / 4;
     const int64_t ch = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const int lane = static_cast<int>(threadIdx.x & 31);
@@ -467,8 +467,8 @@ __global__ void __launch_bounds__(256, CHUNKS && sizeof(T) == 8 ? 3 : 0) k_tet4_
 // Chunked blocks outside the force (VJP, lumped mass): the per-element (per-patch) kernels
 // write corner values to scratch[NN u + a] (unit u, corner a), and a warp per chunk sums
 // them per distinct node with the chunk's plan into the block's slots.
-template <int NN>
-__global__ void __launch_bounds__(256) k_chunk_sum(GaussBlockDev b, const double4* __restrict__ scratch,
+template <int NN, typename B>
+__global__ void __launch_bounds__(256) k_chunk_sum(B b, const double4* __restrict__ scratch,
                                                     double4* __restrict__ slots) {
     const int64_t ch = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const int lane = static_cast<int>(threadIdx.x & 31);
@@ -1549,7 +1549,7 @@ __device__ __forceinline__ void load_cell12<double>(const double* p, double* g) 
     }
 }
 
-template <typename T, int MAT>
+template <typename T, int MAT, bool CHUNKS>
 __global__ void __launch_bounds__(kHex6Block, hex6_min_blocks<T>()) k_cell_hex6_force(CellBlockDev b, const double4* U4,
                                                                                     vec4_t<T>* slots, int* status) {
     const int64_t gt = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -1559,7 +1559,15 @@ __global__ void __launch_bounds__(kHex6Block, hex6_min_blocks<T>()) k_cell_hex6_
     const int64_t pp = valid ? p : 0;
     const int4* pn4 = reinterpret_cast<const int4*>(b.patch_nodes + pp * 8);
     const int4 lo = pn4[0], hi = pn4[1];
-    asm volatile("prefetch.global.L2 [%0];" ::"l"(b.slot_pos + pp * 8));
+    if (CHUNKS) {
+        // the lane's chunk plan (warp chunks over the half patches gt)
+        const int64_t gu = gt < 2 * b.num_patches ? gt : 0;
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(b.chunk_code + gu));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(b.chunk_rank + gu));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(b.chunk_pos + 4 * gu));
+    } else {
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(b.slot_pos + pp * 8));
+    }
     const int32_t n0 = lo.x, n3 = lo.w;
     int32_t nr[4];
     nr[0] = r ? hi.y : lo.y;
@@ -1624,16 +1632,39 @@ __global__ void __launch_bounds__(kHex6Block, hex6_min_blocks<T>()) k_cell_hex6_
         acc3[i] += __shfl_xor_sync(kFull, acc3[i], 1);
         accr[0][i] += __shfl_xor_sync(kFull, accr[3][i], 1);
     }
-    if (!valid) return;
-    const int32_t* sp = b.slot_pos + p * 8;
-    int32_t pos = sp[r ? 5 : 1];
-    if (pos >= 0) slots[pos] = make4(accr[0][0], accr[0][1], accr[0][2]);
-    pos = sp[r ? 6 : 2];
-    if (pos >= 0) slots[pos] = make4(accr[1][0], accr[1][1], accr[1][2]);
-    pos = sp[r ? 7 : 4];
-    if (pos >= 0) slots[pos] = make4(accr[2][0], accr[2][1], accr[2][2]);
-    pos = sp[r ? 3 : 0];
-    if (pos >= 0) slots[pos] = r ? make4(acc3[0], acc3[1], acc3[2]) : make4(acc0[0], acc0[1], acc0[2]);
+    if constexpr (!CHUNKS) {
+        if (!valid) return;
+        const int32_t* sp = b.slot_pos + p * 8;
+        int32_t pos = sp[r ? 5 : 1];
+        if (pos >= 0) slots[pos] = make4(accr[0][0], accr[0][1], accr[0][2]);
+        pos = sp[r ? 6 : 2];
+        if (pos >= 0) slots[pos] = make4(accr[1][0], accr[1][1], accr[1][2]);
+        pos = sp[r ? 7 : 4];
+        if (pos >= 0) slots[pos] = make4(accr[2][0], accr[2][1], accr[2][2]);
+        pos = sp[r ? 3 : 0];
+        if (pos >= 0) slots[pos] = r ? make4(acc3[0], acc3[1], acc3[2]) : make4(acc0[0], acc0[1], acc0[2]);
+    } else {
+        // as in k_tet4_hex6_force: the four node sums summed per distinct node over the warp
+        __shared__ T ent[kHex6Block / 32][3][128];
+        T(&st)[3][128] = ent[threadIdx.x >> 5];
+        const int lane = static_cast<int>(threadIdx.x & 31);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            st[i][lane] = accr[0][i];
+            st[i][32 + lane] = accr[1][i];
+            st[i][64 + lane] = accr[2][i];
+            st[i][96 + lane] = r ? acc3[i] : acc0[i];
+        }
+        __syncwarp();
+        const int64_t ch = gt >> 5;
+        if (32 * ch >= 2 * b.num_patches) return;  // the whole warp
+        const ChunkLane<4> L = chunk_lane<4>(b, ch, lane, true);
+        chunk_reduce<T, 4>(L, lane, [&](int q, T(&v)[3]) {
+            v[0] = st[0][q];
+            v[1] = st[1][q];
+            v[2] = st[2][q];
+        }, slots);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -3321,10 +3352,16 @@ int launch_cell_force(const CellBlockDev& b, int mixed, const double4* U4, void*
     }
     if (b.patched == 2) {
         const unsigned grid = grid_for(2 * b.num_patches, kHex6Block);
-        if (mixed) {
-            AM_DISPATCH_MAT(b.material, (launch_pdl(k_cell_hex6_force<float, M>, grid, kHex6Block, s, b, U4, static_cast<float4*>(slots), status)));
+        if (b.chunk_ptr != nullptr) {
+            if (mixed) {
+                AM_DISPATCH_MAT(b.material, (launch_pdl(k_cell_hex6_force<float, M, true>, grid, kHex6Block, s, b, U4, static_cast<float4*>(slots), status)));
+            } else {
+                AM_DISPATCH_MAT(b.material, (launch_pdl(k_cell_hex6_force<double, M, true>, grid, kHex6Block, s, b, U4, static_cast<double4*>(slots), status)));
+            }
+        } else if (mixed) {
+            AM_DISPATCH_MAT(b.material, (launch_pdl(k_cell_hex6_force<float, M, false>, grid, kHex6Block, s, b, U4, static_cast<float4*>(slots), status)));
         } else {
-            AM_DISPATCH_MAT(b.material, (launch_pdl(k_cell_hex6_force<double, M>, grid, kHex6Block, s, b, U4, static_cast<double4*>(slots), status)));
+            AM_DISPATCH_MAT(b.material, (launch_pdl(k_cell_hex6_force<double, M, false>, grid, kHex6Block, s, b, U4, static_cast<double4*>(slots), status)));
         }
         return 1;
     }
@@ -3459,12 +3496,20 @@ void launch_hex6_patch_dx(const int32_t* patch_nodes, int64_t num_patches, const
 
 void launch_chunk_positions(const GaussBlockDev& b, int32_t* out, cudaStream_t s) {
     if (b.chunk_units == 0) return;
-    k_chunk_positions<4><<<grid_for(b.chunk_units, 256), 256, 0, s>>>(b, out);
+    k_chunk_positions<4, GaussBlockDev><<<grid_for(b.chunk_units, 256), 256, 0, s>>>(b, out);
+}
+void launch_chunk_positions(const CellBlockDev& b, int32_t* out, cudaStream_t s) {
+    if (b.chunk_units == 0) return;
+    k_chunk_positions<4, CellBlockDev><<<grid_for(b.chunk_units, 256), 256, 0, s>>>(b, out);
 }
 
 void launch_chunk_sum(const GaussBlockDev& b, const double4* scratch, double4* slots, cudaStream_t s) {
     if (b.chunk_units == 0) return;
-    k_chunk_sum<4><<<grid_for(b.chunk_units, 256), 256, 0, s>>>(b, scratch, slots);
+    k_chunk_sum<4, GaussBlockDev><<<grid_for(b.chunk_units, 256), 256, 0, s>>>(b, scratch, slots);
+}
+void launch_chunk_sum(const CellBlockDev& b, const double4* scratch, double4* slots, cudaStream_t s) {
+    if (b.chunk_units == 0) return;
+    k_chunk_sum<4, CellBlockDev><<<grid_for(b.chunk_units, 256), 256, 0, s>>>(b, scratch, slots);
 }
 
 void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const double4* X4, double4* slots,

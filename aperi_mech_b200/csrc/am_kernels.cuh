@@ -130,6 +130,13 @@ struct CellBlockDev {
     void* cmat;
     int32_t group_items[2];  // items per warp (8, or 1 for items of many entries): cell side, node side
     int32_t unroll[2];  // rows per lane in flight (1, 2 or 4): cell kernel, gather kernel
+    // Warp chunks of cells grouped as split hexes (patched == 2), as GaussBlockDev's for
+    // split-hex tet patches: units are half patches. null: one slot per patch node.
+    const int32_t* chunk_ptr;
+    const uint32_t* chunk_code;
+    const uint32_t* chunk_rank;
+    const int32_t* chunk_pos;
+    int64_t chunk_units;
 };
 constexpr int kFbarStride = 20;
 
@@ -182,8 +189,10 @@ void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const dou
                                cudaStream_t s);
 // Chunked blocks: per-corner values (scratch[nn e + a]) summed into the block's slots.
 void launch_chunk_sum(const GaussBlockDev& b, const double4* scratch, double4* slots, cudaStream_t s);
+void launch_chunk_sum(const CellBlockDev& b, const double4* scratch, double4* slots, cudaStream_t s);
 // Chunked blocks: the run-end slot positions of every lane (at am_finalize, after the layout).
 void launch_chunk_positions(const GaussBlockDev& b, int32_t* out, cudaStream_t s);
+void launch_chunk_positions(const CellBlockDev& b, int32_t* out, cudaStream_t s);
 
 // f (N x 3, row-major) = gather of the slots (FP64 or FP32 slots), overwrite or accumulate.
 void launch_gather_force(const NodeDev& nd, int mixed, const void* slots, double* f, int accumulate, cudaStream_t s);

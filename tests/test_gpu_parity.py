@@ -168,8 +168,9 @@ def test_smoothed_cells_parity(gpu, oracle_lib):
 @pytest.mark.parametrize("material", ["neo_hookean", "elastic", "linear_elastic"])
 def test_element_cells_grouped_as_split_hexes(gpu, oracle_lib, monkeypatch, material):
     """Element smoothing cells of a split-hex tet mesh run as patches (one slot per patch
-    node, a third of the slots): the force (FP64 and mixed), the VJP and 30 steps with
-    per-cell moduli against the oracle, grouped and with patching off."""
+    node, a third of the slots; with warp chunks, the default, one per distinct node of a
+    warp's 16 patches): the force (FP64 and mixed), the VJP and 30 steps with per-cell
+    moduli against the oracle, grouped with and without chunks and with patching off."""
     from aperi_mech_b200 import mesh
     from aperi_mech_b200.model import BoundaryCondition, ExplicitDynamics
     from aperi_mech_b200.smoothing import element_smoothing_part
@@ -191,10 +192,12 @@ def test_element_cells_grouped_as_split_hexes(gpu, oracle_lib, monkeypatch, mate
     zero = np.zeros_like(coords)
     want_s = op.steps(zero, v0, op.init_acceleration(zero), np.full(30, dt))
     slots = {}
-    for patches in ("2", "0"):  # split-hex grouping (the default), and no grouping
+    # split-hex grouping with warp chunks (the default), without them, and no grouping
+    for patches, chunks in (("2", "1"), ("2", "0"), ("0", "1")):
         monkeypatch.setenv("APERI_B200_TET4_PATCHES", patches)
+        monkeypatch.setenv("APERI_B200_WARP_CHUNKS", chunks)
         with ExplicitDynamics(coords, [part], bcs, mass=mass) as m:
-            slots[patches] = m.layout()["used_slots"]
+            slots[patches + chunks] = m.layout()["used_slots"]
             assert rel_err(m.internal_force(u), want_f) < FP64_TOL
             assert rel_err(m.internal_force(u, "mixed"), want_f) < MIXED_FORCE_TOL
             for g, w in zip(m.vjp_force(u, lam), want_v):
@@ -204,7 +207,8 @@ def test_element_cells_grouped_as_split_hexes(gpu, oracle_lib, monkeypatch, mate
             m.run(30, dt)
             for g, w in zip(m.get_state(), want_s):
                 assert rel_err(g, w) < FP64_TOL
-    assert 3 * slots["2"] == slots["0"] == 4 * conn.shape[0]
+    assert 3 * slots["20"] == slots["01"] == 4 * conn.shape[0]
+    assert slots["21"] < slots["20"] // 2
 
 
 # ---- time integration ----------------------------------------------------------------
