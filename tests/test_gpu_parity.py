@@ -530,6 +530,39 @@ def test_warp_chunks(gpu, oracle_lib, monkeypatch, material, path):
     assert slots["0"] == per_node * conn.shape[0] and slots["1"] < slots["0"] // 2
 
 
+def test_warp_chunks_fan_mesh(gpu, oracle_lib, monkeypatch):
+    """Every tet shares node 0 (a fan of 100 tets about it, with neighbouring tets sharing two
+    more nodes), so in each warp chunk node 0's run holds 32 entries over eight lanes and is
+    summed by the scan across lanes: FP64 force, lumped mass and VJP against the oracle, with
+    and without warp chunks."""
+    from aperi_mech_b200.model import ExplicitDynamics, Part
+
+    monkeypatch.setenv("APERI_B200_TET4_PATCHES", "0")
+    rng = np.random.default_rng(21)
+    n = 102
+    t = np.linspace(0.0, 6.0 * np.pi, n)
+    ring = np.stack([np.cos(t), np.sin(t), 0.3 * t / np.pi + 0.2 * rng.standard_normal(n)], axis=1)
+    coords = np.vstack([np.zeros((1, 3)), ring + 0.05 * rng.standard_normal(ring.shape)])
+    conn = np.array([[0, i, i + 1, i + 2] for i in range(1, n - 1)], dtype=np.int32)
+    x = coords[conn]
+    det = np.einsum("ij,ij->i", np.cross(x[:, 1] - x[:, 0], x[:, 2] - x[:, 0]), x[:, 3] - x[:, 0])
+    conn[det < 0, 1], conn[det < 0, 2] = conn[det < 0, 2], conn[det < 0, 1].copy()
+    parts = [Part("tet4", _material("neo_hookean"), conn=conn)]
+    u = 1e-3 * rng.standard_normal(coords.shape)
+    lam = rng.standard_normal(coords.shape)
+    op = oracle_lib.OracleProblem(coords, parts)
+    want_f, want_v = op.internal_force(u), op.vjp_force(u, lam)
+    for chunks in ("1", "0"):
+        monkeypatch.setenv("APERI_B200_WARP_CHUNKS", chunks)
+        with ExplicitDynamics(coords, parts) as m:
+            # FP64 only: the spiral's sliver tets would test the mixed path's conditioning, not
+            # the chunk sums (the same code in both precisions, checked by test_warp_chunks)
+            assert rel_err(m.internal_force(u), want_f) < FP64_TOL
+            assert rel_err(m.mass(), op.lumped_mass()) < 1e-14
+            for g, w in zip(m.vjp_force(u, lam), want_v):
+                assert rel_err(g, w) < 1e-11
+
+
 # ---- Tet4 element patches ----------------------------------------------------------------
 @pytest.mark.parametrize("layout", ["unpatched", "irregular_patches", "shuffled"])
 def test_tet4_patch_layouts(gpu, oracle_lib, monkeypatch, layout):
