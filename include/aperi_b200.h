@@ -298,8 +298,10 @@ int am_element_order(int64_t num_nodes, const double* coords, int64_t num_elems,
 /* ---- diagnostics ---- */
 const char* am_last_error(const am_ctx* ctx);
 const char* am_status_string(int status);
-/* Force-slot layout after am_finalize: node-major slots referenced by nodes, and the
- * number of Tet4 blocks assembled through element patches. */
+/* Force-slot layout after am_finalize: node-major slots referenced by nodes (one per
+ * element node, patch node, cell entry or, for blocks run in warp chunks, distinct node of
+ * a chunk; APERI_B200_WARP_CHUNKS=0 turns the chunks off), and the number of Tet4 blocks
+ * assembled through element patches. */
 int am_get_layout(const am_ctx* ctx, int64_t* used_slots, int32_t* patched_tet4_blocks);
 /* Kernel launches issued by this context so far (all kinds). */
 int64_t am_launch_count(const am_ctx* ctx);
