@@ -3527,16 +3527,21 @@ void launch_gauss_volume_slots(const GaussBlockDev& b, double density, const dou
 // in L2 (126 MB on B200), else 4: on B200 the eight-deep batch was ~10% faster for
 // the 70^3 Tet4 mesh's 44 MB of FP32 slots and ~5-10% slower for the 128^3 Hex8
 // mesh's 268 MB.
-// Lanes per node. Meshes of Gauss elements (at most a dozen slots per node) take two lanes
-// (each reads every other slot of the node's contiguous range, so a warp's loads cover
-// whole lines, and a butterfly adds the halves) for FP64 slots, and for FP32 slots when
-// the slot array sits in L2; FP32 slots streaming from HBM keep one lane per node. On
-// B200: 70^3 Tet4 node kernel 23.1 -> 21.3 us mixed and 32.0 -> 28.8 us FP64, 128^3
-// Hex8 153.9 -> 133.8 us FP64, but 95.2 -> 103.5 us mixed. Cell meshes with tens of
-// slots per node take four or eight lanes.
+// Lanes per node. Up to six slots per node (the warp-chunked tet meshes: 3.4 per node on
+// the split-hex 70^3 mesh, 5.7 with one thread per tet; one per node and block for cells in
+// the cell-stress form) take one lane: on B200 the 70^3 split-hex node kernel ran 14.6
+// against 18.9 us (mixed) and 19.4 against 21.0 us (FP64) with two. Meshes of Gauss
+// elements with up to a dozen slots per node take two lanes (each reads every other slot
+// of the node's contiguous range, so a warp's loads cover whole lines, and a butterfly adds
+// the halves) for FP64 slots, and for FP32 slots when the slot array sits in L2; FP32 slots
+// streaming from HBM keep one lane per node. On B200, before the warp chunks: 70^3 Tet4 node
+// kernel 23.1 -> 21.3 us mixed and 32.0 -> 28.8 us FP64, 128^3 Hex8 153.9 -> 133.8 us
+// FP64, but 95.2 -> 103.5 us mixed. Cell meshes with tens of slots per node take four or
+// eight lanes.
 inline int node_lanes(const NodeDev& nd, int mixed) {
     if (nd.lanes == 1 || nd.lanes == 2 || nd.lanes == 4 || nd.lanes == 8) return nd.lanes;
     const double per_node = static_cast<double>(nd.num_slots) / static_cast<double>(nd.num_nodes);
+    if (per_node <= 6.0) return 1;
     if (per_node <= 12.0) return (!mixed || nd.num_slots * 16 <= (int64_t{64} << 20)) ? 2 : 1;
     // one thread per tet on a tet mesh (about 23 slots per node): 2 lanes ran the node
     // kernel in 40.9 us against 49.8 (1), 47.6 (4) and 60.2 (8) on the renumbered 70^3 mesh
