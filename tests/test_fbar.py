@@ -366,3 +366,20 @@ def test_fbar_vjp_refused_outside_the_cell_stress_form(gpu, oracle_lib, monkeypa
         assert e.value.code == AM_ESTATE
         want = oracle_lib.OracleProblem(X, [cells.part], mass=cells.mass).internal_force(u)
         assert rel_err(m.internal_force(u), want) < 1e-12
+
+
+@pytest.mark.parametrize("kind", ["neo_hookean", "elastic"])
+def test_oracle_fbar_vjp_is_symmetric(oracle_lib, kind):
+    """The F-bar force is the gradient of sum_s V_s psi(Fbar_s), so its Jacobian is
+    symmetric: mu . VJP(u, lam) equals lam . VJP(u, mu) for any two directions."""
+    n = 3
+    X, T = _box(n, seed=16)
+    mat = _material(kind)
+    fb, _, _ = _oracle_parts(oracle_lib, X, T, mat, n)
+    rng = np.random.default_rng(17)
+    u = 1e-2 * rng.standard_normal(X.shape)
+    lam, mu = rng.standard_normal(X.shape), rng.standard_normal(X.shape)
+    op = oracle_lib.OracleProblem(X, [fb])
+    a = np.sum(mu * op.vjp_force(u, lam)[0])
+    b = np.sum(lam * op.vjp_force(u, mu)[0])
+    assert abs(a - b) < 1e-12 * max(abs(a), abs(b))
