@@ -20,7 +20,7 @@ LIB = LIBDIR / "libaperi_b200.so"
 SOURCES = [CSRC / "am_kernels.cu", CSRC / "am_context.cu", CSRC / "am_noalloc.cu", CSRC / "am_rkpm.cu",
            CSRC / "am_diag.cu"]
 HEADERS = [CSRC / "am_kernels.cuh", CSRC / "am_math.cuh", CSRC / "am_host.hpp", CSRC / "am_order.hpp",
-           ROOT / "include" / "aperi_b200.h"]
+           CSRC / "am_chunks.hpp", ROOT / "include" / "aperi_b200.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -6,7 +6,9 @@ their node in code order and sorted by (rank, code), four to a lane. The reducti
 lane sums the runs among its four entries, an inclusive segmented scan over the lanes
 carries a run across lane boundaries, and the lane holding a node's last entry writes it.
 Every distinct node of the chunk must be written exactly once with the sum of its entries,
-including nodes that repeat within a unit, runs that span many lanes and partial chunks."""
+including nodes that repeat within a unit, runs that span many lanes and partial chunks. The
+library's own C++ plan builder (am_chunks.hpp, compiled here with g++) must produce the
+restated plan byte for byte."""
 from __future__ import annotations
 
 import numpy as np
@@ -115,3 +117,71 @@ def test_warp_chunk_sums_match_direct_sums(case):
                 mask = conn[32 * c:32 * c + n] == node
                 want = vals[32 * c:32 * c + n][mask].sum(axis=0)
                 assert np.allclose(got[k], want, rtol=1e-13, atol=1e-13)
+
+
+def _build_dump(tmp_path):
+    import subprocess
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parent.parent
+    exe = tmp_path / "chunk_plan_dump"
+    res = subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-Werror",
+                          f"-I{root / 'aperi_mech_b200' / 'csrc'}", str(root / "tests" / "cxx" / "chunk_plan_dump.cpp"),
+                          "-o", str(exe)], capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr
+    return exe
+
+
+def _library_plan(exe, tmp_path, conn):
+    import subprocess
+
+    src, dst = tmp_path / "conn.bin", tmp_path / "plan.bin"
+    with open(src, "wb") as f:
+        np.array(conn.shape, dtype="<i8").tofile(f)
+        np.ascontiguousarray(conn, dtype="<i4").tofile(f)
+    assert subprocess.run([str(exe), str(src), str(dst)]).returncode == 0
+    raw = open(dst, "rb").read()
+    ok, C, G = np.frombuffer(raw[:24], dtype="<i8")
+    words = 32 * C * conn.shape[1] // 4
+    rest = np.frombuffer(raw[24:], dtype="<i4")
+    ptr, nodes = rest[:C + 1], rest[C + 1:C + 1 + G]
+    code = np.frombuffer(raw[24 + 4 * (C + 1 + G):], dtype="<u4")[:words]
+    rank = np.frombuffer(raw[24 + 4 * (C + 1 + G + words):], dtype="<u4")[:words]
+    return bool(ok), ptr, nodes, code, rank
+
+
+def _bytes(words):
+    return np.stack([(words >> (8 * k)) & 0xFF for k in range(4)], axis=-1).reshape(-1)
+
+
+def test_library_plan_builder_matches_restatement(tmp_path):
+    """The C++ builder the library runs at set-up (am_chunks.hpp) gives, chunk by chunk, the
+    distinct nodes, the sorted entry codes and the node ranks of the restatement above."""
+    exe = _build_dump(tmp_path)
+    rng = np.random.default_rng(7)
+    for case in CASES:
+        E = int(rng.integers(1, 200))
+        conn = {"few_nodes": rng.integers(0, 4, size=(E, 4)),
+                "fan": np.column_stack([np.zeros(E, int), rng.integers(1, 200, size=(E, 3))])}.get(
+            case, rng.integers(0, 500, size=(E, 4)))
+        if case == "repeated":
+            conn[:, 2] = conn[:, 0]
+        ok, ptr, nodes, code, rank = _library_plan(exe, tmp_path, conn)
+        assert ok and ptr[0] == 0 and ptr.size == (E + 31) // 32 + 1
+        cb, rb = _bytes(code).reshape(-1, 128), _bytes(rank).reshape(-1, 128)
+        for c in range(ptr.size - 1):
+            codes, ranks, order = chunk_plan(conn, c)
+            assert list(nodes[ptr[c]:ptr[c + 1]]) == order, (case, c)
+            assert np.array_equal(cb[c], codes.reshape(-1)) and np.array_equal(rb[c], ranks.reshape(-1)), (case, c)
+
+
+def test_library_plan_builder_refuses_chunks_beyond_rank_bytes(tmp_path):
+    """Eight-node elements with no shared nodes put 256 distinct nodes in a chunk, more than
+    the rank bytes hold: the builder reports failure (the block then keeps one slot per
+    element node)."""
+    exe = _build_dump(tmp_path)
+    conn = np.arange(32 * 8, dtype=np.int32).reshape(32, 8)
+    ok, *_ = _library_plan(exe, tmp_path, conn)
+    assert not ok
+    ok, *_ = _library_plan(exe, tmp_path, conn[:, :4].copy())
+    assert ok
